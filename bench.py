@@ -1,0 +1,411 @@
+"""Benchmark of the probe-particle AFM hot path on B200.
+
+Step = one pass of the plain path over one synthetic system: (a) LJ + Coulomb
+force-grid build, (b) FIRE relaxation of every pixel down its z-stroke
+(relaxStrokes semantics, <= 1000 steps, |F| < 1e-5 eV/A), (c) 9-point
+finite-amplitude df at every height.  Workload: 1140-ion NaCl(100) slab +
+60-atom molecule (1200 atoms), grid 480x480x240 (48x48x24 A at 0.1 A), 480x480
+pixels x 60 z-steps (synthetic, seeded; see spammm_b200/synthetic.py).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` = px*z per second of the whole step
+with inputs resident in HBM (CUDA events around the K timed steps, max over
+ranks); `e2e` = the same through the drop-in AFMulator API with host buffers
+(uploads and downloads inside the timed region).  Under torchrun each rank runs
+its own replica of the workload (the path has no exchange step).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "probe relax px·z/s; batched fwd+adjoint images/s vs plain, Δf err≤1e-3"
+UNIT = "px·z/s"
+# algorithmic work per (node, atom) pair, FMA = 2 flops: LJ 26, Morse 28, +23 per non-zero tip-charge site
+FLOPS_PAIR = {0: 26, 1: 28}
+FLOPS_SITE = 23
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="plain_large", choices=["plain_large", "plain_small"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def make_config(name):
+    from spammm_b200 import synthetic
+    return synthetic.plain_large() if name == "plain_large" else synthetic.plain_small()
+
+
+def config_dict(cfg, l2_note):
+    return {"workload": f"{cfg.name}: {len(cfg.atoms)} atoms, grid {'x'.join(map(str, cfg.ngrid))} at "
+                        f"{cfg.step} A, {len(cfg.scan_xs)}x{len(cfg.scan_ys)} px x {cfg.nz} z, FIRE<= {cfg.max_iter}, "
+                        f"|F|<{np.sqrt(cfg.f2conv):.0e} eV/A, df amp {cfg.amp} A",
+            "atoms": int(len(cfg.atoms)), "grid": list(cfg.ngrid), "pixels": [len(cfg.scan_xs), len(cfg.scan_ys)],
+            "nz": cfg.nz, "potential": "LJ" if cfg.kind == 0 else "Morse", "l2": l2_note}
+
+
+def grid_vectors(cfg):
+    o = cfg.origin
+    p0 = np.array([o[0], o[1], o[2], 0], np.float32)
+    s = cfg.step
+    return p0, np.array([s, 0, 0, 0], np.float32), np.array([0, s, 0, 0], np.float32), np.array([0, 0, s, 0],
+                                                                                                np.float32)
+
+
+def scan_points(cfg):
+    gx, gy = np.meshgrid(cfg.scan_xs, cfg.scan_ys, indexing="ij")
+    pts = np.zeros((cfg.n_pix, 4), np.float32)
+    pts[:, 0] = gx.ravel()
+    pts[:, 1] = gy.ravel()
+    pts[:, 2] = np.float32(cfg.z_top)
+    return pts
+
+
+def scan_params(cfg, dinv):
+    from spammm_b200 import _lib
+    return _lib.make_scan_params(dinv=dinv, dTip=[0, 0, -cfg.dz, 0], stiffness=cfg.stiffness, dpos0=cfg.dpos0,
+                                 relax_params=[0.5, 0.1, 0.02, 0.5], nz=cfg.nz, max_iter=cfg.max_iter,
+                                 f2conv=cfg.f2conv, fire=True, flip_z=True, raster_ny=len(cfg.scan_ys))
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+# ---------------------------------------------------------------------------- CPU (oracle) sample
+def cpu_sample(cfg, threads=None):
+    """Times the oracle port (C restatement, OpenMP) on a bounded sample of the
+    workload and extrapolates to the full step.  Returns (px*z/s, details)."""
+    from oracle import oracle as O
+    if threads:
+        O.set_num_threads(threads)
+    nthreads = O.num_threads()
+    p0, dA, dB, dC = grid_vectors(cfg)
+    # (a) grid build: a slab of nodes spanning the probe heights, timed and scaled by node count
+    nx, ny, nz = cfg.ngrid
+    n_nodes = min(nx * ny * nz, max(nx * 8, int(3e8 / max(len(cfg.atoms), 1)) // 1))
+    iz0 = int((cfg.z_top - cfg.origin[2]) / cfg.step) - 2
+    node0 = max(0, iz0) * nx * ny
+    t0 = time.perf_counter()
+    O.grid_build(cfg.kind, cfg.atoms, cfg.params, cfg.ngrid, p0, dA, dB, dC, cfg.tipQs, cfg.tipQZs, prec="f32",
+                 node0=node0, nnodes=n_nodes)
+    t_grid = (time.perf_counter() - t0) * (nx * ny * nz) / n_nodes
+    # (b) relaxation of a pixel patch on a CPU-built sub-grid around it
+    patch = 24
+    cx, cy = len(cfg.scan_xs) // 2, len(cfg.scan_ys) // 2
+    xs = cfg.scan_xs[cx - patch // 2: cx + patch // 2]
+    ys = cfg.scan_ys[cy - patch // 2: cy + patch // 2]
+    margin = 3.0
+    sx0 = float(xs[0]) - margin
+    sy0 = float(ys[0]) - margin
+    sz0 = cfg.z_top - cfg.dz * cfg.nz - 1.5
+    snx = int(np.ceil((float(xs[-1]) - float(xs[0]) + 2 * margin) / cfg.step)) + 1
+    sny = int(np.ceil((float(ys[-1]) - float(ys[0]) + 2 * margin) / cfg.step)) + 1
+    snz = int(np.ceil((cfg.z_top + 1.5 - sz0) / cfg.step)) + 1
+    sp0 = np.array([sx0, sy0, sz0, 0], np.float32)
+    t0 = time.perf_counter()
+    sub = O.grid_build(cfg.kind, cfg.atoms, cfg.params, (snx, sny, snz), sp0, dA, dB, dC, cfg.tipQs, cfg.tipQZs,
+                       prec="f32")
+    t_sub = time.perf_counter() - t0
+    L = np.array([snx, sny, snz]) * cfg.step
+    dinv = O.dinv_axis_aligned(L, sp0[:3], (snx, sny, snz))
+    gx, gy = np.meshgrid(xs, ys, indexing="ij")
+    pts = np.zeros((gx.size, 4), np.float32)
+    pts[:, 0], pts[:, 1], pts[:, 2] = gx.ravel(), gy.ravel(), cfg.z_top
+    t0 = time.perf_counter()
+    FEs, _ = O.relax_strokes(sub, dinv, pts, cfg.nz, [0, 0, -cfg.dz, 0], cfg.stiffness, cfg.dpos0,
+                             [0.5, 0.1, 0.02, 0.5], cfg.max_iter, cfg.f2conv, True, True)
+    t_relax = (time.perf_counter() - t0) * cfg.n_pix / pts.shape[0]
+    # (c) df on the patch volume
+    t0 = time.perf_counter()
+    O.compute_df_amp_dir(FEs.reshape(len(xs), len(ys), cfg.nz, 4), (cfg.step, cfg.step, cfg.dz), (0, 0, 1), cfg.amp)
+    t_df = (time.perf_counter() - t0) * cfg.n_pix / pts.shape[0]
+    total = t_grid + t_relax + t_df
+    det = {"kind": "port", "cores": int(nthreads),
+           "sample": f"oracle C/OpenMP FP32: grid build of {n_nodes} of {nx * ny * nz} nodes, relaxation of a "
+                     f"{len(xs)}x{len(ys)}-pixel patch on a {snx}x{sny}x{snz} sub-grid ({t_sub:.2f} s), numpy df on "
+                     f"the patch; extrapolated by node/pixel counts",
+           "stage_s": {"grid": t_grid, "relax": t_relax, "df": t_df}}
+    return cfg.pxz / total, det
+
+
+# ---------------------------------------------------------------------------- GPU arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from spammm_b200 import gpu, _lib, AFM
+    from spammm_b200.AFM import AFMulator
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    cfg = make_config(args.config)
+    nx, ny, nz = cfg.ngrid
+    p0, dA, dB, dC = grid_vectors(cfg)
+    L = np.array(cfg.ngrid) * cfg.step
+    dinv = AFMulator._make_dinv_axis_aligned(L, cfg.origin.astype(np.float32), cfg.ngrid)
+    P = scan_params(cfg, dinv)
+    atoms_d = torch.from_numpy(cfg.atoms).to(dev)
+    prm_d = torch.from_numpy(cfg.params).to(dev)
+    pts_d = torch.from_numpy(scan_points(cfg)).to(dev)
+    grid = torch.empty((nz, ny, nx, 4), dtype=torch.float32, device=dev)
+    FEs = torch.empty((cfg.n_pix, cfg.nz, 4), dtype=torch.float32, device=dev)
+    disps = torch.empty_like(FEs)
+    npx, npy = len(cfg.scan_xs), len(cfg.scan_ys)
+    spacing = (cfg.step, cfg.step, cfg.dz)
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    stage = np.zeros(3)
+
+    def step(record):
+        if record:
+            ev[0].record(stream)
+        gpu.grid_build(cfg.kind, atoms_d, prm_d, cfg.ngrid, p0, dA, dB, dC, cfg.tipQs, cfg.tipQZs, out=grid)
+        if record:
+            ev[1].record(stream)
+        gpu.relax_strokes(grid, P, pts_d, FEs=FEs, disps=disps)
+        if record:
+            ev[2].record(stream)
+        df = gpu.df_amp_dir(FEs.view(npx, npy, cfg.nz, 4), spacing, (0, 0, 1), cfg.amp)
+        if record:
+            ev[3].record(stream)
+        return df
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for _ in range(args.steps):
+        step(True)
+        stream.synchronize()
+        stage += [ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3])]
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms_total = t0.elapsed_time(t1)
+    stage /= args.steps
+    if world > 1:
+        t = torch.tensor([ms_total], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    # the events above wrap each stage; the sum of stages is the kernel time of a step (host syncs excluded)
+    value = world * cfg.pxz / (ms_step * 1e-3)
+    iters = None
+    out = {}
+
+    # ---- e2e through the drop-in API (host buffers)
+    e2e = None
+    if not args.no_e2e:
+        afm = AFMulator(use_morse=(cfg.kind == 1))
+        afm.n_relax_max, afm.f2conv = cfg.max_iter, cfg.f2conv
+        afm.tipQs, afm.tipQZs = cfg.tipQs, cfg.tipQZs
+
+        def e2e_step():
+            afm.atoms_arr = cfg.atoms.copy()
+            afm.cLJs_arr = cfg.params.copy()
+            afm.setup_grid_world(cfg.origin, L, cfg.ngrid)
+            afm.make_forcefield()
+            afm.setup_fdbm_grid_from_img(afm.img_FF, cfg.ngrid, cfg.origin, cfg.step)
+            hs = (cfg.z_top - cfg.dz * np.arange(cfg.nz)[::-1]).astype(np.float32)
+            F, disp = afm.scan_fdbm(cfg.scan_xs, cfg.scan_ys, hs, mol_z=0.0, bond_length=0.0,
+                                    stiffness=cfg.stiffness, dpos0=cfg.dpos0)
+            df = AFM.compute_df_amp_dir(F, spacing, (0., 0., 1.), cfg.amp)
+            return F, disp, df
+
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ke = max(1, min(args.steps, 3))
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(ke):
+            F, disp, df_h = e2e_step()
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ms_e = a0.elapsed_time(a1)
+        if world > 1:
+            t = torch.tensor([ms_e], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms_e = float(t.item())
+        h2d = cfg.atoms.nbytes + cfg.params.nbytes + cfg.n_pix * 16 + F.nbytes  # atoms, params, points, FEs for df
+        d2h = F.nbytes + 3 * F[..., 0].nbytes + df_h.nbytes  # FEs, tip displacement, df
+        e2e = {"value": world * cfg.pxz / (ms_e / ke * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e / ke,
+               "path": "AFMulator.setup_grid_world/make_forcefield/scan_fdbm + compute_df_amp_dir (numpy in/out)"}
+
+    # ---- roofline of the dominant kernel
+    peaks = measured_peaks()
+    fp32_peak = gpu.fp32_peak_flops(1 << 15)
+    ns = int(np.count_nonzero(cfg.tipQs))
+    flops = cfg.pairs * (FLOPS_PAIR[cfg.kind] + FLOPS_SITE * ns)
+    ach_fp32 = flops / (stage[0] * 1e-3)
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    slab_nodes = nx * ny * (int(np.ceil((cfg.dz * cfg.nz + 2.0) / cfg.step)) + 2)
+    relax_bytes = cfg.pxz * 32 + slab_nodes * 16
+    ach_relax = relax_bytes / (stage[1] * 1e-3) / 1e9
+    df_bytes = cfg.pxz * (16 + 4)
+    names = ["grid_build_kernel", "relax_kernel<0>", "df_amp_dir_kernel"]
+    dom = int(np.argmax(stage))
+    if dom == 0:
+        roof = {"kernel": names[0], "bound": "fp32", "achieved": ach_fp32 / 1e12, "peak": fp32_peak / 1e12,
+                "unit": "TFLOP/s", "frac": ach_fp32 / fp32_peak, "traffic": None,
+                "peak_source": "measured live: FFMA-chain probe (spm_fp32_peak_probe) on this GPU",
+                "algorithmic": f"{cfg.pairs:.3e} (node,atom) pairs x {FLOPS_PAIR[cfg.kind] + FLOPS_SITE * ns} "
+                               f"flops"}
+    else:
+        roof = {"kernel": names[dom], "bound": "hbm", "achieved": ach_relax if dom == 1 else
+                df_bytes / (stage[2] * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s", "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback"}
+        roof["frac"] = roof["achieved"] / hbm_peak
+    out.update(stage_ms={"grid_build": stage[0], "relax": stage[1], "df": stage[2]},
+               stage_roofline={"grid_build_tflops": ach_fp32 / 1e12, "fp32_peak_tflops": fp32_peak / 1e12,
+                               "relax_alg_gbs": ach_relax, "relax_alg_bytes": relax_bytes,
+                               "df_alg_gbs": df_bytes / (stage[2] * 1e-3) / 1e9})
+    if rank != 0:
+        return None
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded NaCl slab + planar molecule)",
+            "config": config_dict(cfg, "inputs larger than L2 (grid 885 MB) -- no flush needed"),
+            "roofline": roof, "gpu_launches": 3 * args.steps, "clocks": clk, "e2e": e2e}
+    line.update(out)
+    line["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
+    if not args.no_cpu and world == 1:
+        v, det = cpu_sample(cfg)
+        det["value"] = v
+        det["unit"] = UNIT
+        line["cpu_baseline"] = det
+    return line
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    cfg = make_config(args.config)
+    for _ in range(args.warmup):
+        cpu_sample(cfg)
+    vals = []
+    dets = None
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, dets = cpu_sample(cfg)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    value = float(np.median(vals))
+    dets["value"] = value
+    dets["unit"] = UNIT
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": cfg.pxz / value * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded NaCl slab + planar molecule)",
+            "config": config_dict(cfg, "CPU"), "impl": "reference", "cpu_baseline": dets,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's path is PyOpenCL (no OpenCL platform here); this arm times the C/OpenMP "
+                    f"restatement of its kernels on the host cores; wall {wall:.1f} s"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        if world > 1:
+            import datetime
+            import torch
+            torch.cuda.set_device(local_rank)
+            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        line = run_ours(args, rank, world, local_rank)
+        if world > 1:
+            import torch
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,199 @@
+/*
+ * spm_b200.h -- C ABI of libspmb200.so, the sm_100a implementation of
+ * SPAMMM's probe-particle AFM hot path:
+ *   (a) force-grid build, (b) FIRE probe relaxation down z-strokes,
+ *   (c) Fz -> df conversion, plus the grid-free direct Morse path and its
+ *   implicit-function adjoint.
+ *
+ * Conventions (identical to the reference's OpenCL buffers/images):
+ *   - every pointer argument is a DEVICE pointer unless the comment says
+ *     "host"; float4 arrays are (n,4) float32 rows, C order;
+ *   - the force grid is (nz,ny,nx,4) float32, x fastest, channels
+ *     (Fx,Fy,Fz,E): the layout of the reference's RGBA float image3d_t;
+ *   - scan points are (n_scan,4) float32 rows (x,y,z,0), raster ix-major
+ *     (spammm/SPM/AFM.py:82-95); per-state outputs are (n_scan,nz,4), iz=0 at
+ *     the first (highest) tip position unless SPM_FLAG_FLIP_Z is set;
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream); every call
+ *     is asynchronous on that stream and allocates no device memory unless a
+ *     comment says otherwise;
+ *   - every function returns SPM_OK (0) or an SPM_ERR_* code and leaves a
+ *     message for spm_last_error() (thread-local).
+ */
+#ifndef SPM_B200_H
+#define SPM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPM_ABI_VERSION 1
+
+enum spm_status {
+    SPM_OK = 0,
+    SPM_ERR_ARG = 1,          /* null pointer, non-positive size, size overflow, bad flag */
+    SPM_ERR_CUDA = 2,         /* CUDA launch or runtime error (text in spm_last_error) */
+    SPM_ERR_UNSUPPORTED = 3,  /* input outside a kernel's stated limits (e.g. atom count) */
+    SPM_ERR_TIMEOUT = 4       /* a bounded device-side wait gave up */
+};
+
+/* Potential kinds for the grid build / pair law. */
+#define SPM_KIND_LJ    0      /* params (na,2) = (c6, c12)          AFM.cl:738-745 */
+#define SPM_KIND_MORSE 1      /* params (na,4) = (R0, E0, K<0, 0)    AFM.cl:747-757 */
+
+/* Element type of (n,4) FE volumes accepted by the df functions. */
+#define SPM_F32 0
+#define SPM_F64 1
+
+/* spm_scan_params.flags */
+#define SPM_FLAG_FIRE   1     /* FIRE integrator (OPT_FIRE=1); else plain damping (OPT_FIRE=0) */
+#define SPM_FLAG_FLIP_Z 2     /* store iz reversed: the z flip AFMulator.scan_fdbm applies (AFM.py:627-633) */
+
+/* Scan/tip parameters shared by the relaxation and sampling kernels.  Field
+ * names follow the reference's kernel arguments (kernels/AFM.cl:345-562). */
+typedef struct spm_scan_params {
+    float dinvA[4], dinvB[4], dinvC[4];  /* world -> normalized grid coordinate (.w = -o/L + 0.5/n) */
+    float tipA[4], tipB[4], tipC[4];     /* tip frame rows; tipC[3] = dtip for the tilted kernels */
+    float dTip[4];                       /* per-z tip step for relaxStrokes / raw sampling */
+    float stiffness[4];                  /* (kx,ky,kz,k_radial) eV/A^2, negative = restoring */
+    float dpos0[4];                      /* probe rest offset (xyz) and radial bond length (w) */
+    float relax_params[4];               /* (dt, damp, -, -) */
+    float surfFF[4];                     /* surface bias along tipC (x) */
+    int   nz;                            /* z-steps per stroke */
+    int   max_iter;                      /* integrator steps per z-step (reference: N_RELAX_STEP_MAX=128) */
+    float f2conv;                        /* |F|^2 convergence threshold (reference: F2CONV=1e-8) */
+    int   flags;                         /* SPM_FLAG_* */
+    int   raster_ny;                     /* >0: points form an ix-major (n_scan/raster_ny, raster_ny)
+                                            raster; lets the kernels give each warp a compact
+                                            4x8 pixel block (results do not depend on it) */
+} spm_scan_params;
+
+/* Library/ABI identification. */
+int spm_abi_version(void);
+/* Last error message of the calling thread ("" if none). */
+const char* spm_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * (a) Force-grid build.
+ * Replaces AFMulator.make_forcefield (spammm/SPM/AFM.py:897-946) ->
+ * evalLJC_QZs_toImg (kernels/AFM.cl:916-991) / evalMorseC_QZs_toImg
+ * (kernels/AFM.cl:996-1056).  Node (ia,ib,ic) sits at p0 + dA*ia + dB*ib +
+ * dC*ic; value = sum over atoms of the LJ or Morse pair law plus the Coulomb
+ * law at the four tip-charge sites node + zhat*QZs[k] weighted by
+ * Qs[k]*14.3996448915; nodes with |E| > 100 are rescaled by 100/|E|.
+ *   atoms  (n_atoms,4) = (x,y,z,Q);  params per SPM_KIND_*;
+ *   p0,dA,dB,dC,Qs,QZs: HOST float[4];  grid out (nz,ny,nx,4).
+ * Requires dC = (0,0,dz) (true for every reference grid constructor). */
+int spm_grid_build(int kind, int n_atoms, const float* atoms, const float* params,
+                   float* grid, int nx, int ny, int nz,
+                   const float* p0, const float* dA, const float* dB, const float* dC,
+                   const float* Qs, const float* QZs, void* stream);
+
+/* ------------------------------------------------------------------------
+ * (b) Probe relaxation on the grid.
+ * spm_relax_strokes replaces AFMulator.scan_fdbm's launch of relaxStrokes
+ * (spammm/SPM/AFM.py:607-617 -> kernels/AFM.cl:345-394): per pixel and z-step,
+ * up to max_iter integrator steps on the trilinearly sampled grid force plus
+ * tipForce; stores the last in-loop sample FE and the displacement
+ * pos - (tipPos + dpos0).  Uses p->dTip, ignores the tip frame.
+ *   FEs, disps out: (n_scan, p->nz, 4). */
+int spm_relax_strokes(const float* grid, int nx, int ny, int nz,
+                      const float* points, int n_scan, const spm_scan_params* p,
+                      float* FEs, float* disps, void* stream);
+
+/* Replaces AFMulator.run_scan -> relaxStrokesTilted (spammm/SPM/AFM.py:950-1010,
+ * kernels/AFM.cl:478-562): tip-frame spring, surface bias, re-sampled FE after
+ * the loop, output rotated into the tip frame.  dtip = p->tipC[3]. */
+int spm_relax_strokes_tilted(const float* grid, int nx, int ny, int nz,
+                             const float* points, int n_scan, const spm_scan_params* p,
+                             float* FEs, void* stream);
+
+/* Replaces AFMulator.get_raw_FE -> getFEinStrokesTilted (spammm/SPM/AFM.py:2523-2580,
+ * kernels/AFM.cl:210-233): unrelaxed samples at point + dpos0 + iz*dTip,
+ * rotated into the tip frame. */
+int spm_fe_in_strokes_tilted(const float* grid, int nx, int ny, int nz,
+                             const float* points, int n_scan, const spm_scan_params* p,
+                             float* FEs, void* stream);
+
+/* ------------------------------------------------------------------------
+ * (c) Frequency shift.  FE volumes are (nx,ny,nz,4) float32 or float64
+ * (fes_dtype = SPM_F32 / SPM_F64), as the reference's NumPy functions accept
+ * either.
+ * spm_df_amp_dir replaces compute_df_amp_dir (spammm/SPM/AFM.py:3203-3236):
+ * F_n = F.n on the (nx,ny,nz,4) volume FEs (iz=0 lowest), 9-point
+ * Gauss-Chebyshev average of -d(F_n)/ds over the oscillation s in [-amp,amp]
+ * (linear interpolation with clamped indices, numpy.gradient differences),
+ * evaluated in FP64.  n, dr: HOST double[3] (n normalised by the caller,
+ * dr = grid spacing).  out_iz: DEVICE int[n_out] list of z indices to emit
+ * (NULL = all nz, n_out ignored; an index outside [0,nz) yields NaN).
+ * df out: (nx,ny,n_out) float32. */
+int spm_df_amp_dir(const void* FEs, int fes_dtype, int nx, int ny, int nz, const double* n,
+                   const double* dr, double amp, const int* out_iz, int n_out, float* df, void* stream);
+
+/* Replaces compute_df_dir (spammm/SPM/AFM.py:3105-3123): df = -n.grad(F.n)
+ * without amplitude averaging; df out (nx,ny,nz) float64. */
+int spm_df_dir(const void* FEs, int fes_dtype, int nx, int ny, int nz, const double* n,
+               const double* dr, double* df, void* stream);
+
+/* Replaces compute_dissipation (spammm/SPM/AFM.py:3238-3277): for each output
+ * height i, |trapz over the index list idx[off[i]..off[i+1]) of
+ * (F_fwd - F_bwd).n dz| with abscissae h_scan.  n: HOST double[3];
+ * h_scan (DEVICE double[nz]), off (DEVICE int[n_out+1]), idx (DEVICE int[]);
+ * an index outside [0,nz) yields NaN.  E out (nx,ny,n_out) float32. */
+int spm_dissipation(const void* FEs_fwd, const void* FEs_bwd, int fes_dtype, int nx, int ny, int nz,
+                    const double* n, const double* h_scan, const int* off, const int* idx,
+                    int n_out, float* E_diss, void* stream);
+
+/* Replaces df_loss_seed (spammm/SPM/AFM.py:3125-3200): central-difference df of
+ * Fz = FEs[...,2] with |dtip|, L = 0.5*sum(w (df - target)^2)/sum(w) and the
+ * exact transpose dL/dFEs (only the z channel non-zero).  target, weights
+ * (nx,ny,nz) float64 (weights NULL = 1 inside, 0 on the two boundary slices);
+ * df_out (nx,ny,nz) f64, dL_dFEs (nx,ny,nz,4) f32, loss_out: device double[1].
+ * Uses `scratch` (device, >= spm_df_loss_scratch_bytes(nx,ny,nz) bytes). */
+int spm_df_loss_seed(const void* FEs, int fes_dtype, const double* target, const double* weights,
+                     int nx, int ny, int nz, double dtip, double* df_out, float* dL_dFEs,
+                     double* loss_out, void* scratch, void* stream);
+long long spm_df_loss_scratch_bytes(int nx, int ny, int nz);
+
+/* ------------------------------------------------------------------------
+ * Differentiable grid-free Morse+Coulomb path.
+ * spm_relax_direct_morse replaces AFMulator.run_scan_morse_direct
+ * (spammm/SPM/AFM.py:2063-2233) -> relaxStrokesTiltedMorseDirect
+ * (kernels/AFM.cl:1419-1511): uncapped direct pair sum, convergence tested
+ * before each update, PPs = (pos, +iters converged / -iters not).
+ * atoms (n_atoms,4), cMs (n_atoms,4) = (R0,E0,K,0); Qs,QZs HOST float[4];
+ * FEs, PPs out (n_scan,nz,4).  1 <= n_atoms <= SPM_DIRECT_MAX_ATOMS. */
+#define SPM_DIRECT_MAX_ATOMS 4096
+int spm_relax_direct_morse(int n_atoms, const float* atoms, const float* cMs,
+                           const float* points, int n_scan, const spm_scan_params* p,
+                           const float* Qs, const float* QZs,
+                           float* FEs, float* PPs, void* stream);
+
+/* Replaces morseDirectStateAdjoint (kernels/AFM.cl:1711-1845): per state the
+ * implicit-function adjoint J lambda = b at the stored PP; lambdas (n_state,4),
+ * diag (n_state,4) = (residual, lambda_min, cond, status 0..4). */
+int spm_adjoint_direct_state(int n_atoms, const float* atoms, const float* cMs,
+                             const float* points, int n_scan, const spm_scan_params* p,
+                             const float* Qs, const float* QZs, const float* PPs,
+                             const float* dL_dFEs, float* lambdas, float* diag, void* stream);
+
+/* Replaces morseDirectParamPartials + reduceMorseDirectParamPartials
+ * (kernels/AFM.cl:1850-2029): grad (n_atoms,6) float32 = per-atom
+ * d(loss)/d(x,y,z,R0,E0,Q), reduced deterministically (no atomics) through
+ * `scratch` (device, >= spm_adjoint_direct_scratch_bytes(...) bytes). */
+int spm_adjoint_direct_params(int n_atoms, const float* atoms, const float* cMs,
+                              const float* points, int n_scan, const spm_scan_params* p,
+                              const float* Qs, const float* QZs, const float* PPs,
+                              const float* dL_dFEs, const float* lambdas,
+                              float* grad, void* scratch, void* stream);
+long long spm_adjoint_direct_scratch_bytes(int n_atoms, int n_scan);
+
+/* ------------------------------------------------------------------------
+ * Measurement helper (not part of the reference interface): runs a dependent
+ * FFMA chain on every SM and writes the achieved FP32 FLOP/s to *out_flops
+ * (host double).  Blocking. */
+int spm_fp32_peak_probe(int iters, double* out_flops, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPM_B200_H */

@@ -1,0 +1,71 @@
+// capi.cu -- library-wide C ABI pieces: error text, ABI version and the FP32
+// peak probe used as the denominator of the grid-build roofline.
+#include "spm_internal.cuh"
+#include <cstring>
+
+namespace spm {
+
+static thread_local char g_last_error[1024] = {0};
+
+int set_error(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+void clear_error() { g_last_error[0] = 0; }
+
+namespace {
+
+constexpr int PROBE_CHAINS = 8;
+
+// PROBE_CHAINS independent FFMA chains per thread; FLOPs = 2 * chains * iters.
+__global__ void __launch_bounds__(256) fp32_probe_kernel(int iters, float seed, float* sink) {
+    float a[PROBE_CHAINS];
+#pragma unroll
+    for (int c = 0; c < PROBE_CHAINS; c++) a[c] = seed + (float)(threadIdx.x + c);
+    const float m = 0.999999f, b = 1e-7f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int c = 0; c < PROBE_CHAINS; c++) a[c] = fmaf(a[c], m, b);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < PROBE_CHAINS; c++) s += a[c];
+    if (s == 1234.5678f) sink[0] = s;  // never true for this seed: keeps the chains live
+}
+
+}  // namespace
+}  // namespace spm
+
+extern "C" int spm_abi_version(void) { return SPM_ABI_VERSION; }
+
+extern "C" const char* spm_last_error(void) { return spm::g_last_error; }
+
+extern "C" int spm_fp32_peak_probe(int iters, double* out_flops, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(iters > 0 && out_flops, "spm_fp32_peak_probe: iters must be > 0 and out_flops non-null");
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return set_error(SPM_ERR_CUDA, "spm_fp32_peak_probe: cannot query the device");
+    cudaStream_t st = as_stream(stream);
+    const int blocks = sms * 8, threads = 256;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    fp32_probe_kernel<<<blocks, threads, 0, st>>>(iters / 4, 1.0f, nullptr);  // warm-up
+    cudaEventRecord(e0, st);
+    fp32_probe_kernel<<<blocks, threads, 0, st>>>(iters, 1.0f, nullptr);
+    cudaEventRecord(e1, st);
+    cudaError_t err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (err != cudaSuccess) return set_error(SPM_ERR_CUDA, "spm_fp32_peak_probe: %s", cudaGetErrorString(err));
+    *out_flops = 2.0 * PROBE_CHAINS * (double)iters * blocks * threads / (ms * 1e-3);
+    return SPM_OK;
+}

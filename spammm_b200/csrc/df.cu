@@ -1,0 +1,411 @@
+// df.cu -- stage (c): frequency shift, dissipation and the df loss seed.
+//
+// Replaces the host NumPy/SciPy post-processing of SPAMMM:
+//   compute_df_amp_dir  spammm/SPM/AFM.py:3203-3236 (9-point Gauss-Chebyshev,
+//                       scipy.ndimage.map_coordinates(order=1, mode='nearest'),
+//                       numpy.gradient with edge_order=1)
+//   compute_df_dir      spammm/SPM/AFM.py:3105-3123
+//   compute_dissipation spammm/SPM/AFM.py:3238-3277
+//   df_loss_seed        spammm/SPM/AFM.py:3125-3200
+// All arithmetic is FP64, as on the reference host.  The FEs volume is
+// (nx,ny,nz,4) float32 with z fastest; these kernels are HBM/L2 bound (a few
+// reads of one float4 per output element), one thread per output element.
+// Compiled with -fmad=false so the FP64 expression order matches NumPy's.
+#include "spm_internal.cuh"
+#include <cmath>
+#include <vector>
+
+namespace spm {
+namespace {
+
+constexpr int DF_THREADS = 256;
+constexpr int NQ = 9;  // Gauss-Chebyshev nodes
+
+struct DfGeom {
+    int nx, ny, nz;
+    double n[3];       // oscillation direction (unit)
+    double dr[3];      // spacing
+    double shift[3];   // amp * n / dr
+    double uk[NQ];     // cos((2k+1) pi / 18)
+    double wk;         // 1/9
+    int act[3];        // active axes (|n| > 1e-15)
+    int nact;
+};
+
+// One (Fx,Fy,Fz,E) row of an FP32 or FP64 volume, widened to double.
+struct Row {
+    double x, y, z, w;
+};
+__device__ __forceinline__ Row load_row(const float* __restrict__ v, size_t i) {
+    const float4 f = __ldg(reinterpret_cast<const float4*>(v) + i);
+    return Row{(double)f.x, (double)f.y, (double)f.z, (double)f.w};
+}
+__device__ __forceinline__ Row load_row(const double* __restrict__ v, size_t i) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(v) + 2 * i);
+    const double2 b = __ldg(reinterpret_cast<const double2*>(v) + 2 * i + 1);
+    return Row{a.x, a.y, b.x, b.y};
+}
+
+template <typename T>
+__device__ __forceinline__ double fn_at(const T* __restrict__ FEs, const DfGeom& P, int ix, int iy, int iz) {
+    const Row f = load_row(FEs, ((size_t)ix * P.ny + iy) * P.nz + iz);
+    return (f.x * P.n[0] + f.y * P.n[1]) + f.z * P.n[2];
+}
+
+__device__ __forceinline__ int clampi(int i, int n) { return i < 0 ? 0 : (i >= n ? n - 1 : i); }
+
+// map_coordinates(F_n, (ix,iy,iz) + u*shift, order=1, mode='nearest'):
+// per-axis weights (1-t, t) at floor(c), clamped indices, corners summed with
+// the last axis fastest and each term formed as ((f*w0)*w1)*w2.
+template <typename T>
+__device__ double shifted_fn(const T* __restrict__ FEs, const DfGeom& P, int ix, int iy, int iz, double u) {
+    const int dims[3] = {P.nx, P.ny, P.nz};
+    const int idx[3] = {ix, iy, iz};
+    int i0[3];
+    double w[3][2];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double c = (double)idx[d] + u * P.shift[d];
+        const double fl = floor(c);
+        const double t = c - fl;
+        i0[d] = (int)fl;
+        w[d][0] = 1.0 - t;
+        w[d][1] = t;
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int a0 = 0; a0 < 2; a0++) {
+        if (w[0][a0] == 0.0) continue;
+#pragma unroll
+        for (int a1 = 0; a1 < 2; a1++) {
+            if (w[1][a1] == 0.0) continue;
+#pragma unroll
+            for (int a2 = 0; a2 < 2; a2++) {
+                if (w[2][a2] == 0.0) continue;
+                double coeff = fn_at(FEs, P, clampi(i0[0] + a0, dims[0]), clampi(i0[1] + a1, dims[1]),
+                                     clampi(i0[2] + a2, dims[2]));
+                coeff *= w[0][a0];
+                coeff *= w[1][a1];
+                coeff *= w[2][a2];
+                acc += coeff;
+            }
+        }
+    }
+    return acc;
+}
+
+// numpy.gradient(S, dr, axis) at one point, uniform spacing, edge_order=1.
+template <bool AMP, typename T>
+__device__ double grad_at(const T* __restrict__ FEs, const DfGeom& P, int ax, int ix, int iy, int iz, double u) {
+    const int dims[3] = {P.nx, P.ny, P.nz};
+    int idx[3] = {ix, iy, iz};
+    const int i = idx[ax], n = dims[ax];
+    auto S = [&](int j) {
+        int q[3] = {idx[0], idx[1], idx[2]};
+        q[ax] = j;
+        return AMP ? shifted_fn(FEs, P, q[0], q[1], q[2], u) : fn_at(FEs, P, q[0], q[1], q[2]);
+    };
+    if (i == 0) return (S(1) - S(0)) / P.dr[ax];
+    if (i == n - 1) return (S(n - 1) - S(n - 2)) / P.dr[ax];
+    return (S(i + 1) - S(i - 1)) / (2.0 * P.dr[ax]);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(DF_THREADS)
+df_amp_dir_kernel(const T* __restrict__ FEs, DfGeom P, const int* __restrict__ out_iz, int n_out,
+                  float* __restrict__ df) {
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)P.nx * P.ny * n_out;
+    if (gid >= total) return;
+    const int o = (int)(gid % n_out);
+    const long long pix = gid / n_out;
+    const int iy = (int)(pix % P.ny), ix = (int)(pix / P.ny);
+    const int iz = out_iz ? out_iz[o] : o;
+    if (iz < 0 || iz >= P.nz) {  // invalid selection: flag the element instead of reading out of bounds
+        df[gid] = __int_as_float(0x7fc00000);
+        return;
+    }
+    double acc = 0.0;
+    for (int k = 0; k < NQ; k++) {
+        for (int a = 0; a < P.nact; a++) {
+            const int ax = P.act[a];
+            const double g = grad_at<true>(FEs, P, ax, ix, iy, iz, P.uk[k]);
+            acc -= (P.wk * P.n[ax]) * g;
+        }
+    }
+    df[gid] = (float)acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(DF_THREADS)
+df_dir_kernel(const T* __restrict__ FEs, DfGeom P, double* __restrict__ df) {
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)P.nx * P.ny * P.nz;
+    if (gid >= total) return;
+    const int iz = (int)(gid % P.nz);
+    const long long pix = gid / P.nz;
+    const int iy = (int)(pix % P.ny), ix = (int)(pix / P.ny);
+    double acc = 0.0;
+    for (int a = 0; a < P.nact; a++) {
+        const int ax = P.act[a];
+        acc -= P.n[ax] * grad_at<false>(FEs, P, ax, ix, iy, iz, 0.0);
+    }
+    df[gid] = acc;
+}
+
+struct DissGeom {
+    int nx, ny, nz, n_out;
+    double n[3];
+};
+
+// |sum_j (x[j+1]-x[j]) * (y[j] + y[j+1]) / 2| over the masked heights.
+template <typename T>
+__global__ void __launch_bounds__(DF_THREADS)
+dissipation_kernel(const T* __restrict__ Ff, const T* __restrict__ Fb, DissGeom P,
+                   const double* __restrict__ h, const int* __restrict__ off, const int* __restrict__ idx,
+                   float* __restrict__ E) {
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)P.nx * P.ny * P.n_out;
+    if (gid >= total) return;
+    const int o = (int)(gid % P.n_out);
+    const long long pix = gid / P.n_out;
+    auto dF = [&](int j) {
+        const Row a = load_row(Ff, (size_t)pix * P.nz + j), b = load_row(Fb, (size_t)pix * P.nz + j);
+        const double fa = (a.x * P.n[0] + a.y * P.n[1]) + a.z * P.n[2];
+        const double fbv = (b.x * P.n[0] + b.y * P.n[1]) + b.z * P.n[2];
+        return fa - fbv;
+    };
+    double acc = 0.0;
+    const int j0 = off[o], j1 = off[o + 1];
+    for (int t = j0; t + 1 < j1; t++) {
+        const int a = idx[t], b = idx[t + 1];
+        if (a < 0 || a >= P.nz || b < 0 || b >= P.nz) {  // invalid index list: flag, never read out of bounds
+            acc = __longlong_as_double(0x7ff8000000000000LL);
+            break;
+        }
+        acc += (h[b] - h[a]) * (dF(a) + dF(b)) / 2.0;
+    }
+    E[gid] = (float)fabs(acc);
+}
+
+// ---- df loss seed: df, per-block partial sums of w and w*(df-t)^2 ----------
+constexpr int LS_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(LS_THREADS)
+loss_partials_kernel(const T* __restrict__ FEs, const double* __restrict__ tgt, const double* __restrict__ wts,
+                     int nx, int ny, int nz, double dz2, double* __restrict__ df_out, double* __restrict__ partial) {
+    __shared__ double s_w[LS_THREADS], s_l[LS_THREADS];
+    const long long total = (long long)nx * ny * nz;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double w = 0.0, l = 0.0;
+    if (gid < total) {
+        const int iz = (int)(gid % nz);
+        double d = 0.0;
+        if (iz > 0 && iz < nz - 1) {
+            const double fp = load_row(FEs, gid + 1).z, fm = load_row(FEs, gid - 1).z;
+            d = -(fp - fm) / dz2;
+        }
+        df_out[gid] = d;
+        w = wts ? wts[gid] : ((iz > 0 && iz < nz - 1) ? 1.0 : 0.0);
+        const double diff = d - tgt[gid];
+        l = w * (diff * diff);
+    }
+    s_w[threadIdx.x] = w;
+    s_l[threadIdx.x] = l;
+    __syncthreads();
+    for (int s = LS_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            s_w[threadIdx.x] += s_w[threadIdx.x + s];
+            s_l[threadIdx.x] += s_l[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = s_w[0];
+        partial[2 * blockIdx.x + 1] = s_l[0];
+    }
+}
+
+// One CTA folds the per-block partials in a fixed order: (wsum, loss).
+__global__ void __launch_bounds__(LS_THREADS)
+loss_final_kernel(const double* __restrict__ partial, int nblk, double* __restrict__ sums, double* __restrict__ loss) {
+    __shared__ double s_w[LS_THREADS], s_l[LS_THREADS];
+    double w = 0.0, l = 0.0;
+    for (int i = threadIdx.x; i < nblk; i += LS_THREADS) {
+        w += partial[2 * i];
+        l += partial[2 * i + 1];
+    }
+    s_w[threadIdx.x] = w;
+    s_l[threadIdx.x] = l;
+    __syncthreads();
+    for (int s = LS_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            s_w[threadIdx.x] += s_w[threadIdx.x + s];
+            s_l[threadIdx.x] += s_l[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        sums[0] = s_w[0];
+        sums[1] = s_l[0];
+        loss[0] = 0.5 * s_l[0] / s_w[0];
+    }
+}
+
+// dL/dFz = transpose of the central-difference stencil applied to w*(df-t)/wsum.
+__global__ void __launch_bounds__(LS_THREADS)
+loss_grad_kernel(const double* __restrict__ df, const double* __restrict__ tgt, const double* __restrict__ wts,
+                 const double* __restrict__ sums, int nx, int ny, int nz, double coeff, float4* __restrict__ dL) {
+    const long long total = (long long)nx * ny * nz;
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= total) return;
+    const int iz = (int)(gid % nz);
+    const double wsum = sums[0];
+    auto g = [&](long long j) {
+        const int jz = (int)(j % nz);
+        const double w = wts ? wts[j] : ((jz > 0 && jz < nz - 1) ? 1.0 : 0.0);
+        return w * (df[j] - tgt[j]) / wsum;
+    };
+    double v;
+    if (iz == 0) v = g(gid + 1) * coeff;
+    else if (iz == nz - 1) v = -g(gid - 1) * coeff;
+    else v = (g(gid + 1) - g(gid - 1)) * coeff;
+    dL[gid] = make_float4(0.f, 0.f, (float)v, 0.f);
+}
+
+int fill_geom(DfGeom& P, int nx, int ny, int nz, const double* n, const double* dr, double amp) {
+    P.nx = nx; P.ny = ny; P.nz = nz;
+    P.nact = 0;
+    for (int d = 0; d < 3; d++) {
+        P.n[d] = n[d];
+        P.dr[d] = dr[d];
+        P.shift[d] = (amp * n[d]) / dr[d];
+        if (fabs(n[d]) > 1e-15) P.act[P.nact++] = d;
+    }
+    for (int k = 0; k < NQ; k++) P.uk[k] = cos((double)(2 * k + 1) / (double)(2 * NQ) * M_PI);
+    P.wk = 1.0 / NQ;
+    const int dims[3] = {nx, ny, nz};
+    for (int a = 0; a < P.nact; a++)
+        if (dims[P.act[a]] < 2)
+            return set_error(SPM_ERR_ARG, "df: FEs axis %d needs at least 2 samples for this oscillation direction",
+                             P.act[a]);
+    return SPM_OK;
+}
+
+}  // namespace
+}  // namespace spm
+
+extern "C" int spm_df_amp_dir(const void* FEs, int fes_dtype, int nx, int ny, int nz, const double* n,
+                              const double* dr, double amp, const int* out_iz, int n_out, float* df, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(FEs && df && n && dr, "spm_df_amp_dir: null pointer");
+    SPM_REQUIRE(fes_dtype == SPM_F32 || fes_dtype == SPM_F64, "spm_df_amp_dir: fes_dtype=%d", fes_dtype);
+    SPM_REQUIRE(nx > 0 && ny > 0 && nz > 0, "spm_df_amp_dir: dims (%d,%d,%d) must be positive", nx, ny, nz);
+    SPM_REQUIRE(aligned16(FEs), "spm_df_amp_dir: FEs not 16-byte aligned");
+    for (int d = 0; d < 3; d++)
+        SPM_REQUIRE(std::isfinite(n[d]) && std::isfinite(dr[d]) && dr[d] > 0.0,
+                    "spm_df_amp_dir: n/dr must be finite with dr > 0");
+    SPM_REQUIRE(std::isfinite(amp), "spm_df_amp_dir: amp must be finite");
+    DfGeom P;
+    int rc = fill_geom(P, nx, ny, nz, n, dr, amp);
+    if (rc) return rc;
+    if (out_iz == nullptr) n_out = nz;
+    SPM_REQUIRE(n_out >= 0, "spm_df_amp_dir: n_out=%d < 0", n_out);
+    const long long total = (long long)nx * ny * n_out;
+    if (total == 0) return SPM_OK;
+    const unsigned nb = (unsigned)((total + DF_THREADS - 1) / DF_THREADS);
+    if (fes_dtype == SPM_F32)
+        df_amp_dir_kernel<<<nb, DF_THREADS, 0, as_stream(stream)>>>(static_cast<const float*>(FEs), P, out_iz, n_out, df);
+    else
+        df_amp_dir_kernel<<<nb, DF_THREADS, 0, as_stream(stream)>>>(static_cast<const double*>(FEs), P, out_iz, n_out, df);
+    return check_launch("spm_df_amp_dir");
+}
+
+extern "C" int spm_df_dir(const void* FEs, int fes_dtype, int nx, int ny, int nz, const double* n, const double* dr,
+                          double* df, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(FEs && df && n && dr, "spm_df_dir: null pointer");
+    SPM_REQUIRE(fes_dtype == SPM_F32 || fes_dtype == SPM_F64, "spm_df_dir: fes_dtype=%d", fes_dtype);
+    SPM_REQUIRE(nx > 0 && ny > 0 && nz > 0, "spm_df_dir: dims (%d,%d,%d) must be positive", nx, ny, nz);
+    SPM_REQUIRE(aligned16(FEs), "spm_df_dir: FEs not 16-byte aligned");
+    for (int d = 0; d < 3; d++)
+        SPM_REQUIRE(std::isfinite(n[d]) && std::isfinite(dr[d]) && dr[d] > 0.0, "spm_df_dir: n/dr must be finite, dr > 0");
+    DfGeom P;
+    int rc = fill_geom(P, nx, ny, nz, n, dr, 0.0);
+    if (rc) return rc;
+    const long long total = (long long)nx * ny * nz;
+    const unsigned nb = (unsigned)((total + DF_THREADS - 1) / DF_THREADS);
+    if (fes_dtype == SPM_F32)
+        df_dir_kernel<<<nb, DF_THREADS, 0, as_stream(stream)>>>(static_cast<const float*>(FEs), P, df);
+    else
+        df_dir_kernel<<<nb, DF_THREADS, 0, as_stream(stream)>>>(static_cast<const double*>(FEs), P, df);
+    return check_launch("spm_df_dir");
+}
+
+extern "C" int spm_dissipation(const void* FEs_fwd, const void* FEs_bwd, int fes_dtype, int nx, int ny, int nz,
+                               const double* n, const double* h_scan, const int* off, const int* idx, int n_out,
+                               float* E_diss, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(FEs_fwd && FEs_bwd && n && h_scan && off && idx && E_diss, "spm_dissipation: null pointer");
+    SPM_REQUIRE(fes_dtype == SPM_F32 || fes_dtype == SPM_F64, "spm_dissipation: fes_dtype=%d", fes_dtype);
+    SPM_REQUIRE(nx > 0 && ny > 0 && nz > 0 && n_out >= 0, "spm_dissipation: bad dims (%d,%d,%d) n_out=%d", nx, ny, nz,
+                n_out);
+    SPM_REQUIRE(aligned16(FEs_fwd) && aligned16(FEs_bwd), "spm_dissipation: FEs not 16-byte aligned");
+    DissGeom P;
+    P.nx = nx; P.ny = ny; P.nz = nz; P.n_out = n_out;
+    for (int d = 0; d < 3; d++) P.n[d] = n[d];
+    const long long total = (long long)nx * ny * n_out;
+    if (total == 0) return SPM_OK;
+    const unsigned nb = (unsigned)((total + DF_THREADS - 1) / DF_THREADS);
+    if (fes_dtype == SPM_F32)
+        dissipation_kernel<<<nb, DF_THREADS, 0, as_stream(stream)>>>(static_cast<const float*>(FEs_fwd),
+                                                                     static_cast<const float*>(FEs_bwd), P, h_scan,
+                                                                     off, idx, E_diss);
+    else
+        dissipation_kernel<<<nb, DF_THREADS, 0, as_stream(stream)>>>(static_cast<const double*>(FEs_fwd),
+                                                                     static_cast<const double*>(FEs_bwd), P, h_scan,
+                                                                     off, idx, E_diss);
+    return check_launch("spm_dissipation");
+}
+
+extern "C" long long spm_df_loss_scratch_bytes(int nx, int ny, int nz) {
+    const long long total = (long long)nx * ny * nz;
+    if (nx <= 0 || ny <= 0 || nz <= 0) return 0;
+    const long long nblk = (total + spm::LS_THREADS - 1) / spm::LS_THREADS;
+    return (2 * nblk + 2) * (long long)sizeof(double);
+}
+
+extern "C" int spm_df_loss_seed(const void* FEs, int fes_dtype, const double* target, const double* weights, int nx,
+                                int ny, int nz, double dtip, double* df_out, float* dL_dFEs, double* loss_out,
+                                void* scratch, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(FEs && target && df_out && dL_dFEs && loss_out && scratch, "spm_df_loss_seed: null pointer");
+    SPM_REQUIRE(fes_dtype == SPM_F32 || fes_dtype == SPM_F64, "spm_df_loss_seed: fes_dtype=%d", fes_dtype);
+    SPM_REQUIRE(nx > 0 && ny > 0, "spm_df_loss_seed: nx=%d ny=%d must be positive", nx, ny);
+    SPM_REQUIRE(nz >= 3, "spm_df_loss_seed: need nz>=3 for central difference, got nz=%d", nz);
+    SPM_REQUIRE(dtip < 0.0, "spm_df_loss_seed: dtip must be <0, got dtip=%g", dtip);
+    SPM_REQUIRE(aligned16(FEs) && aligned16(dL_dFEs), "spm_df_loss_seed: FEs/dL_dFEs not 16-byte aligned");
+    SPM_REQUIRE((reinterpret_cast<uintptr_t>(scratch) & 7u) == 0, "spm_df_loss_seed: scratch not 8-byte aligned");
+    const long long total = (long long)nx * ny * nz;
+    const long long nblk = (total + LS_THREADS - 1) / LS_THREADS;
+    SPM_REQUIRE(nblk < (1LL << 31), "spm_df_loss_seed: volume too large");
+    double* partial = reinterpret_cast<double*>(scratch);
+    double* sums = partial + 2 * nblk;
+    const double dz = fabs(dtip);
+    cudaStream_t st = as_stream(stream);
+    if (fes_dtype == SPM_F32)
+        loss_partials_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(static_cast<const float*>(FEs), target, weights,
+                                                                    nx, ny, nz, 2.0 * dz, df_out, partial);
+    else
+        loss_partials_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(static_cast<const double*>(FEs), target, weights,
+                                                                    nx, ny, nz, 2.0 * dz, df_out, partial);
+    loss_final_kernel<<<1, LS_THREADS, 0, st>>>(partial, (int)nblk, sums, loss_out);
+    loss_grad_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(df_out, target, weights, sums, nx, ny, nz,
+                                                            1.0 / (2.0 * dz), reinterpret_cast<float4*>(dL_dFEs));
+    return check_launch("spm_df_loss_seed");
+}

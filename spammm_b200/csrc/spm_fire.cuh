@@ -1,0 +1,141 @@
+// spm_fire.cuh -- device helpers of the probe-relaxation kernels.
+//
+// The operation order here is the canonical FP32 order of this library:
+// every fused multiply-add is an explicit __fmaf_rn and the translation units
+// that include this header are compiled with -fmad=false, IEEE sqrt and IEEE
+// division.  The relaxation results are therefore a pure function of the
+// inputs, independent of compiler contraction choices.
+//
+// Semantics follow SPAMMM kernels/AFM.cl: tipForce :53-58, interpFE :100-105
+// (REPEAT + LINEAR sampler with normalized coordinates, :49), update_FIRE
+// :136-157, rotMat/rotMatT kernels/common.cl:43-44.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace spm {
+
+struct V3 {
+    float x, y, z;
+};
+
+__device__ __forceinline__ V3 mk3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 sub3(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 add3(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ float dot3(V3 a, V3 b) {
+    return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, __fmul_rn(a.x, b.x)));
+}
+__device__ __forceinline__ V3 rotmat(V3 v, V3 a, V3 b, V3 c) { return V3{dot3(v, a), dot3(v, b), dot3(v, c)}; }
+__device__ __forceinline__ V3 rotmatT(V3 v, V3 a, V3 b, V3 c) {
+    return V3{__fmaf_rn(c.x, v.z, __fmaf_rn(b.x, v.y, __fmul_rn(a.x, v.x))),
+              __fmaf_rn(c.y, v.z, __fmaf_rn(b.y, v.y, __fmul_rn(a.y, v.x))),
+              __fmaf_rn(c.z, v.z, __fmaf_rn(b.z, v.y, __fmul_rn(a.z, v.x)))};
+}
+
+// Harmonic 3D spring + radial bond: (d - d0.xyz)*k.xyz + d*(k.w*(r - d0.w)/r)
+__device__ __forceinline__ V3 tip_force(V3 d, float4 k, float4 d0) {
+    float r = __fsqrt_rn(dot3(d, d));
+    r = fmaxf(r, 1e-10f);
+    float s = __fdiv_rn(__fmul_rn(k.w, r - d0.w), r);
+    return V3{__fmaf_rn(d.x, s, __fmul_rn(d.x - d0.x, k.x)),
+              __fmaf_rn(d.y, s, __fmul_rn(d.y - d0.y, k.y)),
+              __fmaf_rn(d.z, s, __fmul_rn(d.z - d0.z, k.z))};
+}
+
+struct Integrator {
+    float dt, damp, dtmin, dtmax, damp0;
+};
+
+// FIRE velocity mixing (Bitzek et al., PRL 97, 170201 (2006)) or plain damping,
+// followed by v += f*dt, pos += v*dt.
+__device__ __forceinline__ void md_step(V3 f, V3& v, V3& pos, Integrator& I, bool use_fire) {
+    if (use_fire) {
+        float ff = dot3(f, f);
+        float vv = dot3(v, v);
+        float vf = dot3(v, f);
+        if (vf < 0.f) {
+            v.x = __fmul_rn(v.x, 0.f); v.y = __fmul_rn(v.y, 0.f); v.z = __fmul_rn(v.z, 0.f);
+            I.dt = fmaxf(I.dtmin, __fmul_rn(I.dt, 0.5f));
+            I.damp = I.damp0;
+        } else {
+            float cf = __fmul_rn(I.damp, __fsqrt_rn(__fdiv_rn(vv, ff + 1e-8f)));
+            float cv = 1.f - I.damp;
+            v.x = __fmaf_rn(f.x, cf, __fmul_rn(v.x, cv));
+            v.y = __fmaf_rn(f.y, cf, __fmul_rn(v.y, cv));
+            v.z = __fmaf_rn(f.z, cf, __fmul_rn(v.z, cv));
+            I.dt = fminf(I.dtmax, __fmul_rn(I.dt, 1.1f));
+            I.damp = __fmul_rn(I.damp, 0.99f);
+        }
+    } else {
+        float cv = 1.f - I.damp;
+        v.x = __fmul_rn(v.x, cv); v.y = __fmul_rn(v.y, cv); v.z = __fmul_rn(v.z, cv);
+    }
+    v.x = __fmaf_rn(f.x, I.dt, v.x);
+    v.y = __fmaf_rn(f.y, I.dt, v.y);
+    v.z = __fmaf_rn(f.z, I.dt, v.z);
+    pos.x = __fmaf_rn(v.x, I.dt, pos.x);
+    pos.y = __fmaf_rn(v.y, I.dt, pos.y);
+    pos.z = __fmaf_rn(v.z, I.dt, pos.z);
+}
+
+// REPEAT addressing + linear filter along one axis (OpenCL 1.2 sec. 8.2).
+__device__ __forceinline__ bool tex_axis(float u, int n, int& i0, int& i1, float& a) {
+    float s = u - floorf(u);
+    float t = __fmaf_rn(s, (float)n, -0.5f);
+    if (!(t >= -1.f && t < (float)n)) return false;
+    float fi = floorf(t);
+    a = t - fi;
+    int i = (int)fi;
+    if (i < 0) i += n;
+    int j = i + 1;
+    if (j >= n) j -= n;
+    i0 = i;
+    i1 = j;
+    return true;
+}
+
+__device__ __forceinline__ float lerp_c(float a, float ma, float f0, float f1) {
+    return __fmaf_rn(a, f1, __fmul_rn(ma, f0));
+}
+
+__device__ __forceinline__ float4 lerp4(float a, float ma, float4 f0, float4 f1) {
+    return make_float4(lerp_c(a, ma, f0.x, f1.x), lerp_c(a, ma, f0.y, f1.y), lerp_c(a, ma, f0.z, f1.z),
+                       lerp_c(a, ma, f0.w, f1.w));
+}
+
+struct GridView {
+    const float4* __restrict__ g;
+    int nx, ny, nz;
+    float4 dA, dB, dC;  // normalized-coordinate transform rows
+};
+
+// interpFE: exact FP32 trilinear sample with periodic wrap.
+__device__ __forceinline__ float4 interp_fe(const GridView& G, V3 p) {
+    float u = __fmaf_rn(p.x, G.dA.x, __fmaf_rn(p.y, G.dA.y, __fmaf_rn(p.z, G.dA.z, G.dA.w)));
+    float v = __fmaf_rn(p.x, G.dB.x, __fmaf_rn(p.y, G.dB.y, __fmaf_rn(p.z, G.dB.z, G.dB.w)));
+    float w = __fmaf_rn(p.x, G.dC.x, __fmaf_rn(p.y, G.dC.y, __fmaf_rn(p.z, G.dC.z, G.dC.w)));
+    int x0, x1, y0, y1, z0, z1;
+    float ax, ay, az;
+    bool ok = tex_axis(u, G.nx, x0, x1, ax);
+    ok = tex_axis(v, G.ny, y0, y1, ay) && ok;
+    ok = tex_axis(w, G.nz, z0, z1, az) && ok;
+    if (!ok) {
+        float nan = __int_as_float(0x7fc00000);
+        return make_float4(nan, nan, nan, nan);
+    }
+    float mx = 1.f - ax, my = 1.f - ay, mz = 1.f - az;
+    size_t r00 = ((size_t)z0 * G.ny + y0) * G.nx, r10 = ((size_t)z0 * G.ny + y1) * G.nx;
+    size_t r01 = ((size_t)z1 * G.ny + y0) * G.nx, r11 = ((size_t)z1 * G.ny + y1) * G.nx;
+    float4 f000 = __ldg(G.g + r00 + x0), f100 = __ldg(G.g + r00 + x1);
+    float4 f010 = __ldg(G.g + r10 + x0), f110 = __ldg(G.g + r10 + x1);
+    float4 f001 = __ldg(G.g + r01 + x0), f101 = __ldg(G.g + r01 + x1);
+    float4 f011 = __ldg(G.g + r11 + x0), f111 = __ldg(G.g + r11 + x1);
+    float4 c00 = lerp4(ax, mx, f000, f100);
+    float4 c10 = lerp4(ax, mx, f010, f110);
+    float4 c01 = lerp4(ax, mx, f001, f101);
+    float4 c11 = lerp4(ax, mx, f011, f111);
+    float4 c0 = lerp4(ay, my, c00, c10);
+    float4 c1 = lerp4(ay, my, c01, c11);
+    return lerp4(az, mz, c0, c1);
+}
+
+}  // namespace spm
