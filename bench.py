@@ -38,7 +38,7 @@ FLOPS_SITE = 23
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="plain_large", choices=["plain_large", "plain_small"])
@@ -99,7 +99,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -269,8 +269,13 @@ def run_ours(args, rank, world, local_rank):
     ms_step = ms_total / args.steps
     # the events above wrap each stage; the sum of stages is the kernel time of a step (host syncs excluded)
     value = world * cfg.pxz / (ms_step * 1e-3)
-    iters = None
     out = {}
+    # FIRE telemetry (outside the timed region): integrator steps per px*z
+    cnt = torch.empty(cfg.n_pix, dtype=torch.int32, device=dev)
+    gpu.relax_strokes(grid, P, pts_d, FEs=FEs, disps=disps, iter_count=cnt)
+    steps_total = float(cnt.double().sum().item())
+    out["fire"] = {"steps_per_pxz": steps_total / cfg.pxz, "max_steps_pixel": int(cnt.max().item()),
+                   "sampled_bytes_per_launch": steps_total * 8 * 16}
 
     # ---- e2e through the drop-in API (host buffers)
     e2e = None

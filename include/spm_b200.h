@@ -100,6 +100,14 @@ int spm_relax_strokes(const float* grid, int nx, int ny, int nz,
                       const float* points, int n_scan, const spm_scan_params* p,
                       float* FEs, float* disps, void* stream);
 
+/* spm_relax_strokes plus telemetry: iter_count (DEVICE int[n_scan], may be
+ * NULL) receives each pixel's integrator steps summed over its z-steps.  No
+ * counterpart in the reference (its kernel reports nothing); results are
+ * identical to spm_relax_strokes. */
+int spm_relax_strokes_counted(const float* grid, int nx, int ny, int nz,
+                              const float* points, int n_scan, const spm_scan_params* p,
+                              float* FEs, float* disps, int* iter_count, void* stream);
+
 /* Replaces AFMulator.run_scan -> relaxStrokesTilted (spammm/SPM/AFM.py:950-1010,
  * kernels/AFM.cl:478-562): tip-frame spring, surface bias, re-sampled FE after
  * the loop, output rotated into the tip frame.  dtip = p->tipC[3]. */

@@ -715,8 +715,11 @@ def _to_np(t):
 
 
 def _volume(FEs, ncopy=3):
-    """(nx,ny,nz,4) float32/float64 volume holding the first ncopy channels of FEs."""
+    """(nx,ny,nz,4) float32/float64 volume holding the first ncopy channels of FEs
+    (FEs itself when it already is one: the kernels read channels 0-2 only)."""
     dt = np.float64 if FEs.dtype == np.float64 else np.float32
+    if FEs.dtype == dt and FEs.shape[-1] == 4 and FEs.flags.c_contiguous:
+        return FEs
     vol = np.zeros(FEs.shape[:3] + (4,), dtype=dt)
     vol[..., :ncopy] = FEs[..., :ncopy]
     return vol

@@ -88,6 +88,7 @@ _SIGNATURES = {
     "spm_last_error": (ctypes.c_char_p, []),
     "spm_grid_build": (_i, [_i, _i, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "spm_relax_strokes": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp, _vp]),
+    "spm_relax_strokes_counted": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp, _vp, _vp]),
     "spm_relax_strokes_tilted": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp]),
     "spm_fe_in_strokes_tilted": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp]),
     "spm_df_amp_dir": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _d, _vp, _i, _vp, _vp]),

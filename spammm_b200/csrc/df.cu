@@ -136,6 +136,62 @@ df_amp_dir_kernel(const T* __restrict__ FEs, DfGeom P, const int* __restrict__ o
     df[gid] = (float)acc;
 }
 
+// Oscillation along +-z only (the common case): one warp per pixel column.
+// The column's F_n values are staged once in shared memory (coalesced reads of
+// nz contiguous rows); each lane then evaluates its output heights with the
+// same expression sequence as df_amp_dir_kernel (x/y weights are exactly 1
+// there and the zero-weight corners are skipped), so results are identical.
+constexpr int DFZ_WARPS = 8;
+constexpr int DFZ_MAXNZ = 512;
+
+template <typename T>
+__global__ void __launch_bounds__(DFZ_WARPS * 32)
+df_amp_z_kernel(const T* __restrict__ FEs, DfGeom P, const int* __restrict__ out_iz, int n_out,
+                float* __restrict__ df) {
+    __shared__ double s_fn[DFZ_WARPS][DFZ_MAXNZ];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const long long pix = (long long)blockIdx.x * DFZ_WARPS + w;
+    if (pix >= (long long)P.nx * P.ny) return;  // whole warp exits together: no CTA barrier below
+    const int nz = P.nz;
+    double* fn = s_fn[w];
+    for (int z = l; z < nz; z += 32) {
+        const Row f = load_row(FEs, (size_t)pix * nz + z);
+        fn[z] = (f.x * P.n[0] + f.y * P.n[1]) + f.z * P.n[2];
+    }
+    __syncwarp();
+    const double sh = P.shift[2], dr = P.dr[2], nzc = P.n[2];
+    auto S = [&](int j, double u) {
+        const double c = (double)j + u * sh;
+        const double fl = floor(c);
+        const double t = c - fl;
+        const int i0 = (int)fl;
+        const double w0 = 1.0 - t, w1 = t;
+        double acc = 0.0;
+        if (w0 != 0.0) acc += fn[clampi(i0, nz)] * w0;
+        if (w1 != 0.0) acc += fn[clampi(i0 + 1, nz)] * w1;
+        return acc;
+    };
+    for (int o = l; o < n_out; o += 32) {
+        const int iz = out_iz ? out_iz[o] : o;
+        float res;
+        if (iz < 0 || iz >= nz) {
+            res = __int_as_float(0x7fc00000);
+        } else {
+            double acc = 0.0;
+            for (int k = 0; k < NQ; k++) {
+                const double u = P.uk[k];
+                double g;
+                if (iz == 0) g = (S(1, u) - S(0, u)) / dr;
+                else if (iz == nz - 1) g = (S(nz - 1, u) - S(nz - 2, u)) / dr;
+                else g = (S(iz + 1, u) - S(iz - 1, u)) / (2.0 * dr);
+                acc -= (P.wk * nzc) * g;
+            }
+            res = (float)acc;
+        }
+        df[pix * n_out + o] = res;
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(DF_THREADS)
 df_dir_kernel(const T* __restrict__ FEs, DfGeom P, double* __restrict__ df) {
@@ -315,6 +371,17 @@ extern "C" int spm_df_amp_dir(const void* FEs, int fes_dtype, int nx, int ny, in
     SPM_REQUIRE(n_out >= 0, "spm_df_amp_dir: n_out=%d < 0", n_out);
     const long long total = (long long)nx * ny * n_out;
     if (total == 0) return SPM_OK;
+    if (n[0] == 0.0 && n[1] == 0.0 && nz <= DFZ_MAXNZ) {  // z-only oscillation: column kernel
+        const long long npix = (long long)nx * ny;
+        const unsigned nb = (unsigned)((npix + DFZ_WARPS - 1) / DFZ_WARPS);
+        if (fes_dtype == SPM_F32)
+            df_amp_z_kernel<<<nb, DFZ_WARPS * 32, 0, as_stream(stream)>>>(static_cast<const float*>(FEs), P, out_iz,
+                                                                           n_out, df);
+        else
+            df_amp_z_kernel<<<nb, DFZ_WARPS * 32, 0, as_stream(stream)>>>(static_cast<const double*>(FEs), P, out_iz,
+                                                                           n_out, df);
+        return check_launch("spm_df_amp_dir");
+    }
     const unsigned nb = (unsigned)((total + DF_THREADS - 1) / DF_THREADS);
     if (fes_dtype == SPM_F32)
         df_amp_dir_kernel<<<nb, DF_THREADS, 0, as_stream(stream)>>>(static_cast<const float*>(FEs), P, out_iz, n_out, df);

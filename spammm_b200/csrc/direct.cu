@@ -441,7 +441,8 @@ adjoint_reduce_kernel(const float* __restrict__ partial, int n_chunks, float* __
 
 int common_checks(const char* who, int na, const float* atoms, const float* cMs, const float* points, int n_scan,
                   const spm_scan_params* p) {
-    SPM_REQUIRE(p != nullptr && atoms && cMs && points, "%s: null pointer", who);
+    SPM_REQUIRE(p != nullptr && atoms && cMs, "%s: null pointer", who);
+    SPM_REQUIRE(points || n_scan == 0, "%s: null points", who);
     if (na < 1 || na > SPM_DIRECT_MAX_ATOMS)
         return set_error(SPM_ERR_UNSUPPORTED, "%s: n_atoms=%d out of range [1,%d]", who, na, SPM_DIRECT_MAX_ATOMS);
     SPM_REQUIRE(n_scan >= 0 && p->nz >= 0, "%s: n_scan=%d nz=%d must be >= 0", who, n_scan, p->nz);

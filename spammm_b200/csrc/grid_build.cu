@@ -3,17 +3,21 @@
 // Replaces evalLJC_QZs_toImg / evalMorseC_QZs_toImg (SPAMMM kernels/AFM.cl:
 // 916-1056) behind AFMulator.make_forcefield (spammm/SPM/AFM.py:897-946).
 //
-// B200 shape: one thread owns a z-column of ZB nodes at fixed (ia,ib); a CTA
-// is 32 (x) x 4 (y) threads, so stores of the (nz,ny,nx,4) grid are 512-byte
-// coalesced rows.  Atoms are staged TILE at a time in shared memory already
-// transformed for the inner loop (Morse: K*log2(e), -K*R0*log2(e), E0,
-// -2*K*E0; LJ: c6, c12, 6*c6, 12*c12; Coulomb: Q*Qs[k]*COULOMB_CONST per
-// non-zero tip site), read back as warp-uniform broadcasts.  Because every
-// reference grid has dC = (0,0,dz), the in-plane part dx^2+dy^2+R2SAFE of each
-// pair distance is computed once per (thread, atom) and reused by the ZB nodes
-// and the tip-charge sites.  Transcendentals use the MUFU approximations
-// (rsqrt.approx, ex2.approx); the rest is FP32 FMA.  The instruction mix per
-// (node, atom) pair is FP32/MUFU bound, not memory bound.
+// B200 shape.  One thread owns a z-column of GB_ZB nodes at fixed (ia,ib); a
+// CTA is 32 (x) x 4 (y) threads, so stores of the (nz,ny,nx,4) grid are
+// 512-byte coalesced rows.  Atoms are staged GB_TILE at a time in shared
+// memory already transformed for the inner loop, read back as warp-uniform
+// broadcasts.  The work per (node, atom) pair is FP32 FMA + MUFU bound, so the
+// inner loop is written to minimise issued instructions:
+//   * every reference grid has dC = (0,0,dz): dx^2+dy^2+R2SAFE of a pair is
+//     computed once per (thread, atom) and shared by the column's nodes;
+//   * nodes are evaluated two at a time with Blackwell's packed FP32
+//     instructions (fma/mul/add/sub .f32x2), halving the FP32 issue count;
+//   * tip-charge sites with a zero z-offset sit on the node itself; their
+//     charges are merged into one term that reuses the pair law's 1/r (one
+//     MUFU rsqrt per pair in total for LJ + on-node Coulomb); sites with a
+//     non-zero offset get their own rsqrt.
+// Transcendentals use MUFU approximations (rsqrt.approx, ex2.approx).
 #include "spm_internal.cuh"
 
 namespace spm {
@@ -21,12 +25,43 @@ namespace {
 
 constexpr int GB_TX = 32;     // threads along x
 constexpr int GB_TY = 4;      // threads along y
-constexpr int GB_ZB = 8;      // nodes along z per thread
+constexpr int GB_ZB = 8;      // nodes along z per thread (4 packed pairs)
+constexpr int GB_ZP = GB_ZB / 2;
 constexpr int GB_TILE = 256;  // atoms per shared-memory tile
 constexpr float R2SAFE = 1e-4f;
 constexpr float COULOMB_CONST = 14.3996448915f;
 constexpr float LOG2E = 1.4426950408889634f;
 
+typedef unsigned long long f2;  // two packed float32 lanes (lo = node 2p, hi = node 2p+1)
+
+__device__ __forceinline__ f2 pk(float lo, float hi) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk(f2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+    f2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+    f2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+    f2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
 __device__ __forceinline__ float fast_rsqrt(float x) {
     float y;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -37,11 +72,17 @@ __device__ __forceinline__ float fast_ex2(float x) {
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
-__device__ __forceinline__ float fast_rcp(float x) {
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
+__device__ __forceinline__ f2 rsqrt2(f2 x) {
+    float a, b;
+    upk(x, a, b);
+    return pk(fast_rsqrt(a), fast_rsqrt(b));
 }
+__device__ __forceinline__ f2 ex2_2(f2 x) {
+    float a, b;
+    upk(x, a, b);
+    return pk(fast_ex2(a), fast_ex2(b));
+}
+__device__ __forceinline__ f2 bc(float v) { return pk(v, v); }
 
 struct GridGeom {
     int nx, ny, nz;
@@ -49,17 +90,20 @@ struct GridGeom {
 };
 
 struct TipSites {
-    float qs[4];   // Qs[k]*COULOMB_CONST of the non-zero sites, compacted
-    float qz[4];   // matching world-z offsets
+    float qs_on;   // sum of Qs[k]*COULOMB_CONST over sites with QZs[k] == 0
+    float qs[4];   // Qs[k]*COULOMB_CONST of the non-zero sites with QZs[k] != 0
+    float qz[4];   // their z-offsets
 };
 
-template <int KIND, int NS>
+// KIND: SPM_KIND_LJ / SPM_KIND_MORSE; ON: an on-node charge term exists;
+// NOFF: number of off-node sites.
+template <int KIND, bool ON, int NOFF>
 __global__ void __launch_bounds__(GB_TX * GB_TY)
 grid_build_kernel(int na, const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
                   float4* __restrict__ grid, GridGeom G, TipSites S) {
-    __shared__ float4 s_pos[GB_TILE];                 // (x, y, z, -)
-    __shared__ float4 s_prm[GB_TILE];                 // transformed pair parameters
-    __shared__ float s_q[NS > 0 ? NS : 1][GB_TILE];   // Q*Qs[k]*C per site
+    __shared__ float4 s_pos[GB_TILE];                   // (x, y, z, Q*qs_on)
+    __shared__ float4 s_prm[GB_TILE];                   // transformed pair parameters
+    __shared__ float s_q[NOFF > 0 ? NOFF : 1][GB_TILE];  // Q*Qs[k]*C per off-node site
 
     const int tid = threadIdx.y * GB_TX + threadIdx.x;
     const int ia = blockIdx.x * GB_TX + threadIdx.x;
@@ -70,75 +114,88 @@ grid_build_kernel(int na, const float4* __restrict__ atoms, const float* __restr
     const float px = G.p0.x + G.dA.x * (float)ia + G.dB.x * (float)ib;
     const float py = G.p0.y + G.dA.y * (float)ia + G.dB.y * (float)ib;
     const float pzb = G.p0.z + G.dA.z * (float)ia + G.dB.z * (float)ib;
-    float pz[GB_ZB];
+    f2 pz[GB_ZP];
 #pragma unroll
-    for (int j = 0; j < GB_ZB; j++) pz[j] = pzb + G.dC.z * (float)(ic0 + j);
+    for (int p = 0; p < GB_ZP; p++)
+        pz[p] = pk(pzb + G.dC.z * (float)(ic0 + 2 * p), pzb + G.dC.z * (float)(ic0 + 2 * p + 1));
 
-    float fx[GB_ZB], fy[GB_ZB], fz[GB_ZB], fe[GB_ZB];
+    const f2 zero = pk(0.f, 0.f);
+    f2 fx[GB_ZP], fy[GB_ZP], fz[GB_ZP], fe[GB_ZP];
 #pragma unroll
-    for (int j = 0; j < GB_ZB; j++) { fx[j] = 0.f; fy[j] = 0.f; fz[j] = 0.f; fe[j] = 0.f; }
+    for (int p = 0; p < GB_ZP; p++) { fx[p] = zero; fy[p] = zero; fz[p] = zero; fe[p] = zero; }
+    const f2 two = bc(2.f), one = bc(1.f);
 
     for (int t0 = 0; t0 < na; t0 += GB_TILE) {
         const int nt = min(GB_TILE, na - t0);
         for (int j = tid; j < nt; j += GB_TX * GB_TY) {
             float4 a = __ldg(atoms + t0 + j);
             const float* pr = params + (size_t)(t0 + j) * pstride;
-            s_pos[j] = make_float4(a.x, a.y, a.z, 0.f);
+            s_pos[j] = make_float4(a.x, a.y, a.z, a.w * S.qs_on);
             if (KIND == SPM_KIND_MORSE) {
                 float R0 = __ldg(pr + 0), E0 = __ldg(pr + 1), K = __ldg(pr + 2);
                 s_prm[j] = make_float4(K * LOG2E, -K * R0 * LOG2E, E0, -2.f * K * E0);
             } else {
                 float c6 = __ldg(pr + 0), c12 = __ldg(pr + 1);
-                s_prm[j] = make_float4(c6, c12, 6.f * c6, 12.f * c12);
+                s_prm[j] = make_float4(-c6, c12, -6.f * c6, 12.f * c12);
             }
 #pragma unroll
-            for (int k = 0; k < NS; k++) s_q[k][j] = a.w * S.qs[k];
+            for (int k = 0; k < NOFF; k++) s_q[k][j] = a.w * S.qs[k];
         }
         __syncthreads();
         if (active) {
-#pragma unroll 2
+#pragma unroll 1
             for (int j = 0; j < nt; j++) {
                 const float4 a = s_pos[j];
                 const float4 c = s_prm[j];
-                const float dx = px - a.x;
-                const float dy = py - a.y;
-                const float dxy2 = fmaf(dx, dx, fmaf(dy, dy, R2SAFE));
+                const float dxs = px - a.x;
+                const float dys = py - a.y;
+                const float dxy2s = fmaf(dxs, dxs, fmaf(dys, dys, R2SAFE));
+                const f2 dx = bc(dxs), dy = bc(dys), dxy2 = bc(dxy2s), az = bc(a.z);
+                const f2 c0 = bc(c.x), c1 = bc(c.y), c2 = bc(c.z), c3 = bc(c.w);
+                const f2 qon = bc(a.w);
 #pragma unroll
-                for (int n = 0; n < GB_ZB; n++) {
-                    const float dz = pz[n] - a.z;
-                    const float r2 = fmaf(dz, dz, dxy2);
+                for (int p = 0; p < GB_ZP; p++) {
+                    const f2 dz = sub2(pz[p], az);
+                    const f2 r2 = fma2(dz, dz, dxy2);
+                    const f2 rs = rsqrt2(r2);
+                    f2 s;
                     if (KIND == SPM_KIND_MORSE) {
-                        // E = E0 e (e-2), F = dp * (-2 K E0 e (e-1)) / r, e = exp(K (r-R0))
-                        const float rs = fast_rsqrt(r2);
-                        const float r = r2 * rs;
-                        const float e = fast_ex2(fmaf(c.x, r, c.y));
-                        const float E0e = c.z * e;
-                        fe[n] = fmaf(E0e, e - 2.f, fe[n]);
-                        const float s = (c.w * e) * (e - 1.f) * rs;
-                        fx[n] = fmaf(dx, s, fx[n]);
-                        fy[n] = fmaf(dy, s, fy[n]);
-                        fz[n] = fmaf(dz, s, fz[n]);
+                        // E = E0 e (e-2), F = dp * (-2 K E0) e (e-1) / r, e = exp(K (r-R0))
+                        const f2 r = mul2(r2, rs);
+                        const f2 e = ex2_2(fma2(c0, r, c1));
+                        fe[p] = fma2(mul2(c2, e), sub2(e, two), fe[p]);
+                        s = mul2(mul2(mul2(c3, e), sub2(e, one)), rs);
+                        if (ON) {
+                            const f2 Ek = mul2(qon, rs);
+                            fe[p] = add2(fe[p], Ek);
+                            s = fma2(Ek, mul2(rs, rs), s);
+                        }
                     } else {
                         // E = (c12 ir6 - c6) ir6, F = dp * (12 c12 ir6 - 6 c6) ir6 ir2
-                        const float ir2 = fast_rcp(r2);
-                        const float ir6 = ir2 * ir2 * ir2;
-                        fe[n] = fmaf(fmaf(c.y, ir6, -c.x), ir6, fe[n]);
-                        const float s = fmaf(c.w, ir6, -c.z) * ir6 * ir2;
-                        fx[n] = fmaf(dx, s, fx[n]);
-                        fy[n] = fmaf(dy, s, fy[n]);
-                        fz[n] = fmaf(dz, s, fz[n]);
+                        const f2 ir2 = mul2(rs, rs);
+                        const f2 ir6 = mul2(mul2(ir2, ir2), ir2);
+                        fe[p] = fma2(fma2(c1, ir6, c0), ir6, fe[p]);
+                        s = mul2(mul2(fma2(c3, ir6, c2), ir6), ir2);
+                        if (ON) {
+                            const f2 Ek = mul2(qon, rs);
+                            fe[p] = add2(fe[p], Ek);
+                            s = fma2(Ek, ir2, s);
+                        }
                     }
+                    fx[p] = fma2(dx, s, fx[p]);
+                    fy[p] = fma2(dy, s, fy[p]);
+                    fz[p] = fma2(dz, s, fz[p]);
 #pragma unroll
-                    for (int k = 0; k < NS; k++) {
+                    for (int k = 0; k < NOFF; k++) {
                         // Coulomb at the tip-charge site node + zhat*QZs[k]
-                        const float dzk = dz + S.qz[k];
-                        const float rs = fast_rsqrt(fmaf(dzk, dzk, dxy2));
-                        const float Ek = s_q[k][j] * rs;
-                        fe[n] += Ek;
-                        const float s = Ek * rs * rs;
-                        fx[n] = fmaf(dx, s, fx[n]);
-                        fy[n] = fmaf(dy, s, fy[n]);
-                        fz[n] = fmaf(dzk, s, fz[n]);
+                        const f2 dzk = add2(dz, bc(S.qz[k]));
+                        const f2 rsk = rsqrt2(fma2(dzk, dzk, dxy2));
+                        const f2 Ek = mul2(bc(s_q[k][j]), rsk);
+                        fe[p] = add2(fe[p], Ek);
+                        const f2 sk = mul2(mul2(Ek, rsk), rsk);
+                        fx[p] = fma2(dx, sk, fx[p]);
+                        fy[p] = fma2(dy, sk, fy[p]);
+                        fz[p] = fma2(dzk, sk, fz[p]);
                     }
                 }
             }
@@ -147,28 +204,43 @@ grid_build_kernel(int na, const float4* __restrict__ atoms, const float* __restr
     }
     if (!active) return;
 #pragma unroll
-    for (int n = 0; n < GB_ZB; n++) {
-        const int ic = ic0 + n;
-        if (ic >= G.nz) break;
-        float4 o = make_float4(fx[n], fy[n], fz[n], fe[n]);
-        // |E| > 100 cap of the reference builders (AFM.cl:1053-1054)
-        const float renorm = __fdiv_rn(100.f, fabsf(o.w));
-        if (renorm < 1.f) { o.x *= renorm; o.y *= renorm; o.z *= renorm; o.w *= renorm; }
-        grid[((size_t)ic * G.ny + ib) * G.nx + ia] = o;
+    for (int p = 0; p < GB_ZP; p++) {
+        float x[2], y[2], z[2], e[2];
+        upk(fx[p], x[0], x[1]);
+        upk(fy[p], y[0], y[1]);
+        upk(fz[p], z[0], z[1]);
+        upk(fe[p], e[0], e[1]);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int ic = ic0 + 2 * p + h;
+            if (ic >= G.nz) break;
+            float4 o = make_float4(x[h], y[h], z[h], e[h]);
+            // |E| > 100 cap of the reference builders (AFM.cl:1053-1054)
+            const float renorm = __fdiv_rn(100.f, fabsf(o.w));
+            if (renorm < 1.f) { o.x *= renorm; o.y *= renorm; o.z *= renorm; o.w *= renorm; }
+            grid[((size_t)ic * G.ny + ib) * G.nx + ia] = o;
+        }
     }
 }
 
-template <int KIND>
-int launch_ns(int ns, dim3 grid, dim3 block, cudaStream_t st, int na, const float4* atoms, const float* params,
-              int pstride, float4* out, const GridGeom& G, const TipSites& S) {
-    switch (ns) {
-        case 0: grid_build_kernel<KIND, 0><<<grid, block, 0, st>>>(na, atoms, params, pstride, out, G, S); break;
-        case 1: grid_build_kernel<KIND, 1><<<grid, block, 0, st>>>(na, atoms, params, pstride, out, G, S); break;
-        case 2: grid_build_kernel<KIND, 2><<<grid, block, 0, st>>>(na, atoms, params, pstride, out, G, S); break;
-        case 3: grid_build_kernel<KIND, 3><<<grid, block, 0, st>>>(na, atoms, params, pstride, out, G, S); break;
-        default: grid_build_kernel<KIND, 4><<<grid, block, 0, st>>>(na, atoms, params, pstride, out, G, S); break;
+template <int KIND, bool ON>
+int launch_noff(int noff, dim3 grd, dim3 block, cudaStream_t st, int na, const float4* atoms, const float* params,
+                int pstride, float4* out, const GridGeom& G, const TipSites& S) {
+    switch (noff) {
+        case 0: grid_build_kernel<KIND, ON, 0><<<grd, block, 0, st>>>(na, atoms, params, pstride, out, G, S); break;
+        case 1: grid_build_kernel<KIND, ON, 1><<<grd, block, 0, st>>>(na, atoms, params, pstride, out, G, S); break;
+        case 2: grid_build_kernel<KIND, ON, 2><<<grd, block, 0, st>>>(na, atoms, params, pstride, out, G, S); break;
+        case 3: grid_build_kernel<KIND, ON, 3><<<grd, block, 0, st>>>(na, atoms, params, pstride, out, G, S); break;
+        default: grid_build_kernel<KIND, ON, 4><<<grd, block, 0, st>>>(na, atoms, params, pstride, out, G, S); break;
     }
     return check_launch("spm_grid_build");
+}
+
+template <int KIND>
+int launch_kind(bool on, int noff, dim3 grd, dim3 block, cudaStream_t st, int na, const float4* atoms,
+                const float* params, int pstride, float4* out, const GridGeom& G, const TipSites& S) {
+    if (on) return launch_noff<KIND, true>(noff, grd, block, st, na, atoms, params, pstride, out, G, S);
+    return launch_noff<KIND, false>(noff, grd, block, st, na, atoms, params, pstride, out, G, S);
 }
 
 }  // namespace
@@ -198,9 +270,18 @@ extern "C" int spm_grid_build(int kind, int n_atoms, const float* atoms, const f
     G.dB = make_float4(dB[0], dB[1], dB[2], dB[3]);
     G.dC = make_float4(dC[0], dC[1], dC[2], dC[3]);
     TipSites S = {};
-    int ns = 0;
+    int noff = 0;
+    bool on = false;
     for (int k = 0; k < 4; k++) {
-        if (Qs[k] != 0.f) { S.qs[ns] = Qs[k] * COULOMB_CONST; S.qz[ns] = QZs[k]; ns++; }
+        if (Qs[k] == 0.f) continue;  // a zero-charge site only adds zeros
+        if (QZs[k] == 0.f) {
+            S.qs_on += Qs[k] * COULOMB_CONST;
+            on = true;
+        } else {
+            S.qs[noff] = Qs[k] * COULOMB_CONST;
+            S.qz[noff] = QZs[k];
+            noff++;
+        }
     }
     dim3 block(GB_TX, GB_TY, 1);
     dim3 grd((nx + GB_TX - 1) / GB_TX, (ny + GB_TY - 1) / GB_TY, (nz + GB_ZB - 1) / GB_ZB);
@@ -208,6 +289,6 @@ extern "C" int spm_grid_build(int kind, int n_atoms, const float* atoms, const f
     cudaStream_t st = as_stream(stream);
     const float4* a4 = reinterpret_cast<const float4*>(atoms);
     float4* g4 = reinterpret_cast<float4*>(grid);
-    if (kind == SPM_KIND_MORSE) return launch_ns<SPM_KIND_MORSE>(ns, grd, block, st, n_atoms, a4, params, pstride, g4, G, S);
-    return launch_ns<SPM_KIND_LJ>(ns, grd, block, st, n_atoms, a4, params, pstride, g4, G, S);
+    if (kind == SPM_KIND_MORSE) return launch_kind<SPM_KIND_MORSE>(on, noff, grd, block, st, n_atoms, a4, params, pstride, g4, G, S);
+    return launch_kind<SPM_KIND_LJ>(on, noff, grd, block, st, n_atoms, a4, params, pstride, g4, G, S);
 }

@@ -48,7 +48,7 @@ __device__ __forceinline__ float4 ld4(const float* a) { return make_float4(a[0],
 template <int MODE>
 __global__ void __launch_bounds__(RX_THREADS)
 relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
-             float4* __restrict__ FEs, float4* __restrict__ disps) {
+             float4* __restrict__ FEs, float4* __restrict__ disps, int* __restrict__ iter_count) {
     const int k = pixel_of_thread(n_scan, P.raster_ny);
     if (k < 0) return;
     const bool fire = (P.flags & SPM_FLAG_FIRE) != 0;
@@ -82,7 +82,7 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
     float4* dp_out = (MODE == 0) ? disps + (size_t)k * nzs : nullptr;
     V3 v = mk3(0.f, 0.f, 0.f);
     float4 fe = make_float4(0.f, 0.f, 0.f, 0.f);
-    int iz = 0, it = 0;
+    int iz = 0, it = 0, total_it = 0;
     const int max_iter = P.max_iter;
     while (iz < nzs) {
         bool done = max_iter <= 0;
@@ -101,6 +101,7 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
             }
             md_step(f, v, pos, I, fire);
             ++it;
+            ++total_it;
             done = (dot3(f, f) < P.f2conv) || (it >= max_iter);
         }
         if (done) {
@@ -122,6 +123,7 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
             ++iz;
         }
     }
+    if (iter_count) iter_count[k] = total_it;
 }
 
 __global__ void __launch_bounds__(RX_THREADS)
@@ -147,10 +149,12 @@ raw_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_para
 int check_scan_args(const char* who, const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
                     const spm_scan_params* p, const float* out0) {
     SPM_REQUIRE(p != nullptr, "%s: null params", who);
-    SPM_REQUIRE(grid && points && out0, "%s: null grid/points/output pointer", who);
     SPM_REQUIRE(nx > 0 && ny > 0 && nz > 0, "%s: grid dims (%d,%d,%d) must be positive", who, nx, ny, nz);
     SPM_REQUIRE(n_scan >= 0, "%s: n_scan=%d < 0", who, n_scan);
     SPM_REQUIRE(p->nz >= 0, "%s: nz=%d < 0", who, p->nz);
+    SPM_REQUIRE(grid != nullptr, "%s: null grid", who);
+    if (n_scan > 0 && p->nz > 0)  // empty scans may pass null point/output buffers
+        SPM_REQUIRE(points && out0, "%s: null points/output pointer", who);
     SPM_REQUIRE(aligned16(grid) && aligned16(points) && aligned16(out0), "%s: buffers must be 16-byte aligned", who);
     long long t = 0;
     SPM_REQUIRE(mul_ok((long long)nx * ny, nz, &t), "%s: grid size overflows", who);
@@ -189,16 +193,22 @@ spm_scan_params normalized(const spm_scan_params* p, int n_scan) {
 
 extern "C" int spm_relax_strokes(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
                                  const spm_scan_params* p, float* FEs, float* disps, void* stream) {
+    return spm_relax_strokes_counted(grid, nx, ny, nz, points, n_scan, p, FEs, disps, nullptr, stream);
+}
+
+extern "C" int spm_relax_strokes_counted(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
+                                         const spm_scan_params* p, float* FEs, float* disps, int* iter_count,
+                                         void* stream) {
     using namespace spm;
     clear_error();
     int rc = check_scan_args("spm_relax_strokes", grid, nx, ny, nz, points, n_scan, p, FEs);
     if (rc) return rc;
-    SPM_REQUIRE(disps != nullptr && aligned16(disps), "spm_relax_strokes: disps null or misaligned");
     if (n_scan == 0 || p->nz == 0) return SPM_OK;
+    SPM_REQUIRE(disps != nullptr && aligned16(disps), "spm_relax_strokes: disps null or misaligned");
     spm_scan_params P = normalized(p, n_scan);
     relax_kernel<0><<<blocks_for(n_scan, P), RX_THREADS, 0, as_stream(stream)>>>(
         make_view(grid, nx, ny, nz, p), reinterpret_cast<const float4*>(points), n_scan, P,
-        reinterpret_cast<float4*>(FEs), reinterpret_cast<float4*>(disps));
+        reinterpret_cast<float4*>(FEs), reinterpret_cast<float4*>(disps), iter_count);
     return check_launch("spm_relax_strokes");
 }
 
@@ -212,7 +222,7 @@ extern "C" int spm_relax_strokes_tilted(const float* grid, int nx, int ny, int n
     spm_scan_params P = normalized(p, n_scan);
     relax_kernel<1><<<blocks_for(n_scan, P), RX_THREADS, 0, as_stream(stream)>>>(
         make_view(grid, nx, ny, nz, p), reinterpret_cast<const float4*>(points), n_scan, P,
-        reinterpret_cast<float4*>(FEs), nullptr);
+        reinterpret_cast<float4*>(FEs), nullptr, nullptr);
     return check_launch("spm_relax_strokes_tilted");
 }
 

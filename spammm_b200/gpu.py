@@ -68,16 +68,19 @@ def _grid_dims(grid):
     return int(nx), int(ny), int(nz)
 
 
-def relax_strokes(grid, params, points, FEs=None, disps=None):
-    """relaxStrokes over (n_scan,4) points -> FEs, disps (n_scan,nz,4)."""
+def relax_strokes(grid, params, points, FEs=None, disps=None, iter_count=None):
+    """relaxStrokes over (n_scan,4) points -> FEs, disps (n_scan,nz,4).
+    iter_count: optional int32 CUDA tensor (n_scan,) receiving per-pixel step totals."""
     nx, ny, nz = _grid_dims(grid)
     points = _as_dev(points, F32, (4,), "points")
     n_scan = points.shape[0]
     shape = (n_scan, params.nz, 4)
     FEs = torch.empty(shape, dtype=F32, device=points.device) if FEs is None else FEs
     disps = torch.empty(shape, dtype=F32, device=points.device) if disps is None else disps
-    rc = lib().spm_relax_strokes(ptr(grid), nx, ny, nz, ptr(points), n_scan, ctypes.byref(params), ptr(FEs),
-                                 ptr(disps), stream_ptr())
+    if iter_count is not None and (iter_count.dtype != torch.int32 or iter_count.numel() < n_scan):
+        raise ValueError("iter_count must be an int32 tensor with n_scan entries")
+    rc = lib().spm_relax_strokes_counted(ptr(grid), nx, ny, nz, ptr(points), n_scan, ctypes.byref(params), ptr(FEs),
+                                         ptr(disps), ptr(iter_count), stream_ptr())
     check(rc, "spm_relax_strokes")
     return FEs, disps
 

@@ -204,6 +204,20 @@ def test_df_kernels_match_reference(cuda, golden):
     np.testing.assert_allclose(AFM.compute_df_amp(g["Fz"], 0.1, 0.6), g["compute_df_amp"], rtol=1e-6, atol=1e-6)
 
 
+def test_df_z_column_kernel_matches_generic_kernel(cuda):
+    """n = z takes the column kernel; n = (1e-300, 0, 1) takes the generic kernel with
+    exactly the same arithmetic (the x shift rounds to zero) -> identical bits."""
+    rng = np.random.default_rng(11)
+    for dt in (np.float32, np.float64):
+        FEs = rng.standard_normal((7, 5, 43, 4)).astype(dt)
+        a = gpu.df_amp_dir(FEs, (0.1, 0.1, 0.1), (0, 0, 1), 1.0).cpu().numpy()
+        b = gpu.df_amp_dir(FEs, (0.1, 0.1, 0.1), (1e-300, 0, 1), 1.0).cpu().numpy()
+        assert np.array_equal(a, b)
+        a = gpu.df_amp_dir(FEs, (0.1, 0.1, 0.1), (0, 0, -1), 0.37, out_iz=[0, 42, 5]).cpu().numpy()
+        b = gpu.df_amp_dir(FEs, (0.1, 0.1, 0.1), (1e-300, 0, -1), 0.37, out_iz=[0, 42, 5]).cpu().numpy()
+        assert np.array_equal(a, b)
+
+
 def test_df_selected_slices(cuda):
     rng = np.random.default_rng(2)
     FEs = rng.standard_normal((9, 8, 31, 4)).astype(np.float32)
