@@ -100,13 +100,22 @@ int spm_relax_strokes(const float* grid, int nx, int ny, int nz,
                       const float* points, int n_scan, const spm_scan_params* p,
                       float* FEs, float* disps, void* stream);
 
-/* spm_relax_strokes plus telemetry: iter_count (DEVICE int[n_scan], may be
- * NULL) receives each pixel's integrator steps summed over its z-steps.  No
- * counterpart in the reference (its kernel reports nothing); results are
- * identical to spm_relax_strokes. */
-int spm_relax_strokes_counted(const float* grid, int nx, int ny, int nz,
-                              const float* points, int n_scan, const spm_scan_params* p,
-                              float* FEs, float* disps, int* iter_count, void* stream);
+/* Extended form of spm_relax_strokes (mode SPM_RELAX_STROKES) and
+ * spm_relax_strokes_tilted (mode SPM_RELAX_TILTED, disps unused); no
+ * counterpart in the reference, results identical to those two calls.
+ *   iter_count: DEVICE int[n_scan] or NULL -- each pixel's integrator steps
+ *               summed over its z-steps (telemetry);
+ *   workspace:  DEVICE buffer of spm_relax_workspace_bytes() bytes or NULL.
+ *               With a workspace, lanes take pixels from a device-side counter
+ *               (dynamic load balance across lanes, warps and CTA waves); the
+ *               call resets it on `stream`.  Calls that overlap on the device
+ *               must not share a workspace. */
+#define SPM_RELAX_STROKES 0
+#define SPM_RELAX_TILTED  1
+long long spm_relax_workspace_bytes(void);
+int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz,
+                 const float* points, int n_scan, const spm_scan_params* p,
+                 float* FEs, float* disps, int* iter_count, void* workspace, void* stream);
 
 /* Replaces AFMulator.run_scan -> relaxStrokesTilted (spammm/SPM/AFM.py:950-1010,
  * kernels/AFM.cl:478-562): tip-frame spring, surface bias, re-sampled FE after

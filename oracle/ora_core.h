@@ -51,6 +51,10 @@ static inline SFX(v3) SFX(rotmatT)(SFX(v3) v, SFX(v3) a, SFX(v3) b, SFX(v3) c) {
 /* tipForce                                               AFM.cl:53-58
  * (dpos-dpos0.xyz)*k.xyz + dpos*(k.w*(r-dpos0.w)/r), r = max(|dpos|,1e-10) */
 static inline SFX(v3) SFX(tip_force)(SFX(v3) d, const REAL* k, const REAL* d0) {
+    /* k.w == 0: the radial term is exactly +-0 and is skipped (the CUDA kernels
+     * skip it too; only the sign of an all-zero component can differ). */
+    if (k[3] == (REAL)0)
+        return SFX(mk3)((d.x - d0[0]) * k[0], (d.y - d0[1]) * k[1], (d.z - d0[2]) * k[2]);
     REAL r = SQRT(SFX(dot3)(d, d));
     r = FMAX(r, (REAL)1e-10);
     REAL s = (k[3] * (r - d0[3])) / r;

@@ -25,6 +25,8 @@ SPM_KIND_MORSE = 1
 SPM_F32 = 0
 SPM_F64 = 1
 SPM_FLAG_FIRE = 1
+SPM_RELAX_STROKES = 0
+SPM_RELAX_TILTED = 1
 SPM_FLAG_FLIP_Z = 2
 
 _f4 = ctypes.c_float * 4
@@ -88,7 +90,8 @@ _SIGNATURES = {
     "spm_last_error": (ctypes.c_char_p, []),
     "spm_grid_build": (_i, [_i, _i, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "spm_relax_strokes": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp, _vp]),
-    "spm_relax_strokes_counted": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp, _vp, _vp]),
+    "spm_relax_ex": (_i, [_i, _vp, _i, _i, _i, _vp, _i, _P, _vp, _vp, _vp, _vp, _vp]),
+    "spm_relax_workspace_bytes": (_ll, []),
     "spm_relax_strokes_tilted": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp]),
     "spm_fe_in_strokes_tilted": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp]),
     "spm_df_amp_dir": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _d, _vp, _i, _vp, _vp]),

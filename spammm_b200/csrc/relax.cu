@@ -5,16 +5,18 @@
 // (AFM.cl:478-562, AFMulator.run_scan, AFM.py:995-1004) and the raw sampler
 // getFEinStrokesTilted (AFM.cl:210-233, AFMulator.get_raw_FE, AFM.py:2565-2574).
 //
-// The reference launches one work-item per work-group (local size 1).  Here a
-// CTA of 128 threads covers an 8 (ix) x 16 (iy) pixel block and each warp a
-// compact 4 x 8 block, so the eight texel rows a warp reads per step overlap in
-// L1.  The stroke state (pos, v, dt, damp, tipPos) lives in registers.  Each
-// lane runs its own (z-step, iteration) sequence as one flattened loop: a lane
-// that converges moves straight on to its next z-step instead of waiting for
-// the slowest lane of the warp, so a warp costs max over lanes of the TOTAL
-// iterations rather than the sum over z of per-step maxima.  Per-pixel
-// arithmetic is exactly the reference's sequence (see spm_fire.cuh), so the
-// flattening changes no result bit.
+// The reference launches one work-item per work-group (local size 1).  Here
+// every lane runs one flattened loop over (pixel, z-step, integrator step) with
+// the stroke state (pos, v, dt, damp, tipPos) in registers:
+//   * a lane that converges moves straight on to its next z-step, and -- when
+//     a device-side pixel counter is supplied -- a lane that finishes its pixel
+//     takes the next one (warp-aggregated atomicAdd), so no lane idles while
+//     the slowest lane of its warp or the last CTA wave finishes;
+//   * pixels are handed out in 4 (ix) x 8 (iy) tiles, so the eight texel rows
+//     a warp reads per step overlap in L1 and the in-flight set stays local;
+//   * node offsets are 32-bit when the grid has fewer than 2^32 nodes.
+// Per-pixel arithmetic is exactly the reference's sequence (spm_fire.cuh), so
+// neither the scheduling nor the flattening changes a result bit.
 //
 // This translation unit is compiled with -fmad=false: the only fused
 // multiply-adds are the explicit __fmaf_rn calls shared with the CPU oracle.
@@ -26,7 +28,7 @@ namespace {
 
 constexpr int RX_THREADS = 128;
 
-// Pixel owned by this thread (ix-major raster index k) or -1.
+// Pixel of this thread under the static schedule (one pixel per lane), or -1.
 __device__ __forceinline__ int pixel_of_thread(int n_scan, int raster_ny) {
     if (raster_ny > 0) {
         const int nxr = n_scan / raster_ny;
@@ -42,58 +44,85 @@ __device__ __forceinline__ int pixel_of_thread(int n_scan, int raster_ny) {
     return k < n_scan ? k : -1;
 }
 
+// Next pixel from the device counter (dynamic schedule), or -1 when drained.
+// Counter slot t maps to tile t/32 (4x8 pixels, tiles ordered iy-fastest).
+__device__ __forceinline__ int next_pixel(unsigned* counter, int n_scan, int raster_ny) {
+    const unsigned lane = threadIdx.x & 31u;
+    const int ny = raster_ny;
+    const int nxr = ny > 0 ? n_scan / ny : 0;
+    const unsigned nty = ny > 0 ? (unsigned)(ny + 7) / 8 : 0u;
+    const unsigned nslots = ny > 0 ? ((unsigned)(nxr + 3) / 4) * nty * 32u : (unsigned)n_scan;
+    while (true) {
+        const unsigned m = __activemask();
+        const int leader = __ffs(m) - 1;
+        const unsigned rank = __popc(m & ((1u << lane) - 1u));
+        unsigned base = 0;
+        if ((int)lane == leader) base = atomicAdd(counter, (unsigned)__popc(m));
+        base = __shfl_sync(m, base, leader);
+        const unsigned t = base + rank;
+        if (t >= nslots) return -1;
+        if (ny <= 0) return (int)t;
+        const unsigned tile = t >> 5, r = t & 31u;
+        const int ix = (int)((tile / nty) * 4 + (r >> 3));
+        const int iy = (int)((tile % nty) * 8 + (r & 7));
+        if (ix < nxr && iy < ny) return ix * ny + iy;
+        // an edge tile's slot outside the raster: draw again (t only grows: bounded)
+    }
+}
+
 __device__ __forceinline__ float4 ld4(const float* a) { return make_float4(a[0], a[1], a[2], a[3]); }
 
 // MODE 0: relaxStrokes; MODE 1: relaxStrokesTilted.
-template <int MODE>
+template <int MODE, typename IDX>
 __global__ void __launch_bounds__(RX_THREADS)
 relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
-             float4* __restrict__ FEs, float4* __restrict__ disps, int* __restrict__ iter_count) {
-    const int k = pixel_of_thread(n_scan, P.raster_ny);
-    if (k < 0) return;
+             float4* __restrict__ FEs, float4* __restrict__ disps, int* __restrict__ iter_count,
+             unsigned* __restrict__ counter) {
     const bool fire = (P.flags & SPM_FLAG_FIRE) != 0;
     const bool flip = (P.flags & SPM_FLAG_FLIP_Z) != 0;
     const int nzs = P.nz;
+    const int max_iter = P.max_iter;
     const float4 kk = ld4(P.stiffness), d0 = ld4(P.dpos0);
     const float4 tc = ld4(P.tipC);
     const V3 a = mk3(P.tipA[0], P.tipA[1], P.tipA[2]);
     const V3 b = mk3(P.tipB[0], P.tipB[1], P.tipB[2]);
     const V3 c = mk3(tc.x, tc.y, tc.z);
     const float surf = P.surfFF[0];
+    const V3 dTip = (MODE == 0) ? mk3(P.dTip[0], P.dTip[1], P.dTip[2])
+                                : mk3(__fmul_rn(c.x, tc.w), __fmul_rn(c.y, tc.w), __fmul_rn(c.z, tc.w));
+    const V3 d0r = (MODE == 0) ? mk3(d0.x, d0.y, d0.z) : rotmatT(mk3(d0.x, d0.y, d0.z), a, b, c);
 
-    const float4 p4 = pts[k];
-    V3 tip = mk3(p4.x, p4.y, p4.z);
-    V3 pos, dTip;
-    if (MODE == 0) {
-        pos = mk3(tip.x + d0.x, tip.y + d0.y, tip.z + d0.z);
-        dTip = mk3(P.dTip[0], P.dTip[1], P.dTip[2]);
-    } else {
-        pos = add3(tip, rotmatT(mk3(d0.x, d0.y, d0.z), a, b, c));
-        dTip = mk3(__fmul_rn(c.x, tc.w), __fmul_rn(c.y, tc.w), __fmul_rn(c.z, tc.w));
-    }
+    int k = counter ? next_pixel(counter, n_scan, P.raster_ny) : pixel_of_thread(n_scan, P.raster_ny);
+    V3 tip, pos, v;
     Integrator I;
-    I.dt = P.relax_params[0];
-    I.damp = P.relax_params[1];
-    I.dtmax = I.dt;
-    I.dtmin = __fmul_rn(I.dtmax, 0.1f);
-    I.damp0 = I.damp;
-
-    float4* fe_out = FEs + (size_t)k * nzs;
-    float4* dp_out = (MODE == 0) ? disps + (size_t)k * nzs : nullptr;
-    V3 v = mk3(0.f, 0.f, 0.f);
-    float4 fe = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 fe;
     int iz = 0, it = 0, total_it = 0;
-    const int max_iter = P.max_iter;
-    while (iz < nzs) {
+    auto start = [&](int kp) {
+        const float4 p4 = pts[kp];
+        tip = mk3(p4.x, p4.y, p4.z);
+        pos = (MODE == 0) ? mk3(tip.x + d0r.x, tip.y + d0r.y, tip.z + d0r.z) : add3(tip, d0r);
+        I.dt = P.relax_params[0];
+        I.damp = P.relax_params[1];
+        I.dtmax = I.dt;
+        I.dtmin = __fmul_rn(I.dtmax, 0.1f);
+        I.damp0 = I.damp;
+        v = mk3(0.f, 0.f, 0.f);
+        fe = make_float4(0.f, 0.f, 0.f, 0.f);
+        iz = 0;
+        it = 0;
+        total_it = 0;
+    };
+    if (k >= 0) start(k);
+    while (k >= 0) {
         bool done = max_iter <= 0;
         if (!done) {
-            fe = interp_fe(G, pos);
+            fe = interp_fe<IDX>(G, pos);
             V3 f;
             if (MODE == 0) {
-                V3 ft = tip_force(sub3(pos, tip), kk, d0);
+                const V3 ft = tip_force(sub3(pos, tip), kk, d0);
                 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
             } else {
-                V3 ft = rotmatT(tip_force(rotmat(sub3(pos, tip), a, b, c), kk, d0), a, b, c);
+                const V3 ft = rotmatT(tip_force(rotmat(sub3(pos, tip), a, b, c), kk, d0), a, b, c);
                 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
                 f.x = __fmaf_rn(c.x, surf, f.x);
                 f.y = __fmaf_rn(c.y, surf, f.y);
@@ -106,24 +135,28 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
         }
         if (done) {
             const int oz = flip ? (nzs - 1 - iz) : iz;
+            const size_t o = (size_t)k * nzs + oz;
             if (MODE == 0) {
-                fe_out[oz] = fe;
+                FEs[o] = fe;
                 const V3 ref = mk3(tip.x + d0.x, tip.y + d0.y, tip.z + d0.z);
-                dp_out[oz] = make_float4(pos.x - ref.x, pos.y - ref.y, pos.z - ref.z, 0.f);
+                disps[o] = make_float4(pos.x - ref.x, pos.y - ref.y, pos.z - ref.z, 0.f);
             } else {
-                const float4 g = interp_fe(G, pos);
+                const float4 g = interp_fe<IDX>(G, pos);
                 const V3 r = rotmat(mk3(g.x, g.y, g.z), a, b, c);
-                fe_out[oz] = make_float4(r.x, r.y, r.z, g.w);
+                FEs[o] = make_float4(r.x, r.y, r.z, g.w);
             }
             tip = add3(tip, dTip);
             pos = add3(pos, dTip);
             v = mk3(0.f, 0.f, 0.f);
             fe = make_float4(0.f, 0.f, 0.f, 0.f);
             it = 0;
-            ++iz;
+            if (++iz == nzs) {
+                if (iter_count) iter_count[k] = total_it;
+                k = counter ? next_pixel(counter, n_scan, P.raster_ny) : -1;
+                if (k >= 0) start(k);
+            }
         }
     }
-    if (iter_count) iter_count[k] = total_it;
 }
 
 __global__ void __launch_bounds__(RX_THREADS)
@@ -139,7 +172,7 @@ raw_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_para
     const bool flip = (P.flags & SPM_FLAG_FLIP_Z) != 0;
     float4* out = FEs + (size_t)k * P.nz;
     for (int iz = 0; iz < P.nz; iz++) {
-        const float4 g = interp_fe(G, pos);
+        const float4 g = interp_fe<size_t>(G, pos);
         const V3 r = rotmat(mk3(g.x, g.y, g.z), a, b, c);
         out[flip ? (P.nz - 1 - iz) : iz] = make_float4(r.x, r.y, r.z, g.w);
         pos = add3(pos, dTip);
@@ -174,7 +207,7 @@ GridView make_view(const float* grid, int nx, int ny, int nz, const spm_scan_par
     return G;
 }
 
-int blocks_for(int n_scan, const spm_scan_params& P) {
+int static_blocks(int n_scan, const spm_scan_params& P) {
     if (P.raster_ny > 0) {
         const int nxr = n_scan / P.raster_ny;
         return ((nxr + 7) / 8) * ((P.raster_ny + 15) / 16);
@@ -188,42 +221,74 @@ spm_scan_params normalized(const spm_scan_params* p, int n_scan) {
     return P;
 }
 
+template <int MODE, typename IDX>
+int launch_relax(const GridView& G, const float4* pts, int n_scan, const spm_scan_params& P, float4* FEs,
+                 float4* disps, int* iter_count, unsigned* counter, cudaStream_t st) {
+    auto kern = relax_kernel<MODE, IDX>;
+    int blocks = static_blocks(n_scan, P);
+    if (counter) {
+        // persistent: as many CTAs as are co-resident; the counter balances the rest
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RX_THREADS, 0) != cudaSuccess)
+            return set_error(SPM_ERR_CUDA, "relax: cannot query the device occupancy");
+        const int cap = sms * (per_sm > 0 ? per_sm : 1);
+        const int need = (n_scan + RX_THREADS - 1) / RX_THREADS;
+        blocks = need < cap ? need : cap;
+        if (cudaMemsetAsync(counter, 0, sizeof(unsigned), st) != cudaSuccess)
+            return set_error(SPM_ERR_CUDA, "relax: cannot reset the pixel counter");
+    }
+    kern<<<blocks, RX_THREADS, 0, st>>>(G, pts, n_scan, P, FEs, disps, iter_count, counter);
+    return check_launch("relax");
+}
+
+template <int MODE>
+int launch_mode(const GridView& G, long long nodes, const float4* pts, int n_scan, const spm_scan_params& P,
+                float4* FEs, float4* disps, int* iter_count, unsigned* counter, cudaStream_t st) {
+    if (nodes < (1LL << 32))
+        return launch_relax<MODE, unsigned>(G, pts, n_scan, P, FEs, disps, iter_count, counter, st);
+    return launch_relax<MODE, size_t>(G, pts, n_scan, P, FEs, disps, iter_count, counter, st);
+}
+
 }  // namespace
 }  // namespace spm
 
-extern "C" int spm_relax_strokes(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
-                                 const spm_scan_params* p, float* FEs, float* disps, void* stream) {
-    return spm_relax_strokes_counted(grid, nx, ny, nz, points, n_scan, p, FEs, disps, nullptr, stream);
-}
+extern "C" long long spm_relax_workspace_bytes(void) { return 16; }
 
-extern "C" int spm_relax_strokes_counted(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
-                                         const spm_scan_params* p, float* FEs, float* disps, int* iter_count,
-                                         void* stream) {
+extern "C" int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
+                            const spm_scan_params* p, float* FEs, float* disps, int* iter_count, void* workspace,
+                            void* stream) {
     using namespace spm;
     clear_error();
-    int rc = check_scan_args("spm_relax_strokes", grid, nx, ny, nz, points, n_scan, p, FEs);
+    SPM_REQUIRE(mode == SPM_RELAX_STROKES || mode == SPM_RELAX_TILTED, "spm_relax_ex: mode=%d", mode);
+    int rc = check_scan_args("spm_relax_ex", grid, nx, ny, nz, points, n_scan, p, FEs);
     if (rc) return rc;
     if (n_scan == 0 || p->nz == 0) return SPM_OK;
-    SPM_REQUIRE(disps != nullptr && aligned16(disps), "spm_relax_strokes: disps null or misaligned");
+    if (mode == SPM_RELAX_STROKES)
+        SPM_REQUIRE(disps != nullptr && aligned16(disps), "spm_relax_ex: disps null or misaligned");
+    SPM_REQUIRE(workspace == nullptr || (reinterpret_cast<uintptr_t>(workspace) & 3u) == 0,
+                "spm_relax_ex: workspace not 4-byte aligned");
     spm_scan_params P = normalized(p, n_scan);
-    relax_kernel<0><<<blocks_for(n_scan, P), RX_THREADS, 0, as_stream(stream)>>>(
-        make_view(grid, nx, ny, nz, p), reinterpret_cast<const float4*>(points), n_scan, P,
-        reinterpret_cast<float4*>(FEs), reinterpret_cast<float4*>(disps), iter_count);
-    return check_launch("spm_relax_strokes");
+    const GridView G = make_view(grid, nx, ny, nz, p);
+    const long long nodes = (long long)nx * ny * nz;
+    const float4* pt = reinterpret_cast<const float4*>(points);
+    unsigned* ctr = static_cast<unsigned*>(workspace);
+    cudaStream_t st = as_stream(stream);
+    if (mode == SPM_RELAX_STROKES)
+        return launch_mode<0>(G, nodes, pt, n_scan, P, reinterpret_cast<float4*>(FEs),
+                              reinterpret_cast<float4*>(disps), iter_count, ctr, st);
+    return launch_mode<1>(G, nodes, pt, n_scan, P, reinterpret_cast<float4*>(FEs), nullptr, iter_count, ctr, st);
+}
+
+extern "C" int spm_relax_strokes(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
+                                 const spm_scan_params* p, float* FEs, float* disps, void* stream) {
+    return spm_relax_ex(SPM_RELAX_STROKES, grid, nx, ny, nz, points, n_scan, p, FEs, disps, nullptr, nullptr, stream);
 }
 
 extern "C" int spm_relax_strokes_tilted(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
                                         const spm_scan_params* p, float* FEs, void* stream) {
-    using namespace spm;
-    clear_error();
-    int rc = check_scan_args("spm_relax_strokes_tilted", grid, nx, ny, nz, points, n_scan, p, FEs);
-    if (rc) return rc;
-    if (n_scan == 0 || p->nz == 0) return SPM_OK;
-    spm_scan_params P = normalized(p, n_scan);
-    relax_kernel<1><<<blocks_for(n_scan, P), RX_THREADS, 0, as_stream(stream)>>>(
-        make_view(grid, nx, ny, nz, p), reinterpret_cast<const float4*>(points), n_scan, P,
-        reinterpret_cast<float4*>(FEs), nullptr, nullptr);
-    return check_launch("spm_relax_strokes_tilted");
+    return spm_relax_ex(SPM_RELAX_TILTED, grid, nx, ny, nz, points, n_scan, p, FEs, nullptr, nullptr, nullptr, stream);
 }
 
 extern "C" int spm_fe_in_strokes_tilted(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
@@ -234,7 +299,7 @@ extern "C" int spm_fe_in_strokes_tilted(const float* grid, int nx, int ny, int n
     if (rc) return rc;
     if (n_scan == 0 || p->nz == 0) return SPM_OK;
     spm_scan_params P = normalized(p, n_scan);
-    raw_kernel<<<blocks_for(n_scan, P), RX_THREADS, 0, as_stream(stream)>>>(
+    raw_kernel<<<static_blocks(n_scan, P), RX_THREADS, 0, as_stream(stream)>>>(
         make_view(grid, nx, ny, nz, p), reinterpret_cast<const float4*>(points), n_scan, P,
         reinterpret_cast<float4*>(FEs));
     return check_launch("spm_fe_in_strokes_tilted");

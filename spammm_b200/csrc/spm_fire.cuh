@@ -31,8 +31,12 @@ __device__ __forceinline__ V3 rotmatT(V3 v, V3 a, V3 b, V3 c) {
               __fmaf_rn(c.z, v.z, __fmaf_rn(b.z, v.y, __fmul_rn(a.z, v.x)))};
 }
 
-// Harmonic 3D spring + radial bond: (d - d0.xyz)*k.xyz + d*(k.w*(r - d0.w)/r)
+// Harmonic 3D spring + radial bond: (d - d0.xyz)*k.xyz + d*(k.w*(r - d0.w)/r).
+// With k.w == 0 the radial term is exactly +-0 and is skipped (only the sign of
+// an all-zero component can differ from adding it; the oracle does the same).
 __device__ __forceinline__ V3 tip_force(V3 d, float4 k, float4 d0) {
+    if (k.w == 0.f)
+        return V3{__fmul_rn(d.x - d0.x, k.x), __fmul_rn(d.y - d0.y, k.y), __fmul_rn(d.z - d0.z, k.z)};
     float r = __fsqrt_rn(dot3(d, d));
     r = fmaxf(r, 1e-10f);
     float s = __fdiv_rn(__fmul_rn(k.w, r - d0.w), r);
@@ -108,7 +112,9 @@ struct GridView {
     float4 dA, dB, dC;  // normalized-coordinate transform rows
 };
 
-// interpFE: exact FP32 trilinear sample with periodic wrap.
+// interpFE: exact FP32 trilinear sample with periodic wrap.  IDX is the type
+// of the node offsets (unsigned for grids below 2^32 nodes, size_t above).
+template <typename IDX = size_t>
 __device__ __forceinline__ float4 interp_fe(const GridView& G, V3 p) {
     float u = __fmaf_rn(p.x, G.dA.x, __fmaf_rn(p.y, G.dA.y, __fmaf_rn(p.z, G.dA.z, G.dA.w)));
     float v = __fmaf_rn(p.x, G.dB.x, __fmaf_rn(p.y, G.dB.y, __fmaf_rn(p.z, G.dB.z, G.dB.w)));
@@ -123,8 +129,8 @@ __device__ __forceinline__ float4 interp_fe(const GridView& G, V3 p) {
         return make_float4(nan, nan, nan, nan);
     }
     float mx = 1.f - ax, my = 1.f - ay, mz = 1.f - az;
-    size_t r00 = ((size_t)z0 * G.ny + y0) * G.nx, r10 = ((size_t)z0 * G.ny + y1) * G.nx;
-    size_t r01 = ((size_t)z1 * G.ny + y0) * G.nx, r11 = ((size_t)z1 * G.ny + y1) * G.nx;
+    const IDX r00 = ((IDX)z0 * G.ny + y0) * G.nx, r10 = ((IDX)z0 * G.ny + y1) * G.nx;
+    const IDX r01 = ((IDX)z1 * G.ny + y0) * G.nx, r11 = ((IDX)z1 * G.ny + y1) * G.nx;
     float4 f000 = __ldg(G.g + r00 + x0), f100 = __ldg(G.g + r00 + x1);
     float4 f010 = __ldg(G.g + r10 + x0), f110 = __ldg(G.g + r10 + x1);
     float4 f001 = __ldg(G.g + r01 + x0), f101 = __ldg(G.g + r01 + x1);

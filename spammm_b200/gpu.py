@@ -68,9 +68,18 @@ def _grid_dims(grid):
     return int(nx), int(ny), int(nz)
 
 
-def relax_strokes(grid, params, points, FEs=None, disps=None, iter_count=None):
+def _workspace(device):
+    """A fresh relaxation workspace (the pixel counter); per call, so concurrent
+    launches on different streams never share one."""
+    n = int(lib().spm_relax_workspace_bytes())
+    return torch.empty(((n + 3) // 4,), dtype=torch.int32, device=device)
+
+
+def relax_strokes(grid, params, points, FEs=None, disps=None, iter_count=None, dynamic=True):
     """relaxStrokes over (n_scan,4) points -> FEs, disps (n_scan,nz,4).
-    iter_count: optional int32 CUDA tensor (n_scan,) receiving per-pixel step totals."""
+
+    iter_count: optional int32 CUDA tensor (n_scan,) receiving per-pixel step
+    totals; dynamic: lanes draw pixels from a device counter (same results)."""
     nx, ny, nz = _grid_dims(grid)
     points = _as_dev(points, F32, (4,), "points")
     n_scan = points.shape[0]
@@ -79,19 +88,21 @@ def relax_strokes(grid, params, points, FEs=None, disps=None, iter_count=None):
     disps = torch.empty(shape, dtype=F32, device=points.device) if disps is None else disps
     if iter_count is not None and (iter_count.dtype != torch.int32 or iter_count.numel() < n_scan):
         raise ValueError("iter_count must be an int32 tensor with n_scan entries")
-    rc = lib().spm_relax_strokes_counted(ptr(grid), nx, ny, nz, ptr(points), n_scan, ctypes.byref(params), ptr(FEs),
-                                         ptr(disps), ptr(iter_count), stream_ptr())
+    ws = _workspace(points.device) if dynamic else None
+    rc = lib().spm_relax_ex(_lib.SPM_RELAX_STROKES, ptr(grid), nx, ny, nz, ptr(points), n_scan, ctypes.byref(params),
+                            ptr(FEs), ptr(disps), ptr(iter_count), ptr(ws), stream_ptr())
     check(rc, "spm_relax_strokes")
     return FEs, disps
 
 
-def relax_strokes_tilted(grid, params, points, FEs=None):
+def relax_strokes_tilted(grid, params, points, FEs=None, dynamic=True):
     nx, ny, nz = _grid_dims(grid)
     points = _as_dev(points, F32, (4,), "points")
     n_scan = points.shape[0]
     FEs = torch.empty((n_scan, params.nz, 4), dtype=F32, device=points.device) if FEs is None else FEs
-    rc = lib().spm_relax_strokes_tilted(ptr(grid), nx, ny, nz, ptr(points), n_scan, ctypes.byref(params), ptr(FEs),
-                                        stream_ptr())
+    ws = _workspace(points.device) if dynamic else None
+    rc = lib().spm_relax_ex(_lib.SPM_RELAX_TILTED, ptr(grid), nx, ny, nz, ptr(points), n_scan, ctypes.byref(params),
+                            ptr(FEs), None, None, ptr(ws), stream_ptr())
     check(rc, "spm_relax_strokes_tilted")
     return FEs
 

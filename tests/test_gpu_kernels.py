@@ -122,6 +122,26 @@ def test_relax_strokes_pixel_mapping_does_not_change_results(cuda):
         assert torch.equal(x[0], y[0]) and torch.equal(x[1], y[1])
 
 
+def test_relax_dynamic_schedule_is_bit_identical(cuda):
+    """Pixel counter (dynamic) vs one-pixel-per-lane (static) schedule, raster and
+    1-D maps, strokes and tilted: identical FEs, displacements and step counts."""
+    grid, dinv, pts, nz = _relax_setup(seed=8, n_side=23)
+    pt = torch.from_numpy(pts).cuda()
+    for ny in (25, 0):
+        P = _lib.make_scan_params(dinv=dinv, dTip=[0, 0, -0.1, 0], stiffness=[-0.0156, -0.0156, -1.25, 0],
+                                  relax_params=[0.5, 0.1, 0.02, 0.5], nz=nz, max_iter=1000, f2conv=1e-10,
+                                  flip_z=True, raster_ny=ny)
+        ca = torch.empty(pt.shape[0], dtype=torch.int32, device="cuda")
+        cb = torch.empty_like(ca)
+        a = gpu.relax_strokes(grid, P, pt, iter_count=ca, dynamic=True)
+        b = gpu.relax_strokes(grid, P, pt, iter_count=cb, dynamic=False)
+        assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) and torch.equal(ca, cb)
+        assert int(ca.min()) >= nz
+        t1 = gpu.relax_strokes_tilted(grid, P, pt, dynamic=True)
+        t2 = gpu.relax_strokes_tilted(grid, P, pt, dynamic=False)
+        assert torch.equal(t1, t2)
+
+
 def test_relax_strokes_empty_and_ragged(cuda):
     grid, dinv, pts, nz = _relax_setup()
     P = _lib.make_scan_params(dinv=dinv, dTip=[0, 0, -0.1, 0], stiffness=[-0.02, -0.02, -1, 0],
