@@ -166,6 +166,26 @@ int spm_dissipation(const void* FEs_fwd, const void* FEs_bwd, int fes_dtype, int
  * (nx,ny,nz) float64 (weights NULL = 1 inside, 0 on the two boundary slices);
  * df_out (nx,ny,nz) f64, dL_dFEs (nx,ny,nz,4) f32, loss_out: device double[1].
  * Uses `scratch` (device, >= spm_df_loss_scratch_bytes(nx,ny,nz) bytes). */
+/* spm_df_loss_seed for callers that cannot allocate device memory around the
+ * call (their allocator owns all device memory, or a cudaMalloc/cudaFree and
+ * its implicit synchronisation is not allowed in their loop).  No counterpart
+ * in the reference.  It takes no scratch: the per-block partial sums live in a
+ * fixed 1 MiB device array inside the library, which every GPU that loads the
+ * library holds until the process exits.  Limits and rules:
+ *   - nx*ny*nz <= SPM_DF_LOSS_NOALLOC_MAX_ELEMS, else SPM_ERR_UNSUPPORTED;
+ *   - the first call on each device looks up that array's device address
+ *     (cudaGetSymbolAddress, with the device current); make that first call
+ *     before any stream capture;
+ *   - all calls on a device share the array: calls that overlap on the GPU
+ *     (e.g. on two streams at once) race and give wrong results; serialise them;
+ *   - every slot a call reads is written earlier by the same call, so no state
+ *     carries over from the previous call;
+ *   - allocates nothing (no cudaMalloc/cudaFree or allocating library call). */
+#define SPM_DF_LOSS_NOALLOC_MAX_ELEMS 16777216LL
+int spm_df_loss_seed_noalloc(const void* FEs, int fes_dtype, const double* target, const double* weights,
+                             int nx, int ny, int nz, double dtip, double* df_out, float* dL_dFEs,
+                             double* loss_out, void* stream);
+
 int spm_df_loss_seed(const void* FEs, int fes_dtype, const double* target, const double* weights,
                      int nx, int ny, int nz, double dtip, double* df_out, float* dL_dFEs,
                      double* loss_out, void* scratch, void* stream);

@@ -99,6 +99,7 @@ _SIGNATURES = {
     "spm_dissipation": (_i, [_vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp]),
     "spm_df_loss_seed": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _d, _vp, _vp, _vp, _vp, _vp]),
     "spm_df_loss_scratch_bytes": (_ll, [_i, _i, _i]),
+    "spm_df_loss_seed_noalloc": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _d, _vp, _vp, _vp, _vp]),
     "spm_relax_direct_morse": (_i, [_i, _vp, _vp, _vp, _i, _P, _vp, _vp, _vp, _vp, _vp]),
     "spm_adjoint_direct_state": (_i, [_i, _vp, _vp, _vp, _i, _P, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "spm_adjoint_direct_params": (_i, [_i, _vp, _vp, _vp, _i, _P, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

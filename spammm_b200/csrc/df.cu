@@ -476,3 +476,91 @@ extern "C" int spm_df_loss_seed(const void* FEs, int fes_dtype, const double* ta
                                                             1.0 / (2.0 * dz), reinterpret_cast<float4*>(dL_dFEs));
     return check_launch("spm_df_loss_seed");
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free df loss seed.
+//
+// Some callers cannot allocate device memory around this call: code that runs
+// inside a host framework whose allocator owns all device memory (and may not
+// be re-entered from the loss callback), callers that must never trigger an
+// implicit device synchronisation from cudaMalloc/cudaFree in a latency-bound
+// fitting loop, or callers that hold device memory budgets fixed up front.
+// For them spm_df_loss_seed_noalloc takes no scratch argument: its per-block
+// partial sums live in a fixed file-scope device array of
+// SPM_DF_LOSS_NOALLOC_MAX_ELEMS / 256 (w, w*diff^2) pairs (1 MiB) that every
+// GPU loading this library holds until the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace spm {
+namespace {
+
+constexpr long long NOALLOC_MAX_BLOCKS = SPM_DF_LOSS_NOALLOC_MAX_ELEMS / LS_THREADS;
+// Shared by every call on a device: partials of block b at [2b, 2b+1], the
+// final (wsum, sum) pair after them.  Each call overwrites every slot it later
+// reads, so nothing has to be cleared between calls.
+static __device__ __align__(256) double g_loss_scratch[2 * NOALLOC_MAX_BLOCKS + 2];
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_scratch_mutex;
+double* g_scratch_addr[MAX_DEVICES] = {nullptr};
+
+// Device address of g_loss_scratch on the current device (resolved once per
+// device with that device current; the host-side symbol is not a device address).
+int loss_scratch_address(double** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error(SPM_ERR_CUDA, "spm_df_loss_seed_noalloc: cudaGetDevice: %s",
+                                           cudaGetErrorString(e));
+    if (dev < 0 || dev >= MAX_DEVICES)
+        return set_error(SPM_ERR_UNSUPPORTED, "spm_df_loss_seed_noalloc: device ordinal %d >= %d", dev, MAX_DEVICES);
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (g_scratch_addr[dev] == nullptr) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_loss_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            return set_error(SPM_ERR_CUDA, "spm_df_loss_seed_noalloc: cudaGetSymbolAddress: %s",
+                             cudaGetErrorString(e));
+        g_scratch_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_scratch_addr[dev];
+    return SPM_OK;
+}
+
+}  // namespace
+}  // namespace spm
+
+extern "C" int spm_df_loss_seed_noalloc(const void* FEs, int fes_dtype, const double* target, const double* weights,
+                                        int nx, int ny, int nz, double dtip, double* df_out, float* dL_dFEs,
+                                        double* loss_out, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(FEs && target && df_out && dL_dFEs && loss_out, "spm_df_loss_seed_noalloc: null pointer");
+    SPM_REQUIRE(fes_dtype == SPM_F32 || fes_dtype == SPM_F64, "spm_df_loss_seed_noalloc: fes_dtype=%d", fes_dtype);
+    SPM_REQUIRE(nx > 0 && ny > 0, "spm_df_loss_seed_noalloc: nx=%d ny=%d must be positive", nx, ny);
+    SPM_REQUIRE(nz >= 3, "spm_df_loss_seed_noalloc: need nz>=3 for central difference, got nz=%d", nz);
+    SPM_REQUIRE(dtip < 0.0, "spm_df_loss_seed_noalloc: dtip must be <0, got dtip=%g", dtip);
+    SPM_REQUIRE(aligned16(FEs) && aligned16(dL_dFEs), "spm_df_loss_seed_noalloc: FEs/dL_dFEs not 16-byte aligned");
+    const long long total = (long long)nx * ny * nz;
+    if (total > SPM_DF_LOSS_NOALLOC_MAX_ELEMS)
+        return set_error(SPM_ERR_UNSUPPORTED,
+                         "spm_df_loss_seed_noalloc: volume of %lld elements exceeds the fixed scratch limit of %lld "
+                         "(use spm_df_loss_seed with caller scratch)", total, (long long)SPM_DF_LOSS_NOALLOC_MAX_ELEMS);
+    double* partial = nullptr;
+    int rc = loss_scratch_address(&partial);
+    if (rc) return rc;
+    const long long nblk = (total + LS_THREADS - 1) / LS_THREADS;
+    double* sums = partial + 2 * nblk;
+    const double dz = fabs(dtip);
+    cudaStream_t st = as_stream(stream);
+    if (fes_dtype == SPM_F32)
+        loss_partials_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(static_cast<const float*>(FEs), target, weights,
+                                                                    nx, ny, nz, 2.0 * dz, df_out, partial);
+    else
+        loss_partials_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(static_cast<const double*>(FEs), target, weights,
+                                                                    nx, ny, nz, 2.0 * dz, df_out, partial);
+    loss_final_kernel<<<1, LS_THREADS, 0, st>>>(partial, (int)nblk, sums, loss_out);
+    loss_grad_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(df_out, target, weights, sums, nx, ny, nz,
+                                                            1.0 / (2.0 * dz), reinterpret_cast<float4*>(dL_dFEs));
+    return check_launch("spm_df_loss_seed_noalloc");
+}
