@@ -112,6 +112,12 @@ int spm_relax_strokes(const float* grid, int nx, int ny, int nz,
  *               must not share a workspace. */
 #define SPM_RELAX_STROKES 0
 #define SPM_RELAX_TILTED  1
+/* SPM_RELAX_PP: the tilted relaxation with the direct path's equilibrium
+ * bookkeeping (kernels/AFM.cl:1441-1505) on the grid -- convergence tested
+ * before each update, FEs sampled at the stored position, and `disps`
+ * receiving PPs = (pos, +iters converged / -iters not).  The forward of the
+ * differentiable grid path (spm_adjoint_grid_*). */
+#define SPM_RELAX_PP      2
 long long spm_relax_workspace_bytes(void);
 int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz,
                  const float* points, int n_scan, const spm_scan_params* p,
@@ -223,6 +229,41 @@ int spm_adjoint_direct_params(int n_atoms, const float* atoms, const float* cMs,
                               const float* dL_dFEs, const float* lambdas,
                               float* grad, void* scratch, void* stream);
 long long spm_adjoint_direct_scratch_bytes(int n_atoms, int n_scan);
+
+/* ------------------------------------------------------------------------
+ * Differentiable grid path (no counterpart in the reference, which
+ * differentiates only its grid-free direct path, kernels/AFM.cl:1711-2029).
+ * Forward: spm_grid_build + spm_relax_ex(SPM_RELAX_PP) -> FEs, PPs.
+ *
+ * spm_adjoint_grid_state: per state, at the stored equilibrium PPs, solves
+ * J^T lambda = b with J = dF_grid/dq + R^T (dg/dd) R (F_grid = trilinear
+ * interpolant of the grid forces, g = tip spring) and
+ * b = (dF_grid/dq)^T R^T u_xyz + grad(E_grid) u_w, u = dL_dFEs[state].
+ * Writes ubar = (R^T u_xyz - lambda, u_w), dk = the state's d(loss)/d(stiffness)
+ * terms, diag = (residual, lambda_min, cond, status) with status 0 ok,
+ * 1 not converged / residual >= 5e-4, 2 non-finite, 3 unstable, 4 singular or
+ * ill-conditioned, 5 touches a node rescaled by the |E|>100 cap (masked:
+ * ubar = dk = 0).  All (n_scan*nz,4) float32. */
+int spm_adjoint_grid_state(const float* grid, int nx, int ny, int nz,
+                           const float* points, int n_scan, const spm_scan_params* p,
+                           const float* PPs, const float* dL_dFEs,
+                           float* ubar, float* dk, float* diag, void* stream);
+
+/* spm_adjoint_grid_params: d(loss)/d(atom parameters) through the grid build
+ * (atomics-free: each state's 8 trilinear corner nodes are revisited per atom
+ * and the pair-law derivatives contracted with ubar; FP64 accumulation, fixed
+ * reduction order) and d(loss)/d(stiffness).  kind/atoms/params/p0/dA/dB/dC/
+ * Qs/QZs as spm_grid_build (HOST float[4] vectors); grid, nx, ny, nz, p as the
+ * forward.  grad out (n_atoms,6) double = (x, y, z, P1, P2, Q) with
+ * (P1,P2) = (c6,c12) for LJ, (R0,E0) for Morse; dk_sum out double[4] =
+ * d(loss)/d(stiffness.xyzw).  scratch >= spm_adjoint_grid_scratch_bytes. */
+int spm_adjoint_grid_params(int kind, int n_atoms, const float* atoms, const float* params,
+                            const float* p0, const float* dA, const float* dB, const float* dC,
+                            const float* Qs, const float* QZs, const float* grid, int nx, int ny, int nz,
+                            const spm_scan_params* p, const float* PPs, const float* ubar,
+                            const float* dk, long long n_state, double* grad, double* dk_sum,
+                            void* scratch, void* stream);
+long long spm_adjoint_grid_scratch_bytes(int n_atoms, long long n_state);
 
 /* ------------------------------------------------------------------------
  * Measurement helper (not part of the reference interface): runs a dependent

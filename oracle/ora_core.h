@@ -340,3 +340,48 @@ static void SFX(relax_direct_pixel)(int na, const REAL* atoms, const REAL* cMs, 
     }
     if (quirks & 2) { carry[0] = dt; carry[1] = damp; }
 }
+
+/* Grid relaxation with the direct path's bookkeeping (convergence tested
+ * before each update, PPs = (pos, +iters / -iters), FE re-sampled only when
+ * the position moved after the last sample): relaxStrokesTilted's tip frame,
+ * spring and surface bias (AFM.cl:478-562) with the control flow of
+ * relaxStrokesTiltedMorseDirect (AFM.cl:1441-1505).  Used by the
+ * differentiable grid path, whose implicit adjoint needs the equilibrium. */
+static void SFX(relax_pp_pixel)(const GRID_T* g, const SFX(gridref)* G, const float* pt, int nzs,
+                                const REAL* tA, const REAL* tB, const REAL* tC, const REAL* k,
+                                const REAL* d0, const REAL* relax, const REAL* surf, int max_iter,
+                                REAL f2conv, int use_fire, REAL* FEs, REAL* PPs) {
+    SFX(v3) a = SFX(mk3)(tA[0], tA[1], tA[2]);
+    SFX(v3) b = SFX(mk3)(tB[0], tB[1], tB[2]);
+    SFX(v3) c = SFX(mk3)(tC[0], tC[1], tC[2]);
+    SFX(v3) dTip = SFX(mk3)(c.x * tC[3], c.y * tC[3], c.z * tC[3]);
+    SFX(v3) d0r = SFX(rotmatT)(SFX(mk3)(d0[0], d0[1], d0[2]), a, b, c);
+    SFX(v3) tip = SFX(mk3)((REAL)pt[0], (REAL)pt[1], (REAL)pt[2]);
+    SFX(v3) pos = SFX(add3)(tip, d0r);
+    REAL dt = relax[0], damp = relax[1];
+    REAL dtmax = dt, dtmin = dtmax * (REAL)0.1, damp0 = damp;
+    for (int iz = 0; iz < nzs; iz++) {
+        SFX(v3) v = SFX(mk3)(0, 0, 0);
+        REAL fe[4] = {0, 0, 0, 0};
+        int itr = 0, conv = 0;
+        for (int i = 0; i < max_iter; i++) {
+            itr = i + 1;
+            SFX(interp_fe)(g, G->nx, G->ny, G->nz, G->dA, G->dB, G->dC, pos, fe);
+            SFX(v3) dl = SFX(rotmat)(SFX(sub3)(pos, tip), a, b, c);
+            SFX(v3) ft = SFX(rotmatT)(SFX(tip_force)(dl, k, d0), a, b, c);
+            SFX(v3) f = SFX(mk3)(fe[0] + ft.x, fe[1] + ft.y, fe[2] + ft.z);
+            f.x = FMA(c.x, surf[0], f.x); f.y = FMA(c.y, surf[0], f.y); f.z = FMA(c.z, surf[0], f.z);
+            if (SFX(dot3)(f, f) < f2conv) { conv = 1; break; }
+            SFX(md_step)(f, &v, &pos, &dt, &damp, dtmin, dtmax, damp0, use_fire);
+        }
+        if (!conv) SFX(interp_fe)(g, G->nx, G->ny, G->nz, G->dA, G->dB, G->dC, pos, fe);
+        SFX(v3) fr = SFX(rotmat)(SFX(mk3)(fe[0], fe[1], fe[2]), a, b, c);
+        FEs[iz * 4 + 0] = fr.x; FEs[iz * 4 + 1] = fr.y; FEs[iz * 4 + 2] = fr.z; FEs[iz * 4 + 3] = fe[3];
+        int finite = isfinite(fe[0]) && isfinite(fe[1]) && isfinite(fe[2]) && isfinite(fe[3]) &&
+                     isfinite(pos.x) && isfinite(pos.y) && isfinite(pos.z);
+        PPs[iz * 4 + 0] = pos.x; PPs[iz * 4 + 1] = pos.y; PPs[iz * 4 + 2] = pos.z;
+        PPs[iz * 4 + 3] = (REAL)((conv && finite) ? itr : -itr);
+        tip = SFX(add3)(tip, dTip);
+        pos = SFX(add3)(pos, dTip);
+    }
+}

@@ -58,6 +58,8 @@ def lib():
         "ora_set_num_threads": (None, [_i]),
         "ora_grid_build_d": (None, [_i, _i, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _ll, _ll, _vp]),
         "ora_grid_build_f": (None, [_i, _i, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _ll, _ll, _vp]),
+        "ora_grid_build_d64": (None, [_i, _i, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _ll, _ll,
+                                      _vp]),
         "ora_pair_fe_d": (None, [_i, _i, _vp, _vp, _i, _vp, _i, _vp, _vp, _vp]),
         "ora_relax_strokes_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _i, _f, _i,
                                        _i, _vp, _vp]),
@@ -71,6 +73,10 @@ def lib():
         "ora_raw_tilted_d": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
         "ora_relax_direct_d": (None, [_i, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
                                       _d, _i, _vp, _vp]),
+        "ora_relax_pp_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                  _i, _f, _i, _vp, _vp]),
+        "ora_relax_pp_d": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                  _i, _d, _i, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -101,7 +107,11 @@ def set_num_threads(n):
 
 # ---------------------------------------------------------------- stage (a)
 def grid_build(kind, atoms, params, n, p0, dA, dB, dC, Qs, QZs, prec="f64", node0=0, nnodes=None):
-    """Force grid (nz,ny,nx,4) (or a flattened node slice when nnodes is given)."""
+    """Force grid (nz,ny,nx,4) (or a flattened node slice when nnodes is given).
+
+    prec: 'f32' (FP32 arithmetic), 'f64' (FP64 arithmetic on float32 inputs, as
+    the reference kernel receives them) or 'f64in' (FP64 arithmetic and inputs)."""
+    atoms_in, params_in = atoms, params
     nx, ny, nz = (int(v) for v in n)
     atoms = np.ascontiguousarray(atoms, dtype=np.float32).reshape(-1, 4)
     pstride = 2 if kind == 0 else 4
@@ -110,10 +120,16 @@ def grid_build(kind, atoms, params, n, p0, dA, dB, dC, Qs, QZs, prec="f64", node
     full = nnodes is None
     if full:
         node0, nnodes = 0, total
-    dt = np.float64 if prec == "f64" else np.float32
+    dt = np.float64 if prec in ("f64", "f64in") else np.float32
     out = np.zeros((nnodes, 4), dtype=dt)
-    vs = [_v4(v) for v in (p0, dA, dB, dC, Qs, QZs)]
-    fn = lib().ora_grid_build_d if prec == "f64" else lib().ora_grid_build_f
+    if prec == "f64in":  # FP64 inputs as given (no float32 rounding of atoms / parameters)
+        atoms = np.ascontiguousarray(atoms_in, dtype=np.float64).reshape(-1, 4)
+        params = np.ascontiguousarray(params_in, dtype=np.float64).reshape(-1, pstride)
+        vs = [_v4(v, np.float64) for v in (p0, dA, dB, dC, Qs, QZs)]
+        fn = lib().ora_grid_build_d64
+    else:
+        vs = [_v4(v) for v in (p0, dA, dB, dC, Qs, QZs)]
+        fn = lib().ora_grid_build_d if prec == "f64" else lib().ora_grid_build_f
     fn(int(kind), atoms.shape[0], _p(atoms), _p(params), pstride, nx, ny, nz, *[_p(v) for v in vs], int(node0),
        int(nnodes), _p(out))
     return out.reshape(nz, ny, nx, 4) if full else out
@@ -168,6 +184,23 @@ def relax_tilted(grid, dinv, pts, nz, tipA, tipB, tipC, stiffness, dpos0, relax,
     fn(_p(g), *_grid_args(g), *[_p(v) for v in vs], _p(pts), n_scan, int(nz), *[_p(v) for v in ps], int(max_iter),
        float(f2conv), int(bool(use_fire)), _p(FEs))
     return FEs
+
+
+def relax_pp(grid, dinv, pts, nz, tipA, tipB, tipC, stiffness, dpos0, relax, surfFF, max_iter=128, f2conv=1e-8,
+             use_fire=True, prec="f32"):
+    """Grid relaxation with equilibrium bookkeeping -> FEs, PPs (n_scan,nz,4)."""
+    dt = np.float32 if prec == "f32" else np.float64
+    g = np.ascontiguousarray(grid, dtype=dt)
+    pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 4)
+    n_scan = pts.shape[0]
+    FEs = np.zeros((n_scan, nz, 4), dtype=dt)
+    PPs = np.zeros((n_scan, nz, 4), dtype=dt)
+    vs = [_v4(v, dt) for v in (dinv[0], dinv[1], dinv[2])]
+    ps = [_v4(v, dt) for v in (tipA, tipB, tipC, stiffness, dpos0, relax, surfFF)]
+    fn = lib().ora_relax_pp_f if prec == "f32" else lib().ora_relax_pp_d
+    fn(_p(g), *_grid_args(g), *[_p(v) for v in vs], _p(pts), n_scan, int(nz), *[_p(v) for v in ps], int(max_iter),
+       float(f2conv), int(bool(use_fire)), _p(FEs), _p(PPs))
+    return FEs, PPs
 
 
 def raw_tilted(grid, dinv, pts, nz, tipA, tipB, tipC, dTip, dpos0, prec="f32"):

@@ -130,6 +130,15 @@ void ora_grid_build_d(int kind, int na, const float* atoms, const float* prm, in
     GRID_BUILD_BODY(double, d_, double)
 }
 
+/* FP64 grid build from FP64 inputs (finite-difference checks perturb atoms by
+ * less than float32 resolves). */
+void ora_grid_build_d64(int kind, int na, const double* atoms, const double* prm, int pstride,
+                        int nx, int ny, int nz, const double* p0, const double* dA, const double* dB,
+                        const double* dC, const double* Qs, const double* QZs,
+                        long long node0, long long nnodes, double* out) {
+    GRID_BUILD_BODY(double, d_, double)
+}
+
 void ora_grid_build_f(int kind, int na, const float* atoms, const float* prm, int pstride,
                       int nx, int ny, int nz, const float* p0, const float* dA, const float* dB,
                       const float* dC, const float* Qs, const float* QZs,
@@ -255,4 +264,31 @@ void ora_relax_direct_d(int na, const double* atoms, const double* cMs, const fl
     for (int i = 0; i < nscan; i++)
         relax_direct_pixel_d(na, atoms, cMs, pts + 4 * (size_t)i, nzs, a, b, c, kk, dd, rr, ss, qs, qz,
                              max_iter, f2conv, FEs + (size_t)i * nzs * 4, PPs + (size_t)i * nzs * 4, quirks, NULL);
+}
+
+/* Grid relaxation with converged-position telemetry (see relax_pp_pixel). */
+void ora_relax_pp_f(const float* grid, int nx, int ny, int nz, const float* dinvA, const float* dinvB,
+                    const float* dinvC, const float* pts, int nscan, int nzs, const float* tA, const float* tB,
+                    const float* tC, const float* k, const float* d0, const float* relax, const float* surf,
+                    int max_iter, float f2conv, int use_fire, float* FEs, float* PPs) {
+    gridref_f G; G.nx = nx; G.ny = ny; G.nz = nz;
+    cvt4_f(dinvA, G.dA); cvt4_f(dinvB, G.dB); cvt4_f(dinvC, G.dC);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < nscan; i++)
+        relax_pp_pixel_f(grid, &G, pts + 4 * (size_t)i, nzs, tA, tB, tC, k, d0, relax, surf, max_iter, f2conv,
+                         use_fire, FEs + (size_t)i * nzs * 4, PPs + (size_t)i * nzs * 4);
+}
+
+/* FP64 variant: every parameter vector is double (used by finite-difference
+ * checks, whose perturbations are below float32 resolution). */
+void ora_relax_pp_d(const double* grid, int nx, int ny, int nz, const double* dinvA, const double* dinvB,
+                    const double* dinvC, const float* pts, int nscan, int nzs, const double* tA, const double* tB,
+                    const double* tC, const double* k, const double* d0, const double* relax, const double* surf,
+                    int max_iter, double f2conv, int use_fire, double* FEs, double* PPs) {
+    gridref_d G; G.nx = nx; G.ny = ny; G.nz = nz;
+    for (int c = 0; c < 4; c++) { G.dA[c] = dinvA[c]; G.dB[c] = dinvB[c]; G.dC[c] = dinvC[c]; }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < nscan; i++)
+        relax_pp_pixel_d(grid, &G, pts + 4 * (size_t)i, nzs, tA, tB, tC, k, d0, relax, surf, max_iter, f2conv, use_fire,
+                         FEs + (size_t)i * nzs * 4, PPs + (size_t)i * nzs * 4);
 }

@@ -27,6 +27,7 @@ SPM_F64 = 1
 SPM_FLAG_FIRE = 1
 SPM_RELAX_STROKES = 0
 SPM_RELAX_TILTED = 1
+SPM_RELAX_PP = 2
 SPM_FLAG_FLIP_Z = 2
 
 _f4 = ctypes.c_float * 4
@@ -105,6 +106,10 @@ _SIGNATURES = {
     "spm_adjoint_direct_params": (_i, [_i, _vp, _vp, _vp, _i, _P, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "spm_adjoint_direct_scratch_bytes": (_ll, [_i, _i]),
     "spm_fp32_peak_probe": (_i, [_i, ctypes.POINTER(ctypes.c_double), _vp]),
+    "spm_adjoint_grid_state": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "spm_adjoint_grid_params": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _P, _vp, _vp,
+                                     _vp, _ll, _vp, _vp, _vp, _vp]),
+    "spm_adjoint_grid_scratch_bytes": (_ll, [_i, _ll]),
 }
 
 

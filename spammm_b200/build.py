@@ -25,7 +25,7 @@ UNITS = {
     "relax.cu": ["-fmad=false"],
     "df.cu": ["-fmad=false"],
     "direct.cu": [],
-    "adjoint.cu": [],
+    "adjoint_grid.cu": [],
     "batched.cu": [],
 }
 

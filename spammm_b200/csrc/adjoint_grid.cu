@@ -1,0 +1,451 @@
+// adjoint_grid.cu -- implicit-function adjoint of the grid path: d(loss)/d(atom
+// positions, charges, LJ or Morse parameters, tip stiffness) through
+// (a) the force-grid build and (b) the relaxation on that grid.
+//
+// The reference differentiates only its grid-free direct path
+// (kernels/AFM.cl:1711-2029); this extends the same implicit-function
+// construction to the grid path.  At a converged state q* (forward:
+// SPM_RELAX_PP) the total force G(q) = F_grid(q) + R^T g(R(q - tip)) + c*surf
+// vanishes; F_grid is the trilinear interpolant of the grid's force channels.
+//   J  = dF_grid/dq + R^T (dg/dd) R          (F_grid is not a gradient field:
+//                                             J is not symmetric)
+//   b  = (dF_grid/dq)^T R^T u_xyz + grad(E_grid) u_w
+//   J^T lambda = b,   ubar = (R^T u_xyz - lambda, u_w)
+// and for any parameter theta of the grid values g(node) or of the spring,
+//   dL/dtheta = sum_states sum_corners w * ubar . dg(node)/dtheta  -  lambda . dG_tip/dtheta.
+//
+// Kernels:
+//   adjoint_grid_state_kernel  one thread per state: the 3x3 solve in registers,
+//                              status gates (non-converged / non-finite /
+//                              unstable / singular / touches a |E|>100-capped
+//                              node, where the cap makes g non-differentiable),
+//                              ubar and the per-state spring-gradient terms.
+//   adjoint_grid_atoms_kernel  CTA per (atom, chunk of 1024 states): each state's
+//                              eight trilinear corner nodes are revisited and the
+//                              pair-law derivatives evaluated there (a
+//                              state-major gather: no scatter onto the grid, no
+//                              atomics), FP64 accumulation, fixed-order CTA
+//                              tree, then a fixed-order fold over chunks.
+#include "spm_internal.cuh"
+#include "spm_fire.cuh"
+
+namespace spm {
+namespace {
+
+constexpr int AG_THREADS = 128;
+constexpr int AG_PER_THREAD = 8;
+constexpr int AG_CHUNK = AG_THREADS * AG_PER_THREAD;
+constexpr float R2SAFE = 1e-4f;
+constexpr float COULOMB_CONST = 14.3996448915f;
+
+struct Corners {
+    int x[2], y[2], z[2];
+    float ax, ay, az;
+    bool ok;
+};
+
+// Texel cell of a point (the same REPEAT/LINEAR addressing as interp_fe).
+__device__ __forceinline__ Corners corners_of(const GridView& G, V3 p) {
+    Corners C;
+    const float u = __fmaf_rn(p.x, G.dA.x, __fmaf_rn(p.y, G.dA.y, __fmaf_rn(p.z, G.dA.z, G.dA.w)));
+    const float v = __fmaf_rn(p.x, G.dB.x, __fmaf_rn(p.y, G.dB.y, __fmaf_rn(p.z, G.dB.z, G.dB.w)));
+    const float w = __fmaf_rn(p.x, G.dC.x, __fmaf_rn(p.y, G.dC.y, __fmaf_rn(p.z, G.dC.z, G.dC.w)));
+    C.ok = tex_axis(u, G.nx, C.x[0], C.x[1], C.ax);
+    C.ok = tex_axis(v, G.ny, C.y[0], C.y[1], C.ay) && C.ok;
+    C.ok = tex_axis(w, G.nz, C.z[0], C.z[1], C.az) && C.ok;
+    return C;
+}
+
+struct Sites {
+    float qs[4];  // Qs[k]*COULOMB_CONST
+    float qz[4];
+};
+
+__global__ void __launch_bounds__(AG_THREADS)
+adjoint_grid_state_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
+                          const float4* __restrict__ PPs, const float4* __restrict__ dL, float4* __restrict__ ubar,
+                          float4* __restrict__ dk, float4* __restrict__ diag) {
+    const long long st = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (st >= (long long)n_scan * P.nz) return;
+    const int iscan = (int)(st / P.nz), iz = (int)(st % P.nz);
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto fail = [&](float res, float lmin, float cond, float status) {
+        ubar[st] = zero;
+        dk[st] = zero;
+        diag[st] = make_float4(res, lmin, cond, status);
+    };
+    const float4 pp = PPs[st], u = dL[st];
+    if (!(isfinite(pp.x) && isfinite(pp.y) && isfinite(pp.z) && isfinite(pp.w) && isfinite(u.x) && isfinite(u.y) &&
+          isfinite(u.z) && isfinite(u.w))) { fail(0.f, 0.f, 0.f, 2.f); return; }
+    if (pp.w <= 0.f) { fail(0.f, 0.f, 0.f, 1.f); return; }
+    const V3 a = mk3(P.tipA[0], P.tipA[1], P.tipA[2]);
+    const V3 b = mk3(P.tipB[0], P.tipB[1], P.tipB[2]);
+    const V3 c = mk3(P.tipC[0], P.tipC[1], P.tipC[2]);
+    const float4 p4 = pts[iscan];
+    const V3 tip = mk3(p4.x + c.x * P.tipC[3] * (float)iz, p4.y + c.y * P.tipC[3] * (float)iz,
+                       p4.z + c.z * P.tipC[3] * (float)iz);
+    const V3 q = mk3(pp.x, pp.y, pp.z);
+    const Corners C = corners_of(G, q);
+    if (!C.ok) { fail(0.f, 0.f, 0.f, 2.f); return; }
+    // value and texel-coordinate derivatives of the 4 channels
+    float val[4] = {0, 0, 0, 0}, dx[4] = {0, 0, 0, 0}, dy[4] = {0, 0, 0, 0}, dz[4] = {0, 0, 0, 0};
+    bool capped = false;
+    for (int k = 0; k < 2; k++)
+        for (int j = 0; j < 2; j++)
+            for (int i = 0; i < 2; i++) {
+                const float4 f = __ldg(G.g + ((size_t)C.z[k] * G.ny + C.y[j]) * G.nx + C.x[i]);
+                capped |= fabsf(f.w) >= 99.9999f;
+                const float wx = i ? C.ax : 1.f - C.ax, wy = j ? C.ay : 1.f - C.ay, wz = k ? C.az : 1.f - C.az;
+                const float sx = i ? 1.f : -1.f, sy = j ? 1.f : -1.f, sz = k ? 1.f : -1.f;
+                const float fc[4] = {f.x, f.y, f.z, f.w};
+                for (int ch = 0; ch < 4; ch++) {
+                    val[ch] += wx * wy * wz * fc[ch];
+                    dx[ch] += sx * wy * wz * fc[ch];
+                    dy[ch] += wx * sy * wz * fc[ch];
+                    dz[ch] += wx * wy * sz * fc[ch];
+                }
+            }
+    // dt_axis/dq_m = n_axis * dinv_axis[m]
+    const float ta[3] = {G.nx * G.dA.x, G.nx * G.dA.y, G.nx * G.dA.z};
+    const float tb[3] = {G.ny * G.dB.x, G.ny * G.dB.y, G.ny * G.dB.z};
+    const float tc[3] = {G.nz * G.dC.x, G.nz * G.dC.y, G.nz * G.dC.z};
+    float Jg[3][3], gE[3];
+    for (int m = 0; m < 3; m++) {
+        for (int ch = 0; ch < 3; ch++) Jg[ch][m] = dx[ch] * ta[m] + dy[ch] * tb[m] + dz[ch] * tc[m];
+        gE[m] = dx[3] * ta[m] + dy[3] * tb[m] + dz[3] * tc[m];
+    }
+    // tip spring in the tip frame
+    const float4 kk = make_float4(P.stiffness[0], P.stiffness[1], P.stiffness[2], P.stiffness[3]);
+    const float4 d0 = make_float4(P.dpos0[0], P.dpos0[1], P.dpos0[2], P.dpos0[3]);
+    const V3 dl = rotmat(sub3(q, tip), a, b, c);
+    const V3 ft = rotmatT(tip_force(dl, kk, d0), a, b, c);
+    const float surf = P.surfFF[0];
+    const V3 Gv = mk3(val[0] + ft.x + c.x * surf, val[1] + ft.y + c.y * surf, val[2] + ft.z + c.z * surf);
+    const float resid = sqrtf(Gv.x * Gv.x + Gv.y * Gv.y + Gv.z * Gv.z);
+    if (resid >= 5e-4f) { fail(resid, 0.f, 0.f, 1.f); return; }
+    if (capped) { fail(resid, 0.f, 0.f, 5.f); return; }
+    float r = sqrtf(dl.x * dl.x + dl.y * dl.y + dl.z * dl.z);
+    r = fmaxf(r, 1e-10f);
+    const float phi = (kk.w == 0.f) ? 0.f : kk.w * (1.f - d0.w / r);
+    const float beta = (kk.w == 0.f) ? 0.f : kk.w * d0.w / (r * r * r);
+    const float Jt[3][3] = {{kk.x + phi + beta * dl.x * dl.x, beta * dl.x * dl.y, beta * dl.x * dl.z},
+                            {beta * dl.y * dl.x, kk.y + phi + beta * dl.y * dl.y, beta * dl.y * dl.z},
+                            {beta * dl.z * dl.x, beta * dl.z * dl.y, kk.z + phi + beta * dl.z * dl.z}};
+    const float R[3][3] = {{a.x, a.y, a.z}, {b.x, b.y, b.z}, {c.x, c.y, c.z}};
+    float J[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            float s = Jg[i][j];
+            for (int m = 0; m < 3; m++)
+                for (int n = 0; n < 3; n++) s += R[m][i] * Jt[m][n] * R[n][j];
+            J[i][j] = s;
+        }
+    // b = Jg^T R^T u_xyz + gE u_w
+    const V3 uw = rotmatT(mk3(u.x, u.y, u.z), a, b, c);
+    const float uv[3] = {uw.x, uw.y, uw.z};
+    float bv[3];
+    for (int m = 0; m < 3; m++) bv[m] = Jg[0][m] * uv[0] + Jg[1][m] * uv[1] + Jg[2][m] * uv[2] + gE[m] * u.w;
+    // J^T lambda = b via the adjugate: (J^T)^-1 = adj(J)^T / det(J)
+    float A[3][3];  // A = adj(J): A[i][j] = cofactor(J)[j][i]
+    A[0][0] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    A[0][1] = J[0][2] * J[2][1] - J[0][1] * J[2][2];
+    A[0][2] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+    A[1][0] = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    A[1][1] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+    A[1][2] = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+    A[2][0] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    A[2][1] = J[0][1] * J[2][0] - J[0][0] * J[2][1];
+    A[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    const float det = J[0][0] * A[0][0] + J[0][1] * A[1][0] + J[0][2] * A[2][0];
+    const float scale = fmaxf(fmaxf(fabsf(J[0][0]), fmaxf(fabsf(J[1][1]), fabsf(J[2][2]))), 1e-20f);
+    if (!(fabsf(det) >= 1e-18f * scale * scale * scale)) { fail(resid, 0.f, 0.f, 4.f); return; }
+    const float id = 1.f / det;
+    float lam[3];
+    for (int i = 0; i < 3; i++) lam[i] = (A[0][i] * bv[0] + A[1][i] * bv[1] + A[2][i] * bv[2]) * id;
+    if (!(isfinite(lam[0]) && isfinite(lam[1]) && isfinite(lam[2]))) { fail(resid, 0.f, 0.f, 2.f); return; }
+    // stability: smallest eigenvalue of the symmetric part of -J (closed form for 3x3)
+    const float s00 = -J[0][0], s11 = -J[1][1], s22 = -J[2][2];
+    const float s01 = -0.5f * (J[0][1] + J[1][0]), s02 = -0.5f * (J[0][2] + J[2][0]), s12 = -0.5f * (J[1][2] + J[2][1]);
+    float lmin;
+    {
+        const float p1 = s01 * s01 + s02 * s02 + s12 * s12;
+        const float qm = (s00 + s11 + s22) / 3.f;
+        const float p2 = (s00 - qm) * (s00 - qm) + (s11 - qm) * (s11 - qm) + (s22 - qm) * (s22 - qm) + 2.f * p1;
+        const float pp2 = sqrtf(p2 / 6.f);
+        if (pp2 < 1e-20f) {
+            lmin = qm;
+        } else {
+            const float b00 = (s00 - qm) / pp2, b11 = (s11 - qm) / pp2, b22 = (s22 - qm) / pp2;
+            const float b01 = s01 / pp2, b02 = s02 / pp2, b12 = s12 / pp2;
+            const float detB = b00 * (b11 * b22 - b12 * b12) - b01 * (b01 * b22 - b12 * b02) +
+                               b02 * (b01 * b12 - b11 * b02);
+            const float phi3 = acosf(fmaxf(-1.f, fminf(1.f, 0.5f * detB))) / 3.f;
+            const float e1 = qm + 2.f * pp2 * cosf(phi3);
+            const float e3 = qm + 2.f * pp2 * cosf(phi3 + 2.0943951023931953f);
+            lmin = fminf(e1, fminf(3.f * qm - e1 - e3, e3));
+        }
+    }
+    if (lmin <= 1e-5f) { fail(resid, lmin, 0.f, 3.f); return; }
+    float jinf = 0.f, ainf = 0.f;
+    for (int i = 0; i < 3; i++) {
+        jinf = fmaxf(jinf, fabsf(J[i][0]) + fabsf(J[i][1]) + fabsf(J[i][2]));
+        ainf = fmaxf(ainf, fabsf(A[i][0]) + fabsf(A[i][1]) + fabsf(A[i][2]));
+    }
+    const float cond = jinf * ainf / fabsf(det);
+    if (!(cond < 1e6f)) { fail(resid, lmin, cond, 4.f); return; }
+    ubar[st] = make_float4(uv[0] - lam[0], uv[1] - lam[1], uv[2] - lam[2], u.w);
+    // spring-parameter terms  -lambda . R^T dg/dk   (lambda in the tip frame: R lambda)
+    const V3 lt = rotmat(mk3(lam[0], lam[1], lam[2]), a, b, c);
+    const float rw = (r - d0.w) / r;
+    dk[st] = make_float4(-lt.x * (dl.x - d0.x), -lt.y * (dl.y - d0.y), -lt.z * (dl.z - d0.z),
+                         -(lt.x * dl.x + lt.y * dl.y + lt.z * dl.z) * rw);
+    diag[st] = make_float4(resid, lmin, cond, 0.f);
+}
+
+struct NodeGeom {
+    float4 p0, dA, dB, dC;
+};
+
+// Pair-law parameter derivatives at one grid node, contracted with the
+// node's adjoint weights (uF: force channels, uE: energy channel).
+template <int KIND>
+__device__ __forceinline__ void pair_grad(V3 node, float4 at, float p1, float p2, float p3, const Sites& S, V3 uF,
+                                          float uE, double* acc) {
+    const V3 dp = mk3(node.x - at.x, node.y - at.y, node.z - at.z);
+    const float r2 = dp.x * dp.x + dp.y * dp.y + dp.z * dp.z + R2SAFE;
+    const float du = dp.x * uF.x + dp.y * uF.y + dp.z * uF.z;
+    float s, dsdr2, E_dummy;
+    float g_p1, g_p2;
+    if (KIND == SPM_KIND_LJ) {
+        const float c6 = p1, c12 = p2;
+        const float ir2 = 1.f / r2;
+        const float ir6 = ir2 * ir2 * ir2;
+        const float ir8 = ir6 * ir2;
+        const float ir14 = ir8 * ir6;
+        s = 12.f * c12 * ir14 - 6.f * c6 * ir8;
+        dsdr2 = -84.f * c12 * ir14 * ir2 + 24.f * c6 * ir8 * ir2;
+        g_p1 = du * (-6.f * ir8) + uE * (-ir6);           // c6
+        g_p2 = du * (12.f * ir14) + uE * (ir6 * ir6);     // c12
+        E_dummy = 0.f;
+    } else {
+        const float R0 = p1, E0 = p2, K = p3;
+        const float r = sqrtf(r2);
+        const float e = expf(K * (r - R0));
+        const float Ep = 2.f * K * E0 * e * (e - 1.f);
+        const float Epp = 2.f * K * K * E0 * e * (2.f * e - 1.f);
+        s = -Ep / r;
+        dsdr2 = -(Epp / r - Ep / (r * r)) / (2.f * r);
+        g_p1 = du * (Epp / r) + uE * (-Ep);                                  // R0
+        g_p2 = du * (-2.f * K * e * (e - 1.f) / r) + uE * (e * (e - 2.f));    // E0
+        E_dummy = 0.f;
+    }
+    (void)E_dummy;
+    // d/da of (uF.F + uE E) = -(s uF + 2 s' (dp.uF) dp) + uE F,   F = s dp
+    float gx = -(s * uF.x + 2.f * dsdr2 * du * dp.x) + uE * s * dp.x;
+    float gy = -(s * uF.y + 2.f * dsdr2 * du * dp.y) + uE * s * dp.y;
+    float gz = -(s * uF.z + 2.f * dsdr2 * du * dp.z) + uE * s * dp.z;
+    float gq = 0.f;
+    for (int k = 0; k < 4; k++) {
+        if (S.qs[k] == 0.f) continue;
+        const V3 dk = mk3(dp.x, dp.y, dp.z + S.qz[k]);
+        const float rk2 = dk.x * dk.x + dk.y * dk.y + dk.z * dk.z + R2SAFE;
+        const float irk = rsqrtf(rk2);
+        const float irk3 = irk * irk * irk;
+        const float sk = S.qs[k] * at.w * irk3;
+        const float dsk = -1.5f * sk / rk2;
+        const float duk = dk.x * uF.x + dk.y * uF.y + dk.z * uF.z;
+        gx += -(sk * uF.x + 2.f * dsk * duk * dk.x) + uE * sk * dk.x;
+        gy += -(sk * uF.y + 2.f * dsk * duk * dk.y) + uE * sk * dk.y;
+        gz += -(sk * uF.z + 2.f * dsk * duk * dk.z) + uE * sk * dk.z;
+        gq += duk * (S.qs[k] * irk3) + uE * (S.qs[k] * irk);
+    }
+    acc[0] += gx;
+    acc[1] += gy;
+    acc[2] += gz;
+    acc[3] += g_p1;
+    acc[4] += g_p2;
+    acc[5] += gq;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(AG_THREADS)
+adjoint_grid_atoms_kernel(int na, const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
+                          Sites S, NodeGeom NG, GridView G, const float4* __restrict__ PPs,
+                          const float4* __restrict__ ubar, long long n_state, double* __restrict__ partial) {
+    __shared__ double red[6][AG_THREADS];
+    const int ia = blockIdx.y;
+    const float4 at = __ldg(atoms + ia);
+    const float* pr = params + (size_t)ia * pstride;
+    const float p1 = __ldg(pr + 0), p2 = __ldg(pr + 1), p3 = (pstride > 2) ? __ldg(pr + 2) : 0.f;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const long long s0 = (long long)blockIdx.x * AG_CHUNK;
+    for (int t = 0; t < AG_PER_THREAD; t++) {
+        const long long st = s0 + (long long)t * AG_THREADS + threadIdx.x;
+        if (st >= n_state) break;
+        const float4 ub = __ldg(ubar + st);
+        if (ub.x == 0.f && ub.y == 0.f && ub.z == 0.f && ub.w == 0.f) continue;
+        const float4 pp = __ldg(PPs + st);
+        const Corners C = corners_of(G, mk3(pp.x, pp.y, pp.z));
+        if (!C.ok) continue;
+        for (int k = 0; k < 2; k++)
+            for (int j = 0; j < 2; j++)
+                for (int i = 0; i < 2; i++) {
+                    const float w = (i ? C.ax : 1.f - C.ax) * (j ? C.ay : 1.f - C.ay) * (k ? C.az : 1.f - C.az);
+                    if (w == 0.f) continue;
+                    const int ix = C.x[i], iy = C.y[j], iz = C.z[k];
+                    const V3 node = mk3(NG.p0.x + NG.dA.x * ix + NG.dB.x * iy + NG.dC.x * iz,
+                                        NG.p0.y + NG.dA.y * ix + NG.dB.y * iy + NG.dC.y * iz,
+                                        NG.p0.z + NG.dA.z * ix + NG.dB.z * iy + NG.dC.z * iz);
+                    pair_grad<KIND>(node, at, p1, p2, p3, S, mk3(w * ub.x, w * ub.y, w * ub.z), w * ub.w, acc);
+                }
+    }
+#pragma unroll
+    for (int c6 = 0; c6 < 6; c6++) red[c6][threadIdx.x] = acc[c6];
+    __syncthreads();
+    for (int s = AG_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+#pragma unroll
+            for (int c6 = 0; c6 < 6; c6++) red[c6][threadIdx.x] += red[c6][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) partial[((size_t)ia * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// out[r*cols + c] = sum over chunks of in[(r*chunks + ch)*cols + c], fixed order.
+__global__ void __launch_bounds__(256)
+fold_chunks_kernel(const double* __restrict__ in, int chunks, int cols, double* __restrict__ out) {
+    __shared__ double red[256];
+    const int r = blockIdx.x, c = blockIdx.y;
+    double acc = 0.0;
+    for (int ch = threadIdx.x; ch < chunks; ch += 256) acc += in[((size_t)r * chunks + ch) * cols + c];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[(size_t)r * cols + c] = red[0];
+}
+
+// Per-chunk sums of float4 rows (spring-gradient terms) in FP64.
+__global__ void __launch_bounds__(256)
+sum_rows_kernel(const float4* __restrict__ rows, long long n, double* __restrict__ partial) {
+    __shared__ double red[4][256];
+    double acc[4] = {0, 0, 0, 0};
+    const long long base = (long long)blockIdx.x * 256 * 8;
+    for (int t = 0; t < 8; t++) {
+        const long long i = base + (long long)t * 256 + threadIdx.x;
+        if (i < n) {
+            const float4 v = __ldg(rows + i);
+            acc[0] += v.x; acc[1] += v.y; acc[2] += v.z; acc[3] += v.w;
+        }
+    }
+    for (int c = 0; c < 4; c++) red[c][threadIdx.x] = acc[c];
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int c = 0; c < 4; c++) red[c][threadIdx.x] += red[c][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) partial[(size_t)blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+GridView view_of(const float* grid, int nx, int ny, int nz, const spm_scan_params* p) {
+    GridView G;
+    G.g = reinterpret_cast<const float4*>(grid);
+    G.nx = nx; G.ny = ny; G.nz = nz;
+    G.dA = make_float4(p->dinvA[0], p->dinvA[1], p->dinvA[2], p->dinvA[3]);
+    G.dB = make_float4(p->dinvB[0], p->dinvB[1], p->dinvB[2], p->dinvB[3]);
+    G.dC = make_float4(p->dinvC[0], p->dinvC[1], p->dinvC[2], p->dinvC[3]);
+    return G;
+}
+
+long long n_chunks(long long n_state) { return n_state > 0 ? (n_state + AG_CHUNK - 1) / AG_CHUNK : 1; }
+long long n_rowblocks(long long n_state) { return n_state > 0 ? (n_state + 2047) / 2048 : 1; }
+
+}  // namespace
+}  // namespace spm
+
+extern "C" int spm_adjoint_grid_state(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
+                                      const spm_scan_params* p, const float* PPs, const float* dL_dFEs, float* ubar,
+                                      float* dk, float* diag, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(p && grid, "spm_adjoint_grid_state: null grid/params");
+    SPM_REQUIRE(nx > 0 && ny > 0 && nz > 0 && n_scan >= 0 && p->nz >= 0, "spm_adjoint_grid_state: bad sizes");
+    const long long n_state = (long long)n_scan * p->nz;
+    if (n_state == 0) return SPM_OK;
+    SPM_REQUIRE(points && PPs && dL_dFEs && ubar && dk && diag, "spm_adjoint_grid_state: null pointer");
+    SPM_REQUIRE(aligned16(grid) && aligned16(points) && aligned16(PPs) && aligned16(dL_dFEs) && aligned16(ubar) &&
+                aligned16(dk) && aligned16(diag), "spm_adjoint_grid_state: buffers not 16-byte aligned");
+    adjoint_grid_state_kernel<<<(unsigned)((n_state + AG_THREADS - 1) / AG_THREADS), AG_THREADS, 0,
+                                as_stream(stream)>>>(
+        view_of(grid, nx, ny, nz, p), reinterpret_cast<const float4*>(points), n_scan, *p,
+        reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(dL_dFEs),
+        reinterpret_cast<float4*>(ubar), reinterpret_cast<float4*>(dk), reinterpret_cast<float4*>(diag));
+    return check_launch("spm_adjoint_grid_state");
+}
+
+extern "C" long long spm_adjoint_grid_scratch_bytes(int n_atoms, long long n_state) {
+    using namespace spm;
+    if (n_atoms < 0 || n_state < 0) return 0;
+    return ((long long)n_atoms * n_chunks(n_state) * 6 + n_rowblocks(n_state) * 4) * (long long)sizeof(double);
+}
+
+extern "C" int spm_adjoint_grid_params(int kind, int n_atoms, const float* atoms, const float* params,
+                                       const float* p0, const float* dA, const float* dB, const float* dC,
+                                       const float* Qs, const float* QZs, const float* grid, int nx, int ny, int nz,
+                                       const spm_scan_params* p, const float* PPs, const float* ubar,
+                                       const float* dk, long long n_state, double* grad, double* dk_sum,
+                                       void* scratch, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(kind == SPM_KIND_LJ || kind == SPM_KIND_MORSE, "spm_adjoint_grid_params: kind=%d", kind);
+    SPM_REQUIRE(n_atoms >= 0 && n_atoms <= 65535, "spm_adjoint_grid_params: n_atoms=%d outside [0,65535]", n_atoms);
+    SPM_REQUIRE(p && p0 && dA && dB && dC && Qs && QZs && grid && grad && dk_sum && scratch,
+                "spm_adjoint_grid_params: null pointer");
+    SPM_REQUIRE(n_state >= 0 && nx > 0 && ny > 0 && nz > 0, "spm_adjoint_grid_params: bad sizes");
+    if (n_state > 0)
+        SPM_REQUIRE(PPs && ubar && dk && aligned16(PPs) && aligned16(ubar) && aligned16(dk),
+                    "spm_adjoint_grid_params: state buffers null or misaligned");
+    if (n_atoms > 0) SPM_REQUIRE(atoms && params && aligned16(atoms), "spm_adjoint_grid_params: null atoms/params");
+    SPM_REQUIRE((reinterpret_cast<uintptr_t>(scratch) & 7u) == 0, "spm_adjoint_grid_params: scratch not 8-byte aligned");
+    Sites S = {};
+    for (int k = 0; k < 4; k++) { S.qs[k] = Qs[k] * COULOMB_CONST; S.qz[k] = QZs[k]; }
+    NodeGeom NG;
+    NG.p0 = make_float4(p0[0], p0[1], p0[2], p0[3]);
+    NG.dA = make_float4(dA[0], dA[1], dA[2], dA[3]);
+    NG.dB = make_float4(dB[0], dB[1], dB[2], dB[3]);
+    NG.dC = make_float4(dC[0], dC[1], dC[2], dC[3]);
+    const long long chunks = n_chunks(n_state);
+    const long long rb = n_rowblocks(n_state);
+    SPM_REQUIRE(chunks < (1LL << 31), "spm_adjoint_grid_params: too many states");
+    double* part = static_cast<double*>(scratch);
+    double* dkpart = part + (size_t)n_atoms * chunks * 6;
+    cudaStream_t st = as_stream(stream);
+    const GridView G = view_of(grid, nx, ny, nz, p);
+    const int pstride = kind == SPM_KIND_MORSE ? 4 : 2;
+    if (n_atoms > 0) {
+        if (n_state > 0) {
+            dim3 grd((unsigned)chunks, (unsigned)n_atoms);
+            if (kind == SPM_KIND_LJ)
+                adjoint_grid_atoms_kernel<SPM_KIND_LJ><<<grd, AG_THREADS, 0, st>>>(
+                    n_atoms, reinterpret_cast<const float4*>(atoms), params, pstride, S, NG, G,
+                    reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar), n_state, part);
+            else
+                adjoint_grid_atoms_kernel<SPM_KIND_MORSE><<<grd, AG_THREADS, 0, st>>>(
+                    n_atoms, reinterpret_cast<const float4*>(atoms), params, pstride, S, NG, G,
+                    reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar), n_state, part);
+        } else if (cudaMemsetAsync(part, 0, (size_t)n_atoms * 6 * sizeof(double), st) != cudaSuccess) {
+            return set_error(SPM_ERR_CUDA, "spm_adjoint_grid_params: memset failed");
+        }
+        fold_chunks_kernel<<<dim3((unsigned)n_atoms, 6), 256, 0, st>>>(part, n_state > 0 ? (int)chunks : 1, 6, grad);
+    }
+    if (n_state > 0) {
+        sum_rows_kernel<<<(unsigned)rb, 256, 0, st>>>(reinterpret_cast<const float4*>(dk), n_state, dkpart);
+        fold_chunks_kernel<<<dim3(1, 4), 256, 0, st>>>(dkpart, (int)rb, 4, dk_sum);
+    } else if (cudaMemsetAsync(dk_sum, 0, 4 * sizeof(double), st) != cudaSuccess) {
+        return set_error(SPM_ERR_CUDA, "spm_adjoint_grid_params: memset failed");
+    }
+    return check_launch("spm_adjoint_grid_params");
+}

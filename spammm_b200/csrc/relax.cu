@@ -114,6 +114,46 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
     };
     if (k >= 0) start(k);
     while (k >= 0) {
+        if (MODE == 2) {
+            // equilibrium bookkeeping of the direct path: test before the update
+            bool done = true, conv = false;
+            if (it < max_iter) {
+                ++it;
+                ++total_it;
+                fe = interp_fe<IDX>(G, pos);
+                const V3 ft = rotmatT(tip_force(rotmat(sub3(pos, tip), a, b, c), kk, d0), a, b, c);
+                V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
+                f.x = __fmaf_rn(c.x, surf, f.x);
+                f.y = __fmaf_rn(c.y, surf, f.y);
+                f.z = __fmaf_rn(c.z, surf, f.z);
+                if (dot3(f, f) < P.f2conv) {
+                    conv = true;
+                } else {
+                    md_step(f, v, pos, I, fire);
+                    done = (it >= max_iter);
+                }
+            }
+            if (done) {
+                if (!conv) fe = interp_fe<IDX>(G, pos);  // the position moved after the last sample
+                const size_t o = (size_t)k * nzs + iz;
+                const V3 r = rotmat(mk3(fe.x, fe.y, fe.z), a, b, c);
+                FEs[o] = make_float4(r.x, r.y, r.z, fe.w);
+                const bool finite = isfinite(fe.x) && isfinite(fe.y) && isfinite(fe.z) && isfinite(fe.w) &&
+                                    isfinite(pos.x) && isfinite(pos.y) && isfinite(pos.z);
+                disps[o] = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
+                tip = add3(tip, dTip);
+                pos = add3(pos, dTip);
+                v = mk3(0.f, 0.f, 0.f);
+                fe = make_float4(0.f, 0.f, 0.f, 0.f);
+                it = 0;
+                if (++iz == nzs) {
+                    if (iter_count) iter_count[k] = total_it;
+                    k = counter ? next_pixel(counter, n_scan, P.raster_ny) : -1;
+                    if (k >= 0) start(k);
+                }
+            }
+            continue;
+        }
         bool done = max_iter <= 0;
         if (!done) {
             fe = interp_fe<IDX>(G, pos);
@@ -261,12 +301,13 @@ extern "C" int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz,
                             void* stream) {
     using namespace spm;
     clear_error();
-    SPM_REQUIRE(mode == SPM_RELAX_STROKES || mode == SPM_RELAX_TILTED, "spm_relax_ex: mode=%d", mode);
+    SPM_REQUIRE(mode == SPM_RELAX_STROKES || mode == SPM_RELAX_TILTED || mode == SPM_RELAX_PP,
+                "spm_relax_ex: mode=%d", mode);
     int rc = check_scan_args("spm_relax_ex", grid, nx, ny, nz, points, n_scan, p, FEs);
     if (rc) return rc;
     if (n_scan == 0 || p->nz == 0) return SPM_OK;
-    if (mode == SPM_RELAX_STROKES)
-        SPM_REQUIRE(disps != nullptr && aligned16(disps), "spm_relax_ex: disps null or misaligned");
+    if (mode != SPM_RELAX_TILTED)
+        SPM_REQUIRE(disps != nullptr && aligned16(disps), "spm_relax_ex: disps/PPs null or misaligned");
     SPM_REQUIRE(workspace == nullptr || (reinterpret_cast<uintptr_t>(workspace) & 3u) == 0,
                 "spm_relax_ex: workspace not 4-byte aligned");
     spm_scan_params P = normalized(p, n_scan);
@@ -277,6 +318,9 @@ extern "C" int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz,
     cudaStream_t st = as_stream(stream);
     if (mode == SPM_RELAX_STROKES)
         return launch_mode<0>(G, nodes, pt, n_scan, P, reinterpret_cast<float4*>(FEs),
+                              reinterpret_cast<float4*>(disps), iter_count, ctr, st);
+    if (mode == SPM_RELAX_PP)
+        return launch_mode<2>(G, nodes, pt, n_scan, P, reinterpret_cast<float4*>(FEs),
                               reinterpret_cast<float4*>(disps), iter_count, ctr, st);
     return launch_mode<1>(G, nodes, pt, n_scan, P, reinterpret_cast<float4*>(FEs), nullptr, iter_count, ctr, st);
 }

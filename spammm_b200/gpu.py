@@ -107,6 +107,62 @@ def relax_strokes_tilted(grid, params, points, FEs=None, dynamic=True):
     return FEs
 
 
+def relax_pp(grid, params, points, FEs=None, PPs=None, iter_count=None, dynamic=True):
+    """Grid relaxation with equilibrium bookkeeping (SPM_RELAX_PP) -> FEs, PPs (n_scan,nz,4).
+
+    FEs: tip-frame sample FE at the stored position; PPs = (pos, +iters / -iters)."""
+    nx, ny, nz = _grid_dims(grid)
+    points = _as_dev(points, F32, (4,), "points")
+    n_scan = points.shape[0]
+    shape = (n_scan, params.nz, 4)
+    FEs = torch.empty(shape, dtype=F32, device=points.device) if FEs is None else FEs
+    PPs = torch.empty(shape, dtype=F32, device=points.device) if PPs is None else PPs
+    ws = _workspace(points.device) if dynamic else None
+    rc = lib().spm_relax_ex(_lib.SPM_RELAX_PP, ptr(grid), nx, ny, nz, ptr(points), n_scan, ctypes.byref(params),
+                            ptr(FEs), ptr(PPs), ptr(iter_count), ptr(ws), stream_ptr())
+    check(rc, "spm_relax_ex(PP)")
+    return FEs, PPs
+
+
+def adjoint_grid_state(grid, params, points, PPs, dL_dFEs):
+    """Per-state implicit adjoint on the grid -> ubar, dk, diag (n_state,4)."""
+    nx, ny, nz = _grid_dims(grid)
+    points = _as_dev(points, F32, (4,), "points")
+    PPs = _as_dev(PPs, F32, (4,), "PPs").reshape(-1, 4)
+    dL = _as_dev(dL_dFEs, F32, (4,), "dL_dFEs").reshape(-1, 4)
+    n_scan = points.shape[0]
+    if PPs.shape[0] != n_scan * params.nz or dL.shape[0] != PPs.shape[0]:
+        raise ValueError("PPs/dL_dFEs must hold n_scan*nz states")
+    ubar, dk, diag = torch.empty_like(PPs), torch.empty_like(PPs), torch.empty_like(PPs)
+    rc = lib().spm_adjoint_grid_state(ptr(grid), nx, ny, nz, ptr(points), n_scan, ctypes.byref(params), ptr(PPs),
+                                      ptr(dL), ptr(ubar), ptr(dk), ptr(diag), stream_ptr())
+    check(rc, "spm_adjoint_grid_state")
+    return ubar, dk, diag
+
+
+def adjoint_grid_params(kind, atoms, params_atoms, p0, dA, dB, dC, Qs, QZs, grid, scan_params, PPs, ubar, dk):
+    """Atom and spring gradients of the grid path -> grad (na,6) f64 (x,y,z,P1,P2,Q), dk (4,) f64."""
+    nx, ny, nz = _grid_dims(grid)
+    atoms = _as_dev(atoms, F32, (4,), "atoms")
+    pcols = 2 if kind == _lib.SPM_KIND_LJ else 4
+    prm = _as_dev(params_atoms, F32, (pcols,), "params")
+    PPs = _as_dev(PPs, F32, (4,), "PPs").reshape(-1, 4)
+    ubar = _as_dev(ubar, F32, (4,), "ubar").reshape(-1, 4)
+    dk = _as_dev(dk, F32, (4,), "dk").reshape(-1, 4)
+    na, n_state = int(atoms.shape[0]), int(PPs.shape[0])
+    grad = torch.empty((na, 6), dtype=F64, device=atoms.device)
+    dk_sum = torch.empty((4,), dtype=F64, device=atoms.device)
+    nbytes = int(lib().spm_adjoint_grid_scratch_bytes(na, n_state))
+    scratch = torch.empty((max(nbytes, 8) + 7) // 8, dtype=F64, device=atoms.device)
+    hv = [hostvec(v) for v in (p0, dA, dB, dC, Qs, QZs)]
+    rc = lib().spm_adjoint_grid_params(int(kind), na, ptr(atoms) if na else None, ptr(prm) if na else None,
+                                       *[hptr(h) for h in hv], ptr(grid), nx, ny, nz, ctypes.byref(scan_params),
+                                       ptr(PPs), ptr(ubar), ptr(dk), n_state, ptr(grad), ptr(dk_sum), ptr(scratch),
+                                       stream_ptr())
+    check(rc, "spm_adjoint_grid_params")
+    return grad, dk_sum
+
+
 def fe_in_strokes_tilted(grid, params, points, FEs=None):
     nx, ny, nz = _grid_dims(grid)
     points = _as_dev(points, F32, (4,), "points")
