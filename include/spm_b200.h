@@ -266,6 +266,136 @@ int spm_adjoint_grid_params(int kind, int n_atoms, const float* atoms, const flo
 long long spm_adjoint_grid_scratch_bytes(int n_atoms, long long n_state);
 
 /* ------------------------------------------------------------------------
+ * Batched grid path: many molecules of uneven atom count, grid size and scan
+ * window, each stage ONE launch over the whole batch (no counterpart in the
+ * reference, whose AFMulator (spammm/SPM/AFM.py) handles one molecule per
+ * call).  Per molecule the results equal the per-molecule calls
+ * spm_grid_build -> spm_relax_ex(SPM_RELAX_PP) -> spm_adjoint_grid_state on
+ * the same inputs: forward values bit for bit, gradients up to the order of
+ * the FP64 sums.  Scans are z-strokes: one probe frame and spring shared by
+ * the batch (spm_scan_params), per-molecule grids, rasters and z-step counts.
+ *
+ * SLABS.  A molecule stores only layers [z_lo, z_lo + nz_slab) of its full
+ * (nx,ny,nz) grid.  They are built and sampled in the full grid's coordinates,
+ * so stored values and samples are bit-identical to the full grid's; a probe
+ * that needs a layer outside the slab stops at once and its state reports
+ * "not converged" (FEs NaN, PPs.w = -iterations).
+ *
+ * DESCRIPTORS.  One spm_batch_mol per molecule, in the order work is handed
+ * out; every *_off field is non-decreasing in that order (kernels locate a
+ * work item's molecule by binary search).  The caller fills the geometry
+ * fields and the buffer offsets: atom_off, pix_off and state_off contiguous
+ * from 0 (each molecule's rows right after the previous molecule's), grid_off
+ * increasing with non-overlapping slabs;
+ * spm_batch_prepare fills tile_off, slot_off, unit_off and chunk_off for a
+ * given spm_batch_shape, which every launch on these descriptors must then
+ * be given unchanged.  The descriptor array is copied to device memory by the
+ * caller; launches take the DEVICE copy.  Layouts:
+ *   atoms  (total_atoms,4) x,y,z,Q;  params (total_atoms,2) LJ c6,c12 or
+ *          (total_atoms,4) Morse R0,E0,K,-
+ *   grid   float4 slabs, (nz_slab,ny,nx) each, at grid_off
+ *   points (total_pixels,4) tip start positions (raster ix-major when
+ *          raster_ny > 0, as spm_relax_ex)
+ *   states (total_states,4) per molecule n_scan x nz_steps, z-step fastest */
+typedef struct spm_batch_mol {
+    long long grid_off;   /* float4 index of the slab */
+    long long state_off;  /* first state */
+    long long tile_off;   /* first grid-build tile              (spm_batch_prepare) */
+    long long slot_off;   /* first relaxation slot              (spm_batch_prepare) */
+    long long unit_off;   /* first adjoint node-chunk unit      (spm_batch_prepare) */
+    long long chunk_off;  /* first 256-state loss chunk         (spm_batch_prepare) */
+    long long row_off;    /* first (unit, atom) adjoint partial (spm_batch_prepare) */
+    int atom_off, n_atoms;
+    int pix_off, n_scan;
+    int nx, ny, nz;       /* full grid */
+    int z_lo, nz_slab;    /* stored layers */
+    int nz_steps;         /* z-steps of every stroke */
+    int raster_ny;        /* > 0: points form an (n_scan/raster_ny) x raster_ny raster */
+    int reserved;
+    float p0[4], dA[4], dB[4], dC[4];   /* node geometry (dA,dB,dC as spm_grid_build) */
+    float dinvA[4], dinvB[4], dinvC[4]; /* sampling transform (as spm_scan_params) */
+} spm_batch_mol;
+
+/* Launch shapes; spm_batch_default_shape() gives a valid default, the
+ * autotuner in the Python package searches the rest. */
+typedef struct spm_batch_shape {
+    int gb_ty;          /* grid build: CTA = 32 x gb_ty threads, gb_ty in {2,4,8} */
+    int gb_zb;          /* grid build: nodes along z per thread, 8 or 16 */
+    int rx_threads;     /* relaxation CTA size: 64, 128 or 256 */
+    int rx_tile_h;      /* relaxation pixel tile: (32/rx_tile_h) x rx_tile_h pixels, power of two <= 32 */
+    int rx_ctas_per_sm; /* persistent relaxation CTAs per SM, 0 = occupancy maximum */
+    int adj_chunk;      /* slab nodes per adjoint unit: multiple of 1024 in [1024, 1048576] */
+} spm_batch_shape;
+
+spm_batch_shape spm_batch_default_shape(void);
+
+/* Validates the descriptors (HOST array) and fills tile_off, slot_off,
+ * unit_off, chunk_off and row_off for `shape`.  totals_out (HOST
+ * long long[SPM_BATCH_TOTALS]) = (tiles, slots, units, chunks, states, atoms,
+ * pixels, grid float4s, rows). */
+#define SPM_BATCH_TOTALS 9
+int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch_shape* shape, long long* totals_out);
+
+/* Force-grid slabs of every molecule (pair laws, tip sites and the |E|>100
+ * cap as spm_grid_build).  n_tiles = totals_out[0]. */
+int spm_batch_grid_build(int kind, int n_mol, const spm_batch_mol* mols, long long n_tiles,
+                         const spm_batch_shape* shape, const float* atoms, const float* params,
+                         const float* Qs, const float* QZs, float* grid, void* stream);
+
+/* SPM_RELAX_PP relaxation of every stroke of every molecule in one persistent
+ * launch: lanes draw (molecule, pixel) slots from a device counter in
+ * `workspace` (>= spm_relax_workspace_bytes() bytes, reset by the call).
+ * p: probe frame, spring, FIRE settings, flags, tipC[3] = z-step; its dinv*,
+ * nz and raster_ny are ignored (per-molecule values come from mols).
+ * FEs, PPs out (total_states,4); iter_count (total_pixels) or NULL. */
+int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n_slots, const spm_batch_shape* shape,
+                    const float* grid, const float* points, const spm_scan_params* p,
+                    float* FEs, float* PPs, int* iter_count, void* workspace, void* stream);
+
+/* Frequency shift of every stroke, as spm_df_amp_dir with n = z and
+ * dr = |dtip| on the stroke taken in ascending z (the stroke reversed), the
+ * result written back in stroke order: df out (total_states) float32.
+ * Strokes with nz_steps < 2 or > 512 get NaN. */
+int spm_batch_df_amp(int n_mol, const spm_batch_mol* mols, long long n_pixels, const float* FEs,
+                     double dtip, double amp, float* df, void* stream);
+
+/* df loss of every molecule, as spm_df_loss_seed on its (n_scan,1,nz_steps)
+ * volume: target, weights (total_states) float64 (weights NULL = 1 inside,
+ * 0 on each stroke's first and last z-step); df_out (total_states) f64;
+ * dL_dFEs (total_states,4) f32; loss_out (n_mol) f64 in descriptor order.
+ * A molecule with nz_steps < 3 gets loss NaN and dL_dFEs = 0.
+ * scratch >= spm_batch_loss_scratch_bytes(n_chunks, n_mol). */
+int spm_batch_df_loss_seed(int n_mol, const spm_batch_mol* mols, long long n_chunks, const float* FEs,
+                           const double* target, const double* weights, double dtip, double* df_out,
+                           float* dL_dFEs, double* loss_out, void* scratch, void* stream);
+long long spm_batch_loss_scratch_bytes(long long n_chunks, int n_mol);
+
+/* spm_adjoint_grid_state over the batch (same outputs per state). */
+int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_states, const float* grid,
+                            const float* points, const spm_scan_params* p, const float* PPs,
+                            const float* dL_dFEs, float* ubar, float* dk, float* diag, void* stream);
+
+/* spm_adjoint_grid_params over the batch, node-major: grad (total_atoms,6)
+ * double as spm_adjoint_grid_params, dk_sum double[4] summed over the whole
+ * batch (one probe).
+ *   1. the states' w*ubar are scattered onto an adjoint grid over each slab
+ *      (the transpose of the trilinear sample) in 64-bit fixed point with a
+ *      per-molecule power-of-two scale (2^42 / max|ubar|), so the integer
+ *      sums are exact and order-independent: bit-reproducible;
+ *   2. an atomics-free scatter by atom tiles: each CTA stages a chunk of
+ *      non-zero adjoint-grid nodes in shared memory and every thread owns one
+ *      atom (and a phase of the chunk), evaluating the pair-law derivatives of
+ *      its atom at each staged node; per-(chunk, atom) FP64 partials are folded
+ *      per atom in a fixed order.
+ * totals: the HOST array of spm_batch_prepare; scratch (device) >=
+ * spm_batch_adjoint_scratch_bytes(totals, n_mol). */
+int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol* mols, const long long* totals,
+                             const spm_batch_shape* shape, const float* atoms, const float* params,
+                             const float* Qs, const float* QZs, const float* PPs, const float* ubar,
+                             const float* dk, double* grad, double* dk_sum, void* scratch, void* stream);
+long long spm_batch_adjoint_scratch_bytes(const long long* totals, int n_mol);
+
+/* ------------------------------------------------------------------------
  * Measurement helper (not part of the reference interface): runs a dependent
  * FFMA chain on every SM and writes the achieved FP32 FLOP/s to *out_flops
  * (host double).  Blocking. */

@@ -77,6 +77,37 @@ def make_scan_params(*, dinv=None, tipA=None, tipB=None, tipC=None, dTip=None, s
     return p
 
 
+class BatchMol(ctypes.Structure):
+    """Mirror of ``spm_batch_mol`` (one molecule of a batch)."""
+    _fields_ = [
+        ("grid_off", ctypes.c_longlong), ("state_off", ctypes.c_longlong),
+        ("tile_off", ctypes.c_longlong), ("slot_off", ctypes.c_longlong),
+        ("unit_off", ctypes.c_longlong), ("chunk_off", ctypes.c_longlong),
+        ("row_off", ctypes.c_longlong),
+        ("atom_off", ctypes.c_int), ("n_atoms", ctypes.c_int),
+        ("pix_off", ctypes.c_int), ("n_scan", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("z_lo", ctypes.c_int), ("nz_slab", ctypes.c_int),
+        ("nz_steps", ctypes.c_int), ("raster_ny", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("p0", _f4), ("dA", _f4), ("dB", _f4), ("dC", _f4),
+        ("dinvA", _f4), ("dinvB", _f4), ("dinvC", _f4),
+    ]
+
+
+class BatchShape(ctypes.Structure):
+    """Mirror of ``spm_batch_shape`` (launch shapes of the batched kernels)."""
+    _fields_ = [
+        ("gb_ty", ctypes.c_int), ("gb_zb", ctypes.c_int), ("rx_threads", ctypes.c_int),
+        ("rx_tile_h", ctypes.c_int), ("rx_ctas_per_sm", ctypes.c_int), ("adj_chunk", ctypes.c_int),
+    ]
+
+    def key(self):
+        return tuple(getattr(self, f) for f, _ in self._fields_)
+
+    def __repr__(self):
+        return "BatchShape(" + ", ".join(f"{f}={getattr(self, f)}" for f, _ in self._fields_) + ")"
+
+
 _lib = None
 _load_error = None
 
@@ -85,6 +116,9 @@ _i = ctypes.c_int
 _d = ctypes.c_double
 _ll = ctypes.c_longlong
 _P = ctypes.POINTER(ScanParams)
+_BS = ctypes.POINTER(BatchShape)
+_LLP = ctypes.POINTER(ctypes.c_longlong)
+SPM_BATCH_TOTALS = 9
 
 _SIGNATURES = {
     "spm_abi_version": (_i, []),
@@ -110,6 +144,17 @@ _SIGNATURES = {
     "spm_adjoint_grid_params": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _P, _vp, _vp,
                                      _vp, _ll, _vp, _vp, _vp, _vp]),
     "spm_adjoint_grid_scratch_bytes": (_ll, [_i, _ll]),
+    "spm_batch_default_shape": (BatchShape, []),
+    "spm_batch_prepare": (_i, [ctypes.POINTER(BatchMol), _i, _BS, _LLP]),
+    "spm_batch_grid_build": (_i, [_i, _i, _vp, _ll, _BS, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "spm_batch_relax": (_i, [_i, _vp, _ll, _BS, _vp, _vp, _P, _vp, _vp, _vp, _vp, _vp]),
+    "spm_batch_df_amp": (_i, [_i, _vp, _ll, _vp, _d, _d, _vp, _vp]),
+    "spm_batch_df_loss_seed": (_i, [_i, _vp, _ll, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _vp]),
+    "spm_batch_loss_scratch_bytes": (_ll, [_ll, _i]),
+    "spm_batch_adjoint_state": (_i, [_i, _vp, _ll, _vp, _vp, _P, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "spm_batch_adjoint_params": (_i, [_i, _i, _vp, _LLP, _BS, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                      _vp]),
+    "spm_batch_adjoint_scratch_bytes": (_ll, [_LLP, _i]),
 }
 
 

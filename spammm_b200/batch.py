@@ -1,0 +1,445 @@
+"""Batched probe-particle AFM: many molecules per launch, replayed as a CUDA graph.
+
+The reference's AFMulator (spammm/SPM/AFM.py) images one molecule per call:
+make_forcefield -> run_scan -> df.  ``AFMBatch`` runs the same grid path for a
+whole batch of molecules with uneven atom counts, grid sizes and scan windows,
+each stage ONE launch over the batch (the spm_batch_* entry points of
+include/spm_b200.h):
+
+  spm_batch_grid_build     force-grid slabs of every molecule
+  spm_batch_relax          persistent SPM_RELAX_PP relaxation; lanes draw
+                           (molecule, pixel) slots from one device counter
+  spm_batch_df_amp         amplitude-averaged df of every stroke
+  spm_batch_df_loss_seed   per-molecule df loss and dL/dFEs
+  spm_batch_adjoint_state  implicit-function adjoint of every state
+  spm_batch_adjoint_params gather through the grid build: d(loss)/d(atoms)
+
+Per molecule the results are those of the per-molecule calls (grid_build ->
+relax_pp -> adjoint on the same GridScanSpec): forward values bit for bit.
+Only the z-layers the probe can reach (the tip's z-range plus ``slab_margin``
+on both sides) are built and stored; a probe that leaves them is reported as
+not converged instead of sampling the missing layers.
+
+Molecules are laid out in descending order of relaxation work (longest
+first), so the persistent relaxation ends with small molecules filling in.
+All accessors take and return molecules in the caller's order.
+"""
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import BatchMol, BatchShape, check, f4, hostvec, hptr, lib, ptr, stream_ptr
+from .diff import GridScanSpec
+
+F32 = torch.float32
+F64 = torch.float64
+
+
+@dataclass
+class BatchItem:
+    """One molecule: atoms, force-grid geometry and scan raster."""
+    atoms: np.ndarray     # (na,4) x,y,z,Q
+    params: np.ndarray    # (na,2) LJ c6,c12 or (na,4) Morse R0,E0,K,-
+    origin: np.ndarray    # (3,) grid origin [A]
+    step: float           # node spacing [A]
+    ngrid: tuple          # (nx,ny,nz)
+    xs: np.ndarray        # raster x coordinates
+    ys: np.ndarray        # raster y coordinates
+    z_top: float          # first tip z
+    nz: int               # z-steps per stroke
+
+    @property
+    def n_scan(self):
+        return len(self.xs) * len(self.ys)
+
+    def points(self):
+        """(n_scan,4) tip start points, ix-major raster."""
+        X, Y = np.meshgrid(np.asarray(self.xs, np.float32), np.asarray(self.ys, np.float32), indexing="ij")
+        pts = np.zeros((X.size, 4), np.float32)
+        pts[:, 0] = X.ravel()
+        pts[:, 1] = Y.ravel()
+        pts[:, 2] = np.float32(self.z_top)
+        return pts
+
+    def spec(self, kind, probe, dtip):
+        """The per-molecule GridScanSpec of this item (the unbatched path)."""
+        return GridScanSpec(kind=kind, ngrid=tuple(int(v) for v in self.ngrid), origin=np.asarray(self.origin),
+                            step=float(self.step), points=self.points(), nz=int(self.nz), dtip=float(dtip),
+                            tipQs=hostvec(probe.tipQs), tipQZs=hostvec(probe.tipQZs), dpos0=hostvec(probe.dpos0),
+                            relax_params=hostvec(probe.relax_params), max_iter=int(probe.max_iter),
+                            f2conv=float(probe.f2conv), raster_ny=len(self.ys), strict=False)
+
+
+def _default_stiffness():
+    from .AFM import stiffness_Nm_to_eVA2
+    kxy, kz = stiffness_Nm_to_eVA2(0.25), stiffness_Nm_to_eVA2(20.0)
+    return np.array([-kxy, -kxy, -kz, 0.0], np.float32)
+
+
+@dataclass
+class ProbeSpec:
+    """Probe shared by a batch: spring (eV/A^2, negative = restoring), tip
+    charges, FIRE settings."""
+    stiffness: np.ndarray = field(default_factory=_default_stiffness)
+    dpos0: np.ndarray = field(default_factory=lambda: np.zeros(4, np.float32))
+    tipQs: np.ndarray = field(default_factory=lambda: np.array([-0.05, 0, 0, 0], np.float32))
+    tipQZs: np.ndarray = field(default_factory=lambda: np.zeros(4, np.float32))
+    relax_params: np.ndarray = field(default_factory=lambda: np.array([0.5, 0.1, 0.02, 0.5], np.float32))
+    max_iter: int = 1000
+    f2conv: float = 1e-10
+
+
+def slab_range(item, probe, dtip, margin):
+    """Stored layers [z_lo, z_lo + nz_slab) of the item's grid: every layer a
+    trilinear sample can touch while the probe stays within `margin` A of the
+    tip's z-range (+ dpos0.z).  The full grid when that range reaches an edge
+    (the periodic wrap then needs both ends)."""
+    nzg = int(item.ngrid[2])
+    z_first = float(item.z_top) + float(probe.dpos0[2])
+    z_last = z_first + (int(item.nz) - 1) * float(dtip)
+    lo_z, hi_z = min(z_first, z_last) - margin, max(z_first, z_last) + margin
+    oz, h = float(item.origin[2]), float(item.step)
+    t_lo, t_hi = (lo_z - oz) / h, (hi_z - oz) / h
+    z_lo = int(math.floor(t_lo))
+    z_hi = int(math.floor(t_hi)) + 2
+    if z_lo < 0 or z_hi > nzg:
+        return 0, nzg
+    return z_lo, z_hi - z_lo
+
+
+class BatchPlan:
+    """Host side of a batch: descriptors in work order and the concatenated
+    atom / parameter / point arrays (no device memory; see AFMBatch)."""
+
+    def __init__(self, items, kind=0, probe=None, dtip=-0.1, slab_margin=1.5, order="lpt"):
+        if not items:
+            raise ValueError("a batch needs at least one molecule")
+        if dtip >= 0:
+            raise ValueError(f"dtip must be < 0 (approach), got {dtip}")
+        self.kind = int(kind)
+        self.probe = probe or ProbeSpec()
+        self.dtip = float(dtip)
+        self.items = list(items)
+        n = len(items)
+        self.n = n
+        cost = np.array([it.n_scan * it.nz for it in items], np.int64)
+        self.order = np.argsort(-cost, kind="stable") if order == "lpt" else np.arange(n)
+        self.pos = np.empty(n, np.int64)
+        self.pos[self.order] = np.arange(n)
+        pcols = 2 if self.kind == _lib.SPM_KIND_LJ else 4
+        self.mols = (BatchMol * n)()
+        atoms_l, params_l, pts_l = [], [], []
+        ao = po = so = go = 0
+        for j, i in enumerate(self.order):
+            it = items[i]
+            a = np.asarray(it.atoms, np.float32).reshape(-1, 4)
+            p = np.asarray(it.params, np.float32).reshape(len(a), -1)
+            if p.shape[1] != pcols:
+                raise ValueError(f"molecule {i}: params need {pcols} columns for kind {kind}")
+            spec = it.spec(self.kind, self.probe, self.dtip)
+            p0, dA, dB, dC = spec.vectors()
+            dinv = spec.dinv()
+            nx, ny, nzg = (int(v) for v in it.ngrid)
+            z_lo, nzs = slab_range(it, self.probe, self.dtip, slab_margin)
+            D = self.mols[j]
+            D.grid_off, D.state_off = go, so
+            D.atom_off, D.n_atoms = ao, len(a)
+            D.pix_off, D.n_scan = po, it.n_scan
+            D.nx, D.ny, D.nz = nx, ny, nzg
+            D.z_lo, D.nz_slab = z_lo, nzs
+            D.nz_steps, D.raster_ny = int(it.nz), len(it.ys)
+            D.p0, D.dA, D.dB, D.dC = f4(p0), f4(dA), f4(dB), f4(dC)
+            D.dinvA, D.dinvB, D.dinvC = f4(dinv[0]), f4(dinv[1]), f4(dinv[2])
+            atoms_l.append(a)
+            params_l.append(p)
+            pts_l.append(it.points())
+            ao += len(a)
+            po += it.n_scan
+            so += it.n_scan * int(it.nz)
+            go += nx * ny * nzs
+        self.atoms = np.ascontiguousarray(np.concatenate(atoms_l))
+        self.params = np.ascontiguousarray(np.concatenate(params_l))
+        self.points = np.ascontiguousarray(np.concatenate(pts_l))
+        self.total_atoms, self.total_pixels, self.total_states, self.grid_float4 = ao, po, so, go
+        self.shape = None
+
+    def prepare(self, shape):
+        """spm_batch_prepare for `shape`: fills the work prefixes; returns the totals."""
+        shape = BatchShape(*shape.key())
+        totals = (ctypes.c_longlong * _lib.SPM_BATCH_TOTALS)()
+        check(lib().spm_batch_prepare(self.mols, self.n, ctypes.byref(shape), totals), "spm_batch_prepare")
+        self.shape = shape
+        self.totals = totals
+        (self.n_tiles, self.n_slots, self.n_units, self.n_chunks) = list(totals)[:4]
+        self.n_rows = totals[8]
+        return list(totals)
+
+    def desc(self, i):
+        """Descriptor of molecule i (caller's order)."""
+        return self.mols[int(self.pos[i])]
+
+
+class AFMBatch:
+    """A batch of molecules resident on one GPU (see the module docstring).
+
+    items: list of BatchItem; kind: 0 LJ / 1 Morse (one kind per batch);
+    probe: ProbeSpec; dtip: z-step (< 0: approach); slab_margin: A of z above
+    and below the tip's range whose layers are built; shape: BatchShape (None =
+    library default; ``spammm_b200.autotune`` searches better ones)."""
+
+    def __init__(self, items, kind=0, probe=None, dtip=-0.1, slab_margin=1.5, shape=None, order="lpt"):
+        _lib.require_cuda()
+        plan = BatchPlan(items, kind, probe, dtip, slab_margin, order)
+        self.plan = plan
+        self.dev = torch.device("cuda", torch.cuda.current_device())
+        self.kind, self.probe, self.dtip, self.items, self.n = plan.kind, plan.probe, plan.dtip, plan.items, plan.n
+        self.order, self.pos, self.mols = plan.order, plan.pos, plan.mols
+        ao, po, so, go = plan.total_atoms, plan.total_pixels, plan.total_states, plan.grid_float4
+        self.total_atoms, self.total_pixels, self.total_states, self.grid_float4 = ao, po, so, go
+        dev = self.dev
+        self.atoms = torch.as_tensor(plan.atoms, device=dev).contiguous()
+        self.params = torch.as_tensor(plan.params, device=dev).contiguous()
+        self.points = torch.as_tensor(plan.points, device=dev).contiguous()
+        self.grid = torch.empty((go, 4), dtype=F32, device=dev)
+        self.FEs = torch.empty((so, 4), dtype=F32, device=dev)
+        self.PPs = torch.empty((so, 4), dtype=F32, device=dev)
+        self.iter_count = torch.empty((po,), dtype=torch.int32, device=dev)
+        self.df = torch.empty((so,), dtype=F32, device=dev)
+        self.workspace = torch.zeros((max(1, int(lib().spm_relax_workspace_bytes()) // 4),), dtype=torch.int32,
+                                     device=dev)
+        # loss / adjoint buffers
+        self.target = torch.zeros((so,), dtype=F64, device=dev)
+        self.weights = None
+        self.df_c = torch.empty((so,), dtype=F64, device=dev)
+        self.dL = torch.empty((so, 4), dtype=F32, device=dev)
+        self.loss = torch.empty((self.n,), dtype=F64, device=dev)
+        self.ubar = torch.empty((so, 4), dtype=F32, device=dev)
+        self.dk = torch.empty((so, 4), dtype=F32, device=dev)
+        self.diag = torch.empty((so, 4), dtype=F32, device=dev)
+        self.grad = torch.empty((ao, 6), dtype=F64, device=dev)
+        self.dk_sum = torch.empty((4,), dtype=F64, device=dev)
+        self._Qs = hostvec(self.probe.tipQs)
+        self._QZs = hostvec(self.probe.tipQZs)
+        self.scan_params = _lib.make_scan_params(tipC=[0, 0, 1, self.dtip], stiffness=self.probe.stiffness,
+                                                 dpos0=self.probe.dpos0, relax_params=self.probe.relax_params,
+                                                 nz=0, max_iter=self.probe.max_iter, f2conv=self.probe.f2conv,
+                                                 fire=True)
+        self.shape = None
+        self.set_shape(shape if shape is not None else lib().spm_batch_default_shape())
+
+    # ------------------------------------------------------------ planning
+    def set_shape(self, shape):
+        """Number the work items for `shape` and upload the descriptors."""
+        totals = self.plan.prepare(shape)
+        self.shape = self.plan.shape
+        (self.n_tiles, self.n_slots, self.n_units, self.n_chunks, states, atoms, pixels, gend, self.n_rows) = totals
+        assert (states, atoms, pixels, gend) == (self.total_states, self.total_atoms, self.total_pixels,
+                                                 self.grid_float4)
+        raw = bytes(memoryview(self.mols).cast("B"))
+        self.mols_d = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(self.dev)
+        self.loss_scratch = torch.empty((max(1, lib().spm_batch_loss_scratch_bytes(self.n_chunks, self.n) // 8),),
+                                        dtype=F64, device=self.dev)
+        self._adj_bytes = int(lib().spm_batch_adjoint_scratch_bytes(self.plan.totals, self.n))
+        self.adj_scratch = None  # allocated by the first adjoint (it holds the adjoint grid: 32 B per slab node)
+        return self
+
+    def desc(self, i):
+        """Descriptor of molecule i (caller's order)."""
+        return self.plan.desc(i)
+
+    # ------------------------------------------------------------ stages
+    def build_grids(self):
+        rc = lib().spm_batch_grid_build(self.kind, self.n, ptr(self.mols_d), self.n_tiles, ctypes.byref(self.shape),
+                                        ptr(self.atoms), ptr(self.params), hptr(self._Qs), hptr(self._QZs),
+                                        ptr(self.grid), stream_ptr())
+        check(rc, "spm_batch_grid_build")
+
+    def relax(self):
+        rc = lib().spm_batch_relax(self.n, ptr(self.mols_d), self.n_slots, ctypes.byref(self.shape), ptr(self.grid),
+                                   ptr(self.points), ctypes.byref(self.scan_params), ptr(self.FEs), ptr(self.PPs),
+                                   ptr(self.iter_count), ptr(self.workspace), stream_ptr())
+        check(rc, "spm_batch_relax")
+
+    def df_amp(self, amp=1.0):
+        rc = lib().spm_batch_df_amp(self.n, ptr(self.mols_d), self.total_pixels, ptr(self.FEs), self.dtip,
+                                    float(amp), ptr(self.df), stream_ptr())
+        check(rc, "spm_batch_df_amp")
+
+    def loss_seed(self):
+        rc = lib().spm_batch_df_loss_seed(self.n, ptr(self.mols_d), self.n_chunks, ptr(self.FEs), ptr(self.target),
+                                          ptr(self.weights), self.dtip, ptr(self.df_c), ptr(self.dL), ptr(self.loss),
+                                          ptr(self.loss_scratch), stream_ptr())
+        check(rc, "spm_batch_df_loss_seed")
+
+    def adjoint_state(self):
+        rc = lib().spm_batch_adjoint_state(self.n, ptr(self.mols_d), self.total_states, ptr(self.grid),
+                                           ptr(self.points), ctypes.byref(self.scan_params), ptr(self.PPs),
+                                           ptr(self.dL), ptr(self.ubar), ptr(self.dk), ptr(self.diag), stream_ptr())
+        check(rc, "spm_batch_adjoint_state")
+
+    def adjoint_params(self):
+        if self.adj_scratch is None:
+            self.adj_scratch = torch.empty(((self._adj_bytes + 15) // 16, 2), dtype=F64, device=self.dev)
+        rc = lib().spm_batch_adjoint_params(self.kind, self.n, ptr(self.mols_d), self.plan.totals,
+                                            ctypes.byref(self.shape), ptr(self.atoms), ptr(self.params),
+                                            hptr(self._Qs), hptr(self._QZs), ptr(self.PPs), ptr(self.ubar),
+                                            ptr(self.dk), ptr(self.grad), ptr(self.dk_sum), ptr(self.adj_scratch),
+                                            stream_ptr())
+        check(rc, "spm_batch_adjoint_params")
+
+    def forward(self, amp=None):
+        """Grid slabs + relaxation (+ amplitude df when amp is given)."""
+        self.build_grids()
+        self.relax()
+        if amp is not None:
+            self.df_amp(amp)
+
+    def forward_adjoint(self):
+        """Forward, per-molecule df loss against self.target, adjoint ->
+        self.loss (n, work order), self.grad (total_atoms,6), self.dk_sum."""
+        self.build_grids()
+        self.relax()
+        self.loss_seed()
+        self.adjoint_state()
+        self.adjoint_params()
+        if self._mask_failed:
+            self._update_mask()
+
+    _mask_failed = False
+
+    def enable_failure_mask(self):
+        """Keep the loss consistent with its gradient: after each
+        forward_adjoint, states whose adjoint failed (not converged, unstable
+        -- where the probe flips --, singular, capped) and their z-neighbours,
+        whose central-difference df sees them, get weight 0 in the next call's
+        loss.  Their gradient is zero already; without the mask their share of
+        the loss would move in ways the gradient cannot see."""
+        w = np.ones(self.total_states, np.float64)
+        for i in range(self.n):
+            D = self.mols[i]
+            if D.nz_steps > 0:
+                v = w[D.state_off:D.state_off + D.n_scan * D.nz_steps].reshape(D.n_scan, D.nz_steps)
+                v[:, 0] = 0.0
+                v[:, -1] = 0.0
+        self.w_base = torch.as_tensor(w, device=self.dev)
+        self.weights = self.w_base.clone()
+        self._mask_failed = True
+
+    def _update_mask(self):
+        ok = self.diag[:, 3] == 0
+        ok = ok & torch.roll(ok, 1) & torch.roll(ok, -1)  # rolls cross strokes only at weight-0 ends
+        torch.mul(self.w_base, ok, out=self.weights)
+
+    # ------------------------------------------------------------ data in/out
+    def _rows(self, i, what):
+        D = self.desc(i)
+        if what == "state":
+            return D.state_off, D.state_off + D.n_scan * D.nz_steps
+        if what == "pixel":
+            return D.pix_off, D.pix_off + D.n_scan
+        return D.atom_off, D.atom_off + D.n_atoms
+
+    def fes(self, i):
+        a, b = self._rows(i, "state")
+        D = self.desc(i)
+        return self.FEs[a:b].view(D.n_scan, D.nz_steps, 4)
+
+    def pps(self, i):
+        a, b = self._rows(i, "state")
+        D = self.desc(i)
+        return self.PPs[a:b].view(D.n_scan, D.nz_steps, 4)
+
+    def df_image(self, i):
+        """(nx_r, ny_r, nz) amplitude df of molecule i (stroke order: z-step 0 highest)."""
+        a, b = self._rows(i, "state")
+        it = self.items[i]
+        return self.df[a:b].view(len(it.xs), len(it.ys), it.nz)
+
+    def df_central(self, i):
+        a, b = self._rows(i, "state")
+        it = self.items[i]
+        return self.df_c[a:b].view(len(it.xs), len(it.ys), it.nz)
+
+    def atoms_of(self, i):
+        a, b = self._rows(i, "atom")
+        return self.atoms[a:b]
+
+    def grad_of(self, i):
+        """(na,6) d(loss_i)/d(x, y, z, P1, P2, Q) of molecule i."""
+        a, b = self._rows(i, "atom")
+        return self.grad[a:b]
+
+    def loss_of(self, i):
+        return self.loss[int(self.pos[i])]
+
+    def set_atoms(self, i, atoms):
+        a, b = self._rows(i, "atom")
+        self.atoms[a:b].copy_(torch.as_tensor(np.asarray(atoms, np.float32).reshape(-1, 4), device=self.dev))
+
+    def set_target(self, i, df_target):
+        """Target df (nx_r, ny_r, nz) of molecule i for the loss."""
+        a, b = self._rows(i, "state")
+        self.target[a:b].copy_(torch.as_tensor(np.asarray(df_target, np.float64).ravel(), device=self.dev)
+                               if not isinstance(df_target, torch.Tensor) else df_target.reshape(-1).to(F64))
+
+    def capture(self, fn, warmup=1):
+        """CUDA graph of fn() (launches on the capture stream); returns the graph."""
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(warmup):
+                fn()
+        torch.cuda.current_stream().wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            fn()
+        return g
+
+
+class BatchAdam:
+    """Adam (Kingma & Ba, 2015) on the batch's atom positions and charges,
+    written with in-place torch ops on fixed buffers so one fitting step --
+    forward, df loss, adjoint, update -- captures into one CUDA graph.
+    Summing the per-molecule losses makes each molecule's update depend on its
+    own loss only."""
+
+    def __init__(self, batch, lr=0.01, betas=(0.9, 0.999), eps=1e-8, cols=(0, 1, 2, 3)):
+        self.b = batch
+        self.lr, self.b1, self.b2, self.eps = float(lr), float(betas[0]), float(betas[1]), float(eps)
+        self.cols = list(cols)
+        dev = batch.dev
+        na = batch.total_atoms
+        self.m = torch.zeros((na, 4), dtype=F32, device=dev)
+        self.v = torch.zeros((na, 4), dtype=F32, device=dev)
+        self.g = torch.zeros((na, 4), dtype=F32, device=dev)
+        self.t = torch.zeros((), dtype=F32, device=dev)
+        self.mask = torch.zeros((1, 4), dtype=F32, device=dev)
+        self.mask[0, self.cols] = 1.0
+        self._upd = torch.zeros((na, 4), dtype=F32, device=dev)
+
+    def reset(self):
+        self.m.zero_()
+        self.v.zero_()
+        self.t.zero_()
+
+    def step(self):
+        """One fitting step on the current stream (graph-capturable)."""
+        b = self.b
+        b.forward_adjoint()
+        gr = b.grad
+        self.g[:, 0:3].copy_(gr[:, 0:3])
+        self.g[:, 3].copy_(gr[:, 5])
+        self.g.mul_(self.mask)
+        self.t.add_(1.0)
+        self.m.mul_(self.b1).add_(self.g, alpha=1.0 - self.b1)
+        self.v.mul_(self.b2).addcmul_(self.g, self.g, value=1.0 - self.b2)
+        bc1 = 1.0 - torch.pow(self.b1, self.t)
+        bc2 = 1.0 - torch.pow(self.b2, self.t)
+        torch.div(self.v, bc2, out=self._upd)
+        self._upd.sqrt_().add_(self.eps)
+        torch.div(self.m / bc1, self._upd, out=self._upd)
+        b.atoms.sub_(self._upd, alpha=self.lr)

@@ -26,8 +26,19 @@
 //                              state-major gather: no scatter onto the grid, no
 //                              atomics), FP64 accumulation, fixed-order CTA
 //                              tree, then a fixed-order fold over chunks.
+// Batched (spm_batch_*, many molecules per launch), node-major instead:
+//   batch_ubar_max_kernel      per-molecule max |ubar| (fixed-point scale)
+//   batch_scatter_kernel       w * ubar onto each state's 8 corner nodes of an
+//                              adjoint grid, 64-bit fixed point: exact,
+//                              order-independent integer sums
+//   batch_adjoint_nodes_kernel atomics-free scatter by atom tiles: non-zero
+//                              adjoint-grid nodes staged in shared memory, one
+//                              thread per (atom, phase), pair-law derivatives
+//                              at each node once (not once per touching state)
+//   batch_fold_rows_kernel     fixed-order fold of the per-unit partials
 #include "spm_internal.cuh"
 #include "spm_fire.cuh"
+#include "spm_batch.cuh"
 
 namespace spm {
 namespace {
@@ -45,6 +56,8 @@ struct Corners {
 };
 
 // Texel cell of a point (the same REPEAT/LINEAR addressing as interp_fe).
+// Indices are the full grid's; SLAB: ok only if both z layers are stored.
+template <bool SLAB>
 __device__ __forceinline__ Corners corners_of(const GridView& G, V3 p) {
     Corners C;
     const float u = __fmaf_rn(p.x, G.dA.x, __fmaf_rn(p.y, G.dA.y, __fmaf_rn(p.z, G.dA.z, G.dA.w)));
@@ -53,7 +66,17 @@ __device__ __forceinline__ Corners corners_of(const GridView& G, V3 p) {
     C.ok = tex_axis(u, G.nx, C.x[0], C.x[1], C.ax);
     C.ok = tex_axis(v, G.ny, C.y[0], C.y[1], C.ay) && C.ok;
     C.ok = tex_axis(w, G.nz, C.z[0], C.z[1], C.az) && C.ok;
+    if (SLAB)
+        C.ok = C.ok && (unsigned)(C.z[0] - G.z_lo) < (unsigned)G.nz_slab &&
+               (unsigned)(C.z[1] - G.z_lo) < (unsigned)G.nz_slab;
     return C;
+}
+
+// Stored node (x, y, z) of a full grid or a slab (z is the full grid's layer).
+template <bool SLAB>
+__device__ __forceinline__ float4 node_at(const GridView& G, int x, int y, int z) {
+    const int zl = SLAB ? z - G.z_lo : z;
+    return __ldg(G.g + ((size_t)zl * G.ny + y) * G.nx + x);
 }
 
 struct Sites {
@@ -61,31 +84,27 @@ struct Sites {
     float qz[4];
 };
 
-__global__ void __launch_bounds__(AG_THREADS)
-adjoint_grid_state_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
-                          const float4* __restrict__ PPs, const float4* __restrict__ dL, float4* __restrict__ ubar,
-                          float4* __restrict__ dk, float4* __restrict__ diag) {
-    const long long st = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (st >= (long long)n_scan * P.nz) return;
-    const int iscan = (int)(st / P.nz), iz = (int)(st % P.nz);
+// Adjoint of one state: p4 = the stroke's start point, iz = its z-step,
+// pp = stored PP, u = dL/dFEs of the state; writes ubar, dk, diag.
+template <bool SLAB>
+__device__ __forceinline__ void state_adjoint(const GridView& G, const spm_scan_params& P, float4 p4, int iz,
+                                              float4 pp, float4 u, float4* ubar_o, float4* dk_o, float4* diag_o) {
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     auto fail = [&](float res, float lmin, float cond, float status) {
-        ubar[st] = zero;
-        dk[st] = zero;
-        diag[st] = make_float4(res, lmin, cond, status);
+        *ubar_o = zero;
+        *dk_o = zero;
+        *diag_o = make_float4(res, lmin, cond, status);
     };
-    const float4 pp = PPs[st], u = dL[st];
     if (!(isfinite(pp.x) && isfinite(pp.y) && isfinite(pp.z) && isfinite(pp.w) && isfinite(u.x) && isfinite(u.y) &&
           isfinite(u.z) && isfinite(u.w))) { fail(0.f, 0.f, 0.f, 2.f); return; }
     if (pp.w <= 0.f) { fail(0.f, 0.f, 0.f, 1.f); return; }
     const V3 a = mk3(P.tipA[0], P.tipA[1], P.tipA[2]);
     const V3 b = mk3(P.tipB[0], P.tipB[1], P.tipB[2]);
     const V3 c = mk3(P.tipC[0], P.tipC[1], P.tipC[2]);
-    const float4 p4 = pts[iscan];
     const V3 tip = mk3(p4.x + c.x * P.tipC[3] * (float)iz, p4.y + c.y * P.tipC[3] * (float)iz,
                        p4.z + c.z * P.tipC[3] * (float)iz);
     const V3 q = mk3(pp.x, pp.y, pp.z);
-    const Corners C = corners_of(G, q);
+    const Corners C = corners_of<SLAB>(G, q);
     if (!C.ok) { fail(0.f, 0.f, 0.f, 2.f); return; }
     // value and texel-coordinate derivatives of the 4 channels
     float val[4] = {0, 0, 0, 0}, dx[4] = {0, 0, 0, 0}, dy[4] = {0, 0, 0, 0}, dz[4] = {0, 0, 0, 0};
@@ -93,7 +112,7 @@ adjoint_grid_state_kernel(GridView G, const float4* __restrict__ pts, int n_scan
     for (int k = 0; k < 2; k++)
         for (int j = 0; j < 2; j++)
             for (int i = 0; i < 2; i++) {
-                const float4 f = __ldg(G.g + ((size_t)C.z[k] * G.ny + C.y[j]) * G.nx + C.x[i]);
+                const float4 f = node_at<SLAB>(G, C.x[i], C.y[j], C.z[k]);
                 capped |= fabsf(f.w) >= 99.9999f;
                 const float wx = i ? C.ax : 1.f - C.ax, wy = j ? C.ay : 1.f - C.ay, wz = k ? C.az : 1.f - C.az;
                 const float sx = i ? 1.f : -1.f, sy = j ? 1.f : -1.f, sz = k ? 1.f : -1.f;
@@ -193,13 +212,23 @@ adjoint_grid_state_kernel(GridView G, const float4* __restrict__ pts, int n_scan
     }
     const float cond = jinf * ainf / fabsf(det);
     if (!(cond < 1e6f)) { fail(resid, lmin, cond, 4.f); return; }
-    ubar[st] = make_float4(uv[0] - lam[0], uv[1] - lam[1], uv[2] - lam[2], u.w);
+    *ubar_o = make_float4(uv[0] - lam[0], uv[1] - lam[1], uv[2] - lam[2], u.w);
     // spring-parameter terms  -lambda . R^T dg/dk   (lambda in the tip frame: R lambda)
     const V3 lt = rotmat(mk3(lam[0], lam[1], lam[2]), a, b, c);
     const float rw = (r - d0.w) / r;
-    dk[st] = make_float4(-lt.x * (dl.x - d0.x), -lt.y * (dl.y - d0.y), -lt.z * (dl.z - d0.z),
-                         -(lt.x * dl.x + lt.y * dl.y + lt.z * dl.z) * rw);
-    diag[st] = make_float4(resid, lmin, cond, 0.f);
+    *dk_o = make_float4(-lt.x * (dl.x - d0.x), -lt.y * (dl.y - d0.y), -lt.z * (dl.z - d0.z),
+                        -(lt.x * dl.x + lt.y * dl.y + lt.z * dl.z) * rw);
+    *diag_o = make_float4(resid, lmin, cond, 0.f);
+}
+
+__global__ void __launch_bounds__(AG_THREADS)
+adjoint_grid_state_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
+                          const float4* __restrict__ PPs, const float4* __restrict__ dL, float4* __restrict__ ubar,
+                          float4* __restrict__ dk, float4* __restrict__ diag) {
+    const long long st = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (st >= (long long)n_scan * P.nz) return;
+    const int iscan = (int)(st / P.nz), iz = (int)(st % P.nz);
+    state_adjoint<false>(G, P, pts[iscan], iz, PPs[st], dL[st], ubar + st, dk + st, diag + st);
 }
 
 struct NodeGeom {
@@ -267,25 +296,18 @@ __device__ __forceinline__ void pair_grad(V3 node, float4 at, float p1, float p2
     acc[5] += gq;
 }
 
-template <int KIND>
-__global__ void __launch_bounds__(AG_THREADS)
-adjoint_grid_atoms_kernel(int na, const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
-                          Sites S, NodeGeom NG, GridView G, const float4* __restrict__ PPs,
-                          const float4* __restrict__ ubar, long long n_state, double* __restrict__ partial) {
-    __shared__ double red[6][AG_THREADS];
-    const int ia = blockIdx.y;
-    const float4 at = __ldg(atoms + ia);
-    const float* pr = params + (size_t)ia * pstride;
-    const float p1 = __ldg(pr + 0), p2 = __ldg(pr + 1), p3 = (pstride > 2) ? __ldg(pr + 2) : 0.f;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    const long long s0 = (long long)blockIdx.x * AG_CHUNK;
-    for (int t = 0; t < AG_PER_THREAD; t++) {
-        const long long st = s0 + (long long)t * AG_THREADS + threadIdx.x;
-        if (st >= n_state) break;
+// Sum over states [s_begin, s_end) (thread-strided) of one atom's pair-law
+// derivatives at each state's eight corner nodes, weighted by w * ubar.
+template <int KIND, bool SLAB>
+__device__ __forceinline__ void gather_atom(float4 at, float p1, float p2, float p3, const Sites& S,
+                                            const NodeGeom& NG, const GridView& G, const float4* __restrict__ PPs,
+                                            const float4* __restrict__ ubar, long long s_begin, long long s_end,
+                                            double* acc) {
+    for (long long st = s_begin + threadIdx.x; st < s_end; st += blockDim.x) {
         const float4 ub = __ldg(ubar + st);
         if (ub.x == 0.f && ub.y == 0.f && ub.z == 0.f && ub.w == 0.f) continue;
         const float4 pp = __ldg(PPs + st);
-        const Corners C = corners_of(G, mk3(pp.x, pp.y, pp.z));
+        const Corners C = corners_of<SLAB>(G, mk3(pp.x, pp.y, pp.z));
         if (!C.ok) continue;
         for (int k = 0; k < 2; k++)
             for (int j = 0; j < 2; j++)
@@ -299,6 +321,10 @@ adjoint_grid_atoms_kernel(int na, const float4* __restrict__ atoms, const float*
                     pair_grad<KIND>(node, at, p1, p2, p3, S, mk3(w * ub.x, w * ub.y, w * ub.z), w * ub.w, acc);
                 }
     }
+}
+
+// Fixed-order CTA tree of the six accumulators; thread 0..5 write out[0..5].
+__device__ __forceinline__ void cta_sum6(double* acc, double (*red)[AG_THREADS], double* out) {
 #pragma unroll
     for (int c6 = 0; c6 < 6; c6++) red[c6][threadIdx.x] = acc[c6];
     __syncthreads();
@@ -308,7 +334,24 @@ adjoint_grid_atoms_kernel(int na, const float4* __restrict__ atoms, const float*
             for (int c6 = 0; c6 < 6; c6++) red[c6][threadIdx.x] += red[c6][threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x < 6) partial[((size_t)ia * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = red[threadIdx.x][0];
+    if (threadIdx.x < 6) out[threadIdx.x] = red[threadIdx.x][0];
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(AG_THREADS)
+adjoint_grid_atoms_kernel(int na, const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
+                          Sites S, NodeGeom NG, GridView G, const float4* __restrict__ PPs,
+                          const float4* __restrict__ ubar, long long n_state, double* __restrict__ partial) {
+    __shared__ double red[6][AG_THREADS];
+    const int ia = blockIdx.y;
+    const float4 at = __ldg(atoms + ia);
+    const float* pr = params + (size_t)ia * pstride;
+    const float p1 = __ldg(pr + 0), p2 = __ldg(pr + 1), p3 = (pstride > 2) ? __ldg(pr + 2) : 0.f;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const long long s0 = (long long)blockIdx.x * AG_CHUNK;
+    const long long s1 = s0 + AG_CHUNK < n_state ? s0 + AG_CHUNK : n_state;
+    gather_atom<KIND, false>(at, p1, p2, p3, S, NG, G, PPs, ubar, s0, s1, acc);
+    cta_sum6(acc, red, partial + ((size_t)ia * gridDim.x + blockIdx.x) * 6);
 }
 
 // out[r*cols + c] = sum over chunks of in[(r*chunks + ch)*cols + c], fixed order.
@@ -363,8 +406,340 @@ GridView view_of(const float* grid, int nx, int ny, int nz, const spm_scan_param
 long long n_chunks(long long n_state) { return n_state > 0 ? (n_state + AG_CHUNK - 1) / AG_CHUNK : 1; }
 long long n_rowblocks(long long n_state) { return n_state > 0 ? (n_state + 2047) / 2048 : 1; }
 
+Sites make_sites(const float* Qs, const float* QZs) {
+    Sites S = {};
+    for (int k = 0; k < 4; k++) { S.qs[k] = Qs[k] * COULOMB_CONST; S.qz[k] = QZs[k]; }
+    return S;
+}
+
+// ---- batched ----------------------------------------------------------------
+__global__ void __launch_bounds__(AG_THREADS)
+batch_adjoint_state_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states,
+                           const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
+                           const float4* __restrict__ PPs, const float4* __restrict__ dL, float4* __restrict__ ubar,
+                           float4* __restrict__ dk, float4* __restrict__ diag) {
+    const long long st = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (st >= n_states) return;
+    const spm_batch_mol* D = mols + SPM_MOL_BY(state_off, mols, n_mol, st);
+    const long long ls = st - D->state_off;
+    const int nz = D->nz_steps;
+    const int iscan = (int)(ls / nz), iz = (int)(ls % nz);
+    state_adjoint<true>(slab_view(*D, grid), P, pts[D->pix_off + iscan], iz, PPs[st], dL[st], ubar + st, dk + st,
+                        diag + st);
+}
+
+// ---- node-major adjoint through the grid build (batched) -------------------
+// Adjoint grid: per slab node four int64 fixed-point sums (Fx, Fy, Fz, E
+// weights) at the grid's float4 offsets x 4.  A molecule's scale is 2^(42-e)
+// with max|ubar| < 2^e: every contribution |w*ubar| <= 2^42 units and up to
+// 2^20 contributions per node stay below 2^62.
+__device__ __forceinline__ int scale_exp(unsigned umax_bits) {
+    const int eb = (int)((umax_bits >> 23) & 0xffu);
+    return (eb > 0 ? eb : 1) - 126;  // max|ubar| < 2^e
+}
+__device__ __forceinline__ double pow2(int k) { return __longlong_as_double((long long)(1023 + k) << 52); }
+
+// CTA per 256-state chunk: per-molecule max |ubar| (as float bits; order-free).
+__global__ void __launch_bounds__(256)
+batch_ubar_max_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float4* __restrict__ ubar,
+                      unsigned* __restrict__ umax) {
+    __shared__ float s_m[8];
+    const long long ch = blockIdx.x;
+    const int m = SPM_MOL_BY(chunk_off, mols, n_mol, ch);
+    const spm_batch_mol* D = mols + m;
+    const long long nst = (long long)D->n_scan * D->nz_steps;
+    const long long ls = (ch - D->chunk_off) * 256 + threadIdx.x;
+    float v = 0.f;
+    if (ls < nst) {
+        const float4 u = __ldg(ubar + D->state_off + ls);
+        v = fmaxf(fmaxf(fabsf(u.x), fabsf(u.y)), fmaxf(fabsf(u.z), fabsf(u.w)));
+    }
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float w = s_m[0];
+        for (int k = 1; k < 8; k++) w = fmaxf(w, s_m[k]);
+        if (w > 0.f) atomicMax(umax + m, __float_as_uint(w));
+    }
+}
+
+// Thread per state: w * ubar onto the eight corner nodes (exact integer sums).
+__global__ void __launch_bounds__(256)
+batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states,
+                     const float4* __restrict__ PPs, const float4* __restrict__ ubar, const unsigned* __restrict__ umax,
+                     unsigned long long* __restrict__ gq) {
+    const long long st = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (st >= n_states) return;
+    const float4 ub = __ldg(ubar + st);
+    if (ub.x == 0.f && ub.y == 0.f && ub.z == 0.f && ub.w == 0.f) return;
+    const int m = SPM_MOL_BY(state_off, mols, n_mol, st);
+    const spm_batch_mol* D = mols + m;
+    GridView G = slab_view(*D, nullptr);
+    const float4 pp = __ldg(PPs + st);
+    const Corners C = corners_of<true>(G, mk3(pp.x, pp.y, pp.z));
+    if (!C.ok) return;
+    const double scale = pow2(42 - scale_exp(__ldg(umax + m)));
+    unsigned long long* base = gq + (size_t)D->grid_off * 4;
+    for (int k = 0; k < 2; k++)
+        for (int j = 0; j < 2; j++)
+            for (int i = 0; i < 2; i++) {
+                const float w = (i ? C.ax : 1.f - C.ax) * (j ? C.ay : 1.f - C.ay) * (k ? C.az : 1.f - C.az);
+                if (w == 0.f) continue;
+                const size_t node = ((size_t)(C.z[k] - G.z_lo) * G.ny + C.y[j]) * G.nx + C.x[i];
+                unsigned long long* q = base + node * 4;
+                atomicAdd(q + 0, (unsigned long long)__double2ll_rn((double)(w * ub.x) * scale));
+                atomicAdd(q + 1, (unsigned long long)__double2ll_rn((double)(w * ub.y) * scale));
+                atomicAdd(q + 2, (unsigned long long)__double2ll_rn((double)(w * ub.z) * scale));
+                atomicAdd(q + 3, (unsigned long long)__double2ll_rn((double)(w * ub.w) * scale));
+            }
+}
+
+constexpr int NM_THREADS = 256;
+constexpr int NM_PER_THREAD = 4;
+constexpr int NM_STAGE = NM_THREADS * NM_PER_THREAD;  // nodes examined per staging pass
+
+// CTA per node unit (molecule, `chunk` consecutive slab nodes).  Non-zero
+// adjoint-grid nodes are compacted into shared memory; thread t owns atom
+// a0 + t % nag and every P-th staged node (P = 256 / nag phases), so the
+// atom's derivative sums stay in its registers: no atomics, no cross-thread
+// reduction until the phases are folded once per unit.
+template <int KIND>
+__global__ void __launch_bounds__(NM_THREADS)
+batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk,
+                           const float4* __restrict__ atoms, const float* __restrict__ params, int pstride, Sites S,
+                           const unsigned long long* __restrict__ gq, const unsigned* __restrict__ umax,
+                           double* __restrict__ partial) {
+    __shared__ float4 s_pos[NM_STAGE];
+    __shared__ float4 s_g[NM_STAGE];
+    __shared__ double red[6][NM_THREADS];
+    __shared__ int s_wsum[NM_THREADS / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const long long unit = blockIdx.x;
+    const int m = SPM_MOL_BY(unit_off, mols, n_mol, unit);
+    const spm_batch_mol* D = mols + m;
+    const long long lc = unit - D->unit_off;
+    const int nx = D->nx, ny = D->ny, z_lo = D->z_lo;
+    const long long slab = (long long)nx * ny * D->nz_slab;
+    const long long n0 = lc * chunk;
+    const long long n1 = n0 + chunk < slab ? n0 + chunk : slab;
+    const int na = D->n_atoms;
+    NodeGeom NG;
+    NG.p0 = ld4f(D->p0);
+    NG.dA = ld4f(D->dA);
+    NG.dB = ld4f(D->dB);
+    NG.dC = ld4f(D->dC);
+    const double inv_scale = pow2(scale_exp(__ldg(umax + m)) - 42);
+    const ulonglong2* q2 = reinterpret_cast<const ulonglong2*>(gq + (size_t)D->grid_off * 4);
+    for (int a0 = 0; a0 < na; a0 += NM_THREADS) {
+        const int nag = na - a0 < NM_THREADS ? na - a0 : NM_THREADS;
+        const int P = NM_THREADS / nag;
+        const bool act = t < nag * P;
+        const int a = a0 + (act ? t % nag : 0), ph = act ? t / nag : 0;
+        const int ga = D->atom_off + a;
+        const float4 at = __ldg(atoms + ga);
+        const float* pr = params + (size_t)ga * pstride;
+        const float p1 = __ldg(pr + 0), p2 = __ldg(pr + 1), p3 = (pstride > 2) ? __ldg(pr + 2) : 0.f;
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (long long b0 = n0; b0 < n1; b0 += NM_STAGE) {
+            // stage: each thread examines NM_PER_THREAD nodes, compaction by a block scan of counts
+            ulonglong2 lo[NM_PER_THREAD], hi[NM_PER_THREAD];
+            bool nz[NM_PER_THREAD];
+            int cnt = 0;
+#pragma unroll
+            for (int r = 0; r < NM_PER_THREAD; r++) {
+                const long long node = b0 + r * NM_THREADS + t;
+                lo[r] = make_ulonglong2(0ull, 0ull);
+                hi[r] = make_ulonglong2(0ull, 0ull);
+                if (node < n1) {
+                    lo[r] = __ldg(q2 + 2 * node);
+                    hi[r] = __ldg(q2 + 2 * node + 1);
+                }
+                nz[r] = (lo[r].x | lo[r].y | hi[r].x | hi[r].y) != 0ull;
+                cnt += nz[r] ? 1 : 0;
+            }
+            int x = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) s_wsum[warp] = x;
+            __syncthreads();
+            int off = x - cnt, L = 0;
+#pragma unroll
+            for (int w = 0; w < NM_THREADS / 32; w++) {
+                const int c = s_wsum[w];
+                if (w < warp) off += c;
+                L += c;
+            }
+#pragma unroll
+            for (int r = 0; r < NM_PER_THREAD; r++) {
+                if (!nz[r]) continue;
+                const long long li = b0 + r * NM_THREADS + t;  // node index in the slab
+                const int ix = (int)(li % nx);
+                const long long yz = li / nx;
+                const int iy = (int)(yz % ny), iz = (int)(yz / ny) + z_lo;
+                s_pos[off] = make_float4(NG.p0.x + NG.dA.x * ix + NG.dB.x * iy + NG.dC.x * iz,
+                                         NG.p0.y + NG.dA.y * ix + NG.dB.y * iy + NG.dC.y * iz,
+                                         NG.p0.z + NG.dA.z * ix + NG.dB.z * iy + NG.dC.z * iz, 0.f);
+                s_g[off] = make_float4((float)((double)(long long)lo[r].x * inv_scale),
+                                       (float)((double)(long long)lo[r].y * inv_scale),
+                                       (float)((double)(long long)hi[r].x * inv_scale),
+                                       (float)((double)(long long)hi[r].y * inv_scale));
+                off++;
+            }
+            __syncthreads();
+            if (act) {
+                for (int j = ph; j < L; j += P) {
+                    const float4 np = s_pos[j], gg = s_g[j];
+                    pair_grad<KIND>(mk3(np.x, np.y, np.z), at, p1, p2, p3, S, mk3(gg.x, gg.y, gg.z), gg.w, acc);
+                }
+            }
+            __syncthreads();  // s_pos / s_g / s_wsum are restaged next pass
+        }
+#pragma unroll
+        for (int c = 0; c < 6; c++) red[c][t] = act ? acc[c] : 0.0;
+        __syncthreads();
+        if (t < nag) {
+            double* out = partial + ((size_t)D->row_off + (size_t)lc * na + a0 + t) * 6;
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                double s6 = 0.0;
+                for (int q = 0; q < P; q++) s6 += red[c][t + q * nag];
+                out[c] = s6;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// grad[ga*6 + c] = sum over the molecule's node units, fixed order.
+__global__ void __launch_bounds__(256)
+batch_fold_rows_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk, const double* __restrict__ partial,
+                       double* __restrict__ grad) {
+    __shared__ double red[256];
+    const long long ga = blockIdx.x;
+    const int c = blockIdx.y;
+    const spm_batch_mol* D = mols + SPM_MOL_BY(atom_off, mols, n_mol, ga);
+    const long long nst = (long long)D->n_scan * D->nz_steps;
+    const long long slab = (long long)D->nx * D->ny * D->nz_slab;
+    const long long nu = nst > 0 ? (slab + chunk - 1) / chunk : 0;
+    const long long a = ga - D->atom_off;
+    double acc = 0.0;
+    for (long long u = threadIdx.x; u < nu; u += 256) acc += partial[((size_t)D->row_off + u * D->n_atoms + a) * 6 + c];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) grad[ga * 6 + c] = red[0];
+}
+
+// Scratch layout of spm_batch_adjoint_params (byte offsets, 16-byte aligned).
+struct AdjScratch {
+    long long gq, part, dk, umax, total;
+};
+AdjScratch adj_scratch_layout(const long long* totals, int n_mol) {
+    AdjScratch L;
+    auto up16 = [](long long v) { return (v + 15) / 16 * 16; };
+    L.gq = 0;
+    L.part = up16(L.gq + totals[7] * 32);
+    L.dk = up16(L.part + totals[8] * 48);
+    L.umax = up16(L.dk + n_rowblocks(totals[4]) * 32);
+    L.total = up16(L.umax + (long long)n_mol * 4);
+    return L;
+}
+
 }  // namespace
 }  // namespace spm
+
+extern "C" int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_states, const float* grid,
+                                       const float* points, const spm_scan_params* p, const float* PPs,
+                                       const float* dL_dFEs, float* ubar, float* dk, float* diag, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(p, "spm_batch_adjoint_state: null params");
+    SPM_REQUIRE(n_mol >= 0 && n_states >= 0, "spm_batch_adjoint_state: negative sizes");
+    if (n_mol == 0 || n_states == 0) return SPM_OK;
+    SPM_REQUIRE(mols && grid && points && PPs && dL_dFEs && ubar && dk && diag, "spm_batch_adjoint_state: null pointer");
+    SPM_REQUIRE(aligned16(grid) && aligned16(points) && aligned16(PPs) && aligned16(dL_dFEs) && aligned16(ubar) &&
+                aligned16(dk) && aligned16(diag), "spm_batch_adjoint_state: buffers not 16-byte aligned");
+    const long long nb = (n_states + AG_THREADS - 1) / AG_THREADS;
+    SPM_REQUIRE(nb < (1LL << 31), "spm_batch_adjoint_state: too many states");
+    batch_adjoint_state_kernel<<<(unsigned)nb, AG_THREADS, 0, as_stream(stream)>>>(
+        n_mol, mols, n_states, grid, reinterpret_cast<const float4*>(points), *p, reinterpret_cast<const float4*>(PPs),
+        reinterpret_cast<const float4*>(dL_dFEs), reinterpret_cast<float4*>(ubar), reinterpret_cast<float4*>(dk),
+        reinterpret_cast<float4*>(diag));
+    return check_launch("spm_batch_adjoint_state");
+}
+
+extern "C" long long spm_batch_adjoint_scratch_bytes(const long long* totals, int n_mol) {
+    using namespace spm;
+    if (!totals || n_mol < 0) return 0;
+    return adj_scratch_layout(totals, n_mol).total;
+}
+
+extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol* mols, const long long* totals,
+                                        const spm_batch_shape* shape, const float* atoms, const float* params,
+                                        const float* Qs, const float* QZs, const float* PPs, const float* ubar,
+                                        const float* dk, double* grad, double* dk_sum, void* scratch, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(kind == SPM_KIND_LJ || kind == SPM_KIND_MORSE, "spm_batch_adjoint_params: kind=%d", kind);
+    SPM_REQUIRE(shape && totals && Qs && QZs && dk_sum && scratch, "spm_batch_adjoint_params: null pointer");
+    SPM_REQUIRE(n_mol >= 0, "spm_batch_adjoint_params: n_mol=%d", n_mol);
+    const long long n_units = totals[2], n_chunks = totals[3], n_states = totals[4], n_atoms = totals[5];
+    SPM_REQUIRE(n_units >= 0 && n_chunks >= 0 && n_states >= 0 && n_atoms >= 0 && totals[7] >= 0 && totals[8] >= 0,
+                "spm_batch_adjoint_params: negative totals");
+    const int chunk = shape->adj_chunk;
+    SPM_REQUIRE(chunk >= 1024 && chunk <= (1 << 20) && chunk % 1024 == 0, "spm_batch_adjoint_params: adj_chunk=%d",
+                chunk);
+    SPM_REQUIRE((reinterpret_cast<uintptr_t>(scratch) & 15u) == 0, "spm_batch_adjoint_params: scratch not 16-byte aligned");
+    SPM_REQUIRE(n_units < (1LL << 31) && n_chunks < (1LL << 31) && n_atoms < (1LL << 30) &&
+                (n_states + 255) / 256 < (1LL << 31), "spm_batch_adjoint_params: batch too large");
+    cudaStream_t st = as_stream(stream);
+    const AdjScratch SL = adj_scratch_layout(totals, n_mol);
+    char* base = static_cast<char*>(scratch);
+    unsigned long long* gq = reinterpret_cast<unsigned long long*>(base + SL.gq);
+    double* part = reinterpret_cast<double*>(base + SL.part);
+    double* dkpart = reinterpret_cast<double*>(base + SL.dk);
+    unsigned* umax = reinterpret_cast<unsigned*>(base + SL.umax);
+    if (n_mol > 0 && n_atoms > 0) {
+        SPM_REQUIRE(mols && atoms && params && grad && aligned16(atoms), "spm_batch_adjoint_params: null atoms/grad");
+        if (n_states > 0 && n_units > 0) {
+            SPM_REQUIRE(PPs && ubar && aligned16(PPs) && aligned16(ubar),
+                        "spm_batch_adjoint_params: state buffers null or misaligned");
+            if (cudaMemsetAsync(gq, 0, (size_t)totals[7] * 32, st) != cudaSuccess ||
+                cudaMemsetAsync(umax, 0, (size_t)n_mol * 4, st) != cudaSuccess)
+                return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: memset failed");
+            batch_ubar_max_kernel<<<(unsigned)n_chunks, 256, 0, st>>>(n_mol, mols, reinterpret_cast<const float4*>(ubar),
+                                                                      umax);
+            batch_scatter_kernel<<<(unsigned)((n_states + 255) / 256), 256, 0, st>>>(
+                n_mol, mols, n_states, reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar), umax,
+                gq);
+            const Sites S = make_sites(Qs, QZs);
+            const int pstride = kind == SPM_KIND_MORSE ? 4 : 2;
+            if (kind == SPM_KIND_LJ)
+                batch_adjoint_nodes_kernel<SPM_KIND_LJ><<<(unsigned)n_units, NM_THREADS, 0, st>>>(
+                    n_mol, mols, chunk, reinterpret_cast<const float4*>(atoms), params, pstride, S, gq, umax, part);
+            else
+                batch_adjoint_nodes_kernel<SPM_KIND_MORSE><<<(unsigned)n_units, NM_THREADS, 0, st>>>(
+                    n_mol, mols, chunk, reinterpret_cast<const float4*>(atoms), params, pstride, S, gq, umax, part);
+        }
+        batch_fold_rows_kernel<<<dim3((unsigned)n_atoms, 6), 256, 0, st>>>(n_mol, mols, chunk, part, grad);
+    }
+    if (n_states > 0) {
+        SPM_REQUIRE(dk && aligned16(dk), "spm_batch_adjoint_params: null dk");
+        const long long rb = n_rowblocks(n_states);
+        sum_rows_kernel<<<(unsigned)rb, 256, 0, st>>>(reinterpret_cast<const float4*>(dk), n_states, dkpart);
+        fold_chunks_kernel<<<dim3(1, 4), 256, 0, st>>>(dkpart, (int)rb, 4, dk_sum);
+    } else if (cudaMemsetAsync(dk_sum, 0, 4 * sizeof(double), st) != cudaSuccess) {
+        return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: memset failed");
+    }
+    return check_launch("spm_batch_adjoint_params");
+}
 
 extern "C" int spm_adjoint_grid_state(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
                                       const spm_scan_params* p, const float* PPs, const float* dL_dFEs, float* ubar,

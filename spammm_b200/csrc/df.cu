@@ -12,6 +12,7 @@
 // reads of one float4 per output element), one thread per output element.
 // Compiled with -fmad=false so the FP64 expression order matches NumPy's.
 #include "spm_internal.cuh"
+#include "spm_batch.cuh"
 #include <cmath>
 #include <vector>
 
@@ -475,6 +476,224 @@ extern "C" int spm_df_loss_seed(const void* FEs, int fes_dtype, const double* ta
     loss_grad_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(df_out, target, weights, sums, nx, ny, nz,
                                                             1.0 / (2.0 * dz), reinterpret_cast<float4*>(dL_dFEs));
     return check_launch("spm_df_loss_seed");
+}
+
+// ---------------------------------------------------------------------------
+// Batched df and df loss: each molecule's states are its (n_scan,1,nz_steps)
+// volume (z-step fastest, the first z-step highest).  Work items find their
+// molecule through the descriptor prefixes (pix_off, chunk_off); every
+// per-element expression and every reduction order is the single-volume
+// kernel's, so each molecule's results are bit-identical to those calls.
+// ---------------------------------------------------------------------------
+namespace spm {
+namespace {
+
+// Warp per stroke.  The stroke is staged lowest z-step first, so the column
+// is the ascending volume spm_df_amp_dir expects (dr = |dtip| > 0); results
+// are written back in stroke order.
+__global__ void __launch_bounds__(DFZ_WARPS * 32)
+batch_df_amp_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_pix,
+                    const float* __restrict__ FEs, DfGeom P, float* __restrict__ df) {
+    __shared__ double s_fn[DFZ_WARPS][DFZ_MAXNZ];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const long long pix = (long long)blockIdx.x * DFZ_WARPS + w;
+    if (pix >= n_pix) return;  // whole warp exits together: no CTA barrier below
+    const spm_batch_mol* D = mols + SPM_MOL_BY(pix_off, mols, n_mol, pix);
+    const int nz = D->nz_steps;
+    const long long s0 = D->state_off + (pix - D->pix_off) * (long long)nz;
+    if (nz < 2 || nz > DFZ_MAXNZ) {  // no central difference (or no room): flag the stroke
+        for (int o = l; o < nz; o += 32) df[s0 + o] = __int_as_float(0x7fc00000);
+        return;
+    }
+    double* fn = s_fn[w];
+    for (int z = l; z < nz; z += 32) {
+        const Row f = load_row(FEs, (size_t)(s0 + (nz - 1 - z)));
+        fn[z] = (f.x * P.n[0] + f.y * P.n[1]) + f.z * P.n[2];
+    }
+    __syncwarp();
+    const double sh = P.shift[2], dr = P.dr[2], nzc = P.n[2];
+    auto S = [&](int j, double u) {
+        const double c = (double)j + u * sh;
+        const double fl = floor(c);
+        const double t = c - fl;
+        const int i0 = (int)fl;
+        const double w0 = 1.0 - t, w1 = t;
+        double acc = 0.0;
+        if (w0 != 0.0) acc += fn[clampi(i0, nz)] * w0;
+        if (w1 != 0.0) acc += fn[clampi(i0 + 1, nz)] * w1;
+        return acc;
+    };
+    for (int iz = l; iz < nz; iz += 32) {
+        double acc = 0.0;
+        for (int k = 0; k < NQ; k++) {
+            const double u = P.uk[k];
+            double g;
+            if (iz == 0) g = (S(1, u) - S(0, u)) / dr;
+            else if (iz == nz - 1) g = (S(nz - 1, u) - S(nz - 2, u)) / dr;
+            else g = (S(iz + 1, u) - S(iz - 1, u)) / (2.0 * dr);
+            acc -= (P.wk * nzc) * g;
+        }
+        df[s0 + (nz - 1 - iz)] = (float)acc;
+    }
+}
+
+// CTA per 256-state chunk of one molecule: df and the chunk's (w, w*diff^2) sums.
+__global__ void __launch_bounds__(LS_THREADS)
+batch_loss_partials_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float* __restrict__ FEs,
+                           const double* __restrict__ tgt, const double* __restrict__ wts, double dz2,
+                           double* __restrict__ df_out, double* __restrict__ partial) {
+    __shared__ double s_w[LS_THREADS], s_l[LS_THREADS];
+    const long long ch = blockIdx.x;
+    const spm_batch_mol* D = mols + SPM_MOL_BY(chunk_off, mols, n_mol, ch);
+    const int nz = D->nz_steps;
+    const long long nst = (long long)D->n_scan * nz;
+    const long long ls = (ch - D->chunk_off) * LS_THREADS + threadIdx.x;
+    double w = 0.0, l = 0.0;
+    if (ls < nst) {
+        const long long gid = D->state_off + ls;
+        const int iz = (int)(ls % nz);
+        double d = 0.0;
+        if (iz > 0 && iz < nz - 1) {
+            const double fp = load_row(FEs, gid + 1).z, fm = load_row(FEs, gid - 1).z;
+            d = -(fp - fm) / dz2;
+        }
+        df_out[gid] = d;
+        w = wts ? wts[gid] : ((iz > 0 && iz < nz - 1) ? 1.0 : 0.0);
+        const double diff = d - tgt[gid];
+        l = w * (diff * diff);
+    }
+    s_w[threadIdx.x] = w;
+    s_l[threadIdx.x] = l;
+    __syncthreads();
+    for (int s = LS_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            s_w[threadIdx.x] += s_w[threadIdx.x + s];
+            s_l[threadIdx.x] += s_l[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[2 * ch] = s_w[0];
+        partial[2 * ch + 1] = s_l[0];
+    }
+}
+
+// CTA per molecule: fold its chunk partials in the fixed single-volume order.
+__global__ void __launch_bounds__(LS_THREADS)
+batch_loss_final_kernel(const spm_batch_mol* __restrict__ mols, const double* __restrict__ partial,
+                        double* __restrict__ sums, double* __restrict__ loss) {
+    __shared__ double s_w[LS_THREADS], s_l[LS_THREADS];
+    const int m = blockIdx.x;
+    const spm_batch_mol* D = mols + m;
+    const long long nst = (long long)D->n_scan * D->nz_steps;
+    const long long nblk = (nst + LS_THREADS - 1) / LS_THREADS;
+    const double* pm = partial + 2 * D->chunk_off;
+    double w = 0.0, l = 0.0;
+    for (long long i = threadIdx.x; i < nblk; i += LS_THREADS) {
+        w += pm[2 * i];
+        l += pm[2 * i + 1];
+    }
+    s_w[threadIdx.x] = w;
+    s_l[threadIdx.x] = l;
+    __syncthreads();
+    for (int s = LS_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            s_w[threadIdx.x] += s_w[threadIdx.x + s];
+            s_l[threadIdx.x] += s_l[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        sums[2 * m] = s_w[0];
+        sums[2 * m + 1] = s_l[0];
+        loss[m] = 0.5 * s_l[0] / s_w[0];
+    }
+}
+
+__global__ void __launch_bounds__(LS_THREADS)
+batch_loss_grad_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const double* __restrict__ df,
+                       const double* __restrict__ tgt, const double* __restrict__ wts, const double* __restrict__ sums,
+                       double coeff, float4* __restrict__ dL) {
+    const long long ch = blockIdx.x;
+    const int m = SPM_MOL_BY(chunk_off, mols, n_mol, ch);
+    const spm_batch_mol* D = mols + m;
+    const int nz = D->nz_steps;
+    const long long nst = (long long)D->n_scan * nz;
+    const long long ls = (ch - D->chunk_off) * LS_THREADS + threadIdx.x;
+    if (ls >= nst) return;
+    const long long base = D->state_off, gid = base + ls;
+    const int iz = (int)(ls % nz);
+    if (nz < 3) {  // no central difference: no gradient (and the stencil would leave the stroke)
+        dL[gid] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const double wsum = sums[2 * m];
+    auto g = [&](long long j) {
+        const int jz = (int)((j - base) % nz);
+        const double w = wts ? wts[j] : ((jz > 0 && jz < nz - 1) ? 1.0 : 0.0);
+        return w * (df[j] - tgt[j]) / wsum;
+    };
+    double v;
+    if (iz == 0) v = g(gid + 1) * coeff;
+    else if (iz == nz - 1) v = -g(gid - 1) * coeff;
+    else v = (g(gid + 1) - g(gid - 1)) * coeff;
+    dL[gid] = make_float4(0.f, 0.f, (float)v, 0.f);
+}
+
+}  // namespace
+}  // namespace spm
+
+extern "C" int spm_batch_df_amp(int n_mol, const spm_batch_mol* mols, long long n_pixels, const float* FEs,
+                                double dtip, double amp, float* df, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(n_mol >= 0 && n_pixels >= 0, "spm_batch_df_amp: negative sizes");
+    if (n_mol == 0 || n_pixels == 0) return SPM_OK;
+    SPM_REQUIRE(mols && FEs && df, "spm_batch_df_amp: null pointer");
+    SPM_REQUIRE(aligned16(FEs), "spm_batch_df_amp: FEs not 16-byte aligned");
+    SPM_REQUIRE(std::isfinite(dtip) && dtip != 0.0 && std::isfinite(amp), "spm_batch_df_amp: dtip=%g amp=%g", dtip, amp);
+    const double n[3] = {0.0, 0.0, 1.0}, dr[3] = {1.0, 1.0, fabs(dtip)};
+    DfGeom P;
+    int rc = fill_geom(P, 1, 1, 2, n, dr, amp);
+    if (rc) return rc;
+    const long long nb = (n_pixels + DFZ_WARPS - 1) / DFZ_WARPS;
+    SPM_REQUIRE(nb < (1LL << 31), "spm_batch_df_amp: too many pixels");
+    batch_df_amp_kernel<<<(unsigned)nb, DFZ_WARPS * 32, 0, as_stream(stream)>>>(n_mol, mols, n_pixels, FEs, P, df);
+    return check_launch("spm_batch_df_amp");
+}
+
+extern "C" long long spm_batch_loss_scratch_bytes(long long n_chunks, int n_mol) {
+    if (n_chunks < 0 || n_mol < 0) return 0;
+    return (2 * n_chunks + 2 * (long long)n_mol) * (long long)sizeof(double);
+}
+
+extern "C" int spm_batch_df_loss_seed(int n_mol, const spm_batch_mol* mols, long long n_chunks, const float* FEs,
+                                      const double* target, const double* weights, double dtip, double* df_out,
+                                      float* dL_dFEs, double* loss_out, void* scratch, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(n_mol >= 0 && n_chunks >= 0, "spm_batch_df_loss_seed: negative sizes");
+    if (n_mol == 0) return SPM_OK;
+    SPM_REQUIRE(mols && loss_out && scratch, "spm_batch_df_loss_seed: null pointer");
+    SPM_REQUIRE(dtip < 0.0, "spm_batch_df_loss_seed: dtip must be <0, got dtip=%g", dtip);
+    SPM_REQUIRE(n_chunks < (1LL << 31), "spm_batch_df_loss_seed: too many states");
+    SPM_REQUIRE((reinterpret_cast<uintptr_t>(scratch) & 7u) == 0, "spm_batch_df_loss_seed: scratch not 8-byte aligned");
+    if (n_chunks > 0)
+        SPM_REQUIRE(FEs && target && df_out && dL_dFEs && aligned16(FEs) && aligned16(dL_dFEs),
+                    "spm_batch_df_loss_seed: null or misaligned state buffers");
+    double* partial = static_cast<double*>(scratch);
+    double* sums = partial + 2 * n_chunks;
+    const double dz = fabs(dtip);
+    cudaStream_t st = as_stream(stream);
+    if (n_chunks > 0)
+        batch_loss_partials_kernel<<<(unsigned)n_chunks, LS_THREADS, 0, st>>>(n_mol, mols, FEs, target, weights,
+                                                                              2.0 * dz, df_out, partial);
+    batch_loss_final_kernel<<<(unsigned)n_mol, LS_THREADS, 0, st>>>(mols, partial, sums, loss_out);
+    if (n_chunks > 0)
+        batch_loss_grad_kernel<<<(unsigned)n_chunks, LS_THREADS, 0, st>>>(n_mol, mols, df_out, target, weights, sums,
+                                                                          1.0 / (2.0 * dz),
+                                                                          reinterpret_cast<float4*>(dL_dFEs));
+    return check_launch("spm_batch_df_loss_seed");
 }
 
 // ---------------------------------------------------------------------------

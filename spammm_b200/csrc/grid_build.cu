@@ -19,6 +19,7 @@
 //     non-zero offset get their own rsqrt.
 // Transcendentals use MUFU approximations (rsqrt.approx, ex2.approx).
 #include "spm_internal.cuh"
+#include "spm_batch.cuh"
 
 namespace spm {
 namespace {
@@ -26,7 +27,6 @@ namespace {
 constexpr int GB_TX = 32;     // threads along x
 constexpr int GB_TY = 4;      // threads along y
 constexpr int GB_ZB = 8;      // nodes along z per thread (4 packed pairs)
-constexpr int GB_ZP = GB_ZB / 2;
 constexpr int GB_TILE = 256;  // atoms per shared-memory tile
 constexpr float R2SAFE = 1e-4f;
 constexpr float COULOMB_CONST = 14.3996448915f;
@@ -95,39 +95,48 @@ struct TipSites {
     float qz[4];   // their z-offsets
 };
 
+// Node coordinate along one axis: p0 + dA*ia + dB*ib (+ dC*ic), in this
+// fixed operation order in every kernel, so a batched slab node gets the same
+// bits as the same node of a full per-molecule grid.
+__device__ __forceinline__ float node_xy(float p0, float da, float db, int ia, int ib) {
+    return __fmaf_rn(db, (float)ib, __fmaf_rn(da, (float)ia, p0));
+}
+
+// One CTA tile: a (blockDim.x x blockDim.y) patch of z-columns, ZB nodes each
+// starting at global layer ic0; nodes at layers >= zst_hi are not stored, the
+// rest go to out[((ic - zst_lo)*ny + ib)*nx + ia].
 // KIND: SPM_KIND_LJ / SPM_KIND_MORSE; ON: an on-node charge term exists;
 // NOFF: number of off-node sites.
-template <int KIND, bool ON, int NOFF>
-__global__ void __launch_bounds__(GB_TX * GB_TY)
-grid_build_kernel(int na, const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
-                  float4* __restrict__ grid, GridGeom G, TipSites S) {
+template <int KIND, bool ON, int NOFF, int ZB>
+__device__ __forceinline__ void build_tile(int na, const float4* __restrict__ atoms, const float* __restrict__ params,
+                                           int pstride, float4* __restrict__ out, const GridGeom& G,
+                                           const TipSites& S, int ia, int ib, int ic0, int zst_lo, int zst_hi) {
+    constexpr int ZP = ZB / 2;
     __shared__ float4 s_pos[GB_TILE];                   // (x, y, z, Q*qs_on)
     __shared__ float4 s_prm[GB_TILE];                   // transformed pair parameters
     __shared__ float s_q[NOFF > 0 ? NOFF : 1][GB_TILE];  // Q*Qs[k]*C per off-node site
 
-    const int tid = threadIdx.y * GB_TX + threadIdx.x;
-    const int ia = blockIdx.x * GB_TX + threadIdx.x;
-    const int ib = blockIdx.y * GB_TY + threadIdx.y;
-    const int ic0 = blockIdx.z * GB_ZB;
+    const int nthr = blockDim.x * blockDim.y;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const bool active = (ia < G.nx) && (ib < G.ny);
 
-    const float px = G.p0.x + G.dA.x * (float)ia + G.dB.x * (float)ib;
-    const float py = G.p0.y + G.dA.y * (float)ia + G.dB.y * (float)ib;
-    const float pzb = G.p0.z + G.dA.z * (float)ia + G.dB.z * (float)ib;
-    f2 pz[GB_ZP];
+    const float px = node_xy(G.p0.x, G.dA.x, G.dB.x, ia, ib);
+    const float py = node_xy(G.p0.y, G.dA.y, G.dB.y, ia, ib);
+    const float pzb = node_xy(G.p0.z, G.dA.z, G.dB.z, ia, ib);
+    f2 pz[ZP];
 #pragma unroll
-    for (int p = 0; p < GB_ZP; p++)
-        pz[p] = pk(pzb + G.dC.z * (float)(ic0 + 2 * p), pzb + G.dC.z * (float)(ic0 + 2 * p + 1));
+    for (int p = 0; p < ZP; p++)
+        pz[p] = pk(__fmaf_rn(G.dC.z, (float)(ic0 + 2 * p), pzb), __fmaf_rn(G.dC.z, (float)(ic0 + 2 * p + 1), pzb));
 
     const f2 zero = pk(0.f, 0.f);
-    f2 fx[GB_ZP], fy[GB_ZP], fz[GB_ZP], fe[GB_ZP];
+    f2 fx[ZP], fy[ZP], fz[ZP], fe[ZP];
 #pragma unroll
-    for (int p = 0; p < GB_ZP; p++) { fx[p] = zero; fy[p] = zero; fz[p] = zero; fe[p] = zero; }
+    for (int p = 0; p < ZP; p++) { fx[p] = zero; fy[p] = zero; fz[p] = zero; fe[p] = zero; }
     const f2 two = bc(2.f), one = bc(1.f);
 
     for (int t0 = 0; t0 < na; t0 += GB_TILE) {
         const int nt = min(GB_TILE, na - t0);
-        for (int j = tid; j < nt; j += GB_TX * GB_TY) {
+        for (int j = tid; j < nt; j += nthr) {
             float4 a = __ldg(atoms + t0 + j);
             const float* pr = params + (size_t)(t0 + j) * pstride;
             s_pos[j] = make_float4(a.x, a.y, a.z, a.w * S.qs_on);
@@ -154,7 +163,7 @@ grid_build_kernel(int na, const float4* __restrict__ atoms, const float* __restr
                 const f2 c0 = bc(c.x), c1 = bc(c.y), c2 = bc(c.z), c3 = bc(c.w);
                 const f2 qon = bc(a.w);
 #pragma unroll
-                for (int p = 0; p < GB_ZP; p++) {
+                for (int p = 0; p < ZP; p++) {
                     const f2 dz = sub2(pz[p], az);
                     const f2 r2 = fma2(dz, dz, dxy2);
                     const f2 rs = rsqrt2(r2);
@@ -204,7 +213,7 @@ grid_build_kernel(int na, const float4* __restrict__ atoms, const float* __restr
     }
     if (!active) return;
 #pragma unroll
-    for (int p = 0; p < GB_ZP; p++) {
+    for (int p = 0; p < ZP; p++) {
         float x[2], y[2], z[2], e[2];
         upk(fx[p], x[0], x[1]);
         upk(fy[p], y[0], y[1]);
@@ -213,14 +222,22 @@ grid_build_kernel(int na, const float4* __restrict__ atoms, const float* __restr
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int ic = ic0 + 2 * p + h;
-            if (ic >= G.nz) break;
+            if (ic >= zst_hi) break;
             float4 o = make_float4(x[h], y[h], z[h], e[h]);
             // |E| > 100 cap of the reference builders (AFM.cl:1053-1054)
             const float renorm = __fdiv_rn(100.f, fabsf(o.w));
             if (renorm < 1.f) { o.x *= renorm; o.y *= renorm; o.z *= renorm; o.w *= renorm; }
-            grid[((size_t)ic * G.ny + ib) * G.nx + ia] = o;
+            out[((size_t)(ic - zst_lo) * G.ny + ib) * G.nx + ia] = o;
         }
     }
+}
+
+template <int KIND, bool ON, int NOFF>
+__global__ void __launch_bounds__(GB_TX * GB_TY)
+grid_build_kernel(int na, const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
+                  float4* __restrict__ grid, GridGeom G, TipSites S) {
+    build_tile<KIND, ON, NOFF, GB_ZB>(na, atoms, params, pstride, grid, G, S, blockIdx.x * GB_TX + threadIdx.x,
+                                      blockIdx.y * GB_TY + threadIdx.y, blockIdx.z * GB_ZB, 0, G.nz);
 }
 
 template <int KIND, bool ON>
@@ -243,8 +260,130 @@ int launch_kind(bool on, int noff, dim3 grd, dim3 block, cudaStream_t st, int na
     return launch_noff<KIND, false>(noff, grd, block, st, na, atoms, params, pstride, out, G, S);
 }
 
+// Tip-charge sites: zero-offset charges merged into the on-node term.
+TipSites make_sites(const float* Qs, const float* QZs, bool& on, int& noff) {
+    TipSites S = {};
+    noff = 0;
+    on = false;
+    for (int k = 0; k < 4; k++) {
+        if (Qs[k] == 0.f) continue;  // a zero-charge site only adds zeros
+        if (QZs[k] == 0.f) {
+            S.qs_on += Qs[k] * COULOMB_CONST;
+            on = true;
+        } else {
+            S.qs[noff] = Qs[k] * COULOMB_CONST;
+            S.qz[noff] = QZs[k];
+            noff++;
+        }
+    }
+    return S;
+}
+
+// ---- batched slabs ----------------------------------------------------------
+// One CTA per tile of the batch; tiles of a molecule are numbered x fastest,
+// then y, then z over ceil(nx/32) x ceil(ny/TY) x ceil(nz_slab/ZB).
+template <int KIND, bool ON, int NOFF, int ZB>
+__global__ void __launch_bounds__(256)
+batch_grid_build_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float4* __restrict__ atoms,
+                        const float* __restrict__ params, int pstride, float4* __restrict__ grid, TipSites S) {
+    const long long tile = blockIdx.x;
+    const spm_batch_mol* D = mols + SPM_MOL_BY(tile_off, mols, n_mol, tile);
+    const int ty = blockDim.y;
+    const int nx = D->nx, ny = D->ny, z_lo = D->z_lo, nzs = D->nz_slab;
+    const long long lt = tile - D->tile_off;
+    const int ntx = (nx + GB_TX - 1) / GB_TX, nty = (ny + ty - 1) / ty;
+    const int bx = (int)(lt % ntx);
+    const long long r = lt / ntx;
+    const int by = (int)(r % nty);
+    const long long bz = r / nty;
+    if (bz * ZB >= nzs) return;  // whole CTA: outside the slab (prefix of another shape)
+    GridGeom G;
+    G.nx = nx; G.ny = ny; G.nz = D->nz;
+    G.p0 = ld4f(D->p0);
+    G.dA = ld4f(D->dA);
+    G.dB = ld4f(D->dB);
+    G.dC = ld4f(D->dC);
+    const int ao = D->atom_off;
+    build_tile<KIND, ON, NOFF, ZB>(D->n_atoms, atoms + ao, params + (size_t)ao * pstride, pstride, grid + D->grid_off,
+                                   G, S, bx * GB_TX + threadIdx.x, by * ty + threadIdx.y, z_lo + (int)bz * ZB, z_lo,
+                                   z_lo + nzs);
+}
+
+struct BatchLaunch {
+    unsigned blocks;
+    dim3 block;
+    cudaStream_t st;
+    int n_mol;
+    const spm_batch_mol* mols;
+    const float4* atoms;
+    const float* params;
+    int pstride;
+    float4* grid;
+};
+
+template <int KIND, bool ON, int NOFF>
+void launch_batch_zb(int zb, const BatchLaunch& L, const TipSites& S) {
+    if (zb == 16)
+        batch_grid_build_kernel<KIND, ON, NOFF, 16><<<L.blocks, L.block, 0, L.st>>>(L.n_mol, L.mols, L.atoms, L.params,
+                                                                                    L.pstride, L.grid, S);
+    else
+        batch_grid_build_kernel<KIND, ON, NOFF, 8><<<L.blocks, L.block, 0, L.st>>>(L.n_mol, L.mols, L.atoms, L.params,
+                                                                                   L.pstride, L.grid, S);
+}
+
+template <int KIND, bool ON>
+void launch_batch_noff(int noff, int zb, const BatchLaunch& L, const TipSites& S) {
+    switch (noff) {
+        case 0: launch_batch_zb<KIND, ON, 0>(zb, L, S); break;
+        case 1: launch_batch_zb<KIND, ON, 1>(zb, L, S); break;
+        case 2: launch_batch_zb<KIND, ON, 2>(zb, L, S); break;
+        case 3: launch_batch_zb<KIND, ON, 3>(zb, L, S); break;
+        default: launch_batch_zb<KIND, ON, 4>(zb, L, S); break;
+    }
+}
+
+template <int KIND>
+void launch_batch_kind(bool on, int noff, int zb, const BatchLaunch& L, const TipSites& S) {
+    if (on) launch_batch_noff<KIND, true>(noff, zb, L, S);
+    else launch_batch_noff<KIND, false>(noff, zb, L, S);
+}
+
 }  // namespace
 }  // namespace spm
+
+extern "C" int spm_batch_grid_build(int kind, int n_mol, const spm_batch_mol* mols, long long n_tiles,
+                                    const spm_batch_shape* shape, const float* atoms, const float* params,
+                                    const float* Qs, const float* QZs, float* grid, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(kind == SPM_KIND_LJ || kind == SPM_KIND_MORSE, "spm_batch_grid_build: kind=%d", kind);
+    SPM_REQUIRE(shape && Qs && QZs, "spm_batch_grid_build: null shape or host vector");
+    SPM_REQUIRE(n_mol >= 0 && n_tiles >= 0, "spm_batch_grid_build: negative sizes");
+    if (n_mol == 0 || n_tiles == 0) return SPM_OK;
+    SPM_REQUIRE(mols && grid && atoms && params, "spm_batch_grid_build: null device pointer");
+    SPM_REQUIRE(aligned16(grid) && aligned16(atoms) && (reinterpret_cast<uintptr_t>(mols) & 7u) == 0,
+                "spm_batch_grid_build: misaligned buffers");
+    SPM_REQUIRE(shape->gb_ty == 2 || shape->gb_ty == 4 || shape->gb_ty == 8, "spm_batch_grid_build: gb_ty=%d",
+                shape->gb_ty);
+    SPM_REQUIRE(shape->gb_zb == 8 || shape->gb_zb == 16, "spm_batch_grid_build: gb_zb=%d", shape->gb_zb);
+    SPM_REQUIRE(n_tiles <= 0x7fffffffLL, "spm_batch_grid_build: %lld tiles exceed one launch", n_tiles);
+    int noff = 0;
+    bool on = false;
+    const TipSites S = make_sites(Qs, QZs, on, noff);
+    BatchLaunch L;
+    L.blocks = (unsigned)n_tiles;
+    L.block = dim3(GB_TX, shape->gb_ty, 1);
+    L.st = as_stream(stream);
+    L.n_mol = n_mol;
+    L.mols = mols;
+    L.atoms = reinterpret_cast<const float4*>(atoms);
+    L.params = params;
+    L.pstride = (kind == SPM_KIND_MORSE) ? 4 : 2;
+    L.grid = reinterpret_cast<float4*>(grid);
+    if (kind == SPM_KIND_MORSE) launch_batch_kind<SPM_KIND_MORSE>(on, noff, shape->gb_zb, L, S);
+    else launch_batch_kind<SPM_KIND_LJ>(on, noff, shape->gb_zb, L, S);
+    return check_launch("spm_batch_grid_build");
+}
 
 extern "C" int spm_grid_build(int kind, int n_atoms, const float* atoms, const float* params, float* grid,
                               int nx, int ny, int nz, const float* p0, const float* dA, const float* dB,
@@ -269,20 +408,9 @@ extern "C" int spm_grid_build(int kind, int n_atoms, const float* atoms, const f
     G.dA = make_float4(dA[0], dA[1], dA[2], dA[3]);
     G.dB = make_float4(dB[0], dB[1], dB[2], dB[3]);
     G.dC = make_float4(dC[0], dC[1], dC[2], dC[3]);
-    TipSites S = {};
     int noff = 0;
     bool on = false;
-    for (int k = 0; k < 4; k++) {
-        if (Qs[k] == 0.f) continue;  // a zero-charge site only adds zeros
-        if (QZs[k] == 0.f) {
-            S.qs_on += Qs[k] * COULOMB_CONST;
-            on = true;
-        } else {
-            S.qs[noff] = Qs[k] * COULOMB_CONST;
-            S.qz[noff] = QZs[k];
-            noff++;
-        }
-    }
+    const TipSites S = make_sites(Qs, QZs, on, noff);
     dim3 block(GB_TX, GB_TY, 1);
     dim3 grd((nx + GB_TX - 1) / GB_TX, (ny + GB_TY - 1) / GB_TY, (nz + GB_ZB - 1) / GB_ZB);
     const int pstride = (kind == SPM_KIND_MORSE) ? 4 : 2;

@@ -22,6 +22,7 @@
 // multiply-adds are the explicit __fmaf_rn calls shared with the CPU oracle.
 #include "spm_internal.cuh"
 #include "spm_fire.cuh"
+#include "spm_batch.cuh"
 
 namespace spm {
 namespace {
@@ -72,7 +73,72 @@ __device__ __forceinline__ int next_pixel(unsigned* counter, int n_scan, int ras
 
 __device__ __forceinline__ float4 ld4(const float* a) { return make_float4(a[0], a[1], a[2], a[3]); }
 
-// MODE 0: relaxStrokes; MODE 1: relaxStrokesTilted.
+// Probe frame, spring and integrator settings of an SPM_RELAX_PP scan.
+struct PPFrame {
+    V3 a, b, c, dTip, d0r;
+    float4 kk, d0;
+    float surf, f2conv;
+    int max_iter;
+    bool fire;
+};
+
+__device__ __forceinline__ PPFrame pp_frame(const spm_scan_params& P) {
+    PPFrame F;
+    const float4 tc = ld4(P.tipC);
+    F.a = mk3(P.tipA[0], P.tipA[1], P.tipA[2]);
+    F.b = mk3(P.tipB[0], P.tipB[1], P.tipB[2]);
+    F.c = mk3(tc.x, tc.y, tc.z);
+    F.kk = ld4(P.stiffness);
+    F.d0 = ld4(P.dpos0);
+    F.surf = P.surfFF[0];
+    F.f2conv = P.f2conv;
+    F.max_iter = P.max_iter;
+    F.fire = (P.flags & SPM_FLAG_FIRE) != 0;
+    F.dTip = mk3(__fmul_rn(F.c.x, tc.w), __fmul_rn(F.c.y, tc.w), __fmul_rn(F.c.z, tc.w));
+    F.d0r = rotmatT(mk3(F.d0.x, F.d0.y, F.d0.z), F.a, F.b, F.c);
+    return F;
+}
+
+// One SPM_RELAX_PP iteration (the direct path's bookkeeping: the convergence
+// test comes before the update).  Returns true when the z-step is finished;
+// conv tells whether it converged.  SLAB: a sample outside the stored layers
+// (NaN) ends the z-step at once, not converged.
+template <typename IDX, bool SLAB>
+__device__ __forceinline__ bool pp_iter(const GridView& G, const PPFrame& F, V3 tip, V3& pos, V3& v, Integrator& I,
+                                        float4& fe, int& it, int& total_it, bool& conv) {
+    conv = false;
+    if (it >= F.max_iter) return true;
+    ++it;
+    ++total_it;
+    fe = interp_fe<IDX, SLAB>(G, pos);
+    if (SLAB && fe.w != fe.w) return true;
+    const V3 ft = rotmatT(tip_force(rotmat(sub3(pos, tip), F.a, F.b, F.c), F.kk, F.d0), F.a, F.b, F.c);
+    V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
+    f.x = __fmaf_rn(F.c.x, F.surf, f.x);
+    f.y = __fmaf_rn(F.c.y, F.surf, f.y);
+    f.z = __fmaf_rn(F.c.z, F.surf, f.z);
+    if (dot3(f, f) < F.f2conv) {
+        conv = true;
+        return true;
+    }
+    md_step(f, v, pos, I, F.fire);
+    return it >= F.max_iter;
+}
+
+// Outputs of a finished SPM_RELAX_PP z-step: tip-frame FE at the final
+// position and PP = (pos, +iterations if converged and finite, else -iterations).
+template <typename IDX, bool SLAB>
+__device__ __forceinline__ void pp_emit(const GridView& G, const PPFrame& F, V3 pos, float4 fe, int it, bool conv,
+                                        float4* fe_out, float4* pp_out) {
+    if (!conv) fe = interp_fe<IDX, SLAB>(G, pos);  // the position moved after the last sample
+    const V3 r = rotmat(mk3(fe.x, fe.y, fe.z), F.a, F.b, F.c);
+    *fe_out = make_float4(r.x, r.y, r.z, fe.w);
+    const bool finite = isfinite(fe.x) && isfinite(fe.y) && isfinite(fe.z) && isfinite(fe.w) && isfinite(pos.x) &&
+                        isfinite(pos.y) && isfinite(pos.z);
+    *pp_out = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
+}
+
+// MODE 0: relaxStrokes; MODE 1: relaxStrokesTilted; MODE 2: PP (differentiable path).
 template <int MODE, typename IDX>
 __global__ void __launch_bounds__(RX_THREADS)
 relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
@@ -113,34 +179,14 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
         total_it = 0;
     };
     if (k >= 0) start(k);
+    PPFrame F;
+    if (MODE == 2) F = pp_frame(P);
     while (k >= 0) {
         if (MODE == 2) {
-            // equilibrium bookkeeping of the direct path: test before the update
-            bool done = true, conv = false;
-            if (it < max_iter) {
-                ++it;
-                ++total_it;
-                fe = interp_fe<IDX>(G, pos);
-                const V3 ft = rotmatT(tip_force(rotmat(sub3(pos, tip), a, b, c), kk, d0), a, b, c);
-                V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
-                f.x = __fmaf_rn(c.x, surf, f.x);
-                f.y = __fmaf_rn(c.y, surf, f.y);
-                f.z = __fmaf_rn(c.z, surf, f.z);
-                if (dot3(f, f) < P.f2conv) {
-                    conv = true;
-                } else {
-                    md_step(f, v, pos, I, fire);
-                    done = (it >= max_iter);
-                }
-            }
-            if (done) {
-                if (!conv) fe = interp_fe<IDX>(G, pos);  // the position moved after the last sample
+            bool conv;
+            if (pp_iter<IDX, false>(G, F, tip, pos, v, I, fe, it, total_it, conv)) {
                 const size_t o = (size_t)k * nzs + iz;
-                const V3 r = rotmat(mk3(fe.x, fe.y, fe.z), a, b, c);
-                FEs[o] = make_float4(r.x, r.y, r.z, fe.w);
-                const bool finite = isfinite(fe.x) && isfinite(fe.y) && isfinite(fe.z) && isfinite(fe.w) &&
-                                    isfinite(pos.x) && isfinite(pos.y) && isfinite(pos.z);
-                disps[o] = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
+                pp_emit<IDX, false>(G, F, pos, fe, it, conv, FEs + o, disps + o);
                 tip = add3(tip, dTip);
                 pos = add3(pos, dTip);
                 v = mk3(0.f, 0.f, 0.f);
@@ -291,8 +337,143 @@ int launch_mode(const GridView& G, long long nodes, const float4* pts, int n_sca
     return launch_relax<MODE, size_t>(G, pts, n_scan, P, FEs, disps, iter_count, counter, st);
 }
 
+// ---- batched SPM_RELAX_PP ---------------------------------------------------
+// Slot t of the batch -> (molecule, pixel): the molecule owning t by its
+// slot_off prefix; inside a raster molecule slots run over tiles of
+// (32 >> th_log2) (ix) x (1 << th_log2) (iy) pixels, tiles ordered iy-fastest.
+__device__ __forceinline__ bool next_batch_pixel(unsigned* counter, unsigned n_slots, const spm_batch_mol* mols,
+                                                 int n_mol, int th_log2, int& m, int& k) {
+    const unsigned lane = threadIdx.x & 31u;
+    while (true) {
+        const unsigned msk = __activemask();
+        const int leader = __ffs(msk) - 1;
+        const unsigned rank = __popc(msk & ((1u << lane) - 1u));
+        unsigned base = 0;
+        if ((int)lane == leader) base = atomicAdd(counter, (unsigned)__popc(msk));
+        base = __shfl_sync(msk, base, leader);
+        const unsigned t = base + rank;
+        if (t >= n_slots) return false;
+        m = SPM_MOL_BY(slot_off, mols, n_mol, (long long)t);
+        const spm_batch_mol* D = mols + m;
+        const unsigned lt = t - (unsigned)D->slot_off;
+        const int ny = D->raster_ny, n_scan = D->n_scan;
+        if (ny <= 0) {
+            k = (int)lt;
+            if (k < n_scan) return true;
+            continue;  // stale prefix: draw again (t only grows: bounded)
+        }
+        const int nxr = n_scan / ny;
+        const unsigned th = 1u << th_log2;
+        const unsigned nty = ((unsigned)ny + th - 1u) >> th_log2;
+        const unsigned tile = lt >> 5, r = lt & 31u;
+        const int ix = (int)((tile / nty) * (32u >> th_log2) + (r >> th_log2));
+        const int iy = (int)((tile % nty) * th + (r & (th - 1u)));
+        if (ix < nxr && iy < ny) {
+            k = ix * ny + iy;
+            return true;
+        }
+        // an edge tile's slot outside the raster: draw again
+    }
+}
+
+__global__ void __launch_bounds__(256)
+batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
+                   const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
+                   float4* __restrict__ FEs, float4* __restrict__ PPs, int* __restrict__ iter_count,
+                   unsigned* __restrict__ counter) {
+    const PPFrame F = pp_frame(P);
+    int m = 0, k = 0;
+    bool have = next_batch_pixel(counter, n_slots, mols, n_mol, th_log2, m, k);
+    GridView G;
+    long long sbase = 0;
+    int nzs = 0, pix = 0;
+    V3 tip, pos, v;
+    Integrator I;
+    float4 fe;
+    int iz = 0, it = 0, total_it = 0;
+    auto start = [&]() {
+        const spm_batch_mol* D = mols + m;
+        G = slab_view(*D, grid);
+        nzs = D->nz_steps;
+        pix = D->pix_off + k;
+        sbase = D->state_off + (long long)k * nzs;
+        const float4 p4 = pts[pix];
+        tip = mk3(p4.x, p4.y, p4.z);
+        pos = add3(tip, F.d0r);
+        I.dt = P.relax_params[0];
+        I.damp = P.relax_params[1];
+        I.dtmax = I.dt;
+        I.dtmin = __fmul_rn(I.dtmax, 0.1f);
+        I.damp0 = I.damp;
+        v = mk3(0.f, 0.f, 0.f);
+        fe = make_float4(0.f, 0.f, 0.f, 0.f);
+        iz = 0;
+        it = 0;
+        total_it = 0;
+    };
+    if (have) start();
+    while (have) {
+        bool conv;
+        if (pp_iter<unsigned, true>(G, F, tip, pos, v, I, fe, it, total_it, conv)) {
+            const long long o = sbase + iz;
+            pp_emit<unsigned, true>(G, F, pos, fe, it, conv, FEs + o, PPs + o);
+            tip = add3(tip, F.dTip);
+            pos = add3(pos, F.dTip);
+            v = mk3(0.f, 0.f, 0.f);
+            fe = make_float4(0.f, 0.f, 0.f, 0.f);
+            it = 0;
+            if (++iz == nzs) {
+                if (iter_count) iter_count[pix] = total_it;
+                have = next_batch_pixel(counter, n_slots, mols, n_mol, th_log2, m, k);
+                if (have) start();
+            }
+        }
+    }
+}
+
 }  // namespace
 }  // namespace spm
+
+extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n_slots, const spm_batch_shape* shape,
+                               const float* grid, const float* points, const spm_scan_params* p, float* FEs,
+                               float* PPs, int* iter_count, void* workspace, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(shape && p, "spm_batch_relax: null shape/params");
+    SPM_REQUIRE(n_mol >= 0 && n_slots >= 0, "spm_batch_relax: negative sizes");
+    if (n_mol == 0 || n_slots == 0) return SPM_OK;
+    SPM_REQUIRE(n_slots < (1LL << 31), "spm_batch_relax: %lld slots exceed the 31-bit counter", n_slots);
+    SPM_REQUIRE(mols && grid && points && FEs && PPs && workspace, "spm_batch_relax: null device pointer");
+    SPM_REQUIRE(aligned16(grid) && aligned16(points) && aligned16(FEs) && aligned16(PPs) &&
+                (reinterpret_cast<uintptr_t>(workspace) & 3u) == 0 && (reinterpret_cast<uintptr_t>(mols) & 7u) == 0,
+                "spm_batch_relax: misaligned buffers");
+    SPM_REQUIRE((p->flags & ~(SPM_FLAG_FIRE | SPM_FLAG_FLIP_Z)) == 0, "spm_batch_relax: unknown flags 0x%x", p->flags);
+    const int thr = shape->rx_threads, h = shape->rx_tile_h;
+    SPM_REQUIRE(thr == 64 || thr == 128 || thr == 256, "spm_batch_relax: rx_threads=%d", thr);
+    SPM_REQUIRE(h >= 1 && h <= 32 && (h & (h - 1)) == 0, "spm_batch_relax: rx_tile_h=%d", h);
+    SPM_REQUIRE(shape->rx_ctas_per_sm >= 0, "spm_batch_relax: rx_ctas_per_sm=%d", shape->rx_ctas_per_sm);
+    int th_log2 = 0;
+    while ((1 << th_log2) < h) th_log2++;
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_relax_kernel, thr, 0) != cudaSuccess)
+        return set_error(SPM_ERR_CUDA, "spm_batch_relax: cannot query the device occupancy");
+    if (per_sm < 1) per_sm = 1;
+    if (shape->rx_ctas_per_sm > 0 && shape->rx_ctas_per_sm < per_sm) per_sm = shape->rx_ctas_per_sm;
+    const long long need = (n_slots + thr - 1) / thr;
+    const long long cap = (long long)sms * per_sm;
+    const unsigned blocks = (unsigned)(need < cap ? need : cap);
+    cudaStream_t st = as_stream(stream);
+    unsigned* ctr = static_cast<unsigned*>(workspace);
+    if (cudaMemsetAsync(ctr, 0, sizeof(unsigned), st) != cudaSuccess)
+        return set_error(SPM_ERR_CUDA, "spm_batch_relax: cannot reset the slot counter");
+    batch_relax_kernel<<<blocks, thr, 0, st>>>(n_mol, mols, (unsigned)n_slots, th_log2, grid,
+                                               reinterpret_cast<const float4*>(points), *p,
+                                               reinterpret_cast<float4*>(FEs), reinterpret_cast<float4*>(PPs),
+                                               iter_count, ctr);
+    return check_launch("spm_batch_relax");
+}
 
 extern "C" long long spm_relax_workspace_bytes(void) { return 16; }
 

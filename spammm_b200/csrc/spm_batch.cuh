@@ -1,0 +1,42 @@
+// spm_batch.cuh -- helpers shared by the batched kernels.
+//
+// A batch is an array of spm_batch_mol descriptors in device memory.  Work
+// items of every stage (grid tiles, relaxation slots, states, gather units,
+// loss chunks, pixels, atoms) are numbered across the batch by a prefix field
+// of the descriptor; the molecule that owns item x is the largest m with
+// prefix(m) <= x, found by binary search (log2(n_mol) cached loads).
+#pragma once
+#include "spm_internal.cuh"
+#include "spm_fire.cuh"
+
+namespace spm {
+
+template <typename T, T spm_batch_mol::*F>
+__device__ __forceinline__ int find_mol(const spm_batch_mol* __restrict__ mols, int n_mol, long long x) {
+    int lo = 0, hi = n_mol - 1;  // mols[0].*F == 0 <= x
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((long long)__ldg(&(mols[mid].*F)) <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+#define SPM_MOL_BY(field, mols, n, x) find_mol<decltype(spm_batch_mol::field), &spm_batch_mol::field>(mols, n, x)
+
+__device__ __forceinline__ float4 ld4f(const float* a) { return make_float4(__ldg(a), __ldg(a + 1), __ldg(a + 2), __ldg(a + 3)); }
+
+// Sampling view of a molecule's slab (full-grid coordinates, stored layers only).
+__device__ __forceinline__ GridView slab_view(const spm_batch_mol& D, const float* grid) {
+    GridView G;
+    G.g = reinterpret_cast<const float4*>(grid) + D.grid_off;
+    G.nx = D.nx; G.ny = D.ny; G.nz = D.nz;
+    G.dA = ld4f(D.dinvA);
+    G.dB = ld4f(D.dinvB);
+    G.dC = ld4f(D.dinvC);
+    G.z_lo = D.z_lo;
+    G.nz_slab = D.nz_slab;
+    return G;
+}
+
+}  // namespace spm

@@ -110,11 +110,15 @@ struct GridView {
     const float4* __restrict__ g;
     int nx, ny, nz;
     float4 dA, dB, dC;  // normalized-coordinate transform rows
+    int z_lo, nz_slab;  // SLAB views: only layers [z_lo, z_lo + nz_slab) are stored
 };
 
 // interpFE: exact FP32 trilinear sample with periodic wrap.  IDX is the type
 // of the node offsets (unsigned for grids below 2^32 nodes, size_t above).
-template <typename IDX = size_t>
+// SLAB: the grid holds only layers [z_lo, z_lo+nz_slab) of the full grid; the
+// coordinate arithmetic is the full grid's (identical results), and a sample
+// that needs a layer outside the slab returns NaN instead of reading it.
+template <typename IDX = size_t, bool SLAB = false>
 __device__ __forceinline__ float4 interp_fe(const GridView& G, V3 p) {
     float u = __fmaf_rn(p.x, G.dA.x, __fmaf_rn(p.y, G.dA.y, __fmaf_rn(p.z, G.dA.z, G.dA.w)));
     float v = __fmaf_rn(p.x, G.dB.x, __fmaf_rn(p.y, G.dB.y, __fmaf_rn(p.z, G.dB.z, G.dB.w)));
@@ -124,6 +128,11 @@ __device__ __forceinline__ float4 interp_fe(const GridView& G, V3 p) {
     bool ok = tex_axis(u, G.nx, x0, x1, ax);
     ok = tex_axis(v, G.ny, y0, y1, ay) && ok;
     ok = tex_axis(w, G.nz, z0, z1, az) && ok;
+    if (SLAB) {
+        z0 -= G.z_lo;
+        z1 -= G.z_lo;
+        ok = ok && (unsigned)z0 < (unsigned)G.nz_slab && (unsigned)z1 < (unsigned)G.nz_slab;
+    }
     if (!ok) {
         float nan = __int_as_float(0x7fc00000);
         return make_float4(nan, nan, nan, nan);

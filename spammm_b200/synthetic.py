@@ -12,7 +12,9 @@ molecules/slabs with fixed seeds.  Shapes, sizes and value distributions:
                 60-atom C/N/H planar molecule at 3.0 A; grid 48x48x24 A at
                 0.1 A (480x480x240); 480x480 pixels, 60 z-steps of 0.1 A.
   batch         molecules with U{10..120} C/N/O/H atoms, grids 12-32 A per
-                side at 0.1 A, scan windows 64^2-256^2 pixels, 30-60 z-steps.
+                side at 0.1 A (at least the molecule + 3 A on each side),
+                scan windows of 64^2-256^2 pixels over the molecule, 30-60
+                z-steps of 0.1 A ending 4 A above the molecule plane.
 
 Probe (all configs): k_xy = 0.25 N/m, k_z = 20 N/m (harmonic, no radial
 bond), Q = -0.05 e at the probe position; FIRE <= 1000 steps, |F| < 1e-5 eV/A.
@@ -162,12 +164,21 @@ def plain_large(seed=1, kind=0, n_pix=480, nz=60):
                        0.1, k, d0, Qs, QZs)
 
 
-def batch_molecules(n_mol=512, seed=3, kind=0):
-    """n_mol molecules from the batch distribution (see module docstring)."""
+def batch_molecules(n_mol=512, seed=3, kind=0, z_end=4.0, dz=0.1, natoms=(10, 120), side=(12.0, 32.0),
+                    zside=(12.0, 32.0), npx=(64, 256), nzs=(30, 60), pad=3.0):
+    """n_mol BatchItems of the batch distribution: U{10..120} C/N/O/H atoms on
+    honeycomb fragments, grids of U(12,32) A per side (x = y; at least the
+    molecule's extent + 2*pad, so the periodic seam of the grid stays `pad` A
+    away from every atom) and U(12,32) A in z at 0.1 A, square rasters of
+    U{64..256}^2 pixels over the molecule's extent + 1 A on each side,
+    U{30..60} z-steps of dz ending z_end A above the molecule plane.  The grid
+    top sits 2 A above the first tip position.  The ranges are parameters
+    (smaller ones make test batches)."""
+    from .batch import BatchItem
     rng = np.random.default_rng(seed)
     out = []
     for m in range(n_mol):
-        na = int(rng.integers(10, 121))
+        na = int(rng.integers(natoms[0], natoms[1] + 1))
         nH = max(1, int(round(na * rng.uniform(0.15, 0.3))))
         nN = int(rng.integers(0, max(1, na // 10) + 1))
         nO = int(rng.integers(0, max(1, na // 10) + 1))
@@ -175,11 +186,17 @@ def batch_molecules(n_mol=512, seed=3, kind=0):
         pos, Z, q = planar_molecule({"C": nC, "N": nN, "O": nO, "H": nH}, seed * 100003 + m)
         atoms, prm = (_lj_atoms_from_Z if kind == 0 else _morse_atoms_from_Z)(pos, Z)
         atoms[:, 3] = q.astype(np.float32)
-        side = float(rng.uniform(12.0, 32.0))
-        n = int(round(side / 0.1))
-        nzg = int(round(float(rng.uniform(12.0, 32.0)) / 0.1))
-        npx = int(rng.integers(64, 257))
-        nzs = int(rng.integers(30, 61))
-        out.append(dict(atoms=atoms, params=prm, kind=kind, origin=np.array([-side / 2, -side / 2, -4.0]), step=0.1,
-                        ngrid=(n, n, nzg), n_pix=npx, nz=nzs))
+        half = float(np.abs(pos[:, :2]).max())  # molecule centred at the origin
+        cell = max(float(rng.uniform(*side)), 2.0 * (half + pad))
+        n = int(np.ceil(cell / 0.1))
+        nzg = int(round(float(rng.uniform(*zside)) / 0.1))
+        n_px = int(rng.integers(npx[0], npx[1] + 1))
+        n_z = int(rng.integers(nzs[0], nzs[1] + 1))
+        cell = n * 0.1
+        z_top = z_end + (n_z - 1) * dz
+        origin = np.array([-cell / 2, -cell / 2, z_top + 2.0 - nzg * 0.1])
+        win = half + 1.0
+        xs = (-win + (np.arange(n_px) + 0.5) * (2.0 * win / n_px)).astype(np.float32)
+        out.append(BatchItem(atoms=atoms, params=prm, origin=origin, step=0.1, ngrid=(n, n, nzg), xs=xs,
+                             ys=xs.copy(), z_top=float(z_top), nz=n_z))
     return out

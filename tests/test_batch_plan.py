@@ -1,0 +1,114 @@
+"""Host-side planning of batches (no GPU): descriptor layout, work numbering,
+slab ranges and argument validation of spm_batch_prepare."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from spammm_b200 import _lib, synthetic
+from spammm_b200.batch import BatchPlan, ProbeSpec, slab_range
+
+
+def small_items(n=7, seed=5, kind=0):
+    return synthetic.batch_molecules(n, seed=seed, kind=kind, natoms=(10, 40), side=(5, 9), zside=(8, 14),
+                                     npx=(5, 21), nzs=(8, 16))
+
+
+def test_struct_layout():
+    # spm_batch_mol: 7 int64 offsets, 12 int32 fields, 7 float[4] vectors
+    assert ctypes.sizeof(_lib.BatchMol) == 7 * 8 + 12 * 4 + 7 * 16
+    assert ctypes.sizeof(_lib.BatchShape) == 6 * 4
+
+
+@pytest.mark.parametrize("shape_kw", [{}, dict(gb_ty=2, gb_zb=16, rx_tile_h=1, adj_chunk=1024),
+                                      dict(gb_ty=8, rx_tile_h=32, rx_threads=256, adj_chunk=65536)])
+def test_prepare_totals(shape_kw):
+    items = small_items()
+    plan = BatchPlan(items)
+    shape = _lib.lib().spm_batch_default_shape()
+    for k, v in shape_kw.items():
+        setattr(shape, k, v)
+    tot = plan.prepare(shape)
+    tiles = slots = units = chunks = rows = 0
+    th = shape.rx_tile_h
+    tw = 32 // th
+    for j in range(plan.n):
+        D = plan.mols[j]
+        assert (D.tile_off, D.slot_off, D.unit_off, D.chunk_off, D.row_off) == (tiles, slots, units, chunks, rows)
+        tiles += -(-D.nx // 32) * -(-D.ny // shape.gb_ty) * -(-D.nz_slab // shape.gb_zb)
+        nst = D.n_scan * D.nz_steps
+        nxr = D.n_scan // D.raster_ny
+        slots += -(-nxr // tw) * -(-D.raster_ny // th) * 32
+        u = -(-(D.nx * D.ny * D.nz_slab) // shape.adj_chunk)
+        units += u
+        rows += u * D.n_atoms
+        chunks += -(-nst // 256)
+    assert tot[:4] == [tiles, slots, units, chunks]
+    assert tot[4:7] == [plan.total_states, plan.total_atoms, plan.total_pixels]
+    assert tot[7:] == [plan.grid_float4, rows]
+
+
+def test_order_and_offsets():
+    items = small_items(9)
+    plan = BatchPlan(items)
+    cost = [items[i].n_scan * items[i].nz for i in plan.order]
+    assert cost == sorted(cost, reverse=True)
+    assert sorted(plan.order.tolist()) == list(range(len(items)))
+    for i, it in enumerate(items):
+        D = plan.desc(i)
+        a = plan.atoms[D.atom_off:D.atom_off + D.n_atoms]
+        np.testing.assert_array_equal(a, np.asarray(it.atoms, np.float32))
+        pts = plan.points[D.pix_off:D.pix_off + D.n_scan]
+        np.testing.assert_array_equal(pts, it.points())
+        assert D.nz_steps == it.nz and D.raster_ny == len(it.ys)
+
+
+def test_slab_covers_probe_range():
+    probe = ProbeSpec()
+    for it in small_items(12, seed=9):
+        z_lo, nzs = slab_range(it, probe, -0.1, 1.5)
+        oz, h = float(it.origin[2]), float(it.step)
+        for z in (it.z_top + 1.5, it.z_top - (it.nz - 1) * 0.1 - 1.5):
+            t = (z - oz) / h
+            assert z_lo <= np.floor(t) and np.floor(t) + 1 < z_lo + nzs
+        assert 0 <= z_lo and z_lo + nzs <= it.ngrid[2]
+    # a range reaching the grid edge keeps the whole grid (periodic wrap)
+    it = small_items(1)[0]
+    it.z_top = float(it.origin[2]) + 0.05
+    assert slab_range(it, probe, -0.1, 1.5) == (0, it.ngrid[2])
+
+
+def test_prepare_rejects_bad_descriptors():
+    L = _lib.lib()
+    shape = L.spm_batch_default_shape()
+    totals = (ctypes.c_longlong * _lib.SPM_BATCH_TOTALS)()
+    plan = BatchPlan(small_items(4))
+    assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_OK
+    # rows that do not follow the previous molecule's
+    plan.mols[2].atom_off += 1
+    assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_ERR_ARG
+    assert b"follow" in L.spm_last_error()
+    plan.mols[2].atom_off -= 1
+    # slab outside the grid
+    plan.mols[1].nz_slab = plan.mols[1].nz + 1
+    assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_ERR_ARG
+    plan.mols[1].nz_slab = 4
+    # overlapping slabs
+    plan.mols[3].grid_off = plan.mols[2].grid_off
+    assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_ERR_ARG
+    plan = BatchPlan(small_items(4))
+    for field, bad in (("gb_ty", 3), ("gb_zb", 4), ("rx_threads", 96), ("rx_tile_h", 6), ("adj_chunk", 1000)):
+        s = L.spm_batch_default_shape()
+        setattr(s, field, bad)
+        assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(s), totals) == _lib.SPM_ERR_ARG, field
+
+
+def test_partial_raster_falls_back_to_1d():
+    plan = BatchPlan(small_items(3))
+    plan.mols[0].raster_ny = 7 if plan.mols[0].n_scan % 7 else 11
+    if plan.mols[0].n_scan % plan.mols[0].raster_ny == 0:
+        pytest.skip("raster size divisible")
+    tot = plan.prepare(_lib.lib().spm_batch_default_shape())
+    assert plan.mols[0].raster_ny == 0
+    assert plan.mols[1].slot_off == plan.mols[0].n_scan
+    assert tot[1] > 0

@@ -1,0 +1,150 @@
+"""Batched grid path on the GPU: every molecule of a batch against the
+per-molecule calls (bit-exact forward, loss and state adjoint; gradients to
+FP64 summation order), the CPU oracle, CUDA-graph replay and launch shapes."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from spammm_b200 import _lib, gpu, synthetic
+from spammm_b200.batch import AFMBatch, BatchAdam, ProbeSpec
+
+pytestmark = pytest.mark.gpu
+
+
+def _items(kind=0, n=6, seed=21):
+    return synthetic.batch_molecules(n, seed=seed, kind=kind, natoms=(10, 40), side=(5, 9), zside=(8, 14),
+                                     npx=(6, 22), nzs=(8, 16))
+
+
+def _per_molecule(batch, i):
+    """The unbatched path for molecule i: full grid, relax_pp."""
+    it = batch.items[i]
+    spec = it.spec(batch.kind, batch.probe, batch.dtip)
+    p0, dA, dB, dC = spec.vectors()
+    grid = gpu.grid_build(batch.kind, it.atoms.astype(np.float32), it.params.astype(np.float32), spec.ngrid, p0, dA,
+                          dB, dC, spec.tipQs, spec.tipQZs)
+    P = spec.scan_params(batch.probe.stiffness)
+    pts = torch.as_tensor(spec.points, device="cuda")
+    FEs, PPs = gpu.relax_pp(grid, P, pts)
+    return spec, grid, P, pts, FEs, PPs
+
+
+def _target(batch, seed=4):
+    rng = np.random.default_rng(seed)
+    for i, it in enumerate(batch.items):
+        batch.set_target(i, rng.normal(0.0, 0.05, (len(it.xs), len(it.ys), it.nz)))
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_batch_forward_matches_per_molecule(cuda, kind):
+    b = AFMBatch(_items(kind), kind=kind)
+    b.forward(amp=1.0)
+    torch.cuda.synchronize()
+    for i, it in enumerate(b.items):
+        spec, grid, P, pts, FEs, PPs = _per_molecule(b, i)
+        D = b.desc(i)
+        slab = b.grid[D.grid_off:D.grid_off + D.nx * D.ny * D.nz_slab].view(D.nz_slab, D.ny, D.nx, 4)
+        assert torch.equal(slab, grid[D.z_lo:D.z_lo + D.nz_slab]), f"molecule {i}: slab differs from full grid"
+        assert (b.pps(i)[..., 3] > 0).all(), f"molecule {i}: a stroke left the slab or did not converge"
+        assert torch.equal(b.fes(i), FEs) and torch.equal(b.pps(i), PPs), f"molecule {i}: relaxation differs"
+        # df of the stroke, ascending z (dr = |dtip|), as the single-volume call
+        vol = FEs.view(it.n_scan, 1, it.nz, 4).flip(2).contiguous()
+        df = gpu.df_amp_dir(vol, abs(b.dtip), (0., 0., 1.), 1.0).flip(2).reshape(len(it.xs), len(it.ys), it.nz)
+        assert torch.equal(b.df_image(i), df), f"molecule {i}: df differs"
+
+
+def test_batch_relax_matches_oracle(cuda):
+    b = AFMBatch(_items(0, n=3, seed=8))
+    b.forward()
+    torch.cuda.synchronize()
+    for i, it in enumerate(b.items):
+        spec, grid, P, pts, FEs, PPs = _per_molecule(b, i)
+        oFE, oPP = O.relax_pp(grid.cpu().numpy(), spec.dinv(), spec.points, spec.nz, [1, 0, 0, 0], [0, 1, 0, 0],
+                              [0, 0, 1, spec.dtip], b.probe.stiffness, spec.dpos0, spec.relax_params, [0, 0, 0, 0],
+                              spec.max_iter, spec.f2conv, True)
+        assert np.array_equal(b.fes(i).cpu().numpy(), oFE) and np.array_equal(b.pps(i).cpu().numpy(), oPP)
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_batch_loss_and_adjoint_match_per_molecule(cuda, kind):
+    b = AFMBatch(_items(kind, seed=33 + kind), kind=kind)
+    _target(b)
+    b.forward_adjoint()
+    torch.cuda.synchronize()
+    dk_total = torch.zeros(4, dtype=torch.float64, device="cuda")
+    for i, it in enumerate(b.items):
+        spec, grid, P, pts, FEs, PPs = _per_molecule(b, i)
+        a, c = b._rows(i, "state")
+        tgt = b.target[a:c].view(it.n_scan, 1, it.nz)
+        loss, df, dL = gpu.df_loss_seed(FEs.view(it.n_scan, 1, it.nz, 4), tgt, b.dtip)
+        assert torch.equal(b.loss_of(i).reshape(1), loss)
+        assert torch.equal(b.df_c[a:c], df.reshape(-1)) and torch.equal(b.dL[a:c], dL.reshape(-1, 4))
+        ubar, dk, diag = gpu.adjoint_grid_state(grid, P, pts, PPs, dL.reshape(it.n_scan, it.nz, 4))
+        assert torch.equal(b.ubar[a:c], ubar) and torch.equal(b.dk[a:c], dk) and torch.equal(b.diag[a:c], diag)
+        p0, dA, dB, dC = spec.vectors()
+        grad, dks = gpu.adjoint_grid_params(kind, it.atoms.astype(np.float32), it.params.astype(np.float32), p0, dA,
+                                            dB, dC, spec.tipQs, spec.tipQZs, grid, P, PPs, ubar, dk)
+        # node-major sums (batch) vs state-major sums (per molecule): equal up to summation order
+        torch.testing.assert_close(b.grad_of(i), grad, rtol=1e-5, atol=1e-7 * float(grad.abs().max()))
+        dk_total += dks
+    torch.testing.assert_close(b.dk_sum, dk_total, rtol=1e-9, atol=1e-14)
+
+
+def test_batch_shapes_give_same_results(cuda):
+    items = _items(0, n=5, seed=41)
+    ref = AFMBatch(items)
+    _target(ref)
+    ref.forward_adjoint()
+    L = _lib.lib()
+    for kw in (dict(gb_ty=2, gb_zb=16, rx_threads=64, rx_tile_h=1, adj_chunk=1024),
+               dict(gb_ty=8, gb_zb=8, rx_threads=256, rx_tile_h=32, rx_ctas_per_sm=1, adj_chunk=65536)):
+        s = L.spm_batch_default_shape()
+        for k, v in kw.items():
+            setattr(s, k, v)
+        b = AFMBatch(items, shape=s)
+        b.target.copy_(ref.target)
+        b.forward_adjoint()
+        torch.cuda.synchronize()
+        assert torch.equal(b.grid, ref.grid) and torch.equal(b.FEs, ref.FEs) and torch.equal(b.PPs, ref.PPs)
+        assert torch.equal(b.loss, ref.loss) and torch.equal(b.ubar, ref.ubar)
+        torch.testing.assert_close(b.grad, ref.grad, rtol=1e-10, atol=1e-13)
+
+
+def test_batch_graph_replay(cuda):
+    b = AFMBatch(_items(0, n=4, seed=51))
+    _target(b)
+    b.forward_adjoint()
+    torch.cuda.synchronize()
+    eager = [t.clone() for t in (b.FEs, b.PPs, b.loss, b.grad)]
+    g = b.capture(b.forward_adjoint)
+    for t in (b.FEs, b.PPs, b.loss, b.grad, b.grid):
+        t.zero_()
+    g.replay()
+    g.replay()
+    torch.cuda.synchronize()
+    for e, t in zip(eager, (b.FEs, b.PPs, b.loss, b.grad)):
+        assert torch.equal(e, t)
+
+
+def test_batch_adam_reduces_loss(cuda):
+    items = _items(0, n=4, seed=61)
+    truth = AFMBatch(items)
+    truth.forward_adjoint()  # target 0: df_c is the df image of the true structures
+    b = AFMBatch(items)
+    b.target.copy_(truth.df_c)
+    rng = np.random.default_rng(2)
+    for i, it in enumerate(items):
+        a = it.atoms.copy()
+        a[:, :3] += rng.normal(0.0, 0.05, (len(a), 3)).astype(np.float32)
+        b.set_atoms(i, a)
+    opt = BatchAdam(b, lr=0.005, cols=(0, 1, 2))
+    b.forward_adjoint()
+    loss0 = b.loss.clone()
+    g = b.capture(opt.step, warmup=0)
+    for _ in range(15):
+        g.replay()
+    b.forward_adjoint()
+    torch.cuda.synchronize()
+    assert torch.isfinite(b.loss).all()
+    assert float(b.loss.sum()) < float(loss0.sum())
