@@ -325,6 +325,7 @@ typedef struct spm_batch_shape {
     int rx_tile_h;      /* relaxation pixel tile: (32/rx_tile_h) x rx_tile_h pixels, power of two <= 32 */
     int rx_ctas_per_sm; /* persistent relaxation CTAs per SM, 0 = occupancy maximum */
     int adj_chunk;      /* slab nodes per adjoint unit: multiple of 1024 in [1024, 1048576] */
+    int rx_regs;        /* relaxation register budget: 0 = 80 per thread, 1 = 64 (more warps, some spills) */
 } spm_batch_shape;
 
 spm_batch_shape spm_batch_default_shape(void);

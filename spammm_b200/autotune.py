@@ -1,0 +1,122 @@
+"""Launch-shape autotuner of the batched path.
+
+Every batched stage reads only its own fields of ``spm_batch_shape``:
+
+  grid build   gb_ty (CTA rows: 32 x gb_ty threads), gb_zb (z-nodes per thread)
+  relaxation   rx_threads (CTA size), rx_tile_h (pixel tile (32/h) x h per warp
+               draw), rx_regs (80 or 64 registers per thread)
+  adjoint      adj_chunk (slab nodes per node-major unit)
+
+so the stages are tuned one after another, each over its own candidates with
+the others held fixed, by timing the stage's launch with CUDA events on a
+representative sub-batch (every k-th molecule of the work order, so the mix
+of sizes is kept).  Results are cached per (device, workload signature) for
+the process, and optionally in a JSON file.
+"""
+import json
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from .batch import AFMBatch
+
+GRID_CANDIDATES = [dict(gb_ty=ty, gb_zb=zb) for ty in (2, 4, 8) for zb in (8, 16)]
+RELAX_CANDIDATES = [dict(rx_threads=t, rx_tile_h=h, rx_regs=r) for t in (128, 256) for h in (4, 8, 16)
+                    for r in (0, 1)]
+ADJOINT_CANDIDATES = [dict(adj_chunk=c) for c in (4096, 16384, 65536)]
+
+_CACHE = {}
+
+
+def _with(shape, **kw):
+    s = _lib.BatchShape(*shape.key())
+    for k, v in kw.items():
+        setattr(s, k, int(v))
+    return s
+
+
+def _time(fn, reps):
+    fn()
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+def signature(items, kind):
+    """Workload key: molecule count, kind, total atoms / pixels / states."""
+    return (len(items), int(kind), int(sum(len(it.atoms) for it in items)), int(sum(it.n_scan for it in items)),
+            int(sum(it.n_scan * it.nz for it in items)))
+
+
+def sub_batch(items, max_molecules):
+    """Every k-th molecule in order of relaxation work (the batch's own order)."""
+    if len(items) <= max_molecules:
+        return list(items)
+    cost = np.array([it.n_scan * it.nz for it in items])
+    order = np.argsort(-cost, kind="stable")
+    pick = order[np.linspace(0, len(items) - 1, max_molecules).round().astype(int)]
+    return [items[i] for i in sorted(set(pick.tolist()))]
+
+
+def tune(batch, reps=2, adjoint=True, log=None):
+    """Tune batch.shape in place, stage by stage; returns (shape, timings)."""
+    report = {}
+    shape = batch.shape
+
+    def pick(name, cands, run):
+        nonlocal shape
+        res = []
+        for kw in cands:
+            s = _with(shape, **kw)
+            batch.set_shape(s)
+            ms = _time(run, reps)
+            res.append((ms, kw))
+            if log:
+                log(f"autotune {name} {kw}: {ms:.3f} ms")
+        res.sort(key=lambda r: r[0])
+        shape = _with(shape, **res[0][1])
+        report[name] = {"best": res[0][1], "ms": res[0][0], "worst_ms": res[-1][0], "tried": len(res)}
+
+    pick("grid", GRID_CANDIDATES, batch.build_grids)
+    batch.set_shape(shape)
+    batch.build_grids()
+    pick("relax", RELAX_CANDIDATES, batch.relax)
+    if adjoint:
+        batch.set_shape(shape)
+        batch.relax()
+        batch.loss_seed()
+        batch.adjoint_state()
+        pick("adjoint", ADJOINT_CANDIDATES, batch.adjoint_params)
+    batch.set_shape(shape)
+    return shape, report
+
+
+def tuned_shape(items, kind=0, probe=None, dtip=-0.1, max_molecules=24, reps=2, adjoint=True, cache_file=None,
+                log=None):
+    """Best BatchShape for a workload, tuned on a sub-batch of at most
+    max_molecules molecules (cached per device and workload signature)."""
+    dev = torch.cuda.get_device_name()
+    key = json.dumps([dev, signature(items, kind), bool(adjoint)])
+    if key not in _CACHE and cache_file and os.path.exists(cache_file):
+        with open(cache_file) as f:
+            _CACHE.update(json.load(f))
+    if key in _CACHE:
+        return _lib.BatchShape(*_CACHE[key]["shape"]), _CACHE[key]["report"]
+    sub = AFMBatch(sub_batch(items, max_molecules), kind=kind, probe=probe, dtip=dtip)
+    shape, report = tune(sub, reps=reps, adjoint=adjoint, log=log)
+    del sub
+    torch.cuda.empty_cache()
+    _CACHE[key] = {"shape": list(shape.key()), "report": report}
+    if cache_file:
+        with open(cache_file, "w") as f:
+            json.dump(_CACHE, f, indent=1)
+    return shape, report

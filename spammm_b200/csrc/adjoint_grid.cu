@@ -406,12 +406,6 @@ GridView view_of(const float* grid, int nx, int ny, int nz, const spm_scan_param
 long long n_chunks(long long n_state) { return n_state > 0 ? (n_state + AG_CHUNK - 1) / AG_CHUNK : 1; }
 long long n_rowblocks(long long n_state) { return n_state > 0 ? (n_state + 2047) / 2048 : 1; }
 
-Sites make_sites(const float* Qs, const float* QZs) {
-    Sites S = {};
-    for (int k = 0; k < 4; k++) { S.qs[k] = Qs[k] * COULOMB_CONST; S.qz[k] = QZs[k]; }
-    return S;
-}
-
 // ---- batched ----------------------------------------------------------------
 __global__ void __launch_bounds__(AG_THREADS)
 batch_adjoint_state_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states,
@@ -498,6 +492,107 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
 constexpr int NM_THREADS = 256;
 constexpr int NM_PER_THREAD = 4;
 constexpr int NM_STAGE = NM_THREADS * NM_PER_THREAD;  // nodes examined per staging pass
+constexpr int NM_FLUSH = 64;                          // FP32 partial sums folded into FP64 every 64 pairs
+constexpr float LOG2E = 1.4426950408889634f;
+
+__device__ __forceinline__ float mufu_rsqrt(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float mufu_ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Tip-charge sites of the node-major adjoint: sites with a zero z-offset sit on
+// the node and share the pair law's 1/r; the others get their own rsqrt.
+struct NodeSites {
+    float qon;           // sum of Qs[k]*COULOMB_CONST over sites with QZs[k] == 0
+    int noff;
+    float qs[4], qz[4];  // off-node sites
+};
+
+NodeSites make_node_sites(const float* Qs, const float* QZs) {
+    NodeSites S = {};
+    for (int k = 0; k < 4; k++) {
+        if (Qs[k] == 0.f) continue;
+        if (QZs[k] == 0.f) {
+            S.qon += Qs[k] * COULOMB_CONST;
+        } else {
+            S.qs[S.noff] = Qs[k] * COULOMB_CONST;
+            S.qz[S.noff] = QZs[k];
+            S.noff++;
+        }
+    }
+    return S;
+}
+
+// pair_grad's derivatives (same pair laws, same formulas) evaluated the way the
+// grid build evaluates the forward: one MUFU rsqrt per pair for the pair law
+// and the on-node charges together, MUFU ex2 for Morse; FP32, added to acc.
+template <int KIND>
+__device__ __forceinline__ void pair_adj_fast(float4 np, float4 at, float p1, float p2, float p3, const NodeSites& S,
+                                              float4 g, float* acc) {
+    const float dx = np.x - at.x, dy = np.y - at.y, dz = np.z - at.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, R2SAFE)));
+    const float rs = mufu_rsqrt(r2);
+    const float ir2 = rs * rs;
+    const float du = fmaf(dx, g.x, fmaf(dy, g.y, dz * g.z));
+    const float uE = g.w;
+    float s, sp, gp1, gp2;
+    if (KIND == SPM_KIND_LJ) {
+        const float c6 = p1, c12 = p2;
+        const float ir6 = ir2 * ir2 * ir2;
+        const float ir8 = ir6 * ir2;
+        const float ir14 = ir8 * ir6;
+        s = fmaf(12.f * c12, ir14, -6.f * c6 * ir8);
+        sp = fmaf(-84.f * c12, ir14, 24.f * c6 * ir8) * ir2;
+        gp1 = fmaf(du, -6.f * ir8, -uE * ir6);
+        gp2 = fmaf(du, 12.f * ir14, uE * ir6 * ir6);
+    } else {
+        const float R0 = p1, E0 = p2, K = p3;
+        const float r = r2 * rs;
+        const float e = mufu_ex2(K * LOG2E * (r - R0));
+        const float em1 = e - 1.f;
+        const float Ep = 2.f * K * E0 * e * em1;
+        const float Epp = 2.f * K * K * E0 * e * (2.f * e - 1.f);
+        s = -Ep * rs;
+        sp = -(Epp * rs - Ep * ir2) * 0.5f * rs;
+        gp1 = fmaf(du, Epp * rs, -uE * Ep);
+        gp2 = fmaf(du, -2.f * K * e * em1 * rs, uE * e * (e - 2.f));
+    }
+    float gq = 0.f;
+    if (S.qon != 0.f) {
+        const float qr = S.qon * rs;
+        const float sk = qr * at.w * ir2;
+        s += sk;
+        sp = fmaf(-1.5f * sk, ir2, sp);
+        gq = fmaf(du, qr * ir2, uE * qr);
+    }
+    const float A = fmaf(uE, s, -2.f * sp * du);
+    acc[0] += fmaf(A, dx, -s * g.x);
+    acc[1] += fmaf(A, dy, -s * g.y);
+    acc[2] += fmaf(A, dz, -s * g.z);
+    acc[3] += gp1;
+    acc[4] += gp2;
+    for (int k = 0; k < S.noff; k++) {
+        const float dk = dz + S.qz[k];
+        const float rk = mufu_rsqrt(fmaf(dx, dx, fmaf(dy, dy, fmaf(dk, dk, R2SAFE))));
+        const float irk2 = rk * rk;
+        const float qr = S.qs[k] * rk;
+        const float sk = qr * at.w * irk2;
+        const float duk = fmaf(dx, g.x, fmaf(dy, g.y, dk * g.z));
+        const float Ak = fmaf(uE, sk, 3.f * sk * irk2 * duk);
+        acc[0] += fmaf(Ak, dx, -sk * g.x);
+        acc[1] += fmaf(Ak, dy, -sk * g.y);
+        acc[2] += fmaf(Ak, dk, -sk * g.z);
+        gq += fmaf(duk, qr * irk2, uE * qr);
+    }
+    acc[5] += gq;
+}
+
 
 // CTA per node unit (molecule, `chunk` consecutive slab nodes).  Non-zero
 // adjoint-grid nodes are compacted into shared memory; thread t owns atom
@@ -505,11 +600,11 @@ constexpr int NM_STAGE = NM_THREADS * NM_PER_THREAD;  // nodes examined per stag
 // atom's derivative sums stay in its registers: no atomics, no cross-thread
 // reduction until the phases are folded once per unit.
 template <int KIND>
-__global__ void __launch_bounds__(NM_THREADS)
+__global__ void __launch_bounds__(NM_THREADS, 3)
 batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk,
-                           const float4* __restrict__ atoms, const float* __restrict__ params, int pstride, Sites S,
-                           const unsigned long long* __restrict__ gq, const unsigned* __restrict__ umax,
-                           double* __restrict__ partial) {
+                           const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
+                           NodeSites S, const unsigned long long* __restrict__ gq,
+                           const unsigned* __restrict__ umax, double* __restrict__ partial) {
     __shared__ float4 s_pos[NM_STAGE];
     __shared__ float4 s_g[NM_STAGE];
     __shared__ double red[6][NM_THREADS];
@@ -542,20 +637,18 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
         const float p1 = __ldg(pr + 0), p2 = __ldg(pr + 1), p3 = (pstride > 2) ? __ldg(pr + 2) : 0.f;
         double acc[6] = {0, 0, 0, 0, 0, 0};
         for (long long b0 = n0; b0 < n1; b0 += NM_STAGE) {
-            // stage: each thread examines NM_PER_THREAD nodes, compaction by a block scan of counts
-            ulonglong2 lo[NM_PER_THREAD], hi[NM_PER_THREAD];
+            // stage: each thread examines NM_PER_THREAD nodes, compaction by a block scan of counts;
+            // the non-zero nodes are read again (an L1 hit) when they are written to shared memory
             bool nz[NM_PER_THREAD];
             int cnt = 0;
 #pragma unroll
             for (int r = 0; r < NM_PER_THREAD; r++) {
                 const long long node = b0 + r * NM_THREADS + t;
-                lo[r] = make_ulonglong2(0ull, 0ull);
-                hi[r] = make_ulonglong2(0ull, 0ull);
+                nz[r] = false;
                 if (node < n1) {
-                    lo[r] = __ldg(q2 + 2 * node);
-                    hi[r] = __ldg(q2 + 2 * node + 1);
+                    const ulonglong2 lo = __ldg(q2 + 2 * node), hi = __ldg(q2 + 2 * node + 1);
+                    nz[r] = (lo.x | lo.y | hi.x | hi.y) != 0ull;
                 }
-                nz[r] = (lo[r].x | lo[r].y | hi[r].x | hi[r].y) != 0ull;
                 cnt += nz[r] ? 1 : 0;
             }
             int x = cnt;
@@ -577,24 +670,33 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
             for (int r = 0; r < NM_PER_THREAD; r++) {
                 if (!nz[r]) continue;
                 const long long li = b0 + r * NM_THREADS + t;  // node index in the slab
+                const ulonglong2 lo = __ldg(q2 + 2 * li), hi = __ldg(q2 + 2 * li + 1);
                 const int ix = (int)(li % nx);
                 const long long yz = li / nx;
                 const int iy = (int)(yz % ny), iz = (int)(yz / ny) + z_lo;
                 s_pos[off] = make_float4(NG.p0.x + NG.dA.x * ix + NG.dB.x * iy + NG.dC.x * iz,
                                          NG.p0.y + NG.dA.y * ix + NG.dB.y * iy + NG.dC.y * iz,
                                          NG.p0.z + NG.dA.z * ix + NG.dB.z * iy + NG.dC.z * iz, 0.f);
-                s_g[off] = make_float4((float)((double)(long long)lo[r].x * inv_scale),
-                                       (float)((double)(long long)lo[r].y * inv_scale),
-                                       (float)((double)(long long)hi[r].x * inv_scale),
-                                       (float)((double)(long long)hi[r].y * inv_scale));
+                s_g[off] = make_float4((float)((double)(long long)lo.x * inv_scale),
+                                       (float)((double)(long long)lo.y * inv_scale),
+                                       (float)((double)(long long)hi.x * inv_scale),
+                                       (float)((double)(long long)hi.y * inv_scale));
                 off++;
             }
             __syncthreads();
             if (act) {
+                float a32[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                int n32 = 0;
                 for (int j = ph; j < L; j += P) {
-                    const float4 np = s_pos[j], gg = s_g[j];
-                    pair_grad<KIND>(mk3(np.x, np.y, np.z), at, p1, p2, p3, S, mk3(gg.x, gg.y, gg.z), gg.w, acc);
+                    pair_adj_fast<KIND>(s_pos[j], at, p1, p2, p3, S, s_g[j], a32);
+                    if (++n32 == NM_FLUSH) {
+#pragma unroll
+                        for (int c = 0; c < 6; c++) { acc[c] += a32[c]; a32[c] = 0.f; }
+                        n32 = 0;
+                    }
                 }
+#pragma unroll
+                for (int c = 0; c < 6; c++) acc[c] += a32[c];
             }
             __syncthreads();  // s_pos / s_g / s_wsum are restaged next pass
         }
@@ -719,7 +821,7 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             batch_scatter_kernel<<<(unsigned)((n_states + 255) / 256), 256, 0, st>>>(
                 n_mol, mols, n_states, reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar), umax,
                 gq);
-            const Sites S = make_sites(Qs, QZs);
+            const NodeSites S = make_node_sites(Qs, QZs);
             const int pstride = kind == SPM_KIND_MORSE ? 4 : 2;
             if (kind == SPM_KIND_LJ)
                 batch_adjoint_nodes_kernel<SPM_KIND_LJ><<<(unsigned)n_units, NM_THREADS, 0, st>>>(

@@ -19,6 +19,7 @@ extern "C" spm_batch_shape spm_batch_default_shape(void) {
     s.rx_tile_h = 8;
     s.rx_ctas_per_sm = 0;
     s.adj_chunk = 16384;
+    s.rx_regs = 0;
     return s;
 }
 
@@ -38,6 +39,7 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
     SPM_REQUIRE(S.rx_ctas_per_sm >= 0, "spm_batch_prepare: rx_ctas_per_sm=%d", S.rx_ctas_per_sm);
     SPM_REQUIRE(S.adj_chunk >= 1024 && S.adj_chunk <= (1 << 20) && S.adj_chunk % 1024 == 0,
                 "spm_batch_prepare: adj_chunk=%d", S.adj_chunk);
+    SPM_REQUIRE(S.rx_regs == 0 || S.rx_regs == 1, "spm_batch_prepare: rx_regs=%d", S.rx_regs);
     const long long th = S.rx_tile_h, tw = 32 / S.rx_tile_h;
     long long tiles = 0, slots = 0, units = 0, chunks = 0, states = 0, atoms = 0, pixels = 0, grid_end = 0, rows = 0;
     for (int m = 0; m < n_mol; m++) {
@@ -57,6 +59,9 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
         SPM_REQUIRE(D.grid_off >= grid_end, "spm_batch_prepare: molecule %d: grid_off=%lld overlaps the previous slab "
                     "(ends at %lld)", m, D.grid_off, grid_end);
         SPM_REQUIRE(D.dC[0] == 0.f && D.dC[1] == 0.f, "spm_batch_prepare: molecule %d: dC must be (0,0,dz)", m);
+        SPM_REQUIRE(D.dinvA[1] == 0.f && D.dinvA[2] == 0.f && D.dinvB[0] == 0.f && D.dinvB[2] == 0.f &&
+                    D.dinvC[0] == 0.f && D.dinvC[1] == 0.f,
+                    "spm_batch_prepare: molecule %d: the sampling transform must be axis-aligned", m);
         SPM_REQUIRE(D.raster_ny >= 0, "spm_batch_prepare: molecule %d: raster_ny=%d", m, D.raster_ny);
         if (D.raster_ny > 0 && D.n_scan % D.raster_ny != 0) D.raster_ny = 0;  // not a full raster: 1D order
         const long long nst = (long long)D.n_scan * D.nz_steps;

@@ -20,6 +20,7 @@
 // Transcendentals use MUFU approximations (rsqrt.approx, ex2.approx).
 #include "spm_internal.cuh"
 #include "spm_batch.cuh"
+#include "spm_f32x2.cuh"
 
 namespace spm {
 namespace {
@@ -32,36 +33,6 @@ constexpr float R2SAFE = 1e-4f;
 constexpr float COULOMB_CONST = 14.3996448915f;
 constexpr float LOG2E = 1.4426950408889634f;
 
-typedef unsigned long long f2;  // two packed float32 lanes (lo = node 2p, hi = node 2p+1)
-
-__device__ __forceinline__ f2 pk(float lo, float hi) {
-    f2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ void upk(f2 v, float& lo, float& hi) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
-    f2 d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
-    f2 d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f2 add2(f2 a, f2 b) {
-    f2 d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
-    f2 d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
 __device__ __forceinline__ float fast_rsqrt(float x) {
     float y;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -82,8 +53,6 @@ __device__ __forceinline__ f2 ex2_2(f2 x) {
     upk(x, a, b);
     return pk(fast_ex2(a), fast_ex2(b));
 }
-__device__ __forceinline__ f2 bc(float v) { return pk(v, v); }
-
 struct GridGeom {
     int nx, ny, nz;
     float4 p0, dA, dB, dC;

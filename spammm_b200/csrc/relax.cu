@@ -376,15 +376,53 @@ __device__ __forceinline__ bool next_batch_pixel(unsigned* counter, unsigned n_s
     }
 }
 
-__global__ void __launch_bounds__(256)
+// One SPM_RELAX_PP iteration of a z-stroke (probe frame = identity, tipC =
+// (0,0,1,dz)) on an axis-aligned slab: pp_iter with the frame rotations
+// dropped -- with an identity frame they change no value (the sign of an exact
+// zero aside) -- and c*surf reduced to its z part.
+template <typename IDX>
+__device__ __forceinline__ bool pp_iter_z(const AxisView& G, const spm_scan_params& P, V3 tip, V3& pos, V3& v,
+                                          Integrator& I, float4& fe, int& it, int& total_it, bool& conv) {
+    conv = false;
+    if (it >= P.max_iter) return true;
+    ++it;
+    ++total_it;
+    fe = interp_fe_axis<IDX, true>(G, pos);
+    if (fe.w != fe.w) return true;  // outside the slab (or a NaN grid): not converged
+    const V3 ft = tip_force(sub3(pos, tip), ld4(P.stiffness), ld4(P.dpos0));
+    V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
+    f.z = __fadd_rn(f.z, P.surfFF[0]);
+    if (dot3(f, f) < P.f2conv) {
+        conv = true;
+        return true;
+    }
+    md_step(f, v, pos, I, (P.flags & SPM_FLAG_FIRE) != 0);
+    return it >= P.max_iter;
+}
+
+__device__ __forceinline__ AxisView axis_view(const spm_batch_mol* D, const float* grid) {
+    AxisView G;
+    G.g = reinterpret_cast<const float4*>(grid) + D->grid_off;
+    G.nx = D->nx; G.ny = D->ny; G.nz = D->nz;
+    G.z_lo = D->z_lo; G.nz_slab = D->nz_slab;
+    G.ax = D->dinvA[0]; G.aw = D->dinvA[3];
+    G.by = D->dinvB[1]; G.bw = D->dinvB[3];
+    G.cz = D->dinvC[2]; G.cw = D->dinvC[3];
+    return G;
+}
+
+// MINB = 3: up to 80 registers per thread (768 resident threads per SM);
+// MINB = 4: 64 registers (1024 resident threads, a few spilled values).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB)
 batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
                    const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
                    float4* __restrict__ FEs, float4* __restrict__ PPs, int* __restrict__ iter_count,
                    unsigned* __restrict__ counter) {
-    const PPFrame F = pp_frame(P);
+    const float dz = P.tipC[3];
     int m = 0, k = 0;
     bool have = next_batch_pixel(counter, n_slots, mols, n_mol, th_log2, m, k);
-    GridView G;
+    AxisView G;
     long long sbase = 0;
     int nzs = 0, pix = 0;
     V3 tip, pos, v;
@@ -393,13 +431,13 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     int iz = 0, it = 0, total_it = 0;
     auto start = [&]() {
         const spm_batch_mol* D = mols + m;
-        G = slab_view(*D, grid);
+        G = axis_view(D, grid);
         nzs = D->nz_steps;
         pix = D->pix_off + k;
         sbase = D->state_off + (long long)k * nzs;
         const float4 p4 = pts[pix];
         tip = mk3(p4.x, p4.y, p4.z);
-        pos = add3(tip, F.d0r);
+        pos = mk3(tip.x + P.dpos0[0], tip.y + P.dpos0[1], tip.z + P.dpos0[2]);
         I.dt = P.relax_params[0];
         I.damp = P.relax_params[1];
         I.dtmax = I.dt;
@@ -414,13 +452,16 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     if (have) start();
     while (have) {
         bool conv;
-        if (pp_iter<unsigned, true>(G, F, tip, pos, v, I, fe, it, total_it, conv)) {
+        if (pp_iter_z<unsigned>(G, P, tip, pos, v, I, fe, it, total_it, conv)) {
+            if (!conv) fe = interp_fe_axis<unsigned, true>(G, pos);  // the position moved after the last sample
             const long long o = sbase + iz;
-            pp_emit<unsigned, true>(G, F, pos, fe, it, conv, FEs + o, PPs + o);
-            tip = add3(tip, F.dTip);
-            pos = add3(pos, F.dTip);
+            FEs[o] = fe;
+            const bool finite = isfinite(fe.x) && isfinite(fe.y) && isfinite(fe.z) && isfinite(fe.w) &&
+                                isfinite(pos.x) && isfinite(pos.y) && isfinite(pos.z);
+            PPs[o] = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
+            tip.z = __fadd_rn(tip.z, dz);
+            pos.z = __fadd_rn(pos.z, dz);
             v = mk3(0.f, 0.f, 0.f);
-            fe = make_float4(0.f, 0.f, 0.f, 0.f);
             it = 0;
             if (++iz == nzs) {
                 if (iter_count) iter_count[pix] = total_it;
@@ -448,16 +489,21 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
                 (reinterpret_cast<uintptr_t>(workspace) & 3u) == 0 && (reinterpret_cast<uintptr_t>(mols) & 7u) == 0,
                 "spm_batch_relax: misaligned buffers");
     SPM_REQUIRE((p->flags & ~(SPM_FLAG_FIRE | SPM_FLAG_FLIP_Z)) == 0, "spm_batch_relax: unknown flags 0x%x", p->flags);
+    if (!(p->tipA[0] == 1.f && p->tipA[1] == 0.f && p->tipA[2] == 0.f && p->tipB[0] == 0.f && p->tipB[1] == 1.f &&
+          p->tipB[2] == 0.f && p->tipC[0] == 0.f && p->tipC[1] == 0.f && p->tipC[2] == 1.f))
+        return set_error(SPM_ERR_UNSUPPORTED, "spm_batch_relax: batches scan z-strokes: tipA,tipB,tipC must be x,y,z");
     const int thr = shape->rx_threads, h = shape->rx_tile_h;
     SPM_REQUIRE(thr == 64 || thr == 128 || thr == 256, "spm_batch_relax: rx_threads=%d", thr);
     SPM_REQUIRE(h >= 1 && h <= 32 && (h & (h - 1)) == 0, "spm_batch_relax: rx_tile_h=%d", h);
     SPM_REQUIRE(shape->rx_ctas_per_sm >= 0, "spm_batch_relax: rx_ctas_per_sm=%d", shape->rx_ctas_per_sm);
     int th_log2 = 0;
     while ((1 << th_log2) < h) th_log2++;
+    SPM_REQUIRE(shape->rx_regs == 0 || shape->rx_regs == 1, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
+    auto kern = shape->rx_regs ? batch_relax_kernel<4> : batch_relax_kernel<3>;
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_relax_kernel, thr, 0) != cudaSuccess)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, thr, 0) != cudaSuccess)
         return set_error(SPM_ERR_CUDA, "spm_batch_relax: cannot query the device occupancy");
     if (per_sm < 1) per_sm = 1;
     if (shape->rx_ctas_per_sm > 0 && shape->rx_ctas_per_sm < per_sm) per_sm = shape->rx_ctas_per_sm;
@@ -468,7 +514,7 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     unsigned* ctr = static_cast<unsigned*>(workspace);
     if (cudaMemsetAsync(ctr, 0, sizeof(unsigned), st) != cudaSuccess)
         return set_error(SPM_ERR_CUDA, "spm_batch_relax: cannot reset the slot counter");
-    batch_relax_kernel<<<blocks, thr, 0, st>>>(n_mol, mols, (unsigned)n_slots, th_log2, grid,
+    kern<<<blocks, thr, 0, st>>>(n_mol, mols, (unsigned)n_slots, th_log2, grid,
                                                reinterpret_cast<const float4*>(points), *p,
                                                reinterpret_cast<float4*>(FEs), reinterpret_cast<float4*>(PPs),
                                                iter_count, ctr);

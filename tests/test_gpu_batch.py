@@ -85,8 +85,8 @@ def test_batch_loss_and_adjoint_match_per_molecule(cuda, kind):
         p0, dA, dB, dC = spec.vectors()
         grad, dks = gpu.adjoint_grid_params(kind, it.atoms.astype(np.float32), it.params.astype(np.float32), p0, dA,
                                             dB, dC, spec.tipQs, spec.tipQZs, grid, P, PPs, ubar, dk)
-        # node-major sums (batch) vs state-major sums (per molecule): equal up to summation order
-        torch.testing.assert_close(b.grad_of(i), grad, rtol=1e-5, atol=1e-7 * float(grad.abs().max()))
+        # node-major (MUFU rsqrt, FP32 pair terms) vs state-major (IEEE, FP64 per pair) sums
+        torch.testing.assert_close(b.grad_of(i), grad, rtol=1e-4, atol=1e-5 * float(grad.abs().max()))
         dk_total += dks
     torch.testing.assert_close(b.dk_sum, dk_total, rtol=1e-9, atol=1e-14)
 
@@ -108,7 +108,7 @@ def test_batch_shapes_give_same_results(cuda):
         torch.cuda.synchronize()
         assert torch.equal(b.grid, ref.grid) and torch.equal(b.FEs, ref.FEs) and torch.equal(b.PPs, ref.PPs)
         assert torch.equal(b.loss, ref.loss) and torch.equal(b.ubar, ref.ubar)
-        torch.testing.assert_close(b.grad, ref.grad, rtol=1e-10, atol=1e-13)
+        torch.testing.assert_close(b.grad, ref.grad, rtol=1e-6, atol=1e-9 * float(ref.grad.abs().max()))
 
 
 def test_batch_graph_replay(cuda):
@@ -148,3 +148,16 @@ def test_batch_adam_reduces_loss(cuda):
     torch.cuda.synchronize()
     assert torch.isfinite(b.loss).all()
     assert float(b.loss.sum()) < float(loss0.sum())
+
+
+def test_autotune_returns_valid_shape(cuda):
+    from spammm_b200 import autotune
+    items = _items(0, n=5, seed=71)
+    shape, report = autotune.tuned_shape(items, max_molecules=3, reps=1)
+    assert set(report) == {"grid", "relax", "adjoint"}
+    ref = AFMBatch(items)
+    ref.forward()
+    b = AFMBatch(items, shape=shape)
+    b.forward()
+    torch.cuda.synchronize()
+    assert torch.equal(ref.FEs, b.FEs) and torch.equal(ref.PPs, b.PPs)
