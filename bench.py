@@ -44,6 +44,11 @@ def parse():
     ap.add_argument("--config", default="plain_large", choices=["plain_large", "plain_small"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the many-molecule workloads")
+    ap.add_argument("--batch-mols", type=int, default=512)
+    ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--fit-mols", type=int, default=64)
+    ap.add_argument("--fit-steps", type=int, default=100)
     return ap.parse_args()
 
 
@@ -357,12 +362,161 @@ def run_ours(args, rank, world, local_rank):
             "roofline": roof, "gpu_launches": 3 * args.steps, "clocks": clk, "e2e": e2e}
     line.update(out)
     line["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
+    if not args.no_batch and world == 1:
+        line["batched"] = run_batched(args, local_rank)
     if not args.no_cpu and world == 1:
         v, det = cpu_sample(cfg)
         det["value"] = v
         det["unit"] = UNIT
         line["cpu_baseline"] = det
     return line
+
+
+# ---------------------------------------------------------------------------- batched path
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _replay_ms(graph, reps):
+    import torch
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(reps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _plain_images_per_s(items, probe):
+    """The per-image drop-in path (AFMulator: setup_grid_world, make_forcefield,
+    scan_fdbm, compute_df_amp_dir; numpy in/out) on every molecule of the
+    batch, one after another, wall clock."""
+    import torch
+    from spammm_b200 import AFM
+    from spammm_b200.AFM import AFMulator
+
+    def one(it):
+        afm = AFMulator(use_morse=False)
+        afm.n_relax_max, afm.f2conv = probe.max_iter, probe.f2conv
+        afm.tipQs, afm.tipQZs = probe.tipQs, probe.tipQZs
+        afm.atoms_arr = it.atoms.copy()
+        afm.cLJs_arr = it.params.copy()
+        afm.setup_grid_world(it.origin, np.array(it.ngrid) * it.step, it.ngrid)
+        afm.make_forcefield()
+        afm.setup_fdbm_grid_from_img(afm.img_FF, it.ngrid, it.origin, it.step)
+        hs = (it.z_top - 0.1 * np.arange(it.nz)[::-1]).astype(np.float32)
+        F, _ = afm.scan_fdbm(it.xs, it.ys, hs, mol_z=0.0, bond_length=0.0, stiffness=probe.stiffness,
+                             dpos0=probe.dpos0)
+        return AFM.compute_df_amp_dir(F, 0.1, (0., 0., 1.), 1.0)
+
+    one(items[0])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for it in items:
+        one(it)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    return {"images_per_s": len(items) / dt, "ms_per_image": dt / len(items) * 1e3, "molecules": len(items),
+            "path": "AFMulator.setup_grid_world/make_forcefield/scan_fdbm + compute_df_amp_dir per molecule "
+                    "(numpy in/out), the same molecules as the fit, wall clock"}
+
+
+def run_batched(args, dev_index):
+    """Many-molecule workloads: (3) forward images of a 512-molecule batch,
+    (4) 100 Adam steps of batched forward+adjoint fitting on 64 molecules."""
+    import torch
+    from spammm_b200 import autotune, synthetic
+    from spammm_b200.batch import AFMBatch, BatchAdam
+    out = {}
+    # ---- (4) fitting: target df from N(0,0.1 A)-perturbed positions; fit starts at the unperturbed structures
+    items = synthetic.batch_molecules(args.fit_mols, seed=5)
+    shape, tune_rep = autotune.tuned_shape(items, max_molecules=args.fit_mols, reps=1)
+    rng = np.random.default_rng(11)
+    pert = []
+    for it in items:
+        a = it.atoms.copy()
+        a[:, :3] += rng.normal(0.0, 0.1, (len(a), 3)).astype(np.float32)
+        pert.append(a)
+    b = AFMBatch(items, shape=shape)
+    for i, a in enumerate(pert):
+        b.set_atoms(i, a)
+    b.forward_adjoint()  # target 0: df_c is the perturbed structures' df
+    target = b.df_c.clone()
+    start = torch.as_tensor(b.plan.atoms, device=b.atoms.device)
+    truth = b.atoms.clone()
+    b.atoms.copy_(start)
+    b.set_target_states(target)
+    b.enable_failure_mask()
+    opt = BatchAdam(b, lr=0.01, cols=(0, 1, 2, 3))
+    g = b.capture(opt.step, warmup=0)
+    b.forward_adjoint()
+    loss0 = float(b.loss.sum())
+    b.atoms.copy_(start)
+    opt.reset()
+    b.enable_failure_mask()
+    clk = ClockSampler(dev_index)
+    clk.start()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(args.fit_steps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.fit_steps
+    b.forward_adjoint()
+    torch.cuda.synchronize()
+
+    def rmse(x, y):
+        return float(((x[:, :3] - y[:, :3]) ** 2).sum(1).mean().sqrt())
+    st = torch.bincount(b.diag[:, 3].long(), minlength=6).tolist()
+    out["fit"] = {
+        "workload": f"{args.fit_mols} molecules of the batch distribution, target df from N(0,0.1 A)-perturbed "
+                    f"positions, {args.fit_steps} Adam steps (lr 0.01) on positions and charges from the "
+                    "unperturbed structures, one CUDA-graph replay per step (forward + df loss + adjoint + update)",
+        "ms_per_step": ms, "images_per_s": args.fit_mols / (ms * 1e-3), "states_per_step": b.total_states,
+        "loss_start": loss0, "loss_final": float(b.loss.sum()),
+        "rmse_vs_unperturbed_A": rmse(b.atoms, start), "rmse_vs_target_structure_A": rmse(b.atoms, truth),
+        "rmse_start_vs_target_structure_A": rmse(start, truth), "adjoint_status_counts": st,
+        "shape": dict(zip([f for f, _ in type(shape)._fields_], shape.key())), "autotune": tune_rep,
+        "clocks": clocks}
+    sr = {}
+    for name, fn in (("grid", b.build_grids), ("relax", b.relax), ("loss", b.loss_seed),
+                     ("adjoint_state", b.adjoint_state), ("adjoint_params", b.adjoint_params)):
+        e0, e1 = _events()
+        fn()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        sr[name] = e0.elapsed_time(e1)
+    out["fit"]["stage_ms"] = sr
+    out["plain_per_image"] = _plain_images_per_s(items, b.probe)
+    out["fit"]["vs_plain_per_image"] = out["fit"]["images_per_s"] / out["plain_per_image"]["images_per_s"]
+    del g, b, opt
+    torch.cuda.empty_cache()
+    # ---- (3) forward images of a large batch in one graph
+    items = synthetic.batch_molecules(args.batch_mols, seed=3)
+    b = AFMBatch(items, shape=shape)
+    gf = b.capture(lambda: b.forward(amp=1.0))
+    clk = ClockSampler(dev_index)
+    clk.start()
+    ms = _replay_ms(gf, args.batch_steps)
+    clocks = clk.stop()
+    out["forward"] = {
+        "workload": f"{args.batch_mols} molecules: U{{10..120}} atoms, grids 12-32 A per side at 0.1 A (slabs "
+                    f"of the reachable z-layers built), 64^2-256^2 px, 30-60 z-steps; grid slabs + relaxation + "
+                    "df in one CUDA graph",
+        "ms_per_step": ms, "images_per_s": args.batch_mols / (ms * 1e-3), "states": b.total_states,
+        "px_z_per_s": b.total_states / (ms * 1e-3), "slab_gb": b.grid_float4 * 16 / 1e9,
+        "iters_per_state": float(b.iter_count.double().sum()) / b.total_states,
+        "converged_frac": float((b.PPs[:, 3] > 0).float().mean()), "clocks": clocks,
+        "gpu_launches_per_step": 3}
+    del gf, b
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_reference(args, rank, world):

@@ -211,17 +211,10 @@ class AFMBatch:
         self.df = torch.empty((so,), dtype=F32, device=dev)
         self.workspace = torch.zeros((max(1, int(lib().spm_relax_workspace_bytes()) // 4),), dtype=torch.int32,
                                      device=dev)
-        # loss / adjoint buffers
-        self.target = torch.zeros((so,), dtype=F64, device=dev)
-        self.weights = None
-        self.df_c = torch.empty((so,), dtype=F64, device=dev)
-        self.dL = torch.empty((so, 4), dtype=F32, device=dev)
+        # loss / adjoint buffers: allocated by the first loss or adjoint call
+        self.target = self.weights = self.df_c = self.dL = self.ubar = self.dk = self.diag = None
+        self.grad = self.dk_sum = None
         self.loss = torch.empty((self.n,), dtype=F64, device=dev)
-        self.ubar = torch.empty((so, 4), dtype=F32, device=dev)
-        self.dk = torch.empty((so, 4), dtype=F32, device=dev)
-        self.diag = torch.empty((so, 4), dtype=F32, device=dev)
-        self.grad = torch.empty((ao, 6), dtype=F64, device=dev)
-        self.dk_sum = torch.empty((4,), dtype=F64, device=dev)
         self._Qs = hostvec(self.probe.tipQs)
         self._QZs = hostvec(self.probe.tipQZs)
         self.scan_params = _lib.make_scan_params(tipC=[0, 0, 1, self.dtip], stiffness=self.probe.stiffness,
@@ -269,19 +262,39 @@ class AFMBatch:
                                     float(amp), ptr(self.df), stream_ptr())
         check(rc, "spm_batch_df_amp")
 
+    def _ensure_loss_buffers(self):
+        if self.target is None:
+            so, dev = self.total_states, self.dev
+            self.target = torch.zeros((so,), dtype=F64, device=dev)
+            self.df_c = torch.empty((so,), dtype=F64, device=dev)
+            self.dL = torch.empty((so, 4), dtype=F32, device=dev)
+
+    def _ensure_adjoint_buffers(self):
+        self._ensure_loss_buffers()
+        if self.ubar is None:
+            so, dev = self.total_states, self.dev
+            self.ubar = torch.empty((so, 4), dtype=F32, device=dev)
+            self.dk = torch.empty((so, 4), dtype=F32, device=dev)
+            self.diag = torch.empty((so, 4), dtype=F32, device=dev)
+            self.grad = torch.empty((self.total_atoms, 6), dtype=F64, device=dev)
+            self.dk_sum = torch.empty((4,), dtype=F64, device=dev)
+
     def loss_seed(self):
+        self._ensure_loss_buffers()
         rc = lib().spm_batch_df_loss_seed(self.n, ptr(self.mols_d), self.n_chunks, ptr(self.FEs), ptr(self.target),
                                           ptr(self.weights), self.dtip, ptr(self.df_c), ptr(self.dL), ptr(self.loss),
                                           ptr(self.loss_scratch), stream_ptr())
         check(rc, "spm_batch_df_loss_seed")
 
     def adjoint_state(self):
+        self._ensure_adjoint_buffers()
         rc = lib().spm_batch_adjoint_state(self.n, ptr(self.mols_d), self.total_states, ptr(self.grid),
                                            ptr(self.points), ctypes.byref(self.scan_params), ptr(self.PPs),
                                            ptr(self.dL), ptr(self.ubar), ptr(self.dk), ptr(self.diag), stream_ptr())
         check(rc, "spm_batch_adjoint_state")
 
     def adjoint_params(self):
+        self._ensure_adjoint_buffers()
         if self.adj_scratch is None:
             self.adj_scratch = torch.empty(((self._adj_bytes + 15) // 16, 2), dtype=F64, device=self.dev)
         rc = lib().spm_batch_adjoint_params(self.kind, self.n, ptr(self.mols_d), self.plan.totals,
@@ -317,7 +330,11 @@ class AFMBatch:
         -- where the probe flips --, singular, capped) and their z-neighbours,
         whose central-difference df sees them, get weight 0 in the next call's
         loss.  Their gradient is zero already; without the mask their share of
-        the loss would move in ways the gradient cannot see."""
+        the loss would move in ways the gradient cannot see.  Calling it again
+        clears the mask in place (captured graphs keep their buffers)."""
+        if self._mask_failed:
+            self.weights.copy_(self.w_base)
+            return
         w = np.ones(self.total_states, np.float64)
         for i in range(self.n):
             D = self.mols[i]
@@ -325,6 +342,7 @@ class AFMBatch:
                 v = w[D.state_off:D.state_off + D.n_scan * D.nz_steps].reshape(D.n_scan, D.nz_steps)
                 v[:, 0] = 0.0
                 v[:, -1] = 0.0
+        self._ensure_adjoint_buffers()
         self.w_base = torch.as_tensor(w, device=self.dev)
         self.weights = self.w_base.clone()
         self._mask_failed = True
@@ -380,8 +398,14 @@ class AFMBatch:
         a, b = self._rows(i, "atom")
         self.atoms[a:b].copy_(torch.as_tensor(np.asarray(atoms, np.float32).reshape(-1, 4), device=self.dev))
 
+    def set_target_states(self, t):
+        """Target df of every state at once ((total_states,) in the batch's state order)."""
+        self._ensure_loss_buffers()
+        self.target.copy_(t.reshape(-1).to(F64))
+
     def set_target(self, i, df_target):
         """Target df (nx_r, ny_r, nz) of molecule i for the loss."""
+        self._ensure_loss_buffers()
         a, b = self._rows(i, "state")
         self.target[a:b].copy_(torch.as_tensor(np.asarray(df_target, np.float64).ravel(), device=self.dev)
                                if not isinstance(df_target, torch.Tensor) else df_target.reshape(-1).to(F64))

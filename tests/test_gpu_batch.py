@@ -103,7 +103,7 @@ def test_batch_shapes_give_same_results(cuda):
         for k, v in kw.items():
             setattr(s, k, v)
         b = AFMBatch(items, shape=s)
-        b.target.copy_(ref.target)
+        b.set_target_states(ref.target)
         b.forward_adjoint()
         torch.cuda.synchronize()
         assert torch.equal(b.grid, ref.grid) and torch.equal(b.FEs, ref.FEs) and torch.equal(b.PPs, ref.PPs)
@@ -132,7 +132,7 @@ def test_batch_adam_reduces_loss(cuda):
     truth = AFMBatch(items)
     truth.forward_adjoint()  # target 0: df_c is the df image of the true structures
     b = AFMBatch(items)
-    b.target.copy_(truth.df_c)
+    b.set_target_states(truth.df_c)
     rng = np.random.default_rng(2)
     for i, it in enumerate(items):
         a = it.atoms.copy()
