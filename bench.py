@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=3)
     ap.add_argument("--fit-mols", type=int, default=64)
     ap.add_argument("--fit-steps", type=int, default=100)
+    ap.add_argument("--batch-only", action="store_true",
+                    help="run only the many-molecule workloads (small sizes make profiling cases)")
+    ap.add_argument("--no-tune", action="store_true", help="library default launch shapes, no autotuning")
     return ap.parse_args()
 
 
@@ -432,7 +435,11 @@ def run_batched(args, dev_index):
     out = {}
     # ---- (4) fitting: target df from N(0,0.1 A)-perturbed positions; fit starts at the unperturbed structures
     items = synthetic.batch_molecules(args.fit_mols, seed=5)
-    shape, tune_rep = autotune.tuned_shape(items, max_molecules=args.fit_mols, reps=1)
+    if args.no_tune:
+        from spammm_b200 import _lib
+        shape, tune_rep = _lib.lib().spm_batch_default_shape(), None
+    else:
+        shape, tune_rep = autotune.tuned_shape(items, max_molecules=args.fit_mols, reps=1)
     rng = np.random.default_rng(11)
     pert = []
     for it in items:
@@ -551,6 +558,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         line = run_reference(args, rank, world)
+    elif args.batch_only:
+        line = None
+        if rank == 0:
+            line = {"metric": "batched fwd+adjoint images/s", "batched": run_batched(args, local_rank)}
     else:
         if world > 1:
             import datetime

@@ -293,7 +293,10 @@ long long spm_adjoint_grid_scratch_bytes(int n_atoms, long long n_state);
  * caller; launches take the DEVICE copy.  Layouts:
  *   atoms  (total_atoms,4) x,y,z,Q;  params (total_atoms,2) LJ c6,c12 or
  *          (total_atoms,4) Morse R0,E0,K,-
- *   grid   float4 slabs, (nz_slab,ny,nx) each, at grid_off
+ *   grid   x-paired float4 slabs: node idx = ((z - z_lo)*ny + y)*nx + x of a
+ *          molecule holds 2 float4 at grid[2*(grid_off + idx)]: (value(x,y,z),
+ *          value((x+1) mod nx, y, z)), so a trilinear cell row is one 32-byte
+ *          load; the buffer holds 2*totals[7] float4
  *   points (total_pixels,4) tip start positions (raster ix-major when
  *          raster_ny > 0, as spm_relax_ex)
  *   states (total_states,4) per molecule n_scan x nz_steps, z-step fastest */
@@ -338,7 +341,8 @@ spm_batch_shape spm_batch_default_shape(void);
 int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch_shape* shape, long long* totals_out);
 
 /* Force-grid slabs of every molecule (pair laws, tip sites and the |E|>100
- * cap as spm_grid_build).  n_tiles = totals_out[0]. */
+ * cap as spm_grid_build), written in the x-paired layout.
+ * n_tiles = totals_out[0]. */
 int spm_batch_grid_build(int kind, int n_mol, const spm_batch_mol* mols, long long n_tiles,
                          const spm_batch_shape* shape, const float* atoms, const float* params,
                          const float* Qs, const float* QZs, float* grid, void* stream);

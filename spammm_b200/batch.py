@@ -204,7 +204,7 @@ class AFMBatch:
         self.atoms = torch.as_tensor(plan.atoms, device=dev).contiguous()
         self.params = torch.as_tensor(plan.params, device=dev).contiguous()
         self.points = torch.as_tensor(plan.points, device=dev).contiguous()
-        self.grid = torch.empty((go, 4), dtype=F32, device=dev)
+        self.grid = torch.empty((2 * go, 4), dtype=F32, device=dev)  # x-paired slabs: 2 float4 per node
         self.FEs = torch.empty((so, 4), dtype=F32, device=dev)
         self.PPs = torch.empty((so, 4), dtype=F32, device=dev)
         self.iter_count = torch.empty((po,), dtype=torch.int32, device=dev)
@@ -360,6 +360,13 @@ class AFMBatch:
         if what == "pixel":
             return D.pix_off, D.pix_off + D.n_scan
         return D.atom_off, D.atom_off + D.n_atoms
+
+    def slab(self, i):
+        """(nz_slab, ny, nx, 4) view of molecule i's stored layers (the x-paired
+        buffer's first halves; layer 0 is the full grid's layer z_lo)."""
+        D = self.desc(i)
+        n = D.nx * D.ny * D.nz_slab
+        return self.grid.view(-1, 2, 4)[D.grid_off:D.grid_off + n, 0].reshape(D.nz_slab, D.ny, D.nx, 4)
 
     def fes(self, i):
         a, b = self._rows(i, "state")

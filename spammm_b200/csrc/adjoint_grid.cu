@@ -72,11 +72,13 @@ __device__ __forceinline__ Corners corners_of(const GridView& G, V3 p) {
     return C;
 }
 
-// Stored node (x, y, z) of a full grid or a slab (z is the full grid's layer).
+// Stored node (x, y, z) of a full grid or of a batch slab (z is the full
+// grid's layer; batch slabs are x-paired: node idx at G.g[2*idx]).
 template <bool SLAB>
 __device__ __forceinline__ float4 node_at(const GridView& G, int x, int y, int z) {
     const int zl = SLAB ? z - G.z_lo : z;
-    return __ldg(G.g + ((size_t)zl * G.ny + y) * G.nx + x);
+    const size_t idx = ((size_t)zl * G.ny + y) * G.nx + x;
+    return __ldg(G.g + (SLAB ? 2 * idx : idx));
 }
 
 struct Sites {
@@ -459,34 +461,79 @@ batch_ubar_max_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const f
 }
 
 // Thread per state: w * ubar onto the eight corner nodes (exact integer sums).
+// Consecutive lanes are consecutive z-steps of a stroke; when lane l+1's cell
+// sits one layer below lane l's in the same (x,y) cell, lane l+1's upper
+// layer is lane l's lower layer: lane l adds those four corners' sums to its
+// own (integers: exact) and lane l+1 skips them, halving the atomics of a
+// stroke.
 __global__ void __launch_bounds__(256)
 batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states,
                      const float4* __restrict__ PPs, const float4* __restrict__ ubar, const unsigned* __restrict__ umax,
                      unsigned long long* __restrict__ gq) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     const long long st = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (st >= n_states) return;
-    const float4 ub = __ldg(ubar + st);
-    if (ub.x == 0.f && ub.y == 0.f && ub.z == 0.f && ub.w == 0.f) return;
-    const int m = SPM_MOL_BY(state_off, mols, n_mol, st);
-    const spm_batch_mol* D = mols + m;
-    GridView G = slab_view(*D, nullptr);
-    const float4 pp = __ldg(PPs + st);
-    const Corners C = corners_of<true>(G, mk3(pp.x, pp.y, pp.z));
-    if (!C.ok) return;
-    const double scale = pow2(42 - scale_exp(__ldg(umax + m)));
-    unsigned long long* base = gq + (size_t)D->grid_off * 4;
-    for (int k = 0; k < 2; k++)
-        for (int j = 0; j < 2; j++)
-            for (int i = 0; i < 2; i++) {
-                const float w = (i ? C.ax : 1.f - C.ax) * (j ? C.ay : 1.f - C.ay) * (k ? C.az : 1.f - C.az);
-                if (w == 0.f) continue;
-                const size_t node = ((size_t)(C.z[k] - G.z_lo) * G.ny + C.y[j]) * G.nx + C.x[i];
-                unsigned long long* q = base + node * 4;
-                atomicAdd(q + 0, (unsigned long long)__double2ll_rn((double)(w * ub.x) * scale));
-                atomicAdd(q + 1, (unsigned long long)__double2ll_rn((double)(w * ub.y) * scale));
-                atomicAdd(q + 2, (unsigned long long)__double2ll_rn((double)(w * ub.z) * scale));
-                atomicAdd(q + 3, (unsigned long long)__double2ll_rn((double)(w * ub.w) * scale));
+    float4 ub = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (st < n_states) ub = __ldg(ubar + st);
+    bool valid = !(ub.x == 0.f && ub.y == 0.f && ub.z == 0.f && ub.w == 0.f);
+    Corners C = {{0, 0}, {0, 0}, {0, 0}, 0.f, 0.f, 0.f, false};
+    long long stroke = -1;
+    int nx = 0, ny = 0, z_lo = 0;
+    unsigned long long* base = gq;
+    double scale = 0.0;
+    if (valid) {
+        const int m = SPM_MOL_BY(state_off, mols, n_mol, st);
+        const spm_batch_mol* D = mols + m;
+        const GridView G = slab_view(*D, nullptr);
+        const float4 pp = __ldg(PPs + st);
+        C = corners_of<true>(G, mk3(pp.x, pp.y, pp.z));
+        valid = C.ok;
+        stroke = D->pix_off + (st - D->state_off) / D->nz_steps;
+        nx = G.nx; ny = G.ny; z_lo = G.z_lo;
+        base = gq + (size_t)D->grid_off * 4;
+        scale = pow2(42 - scale_exp(__ldg(umax + m)));
+    }
+    // merge tests against the next lane (it gives me its upper layer) and the previous one (I give mine)
+    const bool nb_valid = __shfl_down_sync(FULL, valid, 1);
+    const long long nb_stroke = __shfl_down_sync(FULL, stroke, 1);
+    const int nb_x0 = __shfl_down_sync(FULL, C.x[0], 1), nb_y0 = __shfl_down_sync(FULL, C.y[0], 1);
+    const int nb_z1 = __shfl_down_sync(FULL, C.z[1], 1);
+    const bool take = valid && lane < 31 && nb_valid && nb_stroke == stroke && nb_x0 == C.x[0] && nb_y0 == C.y[0] &&
+                      nb_z1 == C.z[0];
+    const bool pv_valid = __shfl_up_sync(FULL, valid, 1);
+    const long long pv_stroke = __shfl_up_sync(FULL, stroke, 1);
+    const int pv_x0 = __shfl_up_sync(FULL, C.x[0], 1), pv_y0 = __shfl_up_sync(FULL, C.y[0], 1);
+    const int pv_z0 = __shfl_up_sync(FULL, C.z[0], 1);
+    const bool given = valid && lane > 0 && pv_valid && pv_stroke == stroke && pv_x0 == C.x[0] && pv_y0 == C.y[0] &&
+                       C.z[1] == pv_z0;
+    float w[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
+        w[c] = valid ? (i ? C.ax : 1.f - C.ax) * (j ? C.ay : 1.f - C.ay) * (k ? C.az : 1.f - C.az) : 0.f;
+    }
+    const float ubc[4] = {ub.x, ub.y, ub.z, ub.w};
+#pragma unroll
+    for (int ch = 0; ch < 4; ch++) {
+        long long q[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) q[c] = (w[c] == 0.f) ? 0ll : __double2ll_rn((double)(w[c] * ubc[ch]) * scale);
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const long long up = __shfl_down_sync(FULL, q[4 + c], 1);
+            if (take) q[c] += up;
+        }
+        if (valid) {
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                if (c >= 4 && given) continue;
+                if (q[c] == 0) continue;
+                const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
+                const size_t node = ((size_t)(C.z[k] - z_lo) * ny + C.y[j]) * nx + C.x[i];
+                atomicAdd(base + node * 4 + ch, (unsigned long long)q[c]);
             }
+        }
+    }
 }
 
 constexpr int NM_THREADS = 256;

@@ -73,10 +73,13 @@ __device__ __forceinline__ float node_xy(float p0, float da, float db, int ia, i
 
 // One CTA tile: a (blockDim.x x blockDim.y) patch of z-columns, ZB nodes each
 // starting at global layer ic0; nodes at layers >= zst_hi are not stored, the
-// rest go to out[((ic - zst_lo)*ny + ib)*nx + ia].
+// rest go to out[idx], idx = ((ic - zst_lo)*ny + ib)*nx + ia.  PAIRED: the
+// x-paired layout, 2 float4 per node: node idx's value is written to
+// out[2*idx] and to out[2*idx_left + 1], idx_left its (x-1 mod nx) neighbour,
+// so out[2*idx .. 2*idx+1] = (value(x), value(x+1 mod nx)).
 // KIND: SPM_KIND_LJ / SPM_KIND_MORSE; ON: an on-node charge term exists;
 // NOFF: number of off-node sites.
-template <int KIND, bool ON, int NOFF, int ZB>
+template <int KIND, bool ON, int NOFF, int ZB, bool PAIRED = false>
 __device__ __forceinline__ void build_tile(int na, const float4* __restrict__ atoms, const float* __restrict__ params,
                                            int pstride, float4* __restrict__ out, const GridGeom& G,
                                            const TipSites& S, int ia, int ib, int ic0, int zst_lo, int zst_hi) {
@@ -196,7 +199,13 @@ __device__ __forceinline__ void build_tile(int na, const float4* __restrict__ at
             // |E| > 100 cap of the reference builders (AFM.cl:1053-1054)
             const float renorm = __fdiv_rn(100.f, fabsf(o.w));
             if (renorm < 1.f) { o.x *= renorm; o.y *= renorm; o.z *= renorm; o.w *= renorm; }
-            out[((size_t)(ic - zst_lo) * G.ny + ib) * G.nx + ia] = o;
+            const size_t row = ((size_t)(ic - zst_lo) * G.ny + ib) * G.nx;
+            if (PAIRED) {
+                out[2 * (row + ia)] = o;
+                out[2 * (row + (ia > 0 ? ia - 1 : G.nx - 1)) + 1] = o;
+            } else {
+                out[row + ia] = o;
+            }
         }
     }
 }
@@ -273,7 +282,8 @@ batch_grid_build_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const
     G.dB = ld4f(D->dB);
     G.dC = ld4f(D->dC);
     const int ao = D->atom_off;
-    build_tile<KIND, ON, NOFF, ZB>(D->n_atoms, atoms + ao, params + (size_t)ao * pstride, pstride, grid + D->grid_off,
+    build_tile<KIND, ON, NOFF, ZB, true>(D->n_atoms, atoms + ao, params + (size_t)ao * pstride, pstride,
+                                         grid + 2 * D->grid_off,
                                    G, S, bx * GB_TX + threadIdx.x, by * ty + threadIdx.y, z_lo + (int)bz * ZB, z_lo,
                                    z_lo + nzs);
 }

@@ -382,12 +382,12 @@ __device__ __forceinline__ bool next_batch_pixel(unsigned* counter, unsigned n_s
 // zero aside) -- and c*surf reduced to its z part.
 template <typename IDX>
 __device__ __forceinline__ bool pp_iter_z(const AxisView& G, const spm_scan_params& P, V3 tip, V3& pos, V3& v,
-                                          Integrator& I, float4& fe, int& it, int& total_it, bool& conv) {
+                                          float& dt, float& damp, float4& fe, int& it, int& total_it, bool& conv) {
     conv = false;
     if (it >= P.max_iter) return true;
     ++it;
     ++total_it;
-    fe = interp_fe_axis<IDX, true>(G, pos);
+    fe = interp_fe_pair<IDX, true>(G, pos);
     if (fe.w != fe.w) return true;  // outside the slab (or a NaN grid): not converged
     const V3 ft = tip_force(sub3(pos, tip), ld4(P.stiffness), ld4(P.dpos0));
     V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
@@ -396,15 +396,18 @@ __device__ __forceinline__ bool pp_iter_z(const AxisView& G, const spm_scan_para
         conv = true;
         return true;
     }
-    md_step(f, v, pos, I, (P.flags & SPM_FLAG_FIRE) != 0);
+    // the stroke's integrator constants straight from the launch parameters (dtmin = dtmax * 0.1)
+    md_step_c(f, v, pos, dt, damp, __fmul_rn(P.relax_params[0], 0.1f), P.relax_params[0], P.relax_params[1],
+              (P.flags & SPM_FLAG_FIRE) != 0);
     return it >= P.max_iter;
 }
 
 __device__ __forceinline__ AxisView axis_view(const spm_batch_mol* D, const float* grid) {
     AxisView G;
-    G.g = reinterpret_cast<const float4*>(grid) + D->grid_off;
+    G.g = reinterpret_cast<const float4*>(grid) + 2 * D->grid_off;  // x-paired slab
     G.nx = D->nx; G.ny = D->ny; G.nz = D->nz;
     G.z_lo = D->z_lo; G.nz_slab = D->nz_slab;
+    G.fnx = (float)G.nx; G.fny = (float)G.ny; G.fnz = (float)G.nz;
     G.ax = D->dinvA[0]; G.aw = D->dinvA[3];
     G.by = D->dinvB[1]; G.bw = D->dinvB[3];
     G.cz = D->dinvC[2]; G.cw = D->dinvC[3];
@@ -426,7 +429,7 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     long long sbase = 0;
     int nzs = 0, pix = 0;
     V3 tip, pos, v;
-    Integrator I;
+    float dt = 0.f, damp = 0.f;
     float4 fe;
     int iz = 0, it = 0, total_it = 0;
     auto start = [&]() {
@@ -438,11 +441,8 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
         const float4 p4 = pts[pix];
         tip = mk3(p4.x, p4.y, p4.z);
         pos = mk3(tip.x + P.dpos0[0], tip.y + P.dpos0[1], tip.z + P.dpos0[2]);
-        I.dt = P.relax_params[0];
-        I.damp = P.relax_params[1];
-        I.dtmax = I.dt;
-        I.dtmin = __fmul_rn(I.dtmax, 0.1f);
-        I.damp0 = I.damp;
+        dt = P.relax_params[0];
+        damp = P.relax_params[1];
         v = mk3(0.f, 0.f, 0.f);
         fe = make_float4(0.f, 0.f, 0.f, 0.f);
         iz = 0;
@@ -452,12 +452,20 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     if (have) start();
     while (have) {
         bool conv;
-        if (pp_iter_z<unsigned>(G, P, tip, pos, v, I, fe, it, total_it, conv)) {
-            if (!conv) fe = interp_fe_axis<unsigned, true>(G, pos);  // the position moved after the last sample
+        if (pp_iter_z<unsigned>(G, P, tip, pos, v, dt, damp, fe, it, total_it, conv)) {
+            if (!conv) fe = interp_fe_pair<unsigned, true>(G, pos);  // the position moved after the last sample
             const long long o = sbase + iz;
             FEs[o] = fe;
-            const bool finite = isfinite(fe.x) && isfinite(fe.y) && isfinite(fe.z) && isfinite(fe.w) &&
-                                isfinite(pos.x) && isfinite(pos.y) && isfinite(pos.z);
+            // all seven values finite <=> the sum of their products with zero is zero
+            // (x*0 is NaN for x = +-inf or NaN, +-0 otherwise)
+            float z0 = __fmul_rn(fe.x, 0.f);
+            z0 = __fmaf_rn(fe.y, 0.f, z0);
+            z0 = __fmaf_rn(fe.z, 0.f, z0);
+            z0 = __fmaf_rn(fe.w, 0.f, z0);
+            z0 = __fmaf_rn(pos.x, 0.f, z0);
+            z0 = __fmaf_rn(pos.y, 0.f, z0);
+            z0 = __fmaf_rn(pos.z, 0.f, z0);
+            const bool finite = (z0 == 0.f);
             PPs[o] = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
             tip.z = __fadd_rn(tip.z, dz);
             pos.z = __fadd_rn(pos.z, dz);

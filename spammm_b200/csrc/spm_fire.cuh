@@ -51,42 +51,49 @@ struct Integrator {
 };
 
 // FIRE velocity mixing (Bitzek et al., PRL 97, 170201 (2006)) or plain damping,
-// followed by v += f*dt, pos += v*dt.
-__device__ __forceinline__ void md_step(V3 f, V3& v, V3& pos, Integrator& I, bool use_fire) {
+// followed by v += f*dt, pos += v*dt.  dt and damp evolve; dtmin, dtmax and
+// damp0 are the stroke's constants.
+__device__ __forceinline__ void md_step_c(V3 f, V3& v, V3& pos, float& dt, float& damp, float dtmin, float dtmax,
+                                          float damp0, bool use_fire) {
     if (use_fire) {
         float ff = dot3(f, f);
         float vv = dot3(v, v);
         float vf = dot3(v, f);
         if (vf < 0.f) {
             v.x = __fmul_rn(v.x, 0.f); v.y = __fmul_rn(v.y, 0.f); v.z = __fmul_rn(v.z, 0.f);
-            I.dt = fmaxf(I.dtmin, __fmul_rn(I.dt, 0.5f));
-            I.damp = I.damp0;
+            dt = fmaxf(dtmin, __fmul_rn(dt, 0.5f));
+            damp = damp0;
         } else {
-            float cf = __fmul_rn(I.damp, __fsqrt_rn(__fdiv_rn(vv, ff + 1e-8f)));
-            float cv = 1.f - I.damp;
+            float cf = __fmul_rn(damp, __fsqrt_rn(__fdiv_rn(vv, ff + 1e-8f)));
+            float cv = 1.f - damp;
             v.x = __fmaf_rn(f.x, cf, __fmul_rn(v.x, cv));
             v.y = __fmaf_rn(f.y, cf, __fmul_rn(v.y, cv));
             v.z = __fmaf_rn(f.z, cf, __fmul_rn(v.z, cv));
-            I.dt = fminf(I.dtmax, __fmul_rn(I.dt, 1.1f));
-            I.damp = __fmul_rn(I.damp, 0.99f);
+            dt = fminf(dtmax, __fmul_rn(dt, 1.1f));
+            damp = __fmul_rn(damp, 0.99f);
         }
     } else {
-        float cv = 1.f - I.damp;
+        float cv = 1.f - damp;
         v.x = __fmul_rn(v.x, cv); v.y = __fmul_rn(v.y, cv); v.z = __fmul_rn(v.z, cv);
     }
-    v.x = __fmaf_rn(f.x, I.dt, v.x);
-    v.y = __fmaf_rn(f.y, I.dt, v.y);
-    v.z = __fmaf_rn(f.z, I.dt, v.z);
-    pos.x = __fmaf_rn(v.x, I.dt, pos.x);
-    pos.y = __fmaf_rn(v.y, I.dt, pos.y);
-    pos.z = __fmaf_rn(v.z, I.dt, pos.z);
+    v.x = __fmaf_rn(f.x, dt, v.x);
+    v.y = __fmaf_rn(f.y, dt, v.y);
+    v.z = __fmaf_rn(f.z, dt, v.z);
+    pos.x = __fmaf_rn(v.x, dt, pos.x);
+    pos.y = __fmaf_rn(v.y, dt, pos.y);
+    pos.z = __fmaf_rn(v.z, dt, pos.z);
 }
 
-// REPEAT addressing + linear filter along one axis (OpenCL 1.2 sec. 8.2).
-__device__ __forceinline__ bool tex_axis(float u, int n, int& i0, int& i1, float& a) {
+__device__ __forceinline__ void md_step(V3 f, V3& v, V3& pos, Integrator& I, bool use_fire) {
+    md_step_c(f, v, pos, I.dt, I.damp, I.dtmin, I.dtmax, I.damp0, use_fire);
+}
+
+// REPEAT addressing + linear filter along one axis (OpenCL 1.2 sec. 8.2);
+// fn = (float)n.
+__device__ __forceinline__ bool tex_axis(float u, int n, float fn, int& i0, int& i1, float& a) {
     float s = u - floorf(u);
-    float t = __fmaf_rn(s, (float)n, -0.5f);
-    if (!(t >= -1.f && t < (float)n)) return false;
+    float t = __fmaf_rn(s, fn, -0.5f);
+    if (!(t >= -1.f && t < fn)) return false;
     float fi = floorf(t);
     a = t - fi;
     int i = (int)fi;
@@ -96,6 +103,9 @@ __device__ __forceinline__ bool tex_axis(float u, int n, int& i0, int& i1, float
     i0 = i;
     i1 = j;
     return true;
+}
+__device__ __forceinline__ bool tex_axis(float u, int n, int& i0, int& i1, float& a) {
+    return tex_axis(u, n, (float)n, i0, i1, a);
 }
 
 __device__ __forceinline__ float lerp_c(float a, float ma, float f0, float f1) {
@@ -161,6 +171,7 @@ __device__ __forceinline__ float4 interp_fe(const GridView& G, V3 p) {
 struct AxisView {
     const float4* __restrict__ g;
     int nx, ny, nz, z_lo, nz_slab;
+    float fnx, fny, fnz;  // the dimensions as floats (converted once per pixel, not per sample)
     float ax, aw, by, bw, cz, cw;
 };
 
@@ -179,9 +190,9 @@ __device__ __forceinline__ float4 interp_fe_axis(const AxisView& G, V3 p) {
     const float w = __fmaf_rn(p.z, G.cz, G.cw);
     int x0, x1, y0, y1, z0, z1;
     float ax, ay, az;
-    bool ok = tex_axis(u, G.nx, x0, x1, ax);
-    ok = tex_axis(v, G.ny, y0, y1, ay) && ok;
-    ok = tex_axis(w, G.nz, z0, z1, az) && ok;
+    bool ok = tex_axis(u, G.nx, G.fnx, x0, x1, ax);
+    ok = tex_axis(v, G.ny, G.fny, y0, y1, ay) && ok;
+    ok = tex_axis(w, G.nz, G.fnz, z0, z1, az) && ok;
     if (SLAB) {
         z0 -= G.z_lo;
         z1 -= G.z_lo;
@@ -199,6 +210,60 @@ __device__ __forceinline__ float4 interp_fe_axis(const AxisView& G, V3 p) {
     const ulonglong2 f010 = __ldg(g + r10 + x0), f110 = __ldg(g + r10 + x1);
     const ulonglong2 f001 = __ldg(g + r01 + x0), f101 = __ldg(g + r01 + x1);
     const ulonglong2 f011 = __ldg(g + r11 + x0), f111 = __ldg(g + r11 + x1);
+    const ulonglong2 c00 = lerp_pk(AX, MX, f000, f100);
+    const ulonglong2 c10 = lerp_pk(AX, MX, f010, f110);
+    const ulonglong2 c01 = lerp_pk(AX, MX, f001, f101);
+    const ulonglong2 c11 = lerp_pk(AX, MX, f011, f111);
+    const ulonglong2 c0 = lerp_pk(AY, MY, c00, c10);
+    const ulonglong2 c1 = lerp_pk(AY, MY, c01, c11);
+    const ulonglong2 c = lerp_pk(AZ, MZ, c0, c1);
+    float4 r;
+    upk(c.x, r.x, r.y);
+    upk(c.y, r.z, r.w);
+    return r;
+}
+
+// 256-bit read-only load of an x-pair: (value(x), value(x+1)) as packed
+// channel pairs lo = {(Fx,Fy), (Fz,E)} of x and hi = the same of x+1.
+__device__ __forceinline__ void ld_pair(const float4* p, ulonglong2& lo, ulonglong2& hi) {
+    unsigned long long a, b, c, d;
+    asm("ld.global.nc.v4.b64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p));
+    lo = make_ulonglong2(a, b);
+    hi = make_ulonglong2(c, d);
+}
+
+// interp_fe_axis on an x-paired grid (G.g = the pair base: node idx at
+// G.g[2*idx], its +x neighbour (mod nx) at G.g[2*idx + 1]): one 256-bit load
+// per (y, z) row of the texel cell instead of two 128-bit loads; the same
+// operations on the same values, so the same sample.
+template <typename IDX, bool SLAB>
+__device__ __forceinline__ float4 interp_fe_pair(const AxisView& G, V3 p) {
+    const float u = __fmaf_rn(p.x, G.ax, G.aw);
+    const float v = __fmaf_rn(p.y, G.by, G.bw);
+    const float w = __fmaf_rn(p.z, G.cz, G.cw);
+    int x0, x1, y0, y1, z0, z1;
+    float ax, ay, az;
+    bool ok = tex_axis(u, G.nx, G.fnx, x0, x1, ax);
+    ok = tex_axis(v, G.ny, G.fny, y0, y1, ay) && ok;
+    ok = tex_axis(w, G.nz, G.fnz, z0, z1, az) && ok;
+    (void)x1;  // the pair holds it
+    if (SLAB) {
+        z0 -= G.z_lo;
+        z1 -= G.z_lo;
+        ok = ok && (unsigned)z0 < (unsigned)G.nz_slab && (unsigned)z1 < (unsigned)G.nz_slab;
+    }
+    if (!ok) {
+        float nan = __int_as_float(0x7fc00000);
+        return make_float4(nan, nan, nan, nan);
+    }
+    const f2 AX = bc(ax), MX = bc(1.f - ax), AY = bc(ay), MY = bc(1.f - ay), AZ = bc(az), MZ = bc(1.f - az);
+    const IDX r00 = ((IDX)z0 * G.ny + y0) * G.nx + x0, r10 = ((IDX)z0 * G.ny + y1) * G.nx + x0;
+    const IDX r01 = ((IDX)z1 * G.ny + y0) * G.nx + x0, r11 = ((IDX)z1 * G.ny + y1) * G.nx + x0;
+    ulonglong2 f000, f100, f010, f110, f001, f101, f011, f111;
+    ld_pair(G.g + 2 * r00, f000, f100);
+    ld_pair(G.g + 2 * r10, f010, f110);
+    ld_pair(G.g + 2 * r01, f001, f101);
+    ld_pair(G.g + 2 * r11, f011, f111);
     const ulonglong2 c00 = lerp_pk(AX, MX, f000, f100);
     const ulonglong2 c10 = lerp_pk(AX, MX, f010, f110);
     const ulonglong2 c01 = lerp_pk(AX, MX, f001, f101);

@@ -44,8 +44,11 @@ def test_batch_forward_matches_per_molecule(cuda, kind):
     for i, it in enumerate(b.items):
         spec, grid, P, pts, FEs, PPs = _per_molecule(b, i)
         D = b.desc(i)
-        slab = b.grid[D.grid_off:D.grid_off + D.nx * D.ny * D.nz_slab].view(D.nz_slab, D.ny, D.nx, 4)
-        assert torch.equal(slab, grid[D.z_lo:D.z_lo + D.nz_slab]), f"molecule {i}: slab differs from full grid"
+        full = grid[D.z_lo:D.z_lo + D.nz_slab]
+        assert torch.equal(b.slab(i), full), f"molecule {i}: slab differs from full grid"
+        n = D.nx * D.ny * D.nz_slab
+        hi = b.grid.view(-1, 2, 4)[D.grid_off:D.grid_off + n, 1].reshape(D.nz_slab, D.ny, D.nx, 4)
+        assert torch.equal(hi, torch.roll(full, -1, dims=2)), f"molecule {i}: x-pair halves differ"
         assert (b.pps(i)[..., 3] > 0).all(), f"molecule {i}: a stroke left the slab or did not converge"
         assert torch.equal(b.fes(i), FEs) and torch.equal(b.pps(i), PPs), f"molecule {i}: relaxation differs"
         # df of the stroke, ascending z (dr = |dtip|), as the single-volume call
