@@ -118,6 +118,15 @@ int spm_relax_strokes(const float* grid, int nx, int ny, int nz,
  * receiving PPs = (pos, +iters converged / -iters not).  The forward of the
  * differentiable grid path (spm_adjoint_grid_*). */
 #define SPM_RELAX_PP      2
+/* SPM_RELAX_2D: relaxStrokes2D (kernels/AFM.cl:410-450, AFMulator.scan_fdbm_2d
+ * spammm/SPM/AFM.py:644-704): per slice iz the probe z is fixed at
+ * point.z - iz*dh with dh = -p->dTip[2]; x,y start at the anchor and follow
+ * damped MD (v = v*(1-damp) + f*dt, p += v*dt, f = F_grid.xy - K_lat (p -
+ * anchor)) for at most max_iter steps, stopping after the update once
+ * |f|^2 < f2conv; FEs = the grid sample at the final position, disps =
+ * (dx, dy, 0, 0).  K_lat = p->stiffness[0] (> 0), (dt, damp) =
+ * p->relax_params[0..1]; SPM_FLAG_FLIP_Z honoured, the tip frame ignored. */
+#define SPM_RELAX_2D      3
 long long spm_relax_workspace_bytes(void);
 int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz,
                  const float* points, int n_scan, const spm_scan_params* p,
@@ -328,7 +337,9 @@ typedef struct spm_batch_shape {
     int rx_tile_h;      /* relaxation pixel tile: (32/rx_tile_h) x rx_tile_h pixels, power of two <= 32 */
     int rx_ctas_per_sm; /* persistent relaxation CTAs per SM, 0 = occupancy maximum */
     int adj_chunk;      /* slab nodes per adjoint unit: multiple of 1024 in [1024, 1048576] */
-    int rx_regs;        /* relaxation register budget: 0 = 80 per thread, 1 = 64 (more warps, some spills) */
+    int rx_regs;        /* relaxation kernel variant: 0 = 80 registers per thread, 1 = 64 (more warps,
+                           some spills), 2 = the cell's 8 texels kept in registers across FIRE
+                           iterations (112 registers, loads only when the cell changes) */
 } spm_batch_shape;
 
 spm_batch_shape spm_batch_default_shape(void);

@@ -21,6 +21,7 @@
  *   update_FIRE         kernels/AFM.cl:136-157 (FTDEC/FTINC/FDAMP/F2SAFE :124-132)
  *   relaxStrokes        kernels/AFM.cl:345-394
  *   relaxStrokesTilted  kernels/AFM.cl:478-562
+ *   relaxStrokes2D      kernels/AFM.cl:410-450
  *   getFEinStrokesTilted kernels/AFM.cl:210-233
  *   rotMat / rotMatT    kernels/common.cl:43-44
  *   getCoulombAFM/getLJ/getMorse kernels/AFM.cl:730-757
@@ -186,6 +187,39 @@ static void SFX(relax_strokes_pixel)(const GRID_T* g, const SFX(gridref)* G, con
         disps[oz * 4 + 2] = pos.z - ref.z; disps[oz * 4 + 3] = 0;
         tip.x = tip.x + dTip[0]; tip.y = tip.y + dTip[1]; tip.z = tip.z + dTip[2];
         pos.x = pos.x + dTip[0]; pos.y = pos.y + dTip[1]; pos.z = pos.z + dTip[2];
+    }
+}
+
+/* relaxStrokes2D: one pixel                                AFM.cl:410-450
+ * z fixed per slice (pz = az - iz*dh), x,y relaxed by damped MD from the anchor
+ * (reset per slice): f = F_grid.xy - K (p - anchor), v = v*(1-damp) + f*dt,
+ * p += v*dt, stop after the update once |f|^2 < f2conv or after max_iter
+ * steps; FE re-sampled at the final position, disps = (p - anchor, 0, 0). */
+static void SFX(relax_2d_pixel)(const GRID_T* g, const SFX(gridref)* G, const float* pt, int nzs, REAL K,
+                                REAL dh, REAL dt, REAL damp, int max_iter, REAL f2conv, int flip, REAL* FEs,
+                                REAL* disps) {
+    const REAL ax = (REAL)pt[0], ay = (REAL)pt[1], az = (REAL)pt[2];
+    const REAL cv = (REAL)1 - damp;
+    for (int iz = 0; iz < nzs; iz++) {
+        const REAL pz = az - (REAL)iz * dh;
+        REAL px = ax, py = ay, vx = 0, vy = 0;
+        REAL fe[4];
+        for (int i = 0; i < max_iter; i++) {
+            SFX(interp_fe)(g, G->nx, G->ny, G->nz, G->dA, G->dB, G->dC, SFX(mk3)(px, py, pz), fe);
+            const REAL fx = fe[0] - K * (px - ax);
+            const REAL fy = fe[1] - K * (py - ay);
+            vx = FMA(fx, dt, vx * cv);
+            vy = FMA(fy, dt, vy * cv);
+            px = FMA(vx, dt, px);
+            py = FMA(vy, dt, py);
+            if (FMA(fy, fy, fx * fx) < f2conv) break;
+        }
+        SFX(interp_fe)(g, G->nx, G->ny, G->nz, G->dA, G->dB, G->dC, SFX(mk3)(px, py, pz), fe);
+        const int oz = flip ? (nzs - 1 - iz) : iz;
+        FEs[oz * 4 + 0] = fe[0]; FEs[oz * 4 + 1] = fe[1];
+        FEs[oz * 4 + 2] = fe[2]; FEs[oz * 4 + 3] = fe[3];
+        disps[oz * 4 + 0] = px - ax; disps[oz * 4 + 1] = py - ay;
+        disps[oz * 4 + 2] = 0; disps[oz * 4 + 3] = 0;
     }
 }
 

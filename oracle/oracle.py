@@ -67,6 +67,8 @@ def lib():
                                        _i, _vp, _vp]),
         "ora_relax_tilted_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                       _i, _f, _i, _vp]),
+        "ora_relax_2d_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _f, _f, _f, _f, _i, _f, _i, _vp,
+                                  _vp]),
         "ora_relax_tilted_d": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                       _i, _d, _i, _vp]),
         "ora_raw_tilted_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -168,6 +170,20 @@ def relax_strokes(grid, dinv, pts, nz, dTip, stiffness, dpos0, relax, max_iter=1
     fn = lib().ora_relax_strokes_f if prec == "f32" else lib().ora_relax_strokes_d
     fn(_p(g), *_grid_args(g), *[_p(v) for v in vs], _p(pts), n_scan, int(nz), *[_p(v) for v in ps], int(max_iter),
        float(f2conv), int(bool(use_fire)), int(bool(flip)), _p(FEs), _p(disps))
+    return FEs, disps
+
+
+def relax_2d(grid, dinv, pts, nz, K_lat, dh, dt, damp, max_iter=128, f2conv=1e-8, flip=False):
+    """relaxStrokes2D (kernels/AFM.cl:410-450) -> FEs, disps (n_scan,nz,4), canonical FP32."""
+    g = np.ascontiguousarray(grid, dtype=np.float32)
+    pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 4)
+    n_scan = pts.shape[0]
+    FEs = np.zeros((n_scan, nz, 4), dtype=np.float32)
+    disps = np.zeros((n_scan, nz, 4), dtype=np.float32)
+    vs = [_v4(v) for v in (dinv[0], dinv[1], dinv[2])]
+    lib().ora_relax_2d_f(_p(g), *_grid_args(g), *[_p(v) for v in vs], _p(pts), n_scan, int(nz), float(K_lat),
+                         float(dh), float(dt), float(damp), int(max_iter), float(f2conv), int(bool(flip)), _p(FEs),
+                         _p(disps))
     return FEs, disps
 
 

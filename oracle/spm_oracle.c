@@ -193,6 +193,17 @@ void ora_relax_strokes_d(const double* grid, int nx, int ny, int nz, const float
                               use_fire, flip, FEs + (size_t)i * nzs * 4, disps + (size_t)i * nzs * 4);
 }
 
+void ora_relax_2d_f(const float* grid, int nx, int ny, int nz, const float* dinvA, const float* dinvB,
+                    const float* dinvC, const float* pts, int nscan, int nzs, float K, float dh, float dt, float damp,
+                    int max_iter, float f2conv, int flip, float* FEs, float* disps) {
+    gridref_f G; G.nx = nx; G.ny = ny; G.nz = nz;
+    cvt4_f(dinvA, G.dA); cvt4_f(dinvB, G.dB); cvt4_f(dinvC, G.dC);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < nscan; i++)
+        relax_2d_pixel_f(grid, &G, pts + 4 * (size_t)i, nzs, K, dh, dt, damp, max_iter, f2conv, flip,
+                         FEs + (size_t)i * nzs * 4, disps + (size_t)i * nzs * 4);
+}
+
 void ora_relax_tilted_f(const float* grid, int nx, int ny, int nz, const float* dinvA,
                         const float* dinvB, const float* dinvC, const float* pts, int nscan, int nzs,
                         const float* tA, const float* tB, const float* tC, const float* k, const float* d0,

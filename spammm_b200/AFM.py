@@ -328,6 +328,40 @@ class AFMulator:
         tip_disp = {"dx": disps[..., 0], "dy": disps[..., 1], "dz": disps[..., 2]}
         return FEs, tip_disp
 
+    def scan_fdbm_2d(self, scan_xs, scan_ys, probe_heights, mol_z=0.0, K_LAT=0.03, dt=0.3, damp=0.2,
+                     return_device=False):
+        """relaxStrokes2D over a 2D scan (AFM.py:644-704): z fixed per height
+        slice, x,y relaxed by damped MD from the anchor (reset per slice).
+
+        Returns (FEs_relax (nx,ny,nz,4) float32 with iz=0 the lowest height,
+        tip_disp {'dx','dy','dz'} each (nx,ny,nz); dz = 0)."""
+        if self.img_FF_fdbm is None:
+            raise AssertionError("call setup_fdbm_grid() first")
+        nx_s, ny_s, nz_s = len(scan_xs), len(scan_ys), len(probe_heights)
+        heights_desc = np.sort(np.asarray(probe_heights, dtype=np.float64))[::-1]
+        dh = float(heights_desc[0] - heights_desc[-1]) / max(nz_s - 1, 1) if nz_s > 1 else 0.
+        z_start = float(heights_desc[0]) + mol_z
+        gx, gy = np.meshgrid(scan_xs, scan_ys, indexing="ij")
+        pts = np.zeros((nx_s * ny_s, 4), dtype=np.float32)
+        pts[:, 0] = gx.ravel()
+        pts[:, 1] = gy.ravel()
+        pts[:, 2] = z_start
+        self._check_alloc(nx_s * ny_s * nz_s * 16, "scan_fdbm_2d FEs")
+        self.realloc_scan_buffers(nx_s * ny_s, nz_s)
+        P = self._flags_params(dinv=(self.fdbm_dinvA, self.fdbm_dinvB, self.fdbm_dinvC), dTip=[0., 0., -dh, 0.],
+                               stiffness=[K_LAT, 0., 0., 0.], relax_params=[dt, damp, 0., 0.], nz=nz_s, fire=False,
+                               flip_z=True, raster_ny=ny_s)
+        FEs, disps = gpu.relax_2d(self.img_FF_fdbm, P, torch.from_numpy(pts).to(self.device))
+        FEs = FEs.reshape(nx_s, ny_s, nz_s, 4)
+        disps = disps.reshape(nx_s, ny_s, nz_s, 4)
+        _log(1, f"AFMulator.scan_fdbm_2d: Fz min={float(FEs[..., 2].min()):.4f}  max={float(FEs[..., 2].max()):.4f}"
+                f"  mean={float(FEs[..., 2].mean()):.4f} eV/Ang")
+        if not return_device:
+            FEs = FEs.cpu().numpy()
+            disps = disps.cpu().numpy()
+        tip_disp = {"dx": disps[..., 0], "dy": disps[..., 1], "dz": disps[..., 2]}
+        return FEs, tip_disp
+
     # ---------------------------------------------------------------- molecule
     def load_molecule(self, xyz_path):
         self.mol = load_xyz_molecule(xyz_path)

@@ -123,6 +123,42 @@ def shared_postprocess(FEs_full, scan_spec, *, FEs_bwd=None, tip_disp=None, back
                       tip_disp=tip_disp, E_diss=E_diss, backend_name=backend_name, fft_path=fft_path)
 
 
+def compose_and_relax_total(F_total, scan_xs, scan_ys, heights, origin, step, atomPos, K_LAT=None, K_RAD=20.0,
+                            bond_length=4.0, use_gpu_relax=True, ppm_mode=False, afmulator=None,
+                            reuse_fdbm_grid=False, osc_dir=(0., 0., 1.), base_pos=(0., 0., 0.)):
+    """FDBM stage 4 (AFM_utils.py:3111-3201): relax the probe in a total force
+    field F_total (nx,ny,nz,4) and convert to df.
+
+    ppm_mode=True: relaxStrokes with the spherical PPM bond (scan_fdbm);
+    ppm_mode=False: 2-D lateral-only relaxStrokes2D (scan_fdbm_2d).  Returns
+    (df (nx_s,ny_s,nz_s), tip_disp, FEs_relax (nx_s,ny_s,nz_s,4)).  The
+    reference's legacy SciPy CPU relaxation (use_gpu_relax=False) is not part
+    of this implementation."""
+    if not use_gpu_relax:
+        raise NotImplementedError("compose_and_relax_total: the CPU SciPy relaxation is not provided; "
+                                  "use_gpu_relax must be True")
+    if K_LAT is None:
+        K_LAT = afm.K_LAT_HAPALA_EV_A2
+    mol_z = float(np.asarray(atomPos)[:, 2].max())
+    if ppm_mode:
+        if afmulator is None:
+            afmulator = afm.AFMulator(use_morse=False, nloc=32, use_fire=True)
+        if not reuse_fdbm_grid:
+            afmulator.setup_fdbm_grid(F_total, origin, step)
+        FEs_relax, tip_disp = afmulator.scan_fdbm(scan_xs, scan_ys, heights, mol_z=mol_z, K_LAT=K_LAT, K_RAD=K_RAD,
+                                                  bond_length=bond_length, ppm_mode=True, use_fire=True,
+                                                  osc_dir=osc_dir, base_pos=base_pos)
+    else:
+        if afmulator is None:
+            afmulator = afm.AFMulator(use_morse=False, nloc=32, use_fire=False)
+        if not reuse_fdbm_grid:
+            afmulator.setup_fdbm_grid(F_total, origin, step)
+        FEs_relax, tip_disp = afmulator.scan_fdbm_2d(scan_xs, scan_ys, heights, mol_z=mol_z, K_LAT=K_LAT)
+    spacing = (float(scan_xs[1] - scan_xs[0]), float(scan_ys[1] - scan_ys[0]), float(heights[1] - heights[0]))
+    df = afm.compute_df_dir(FEs_relax, spacing, osc_dir=osc_dir)
+    return df, tip_disp, FEs_relax
+
+
 def _morse_atoms_from_Z(atomPos, atomTypes, params_path=None, tip_R=1.452, tip_E=0.0006808, tip_alpha=-1.8):
     """(atoms (na,4), cMs (na,4)) Morse parameters from atomic numbers (AFM_utils.py:3993-4017)."""
     zm = z_map(read_element_types(params_path))

@@ -28,6 +28,7 @@ SPM_FLAG_FIRE = 1
 SPM_RELAX_STROKES = 0
 SPM_RELAX_TILTED = 1
 SPM_RELAX_PP = 2
+SPM_RELAX_2D = 3
 SPM_FLAG_FLIP_Z = 2
 
 _f4 = ctypes.c_float * 4

@@ -4,7 +4,7 @@ Every batched stage reads only its own fields of ``spm_batch_shape``:
 
   grid build   gb_ty (CTA rows: 32 x gb_ty threads), gb_zb (z-nodes per thread)
   relaxation   rx_threads (CTA size), rx_tile_h (pixel tile (32/h) x h per warp
-               draw), rx_regs (80 or 64 registers per thread)
+               draw), rx_regs (80 / 64 registers, or the register texel cache)
   adjoint      adj_chunk (slab nodes per node-major unit)
 
 so the stages are tuned one after another, each over its own candidates with
@@ -24,7 +24,7 @@ from .batch import AFMBatch
 
 GRID_CANDIDATES = [dict(gb_ty=ty, gb_zb=zb) for ty in (2, 4, 8) for zb in (8, 16)]
 RELAX_CANDIDATES = [dict(rx_threads=t, rx_tile_h=h, rx_regs=r) for t in (128, 256) for h in (4, 8, 16)
-                    for r in (0, 1)]
+                    for r in (0, 1, 2)]
 ADJOINT_CANDIDATES = [dict(adj_chunk=c) for c in (4096, 16384, 65536)]
 
 _CACHE = {}

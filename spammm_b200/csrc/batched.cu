@@ -39,7 +39,7 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
     SPM_REQUIRE(S.rx_ctas_per_sm >= 0, "spm_batch_prepare: rx_ctas_per_sm=%d", S.rx_ctas_per_sm);
     SPM_REQUIRE(S.adj_chunk >= 1024 && S.adj_chunk <= (1 << 20) && S.adj_chunk % 1024 == 0,
                 "spm_batch_prepare: adj_chunk=%d", S.adj_chunk);
-    SPM_REQUIRE(S.rx_regs == 0 || S.rx_regs == 1, "spm_batch_prepare: rx_regs=%d", S.rx_regs);
+    SPM_REQUIRE(S.rx_regs >= 0 && S.rx_regs <= 2, "spm_batch_prepare: rx_regs=%d", S.rx_regs);
     const long long th = S.rx_tile_h, tw = 32 / S.rx_tile_h;
     long long tiles = 0, slots = 0, units = 0, chunks = 0, states = 0, atoms = 0, pixels = 0, grid_end = 0, rows = 0;
     for (int m = 0; m < n_mol; m++) {

@@ -2,7 +2,8 @@
 //
 // Replaces relaxStrokes (SPAMMM kernels/AFM.cl:345-394, launched by
 // AFMulator.scan_fdbm, spammm/SPM/AFM.py:607-617), relaxStrokesTilted
-// (AFM.cl:478-562, AFMulator.run_scan, AFM.py:995-1004) and the raw sampler
+// (AFM.cl:478-562, AFMulator.run_scan, AFM.py:995-1004), relaxStrokes2D
+// (AFM.cl:410-450, AFMulator.scan_fdbm_2d, AFM.py:644-704) and the raw sampler
 // getFEinStrokesTilted (AFM.cl:210-233, AFMulator.get_raw_FE, AFM.py:2565-2574).
 //
 // The reference launches one work-item per work-group (local size 1).  Here
@@ -138,7 +139,8 @@ __device__ __forceinline__ void pp_emit(const GridView& G, const PPFrame& F, V3 
     *pp_out = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
 }
 
-// MODE 0: relaxStrokes; MODE 1: relaxStrokesTilted; MODE 2: PP (differentiable path).
+// MODE 0: relaxStrokes; MODE 1: relaxStrokesTilted; MODE 2: PP (differentiable
+// path); MODE 3: relaxStrokes2D.
 template <int MODE, typename IDX>
 __global__ void __launch_bounds__(RX_THREADS)
 relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
@@ -157,6 +159,8 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
     const V3 dTip = (MODE == 0) ? mk3(P.dTip[0], P.dTip[1], P.dTip[2])
                                 : mk3(__fmul_rn(c.x, tc.w), __fmul_rn(c.y, tc.w), __fmul_rn(c.z, tc.w));
     const V3 d0r = (MODE == 0) ? mk3(d0.x, d0.y, d0.z) : rotmatT(mk3(d0.x, d0.y, d0.z), a, b, c);
+    const float dh2 = -P.dTip[2];                  // MODE 3: descent per slice (dTip.z = -dh)
+    const float cv2 = 1.f - P.relax_params[1];     // MODE 3: velocity retention 1 - damp
 
     int k = counter ? next_pixel(counter, n_scan, P.raster_ny) : pixel_of_thread(n_scan, P.raster_ny);
     V3 tip, pos, v;
@@ -166,7 +170,7 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
     auto start = [&](int kp) {
         const float4 p4 = pts[kp];
         tip = mk3(p4.x, p4.y, p4.z);
-        pos = (MODE == 0) ? mk3(tip.x + d0r.x, tip.y + d0r.y, tip.z + d0r.z) : add3(tip, d0r);
+        pos = (MODE == 0) ? mk3(tip.x + d0r.x, tip.y + d0r.y, tip.z + d0r.z) : (MODE == 3 ? tip : add3(tip, d0r));
         I.dt = P.relax_params[0];
         I.damp = P.relax_params[1];
         I.dtmax = I.dt;
@@ -191,6 +195,38 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
                 pos = add3(pos, dTip);
                 v = mk3(0.f, 0.f, 0.f);
                 fe = make_float4(0.f, 0.f, 0.f, 0.f);
+                it = 0;
+                if (++iz == nzs) {
+                    if (iter_count) iter_count[k] = total_it;
+                    k = counter ? next_pixel(counter, n_scan, P.raster_ny) : -1;
+                    if (k >= 0) start(k);
+                }
+            }
+            continue;
+        }
+        if (MODE == 3) {
+            // relaxStrokes2D: z fixed per slice, x,y relaxed by damped MD from the anchor
+            const float pz = tip.z - __fmul_rn((float)iz, dh2);
+            bool done = max_iter <= 0;
+            if (!done) {
+                fe = interp_fe<IDX>(G, mk3(pos.x, pos.y, pz));
+                const float fx = fe.x - __fmul_rn(kk.x, pos.x - tip.x);
+                const float fy = fe.y - __fmul_rn(kk.x, pos.y - tip.y);
+                v.x = __fmaf_rn(fx, P.relax_params[0], __fmul_rn(v.x, cv2));
+                v.y = __fmaf_rn(fy, P.relax_params[0], __fmul_rn(v.y, cv2));
+                pos.x = __fmaf_rn(v.x, P.relax_params[0], pos.x);
+                pos.y = __fmaf_rn(v.y, P.relax_params[0], pos.y);
+                ++it;
+                ++total_it;
+                done = (__fmaf_rn(fy, fy, __fmul_rn(fx, fx)) < P.f2conv) || (it >= max_iter);
+            }
+            if (done) {
+                const int oz = flip ? (nzs - 1 - iz) : iz;
+                const size_t o = (size_t)k * nzs + oz;
+                FEs[o] = interp_fe<IDX>(G, mk3(pos.x, pos.y, pz));
+                disps[o] = make_float4(pos.x - tip.x, pos.y - tip.y, 0.f, 0.f);
+                pos = tip;
+                v = mk3(0.f, 0.f, 0.f);
                 it = 0;
                 if (++iz == nzs) {
                     if (iter_count) iter_count[k] = total_it;
@@ -380,14 +416,21 @@ __device__ __forceinline__ bool next_batch_pixel(unsigned* counter, unsigned n_s
 // (0,0,1,dz)) on an axis-aligned slab: pp_iter with the frame rotations
 // dropped -- with an identity frame they change no value (the sign of an exact
 // zero aside) -- and c*surf reduced to its z part.
-template <typename IDX>
-__device__ __forceinline__ bool pp_iter_z(const AxisView& G, const spm_scan_params& P, V3 tip, V3& pos, V3& v,
-                                          float& dt, float& damp, float4& fe, int& it, int& total_it, bool& conv) {
+template <typename IDX, bool CACHE>
+__device__ __forceinline__ float4 sample_z(const AxisView& G, V3 p, TexelCache& T) {
+    if constexpr (CACHE) return interp_fe_cached<IDX, true>(G, p, T);
+    else return interp_fe_pair<IDX, true>(G, p);
+}
+
+template <typename IDX, bool CACHE>
+__device__ __forceinline__ bool pp_iter_z(const AxisView& G, TexelCache& T, const spm_scan_params& P, V3 tip,
+                                          V3& pos, V3& v, float& dt, float& damp, float4& fe, int& it, int& total_it,
+                                          bool& conv) {
     conv = false;
     if (it >= P.max_iter) return true;
     ++it;
     ++total_it;
-    fe = interp_fe_pair<IDX, true>(G, pos);
+    fe = sample_z<IDX, CACHE>(G, pos, T);
     if (fe.w != fe.w) return true;  // outside the slab (or a NaN grid): not converged
     const V3 ft = tip_force(sub3(pos, tip), ld4(P.stiffness), ld4(P.dpos0));
     V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
@@ -414,9 +457,11 @@ __device__ __forceinline__ AxisView axis_view(const spm_batch_mol* D, const floa
     return G;
 }
 
-// MINB = 3: up to 80 registers per thread (768 resident threads per SM);
-// MINB = 4: 64 registers (1024 resident threads, a few spilled values).
-template <int MINB>
+// Variants (spm_batch_shape.rx_regs): MINB = 3: up to 80 registers per thread
+// (768 resident threads per SM); MINB = 4: 64 registers (1024 threads, a few
+// spilled values); CACHE: texels kept in registers across iterations (112
+// registers, MINB = 2).
+template <int MINB, bool CACHE>
 __global__ void __launch_bounds__(256, MINB)
 batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
                    const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
@@ -426,6 +471,7 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     int m = 0, k = 0;
     bool have = next_batch_pixel(counter, n_slots, mols, n_mol, th_log2, m, k);
     AxisView G;
+    TexelCache T;
     long long sbase = 0;
     int nzs = 0, pix = 0;
     V3 tip, pos, v;
@@ -435,6 +481,7 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     auto start = [&]() {
         const spm_batch_mol* D = mols + m;
         G = axis_view(D, grid);
+        T.x0 = -1;  // new slab: nothing cached
         nzs = D->nz_steps;
         pix = D->pix_off + k;
         sbase = D->state_off + (long long)k * nzs;
@@ -452,8 +499,8 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     if (have) start();
     while (have) {
         bool conv;
-        if (pp_iter_z<unsigned>(G, P, tip, pos, v, dt, damp, fe, it, total_it, conv)) {
-            if (!conv) fe = interp_fe_pair<unsigned, true>(G, pos);  // the position moved after the last sample
+        if (pp_iter_z<unsigned, CACHE>(G, T, P, tip, pos, v, dt, damp, fe, it, total_it, conv)) {
+            if (!conv) fe = sample_z<unsigned, CACHE>(G, pos, T);  // the position moved after the last sample
             const long long o = sbase + iz;
             FEs[o] = fe;
             // all seven values finite <=> the sum of their products with zero is zero
@@ -506,8 +553,9 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     SPM_REQUIRE(shape->rx_ctas_per_sm >= 0, "spm_batch_relax: rx_ctas_per_sm=%d", shape->rx_ctas_per_sm);
     int th_log2 = 0;
     while ((1 << th_log2) < h) th_log2++;
-    SPM_REQUIRE(shape->rx_regs == 0 || shape->rx_regs == 1, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
-    auto kern = shape->rx_regs ? batch_relax_kernel<4> : batch_relax_kernel<3>;
+    SPM_REQUIRE(shape->rx_regs >= 0 && shape->rx_regs <= 2, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
+    auto kern = shape->rx_regs == 2 ? batch_relax_kernel<2, true>
+                                    : (shape->rx_regs == 1 ? batch_relax_kernel<4, false> : batch_relax_kernel<3, false>);
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
@@ -536,8 +584,8 @@ extern "C" int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz,
                             void* stream) {
     using namespace spm;
     clear_error();
-    SPM_REQUIRE(mode == SPM_RELAX_STROKES || mode == SPM_RELAX_TILTED || mode == SPM_RELAX_PP,
-                "spm_relax_ex: mode=%d", mode);
+    SPM_REQUIRE(mode == SPM_RELAX_STROKES || mode == SPM_RELAX_TILTED || mode == SPM_RELAX_PP ||
+                mode == SPM_RELAX_2D, "spm_relax_ex: mode=%d", mode);
     int rc = check_scan_args("spm_relax_ex", grid, nx, ny, nz, points, n_scan, p, FEs);
     if (rc) return rc;
     if (n_scan == 0 || p->nz == 0) return SPM_OK;
@@ -556,6 +604,9 @@ extern "C" int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz,
                               reinterpret_cast<float4*>(disps), iter_count, ctr, st);
     if (mode == SPM_RELAX_PP)
         return launch_mode<2>(G, nodes, pt, n_scan, P, reinterpret_cast<float4*>(FEs),
+                              reinterpret_cast<float4*>(disps), iter_count, ctr, st);
+    if (mode == SPM_RELAX_2D)
+        return launch_mode<3>(G, nodes, pt, n_scan, P, reinterpret_cast<float4*>(FEs),
                               reinterpret_cast<float4*>(disps), iter_count, ctr, st);
     return launch_mode<1>(G, nodes, pt, n_scan, P, reinterpret_cast<float4*>(FEs), nullptr, iter_count, ctr, st);
 }

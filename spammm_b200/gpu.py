@@ -124,6 +124,22 @@ def relax_pp(grid, params, points, FEs=None, PPs=None, iter_count=None, dynamic=
     return FEs, PPs
 
 
+def relax_2d(grid, params, points, FEs=None, disps=None, iter_count=None, dynamic=True):
+    """relaxStrokes2D (SPM_RELAX_2D) over (n_scan,4) anchors -> FEs, disps (n_scan,nz,4).
+    params: stiffness[0] = K_lat, relax_params = (dt, damp), dTip[2] = -dh."""
+    nx, ny, nz = _grid_dims(grid)
+    points = _as_dev(points, F32, (4,), "points")
+    n_scan = points.shape[0]
+    shape = (n_scan, params.nz, 4)
+    FEs = torch.empty(shape, dtype=F32, device=points.device) if FEs is None else FEs
+    disps = torch.empty(shape, dtype=F32, device=points.device) if disps is None else disps
+    ws = _workspace(points.device) if dynamic else None
+    rc = lib().spm_relax_ex(_lib.SPM_RELAX_2D, ptr(grid), nx, ny, nz, ptr(points), n_scan, ctypes.byref(params),
+                            ptr(FEs), ptr(disps), ptr(iter_count), ptr(ws), stream_ptr())
+    check(rc, "spm_relax_ex(2D)")
+    return FEs, disps
+
+
 def adjoint_grid_state(grid, params, points, PPs, dL_dFEs):
     """Per-state implicit adjoint on the grid -> ubar, dk, diag (n_state,4)."""
     nx, ny, nz = _grid_dims(grid)

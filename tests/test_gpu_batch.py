@@ -101,7 +101,8 @@ def test_batch_shapes_give_same_results(cuda):
     ref.forward_adjoint()
     L = _lib.lib()
     for kw in (dict(gb_ty=2, gb_zb=16, rx_threads=64, rx_tile_h=1, adj_chunk=1024),
-               dict(gb_ty=8, gb_zb=8, rx_threads=256, rx_tile_h=32, rx_ctas_per_sm=1, adj_chunk=65536)):
+               dict(gb_ty=8, gb_zb=8, rx_threads=256, rx_tile_h=32, rx_ctas_per_sm=1, adj_chunk=65536, rx_regs=1),
+               dict(rx_threads=128, rx_tile_h=4, rx_regs=2)):
         s = L.spm_batch_default_shape()
         for k, v in kw.items():
             setattr(s, k, v)

@@ -152,3 +152,22 @@ def test_grid_relaxation_matches_reference_loops(golden):
     raw = O.raw_tilted(grid, dinv, pts, nz, [1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0], g["dTip"], g["dpos0"],
                        prec="f64")
     np.testing.assert_allclose(raw, g["raw_FEs"], rtol=1e-12, atol=1e-14)
+
+
+def test_oracle_relax_2d_uniform_field_equilibrium():
+    """relaxStrokes2D restatement (kernels/AFM.cl:410-450): in a uniform lateral
+    force F the damped MD settles at anchor + F/K_lat; z is fixed per slice and
+    the slices are stored lowest-first under flip."""
+    from oracle import oracle as O
+    nx = ny = nz = 16
+    g = np.zeros((nz, ny, nx, 4), np.float32)
+    g[..., 0], g[..., 1], g[..., 3] = 0.01, -0.02, np.arange(nz, dtype=np.float32)[:, None, None]
+    dinv = O.dinv_axis_aligned(np.array([1.6, 1.6, 1.6]), np.zeros(3), (nx, ny, nz))
+    pts = np.array([[0.8, 0.8, 1.2, 0]], np.float32)
+    K = 0.05
+    FEs, D = O.relax_2d(g, dinv, pts, 4, K, 0.1, 0.3, 0.2, 5000, 1e-16, flip=True)
+    np.testing.assert_allclose(D[0, :, 0], 0.01 / K, rtol=1e-4)
+    np.testing.assert_allclose(D[0, :, 1], -0.02 / K, rtol=1e-4)
+    assert not D[..., 2:].any()
+    # E channel = layer index; node k sits at z = k*0.1: slices at z = 1.2 .. 0.9, stored lowest first
+    np.testing.assert_allclose(FEs[0, :, 3], [9.0, 10.0, 11.0, 12.0], atol=1e-4)
