@@ -261,7 +261,7 @@ class AFMulator:
     def download_image_rgba_xyz(self, img, shape):
         """(nz,ny,nx,4) device grid -> (nx,ny,nz,4) host array (AFM.py:474-481)."""
         nx, ny, nz = [int(x) for x in shape[:3]]
-        host = img.reshape(nz, ny, nx, 4).cpu().numpy()
+        host = gpu.to_host(img.reshape(nz, ny, nx, 4))
         return np.ascontiguousarray(host.transpose(2, 1, 0, 3))
 
     # ---------------------------------------------------------------- scans
@@ -323,8 +323,8 @@ class AFMulator:
         FEs = FEs.reshape(nx_s, ny_s, nz_s, 4)
         disps = disps.reshape(nx_s, ny_s, nz_s, 4)
         if not return_device:
-            FEs = FEs.cpu().numpy()
-            disps = disps.cpu().numpy()
+            FEs = gpu.to_host(FEs)
+            disps = gpu.to_host(disps)
         tip_disp = {"dx": disps[..., 0], "dy": disps[..., 1], "dz": disps[..., 2]}
         return FEs, tip_disp
 
@@ -357,8 +357,8 @@ class AFMulator:
         _log(1, f"AFMulator.scan_fdbm_2d: Fz min={float(FEs[..., 2].min()):.4f}  max={float(FEs[..., 2].max()):.4f}"
                 f"  mean={float(FEs[..., 2].mean()):.4f} eV/Ang")
         if not return_device:
-            FEs = FEs.cpu().numpy()
-            disps = disps.cpu().numpy()
+            FEs = gpu.to_host(FEs)
+            disps = gpu.to_host(disps)
         tip_disp = {"dx": disps[..., 0], "dy": disps[..., 1], "dz": disps[..., 2]}
         return FEs, tip_disp
 
@@ -537,7 +537,7 @@ class AFMulator:
         FEs = gpu.relax_strokes_tilted(self.img_FF, P, torch.from_numpy(pts).to(self.device))
         FEs = FEs.reshape(nx_s, ny_s, nz, 4)
         if not return_device:
-            FEs = FEs.cpu().numpy()
+            FEs = gpu.to_host(FEs)
         return FEs, pts[:, :3].reshape(nx_s, ny_s, 3)
 
     def get_raw_FE(self, nxy=(60, 60), nz=21, dtip=-0.2, scan_p0=None, scan_da=None, scan_db=None, bAlloc=True,
@@ -558,7 +558,7 @@ class AFMulator:
         P = self._flags_params(dinv=(self.dinvA, self.dinvB, self.dinvC), tipA=self.tipA, tipB=self.tipB,
                                tipC=self.tipC, dTip=dTip, dpos0=self.dpos0, nz=nz, raster_ny=ny_s)
         FEs = gpu.fe_in_strokes_tilted(self.img_FF, P, torch.from_numpy(pts).to(self.device))
-        return FEs.reshape(nx_s, ny_s, nz, 4).cpu().numpy(), pts[:, :3].reshape(nx_s, ny_s, 3)
+        return gpu.to_host(FEs.reshape(nx_s, ny_s, nz, 4)), pts[:, :3].reshape(nx_s, ny_s, 3)
 
     @property
     def mol_z(self):
@@ -571,7 +571,7 @@ class AFMulator:
         FEs = np.asarray(FEs)
         vol = np.zeros(FEs.shape[:3] + (4,), dtype=np.float32)
         vol[..., 2] = FEs[..., 2]
-        mdf = gpu.df_dir(vol, (1.0, 1.0, 1.0), (0., 0., 1.)).cpu().numpy()  # = -dFz/dz
+        mdf = gpu.to_host(gpu.df_dir(vol, (1.0, 1.0, 1.0), (0., 0., 1.)))  # = -dFz/dz
         return mdf.mean(axis=2) / (2.0 * k_tip)
 
     # ---------------------------------------------------------------- direct Morse
@@ -615,8 +615,8 @@ class AFMulator:
         P = self._flags_params(tipA=self.tipA, tipB=self.tipB, tipC=tipC, stiffness=self.stiffness, dpos0=self.dpos0,
                                relax_params=self.relax_pars, surfFF=self.surfFF, nz=nz, raster_ny=ny_s, fire=True)
         FEs_t, PPs_t = gpu.relax_direct_morse(self.atoms_arr, self.cLJs_arr, pts, P, self.tipQs, self.tipQZs)
-        FEs = FEs_t.reshape(nx_s, ny_s, nz, 4).cpu().numpy()
-        PPs = PPs_t.reshape(nx_s, ny_s, nz, 4).cpu().numpy()
+        FEs = gpu.to_host(FEs_t.reshape(nx_s, ny_s, nz, 4))
+        PPs = gpu.to_host(PPs_t.reshape(nx_s, ny_s, nz, 4))
         points_xyz = pts[:, :3].reshape(nx_s, ny_s, 3)
         finite_mask = np.isfinite(PPs).all(axis=-1)
         bad_mask = (~finite_mask) | (PPs[..., 3] < 0.0)
@@ -714,7 +714,7 @@ class AFMulator:
         pts[:, :3] = points_xyz.reshape(-1, 3)
         lam, diag = gpu.adjoint_direct_state(self.atoms_arr, self.cLJs_arr, pts, P, self.tipQs, self.tipQZs,
                                              PPs.reshape(-1, 4), dL_dFEs.reshape(-1, 4))
-        adjoint_diag = diag.reshape(nx, ny, nz, 4).cpu().numpy()
+        adjoint_diag = gpu.to_host(diag.reshape(nx, ny, nz, 4))
         if not np.isfinite(adjoint_diag).all():
             flat_idx = int(np.argmax(~np.isfinite(adjoint_diag).all(axis=-1)))
             ix, iy, iz = np.unravel_index(flat_idx, (nx, ny, nz))
@@ -745,7 +745,7 @@ class AFMulator:
 
 # ---------------------------------------------------------------- stage (c)
 def _to_np(t):
-    return t.cpu().numpy()
+    return gpu.to_host(t)
 
 
 def _volume(FEs, ncopy=3):

@@ -114,8 +114,8 @@ def shared_postprocess(FEs_full, scan_spec, *, FEs_bwd=None, tip_disp=None, back
         tip_disp = {k: np.zeros((nx, ny, nz_scan), dtype=np.float32) for k in ("dx", "dy", "dz")}
     amp_align = bool(abs(float(osc_n[2])) > 1e-12)
     if not return_device:
-        df, Fz, E_diss = df.cpu().numpy(), Fz.cpu().numpy(), E_diss.cpu().numpy()
-        F = F.cpu().numpy() if on_dev else F
+        df, Fz, E_diss = gpu.to_host(df), gpu.to_host(Fz), gpu.to_host(E_diss)
+        F = gpu.to_host(F) if on_dev else F
     return ScanResult(df=df, Fz=Fz, heights=np.asarray(scan_spec.h_df, dtype=np.float32),
                       heights_Fz=np.asarray(scan_spec.h_Fz, dtype=np.float32),
                       scan_xs=np.asarray(scan_spec.scan_xs, dtype=np.float32),
@@ -242,7 +242,7 @@ def run_morse_pp_afm(tag, atomPos, atomTypes, origin, step, ngrid, outdir=None, 
     sy = slice(pad_y, pad_y + len(scan_ys))
     FEs = FEs_full[sx, sy].contiguous()
     FEs_bwd = FEs_bwd_full[sx, sy].contiguous()
-    tip_disp = {k: v[sx, sy].cpu().numpy() for k, v in tip_disp_full.items()}
+    tip_disp = {k: gpu.to_host(v[sx, sy]) for k, v in tip_disp_full.items()}
     result = shared_postprocess(FEs, scan_spec, FEs_bwd=FEs_bwd, tip_disp=tip_disp, backend_name="morse",
                                 fft_path="none")
     result.tag = tag

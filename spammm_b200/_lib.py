@@ -100,7 +100,7 @@ class BatchShape(ctypes.Structure):
     _fields_ = [
         ("gb_ty", ctypes.c_int), ("gb_zb", ctypes.c_int), ("rx_threads", ctypes.c_int),
         ("rx_tile_h", ctypes.c_int), ("rx_ctas_per_sm", ctypes.c_int), ("adj_chunk", ctypes.c_int),
-        ("rx_regs", ctypes.c_int),
+        ("rx_regs", ctypes.c_int), ("grid_layout", ctypes.c_int),
     ]
 
     def key(self):
@@ -153,7 +153,7 @@ _SIGNATURES = {
     "spm_batch_df_amp": (_i, [_i, _vp, _ll, _vp, _d, _d, _vp, _vp]),
     "spm_batch_df_loss_seed": (_i, [_i, _vp, _ll, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _vp]),
     "spm_batch_loss_scratch_bytes": (_ll, [_ll, _i]),
-    "spm_batch_adjoint_state": (_i, [_i, _vp, _ll, _vp, _vp, _P, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "spm_batch_adjoint_state": (_i, [_i, _vp, _ll, _BS, _vp, _vp, _P, _vp, _vp, _vp, _vp, _vp, _vp]),
     "spm_batch_adjoint_params": (_i, [_i, _i, _vp, _LLP, _BS, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                       _vp]),
     "spm_batch_adjoint_scratch_bytes": (_ll, [_LLP, _i]),

@@ -4,7 +4,9 @@ Every batched stage reads only its own fields of ``spm_batch_shape``:
 
   grid build   gb_ty (CTA rows: 32 x gb_ty threads), gb_zb (z-nodes per thread)
   relaxation   rx_threads (CTA size), rx_tile_h (pixel tile (32/h) x h per warp
-               draw), rx_regs (80 / 64 registers, or the register texel cache)
+               draw), rx_regs (80 / 64 registers, or the register texel cache),
+               grid_layout (x-pair or xz-quad slabs: the grid is rebuilt in the
+               candidate's layout before the relaxation is timed)
   adjoint      adj_chunk (slab nodes per node-major unit)
 
 so the stages are tuned one after another, each over its own candidates with
@@ -23,8 +25,8 @@ from . import _lib
 from .batch import AFMBatch
 
 GRID_CANDIDATES = [dict(gb_ty=ty, gb_zb=zb) for ty in (2, 4, 8) for zb in (8, 16)]
-RELAX_CANDIDATES = [dict(rx_threads=t, rx_tile_h=h, rx_regs=r) for t in (128, 256) for h in (4, 8, 16)
-                    for r in (0, 1, 2)]
+RELAX_CANDIDATES = [dict(rx_threads=t, rx_tile_h=h, rx_regs=r, grid_layout=g) for g in (0, 1) for t in (128, 256)
+                    for h in (4, 8, 16) for r in (0, 1, 2)]
 ADJOINT_CANDIDATES = [dict(adj_chunk=c) for c in (4096, 16384, 65536)]
 
 _CACHE = {}
@@ -67,17 +69,20 @@ def sub_batch(items, max_molecules):
     return [items[i] for i in sorted(set(pick.tolist()))]
 
 
-def tune(batch, reps=2, adjoint=True, log=None):
-    """Tune batch.shape in place, stage by stage; returns (shape, timings)."""
+def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
+    """Tune batch.shape in place, stage by stage; returns (shape, timings).
+    max_grid_bytes: leave out slab layouts whose grid buffer would exceed it."""
     report = {}
     shape = batch.shape
 
-    def pick(name, cands, run):
+    def pick(name, cands, run, prepare=None):
         nonlocal shape
         res = []
         for kw in cands:
             s = _with(shape, **kw)
             batch.set_shape(s)
+            if prepare is not None:
+                prepare()
             ms = _time(run, reps)
             res.append((ms, kw))
             if log:
@@ -89,7 +94,9 @@ def tune(batch, reps=2, adjoint=True, log=None):
     pick("grid", GRID_CANDIDATES, batch.build_grids)
     batch.set_shape(shape)
     batch.build_grids()
-    pick("relax", RELAX_CANDIDATES, batch.relax)
+    cands = RELAX_CANDIDATES if max_grid_bytes is None else [
+        c for c in RELAX_CANDIDATES if (4 if c["grid_layout"] else 2) * batch.grid_float4 * 16 <= max_grid_bytes]
+    pick("relax", cands, batch.relax, prepare=batch.build_grids)
     if adjoint:
         batch.set_shape(shape)
         batch.relax()

@@ -204,7 +204,7 @@ class AFMBatch:
         self.atoms = torch.as_tensor(plan.atoms, device=dev).contiguous()
         self.params = torch.as_tensor(plan.params, device=dev).contiguous()
         self.points = torch.as_tensor(plan.points, device=dev).contiguous()
-        self.grid = torch.empty((2 * go, 4), dtype=F32, device=dev)  # x-paired slabs: 2 float4 per node
+        self.grid = None  # slabs: 2 (x-pairs) or 4 (xz-quads) float4 per node, allocated by set_shape
         self.FEs = torch.empty((so, 4), dtype=F32, device=dev)
         self.PPs = torch.empty((so, 4), dtype=F32, device=dev)
         self.iter_count = torch.empty((po,), dtype=torch.int32, device=dev)
@@ -229,6 +229,10 @@ class AFMBatch:
         """Number the work items for `shape` and upload the descriptors."""
         totals = self.plan.prepare(shape)
         self.shape = self.plan.shape
+        per_node = self.node_stride
+        if self.grid is None or self.grid.shape[0] != per_node * self.grid_float4:
+            self.grid = None  # release the old layout's buffer before allocating the new one
+            self.grid = torch.empty((per_node * self.grid_float4, 4), dtype=F32, device=self.dev)
         (self.n_tiles, self.n_slots, self.n_units, self.n_chunks, states, atoms, pixels, gend, self.n_rows) = totals
         assert (states, atoms, pixels, gend) == (self.total_states, self.total_atoms, self.total_pixels,
                                                  self.grid_float4)
@@ -243,6 +247,11 @@ class AFMBatch:
     def desc(self, i):
         """Descriptor of molecule i (caller's order)."""
         return self.plan.desc(i)
+
+    @property
+    def node_stride(self):
+        """float4 stored per slab node: 2 (x-pairs) or 4 (xz-quads)."""
+        return 4 if self.shape.grid_layout else 2
 
     # ------------------------------------------------------------ stages
     def build_grids(self):
@@ -288,7 +297,8 @@ class AFMBatch:
 
     def adjoint_state(self):
         self._ensure_adjoint_buffers()
-        rc = lib().spm_batch_adjoint_state(self.n, ptr(self.mols_d), self.total_states, ptr(self.grid),
+        rc = lib().spm_batch_adjoint_state(self.n, ptr(self.mols_d), self.total_states, ctypes.byref(self.shape),
+                                           ptr(self.grid),
                                            ptr(self.points), ctypes.byref(self.scan_params), ptr(self.PPs),
                                            ptr(self.dL), ptr(self.ubar), ptr(self.dk), ptr(self.diag), stream_ptr())
         check(rc, "spm_batch_adjoint_state")
@@ -361,12 +371,14 @@ class AFMBatch:
             return D.pix_off, D.pix_off + D.n_scan
         return D.atom_off, D.atom_off + D.n_atoms
 
-    def slab(self, i):
-        """(nz_slab, ny, nx, 4) view of molecule i's stored layers (the x-paired
-        buffer's first halves; layer 0 is the full grid's layer z_lo)."""
+    def slab(self, i, slot=0):
+        """(nz_slab, ny, nx, 4) view of molecule i's stored layers (slot 0: the
+        nodes' own values; layer 0 is the full grid's layer z_lo).  Other slots
+        hold the (x+1), (z+1) and (x+1, z+1) neighbours of the layout."""
         D = self.desc(i)
         n = D.nx * D.ny * D.nz_slab
-        return self.grid.view(-1, 2, 4)[D.grid_off:D.grid_off + n, 0].reshape(D.nz_slab, D.ny, D.nx, 4)
+        k = self.node_stride
+        return self.grid.view(-1, k, 4)[D.grid_off:D.grid_off + n, slot].reshape(D.nz_slab, D.ny, D.nx, 4)
 
     def fes(self, i):
         a, b = self._rows(i, "state")

@@ -73,12 +73,12 @@ __device__ __forceinline__ Corners corners_of(const GridView& G, V3 p) {
 }
 
 // Stored node (x, y, z) of a full grid or of a batch slab (z is the full
-// grid's layer; batch slabs are x-paired: node idx at G.g[2*idx]).
+// grid's layer; batch slabs hold G.stride float4 per node, its value first).
 template <bool SLAB>
 __device__ __forceinline__ float4 node_at(const GridView& G, int x, int y, int z) {
     const int zl = SLAB ? z - G.z_lo : z;
     const size_t idx = ((size_t)zl * G.ny + y) * G.nx + x;
-    return __ldg(G.g + (SLAB ? 2 * idx : idx));
+    return __ldg(G.g + (SLAB ? (size_t)G.stride * idx : idx));
 }
 
 struct Sites {
@@ -399,6 +399,7 @@ GridView view_of(const float* grid, int nx, int ny, int nz, const spm_scan_param
     GridView G;
     G.g = reinterpret_cast<const float4*>(grid);
     G.nx = nx; G.ny = ny; G.nz = nz;
+    G.z_lo = 0; G.nz_slab = nz; G.stride = 1;
     G.dA = make_float4(p->dinvA[0], p->dinvA[1], p->dinvA[2], p->dinvA[3]);
     G.dB = make_float4(p->dinvB[0], p->dinvB[1], p->dinvB[2], p->dinvB[3]);
     G.dC = make_float4(p->dinvC[0], p->dinvC[1], p->dinvC[2], p->dinvC[3]);
@@ -410,7 +411,7 @@ long long n_rowblocks(long long n_state) { return n_state > 0 ? (n_state + 2047)
 
 // ---- batched ----------------------------------------------------------------
 __global__ void __launch_bounds__(AG_THREADS)
-batch_adjoint_state_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states,
+batch_adjoint_state_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states, int stride,
                            const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
                            const float4* __restrict__ PPs, const float4* __restrict__ dL, float4* __restrict__ ubar,
                            float4* __restrict__ dk, float4* __restrict__ diag) {
@@ -420,7 +421,7 @@ batch_adjoint_state_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, lo
     const long long ls = st - D->state_off;
     const int nz = D->nz_steps;
     const int iscan = (int)(ls / nz), iz = (int)(ls % nz);
-    state_adjoint<true>(slab_view(*D, grid), P, pts[D->pix_off + iscan], iz, PPs[st], dL[st], ubar + st, dk + st,
+    state_adjoint<true>(slab_view(*D, grid, stride), P, pts[D->pix_off + iscan], iz, PPs[st], dL[st], ubar + st, dk + st,
                         diag + st);
 }
 
@@ -804,12 +805,15 @@ AdjScratch adj_scratch_layout(const long long* totals, int n_mol) {
 }  // namespace
 }  // namespace spm
 
-extern "C" int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_states, const float* grid,
-                                       const float* points, const spm_scan_params* p, const float* PPs,
-                                       const float* dL_dFEs, float* ubar, float* dk, float* diag, void* stream) {
+extern "C" int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_states,
+                                       const spm_batch_shape* shape, const float* grid, const float* points,
+                                       const spm_scan_params* p, const float* PPs, const float* dL_dFEs, float* ubar,
+                                       float* dk, float* diag, void* stream) {
     using namespace spm;
     clear_error();
-    SPM_REQUIRE(p, "spm_batch_adjoint_state: null params");
+    SPM_REQUIRE(p && shape, "spm_batch_adjoint_state: null params/shape");
+    SPM_REQUIRE(shape->grid_layout == 0 || shape->grid_layout == 1, "spm_batch_adjoint_state: grid_layout=%d",
+                shape->grid_layout);
     SPM_REQUIRE(n_mol >= 0 && n_states >= 0, "spm_batch_adjoint_state: negative sizes");
     if (n_mol == 0 || n_states == 0) return SPM_OK;
     SPM_REQUIRE(mols && grid && points && PPs && dL_dFEs && ubar && dk && diag, "spm_batch_adjoint_state: null pointer");
@@ -818,7 +822,8 @@ extern "C" int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, lon
     const long long nb = (n_states + AG_THREADS - 1) / AG_THREADS;
     SPM_REQUIRE(nb < (1LL << 31), "spm_batch_adjoint_state: too many states");
     batch_adjoint_state_kernel<<<(unsigned)nb, AG_THREADS, 0, as_stream(stream)>>>(
-        n_mol, mols, n_states, grid, reinterpret_cast<const float4*>(points), *p, reinterpret_cast<const float4*>(PPs),
+        n_mol, mols, n_states, shape->grid_layout ? 4 : 2, grid, reinterpret_cast<const float4*>(points), *p,
+        reinterpret_cast<const float4*>(PPs),
         reinterpret_cast<const float4*>(dL_dFEs), reinterpret_cast<float4*>(ubar), reinterpret_cast<float4*>(dk),
         reinterpret_cast<float4*>(diag));
     return check_launch("spm_batch_adjoint_state");

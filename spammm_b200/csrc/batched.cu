@@ -20,6 +20,7 @@ extern "C" spm_batch_shape spm_batch_default_shape(void) {
     s.rx_ctas_per_sm = 0;
     s.adj_chunk = 16384;
     s.rx_regs = 0;
+    s.grid_layout = 0;
     return s;
 }
 
@@ -40,6 +41,7 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
     SPM_REQUIRE(S.adj_chunk >= 1024 && S.adj_chunk <= (1 << 20) && S.adj_chunk % 1024 == 0,
                 "spm_batch_prepare: adj_chunk=%d", S.adj_chunk);
     SPM_REQUIRE(S.rx_regs >= 0 && S.rx_regs <= 2, "spm_batch_prepare: rx_regs=%d", S.rx_regs);
+    SPM_REQUIRE(S.grid_layout == 0 || S.grid_layout == 1, "spm_batch_prepare: grid_layout=%d", S.grid_layout);
     const long long th = S.rx_tile_h, tw = 32 / S.rx_tile_h;
     long long tiles = 0, slots = 0, units = 0, chunks = 0, states = 0, atoms = 0, pixels = 0, grid_end = 0, rows = 0;
     for (int m = 0; m < n_mol; m++) {

@@ -73,13 +73,14 @@ __device__ __forceinline__ float node_xy(float p0, float da, float db, int ia, i
 
 // One CTA tile: a (blockDim.x x blockDim.y) patch of z-columns, ZB nodes each
 // starting at global layer ic0; nodes at layers >= zst_hi are not stored, the
-// rest go to out[idx], idx = ((ic - zst_lo)*ny + ib)*nx + ia.  PAIRED: the
-// x-paired layout, 2 float4 per node: node idx's value is written to
-// out[2*idx] and to out[2*idx_left + 1], idx_left its (x-1 mod nx) neighbour,
-// so out[2*idx .. 2*idx+1] = (value(x), value(x+1 mod nx)).
+// rest go to out[idx], idx = ((ic - zst_lo)*ny + ib)*nx + ia (LAYOUT 1).
+// LAYOUT 2, x-pairs: out[2*idx + dx] = value(x + dx mod nx), so a node's
+// value is also written to its x-1 neighbour's second slot.  LAYOUT 4,
+// xz-quads: out[4*idx + 2*dz + dx] = value(x + dx mod nx, z + dz mod nz_slab),
+// written to the four nodes whose quads contain it.
 // KIND: SPM_KIND_LJ / SPM_KIND_MORSE; ON: an on-node charge term exists;
 // NOFF: number of off-node sites.
-template <int KIND, bool ON, int NOFF, int ZB, bool PAIRED = false>
+template <int KIND, bool ON, int NOFF, int ZB, int LAYOUT = 1>
 __device__ __forceinline__ void build_tile(int na, const float4* __restrict__ atoms, const float* __restrict__ params,
                                            int pstride, float4* __restrict__ out, const GridGeom& G,
                                            const TipSites& S, int ia, int ib, int ic0, int zst_lo, int zst_hi) {
@@ -199,10 +200,19 @@ __device__ __forceinline__ void build_tile(int na, const float4* __restrict__ at
             // |E| > 100 cap of the reference builders (AFM.cl:1053-1054)
             const float renorm = __fdiv_rn(100.f, fabsf(o.w));
             if (renorm < 1.f) { o.x *= renorm; o.y *= renorm; o.z *= renorm; o.w *= renorm; }
-            const size_t row = ((size_t)(ic - zst_lo) * G.ny + ib) * G.nx;
-            if (PAIRED) {
+            const int zl = ic - zst_lo;
+            const size_t row = ((size_t)zl * G.ny + ib) * G.nx;
+            const int il = ia > 0 ? ia - 1 : G.nx - 1;
+            if (LAYOUT == 2) {
                 out[2 * (row + ia)] = o;
-                out[2 * (row + (ia > 0 ? ia - 1 : G.nx - 1)) + 1] = o;
+                out[2 * (row + il) + 1] = o;
+            } else if (LAYOUT == 4) {
+                const int nzs = zst_hi - zst_lo;
+                const size_t rowb = ((size_t)(zl > 0 ? zl - 1 : nzs - 1) * G.ny + ib) * G.nx;
+                out[4 * (row + ia) + 0] = o;
+                out[4 * (row + il) + 1] = o;
+                out[4 * (rowb + ia) + 2] = o;
+                out[4 * (rowb + il) + 3] = o;
             } else {
                 out[row + ia] = o;
             }
@@ -260,7 +270,7 @@ TipSites make_sites(const float* Qs, const float* QZs, bool& on, int& noff) {
 // ---- batched slabs ----------------------------------------------------------
 // One CTA per tile of the batch; tiles of a molecule are numbered x fastest,
 // then y, then z over ceil(nx/32) x ceil(ny/TY) x ceil(nz_slab/ZB).
-template <int KIND, bool ON, int NOFF, int ZB>
+template <int KIND, bool ON, int NOFF, int ZB, int LAYOUT>
 __global__ void __launch_bounds__(256)
 batch_grid_build_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float4* __restrict__ atoms,
                         const float* __restrict__ params, int pstride, float4* __restrict__ grid, TipSites S) {
@@ -282,8 +292,8 @@ batch_grid_build_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const
     G.dB = ld4f(D->dB);
     G.dC = ld4f(D->dC);
     const int ao = D->atom_off;
-    build_tile<KIND, ON, NOFF, ZB, true>(D->n_atoms, atoms + ao, params + (size_t)ao * pstride, pstride,
-                                         grid + 2 * D->grid_off,
+    build_tile<KIND, ON, NOFF, ZB, LAYOUT>(D->n_atoms, atoms + ao, params + (size_t)ao * pstride, pstride,
+                                           grid + LAYOUT * D->grid_off,
                                    G, S, bx * GB_TX + threadIdx.x, by * ty + threadIdx.y, z_lo + (int)bz * ZB, z_lo,
                                    z_lo + nzs);
 }
@@ -298,16 +308,23 @@ struct BatchLaunch {
     const float* params;
     int pstride;
     float4* grid;
+    int layout;  // float4 per node: 2 (x-pairs) or 4 (xz-quads)
 };
+
+template <int KIND, bool ON, int NOFF, int LAYOUT>
+void launch_batch_zl(int zb, const BatchLaunch& L, const TipSites& S) {
+    if (zb == 16)
+        batch_grid_build_kernel<KIND, ON, NOFF, 16, LAYOUT><<<L.blocks, L.block, 0, L.st>>>(
+            L.n_mol, L.mols, L.atoms, L.params, L.pstride, L.grid, S);
+    else
+        batch_grid_build_kernel<KIND, ON, NOFF, 8, LAYOUT><<<L.blocks, L.block, 0, L.st>>>(
+            L.n_mol, L.mols, L.atoms, L.params, L.pstride, L.grid, S);
+}
 
 template <int KIND, bool ON, int NOFF>
 void launch_batch_zb(int zb, const BatchLaunch& L, const TipSites& S) {
-    if (zb == 16)
-        batch_grid_build_kernel<KIND, ON, NOFF, 16><<<L.blocks, L.block, 0, L.st>>>(L.n_mol, L.mols, L.atoms, L.params,
-                                                                                    L.pstride, L.grid, S);
-    else
-        batch_grid_build_kernel<KIND, ON, NOFF, 8><<<L.blocks, L.block, 0, L.st>>>(L.n_mol, L.mols, L.atoms, L.params,
-                                                                                   L.pstride, L.grid, S);
+    if (L.layout == 4) launch_batch_zl<KIND, ON, NOFF, 4>(zb, L, S);
+    else launch_batch_zl<KIND, ON, NOFF, 2>(zb, L, S);
 }
 
 template <int KIND, bool ON>
@@ -345,6 +362,8 @@ extern "C" int spm_batch_grid_build(int kind, int n_mol, const spm_batch_mol* mo
     SPM_REQUIRE(shape->gb_ty == 2 || shape->gb_ty == 4 || shape->gb_ty == 8, "spm_batch_grid_build: gb_ty=%d",
                 shape->gb_ty);
     SPM_REQUIRE(shape->gb_zb == 8 || shape->gb_zb == 16, "spm_batch_grid_build: gb_zb=%d", shape->gb_zb);
+    SPM_REQUIRE(shape->grid_layout == 0 || shape->grid_layout == 1, "spm_batch_grid_build: grid_layout=%d",
+                shape->grid_layout);
     SPM_REQUIRE(n_tiles <= 0x7fffffffLL, "spm_batch_grid_build: %lld tiles exceed one launch", n_tiles);
     int noff = 0;
     bool on = false;
@@ -359,6 +378,7 @@ extern "C" int spm_batch_grid_build(int kind, int n_mol, const spm_batch_mol* mo
     L.params = params;
     L.pstride = (kind == SPM_KIND_MORSE) ? 4 : 2;
     L.grid = reinterpret_cast<float4*>(grid);
+    L.layout = shape->grid_layout ? 4 : 2;
     if (kind == SPM_KIND_MORSE) launch_batch_kind<SPM_KIND_MORSE>(on, noff, shape->gb_zb, L, S);
     else launch_batch_kind<SPM_KIND_LJ>(on, noff, shape->gb_zb, L, S);
     return check_launch("spm_batch_grid_build");

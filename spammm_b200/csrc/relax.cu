@@ -323,6 +323,7 @@ GridView make_view(const float* grid, int nx, int ny, int nz, const spm_scan_par
     GridView G;
     G.g = reinterpret_cast<const float4*>(grid);
     G.nx = nx; G.ny = ny; G.nz = nz;
+    G.z_lo = 0; G.nz_slab = nz; G.stride = 1;
     G.dA = make_float4(p->dinvA[0], p->dinvA[1], p->dinvA[2], p->dinvA[3]);
     G.dB = make_float4(p->dinvB[0], p->dinvB[1], p->dinvB[2], p->dinvB[3]);
     G.dC = make_float4(p->dinvC[0], p->dinvC[1], p->dinvC[2], p->dinvC[3]);
@@ -416,13 +417,13 @@ __device__ __forceinline__ bool next_batch_pixel(unsigned* counter, unsigned n_s
 // (0,0,1,dz)) on an axis-aligned slab: pp_iter with the frame rotations
 // dropped -- with an identity frame they change no value (the sign of an exact
 // zero aside) -- and c*surf reduced to its z part.
-template <typename IDX, bool CACHE>
+template <typename IDX, bool CACHE, int LAYOUT>
 __device__ __forceinline__ float4 sample_z(const AxisView& G, V3 p, TexelCache& T) {
-    if constexpr (CACHE) return interp_fe_cached<IDX, true>(G, p, T);
-    else return interp_fe_pair<IDX, true>(G, p);
+    if constexpr (CACHE) return interp_fe_cached<IDX, true, LAYOUT>(G, p, T);
+    else return interp_fe_cell<IDX, true, LAYOUT>(G, p);
 }
 
-template <typename IDX, bool CACHE>
+template <typename IDX, bool CACHE, int LAYOUT>
 __device__ __forceinline__ bool pp_iter_z(const AxisView& G, TexelCache& T, const spm_scan_params& P, V3 tip,
                                           V3& pos, V3& v, float& dt, float& damp, float4& fe, int& it, int& total_it,
                                           bool& conv) {
@@ -430,7 +431,7 @@ __device__ __forceinline__ bool pp_iter_z(const AxisView& G, TexelCache& T, cons
     if (it >= P.max_iter) return true;
     ++it;
     ++total_it;
-    fe = sample_z<IDX, CACHE>(G, pos, T);
+    fe = sample_z<IDX, CACHE, LAYOUT>(G, pos, T);
     if (fe.w != fe.w) return true;  // outside the slab (or a NaN grid): not converged
     const V3 ft = tip_force(sub3(pos, tip), ld4(P.stiffness), ld4(P.dpos0));
     V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
@@ -445,9 +446,10 @@ __device__ __forceinline__ bool pp_iter_z(const AxisView& G, TexelCache& T, cons
     return it >= P.max_iter;
 }
 
+template <int LAYOUT>
 __device__ __forceinline__ AxisView axis_view(const spm_batch_mol* D, const float* grid) {
     AxisView G;
-    G.g = reinterpret_cast<const float4*>(grid) + 2 * D->grid_off;  // x-paired slab
+    G.g = reinterpret_cast<const float4*>(grid) + LAYOUT * D->grid_off;
     G.nx = D->nx; G.ny = D->ny; G.nz = D->nz;
     G.z_lo = D->z_lo; G.nz_slab = D->nz_slab;
     G.fnx = (float)G.nx; G.fny = (float)G.ny; G.fnz = (float)G.nz;
@@ -461,7 +463,7 @@ __device__ __forceinline__ AxisView axis_view(const spm_batch_mol* D, const floa
 // (768 resident threads per SM); MINB = 4: 64 registers (1024 threads, a few
 // spilled values); CACHE: texels kept in registers across iterations (112
 // registers, MINB = 2).
-template <int MINB, bool CACHE>
+template <int MINB, bool CACHE, int LAYOUT>
 __global__ void __launch_bounds__(256, MINB)
 batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
                    const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
@@ -480,7 +482,7 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     int iz = 0, it = 0, total_it = 0;
     auto start = [&]() {
         const spm_batch_mol* D = mols + m;
-        G = axis_view(D, grid);
+        G = axis_view<LAYOUT>(D, grid);
         T.x0 = -1;  // new slab: nothing cached
         nzs = D->nz_steps;
         pix = D->pix_off + k;
@@ -499,8 +501,8 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     if (have) start();
     while (have) {
         bool conv;
-        if (pp_iter_z<unsigned, CACHE>(G, T, P, tip, pos, v, dt, damp, fe, it, total_it, conv)) {
-            if (!conv) fe = sample_z<unsigned, CACHE>(G, pos, T);  // the position moved after the last sample
+        if (pp_iter_z<unsigned, CACHE, LAYOUT>(G, T, P, tip, pos, v, dt, damp, fe, it, total_it, conv)) {
+            if (!conv) fe = sample_z<unsigned, CACHE, LAYOUT>(G, pos, T);  // the position moved after the last sample
             const long long o = sbase + iz;
             FEs[o] = fe;
             // all seven values finite <=> the sum of their products with zero is zero
@@ -554,8 +556,15 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     int th_log2 = 0;
     while ((1 << th_log2) < h) th_log2++;
     SPM_REQUIRE(shape->rx_regs >= 0 && shape->rx_regs <= 2, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
-    auto kern = shape->rx_regs == 2 ? batch_relax_kernel<2, true>
-                                    : (shape->rx_regs == 1 ? batch_relax_kernel<4, false> : batch_relax_kernel<3, false>);
+    SPM_REQUIRE(shape->grid_layout == 0 || shape->grid_layout == 1, "spm_batch_relax: grid_layout=%d",
+                shape->grid_layout);
+    auto kern = batch_relax_kernel<3, false, 2>;
+    if (shape->grid_layout == 0)
+        kern = shape->rx_regs == 2 ? batch_relax_kernel<2, true, 2>
+                                   : (shape->rx_regs == 1 ? batch_relax_kernel<4, false, 2> : batch_relax_kernel<3, false, 2>);
+    else
+        kern = shape->rx_regs == 2 ? batch_relax_kernel<2, true, 4>
+                                   : (shape->rx_regs == 1 ? batch_relax_kernel<4, false, 4> : batch_relax_kernel<3, false, 4>);
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||

@@ -27,10 +27,11 @@ __device__ __forceinline__ int find_mol(const spm_batch_mol* __restrict__ mols, 
 __device__ __forceinline__ float4 ld4f(const float* a) { return make_float4(__ldg(a), __ldg(a + 1), __ldg(a + 2), __ldg(a + 3)); }
 
 // Sampling view of a molecule's slab (full-grid coordinates, stored layers
-// only; G.g = the base of its x-paired nodes, 2 float4 per node).
-__device__ __forceinline__ GridView slab_view(const spm_batch_mol& D, const float* grid) {
+// only; stride float4 per stored node: 2 x-pairs, 4 xz-quads, value first).
+__device__ __forceinline__ GridView slab_view(const spm_batch_mol& D, const float* grid, int stride = 2) {
     GridView G;
-    G.g = reinterpret_cast<const float4*>(grid) + 2 * D.grid_off;
+    G.g = reinterpret_cast<const float4*>(grid) + (long long)stride * D.grid_off;
+    G.stride = stride;
     G.nx = D.nx; G.ny = D.ny; G.nz = D.nz;
     G.dA = ld4f(D.dinvA);
     G.dB = ld4f(D.dinvB);

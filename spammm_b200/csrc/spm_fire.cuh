@@ -122,6 +122,7 @@ struct GridView {
     int nx, ny, nz;
     float4 dA, dB, dC;  // normalized-coordinate transform rows
     int z_lo, nz_slab;  // SLAB views: only layers [z_lo, z_lo + nz_slab) are stored
+    int stride;         // SLAB views: float4 per stored node (2 x-pairs, 4 xz-quads); node value first
 };
 
 // interpFE: exact FP32 trilinear sample with periodic wrap.  IDX is the type
@@ -232,12 +233,36 @@ __device__ __forceinline__ void ld_pair(const float4* p, ulonglong2& lo, ulonglo
     hi = make_ulonglong2(c, d);
 }
 
-// interp_fe_axis on an x-paired grid (G.g = the pair base: node idx at
-// G.g[2*idx], its +x neighbour (mod nx) at G.g[2*idx + 1]): one 256-bit load
-// per (y, z) row of the texel cell instead of two 128-bit loads; the same
-// operations on the same values, so the same sample.
-template <typename IDX, bool SLAB>
-__device__ __forceinline__ float4 interp_fe_pair(const AxisView& G, V3 p) {
+// The eight texels of cell (x0, y0..y1, z0..z1) of a slab in the x-pair
+// (LAYOUT 2: node idx at G.g[2*idx], its +x neighbour after it) or xz-quad
+// (LAYOUT 4: G.g[4*idx + 2*dz + dx]) layout, as packed channel pairs.  With
+// xz-quads the cell's 8 texels are two 64-byte chunks (rows y0 and y1).
+template <int LAYOUT, typename IDX>
+__device__ __forceinline__ void load_cell(const AxisView& G, int x0, int y0, int y1, int z0, int z1,
+                                          ulonglong2& f000, ulonglong2& f100, ulonglong2& f010, ulonglong2& f110,
+                                          ulonglong2& f001, ulonglong2& f101, ulonglong2& f011, ulonglong2& f111) {
+    if (LAYOUT == 4) {
+        const IDX q0 = ((IDX)z0 * G.ny + y0) * G.nx + x0, q1 = ((IDX)z0 * G.ny + y1) * G.nx + x0;
+        ld_pair(G.g + 4 * q0, f000, f100);
+        ld_pair(G.g + 4 * q0 + 2, f001, f101);
+        ld_pair(G.g + 4 * q1, f010, f110);
+        ld_pair(G.g + 4 * q1 + 2, f011, f111);
+    } else {
+        const IDX r00 = ((IDX)z0 * G.ny + y0) * G.nx + x0, r10 = ((IDX)z0 * G.ny + y1) * G.nx + x0;
+        const IDX r01 = ((IDX)z1 * G.ny + y0) * G.nx + x0, r11 = ((IDX)z1 * G.ny + y1) * G.nx + x0;
+        ld_pair(G.g + 2 * r00, f000, f100);
+        ld_pair(G.g + 2 * r10, f010, f110);
+        ld_pair(G.g + 2 * r01, f001, f101);
+        ld_pair(G.g + 2 * r11, f011, f111);
+    }
+}
+
+// interp_fe_axis on an x-paired (LAYOUT 2) or xz-quad (LAYOUT 4) slab: the
+// same texel addressing and the same lerps on the same values, so the same
+// sample.  (In a slab the cell's upper layer is z0+1, or layer 0 when a
+// full-grid slab wraps; both layouts store exactly that layer.)
+template <typename IDX, bool SLAB, int LAYOUT>
+__device__ __forceinline__ float4 interp_fe_cell(const AxisView& G, V3 p) {
     const float u = __fmaf_rn(p.x, G.ax, G.aw);
     const float v = __fmaf_rn(p.y, G.by, G.bw);
     const float w = __fmaf_rn(p.z, G.cz, G.cw);
@@ -246,7 +271,7 @@ __device__ __forceinline__ float4 interp_fe_pair(const AxisView& G, V3 p) {
     bool ok = tex_axis(u, G.nx, G.fnx, x0, x1, ax);
     ok = tex_axis(v, G.ny, G.fny, y0, y1, ay) && ok;
     ok = tex_axis(w, G.nz, G.fnz, z0, z1, az) && ok;
-    (void)x1;  // the pair holds it
+    (void)x1;  // the pair / quad holds it
     if (SLAB) {
         z0 -= G.z_lo;
         z1 -= G.z_lo;
@@ -257,13 +282,8 @@ __device__ __forceinline__ float4 interp_fe_pair(const AxisView& G, V3 p) {
         return make_float4(nan, nan, nan, nan);
     }
     const f2 AX = bc(ax), MX = bc(1.f - ax), AY = bc(ay), MY = bc(1.f - ay), AZ = bc(az), MZ = bc(1.f - az);
-    const IDX r00 = ((IDX)z0 * G.ny + y0) * G.nx + x0, r10 = ((IDX)z0 * G.ny + y1) * G.nx + x0;
-    const IDX r01 = ((IDX)z1 * G.ny + y0) * G.nx + x0, r11 = ((IDX)z1 * G.ny + y1) * G.nx + x0;
     ulonglong2 f000, f100, f010, f110, f001, f101, f011, f111;
-    ld_pair(G.g + 2 * r00, f000, f100);
-    ld_pair(G.g + 2 * r10, f010, f110);
-    ld_pair(G.g + 2 * r01, f001, f101);
-    ld_pair(G.g + 2 * r11, f011, f111);
+    load_cell<LAYOUT, IDX>(G, x0, y0, y1, z0, z1, f000, f100, f010, f110, f001, f101, f011, f111);
     const ulonglong2 c00 = lerp_pk(AX, MX, f000, f100);
     const ulonglong2 c10 = lerp_pk(AX, MX, f010, f110);
     const ulonglong2 c01 = lerp_pk(AX, MX, f001, f101);
@@ -285,9 +305,9 @@ struct TexelCache {
     ulonglong2 f000, f100, f010, f110, f001, f101, f011, f111;
 };
 
-// interp_fe_pair with a TexelCache: identical values (the same texels, the
+// interp_fe_cell with a TexelCache: identical values (the same texels, the
 // same lerps); loads only when the cell differs from the cached one.
-template <typename IDX, bool SLAB>
+template <typename IDX, bool SLAB, int LAYOUT>
 __device__ __forceinline__ float4 interp_fe_cached(const AxisView& G, V3 p, TexelCache& T) {
     const float u = __fmaf_rn(p.x, G.ax, G.aw);
     const float v = __fmaf_rn(p.y, G.by, G.bw);
@@ -308,12 +328,8 @@ __device__ __forceinline__ float4 interp_fe_cached(const AxisView& G, V3 p, Texe
         return make_float4(nan, nan, nan, nan);
     }
     if (x0 != T.x0 || y0 != T.y0 || z0 != T.z0) {
-        const IDX r00 = ((IDX)z0 * G.ny + y0) * G.nx + x0, r10 = ((IDX)z0 * G.ny + y1) * G.nx + x0;
-        const IDX r01 = ((IDX)z1 * G.ny + y0) * G.nx + x0, r11 = ((IDX)z1 * G.ny + y1) * G.nx + x0;
-        ld_pair(G.g + 2 * r00, T.f000, T.f100);
-        ld_pair(G.g + 2 * r10, T.f010, T.f110);
-        ld_pair(G.g + 2 * r01, T.f001, T.f101);
-        ld_pair(G.g + 2 * r11, T.f011, T.f111);
+        load_cell<LAYOUT, IDX>(G, x0, y0, y1, z0, z1, T.f000, T.f100, T.f010, T.f110, T.f001, T.f101, T.f011,
+                               T.f111);
         T.x0 = x0;
         T.y0 = y0;
         T.z0 = z0;
