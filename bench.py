@@ -304,8 +304,12 @@ def run_ours(args, rank, world, local_rank):
             df = AFM.compute_df_amp_dir(F, spacing, (0., 0., 1.), cfg.amp)
             return F, disp, df
 
-        for _ in range(max(2, args.warmup // 2)):  # two: the pinned host buffers of two live results are cached
-            e2e_step()
+        # warm-up holds each result until the next step returns, as the timed loop does: the pinned host
+        # buffers of two live results are then allocated (cudaHostAlloc) before the timed region
+        held = None
+        for _ in range(max(3, args.warmup)):
+            held = e2e_step()
+        del held
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
