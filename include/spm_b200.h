@@ -302,10 +302,13 @@ long long spm_adjoint_grid_scratch_bytes(int n_atoms, long long n_state);
  * caller; launches take the DEVICE copy.  Layouts:
  *   atoms  (total_atoms,4) x,y,z,Q;  params (total_atoms,2) LJ c6,c12 or
  *          (total_atoms,4) Morse R0,E0,K,-
- *   grid   x-paired float4 slabs: node idx = ((z - z_lo)*ny + y)*nx + x of a
- *          molecule holds 2 float4 at grid[2*(grid_off + idx)]: (value(x,y,z),
- *          value((x+1) mod nx, y, z)), so a trilinear cell row is one 32-byte
- *          load; the buffer holds 2*totals[7] float4
+ *   grid   slabs in one of two layouts (spm_batch_shape.grid_layout), node
+ *          idx = ((z - z_lo)*ny + y)*nx + x of a molecule, zl = z - z_lo:
+ *          0 x-pairs: grid[2*(grid_off + idx) + dx] = value((x+dx) mod nx, y, z),
+ *            a trilinear cell row is one 32-byte load; 2*totals[7] float4;
+ *          1 xz-quads: grid[4*(grid_off + idx) + 2*dz + dx] =
+ *            value((x+dx) mod nx, y, z_lo + (zl+dz) mod nz_slab), a cell's
+ *            two (y) rows are two 64-byte chunks; 4*totals[7] float4
  *   points (total_pixels,4) tip start positions (raster ix-major when
  *          raster_ny > 0, as spm_relax_ex)
  *   states (total_states,4) per molecule n_scan x nz_steps, z-step fastest */
@@ -340,6 +343,8 @@ typedef struct spm_batch_shape {
     int rx_regs;        /* relaxation kernel variant: 0 = 80 registers per thread, 1 = 64 (more warps,
                            some spills), 2 = the cell's 8 texels kept in registers across FIRE
                            iterations (112 registers, loads only when the cell changes) */
+    int grid_layout;    /* slab layout: 0 = x-pairs (2 float4 per node), 1 = xz-quads (4 float4 per
+                           node: half the cache lines per sample, twice the memory) */
 } spm_batch_shape;
 
 spm_batch_shape spm_batch_default_shape(void);
@@ -387,9 +392,10 @@ int spm_batch_df_loss_seed(int n_mol, const spm_batch_mol* mols, long long n_chu
 long long spm_batch_loss_scratch_bytes(long long n_chunks, int n_mol);
 
 /* spm_adjoint_grid_state over the batch (same outputs per state). */
-int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_states, const float* grid,
-                            const float* points, const spm_scan_params* p, const float* PPs,
-                            const float* dL_dFEs, float* ubar, float* dk, float* diag, void* stream);
+int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_states,
+                            const spm_batch_shape* shape, const float* grid, const float* points,
+                            const spm_scan_params* p, const float* PPs, const float* dL_dFEs, float* ubar,
+                            float* dk, float* diag, void* stream);
 
 /* spm_adjoint_grid_params over the batch, node-major: grad (total_atoms,6)
  * double as spm_adjoint_grid_params, dk_sum double[4] summed over the whole

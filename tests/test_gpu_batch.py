@@ -46,9 +46,7 @@ def test_batch_forward_matches_per_molecule(cuda, kind):
         D = b.desc(i)
         full = grid[D.z_lo:D.z_lo + D.nz_slab]
         assert torch.equal(b.slab(i), full), f"molecule {i}: slab differs from full grid"
-        n = D.nx * D.ny * D.nz_slab
-        hi = b.grid.view(-1, 2, 4)[D.grid_off:D.grid_off + n, 1].reshape(D.nz_slab, D.ny, D.nx, 4)
-        assert torch.equal(hi, torch.roll(full, -1, dims=2)), f"molecule {i}: x-pair halves differ"
+        assert torch.equal(b.slab(i, 1), torch.roll(full, -1, dims=2)), f"molecule {i}: x-pair halves differ"
         assert (b.pps(i)[..., 3] > 0).all(), f"molecule {i}: a stroke left the slab or did not converge"
         assert torch.equal(b.fes(i), FEs) and torch.equal(b.pps(i), PPs), f"molecule {i}: relaxation differs"
         # df of the stroke, ascending z (dr = |dtip|), as the single-volume call
@@ -102,7 +100,8 @@ def test_batch_shapes_give_same_results(cuda):
     L = _lib.lib()
     for kw in (dict(gb_ty=2, gb_zb=16, rx_threads=64, rx_tile_h=1, adj_chunk=1024),
                dict(gb_ty=8, gb_zb=8, rx_threads=256, rx_tile_h=32, rx_ctas_per_sm=1, adj_chunk=65536, rx_regs=1),
-               dict(rx_threads=128, rx_tile_h=4, rx_regs=2)):
+               dict(rx_threads=128, rx_tile_h=4, rx_regs=2),
+               dict(grid_layout=1), dict(grid_layout=1, rx_regs=2), dict(grid_layout=1, rx_regs=1, gb_zb=16)):
         s = L.spm_batch_default_shape()
         for k, v in kw.items():
             setattr(s, k, v)
@@ -110,7 +109,14 @@ def test_batch_shapes_give_same_results(cuda):
         b.set_target_states(ref.target)
         b.forward_adjoint()
         torch.cuda.synchronize()
-        assert torch.equal(b.grid, ref.grid) and torch.equal(b.FEs, ref.FEs) and torch.equal(b.PPs, ref.PPs)
+        for i in range(len(items)):
+            assert torch.equal(b.slab(i), ref.slab(i)), (kw, i)
+            if b.shape.grid_layout == 1:  # xz-quads: the (x+1), (z+1), (x+1,z+1) neighbours
+                full = ref.slab(i)
+                assert torch.equal(b.slab(i, 1), torch.roll(full, -1, dims=2))
+                assert torch.equal(b.slab(i, 2), torch.roll(full, -1, dims=0))
+                assert torch.equal(b.slab(i, 3), torch.roll(full, (-1, -1), dims=(0, 2)))
+        assert torch.equal(b.FEs, ref.FEs) and torch.equal(b.PPs, ref.PPs)
         assert torch.equal(b.loss, ref.loss) and torch.equal(b.ubar, ref.ubar)
         torch.testing.assert_close(b.grad, ref.grad, rtol=1e-6, atol=1e-9 * float(ref.grad.abs().max()))
 
