@@ -345,6 +345,9 @@ typedef struct spm_batch_shape {
                            iterations (112 registers, loads only when the cell changes) */
     int grid_layout;    /* slab layout: 0 = x-pairs (2 float4 per node), 1 = xz-quads (4 float4 per
                            node: half the cache lines per sample, twice the memory) */
+    int rx_sync;        /* relaxation schedule: 0 = every lane draws its next pixel when its stroke ends,
+                           1 = a warp draws a pixel tile and its lanes step down the z-steps together
+                           (all lanes sample the same z-layer of neighbouring pixels) */
 } spm_batch_shape;
 
 spm_batch_shape spm_batch_default_shape(void);
@@ -408,9 +411,13 @@ int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_st
  *      non-zero adjoint-grid nodes in shared memory and every thread owns one
  *      atom (and a phase of the chunk), evaluating the pair-law derivatives of
  *      its atom at each staged node; per-(chunk, atom) FP64 partials are folded
- *      per atom in a fixed order.
+ *      per atom in a fixed order.  Blocks of 1024 nodes that no state touched
+ *      are skipped, and every node read is zeroed again.
  * totals: the HOST array of spm_batch_prepare; scratch (device) >=
- * spm_batch_adjoint_scratch_bytes(totals, n_mol). */
+ * spm_batch_adjoint_scratch_bytes(totals, n_mol).  The scratch keeps the
+ * cleared adjoint grid between calls, with a marker that says it is clear:
+ * reuse one scratch buffer call after call; any other content (a fresh
+ * allocation, a call that failed half-way) is cleared by the next call. */
 int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol* mols, const long long* totals,
                              const spm_batch_shape* shape, const float* atoms, const float* params,
                              const float* Qs, const float* QZs, const float* PPs, const float* ubar,

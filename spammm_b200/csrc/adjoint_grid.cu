@@ -436,10 +436,27 @@ __device__ __forceinline__ int scale_exp(unsigned umax_bits) {
 }
 __device__ __forceinline__ double pow2(int k) { return __longlong_as_double((long long)(1023 + k) << 52); }
 
+constexpr int NM_BLOCK_LOG2 = 10;  // touched-block flags: one byte per 1024 adjoint-grid nodes
+constexpr unsigned long long ADJ_CLEAN = 0x4e41454c434d5053ull;  // marker: the adjoint grid is all zero
+constexpr unsigned long long ADJ_DIRTY = 1ull;
+
+// Zeroes the fixed-point adjoint grid (n2 16-byte pairs) unless its marker
+// says it is clear.  The node kernel zeroes every node it reads, so after a
+// completed call the grid is clear again; only a first use, or a call that
+// stopped between the scatter and the node kernel, leaves work here.
+__global__ void __launch_bounds__(256)
+adj_clear_kernel(ulonglong2* __restrict__ gq, long long n2, const unsigned long long* __restrict__ mark) {
+    if (*mark == ADJ_CLEAN) return;
+    for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < n2; i += (long long)gridDim.x * 256)
+        gq[i] = make_ulonglong2(0ull, 0ull);
+}
+
 // CTA per 256-state chunk: per-molecule max |ubar| (as float bits; order-free).
+// Block 0 marks the adjoint grid dirty (the scatter follows).
 __global__ void __launch_bounds__(256)
 batch_ubar_max_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float4* __restrict__ ubar,
-                      unsigned* __restrict__ umax) {
+                      unsigned* __restrict__ umax, unsigned long long* __restrict__ mark) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *mark = ADJ_DIRTY;
     __shared__ float s_m[8];
     const long long ch = blockIdx.x;
     const int m = SPM_MOL_BY(chunk_off, mols, n_mol, ch);
@@ -470,7 +487,7 @@ batch_ubar_max_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const f
 __global__ void __launch_bounds__(256)
 batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states,
                      const float4* __restrict__ PPs, const float4* __restrict__ ubar, const unsigned* __restrict__ umax,
-                     unsigned long long* __restrict__ gq) {
+                     unsigned long long* __restrict__ gq, unsigned char* __restrict__ flags) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const long long st = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -481,6 +498,7 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
     long long stroke = -1;
     int nx = 0, ny = 0, z_lo = 0;
     unsigned long long* base = gq;
+    long long goff = 0;
     double scale = 0.0;
     if (valid) {
         const int m = SPM_MOL_BY(state_off, mols, n_mol, st);
@@ -492,6 +510,7 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
         stroke = D->pix_off + (st - D->state_off) / D->nz_steps;
         nx = G.nx; ny = G.ny; z_lo = G.z_lo;
         base = gq + (size_t)D->grid_off * 4;
+        goff = D->grid_off;
         scale = pow2(42 - scale_exp(__ldg(umax + m)));
     }
     // merge tests against the next lane (it gives me its upper layer) and the previous one (I give mine)
@@ -512,6 +531,20 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
     for (int c = 0; c < 8; c++) {
         const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
         w[c] = valid ? (i ? C.ax : 1.f - C.ax) * (j ? C.ay : 1.f - C.ay) * (k ? C.az : 1.f - C.az) : 0.f;
+    }
+    if (valid) {
+        // flag the 1024-node blocks of the cell's corners for the node kernel: a read first, a
+        // store only if unset (the same few flag bytes are hit by every state of a region); an
+        // upper layer given to the previous lane is that lane's lower layer, flagged there
+        long long last = -1;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
+            if (k == 1 && given) break;
+            const long long blk = (goff + ((long long)(C.z[k] - z_lo) * ny + C.y[j]) * nx + C.x[i]) >> NM_BLOCK_LOG2;
+            if (blk != last && !flags[blk]) flags[blk] = 1;
+            last = blk;
+        }
     }
     const float ubc[4] = {ub.x, ub.y, ub.z, ub.w};
 #pragma unroll
@@ -577,86 +610,123 @@ NodeSites make_node_sites(const float* Qs, const float* QZs) {
     return S;
 }
 
-// pair_grad's derivatives (same pair laws, same formulas) evaluated the way the
-// grid build evaluates the forward: one MUFU rsqrt per pair for the pair law
-// and the on-node charges together, MUFU ex2 for Morse; FP32, added to acc.
-template <int KIND>
-__device__ __forceinline__ void pair_adj_fast(float4 np, float4 at, float p1, float p2, float p3, const NodeSites& S,
-                                              float4 g, float* acc) {
-    const float dx = np.x - at.x, dy = np.y - at.y, dz = np.z - at.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, R2SAFE)));
-    const float rs = mufu_rsqrt(r2);
-    const float ir2 = rs * rs;
-    const float du = fmaf(dx, g.x, fmaf(dy, g.y, dz * g.z));
-    const float uE = g.w;
-    float s, sp, gp1, gp2;
+__device__ __forceinline__ f2 rsqrt2(f2 x) {
+    float a, b;
+    upk(x, a, b);
+    return pk(mufu_rsqrt(a), mufu_rsqrt(b));
+}
+__device__ __forceinline__ f2 ex2_2(f2 x) {
+    float a, b;
+    upk(x, a, b);
+    return pk(mufu_ex2(a), mufu_ex2(b));
+}
+
+// Per-atom constants of the packed pair derivatives (both lanes equal).
+struct AtomC {
+    f2 x, y, z;      // position
+    f2 c0, c1, c2, c3;  // LJ: 12 c12, -6 c6, 168 c12, -48 c6; Morse: K log2e, -K R0 log2e, -2 K E0, 2 K^2 E0
+    f2 c4;           // Morse: -2 K
+    f2 qw;           // Q * qon (on-node tip charges)
+    float q;         // Q
+};
+
+// Derivatives of the pair laws of the grid build (LJ / Morse + point-charge
+// Coulomb, R2SAFE-softened, as pair_grad) at two nodes per call, contracted
+// with the nodes' adjoint vectors g = (gx,gy,gz,gw):
+//   acc[0..2] += dF/d(atom position)^T g   acc[3], acc[4] += dF/d(pair params)^T g
+//   acc[5]    += dF/d(atom charge)^T g
+// with Blackwell's packed FP32 (two nodes per instruction), one MUFU rsqrt per
+// node for the pair law and the on-node charges together, MUFU ex2 for Morse.
+// LJ's acc[3] is accumulated negated (the sign is applied when it is folded).
+template <int KIND, bool ON>
+__device__ __forceinline__ void pair_adj2(f2 nx, f2 ny, f2 nz, f2 gx, f2 gy, f2 gz, f2 gw, const AtomC& C,
+                                          const NodeSites& S, f2* acc) {
+    const f2 dx = sub2(nx, C.x), dy = sub2(ny, C.y), dz = sub2(nz, C.z);
+    const f2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, bc(R2SAFE))));
+    const f2 rs = rsqrt2(r2);
+    const f2 ir2 = mul2(rs, rs);
+    const f2 du = fma2(dx, gx, fma2(dy, gy, mul2(dz, gz)));
+    f2 s, sp2;  // sp2 = -2 s'(r)/r: the Hessian's radial term with the -2 of A folded in
     if (KIND == SPM_KIND_LJ) {
-        const float c6 = p1, c12 = p2;
-        const float ir6 = ir2 * ir2 * ir2;
-        const float ir8 = ir6 * ir2;
-        const float ir14 = ir8 * ir6;
-        s = fmaf(12.f * c12, ir14, -6.f * c6 * ir8);
-        sp = fmaf(-84.f * c12, ir14, 24.f * c6 * ir8) * ir2;
-        gp1 = fmaf(du, -6.f * ir8, -uE * ir6);
-        gp2 = fmaf(du, 12.f * ir14, uE * ir6 * ir6);
+        const f2 ir6 = mul2(mul2(ir2, ir2), ir2);
+        const f2 ir8 = mul2(ir6, ir2);
+        const f2 ir14 = mul2(ir8, ir6);
+        s = fma2(C.c0, ir14, mul2(C.c1, ir8));                // 12 c12 ir14 - 6 c6 ir8
+        sp2 = mul2(fma2(C.c2, ir14, mul2(C.c3, ir8)), ir2);   // (168 c12 ir14 - 48 c6 ir8) ir2
+        acc[3] = fma2(gw, ir6, fma2(du, mul2(bc(6.f), ir8), acc[3]));      // -(d/dc6)
+        acc[4] = fma2(gw, mul2(ir6, ir6), fma2(du, mul2(bc(12.f), ir14), acc[4]));
     } else {
-        const float R0 = p1, E0 = p2, K = p3;
-        const float r = r2 * rs;
-        const float e = mufu_ex2(K * LOG2E * (r - R0));
-        const float em1 = e - 1.f;
-        const float Ep = 2.f * K * E0 * e * em1;
-        const float Epp = 2.f * K * K * E0 * e * (2.f * e - 1.f);
-        s = -Ep * rs;
-        sp = -(Epp * rs - Ep * ir2) * 0.5f * rs;
-        gp1 = fmaf(du, Epp * rs, -uE * Ep);
-        gp2 = fmaf(du, -2.f * K * e * em1 * rs, uE * e * (e - 2.f));
+        const f2 r = mul2(r2, rs);
+        const f2 e = ex2_2(fma2(C.c0, r, C.c1));              // exp(K (r - R0))
+        const f2 em1 = sub2(e, bc(1.f));
+        const f2 nEp = mul2(mul2(C.c2, e), em1);              // -E'
+        const f2 Epp = mul2(mul2(C.c3, e), fma2(bc(2.f), e, bc(-1.f)));
+        s = mul2(nEp, rs);
+        sp2 = mul2(fma2(Epp, rs, mul2(nEp, ir2)), rs);
+        acc[3] = fma2(gw, nEp, fma2(mul2(du, Epp), rs, acc[3]));
+        acc[4] = fma2(mul2(gw, e), sub2(e, bc(2.f)), fma2(mul2(du, mul2(mul2(C.c4, e), em1)), rs, acc[4]));
     }
-    float gq = 0.f;
-    if (S.qon != 0.f) {
-        const float qr = S.qon * rs;
-        const float sk = qr * at.w * ir2;
-        s += sk;
-        sp = fmaf(-1.5f * sk, ir2, sp);
-        gq = fmaf(du, qr * ir2, uE * qr);
+    if (ON) {
+        const f2 qr = mul2(bc(S.qon), rs);
+        const f2 sk = mul2(mul2(C.qw, rs), ir2);
+        s = add2(s, sk);
+        sp2 = fma2(mul2(bc(3.f), sk), ir2, sp2);
+        acc[5] = fma2(gw, qr, fma2(du, mul2(qr, ir2), acc[5]));
     }
-    const float A = fmaf(uE, s, -2.f * sp * du);
-    acc[0] += fmaf(A, dx, -s * g.x);
-    acc[1] += fmaf(A, dy, -s * g.y);
-    acc[2] += fmaf(A, dz, -s * g.z);
-    acc[3] += gp1;
-    acc[4] += gp2;
+    const f2 A = fma2(gw, s, mul2(sp2, du));
+    const f2 ns = mul2(s, bc(-1.f));
+    acc[0] = fma2(A, dx, fma2(ns, gx, acc[0]));
+    acc[1] = fma2(A, dy, fma2(ns, gy, acc[1]));
+    acc[2] = fma2(A, dz, fma2(ns, gz, acc[2]));
     for (int k = 0; k < S.noff; k++) {
-        const float dk = dz + S.qz[k];
-        const float rk = mufu_rsqrt(fmaf(dx, dx, fmaf(dy, dy, fmaf(dk, dk, R2SAFE))));
-        const float irk2 = rk * rk;
-        const float qr = S.qs[k] * rk;
-        const float sk = qr * at.w * irk2;
-        const float duk = fmaf(dx, g.x, fmaf(dy, g.y, dk * g.z));
-        const float Ak = fmaf(uE, sk, 3.f * sk * irk2 * duk);
-        acc[0] += fmaf(Ak, dx, -sk * g.x);
-        acc[1] += fmaf(Ak, dy, -sk * g.y);
-        acc[2] += fmaf(Ak, dk, -sk * g.z);
-        gq += fmaf(duk, qr * irk2, uE * qr);
+        const f2 dk = add2(dz, bc(S.qz[k]));
+        const f2 rk = rsqrt2(fma2(dx, dx, fma2(dy, dy, fma2(dk, dk, bc(R2SAFE)))));
+        const f2 irk2 = mul2(rk, rk);
+        const f2 qr = mul2(bc(S.qs[k]), rk);
+        const f2 sk = mul2(mul2(qr, bc(C.q)), irk2);
+        const f2 duk = fma2(dx, gx, fma2(dy, gy, mul2(dk, gz)));
+        const f2 Ak = fma2(gw, sk, mul2(mul2(bc(3.f), sk), mul2(irk2, duk)));
+        const f2 nsk = mul2(sk, bc(-1.f));
+        acc[0] = fma2(Ak, dx, fma2(nsk, gx, acc[0]));
+        acc[1] = fma2(Ak, dy, fma2(nsk, gy, acc[1]));
+        acc[2] = fma2(Ak, dk, fma2(nsk, gz, acc[2]));
+        acc[5] = fma2(gw, qr, fma2(duk, mul2(qr, irk2), acc[5]));
     }
-    acc[5] += gq;
 }
 
 
+__device__ __forceinline__ f2 lds2(const float* p) { return *reinterpret_cast<const f2*>(p); }
+
+// Dynamic shared memory of batch_adjoint_nodes_kernel: x, y, z, gx, gy, gz, gw
+// of up to 2*NM_STAGE staged nodes (+1 zero-weight pad node), the phase
+// partials and the double-buffered warp counts of the compaction scan.
+constexpr int NM_BUF = 2 * NM_STAGE + 2;
+constexpr size_t NM_SMEM = 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(double) + 2 * (NM_THREADS / 32) * sizeof(int);
+
 // CTA per node unit (molecule, `chunk` consecutive slab nodes).  Non-zero
-// adjoint-grid nodes are compacted into shared memory; thread t owns atom
-// a0 + t % nag and every P-th staged node (P = 256 / nag phases), so the
+// adjoint-grid nodes are compacted into shared memory (one float array per
+// component, so nodes 2i and 2i+1 load as one packed pair); thread t owns atom
+// a0 + t % nag and every P-th staged node pair (P = 256 / nag phases), so the
 // atom's derivative sums stay in its registers: no atomics, no cross-thread
 // reduction until the phases are folded once per unit.
-template <int KIND>
-__global__ void __launch_bounds__(NM_THREADS, 3)
+//   * 1024-node blocks that no state touched (flags, set by the scatter) are
+//     skipped without being read;
+//   * the non-zero nodes of consecutive blocks accumulate in shared memory
+//     until at least NM_STAGE are staged, so every compute phase between two
+//     barriers is dense;
+//   * every non-zero node is zeroed after it is staged (by the last atom
+//     group), so the adjoint grid is left cleared for the next call.
+template <int KIND, bool ON>
+__global__ void __launch_bounds__(NM_THREADS, 2)
 batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk,
                            const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
-                           NodeSites S, const unsigned long long* __restrict__ gq,
+                           NodeSites S, unsigned long long* __restrict__ gq, const unsigned char* __restrict__ flags,
                            const unsigned* __restrict__ umax, double* __restrict__ partial) {
-    __shared__ float4 s_pos[NM_STAGE];
-    __shared__ float4 s_g[NM_STAGE];
-    __shared__ double red[6][NM_THREADS];
-    __shared__ int s_wsum[NM_THREADS / 32];
+    extern __shared__ __align__(16) unsigned char nm_smem[];
+    float(*s_n)[NM_BUF] = reinterpret_cast<float(*)[NM_BUF]>(nm_smem);
+    double(*red)[NM_THREADS] = reinterpret_cast<double(*)[NM_THREADS]>(nm_smem + 7 * NM_BUF * sizeof(float));
+    int(*s_wsum)[NM_THREADS / 32] = reinterpret_cast<int(*)[NM_THREADS / 32]>(
+        nm_smem + 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(double));
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const long long unit = blockIdx.x;
     const int m = SPM_MOL_BY(unit_off, mols, n_mol, unit);
@@ -673,8 +743,10 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
     NG.dB = ld4f(D->dB);
     NG.dC = ld4f(D->dC);
     const double inv_scale = pow2(scale_exp(__ldg(umax + m)) - 42);
-    const ulonglong2* q2 = reinterpret_cast<const ulonglong2*>(gq + (size_t)D->grid_off * 4);
+    ulonglong2* q2 = reinterpret_cast<ulonglong2*>(gq + (size_t)D->grid_off * 4);
+    const long long goff = D->grid_off;
     for (int a0 = 0; a0 < na; a0 += NM_THREADS) {
+        const bool last_group = a0 + NM_THREADS >= na;
         const int nag = na - a0 < NM_THREADS ? na - a0 : NM_THREADS;
         const int P = NM_THREADS / nag;
         const bool act = t < nag * P;
@@ -683,8 +755,69 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
         const float4 at = __ldg(atoms + ga);
         const float* pr = params + (size_t)ga * pstride;
         const float p1 = __ldg(pr + 0), p2 = __ldg(pr + 1), p3 = (pstride > 2) ? __ldg(pr + 2) : 0.f;
+        AtomC C;
+        C.x = bc(at.x);
+        C.y = bc(at.y);
+        C.z = bc(at.z);
+        C.q = at.w;
+        C.qw = bc(at.w * S.qon);
+        if (KIND == SPM_KIND_LJ) {  // p1 = c6, p2 = c12
+            C.c0 = bc(12.f * p2);
+            C.c1 = bc(-6.f * p1);
+            C.c2 = bc(168.f * p2);
+            C.c3 = bc(-48.f * p1);
+            C.c4 = bc(0.f);
+        } else {  // p1 = R0, p2 = E0, p3 = K
+            C.c0 = bc(p3 * LOG2E);
+            C.c1 = bc(-p3 * p1 * LOG2E);
+            C.c2 = bc(-2.f * p3 * p2);
+            C.c3 = bc(2.f * p3 * p3 * p2);
+            C.c4 = bc(-2.f * p3);
+        }
         double acc[6] = {0, 0, 0, 0, 0, 0};
-        for (long long b0 = n0; b0 < n1; b0 += NM_STAGE) {
+        // the staged nodes' derivative sums: FP32 over NM_FLUSH pairs, then FP64
+        auto compute = [&](int L) {
+            if (t == 0 && (L & 1)) {  // pad to whole pairs: a distant node of zero weight adds +-0
+#pragma unroll
+                for (int c = 0; c < 3; c++) s_n[c][L] = 1e4f;
+#pragma unroll
+                for (int c = 3; c < 7; c++) s_n[c][L] = 0.f;
+            }
+            __syncthreads();
+            if (act) {
+                const f2 zero = bc(0.f);
+                f2 a32[6] = {zero, zero, zero, zero, zero, zero};
+                int n32 = 0;
+                const int Lp = (L + 1) >> 1;
+                for (int jp = ph; jp < Lp; jp += P) {
+                    const int j = 2 * jp;
+                    pair_adj2<KIND, ON>(lds2(&s_n[0][j]), lds2(&s_n[1][j]), lds2(&s_n[2][j]), lds2(&s_n[3][j]),
+                                        lds2(&s_n[4][j]), lds2(&s_n[5][j]), lds2(&s_n[6][j]), C, S, a32);
+                    if (++n32 == NM_FLUSH / 2) {
+#pragma unroll
+                        for (int c = 0; c < 6; c++) {
+                            float lo, hi;
+                            upk(a32[c], lo, hi);
+                            acc[c] += (double)lo + (double)hi;
+                            a32[c] = zero;
+                        }
+                        n32 = 0;
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    float lo, hi;
+                    upk(a32[c], lo, hi);
+                    acc[c] += (double)lo + (double)hi;
+                }
+            }
+            __syncthreads();  // the buffer is restaged next
+        };
+        int staged = 0, pass = 0;  // block-uniform
+        for (long long b0 = n0;; b0 += NM_STAGE) {
+            const bool more = b0 < n1;
+            const long long b1 = b0 + NM_STAGE < n1 ? b0 + NM_STAGE : n1;
+            if (more && (flags[(goff + b0) >> NM_BLOCK_LOG2] || flags[(goff + b1 - 1) >> NM_BLOCK_LOG2])) {
             // stage: each thread examines NM_PER_THREAD nodes, compaction by a block scan of counts;
             // the non-zero nodes are read again (an L1 hit) when they are written to shared memory
             bool nz[NM_PER_THREAD];
@@ -693,8 +826,8 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
             for (int r = 0; r < NM_PER_THREAD; r++) {
                 const long long node = b0 + r * NM_THREADS + t;
                 nz[r] = false;
-                if (node < n1) {
-                    const ulonglong2 lo = __ldg(q2 + 2 * node), hi = __ldg(q2 + 2 * node + 1);
+                if (node < b1) {
+                    const ulonglong2 lo = q2[2 * node], hi = q2[2 * node + 1];
                     nz[r] = (lo.x | lo.y | hi.x | hi.y) != 0ull;
                 }
                 cnt += nz[r] ? 1 : 0;
@@ -705,12 +838,13 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
                 const int y = __shfl_up_sync(0xffffffffu, x, o);
                 if (lane >= o) x += y;
             }
-            if (lane == 31) s_wsum[warp] = x;
+            int* ws = s_wsum[pass & 1];  // alternating: no barrier needed before the next pass writes
+            if (lane == 31) ws[warp] = x;
             __syncthreads();
-            int off = x - cnt, L = 0;
+            int off = staged + x - cnt, L = 0;
 #pragma unroll
             for (int w = 0; w < NM_THREADS / 32; w++) {
-                const int c = s_wsum[w];
+                const int c = ws[w];
                 if (w < warp) off += c;
                 L += c;
             }
@@ -718,38 +852,37 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
             for (int r = 0; r < NM_PER_THREAD; r++) {
                 if (!nz[r]) continue;
                 const long long li = b0 + r * NM_THREADS + t;  // node index in the slab
-                const ulonglong2 lo = __ldg(q2 + 2 * li), hi = __ldg(q2 + 2 * li + 1);
-                const int ix = (int)(li % nx);
-                const long long yz = li / nx;
-                const int iy = (int)(yz % ny), iz = (int)(yz / ny) + z_lo;
-                s_pos[off] = make_float4(NG.p0.x + NG.dA.x * ix + NG.dB.x * iy + NG.dC.x * iz,
-                                         NG.p0.y + NG.dA.y * ix + NG.dB.y * iy + NG.dC.y * iz,
-                                         NG.p0.z + NG.dA.z * ix + NG.dB.z * iy + NG.dC.z * iz, 0.f);
-                s_g[off] = make_float4((float)((double)(long long)lo.x * inv_scale),
-                                       (float)((double)(long long)lo.y * inv_scale),
-                                       (float)((double)(long long)hi.x * inv_scale),
-                                       (float)((double)(long long)hi.y * inv_scale));
+                const ulonglong2 lo = q2[2 * li], hi = q2[2 * li + 1];
+                if (last_group) {
+                    q2[2 * li] = make_ulonglong2(0ull, 0ull);
+                    q2[2 * li + 1] = make_ulonglong2(0ull, 0ull);
+                }
+                const unsigned l32 = (unsigned)li, yz = l32 / (unsigned)nx;  // slabs hold < 2^32 nodes
+                const int ix = (int)(l32 - yz * (unsigned)nx);
+                const int iy = (int)(yz % (unsigned)ny), iz = (int)(yz / (unsigned)ny) + z_lo;
+                s_n[0][off] = NG.p0.x + NG.dA.x * ix + NG.dB.x * iy + NG.dC.x * iz;
+                s_n[1][off] = NG.p0.y + NG.dA.y * ix + NG.dB.y * iy + NG.dC.y * iz;
+                s_n[2][off] = NG.p0.z + NG.dA.z * ix + NG.dB.z * iy + NG.dC.z * iz;
+                s_n[3][off] = (float)((double)(long long)lo.x * inv_scale);
+                s_n[4][off] = (float)((double)(long long)lo.y * inv_scale);
+                s_n[5][off] = (float)((double)(long long)hi.x * inv_scale);
+                s_n[6][off] = (float)((double)(long long)hi.y * inv_scale);
                 off++;
             }
-            __syncthreads();
-            if (act) {
-                float a32[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                int n32 = 0;
-                for (int j = ph; j < L; j += P) {
-                    pair_adj_fast<KIND>(s_pos[j], at, p1, p2, p3, S, s_g[j], a32);
-                    if (++n32 == NM_FLUSH) {
-#pragma unroll
-                        for (int c = 0; c < 6; c++) { acc[c] += a32[c]; a32[c] = 0.f; }
-                        n32 = 0;
-                    }
-                }
-#pragma unroll
-                for (int c = 0; c < 6; c++) acc[c] += a32[c];
+            staged += L;
+            ++pass;
             }
-            __syncthreads();  // s_pos / s_g / s_wsum are restaged next pass
+            // compute once at least NM_STAGE nodes are staged (< 2 * NM_STAGE: a pass adds at most
+            // NM_STAGE), and at the end of the unit; one call site, so the body is inlined
+            if (staged >= NM_STAGE || (!more && staged > 0)) {
+                compute(staged);
+                staged = 0;
+            }
+            if (!more) break;
         }
 #pragma unroll
         for (int c = 0; c < 6; c++) red[c][t] = act ? acc[c] : 0.0;
+        if (KIND == SPM_KIND_LJ) red[3][t] = -red[3][t];  // accumulated negated
         __syncthreads();
         if (t < nag) {
             double* out = partial + ((size_t)D->row_off + (size_t)lc * na + a0 + t) * 6;
@@ -764,10 +897,12 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
     }
 }
 
-// grad[ga*6 + c] = sum over the molecule's node units, fixed order.
+// grad[ga*6 + c] = sum over the molecule's node units, fixed order.  When the
+// node kernel ran before it (mark != null), block 0 marks the adjoint grid clear.
 __global__ void __launch_bounds__(256)
 batch_fold_rows_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk, const double* __restrict__ partial,
-                       double* __restrict__ grad) {
+                       double* __restrict__ grad, unsigned long long* __restrict__ mark) {
+    if (mark && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *mark = ADJ_CLEAN;
     __shared__ double red[256];
     const long long ga = blockIdx.x;
     const int c = blockIdx.y;
@@ -787,9 +922,12 @@ batch_fold_rows_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int ch
     if (threadIdx.x == 0) grad[ga * 6 + c] = red[0];
 }
 
-// Scratch layout of spm_batch_adjoint_params (byte offsets, 16-byte aligned).
+// Scratch layout of spm_batch_adjoint_params (byte offsets, 16-byte aligned):
+// the fixed-point adjoint grid, per-unit partials, dk row sums, then the
+// per-molecule |ubar| maxima and the touched-block flags (cleared together),
+// and the adjoint grid's clean marker.
 struct AdjScratch {
-    long long gq, part, dk, umax, total;
+    long long gq, part, dk, umax, flags, mark, total;
 };
 AdjScratch adj_scratch_layout(const long long* totals, int n_mol) {
     AdjScratch L;
@@ -798,7 +936,9 @@ AdjScratch adj_scratch_layout(const long long* totals, int n_mol) {
     L.part = up16(L.gq + totals[7] * 32);
     L.dk = up16(L.part + totals[8] * 48);
     L.umax = up16(L.dk + n_rowblocks(totals[4]) * 32);
-    L.total = up16(L.umax + (long long)n_mol * 4);
+    L.flags = L.umax + (long long)n_mol * 4;
+    L.mark = up16(L.flags + (totals[7] >> NM_BLOCK_LOG2) + 2);
+    L.total = L.mark + 16;
     return L;
 }
 
@@ -860,29 +1000,48 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
     double* part = reinterpret_cast<double*>(base + SL.part);
     double* dkpart = reinterpret_cast<double*>(base + SL.dk);
     unsigned* umax = reinterpret_cast<unsigned*>(base + SL.umax);
+    unsigned char* flags = reinterpret_cast<unsigned char*>(base + SL.flags);
+    unsigned long long* mark = reinterpret_cast<unsigned long long*>(base + SL.mark);
+    bool nodes_ran = false;
     if (n_mol > 0 && n_atoms > 0) {
         SPM_REQUIRE(mols && atoms && params && grad && aligned16(atoms), "spm_batch_adjoint_params: null atoms/grad");
         if (n_states > 0 && n_units > 0) {
             SPM_REQUIRE(PPs && ubar && aligned16(PPs) && aligned16(ubar),
                         "spm_batch_adjoint_params: state buffers null or misaligned");
-            if (cudaMemsetAsync(gq, 0, (size_t)totals[7] * 32, st) != cudaSuccess ||
-                cudaMemsetAsync(umax, 0, (size_t)n_mol * 4, st) != cudaSuccess)
+            static bool smem_set[64] = {};  // the node kernels' dynamic shared memory (> 48 KB), once per device
+            int dev = 0;
+            if (cudaGetDevice(&dev) != cudaSuccess)
+                return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: no current device");
+            if (dev < 0 || dev >= 64 || !smem_set[dev]) {
+                for (auto k : {batch_adjoint_nodes_kernel<SPM_KIND_LJ, true>, batch_adjoint_nodes_kernel<SPM_KIND_LJ, false>,
+                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true>,
+                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false>})
+                    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)NM_SMEM) != cudaSuccess)
+                        return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: cannot set shared memory size");
+                if (dev >= 0 && dev < 64) smem_set[dev] = true;
+            }
+            if (cudaMemsetAsync(umax, 0, (size_t)(SL.mark - SL.umax), st) != cudaSuccess)  // maxima + block flags
                 return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: memset failed");
+            adj_clear_kernel<<<1184, 256, 0, st>>>(reinterpret_cast<ulonglong2*>(gq), totals[7] * 2, mark);
             batch_ubar_max_kernel<<<(unsigned)n_chunks, 256, 0, st>>>(n_mol, mols, reinterpret_cast<const float4*>(ubar),
-                                                                      umax);
+                                                                      umax, mark);
             batch_scatter_kernel<<<(unsigned)((n_states + 255) / 256), 256, 0, st>>>(
                 n_mol, mols, n_states, reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar), umax,
-                gq);
+                gq, flags);
             const NodeSites S = make_node_sites(Qs, QZs);
             const int pstride = kind == SPM_KIND_MORSE ? 4 : 2;
-            if (kind == SPM_KIND_LJ)
-                batch_adjoint_nodes_kernel<SPM_KIND_LJ><<<(unsigned)n_units, NM_THREADS, 0, st>>>(
-                    n_mol, mols, chunk, reinterpret_cast<const float4*>(atoms), params, pstride, S, gq, umax, part);
-            else
-                batch_adjoint_nodes_kernel<SPM_KIND_MORSE><<<(unsigned)n_units, NM_THREADS, 0, st>>>(
-                    n_mol, mols, chunk, reinterpret_cast<const float4*>(atoms), params, pstride, S, gq, umax, part);
+            const bool on = S.qon != 0.f;
+            auto kern = kind == SPM_KIND_LJ ? (on ? batch_adjoint_nodes_kernel<SPM_KIND_LJ, true>
+                                                  : batch_adjoint_nodes_kernel<SPM_KIND_LJ, false>)
+                                            : (on ? batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true>
+                                                  : batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false>);
+            kern<<<(unsigned)n_units, NM_THREADS, NM_SMEM, st>>>(n_mol, mols, chunk,
+                                                                 reinterpret_cast<const float4*>(atoms), params, pstride,
+                                                                 S, gq, flags, umax, part);
+            nodes_ran = true;
         }
-        batch_fold_rows_kernel<<<dim3((unsigned)n_atoms, 6), 256, 0, st>>>(n_mol, mols, chunk, part, grad);
+        batch_fold_rows_kernel<<<dim3((unsigned)n_atoms, 6), 256, 0, st>>>(n_mol, mols, chunk, part, grad,
+                                                                           nodes_ran ? mark : nullptr);
     }
     if (n_states > 0) {
         SPM_REQUIRE(dk && aligned16(dk), "spm_batch_adjoint_params: null dk");

@@ -4,6 +4,7 @@
 // every batched stage across the batch for one launch shape:
 //   tile_off   grid-build CTA tiles  ceil(nx/32) x ceil(ny/gb_ty) x ceil(nz_slab/gb_zb)
 //   slot_off   relaxation slots      raster: 32 per (32/h) x h pixel tile, else one per pixel
+//                                    rounded up to 32 (a warp's 32 slots never span molecules)
 //   unit_off   adjoint node units    ceil(slab nodes/adj_chunk) (0 without states)
 //   chunk_off  loss chunks           ceil(states/256)
 //   row_off    adjoint partial rows  units x n_atoms
@@ -16,11 +17,12 @@ extern "C" spm_batch_shape spm_batch_default_shape(void) {
     s.gb_ty = 4;
     s.gb_zb = 8;
     s.rx_threads = 128;
-    s.rx_tile_h = 8;
+    s.rx_tile_h = 4;
     s.rx_ctas_per_sm = 0;
     s.adj_chunk = 16384;
-    s.rx_regs = 0;
+    s.rx_regs = 2;
     s.grid_layout = 0;
+    s.rx_sync = 1;
     return s;
 }
 
@@ -42,6 +44,7 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
                 "spm_batch_prepare: adj_chunk=%d", S.adj_chunk);
     SPM_REQUIRE(S.rx_regs >= 0 && S.rx_regs <= 2, "spm_batch_prepare: rx_regs=%d", S.rx_regs);
     SPM_REQUIRE(S.grid_layout == 0 || S.grid_layout == 1, "spm_batch_prepare: grid_layout=%d", S.grid_layout);
+    SPM_REQUIRE(S.rx_sync == 0 || S.rx_sync == 1, "spm_batch_prepare: rx_sync=%d", S.rx_sync);
     const long long th = S.rx_tile_h, tw = 32 / S.rx_tile_h;
     long long tiles = 0, slots = 0, units = 0, chunks = 0, states = 0, atoms = 0, pixels = 0, grid_end = 0, rows = 0;
     for (int m = 0; m < n_mol; m++) {
@@ -78,7 +81,7 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
                 const long long nxr = D.n_scan / D.raster_ny;
                 slots += ((nxr + tw - 1) / tw) * ((D.raster_ny + th - 1) / th) * 32;
             } else {
-                slots += D.n_scan;
+                slots += (D.n_scan + 31LL) / 32 * 32;
             }
             const long long u = (slab + S.adj_chunk - 1) / S.adj_chunk;
             units += u;

@@ -12,7 +12,10 @@
 //   * a lane that converges moves straight on to its next z-step, and -- when
 //     a device-side pixel counter is supplied -- a lane that finishes its pixel
 //     takes the next one (warp-aggregated atomicAdd), so no lane idles while
-//     the slowest lane of its warp or the last CTA wave finishes;
+//     the slowest lane of its warp or the last CTA wave finishes.  (Warps that
+//     step down the z-steps together, as the batched kernel does, ran 6% slower
+//     on the 480x480-pixel slab scan, whose slowest pixels need up to 3000
+//     FIRE steps per stroke);
 //   * pixels are handed out in 4 (ix) x 8 (iy) tiles, so the eight texel rows
 //     a warp reads per step overlap in L1 and the in-flight set stays local;
 //   * node offsets are 32-bit when the grid has fewer than 2^32 nodes.
@@ -529,6 +532,99 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     }
 }
 
+// z-synchronised schedule (spm_batch_shape.rx_sync = 1): a warp draws 32
+// slots at once -- one pixel tile of one molecule, slot numbering being
+// 32-aligned per molecule -- and its lanes relax their strokes one z-step at a
+// time, waiting for each other at the end of every z-step.  Every texel load
+// of the warp then reads the same z-layers around neighbouring pixels; the
+// cost is the lanes idling while the tile's slowest pixel of that z-step
+// converges.  Each lane runs exactly the FIRE sequence of the other schedule
+// (pp_iter_z), so the results are the same bits.
+//
+// One lane's stroke of pixel k; every lane of `members` runs the same number
+// of z-steps (the molecule's nz_steps) and meets the others after each.
+template <bool CACHE, int LAYOUT>
+__device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const float* __restrict__ grid,
+                                                  const float4* __restrict__ pts, const spm_scan_params& P,
+                                                  float4* __restrict__ FEs, float4* __restrict__ PPs,
+                                                  int* __restrict__ iter_count, int k, float dz, unsigned members) {
+    const AxisView G = axis_view<LAYOUT>(D, grid);
+    TexelCache T;
+    T.x0 = -1;
+    const int nzs = D->nz_steps;
+    const int pix = D->pix_off + k;
+    const long long sbase = D->state_off + (long long)k * nzs;
+    const float4 p4 = pts[pix];
+    V3 tip = mk3(p4.x, p4.y, p4.z);
+    V3 pos = mk3(tip.x + P.dpos0[0], tip.y + P.dpos0[1], tip.z + P.dpos0[2]);
+    V3 v = mk3(0.f, 0.f, 0.f);
+    float dt = P.relax_params[0], damp = P.relax_params[1];
+    float4 fe = make_float4(0.f, 0.f, 0.f, 0.f);
+    int total_it = 0;
+    for (int iz = 0; iz < nzs; ++iz) {
+        int it = 0;
+        bool conv;
+        while (!pp_iter_z<unsigned, CACHE, LAYOUT>(G, T, P, tip, pos, v, dt, damp, fe, it, total_it, conv)) {
+        }
+        if (!conv) fe = sample_z<unsigned, CACHE, LAYOUT>(G, pos, T);  // the position moved after the last sample
+        const long long o = sbase + iz;
+        FEs[o] = fe;
+        // all seven values finite <=> the sum of their products with zero is zero
+        float z0 = __fmul_rn(fe.x, 0.f);
+        z0 = __fmaf_rn(fe.y, 0.f, z0);
+        z0 = __fmaf_rn(fe.z, 0.f, z0);
+        z0 = __fmaf_rn(fe.w, 0.f, z0);
+        z0 = __fmaf_rn(pos.x, 0.f, z0);
+        z0 = __fmaf_rn(pos.y, 0.f, z0);
+        z0 = __fmaf_rn(pos.z, 0.f, z0);
+        const bool finite = (z0 == 0.f);
+        PPs[o] = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
+        tip.z = __fadd_rn(tip.z, dz);
+        pos.z = __fadd_rn(pos.z, dz);
+        v = mk3(0.f, 0.f, 0.f);
+        __syncwarp(members);  // the tile's lanes start the next z-step together
+    }
+    if (iter_count) iter_count[pix] = total_it;
+}
+
+template <int MINB, bool CACHE, int LAYOUT>
+__global__ void __launch_bounds__(256, MINB)
+batch_relax_sync_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
+                        const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
+                        float4* __restrict__ FEs, float4* __restrict__ PPs, int* __restrict__ iter_count,
+                        unsigned* __restrict__ counter) {
+    const float dz = P.tipC[3];
+    const unsigned lane = threadIdx.x & 31u;
+    while (true) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(counter, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n_slots) return;  // warp-uniform
+        const int m = SPM_MOL_BY(slot_off, mols, n_mol, (long long)base);
+        const spm_batch_mol* D = mols + m;
+        const unsigned lt = base + lane - (unsigned)D->slot_off;
+        const int ny = D->raster_ny, n_scan = D->n_scan;
+        int k;
+        bool valid;
+        if (ny <= 0) {
+            k = (int)lt;
+            valid = k < n_scan;
+        } else {
+            const int nxr = n_scan / ny;
+            const unsigned th = 1u << th_log2;
+            const unsigned nty = ((unsigned)ny + th - 1u) >> th_log2;
+            const unsigned tile = lt >> 5, r = lt & 31u;
+            const int ix = (int)((tile / nty) * (32u >> th_log2) + (r >> th_log2));
+            const int iy = (int)((tile % nty) * th + (r & (th - 1u)));
+            valid = ix < nxr && iy < ny;
+            k = ix * ny + iy;
+        }
+        const unsigned members = __ballot_sync(0xffffffffu, valid);
+        if (valid) relax_tile_stroke<CACHE, LAYOUT>(D, grid, pts, P, FEs, PPs, iter_count, k, dz, members);
+        __syncwarp();  // the whole warp draws the next tile
+    }
+}
+
 }  // namespace
 }  // namespace spm
 
@@ -558,13 +654,17 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     SPM_REQUIRE(shape->rx_regs >= 0 && shape->rx_regs <= 2, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
     SPM_REQUIRE(shape->grid_layout == 0 || shape->grid_layout == 1, "spm_batch_relax: grid_layout=%d",
                 shape->grid_layout);
-    auto kern = batch_relax_kernel<3, false, 2>;
-    if (shape->grid_layout == 0)
-        kern = shape->rx_regs == 2 ? batch_relax_kernel<2, true, 2>
-                                   : (shape->rx_regs == 1 ? batch_relax_kernel<4, false, 2> : batch_relax_kernel<3, false, 2>);
-    else
-        kern = shape->rx_regs == 2 ? batch_relax_kernel<2, true, 4>
-                                   : (shape->rx_regs == 1 ? batch_relax_kernel<4, false, 4> : batch_relax_kernel<3, false, 4>);
+    SPM_REQUIRE(shape->rx_sync == 0 || shape->rx_sync == 1, "spm_batch_relax: rx_sync=%d", shape->rx_sync);
+    using Kern = decltype(&batch_relax_kernel<3, false, 2>);
+    // [rx_sync][grid_layout][rx_regs]
+    static const Kern table[2][2][3] = {
+        {{batch_relax_kernel<3, false, 2>, batch_relax_kernel<4, false, 2>, batch_relax_kernel<2, true, 2>},
+         {batch_relax_kernel<3, false, 4>, batch_relax_kernel<4, false, 4>, batch_relax_kernel<2, true, 4>}},
+        {{batch_relax_sync_kernel<3, false, 2>, batch_relax_sync_kernel<4, false, 2>,
+          batch_relax_sync_kernel<2, true, 2>},
+         {batch_relax_sync_kernel<3, false, 4>, batch_relax_sync_kernel<4, false, 4>,
+          batch_relax_sync_kernel<2, true, 4>}}};
+    const Kern kern = table[shape->rx_sync][shape->grid_layout][shape->rx_regs];
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||

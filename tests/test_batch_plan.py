@@ -17,7 +17,7 @@ def small_items(n=7, seed=5, kind=0):
 def test_struct_layout():
     # spm_batch_mol: 7 int64 offsets, 12 int32 fields, 7 float[4] vectors
     assert ctypes.sizeof(_lib.BatchMol) == 7 * 8 + 12 * 4 + 7 * 16
-    assert ctypes.sizeof(_lib.BatchShape) == 8 * 4
+    assert ctypes.sizeof(_lib.BatchShape) == 9 * 4
 
 
 @pytest.mark.parametrize("shape_kw", [{}, dict(gb_ty=2, gb_zb=16, rx_tile_h=1, adj_chunk=1024),
@@ -97,7 +97,8 @@ def test_prepare_rejects_bad_descriptors():
     plan.mols[3].grid_off = plan.mols[2].grid_off
     assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_ERR_ARG
     plan = BatchPlan(small_items(4))
-    for field, bad in (("gb_ty", 3), ("gb_zb", 4), ("rx_threads", 96), ("rx_tile_h", 6), ("adj_chunk", 1000), ("rx_regs", 3), ("grid_layout", 2)):
+    for field, bad in (("gb_ty", 3), ("gb_zb", 4), ("rx_threads", 96), ("rx_tile_h", 6), ("adj_chunk", 1000), ("rx_regs", 3), ("grid_layout", 2),
+                       ("rx_sync", 2)):
         s = L.spm_batch_default_shape()
         setattr(s, field, bad)
         assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(s), totals) == _lib.SPM_ERR_ARG, field
@@ -110,5 +111,5 @@ def test_partial_raster_falls_back_to_1d():
         pytest.skip("raster size divisible")
     tot = plan.prepare(_lib.lib().spm_batch_default_shape())
     assert plan.mols[0].raster_ny == 0
-    assert plan.mols[1].slot_off == plan.mols[0].n_scan
+    assert plan.mols[1].slot_off == -(-plan.mols[0].n_scan // 32) * 32  # a warp's 32 slots stay in one molecule
     assert tot[1] > 0

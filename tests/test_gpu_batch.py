@@ -98,10 +98,13 @@ def test_batch_shapes_give_same_results(cuda):
     _target(ref)
     ref.forward_adjoint()
     L = _lib.lib()
-    for kw in (dict(gb_ty=2, gb_zb=16, rx_threads=64, rx_tile_h=1, adj_chunk=1024),
-               dict(gb_ty=8, gb_zb=8, rx_threads=256, rx_tile_h=32, rx_ctas_per_sm=1, adj_chunk=65536, rx_regs=1),
-               dict(rx_threads=128, rx_tile_h=4, rx_regs=2),
-               dict(grid_layout=1), dict(grid_layout=1, rx_regs=2), dict(grid_layout=1, rx_regs=1, gb_zb=16)):
+    for kw in (dict(gb_ty=2, gb_zb=16, rx_threads=64, rx_tile_h=1, adj_chunk=1024, rx_sync=0, rx_regs=0),
+               dict(gb_ty=8, gb_zb=8, rx_threads=256, rx_tile_h=32, rx_ctas_per_sm=1, adj_chunk=65536, rx_regs=1,
+                    rx_sync=0),
+               dict(rx_threads=128, rx_tile_h=4, rx_regs=2, rx_sync=0),
+               dict(grid_layout=1, rx_sync=0), dict(grid_layout=1, rx_regs=2), dict(grid_layout=1, rx_regs=1, gb_zb=16),
+               dict(rx_sync=1, rx_regs=0), dict(rx_sync=1, rx_tile_h=1, rx_threads=64, rx_regs=2),
+               dict(rx_sync=1, rx_tile_h=32, rx_regs=1, grid_layout=1)):
         s = L.spm_batch_default_shape()
         for k, v in kw.items():
             setattr(s, k, v)
@@ -118,7 +121,8 @@ def test_batch_shapes_give_same_results(cuda):
                 assert torch.equal(b.slab(i, 3), torch.roll(full, (-1, -1), dims=(0, 2)))
         assert torch.equal(b.FEs, ref.FEs) and torch.equal(b.PPs, ref.PPs)
         assert torch.equal(b.loss, ref.loss) and torch.equal(b.ubar, ref.ubar)
-        torch.testing.assert_close(b.grad, ref.grad, rtol=1e-6, atol=1e-9 * float(ref.grad.abs().max()))
+        # adj_chunk regroups the staged nodes into other FP32 partial sums (FP64 across them)
+        torch.testing.assert_close(b.grad, ref.grad, rtol=1e-5, atol=1e-6 * float(ref.grad.abs().max()))
 
 
 def test_batch_graph_replay(cuda):
@@ -135,6 +139,28 @@ def test_batch_graph_replay(cuda):
     torch.cuda.synchronize()
     for e, t in zip(eager, (b.FEs, b.PPs, b.loss, b.grad)):
         assert torch.equal(e, t)
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_adjoint_scratch_reuse_and_garbage(cuda, kind):
+    """The node kernel leaves the adjoint grid cleared for the next call; a
+    scratch buffer of arbitrary content (no clear marker) is cleared first."""
+    b = AFMBatch(_items(kind, n=4, seed=71 + kind), kind=kind)
+    _target(b)
+    b.forward_adjoint()
+    torch.cuda.synchronize()
+    g1 = b.grad.clone()
+    b.adjoint_params()
+    torch.cuda.synchronize()
+    assert torch.equal(b.grad, g1)
+    b.adj_scratch.view(torch.uint8).random_(0, 256)
+    b.adjoint_params()
+    torch.cuda.synchronize()
+    assert torch.equal(b.grad, g1)
+    b.adj_scratch.view(torch.uint8).fill_(0)  # all-zero buffer: no marker either
+    b.adjoint_params()
+    torch.cuda.synchronize()
+    assert torch.equal(b.grad, g1)
 
 
 def test_batch_adam_reduces_loss(cuda):
