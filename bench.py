@@ -439,6 +439,10 @@ def run_batched(args, dev_index):
     out = {}
     # ---- (4) fitting: target df from N(0,0.1 A)-perturbed positions; fit starts at the unperturbed structures
     items = synthetic.batch_molecules(args.fit_mols, seed=5)
+    # the per-image drop-in path on the same molecules first, on a device that holds no batch
+    from spammm_b200.batch import ProbeSpec
+    plain = _plain_images_per_s(items, ProbeSpec())
+    torch.cuda.empty_cache()
     if args.no_tune:
         from spammm_b200 import _lib
         shape, tune_rep = _lib.lib().spm_batch_default_shape(), None
@@ -504,7 +508,7 @@ def run_batched(args, dev_index):
         torch.cuda.synchronize()
         sr[name] = e0.elapsed_time(e1)
     out["fit"]["stage_ms"] = sr
-    out["plain_per_image"] = _plain_images_per_s(items, b.probe)
+    out["plain_per_image"] = plain
     out["fit"]["vs_plain_per_image"] = out["fit"]["images_per_s"] / out["plain_per_image"]["images_per_s"]
     del g, b, opt
     torch.cuda.empty_cache()
