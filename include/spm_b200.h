@@ -411,8 +411,9 @@ int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_st
  *      non-zero adjoint-grid nodes in shared memory and every thread owns one
  *      atom (and a phase of the chunk), evaluating the pair-law derivatives of
  *      its atom at each staged node; per-(chunk, atom) FP64 partials are folded
- *      per atom in a fixed order.  Blocks of 1024 nodes that no state touched
- *      are skipped, and every node read is zeroed again.
+ *      per atom in a fixed order.  Nodes outside each molecule's box of
+ *      touched rows and layers are not read, and every node read is zeroed
+ *      again.
  * totals: the HOST array of spm_batch_prepare; scratch (device) >=
  * spm_batch_adjoint_scratch_bytes(totals, n_mol).  The scratch keeps the
  * cleared adjoint grid between calls, with a marker that says it is clear:

@@ -436,7 +436,6 @@ __device__ __forceinline__ int scale_exp(unsigned umax_bits) {
 }
 __device__ __forceinline__ double pow2(int k) { return __longlong_as_double((long long)(1023 + k) << 52); }
 
-constexpr int NM_BLOCK_LOG2 = 10;  // touched-block flags: one byte per 1024 adjoint-grid nodes
 constexpr unsigned long long ADJ_CLEAN = 0x4e41454c434d5053ull;  // marker: the adjoint grid is all zero
 constexpr unsigned long long ADJ_DIRTY = 1ull;
 
@@ -451,30 +450,63 @@ adj_clear_kernel(ulonglong2* __restrict__ gq, long long n2, const unsigned long 
         gq[i] = make_ulonglong2(0ull, 0ull);
 }
 
-// CTA per 256-state chunk: per-molecule max |ubar| (as float bits; order-free).
+// CTA per 256-state chunk (one molecule): per-molecule max |ubar| (as float
+// bits; order-free) and the bounding box of the rows and slab layers the
+// scatter will touch, box[4m..4m+3] = max of (ny-1-y, y+1, nz_slab-1-zl, zl+1)
+// over the cell corners of every state with a non-zero ubar (all zero: none).
 // Block 0 marks the adjoint grid dirty (the scatter follows).
 __global__ void __launch_bounds__(256)
 batch_ubar_max_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float4* __restrict__ ubar,
-                      unsigned* __restrict__ umax, unsigned long long* __restrict__ mark) {
+                      const float4* __restrict__ PPs, unsigned* __restrict__ umax, int* __restrict__ box,
+                      unsigned long long* __restrict__ mark) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *mark = ADJ_DIRTY;
     __shared__ float s_m[8];
+    __shared__ int s_b[4][8];
     const long long ch = blockIdx.x;
     const int m = SPM_MOL_BY(chunk_off, mols, n_mol, ch);
     const spm_batch_mol* D = mols + m;
     const long long nst = (long long)D->n_scan * D->nz_steps;
     const long long ls = (ch - D->chunk_off) * 256 + threadIdx.x;
     float v = 0.f;
+    int b[4] = {0, 0, 0, 0};
     if (ls < nst) {
         const float4 u = __ldg(ubar + D->state_off + ls);
         v = fmaxf(fmaxf(fabsf(u.x), fabsf(u.y)), fmaxf(fabsf(u.z), fabsf(u.w)));
+        if (!(u.x == 0.f && u.y == 0.f && u.z == 0.f && u.w == 0.f)) {  // the scatter's test
+            const GridView G = slab_view(*D, nullptr);
+            const float4 pp = __ldg(PPs + D->state_off + ls);
+            const Corners C = corners_of<true>(G, mk3(pp.x, pp.y, pp.z));
+            if (C.ok) {
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    b[0] = max(b[0], G.ny - 1 - C.y[k]);
+                    b[1] = max(b[1], C.y[k] + 1);
+                    b[2] = max(b[2], G.nz_slab - 1 - (C.z[k] - G.z_lo));
+                    b[3] = max(b[3], C.z[k] - G.z_lo + 1);
+                }
+            }
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = v;
+    for (int o = 16; o > 0; o >>= 1) {
+        v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+#pragma unroll
+        for (int k = 0; k < 4; k++) b[k] = max(b[k], __shfl_xor_sync(0xffffffffu, b[k], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_m[threadIdx.x >> 5] = v;
+#pragma unroll
+        for (int k = 0; k < 4; k++) s_b[k][threadIdx.x >> 5] = b[k];
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         float w = s_m[0];
         for (int k = 1; k < 8; k++) w = fmaxf(w, s_m[k]);
         if (w > 0.f) atomicMax(umax + m, __float_as_uint(w));
+    }
+    if (threadIdx.x < 4) {
+        int w = s_b[threadIdx.x][0];
+        for (int k = 1; k < 8; k++) w = max(w, s_b[threadIdx.x][k]);
+        if (w > 0) atomicMax(box + 4 * m + threadIdx.x, w);
     }
 }
 
@@ -487,7 +519,7 @@ batch_ubar_max_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const f
 __global__ void __launch_bounds__(256)
 batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states,
                      const float4* __restrict__ PPs, const float4* __restrict__ ubar, const unsigned* __restrict__ umax,
-                     unsigned long long* __restrict__ gq, unsigned char* __restrict__ flags) {
+                     unsigned long long* __restrict__ gq) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const long long st = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -498,7 +530,6 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
     long long stroke = -1;
     int nx = 0, ny = 0, z_lo = 0;
     unsigned long long* base = gq;
-    long long goff = 0;
     double scale = 0.0;
     if (valid) {
         const int m = SPM_MOL_BY(state_off, mols, n_mol, st);
@@ -510,7 +541,6 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
         stroke = D->pix_off + (st - D->state_off) / D->nz_steps;
         nx = G.nx; ny = G.ny; z_lo = G.z_lo;
         base = gq + (size_t)D->grid_off * 4;
-        goff = D->grid_off;
         scale = pow2(42 - scale_exp(__ldg(umax + m)));
     }
     // merge tests against the next lane (it gives me its upper layer) and the previous one (I give mine)
@@ -531,20 +561,6 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
     for (int c = 0; c < 8; c++) {
         const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
         w[c] = valid ? (i ? C.ax : 1.f - C.ax) * (j ? C.ay : 1.f - C.ay) * (k ? C.az : 1.f - C.az) : 0.f;
-    }
-    if (valid) {
-        // flag the 1024-node blocks of the cell's corners for the node kernel: a read first, a
-        // store only if unset (the same few flag bytes are hit by every state of a region); an
-        // upper layer given to the previous lane is that lane's lower layer, flagged there
-        long long last = -1;
-#pragma unroll
-        for (int c = 0; c < 8; c++) {
-            const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
-            if (k == 1 && given) break;
-            const long long blk = (goff + ((long long)(C.z[k] - z_lo) * ny + C.y[j]) * nx + C.x[i]) >> NM_BLOCK_LOG2;
-            if (blk != last && !flags[blk]) flags[blk] = 1;
-            last = blk;
-        }
     }
     const float ubc[4] = {ub.x, ub.y, ub.z, ub.w};
 #pragma unroll
@@ -709,8 +725,8 @@ constexpr size_t NM_SMEM = 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(
 // a0 + t % nag and every P-th staged node pair (P = 256 / nag phases), so the
 // atom's derivative sums stay in its registers: no atomics, no cross-thread
 // reduction until the phases are folded once per unit.
-//   * 1024-node blocks that no state touched (flags, set by the scatter) are
-//     skipped without being read;
+//   * 1024-node passes outside the molecule's box of touched rows and slab
+//     layers (box, from the ubar-maximum kernel) are skipped without being read;
 //   * the non-zero nodes of consecutive blocks accumulate in shared memory
 //     until at least NM_STAGE are staged, so every compute phase between two
 //     barriers is dense;
@@ -720,7 +736,7 @@ template <int KIND, bool ON>
 __global__ void __launch_bounds__(NM_THREADS, 2)
 batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk,
                            const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
-                           NodeSites S, unsigned long long* __restrict__ gq, const unsigned char* __restrict__ flags,
+                           NodeSites S, unsigned long long* __restrict__ gq, const int* __restrict__ box,
                            const unsigned* __restrict__ umax, double* __restrict__ partial) {
     extern __shared__ __align__(16) unsigned char nm_smem[];
     float(*s_n)[NM_BUF] = reinterpret_cast<float(*)[NM_BUF]>(nm_smem);
@@ -744,7 +760,17 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
     NG.dC = ld4f(D->dC);
     const double inv_scale = pow2(scale_exp(__ldg(umax + m)) - 42);
     ulonglong2* q2 = reinterpret_cast<ulonglong2*>(gq + (size_t)D->grid_off * 4);
-    const long long goff = D->grid_off;
+    // touched rows y in [ylo, yhi] and slab layers in [zlo, zhi] (empty: yhi < 0)
+    const int ylo = ny - 1 - box[4 * m], yhi = box[4 * m + 1] - 1;
+    const int zlo = D->nz_slab - 1 - box[4 * m + 2], zhi = box[4 * m + 3] - 1;
+    auto touched = [&](long long b0, long long b1) {  // may nodes [b0, b1) be non-zero?
+        const unsigned r0 = (unsigned)b0 / (unsigned)nx, r1 = (unsigned)(b1 - 1) / (unsigned)nx;  // rows zl*ny + y
+        const int za = (int)(r0 / (unsigned)ny), zb = (int)(r1 / (unsigned)ny);
+        if (yhi < 0 || zb < zlo || za > zhi) return false;
+        if (za != zb) return true;  // spans a layer boundary: keep
+        const int ya = (int)(r0 - (unsigned)za * ny), yb = (int)(r1 - (unsigned)za * ny);
+        return !(yb < ylo || ya > yhi);
+    };
     for (int a0 = 0; a0 < na; a0 += NM_THREADS) {
         const bool last_group = a0 + NM_THREADS >= na;
         const int nag = na - a0 < NM_THREADS ? na - a0 : NM_THREADS;
@@ -817,7 +843,7 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
         for (long long b0 = n0;; b0 += NM_STAGE) {
             const bool more = b0 < n1;
             const long long b1 = b0 + NM_STAGE < n1 ? b0 + NM_STAGE : n1;
-            if (more && (flags[(goff + b0) >> NM_BLOCK_LOG2] || flags[(goff + b1 - 1) >> NM_BLOCK_LOG2])) {
+            if (more && touched(b0, b1)) {
             // stage: each thread examines NM_PER_THREAD nodes, compaction by a block scan of counts;
             // the non-zero nodes are read again (an L1 hit) when they are written to shared memory
             bool nz[NM_PER_THREAD];
@@ -924,10 +950,10 @@ batch_fold_rows_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int ch
 
 // Scratch layout of spm_batch_adjoint_params (byte offsets, 16-byte aligned):
 // the fixed-point adjoint grid, per-unit partials, dk row sums, then the
-// per-molecule |ubar| maxima and the touched-block flags (cleared together),
-// and the adjoint grid's clean marker.
+// per-molecule |ubar| maxima and touched boxes (cleared together), and the
+// adjoint grid's clean marker.
 struct AdjScratch {
-    long long gq, part, dk, umax, flags, mark, total;
+    long long gq, part, dk, umax, box, mark, total;
 };
 AdjScratch adj_scratch_layout(const long long* totals, int n_mol) {
     AdjScratch L;
@@ -936,8 +962,8 @@ AdjScratch adj_scratch_layout(const long long* totals, int n_mol) {
     L.part = up16(L.gq + totals[7] * 32);
     L.dk = up16(L.part + totals[8] * 48);
     L.umax = up16(L.dk + n_rowblocks(totals[4]) * 32);
-    L.flags = L.umax + (long long)n_mol * 4;
-    L.mark = up16(L.flags + (totals[7] >> NM_BLOCK_LOG2) + 2);
+    L.box = L.umax + (long long)n_mol * 4;
+    L.mark = up16(L.box + (long long)n_mol * 16);
     L.total = L.mark + 16;
     return L;
 }
@@ -1000,7 +1026,7 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
     double* part = reinterpret_cast<double*>(base + SL.part);
     double* dkpart = reinterpret_cast<double*>(base + SL.dk);
     unsigned* umax = reinterpret_cast<unsigned*>(base + SL.umax);
-    unsigned char* flags = reinterpret_cast<unsigned char*>(base + SL.flags);
+    int* box = reinterpret_cast<int*>(base + SL.box);
     unsigned long long* mark = reinterpret_cast<unsigned long long*>(base + SL.mark);
     bool nodes_ran = false;
     if (n_mol > 0 && n_atoms > 0) {
@@ -1020,14 +1046,15 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
                         return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: cannot set shared memory size");
                 if (dev >= 0 && dev < 64) smem_set[dev] = true;
             }
-            if (cudaMemsetAsync(umax, 0, (size_t)(SL.mark - SL.umax), st) != cudaSuccess)  // maxima + block flags
+            if (cudaMemsetAsync(umax, 0, (size_t)(SL.mark - SL.umax), st) != cudaSuccess)  // maxima + boxes
                 return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: memset failed");
             adj_clear_kernel<<<1184, 256, 0, st>>>(reinterpret_cast<ulonglong2*>(gq), totals[7] * 2, mark);
             batch_ubar_max_kernel<<<(unsigned)n_chunks, 256, 0, st>>>(n_mol, mols, reinterpret_cast<const float4*>(ubar),
-                                                                      umax, mark);
+                                                                      reinterpret_cast<const float4*>(PPs), umax, box,
+                                                                      mark);
             batch_scatter_kernel<<<(unsigned)((n_states + 255) / 256), 256, 0, st>>>(
                 n_mol, mols, n_states, reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar), umax,
-                gq, flags);
+                gq);
             const NodeSites S = make_node_sites(Qs, QZs);
             const int pstride = kind == SPM_KIND_MORSE ? 4 : 2;
             const bool on = S.qon != 0.f;
@@ -1037,7 +1064,7 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
                                                   : batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false>);
             kern<<<(unsigned)n_units, NM_THREADS, NM_SMEM, st>>>(n_mol, mols, chunk,
                                                                  reinterpret_cast<const float4*>(atoms), params, pstride,
-                                                                 S, gq, flags, umax, part);
+                                                                 S, gq, box, umax, part);
             nodes_ran = true;
         }
         batch_fold_rows_kernel<<<dim3((unsigned)n_atoms, 6), 256, 0, st>>>(n_mol, mols, chunk, part, grad,
