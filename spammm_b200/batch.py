@@ -7,8 +7,9 @@ each stage ONE launch over the batch (the spm_batch_* entry points of
 include/spm_b200.h):
 
   spm_batch_grid_build     force-grid slabs of every molecule
-  spm_batch_relax          persistent SPM_RELAX_PP relaxation; lanes draw
-                           (molecule, pixel) slots from one device counter
+  spm_batch_relax          persistent SPM_RELAX_PP relaxation; warps draw
+                           pixel tiles from one device counter and step
+                           down the z-steps together
   spm_batch_df_amp         amplitude-averaged df of every stroke
   spm_batch_df_loss_seed   per-molecule df loss and dL/dFEs
   spm_batch_adjoint_state  implicit-function adjoint of every state

@@ -395,24 +395,8 @@ __device__ __forceinline__ bool next_batch_pixel(unsigned* counter, unsigned n_s
         if (t >= n_slots) return false;
         m = SPM_MOL_BY(slot_off, mols, n_mol, (long long)t);
         const spm_batch_mol* D = mols + m;
-        const unsigned lt = t - (unsigned)D->slot_off;
-        const int ny = D->raster_ny, n_scan = D->n_scan;
-        if (ny <= 0) {
-            k = (int)lt;
-            if (k < n_scan) return true;
-            continue;  // stale prefix: draw again (t only grows: bounded)
-        }
-        const int nxr = n_scan / ny;
-        const unsigned th = 1u << th_log2;
-        const unsigned nty = ((unsigned)ny + th - 1u) >> th_log2;
-        const unsigned tile = lt >> 5, r = lt & 31u;
-        const int ix = (int)((tile / nty) * (32u >> th_log2) + (r >> th_log2));
-        const int iy = (int)((tile % nty) * th + (r & (th - 1u)));
-        if (ix < nxr && iy < ny) {
-            k = ix * ny + iy;
-            return true;
-        }
-        // an edge tile's slot outside the raster: draw again
+        if (slot_pixel(D, t - (unsigned)D->slot_off, th_log2, k)) return true;
+        // a slot outside the raster (edge tile) or past the last pixel: draw again (t only grows: bounded)
     }
 }
 
@@ -602,23 +586,8 @@ batch_relax_sync_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsig
         if (base >= n_slots) return;  // warp-uniform
         const int m = SPM_MOL_BY(slot_off, mols, n_mol, (long long)base);
         const spm_batch_mol* D = mols + m;
-        const unsigned lt = base + lane - (unsigned)D->slot_off;
-        const int ny = D->raster_ny, n_scan = D->n_scan;
         int k;
-        bool valid;
-        if (ny <= 0) {
-            k = (int)lt;
-            valid = k < n_scan;
-        } else {
-            const int nxr = n_scan / ny;
-            const unsigned th = 1u << th_log2;
-            const unsigned nty = ((unsigned)ny + th - 1u) >> th_log2;
-            const unsigned tile = lt >> 5, r = lt & 31u;
-            const int ix = (int)((tile / nty) * (32u >> th_log2) + (r >> th_log2));
-            const int iy = (int)((tile % nty) * th + (r & (th - 1u)));
-            valid = ix < nxr && iy < ny;
-            k = ix * ny + iy;
-        }
+        const bool valid = slot_pixel(D, base + lane - (unsigned)D->slot_off, th_log2, k);
         const unsigned members = __ballot_sync(0xffffffffu, valid);
         if (valid) relax_tile_stroke<CACHE, LAYOUT>(D, grid, pts, P, FEs, PPs, iter_count, k, dz, members);
         __syncwarp();  // the whole warp draws the next tile

@@ -26,6 +26,27 @@ __device__ __forceinline__ int find_mol(const spm_batch_mol* __restrict__ mols, 
 
 __device__ __forceinline__ float4 ld4f(const float* a) { return make_float4(__ldg(a), __ldg(a + 1), __ldg(a + 2), __ldg(a + 3)); }
 
+// Pixel k of relaxation slot lt (slot index within molecule D).  With a
+// raster (raster_ny > 0) slots run over tiles of (32 >> th_log2) (ix) x
+// (1 << th_log2) (iy) pixels, 32 slots per tile, tiles ordered iy-fastest;
+// without one, slot lt is pixel lt.  false: the slot lies outside the raster
+// (an edge tile) or past the last pixel.
+__device__ __forceinline__ bool slot_pixel(const spm_batch_mol* D, unsigned lt, int th_log2, int& k) {
+    const int ny = D->raster_ny, n_scan = D->n_scan;
+    if (ny <= 0) {
+        k = (int)lt;
+        return k < n_scan;
+    }
+    const int nxr = n_scan / ny;
+    const unsigned th = 1u << th_log2;
+    const unsigned nty = ((unsigned)ny + th - 1u) >> th_log2;
+    const unsigned tile = lt >> 5, r = lt & 31u;
+    const int ix = (int)((tile / nty) * (32u >> th_log2) + (r >> th_log2));
+    const int iy = (int)((tile % nty) * th + (r & (th - 1u)));
+    k = ix * ny + iy;
+    return ix < nxr && iy < ny;
+}
+
 // Sampling view of a molecule's slab (full-grid coordinates, stored layers
 // only; stride float4 per stored node: 2 x-pairs, 4 xz-quads, value first).
 __device__ __forceinline__ GridView slab_view(const spm_batch_mol& D, const float* grid, int stride = 2) {
