@@ -387,7 +387,10 @@ int spm_batch_df_amp(int n_mol, const spm_batch_mol* mols, long long n_pixels, c
  * volume: target, weights (total_states) float64 (weights NULL = 1 inside,
  * 0 on each stroke's first and last z-step); df_out (total_states) f64;
  * dL_dFEs (total_states,4) f32; loss_out (n_mol) f64 in descriptor order.
- * A molecule with nz_steps < 3 gets loss NaN and dL_dFEs = 0.
+ * A molecule whose weights sum to zero (no pixels, nz_steps < 3 with the
+ * default weights, every state masked) gets loss 0 and dL_dFEs = 0, where
+ * the single-volume formula's 0/0 is NaN: it adds nothing to a batch loss.
+ * With nz_steps < 3 dL_dFEs is 0 (no central difference).
  * scratch >= spm_batch_loss_scratch_bytes(n_chunks, n_mol). */
 int spm_batch_df_loss_seed(int n_mol, const spm_batch_mol* mols, long long n_chunks, const float* FEs,
                            const double* target, const double* weights, double dtip, double* df_out,

@@ -606,7 +606,9 @@ batch_loss_final_kernel(const spm_batch_mol* __restrict__ mols, const double* __
     if (threadIdx.x == 0) {
         sums[2 * m] = s_w[0];
         sums[2 * m + 1] = s_l[0];
-        loss[m] = 0.5 * s_l[0] / s_w[0];
+        // zero total weight (no pixels, or every state masked): the molecule contributes nothing,
+        // where the single-volume formula would give 0/0
+        loss[m] = s_w[0] > 0.0 ? 0.5 * s_l[0] / s_w[0] : 0.0;
     }
 }
 
@@ -628,6 +630,10 @@ batch_loss_grad_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const 
         return;
     }
     const double wsum = sums[2 * m];
+    if (!(wsum > 0.0)) {  // zero total weight: no loss, no gradient
+        dL[gid] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
     auto g = [&](long long j) {
         const int jz = (int)((j - base) % nz);
         const double w = wts ? wts[j] : ((jz > 0 && jz < nz - 1) ? 1.0 : 0.0);

@@ -141,6 +141,50 @@ def test_batch_graph_replay(cuda):
         assert torch.equal(e, t)
 
 
+@pytest.mark.parametrize("sync", [0, 1])
+def test_batch_unrastered_molecule(cuda, sync):
+    """A molecule whose points are no full raster (raster_ny = 0) is relaxed in
+    runs of 32 consecutive pixels, under both schedules; results equal the
+    per-molecule path bit for bit."""
+    items = _items(0, n=3, seed=91)
+    s = _lib.lib().spm_batch_default_shape()
+    s.rx_sync = sync
+    b = AFMBatch(items, shape=s)
+    b.plan.desc(1).raster_ny = 0
+    b.set_shape(s)
+    assert b.desc(1).raster_ny == 0
+    b.forward()
+    torch.cuda.synchronize()
+    for i in range(len(items)):
+        spec, grid, P, pts, FEs, PPs = _per_molecule(b, i)
+        assert torch.equal(b.fes(i), FEs) and torch.equal(b.pps(i), PPs), i
+
+
+def test_batch_with_empty_scan(cuda):
+    """A molecule with no pixels contributes nothing: its loss and gradient are
+    zero and the others' results are those of a batch without it."""
+    import dataclasses
+    items = _items(0, n=3, seed=93)
+    empty = dataclasses.replace(items[1], xs=items[1].xs[:0], ys=items[1].ys[:0])
+    b = AFMBatch([items[0], empty, items[2]])
+    ref = AFMBatch([items[0], items[2]])
+    rng = np.random.default_rng(5)
+    t0, t2 = (rng.normal(0.0, 0.05, (len(it.xs), len(it.ys), it.nz)) for it in (items[0], items[2]))
+    b.set_target(0, t0)
+    b.set_target(2, t2)
+    b.set_target(1, np.zeros((0, 0, empty.nz)))
+    ref.set_target(0, t0)
+    ref.set_target(1, t2)
+    b.forward_adjoint()
+    ref.forward_adjoint()
+    torch.cuda.synchronize()
+    for i, r in ((0, 0), (2, 1)):
+        assert torch.equal(b.fes(i), ref.fes(r)) and torch.equal(b.loss_of(i), ref.loss_of(r))
+        torch.testing.assert_close(b.grad_of(i), ref.grad_of(r), rtol=1e-5,
+                                   atol=1e-6 * float(ref.grad.abs().max()))
+    assert float(b.loss_of(1)) == 0.0 and not b.grad_of(1).any()
+
+
 @pytest.mark.parametrize("kind", [0, 1])
 def test_adjoint_scratch_reuse_and_garbage(cuda, kind):
     """The node kernel leaves the adjoint grid cleared for the next call; a
