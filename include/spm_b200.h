@@ -175,6 +175,21 @@ int spm_dissipation(const void* FEs_fwd, const void* FEs_bwd, int fes_dtype, int
                     const double* n, const double* h_scan, const int* off, const int* idx,
                     int n_out, float* E_diss, void* stream);
 
+/* Replaces the convolveZ kernel (kernels/AFM.cl:666-701): for each of n_col
+ * z-columns and izo < nz_out, Fout[c,izo] = sum over jz < nzw of
+ * Fin[c,izo+jz] * w[jz], nzw = nz_in - nz_out (0..1024; the reference holds
+ * up to 64 weights), all four channels, accumulated in jz order with fused
+ * multiply-adds.  Fin (n_col,nz_in,4), Fout (n_col,nz_out,4) float32; w
+ * (DEVICE float[nzw]). */
+int spm_convolve_z(const float* Fin, int n_col, int nz_in, int nz_out, const float* w, float* Fout,
+                   void* stream);
+
+/* Replaces the izoZ kernel (kernels/AFM.cl:705-723): per column the first
+ * iz >= 1 with Fin[c,iz].z > iso gives zMap[c] = iz + (iso - Fin[c,iz-1].z) /
+ * (Fin[c,iz].z - Fin[c,iz-1].z); no such iz gives -1.  Fin (n_col,nz,4)
+ * float32, zMap (n_col) float32. */
+int spm_izo_z(const float* Fin, int n_col, int nz, float iso, float* zMap, void* stream);
+
 /* Replaces df_loss_seed (spammm/SPM/AFM.py:3125-3200): central-difference df of
  * Fz = FEs[...,2] with |dtip|, L = 0.5*sum(w (df - target)^2)/sum(w) and the
  * exact transpose dL/dFEs (only the z channel non-zero).  target, weights

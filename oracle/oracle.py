@@ -79,6 +79,8 @@ def lib():
                                   _i, _f, _i, _vp, _vp]),
         "ora_relax_pp_d": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                   _i, _d, _i, _vp, _vp]),
+        "ora_convolve_z_f": (None, [_vp, _i, _i, _i, _vp, _vp]),
+        "ora_izo_z_f": (None, [_vp, _i, _i, _f, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -387,6 +389,26 @@ def compute_dissipation(FEs_fwd, FEs_bwd, h_scan, h_df, amp, osc_dir=(0., 0., 1.
         x = h_scan[mask]
         y = dF[:, :, mask]
         out[:, :, i] = np.abs(np.sum(np.diff(x) * (y[:, :, 1:] + y[:, :, :-1]) / 2.0, axis=2))
+    return out
+
+
+def convolve_z(FEs, weights, nz_out):
+    """convolveZ (kernels/AFM.cl:666-701) on the z-columns of FEs (..., nz_in, 4), canonical FP32."""
+    F = np.ascontiguousarray(FEs, dtype=np.float32)
+    nz_in = F.shape[-2]
+    w = np.ascontiguousarray(weights, dtype=np.float32).ravel()
+    assert w.size == nz_in - nz_out
+    out = np.zeros(F.shape[:-2] + (nz_out, 4), np.float32)
+    ncol = int(np.prod(F.shape[:-2]))
+    lib().ora_convolve_z_f(_p(F), ncol, int(nz_in), int(nz_out), _p(w), _p(out))
+    return out
+
+
+def izo_z(FEs, iso):
+    """izoZ (kernels/AFM.cl:705-723) on the z-columns of FEs (..., nz, 4), canonical FP32."""
+    F = np.ascontiguousarray(FEs, dtype=np.float32)
+    out = np.zeros(F.shape[:-2], np.float32)
+    lib().ora_izo_z_f(_p(F), int(out.size), int(F.shape[-2]), float(iso), _p(out))
     return out
 
 

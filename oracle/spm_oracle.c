@@ -303,3 +303,41 @@ void ora_relax_pp_d(const double* grid, int nx, int ny, int nz, const double* di
         relax_pp_pixel_d(grid, &G, pts + 4 * (size_t)i, nzs, tA, tB, tC, k, d0, relax, surf, max_iter, f2conv, use_fire,
                          FEs + (size_t)i * nzs * 4, PPs + (size_t)i * nzs * 4);
 }
+
+/* convolveZ (kernels/AFM.cl:666-701): per z-column c,
+ * Fout[c,izo] = sum over jz < nzin-nzout of Fin[c,izo+jz] * w[jz] on all four
+ * channels, accumulated in jz order from zero (fe += Fin*w, the fused
+ * multiply-add the OpenCL compiler contracts it to). */
+void ora_convolve_z_f(const float* Fin, int ncol, int nzin, int nzout, const float* w, float* Fout) {
+    const int nzw = nzin - nzout;
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < ncol; c++)
+        for (int izo = 0; izo < nzout; izo++) {
+            float fe[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int jz = 0; jz < nzw; jz++) {
+                const float* a = Fin + ((size_t)c * nzin + izo + jz) * 4;
+                for (int k = 0; k < 4; k++) fe[k] = fmaf(a[k], w[jz], fe[k]);
+            }
+            memcpy(Fout + ((size_t)c * nzout + izo) * 4, fe, sizeof fe);
+        }
+}
+
+/* izoZ (kernels/AFM.cl:705-723): per column the first iz >= 1 whose Fz
+ * exceeds iso gives iz + (iso - Fz[iz-1]) / (Fz[iz] - Fz[iz-1]); else -1. */
+void ora_izo_z_f(const float* Fin, int ncol, int nz, float iso, float* zMap) {
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < ncol; c++) {
+        const float* f = Fin + (size_t)c * nz * 4;
+        float oz = f[2], res = -1.f;
+        for (int iz = 1; iz < nz; iz++) {
+            const float fz = f[(size_t)iz * 4 + 2];
+            if (fz > iso) {
+                const float t = (iso - oz) / (fz - oz);
+                res = (float)iz + t;
+                break;
+            }
+            oz = fz;
+        }
+        zMap[c] = res;
+    }
+}

@@ -134,6 +134,8 @@ _SIGNATURES = {
     "spm_df_amp_dir": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _d, _vp, _i, _vp, _vp]),
     "spm_df_dir": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp]),
     "spm_dissipation": (_i, [_vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp]),
+    "spm_convolve_z": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp]),
+    "spm_izo_z": (_i, [_vp, _i, _i, ctypes.c_float, _vp, _vp]),
     "spm_df_loss_seed": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _d, _vp, _vp, _vp, _vp, _vp]),
     "spm_df_loss_scratch_bytes": (_ll, [_i, _i, _i]),
     "spm_df_loss_seed_noalloc": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _d, _vp, _vp, _vp, _vp]),

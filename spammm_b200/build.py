@@ -27,6 +27,7 @@ UNITS = {
     "direct.cu": [],
     "adjoint_grid.cu": [],
     "batched.cu": [],
+    "zmaps.cu": ["-fmad=false"],
 }
 
 

@@ -302,6 +302,40 @@ def dissipation(FEs_fwd, FEs_bwd, h_scan, h_df, amp, osc_dir=(0., 0., 1.)):
     return E
 
 
+def convolve_z(FEs, weights, nz_out):
+    """convolveZ (kernels/AFM.cl:666-701) on every z-column of FEs (..., nz_in, 4)
+    float32: out[..., izo, :] = sum_jz FEs[..., izo + jz, :] * weights[jz],
+    len(weights) = nz_in - nz_out -> (..., nz_out, 4) float32."""
+    FEs = _as_dev(FEs, F32, None, "FEs")
+    if FEs.dim() < 2 or FEs.shape[-1] != 4:
+        raise ValueError(f"FEs must be (..., nz, 4), got {tuple(FEs.shape)}")
+    FEs = FEs.contiguous()
+    nz_in = int(FEs.shape[-2])
+    w = _as_dev(np.asarray(weights, np.float32).ravel() if not isinstance(weights, torch.Tensor) else weights, F32,
+                None, "weights").reshape(-1).contiguous()
+    if int(w.numel()) != nz_in - int(nz_out):
+        raise ValueError(f"{w.numel()} weights for nz_in={nz_in}, nz_out={nz_out}: need nz_in - nz_out")
+    n_col = int(FEs.numel() // (4 * nz_in)) if nz_in else 0
+    out = torch.empty(tuple(FEs.shape[:-2]) + (int(nz_out), 4), dtype=F32, device=FEs.device)
+    check(lib().spm_convolve_z(ptr(FEs), n_col, nz_in, int(nz_out), ptr(w), ptr(out), stream_ptr()), "spm_convolve_z")
+    return out
+
+
+def izo_z(FEs, iso):
+    """izoZ (kernels/AFM.cl:705-723): per z-column of FEs (..., nz, 4) float32
+    the first iz >= 1 with Fz > iso, as iz + the linear fraction from iz-1
+    (-1 when Fz never exceeds iso) -> (...) float32."""
+    FEs = _as_dev(FEs, F32, None, "FEs")
+    if FEs.dim() < 2 or FEs.shape[-1] != 4:
+        raise ValueError(f"FEs must be (..., nz, 4), got {tuple(FEs.shape)}")
+    FEs = FEs.contiguous()
+    nz = int(FEs.shape[-2])
+    out = torch.empty(tuple(FEs.shape[:-2]), dtype=F32, device=FEs.device)
+    n_col = int(out.numel())
+    check(lib().spm_izo_z(ptr(FEs), n_col, nz, float(iso), ptr(out), stream_ptr()), "spm_izo_z")
+    return out
+
+
 def df_loss_seed(FEs, target_df, dtip, weights=None):
     """df_loss_seed on the device -> (loss (1,) f64, df (nx,ny,nz) f64, dL_dFEs (nx,ny,nz,4) f32)."""
     FEs = _fes_volume(FEs)

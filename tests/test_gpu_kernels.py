@@ -276,3 +276,35 @@ def test_dissipation_and_postprocess_match_reference(cuda, golden):
     np.testing.assert_allclose(res.df, g["pp_df"], rtol=1e-6, atol=1e-6 * np.abs(g["pp_df"]).max())
     assert np.array_equal(res.Fz, g["pp_Fz"])
     np.testing.assert_allclose(res.E_diss, g["pp_E"], rtol=1e-6, atol=1e-7)
+
+
+@pytest.mark.parametrize("nzw", [0, 1, 9, 64, 200])
+def test_convolve_z_matches_oracle(cuda, nzw):
+    """convolveZ (kernels/AFM.cl:666-701): bit-identical to the canonical-FP32 oracle."""
+    rng = np.random.default_rng(nzw)
+    nz_in = 230
+    F = rng.normal(size=(7, 5, nz_in, 4)).astype(np.float32)
+    w = rng.normal(size=nzw).astype(np.float32)
+    out = gpu.convolve_z(F, w, nz_in - nzw)
+    torch.cuda.synchronize()
+    assert out.shape == (7, 5, nz_in - nzw, 4)
+    assert np.array_equal(out.cpu().numpy(), O.convolve_z(F, w, nz_in - nzw))
+
+
+def test_izo_z_matches_oracle(cuda):
+    """izoZ (kernels/AFM.cl:705-723): bit-identical to the oracle, including
+    columns that never cross, cross at once, hold NaN, and nz = 1."""
+    rng = np.random.default_rng(7)
+    F = rng.normal(size=(33, 17, 40, 4)).astype(np.float32)
+    F[..., 2] = np.cumsum(np.abs(F[..., 2]), axis=-1) * rng.choice([-1.0, 1.0], size=(33, 17, 1)).astype(np.float32)
+    F[0, :, :, 2] = np.nan
+    F[1, 3, 5, 2] = np.nan
+    for iso in (0.0, 3.5, 1e6, -2.0):
+        z = gpu.izo_z(F, iso)
+        torch.cuda.synchronize()
+        assert z.shape == (33, 17)
+        np.testing.assert_array_equal(z.cpu().numpy(), O.izo_z(F, iso), err_msg=str(iso))  # NaN == NaN here
+    one = np.ones((4, 1, 4), np.float32)
+    assert np.array_equal(gpu.izo_z(one, 0.5).cpu().numpy(), np.full(4, -1.0, np.float32))
+    with pytest.raises(ValueError, match="weights"):
+        gpu.convolve_z(F, np.ones(3, np.float32), 40)

@@ -171,3 +171,30 @@ def test_oracle_relax_2d_uniform_field_equilibrium():
     assert not D[..., 2:].any()
     # E channel = layer index; node k sits at z = k*0.1: slices at z = 1.2 .. 0.9, stored lowest first
     np.testing.assert_allclose(FEs[0, :, 3], [9.0, 10.0, 11.0, 12.0], atol=1e-4)
+
+
+def test_oracle_convolve_z_and_izo_z_known_answers():
+    """convolveZ / izoZ restatements (kernels/AFM.cl:666-723).  The reference has
+    no host caller for these kernels and its OpenCL does not run here, so they
+    are pinned to known answers of the kernel loops: a z-convolution equals the
+    float64 sum of the same products (within FP32 accumulation), a one-weight
+    convolution is a scaled copy, an empty one is zero; the iso height follows
+    the kernel's iz + fraction-from-iz-1 rule, -1 without a crossing."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(3)
+    F = rng.normal(size=(4, 3, 20, 4)).astype(np.float32)
+    for nzw in (0, 1, 5, 17):
+        w = rng.normal(size=nzw).astype(np.float32)
+        out = O.convolve_z(F, w, 20 - nzw)
+        ref = np.zeros(out.shape, np.float64)
+        for jz in range(nzw):
+            ref += F[..., jz:jz + 20 - nzw, :].astype(np.float64) * np.float64(w[jz])
+        np.testing.assert_allclose(out, ref, rtol=0, atol=4e-7 * max(1, nzw) * np.abs(F).max() * max(1.0, np.abs(w).max(initial=0)))
+    np.testing.assert_array_equal(O.convolve_z(F, np.array([2.0], np.float32), 19), 2 * F[..., :19, :])
+    # iso heights
+    z = np.zeros((4, 6, 4), np.float32)
+    z[0, :, 2] = [0, 1, 2, 3, 4, 5]        # crosses 2.5 between iz=2 and 3 -> 3 + 0.5
+    z[1, :, 2] = [0, 0, 0, 0, 0, 0]        # never -> -1
+    z[2, :, 2] = [9, 8, 7, 6, 5, 4]        # Fz[1] > iso at once: 1 + (2.5-9)/(8-9) = 7.5
+    z[3, :, 2] = [0, np.nan, 0, 4, 0, 0]   # NaN never compares greater: crossing at iz=3, from iz=2
+    np.testing.assert_array_equal(O.izo_z(z, 2.5), np.array([3.5, -1.0, 7.5, 3.625], np.float32))
