@@ -47,6 +47,11 @@ enum spm_status {
 /* spm_scan_params.flags */
 #define SPM_FLAG_FIRE   1     /* FIRE integrator (OPT_FIRE=1); else plain damping (OPT_FIRE=0) */
 #define SPM_FLAG_FLIP_Z 2     /* store iz reversed: the z flip AFMulator.scan_fdbm applies (AFM.py:627-633) */
+#define SPM_FLAG_PAIRED 4     /* relaxStrokes only: the first n_scan/2 points start forward strokes, the
+                                 rest backward strokes, which step by -dTip and store iz in the order
+                                 opposite to the forward ones (SPM_FLAG_FLIP_Z inverted): the forward
+                                 and reverse=True scans of AFMulator.scan_fdbm (AFM.py:584-633) in one
+                                 launch; n_scan even */
 
 /* Scan/tip parameters shared by the relaxation and sampling kernels.  Field
  * names follow the reference's kernel arguments (kernels/AFM.cl:345-562). */

@@ -291,9 +291,53 @@ class AFMulator:
         tip_disp {'dx','dy','dz'} each (nx,ny,nz)).  With ``return_device`` the
         arrays stay CUDA tensors.
         """
+        base, stiffness_v, dpos0_v, relax_pars_v = self._scan_fdbm_setup(osc_dir, base_pos, use_fire, K_LAT, K_RAD,
+                                                                         bond_length, stiffness, dpos0, relax_pars)
+        nx_s, ny_s, nz_s = len(scan_xs), len(scan_ys), len(probe_heights)
+        pts, dTip = self._scan_fdbm_points(scan_xs, scan_ys, probe_heights, mol_z, bond_length, base, reverse)
+        n_scan = nx_s * ny_s
+        self._check_alloc(n_scan * nz_s * 16, "scan_fdbm FEs")
+        self.realloc_scan_buffers(n_scan, nz_s)
+        P = self._flags_params(dinv=(self.fdbm_dinvA, self.fdbm_dinvB, self.fdbm_dinvC), dTip=dTip,
+                               stiffness=stiffness_v, dpos0=dpos0_v, relax_params=relax_pars_v, nz=nz_s,
+                               flip_z=not reverse, raster_ny=ny_s)
+        FEs, disps = gpu.relax_strokes(self.img_FF_fdbm, P, torch.from_numpy(pts).to(self.device))
+        return self._scan_outputs(FEs, disps, (nx_s, ny_s, nz_s), return_device)
+
+    def scan_fdbm_pair(self, scan_xs, scan_ys, probe_heights, mol_z=0.0, ppm_mode=True, use_fire=True,
+                       K_LAT=0.03, K_RAD=20.0, bond_length=3.0, stiffness=None, dpos0=None, relax_pars=None,
+                       osc_dir=(0., 0., 1.), base_pos=(0., 0., 0.), return_device=False):
+        """The forward and the backward (reverse=True) strokes of scan_fdbm in
+        one relaxation launch (SPM_FLAG_PAIRED), as run_morse_pp_afm and
+        run_fdbm_pp_from_density (AFM_utils.py:3537-3553, 4091-4108) take them
+        for the dissipation.  Each stroke's arithmetic is that of the separate
+        calls, so the results are theirs bit for bit.
+
+        Returns ((FEs_fwd, tip_disp_fwd), (FEs_bwd, tip_disp_bwd)), both with
+        iz=0 the lowest height, as two scan_fdbm calls return them."""
+        base, stiffness_v, dpos0_v, relax_pars_v = self._scan_fdbm_setup(osc_dir, base_pos, use_fire, K_LAT, K_RAD,
+                                                                         bond_length, stiffness, dpos0, relax_pars)
+        nx_s, ny_s, nz_s = len(scan_xs), len(scan_ys), len(probe_heights)
+        pts_f, dTip = self._scan_fdbm_points(scan_xs, scan_ys, probe_heights, mol_z, bond_length, base, False)
+        pts_b, _ = self._scan_fdbm_points(scan_xs, scan_ys, probe_heights, mol_z, bond_length, base, True)
+        n_scan = nx_s * ny_s
+        self._check_alloc(2 * n_scan * nz_s * 16, "scan_fdbm_pair FEs")
+        self.realloc_scan_buffers(2 * n_scan, nz_s)
+        # the two point sets form one (2 nx) x ny raster: forward strokes, then backward ones
+        P = self._flags_params(dinv=(self.fdbm_dinvA, self.fdbm_dinvB, self.fdbm_dinvC), dTip=dTip,
+                               stiffness=stiffness_v, dpos0=dpos0_v, relax_params=relax_pars_v, nz=nz_s,
+                               flip_z=True, raster_ny=ny_s, paired=True)
+        pts = torch.from_numpy(np.concatenate([pts_f, pts_b])).to(self.device)
+        FEs, disps = gpu.relax_strokes(self.img_FF_fdbm, P, pts)
+        shape = (nx_s, ny_s, nz_s)
+        return (self._scan_outputs(FEs[:n_scan], disps[:n_scan], shape, return_device),
+                self._scan_outputs(FEs[n_scan:], disps[n_scan:], shape, return_device))
+
+    def _scan_fdbm_setup(self, osc_dir, base_pos, use_fire, K_LAT, K_RAD, bond_length, stiffness, dpos0,
+                         relax_pars):
+        """Validated scan frame and probe vectors of scan_fdbm (AFM.py:548-575)."""
         if self.img_FF_fdbm is None:
             raise AssertionError("call setup_fdbm_grid() first")
-        nx_s, ny_s, nz_s = len(scan_xs), len(scan_ys), len(probe_heights)
         osc_n = np.asarray(osc_dir, dtype=np.float32)
         osc_norm = float(np.linalg.norm(osc_n))
         if osc_n.shape != (3,) or not np.isfinite(osc_norm) or osc_norm <= 0.0:
@@ -311,22 +355,16 @@ class AFMulator:
             relax_pars_v = self.relax_pars.copy()
         else:
             relax_pars_v = np.array([0.3, 0.2, 0.03, 0.3], dtype=np.float32)
-        pts, dTip = self._scan_fdbm_points(scan_xs, scan_ys, probe_heights, mol_z, bond_length, base, reverse)
-        n_scan = nx_s * ny_s
-        self._check_alloc(n_scan * nz_s * 16, "scan_fdbm FEs")
-        self.realloc_scan_buffers(n_scan, nz_s)
-        nx, ny, nz = self.fdbm_shape
-        P = self._flags_params(dinv=(self.fdbm_dinvA, self.fdbm_dinvB, self.fdbm_dinvC), dTip=dTip,
-                               stiffness=stiffness_v, dpos0=dpos0_v, relax_params=relax_pars_v, nz=nz_s,
-                               flip_z=not reverse, raster_ny=ny_s)
-        FEs, disps = gpu.relax_strokes(self.img_FF_fdbm, P, torch.from_numpy(pts).to(self.device))
-        FEs = FEs.reshape(nx_s, ny_s, nz_s, 4)
-        disps = disps.reshape(nx_s, ny_s, nz_s, 4)
+        return base, stiffness_v, dpos0_v, relax_pars_v
+
+    @staticmethod
+    def _scan_outputs(FEs, disps, shape, return_device):
+        FEs = FEs.reshape(*shape, 4)
+        disps = disps.reshape(*shape, 4)
         if not return_device:
             FEs = gpu.to_host(FEs)
             disps = gpu.to_host(disps)
-        tip_disp = {"dx": disps[..., 0], "dy": disps[..., 1], "dz": disps[..., 2]}
-        return FEs, tip_disp
+        return FEs, {"dx": disps[..., 0], "dy": disps[..., 1], "dz": disps[..., 2]}
 
     def scan_fdbm_2d(self, scan_xs, scan_ys, probe_heights, mol_z=0.0, K_LAT=0.03, dt=0.3, damp=0.2,
                      return_device=False):

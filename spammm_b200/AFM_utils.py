@@ -236,8 +236,9 @@ def run_morse_pp_afm(tag, atomPos, atomTypes, origin, step, ngrid, outdir=None, 
     kw = dict(mol_z=mol_z, K_LAT=float(scan_spec.K_LAT), K_RAD=float(scan_spec.K_RAD),
               bond_length=float(scan_spec.bond_length), ppm_mode=True, use_fire=True, osc_dir=scan_spec.osc_dir,
               base_pos=(0., 0., 0.), return_device=True)
-    FEs_full, tip_disp_full = afmulator.scan_fdbm(scan_xs_full, scan_ys_full, h_scan, **kw)
-    FEs_bwd_full, _ = afmulator.scan_fdbm(scan_xs_full, scan_ys_full, h_scan, reverse=True, **kw)
+    # forward and backward strokes in one relaxation launch (the reference's two scan_fdbm calls)
+    (FEs_full, tip_disp_full), (FEs_bwd_full, _) = afmulator.scan_fdbm_pair(scan_xs_full, scan_ys_full, h_scan,
+                                                                            **kw)
     sx = slice(pad_x, pad_x + len(scan_xs))
     sy = slice(pad_y, pad_y + len(scan_ys))
     FEs = FEs_full[sx, sy].contiguous()

@@ -165,13 +165,21 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
     const float dh2 = -P.dTip[2];                  // MODE 3: descent per slice (dTip.z = -dh)
     const float cv2 = 1.f - P.relax_params[1];     // MODE 3: velocity retention 1 - damp
 
+    // SPM_FLAG_PAIRED (MODE 0): strokes of the second half go backward
+    const int half = (MODE == 0 && (P.flags & SPM_FLAG_PAIRED)) ? n_scan / 2 : n_scan;
+
     int k = counter ? next_pixel(counter, n_scan, P.raster_ny) : pixel_of_thread(n_scan, P.raster_ny);
     V3 tip, pos, v;
+    V3 dTipS = dTip;  // this stroke's step and z order
+    bool flipS = flip;
     Integrator I;
     float4 fe;
     int iz = 0, it = 0, total_it = 0;
     auto start = [&](int kp) {
         const float4 p4 = pts[kp];
+        const bool bwd = kp >= half;
+        dTipS = bwd ? mk3(-dTip.x, -dTip.y, -dTip.z) : dTip;
+        flipS = flip != bwd;
         tip = mk3(p4.x, p4.y, p4.z);
         pos = (MODE == 0) ? mk3(tip.x + d0r.x, tip.y + d0r.y, tip.z + d0r.z) : (MODE == 3 ? tip : add3(tip, d0r));
         I.dt = P.relax_params[0];
@@ -259,7 +267,7 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
             done = (dot3(f, f) < P.f2conv) || (it >= max_iter);
         }
         if (done) {
-            const int oz = flip ? (nzs - 1 - iz) : iz;
+            const int oz = flipS ? (nzs - 1 - iz) : iz;
             const size_t o = (size_t)k * nzs + oz;
             if (MODE == 0) {
                 FEs[o] = fe;
@@ -270,8 +278,8 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
                 const V3 r = rotmat(mk3(g.x, g.y, g.z), a, b, c);
                 FEs[o] = make_float4(r.x, r.y, r.z, g.w);
             }
-            tip = add3(tip, dTip);
-            pos = add3(pos, dTip);
+            tip = add3(tip, dTipS);
+            pos = add3(pos, dTipS);
             v = mk3(0.f, 0.f, 0.f);
             fe = make_float4(0.f, 0.f, 0.f, 0.f);
             it = 0;
@@ -318,7 +326,8 @@ int check_scan_args(const char* who, const float* grid, int nx, int ny, int nz, 
     SPM_REQUIRE(mul_ok((long long)nx * ny, nz, &t), "%s: grid size overflows", who);
     SPM_REQUIRE(mul_ok(n_scan, (long long)p->nz * 4, &t), "%s: output size overflows", who);
     SPM_REQUIRE(p->raster_ny >= 0, "%s: raster_ny=%d < 0", who, p->raster_ny);
-    SPM_REQUIRE((p->flags & ~(SPM_FLAG_FIRE | SPM_FLAG_FLIP_Z)) == 0, "%s: unknown flags 0x%x", who, p->flags);
+    SPM_REQUIRE((p->flags & ~(SPM_FLAG_FIRE | SPM_FLAG_FLIP_Z | SPM_FLAG_PAIRED)) == 0, "%s: unknown flags 0x%x", who,
+                p->flags);
     return SPM_OK;
 }
 
@@ -666,6 +675,10 @@ extern "C" int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz,
                 mode == SPM_RELAX_2D, "spm_relax_ex: mode=%d", mode);
     int rc = check_scan_args("spm_relax_ex", grid, nx, ny, nz, points, n_scan, p, FEs);
     if (rc) return rc;
+    if (p->flags & SPM_FLAG_PAIRED)
+        SPM_REQUIRE(mode == SPM_RELAX_STROKES && n_scan % 2 == 0,
+                    "spm_relax_ex: SPM_FLAG_PAIRED needs mode SPM_RELAX_STROKES and an even n_scan (mode=%d, n_scan=%d)",
+                    mode, n_scan);
     if (n_scan == 0 || p->nz == 0) return SPM_OK;
     if (mode != SPM_RELAX_TILTED)
         SPM_REQUIRE(disps != nullptr && aligned16(disps), "spm_relax_ex: disps/PPs null or misaligned");
@@ -705,6 +718,7 @@ extern "C" int spm_fe_in_strokes_tilted(const float* grid, int nx, int ny, int n
     clear_error();
     int rc = check_scan_args("spm_fe_in_strokes_tilted", grid, nx, ny, nz, points, n_scan, p, FEs);
     if (rc) return rc;
+    SPM_REQUIRE(!(p->flags & SPM_FLAG_PAIRED), "spm_fe_in_strokes_tilted: SPM_FLAG_PAIRED is for relaxStrokes only");
     if (n_scan == 0 || p->nz == 0) return SPM_OK;
     spm_scan_params P = normalized(p, n_scan);
     raw_kernel<<<static_blocks(n_scan, P), RX_THREADS, 0, as_stream(stream)>>>(

@@ -3,9 +3,10 @@
 the direct Morse path and its VJP against the reference's FP64 oracles."""
 import numpy as np
 import pytest
+import torch
 
 from oracle import oracle as O
-from spammm_b200 import AFM
+from spammm_b200 import AFM, _lib
 from spammm_b200.AFM import AFMulator
 
 pytestmark = pytest.mark.gpu
@@ -49,6 +50,35 @@ def test_scan_fdbm_flip_and_reverse_match_oracle(cuda):
                                   afm.relax_pars, flip=not reverse)
         assert np.array_equal(FEs, oFE.reshape(5, 4, 6, 4))
         assert np.array_equal(disp["dz"], oD.reshape(5, 4, 6, 4)[..., 2])
+
+
+def test_scan_fdbm_pair_equals_two_scans(cuda):
+    """Forward + backward strokes in one launch (SPM_FLAG_PAIRED) give the two
+    scan_fdbm calls' results bit for bit; the C ABI rejects the flag elsewhere."""
+    rng = np.random.default_rng(2)
+    F_total = (0.02 * rng.standard_normal((24, 22, 30, 4))).astype(np.float32)
+    afm = AFMulator(use_morse=True)
+    afm.setup_fdbm_grid(F_total, np.array([-3., -2.75, -1.0], np.float32), 0.25)
+    xs = np.linspace(-1, 1, 7).astype(np.float32)
+    ys = np.linspace(-1, 1, 5).astype(np.float32)
+    hs = np.linspace(3.0, 3.7, 8).astype(np.float32)
+    kw = dict(mol_z=0.2, K_LAT=0.03, K_RAD=20.0, bond_length=3.0, base_pos=(0.05, -0.02, 0.0))
+    (Ff, df_), (Fb, db_) = afm.scan_fdbm_pair(xs, ys, hs, **kw)
+    Ff1, d1 = afm.scan_fdbm(xs, ys, hs, **kw)
+    Fb1, d2 = afm.scan_fdbm(xs, ys, hs, reverse=True, **kw)
+    assert Ff.shape == Fb.shape == (7, 5, 8, 4)
+    assert np.array_equal(Ff, Ff1) and np.array_equal(Fb, Fb1)
+    for c in ("dx", "dy", "dz"):
+        assert np.array_equal(df_[c], d1[c]) and np.array_equal(db_[c], d2[c])
+    assert not np.array_equal(Ff, Fb)  # the strokes differ: hysteresis or at least different start
+    # the flag is relaxStrokes-only and needs an even stroke count
+    from spammm_b200 import gpu
+    P = _lib.make_scan_params(dinv=(afm.fdbm_dinvA, afm.fdbm_dinvB, afm.fdbm_dinvC), nz=4, paired=True)
+    pts = torch.zeros((3, 4), dtype=torch.float32, device="cuda")
+    with pytest.raises(ValueError, match="PAIRED"):
+        gpu.relax_strokes(afm.img_FF_fdbm, P, pts)
+    with pytest.raises(ValueError, match="PAIRED"):
+        gpu.relax_strokes_tilted(afm.img_FF_fdbm, P, torch.zeros((4, 4), dtype=torch.float32, device="cuda"))
 
 
 def _toy(n_atoms, seed):
