@@ -479,7 +479,7 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
     auto start = [&]() {
         const spm_batch_mol* D = mols + m;
         G = axis_view<LAYOUT>(D, grid);
-        T.x0 = -1;  // new slab: nothing cached
+        T.kx = __int_as_float(0x7fc00000);  // new slab: nothing cached (NaN matches no cell)
         nzs = D->nz_steps;
         pix = D->pix_off + k;
         sbase = D->state_off + (long long)k * nzs;
@@ -543,7 +543,7 @@ __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const 
                                                   int* __restrict__ iter_count, int k, float dz, unsigned members) {
     const AxisView G = axis_view<LAYOUT>(D, grid);
     TexelCache T;
-    T.x0 = -1;
+    T.kx = __int_as_float(0x7fc00000);  // nothing cached (NaN matches no cell)
     const int nzs = D->nz_steps;
     const int pix = D->pix_off + k;
     const long long sbase = D->state_off + (long long)k * nzs;

@@ -301,38 +301,67 @@ __device__ __forceinline__ float4 interp_fe_cell(const AxisView& G, V3 p) {
 // iterations: the probe moves ~1e-3..1e-2 A per iteration inside a 0.1 A
 // cell, so the cell rarely changes and most samples need no load at all.
 struct TexelCache {
-    int x0, y0, z0;  // cell (x0 < 0: empty)
+    float kx, ky, kz;  // floor of the cached cell's texel coordinates (NaN: empty)
     ulonglong2 f000, f100, f010, f110, f001, f101, f011, f111;
 };
 
+// tex_axis's first half: the texel coordinate t of u and its floor fi (the
+// lerp weight is t - fi).  The cell's indices, the wrap and the range test
+// are functions of fi alone.
+__device__ __forceinline__ float tex_coord(float u, float fn, float& fi) {
+    const float s = u - floorf(u);
+    const float t = __fmaf_rn(s, fn, -0.5f);
+    fi = floorf(t);
+    return t - fi;
+}
+
+// tex_axis's second half for a given floor fi: false outside the sampler's
+// range [-1, n), else the wrapped indices i0, i1.
+__device__ __forceinline__ bool tex_index(float fi, int n, float fn, int& i0, int& i1) {
+    if (!(fi >= -1.f && fi < fn)) return false;  // <=> t in [-1, fn) for t in [fi, fi + 1)
+    int i = (int)fi;
+    if (i < 0) i += n;
+    int j = i + 1;
+    if (j >= n) j -= n;
+    i0 = i;
+    i1 = j;
+    return true;
+}
+
 // interp_fe_cell with a TexelCache: identical values (the same texels, the
-// same lerps); loads only when the cell differs from the cached one.
+// same lerps); loads only when the cell differs from the cached one.  The
+// cell is identified by the floors of its three texel coordinates, so a
+// sample inside the cached cell needs no index arithmetic, wrap or range test
+// (a cached cell passed them; equal floors give the same indices).
 template <typename IDX, bool SLAB, int LAYOUT>
 __device__ __forceinline__ float4 interp_fe_cached(const AxisView& G, V3 p, TexelCache& T) {
     const float u = __fmaf_rn(p.x, G.ax, G.aw);
     const float v = __fmaf_rn(p.y, G.by, G.bw);
     const float w = __fmaf_rn(p.z, G.cz, G.cw);
-    int x0, x1, y0, y1, z0, z1;
-    float ax, ay, az;
-    bool ok = tex_axis(u, G.nx, G.fnx, x0, x1, ax);
-    ok = tex_axis(v, G.ny, G.fny, y0, y1, ay) && ok;
-    ok = tex_axis(w, G.nz, G.fnz, z0, z1, az) && ok;
-    (void)x1;
-    if (SLAB) {
-        z0 -= G.z_lo;
-        z1 -= G.z_lo;
-        ok = ok && (unsigned)z0 < (unsigned)G.nz_slab && (unsigned)z1 < (unsigned)G.nz_slab;
-    }
-    if (!ok) {
-        float nan = __int_as_float(0x7fc00000);
-        return make_float4(nan, nan, nan, nan);
-    }
-    if (x0 != T.x0 || y0 != T.y0 || z0 != T.z0) {
+    float fx, fy, fz;
+    const float ax = tex_coord(u, G.fnx, fx);
+    const float ay = tex_coord(v, G.fny, fy);
+    const float az = tex_coord(w, G.fnz, fz);
+    if (!(fx == T.kx && fy == T.ky && fz == T.kz)) {  // NaN never equals: an empty cache or a NaN position
+        int x0, x1, y0, y1, z0, z1;
+        bool ok = tex_index(fx, G.nx, G.fnx, x0, x1);
+        ok = tex_index(fy, G.ny, G.fny, y0, y1) && ok;
+        ok = tex_index(fz, G.nz, G.fnz, z0, z1) && ok;
+        (void)x1;
+        if (SLAB) {
+            z0 -= G.z_lo;
+            z1 -= G.z_lo;
+            ok = ok && (unsigned)z0 < (unsigned)G.nz_slab && (unsigned)z1 < (unsigned)G.nz_slab;
+        }
+        if (!ok) {
+            float nan = __int_as_float(0x7fc00000);
+            return make_float4(nan, nan, nan, nan);
+        }
         load_cell<LAYOUT, IDX>(G, x0, y0, y1, z0, z1, T.f000, T.f100, T.f010, T.f110, T.f001, T.f101, T.f011,
                                T.f111);
-        T.x0 = x0;
-        T.y0 = y0;
-        T.z0 = z0;
+        T.kx = fx;
+        T.ky = fy;
+        T.kz = fz;
     }
     const f2 AX = bc(ax), MX = bc(1.f - ax), AY = bc(ay), MY = bc(1.f - ay), AZ = bc(az), MZ = bc(1.f - az);
     const ulonglong2 c00 = lerp_pk(AX, MX, T.f000, T.f100);
