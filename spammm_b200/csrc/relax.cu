@@ -144,11 +144,16 @@ __device__ __forceinline__ void pp_emit(const GridView& G, const PPFrame& F, V3 
 
 // MODE 0: relaxStrokes; MODE 1: relaxStrokesTilted; MODE 2: PP (differentiable
 // path); MODE 3: relaxStrokes2D.
-template <int MODE, typename IDX>
+// CACHE (MODE 0/1): the FIRE loop samples through a register TexelCache (the
+// cell's eight texels reloaded only when the cell changes; same values).
+template <int MODE, typename IDX, bool CACHE>
 __global__ void __launch_bounds__(RX_THREADS)
 relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
              float4* __restrict__ FEs, float4* __restrict__ disps, int* __restrict__ iter_count,
              unsigned* __restrict__ counter) {
+    const float fnx = (float)G.nx, fny = (float)G.ny, fnz = (float)G.nz;
+    TexelCache T;
+    T.kx = __int_as_float(0x7fc00000);  // NaN matches no cell
     const bool fire = (P.flags & SPM_FLAG_FIRE) != 0;
     const bool flip = (P.flags & SPM_FLAG_FLIP_Z) != 0;
     const int nzs = P.nz;
@@ -249,7 +254,8 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
         }
         bool done = max_iter <= 0;
         if (!done) {
-            fe = interp_fe<IDX>(G, pos);
+            if constexpr (CACHE) fe = interp_fe_cached_full<IDX>(G, fnx, fny, fnz, pos, T);
+            else fe = interp_fe<IDX>(G, pos);
             V3 f;
             if (MODE == 0) {
                 const V3 ft = tip_force(sub3(pos, tip), kk, d0);
@@ -359,7 +365,7 @@ spm_scan_params normalized(const spm_scan_params* p, int n_scan) {
 template <int MODE, typename IDX>
 int launch_relax(const GridView& G, const float4* pts, int n_scan, const spm_scan_params& P, float4* FEs,
                  float4* disps, int* iter_count, unsigned* counter, cudaStream_t st) {
-    auto kern = relax_kernel<MODE, IDX>;
+    auto kern = relax_kernel<MODE, IDX, (MODE == 0 || MODE == 1)>;
     int blocks = static_blocks(n_scan, P);
     if (counter) {
         // persistent: as many CTAs as are co-resident; the counter balances the rest

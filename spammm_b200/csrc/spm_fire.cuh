@@ -328,6 +328,59 @@ __device__ __forceinline__ bool tex_index(float fi, int n, float fn, int& i0, in
     return true;
 }
 
+// The packed trilinear blend of a cached cell (interp_fe's lerp order).
+__device__ __forceinline__ float4 blend_cached(const TexelCache& T, float ax, float ay, float az) {
+    const f2 AX = bc(ax), MX = bc(1.f - ax), AY = bc(ay), MY = bc(1.f - ay), AZ = bc(az), MZ = bc(1.f - az);
+    const ulonglong2 c00 = lerp_pk(AX, MX, T.f000, T.f100);
+    const ulonglong2 c10 = lerp_pk(AX, MX, T.f010, T.f110);
+    const ulonglong2 c01 = lerp_pk(AX, MX, T.f001, T.f101);
+    const ulonglong2 c11 = lerp_pk(AX, MX, T.f011, T.f111);
+    const ulonglong2 c0 = lerp_pk(AY, MY, c00, c10);
+    const ulonglong2 c1 = lerp_pk(AY, MY, c01, c11);
+    const ulonglong2 c = lerp_pk(AZ, MZ, c0, c1);
+    float4 r;
+    upk(c.x, r.x, r.y);
+    upk(c.y, r.z, r.w);
+    return r;
+}
+
+// interp_fe on a full (nz,ny,nx) grid with any sampling transform, with a
+// TexelCache: the same texels and lerps, so the same sample; the eight
+// texels are loaded only when the cell (the floors of the three texel
+// coordinates) changes.  fnx, fny, fnz: the dimensions as floats.
+template <typename IDX>
+__device__ __forceinline__ float4 interp_fe_cached_full(const GridView& G, float fnx, float fny, float fnz, V3 p,
+                                                        TexelCache& T) {
+    const float u = __fmaf_rn(p.x, G.dA.x, __fmaf_rn(p.y, G.dA.y, __fmaf_rn(p.z, G.dA.z, G.dA.w)));
+    const float v = __fmaf_rn(p.x, G.dB.x, __fmaf_rn(p.y, G.dB.y, __fmaf_rn(p.z, G.dB.z, G.dB.w)));
+    const float w = __fmaf_rn(p.x, G.dC.x, __fmaf_rn(p.y, G.dC.y, __fmaf_rn(p.z, G.dC.z, G.dC.w)));
+    float fx, fy, fz;
+    const float ax = tex_coord(u, fnx, fx);
+    const float ay = tex_coord(v, fny, fy);
+    const float az = tex_coord(w, fnz, fz);
+    if (!(fx == T.kx && fy == T.ky && fz == T.kz)) {
+        int x0, x1, y0, y1, z0, z1;
+        bool ok = tex_index(fx, G.nx, fnx, x0, x1);
+        ok = tex_index(fy, G.ny, fny, y0, y1) && ok;
+        ok = tex_index(fz, G.nz, fnz, z0, z1) && ok;
+        if (!ok) {
+            float nan = __int_as_float(0x7fc00000);
+            return make_float4(nan, nan, nan, nan);
+        }
+        const IDX r00 = ((IDX)z0 * G.ny + y0) * G.nx, r10 = ((IDX)z0 * G.ny + y1) * G.nx;
+        const IDX r01 = ((IDX)z1 * G.ny + y0) * G.nx, r11 = ((IDX)z1 * G.ny + y1) * G.nx;
+        const ulonglong2* g = reinterpret_cast<const ulonglong2*>(G.g);
+        T.f000 = __ldg(g + r00 + x0); T.f100 = __ldg(g + r00 + x1);
+        T.f010 = __ldg(g + r10 + x0); T.f110 = __ldg(g + r10 + x1);
+        T.f001 = __ldg(g + r01 + x0); T.f101 = __ldg(g + r01 + x1);
+        T.f011 = __ldg(g + r11 + x0); T.f111 = __ldg(g + r11 + x1);
+        T.kx = fx;
+        T.ky = fy;
+        T.kz = fz;
+    }
+    return blend_cached(T, ax, ay, az);
+}
+
 // interp_fe_cell with a TexelCache: identical values (the same texels, the
 // same lerps); loads only when the cell differs from the cached one.  The
 // cell is identified by the floors of its three texel coordinates, so a
@@ -363,18 +416,7 @@ __device__ __forceinline__ float4 interp_fe_cached(const AxisView& G, V3 p, Texe
         T.ky = fy;
         T.kz = fz;
     }
-    const f2 AX = bc(ax), MX = bc(1.f - ax), AY = bc(ay), MY = bc(1.f - ay), AZ = bc(az), MZ = bc(1.f - az);
-    const ulonglong2 c00 = lerp_pk(AX, MX, T.f000, T.f100);
-    const ulonglong2 c10 = lerp_pk(AX, MX, T.f010, T.f110);
-    const ulonglong2 c01 = lerp_pk(AX, MX, T.f001, T.f101);
-    const ulonglong2 c11 = lerp_pk(AX, MX, T.f011, T.f111);
-    const ulonglong2 c0 = lerp_pk(AY, MY, c00, c10);
-    const ulonglong2 c1 = lerp_pk(AY, MY, c01, c11);
-    const ulonglong2 c = lerp_pk(AZ, MZ, c0, c1);
-    float4 r;
-    upk(c.x, r.x, r.y);
-    upk(c.y, r.z, r.w);
-    return r;
+    return blend_cached(T, ax, ay, az);
 }
 
 }  // namespace spm
