@@ -106,15 +106,19 @@ __device__ __forceinline__ PPFrame pp_frame(const spm_scan_params& P) {
 // One SPM_RELAX_PP iteration (the direct path's bookkeeping: the convergence
 // test comes before the update).  Returns true when the z-step is finished;
 // conv tells whether it converged.  SLAB: a sample outside the stored layers
-// (NaN) ends the z-step at once, not converged.
-template <typename IDX, bool SLAB>
+// (NaN) ends the z-step at once, not converged.  CACHE: sample through the
+// texel cache T (full grids; fnx, fny, fnz the dimensions as floats).
+template <typename IDX, bool SLAB, bool CACHE>
 __device__ __forceinline__ bool pp_iter(const GridView& G, const PPFrame& F, V3 tip, V3& pos, V3& v, Integrator& I,
-                                        float4& fe, int& it, int& total_it, bool& conv) {
+                                        float4& fe, int& it, int& total_it, bool& conv, TexelCache& T, float fnx,
+                                        float fny, float fnz) {
+    static_assert(!(CACHE && SLAB), "the texel cache samples full grids");
     conv = false;
     if (it >= F.max_iter) return true;
     ++it;
     ++total_it;
-    fe = interp_fe<IDX, SLAB>(G, pos);
+    if constexpr (CACHE) fe = interp_fe_cached_full<IDX>(G, fnx, fny, fnz, pos, T);
+    else fe = interp_fe<IDX, SLAB>(G, pos);
     if (SLAB && fe.w != fe.w) return true;
     const V3 ft = rotmatT(tip_force(rotmat(sub3(pos, tip), F.a, F.b, F.c), F.kk, F.d0), F.a, F.b, F.c);
     V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
@@ -144,8 +148,9 @@ __device__ __forceinline__ void pp_emit(const GridView& G, const PPFrame& F, V3 
 
 // MODE 0: relaxStrokes; MODE 1: relaxStrokesTilted; MODE 2: PP (differentiable
 // path); MODE 3: relaxStrokes2D.
-// CACHE (MODE 0/1): the FIRE loop samples through a register TexelCache (the
-// cell's eight texels reloaded only when the cell changes; same values).
+// CACHE (MODE 0-2): the FIRE loop samples through a register TexelCache (the
+// cell's eight texels reloaded only when the cell changes; same values; all
+// strokes share the grid, so a lane keeps its cache from pixel to pixel).
 template <int MODE, typename IDX, bool CACHE>
 __global__ void __launch_bounds__(RX_THREADS)
 relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
@@ -204,7 +209,7 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
     while (k >= 0) {
         if (MODE == 2) {
             bool conv;
-            if (pp_iter<IDX, false>(G, F, tip, pos, v, I, fe, it, total_it, conv)) {
+            if (pp_iter<IDX, false, CACHE>(G, F, tip, pos, v, I, fe, it, total_it, conv, T, fnx, fny, fnz)) {
                 const size_t o = (size_t)k * nzs + iz;
                 pp_emit<IDX, false>(G, F, pos, fe, it, conv, FEs + o, disps + o);
                 tip = add3(tip, dTip);
@@ -365,7 +370,7 @@ spm_scan_params normalized(const spm_scan_params* p, int n_scan) {
 template <int MODE, typename IDX>
 int launch_relax(const GridView& G, const float4* pts, int n_scan, const spm_scan_params& P, float4* FEs,
                  float4* disps, int* iter_count, unsigned* counter, cudaStream_t st) {
-    auto kern = relax_kernel<MODE, IDX, (MODE == 0 || MODE == 1)>;
+    auto kern = relax_kernel<MODE, IDX, (MODE <= 2)>;
     int blocks = static_blocks(n_scan, P);
     if (counter) {
         // persistent: as many CTAs as are co-resident; the counter balances the rest
