@@ -732,8 +732,12 @@ constexpr size_t NM_SMEM = 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(
 //     barriers is dense;
 //   * every non-zero node is zeroed after it is staged (by the last atom
 //     group), so the adjoint grid is left cleared for the next call.
+// Three CTAs per SM (80 registers, a few bytes spilled, 3 x 70 KB of shared
+// memory): the loop is bound by its dependency chains, so the third CTA's
+// warps pay (12.2 -> 10.7 ms on the 64-molecule fit against two CTAs at 128
+// registers).
 template <int KIND, bool ON>
-__global__ void __launch_bounds__(NM_THREADS, 2)
+__global__ void __launch_bounds__(NM_THREADS, 3)
 batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk,
                            const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
                            NodeSites S, unsigned long long* __restrict__ gq, const int* __restrict__ box,
