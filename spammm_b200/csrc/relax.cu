@@ -640,19 +640,22 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     SPM_REQUIRE(shape->rx_ctas_per_sm >= 0, "spm_batch_relax: rx_ctas_per_sm=%d", shape->rx_ctas_per_sm);
     int th_log2 = 0;
     while ((1 << th_log2) < h) th_log2++;
-    SPM_REQUIRE(shape->rx_regs >= 0 && shape->rx_regs <= 2, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
+    SPM_REQUIRE(shape->rx_regs >= 0 && shape->rx_regs <= 3, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
     SPM_REQUIRE(shape->grid_layout == 0 || shape->grid_layout == 1, "spm_batch_relax: grid_layout=%d",
                 shape->grid_layout);
     SPM_REQUIRE(shape->rx_sync == 0 || shape->rx_sync == 1, "spm_batch_relax: rx_sync=%d", shape->rx_sync);
     using Kern = decltype(&batch_relax_kernel<3, false, 2>);
-    // [rx_sync][grid_layout][rx_regs]
-    static const Kern table[2][2][3] = {
-        {{batch_relax_kernel<3, false, 2>, batch_relax_kernel<4, false, 2>, batch_relax_kernel<2, true, 2>},
-         {batch_relax_kernel<3, false, 4>, batch_relax_kernel<4, false, 4>, batch_relax_kernel<2, true, 4>}},
+    // [rx_sync][grid_layout][rx_regs]: 0 = 80 registers, 1 = 64, 2 = texel cache at up to 128,
+    // 3 = texel cache squeezed to 80 (some values spilled, 50% more warps)
+    static const Kern table[2][2][4] = {
+        {{batch_relax_kernel<3, false, 2>, batch_relax_kernel<4, false, 2>, batch_relax_kernel<2, true, 2>,
+          batch_relax_kernel<3, true, 2>},
+         {batch_relax_kernel<3, false, 4>, batch_relax_kernel<4, false, 4>, batch_relax_kernel<2, true, 4>,
+          batch_relax_kernel<3, true, 4>}},
         {{batch_relax_sync_kernel<3, false, 2>, batch_relax_sync_kernel<4, false, 2>,
-          batch_relax_sync_kernel<2, true, 2>},
+          batch_relax_sync_kernel<2, true, 2>, batch_relax_sync_kernel<3, true, 2>},
          {batch_relax_sync_kernel<3, false, 4>, batch_relax_sync_kernel<4, false, 4>,
-          batch_relax_sync_kernel<2, true, 4>}}};
+          batch_relax_sync_kernel<2, true, 4>, batch_relax_sync_kernel<3, true, 4>}}};
     const Kern kern = table[shape->rx_sync][shape->grid_layout][shape->rx_regs];
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
