@@ -418,6 +418,14 @@ int spm_batch_df_loss_seed(int n_mol, const spm_batch_mol* mols, long long n_chu
                            float* dL_dFEs, double* loss_out, void* scratch, void* stream);
 long long spm_batch_loss_scratch_bytes(long long n_chunks, int n_mol);
 
+/* Loss weights of a fitting step from the previous step's adjoint status:
+ * weights[s] = w_base[s] if states s-1, s and s+1 (cyclic over the n_states
+ * array) all passed the adjoint gates (diag[.].w == 0), else 0 -- a failed
+ * state and the z-neighbours whose central-difference df sees it leave the
+ * loss.  diag (n_states,4) f32; w_base, weights (n_states) f64. */
+int spm_batch_failure_mask(long long n_states, const float* diag, const double* w_base, double* weights,
+                           void* stream);
+
 /* spm_adjoint_grid_state over the batch (same outputs per state). */
 int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_states,
                             const spm_batch_shape* shape, const float* grid, const float* points,

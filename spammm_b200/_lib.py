@@ -156,6 +156,7 @@ _SIGNATURES = {
     "spm_batch_df_amp": (_i, [_i, _vp, _ll, _vp, _d, _d, _vp, _vp]),
     "spm_batch_df_loss_seed": (_i, [_i, _vp, _ll, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _vp]),
     "spm_batch_loss_scratch_bytes": (_ll, [_ll, _i]),
+    "spm_batch_failure_mask": (_i, [_ll, _vp, _vp, _vp, _vp]),
     "spm_batch_adjoint_state": (_i, [_i, _vp, _ll, _BS, _vp, _vp, _P, _vp, _vp, _vp, _vp, _vp, _vp]),
     "spm_batch_adjoint_params": (_i, [_i, _i, _vp, _LLP, _BS, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                       _vp]),

@@ -359,9 +359,10 @@ class AFMBatch:
         self._mask_failed = True
 
     def _update_mask(self):
-        ok = self.diag[:, 3] == 0
-        ok = ok & torch.roll(ok, 1) & torch.roll(ok, -1)  # rolls cross strokes only at weight-0 ends
-        torch.mul(self.w_base, ok, out=self.weights)
+        # neighbours are taken cyclically over the whole state array: they cross strokes only at
+        # the strokes' first and last z-steps, whose base weight is 0
+        check(lib().spm_batch_failure_mask(self.total_states, ptr(self.diag), ptr(self.w_base), ptr(self.weights),
+                                           stream_ptr()), "spm_batch_failure_mask")
 
     # ------------------------------------------------------------ data in/out
     def _rows(self, i, what):

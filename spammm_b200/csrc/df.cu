@@ -673,6 +673,36 @@ extern "C" long long spm_batch_loss_scratch_bytes(long long n_chunks, int n_mol)
     return (2 * n_chunks + 2 * (long long)n_mol) * (long long)sizeof(double);
 }
 
+namespace spm {
+namespace {
+// weights[s] = w_base[s] * (status[s-1] == 0 && status[s] == 0 && status[s+1] == 0), neighbours
+// taken cyclically over the whole state array, status = diag[.].w.
+__global__ void __launch_bounds__(256)
+failure_mask_kernel(long long n, const float4* __restrict__ diag, const double* __restrict__ w_base,
+                    double* __restrict__ weights) {
+    const long long s = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (s >= n) return;
+    const long long sm = s > 0 ? s - 1 : n - 1, sp = s + 1 < n ? s + 1 : 0;
+    const bool ok = diag[s].w == 0.f && diag[sm].w == 0.f && diag[sp].w == 0.f;
+    weights[s] = w_base[s] * (ok ? 1.0 : 0.0);
+}
+}  // namespace
+}  // namespace spm
+
+extern "C" int spm_batch_failure_mask(long long n_states, const float* diag, const double* w_base, double* weights,
+                                      void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(n_states >= 0, "spm_batch_failure_mask: n_states=%lld", n_states);
+    if (n_states == 0) return SPM_OK;
+    SPM_REQUIRE(diag && w_base && weights && aligned16(diag), "spm_batch_failure_mask: null or misaligned buffers");
+    const long long nb = (n_states + 255) / 256;
+    SPM_REQUIRE(nb < (1LL << 31), "spm_batch_failure_mask: too many states");
+    failure_mask_kernel<<<(unsigned)nb, 256, 0, as_stream(stream)>>>(n_states, reinterpret_cast<const float4*>(diag),
+                                                                     w_base, weights);
+    return check_launch("spm_batch_failure_mask");
+}
+
 extern "C" int spm_batch_df_loss_seed(int n_mol, const spm_batch_mol* mols, long long n_chunks, const float* FEs,
                                       const double* target, const double* weights, double dtip, double* df_out,
                                       float* dL_dFEs, double* loss_out, void* scratch, void* stream) {

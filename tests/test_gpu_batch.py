@@ -142,6 +142,22 @@ def test_batch_graph_replay(cuda):
         assert torch.equal(e, t)
 
 
+def test_failure_mask_kernel(cuda):
+    """spm_batch_failure_mask = w_base * (status of s-1, s, s+1 all 0), cyclic."""
+    n = 100003
+    g = torch.Generator(device="cuda").manual_seed(3)
+    diag = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    diag[:, 3] = (torch.rand(n, device="cuda", generator=g) < 0.05).float() * 3.0
+    diag[0, 3] = 1.0  # a failure at the array's start masks the last state too
+    w_base = torch.rand(n, dtype=torch.float64, device="cuda", generator=g)
+    out = torch.empty_like(w_base)
+    _lib.check(_lib.lib().spm_batch_failure_mask(n, _lib.ptr(diag), _lib.ptr(w_base), _lib.ptr(out),
+                                                 _lib.stream_ptr()), "spm_batch_failure_mask")
+    ok = diag[:, 3] == 0
+    ok = ok & torch.roll(ok, 1) & torch.roll(ok, -1)
+    assert torch.equal(out, w_base * ok) and out[-1] == 0.0
+
+
 @pytest.mark.parametrize("sync", [0, 1])
 def test_batch_unrastered_molecule(cuda, sync):
     """A molecule whose points are no full raster (raster_ny = 0) is relaxed in
