@@ -777,10 +777,20 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
         const int ya = (int)(r0 - (unsigned)za * ny), yb = (int)(r1 - (unsigned)za * ny);
         return !(yb < ylo || ya > yhi);
     };
-    for (int a0 = 0; a0 < na; a0 += NM_THREADS) {
-        const bool last_group = a0 + NM_THREADS >= na;
-        const int nag = na - a0 < NM_THREADS ? na - a0 : NM_THREADS;
+    for (int a0 = 0, nag = 0; a0 < na; a0 += nag) {
+        // atom group: nag atoms x P phases <= 256 threads.  The remaining atoms go in one group when
+        // that keeps >= 85% of the threads busy, else a group of 256/P atoms with P = ceil(256/rem)
+        // and the rest after it (65 atoms: 64 at 4 phases + 1 at 256 instead of 65 at 3)
+        const int rem = na - a0;
+        if (rem >= NM_THREADS) {
+            nag = NM_THREADS;
+        } else if ((NM_THREADS / rem) * rem * 100 >= 85 * NM_THREADS) {
+            nag = rem;
+        } else {
+            nag = NM_THREADS / ((NM_THREADS + rem - 1) / rem);
+        }
         const int P = NM_THREADS / nag;
+        const bool last_group = a0 + nag >= na;
         const bool act = t < nag * P;
         const int a = a0 + (act ? t % nag : 0), ph = act ? t / nag : 0;
         const int ga = D->atom_off + a;
