@@ -551,7 +551,7 @@ batch_loss_partials_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, co
     double w = 0.0, l = 0.0;
     if (ls < nst) {
         const long long gid = D->state_off + ls;
-        const int iz = (int)(ls % nz);
+        const int iz = ls < (1LL << 32) ? (int)((unsigned)ls % (unsigned)nz) : (int)(ls % nz);  // 32-bit when it fits
         double d = 0.0;
         if (iz > 0 && iz < nz - 1) {
             const double fp = load_row(FEs, gid + 1).z, fm = load_row(FEs, gid - 1).z;
@@ -565,16 +565,26 @@ batch_loss_partials_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, co
     s_w[threadIdx.x] = w;
     s_l[threadIdx.x] = l;
     __syncthreads();
-    for (int s = LS_THREADS / 2; s > 0; s >>= 1) {
+    // the single-volume tree (v[t] += v[t+s], s = 128 .. 1): levels >= 32 through shared
+    // memory, the last five in warp 0 by shuffles -- the same additions in the same order
+    for (int s = LS_THREADS / 2; s >= 32; s >>= 1) {
         if (threadIdx.x < s) {
             s_w[threadIdx.x] += s_w[threadIdx.x + s];
             s_l[threadIdx.x] += s_l[threadIdx.x + s];
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        partial[2 * ch] = s_w[0];
-        partial[2 * ch + 1] = s_l[0];
+    if (threadIdx.x < 32) {
+        double vw = s_w[threadIdx.x], vl = s_l[threadIdx.x];
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            vw += __shfl_down_sync(0xffffffffu, vw, s);
+            vl += __shfl_down_sync(0xffffffffu, vl, s);
+        }
+        if (threadIdx.x == 0) {
+            partial[2 * ch] = vw;
+            partial[2 * ch + 1] = vl;
+        }
     }
 }
 
@@ -623,8 +633,8 @@ batch_loss_grad_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const 
     const long long nst = (long long)D->n_scan * nz;
     const long long ls = (ch - D->chunk_off) * LS_THREADS + threadIdx.x;
     if (ls >= nst) return;
-    const long long base = D->state_off, gid = base + ls;
-    const int iz = (int)(ls % nz);
+    const long long gid = D->state_off + ls;
+    const int iz = ls < (1LL << 32) ? (int)((unsigned)ls % (unsigned)nz) : (int)(ls % nz);  // 32-bit when it fits
     if (nz < 3) {  // no central difference: no gradient (and the stencil would leave the stroke)
         dL[gid] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
@@ -634,15 +644,14 @@ batch_loss_grad_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const 
         dL[gid] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
-    auto g = [&](long long j) {
-        const int jz = (int)((j - base) % nz);
+    auto g = [&](long long j, int jz) {  // jz: the z-step of state j
         const double w = wts ? wts[j] : ((jz > 0 && jz < nz - 1) ? 1.0 : 0.0);
         return w * (df[j] - tgt[j]) / wsum;
     };
     double v;
-    if (iz == 0) v = g(gid + 1) * coeff;
-    else if (iz == nz - 1) v = -g(gid - 1) * coeff;
-    else v = (g(gid + 1) - g(gid - 1)) * coeff;
+    if (iz == 0) v = g(gid + 1, 1) * coeff;
+    else if (iz == nz - 1) v = -g(gid - 1, iz - 1) * coeff;
+    else v = (g(gid + 1, iz + 1) - g(gid - 1, iz - 1)) * coeff;
     dL[gid] = make_float4(0.f, 0.f, (float)v, 0.f);
 }
 
