@@ -422,7 +422,14 @@ batch_adjoint_state_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, lo
     const spm_batch_mol* D = mols + SPM_MOL_BY(state_off, mols, n_mol, st);
     const long long ls = st - D->state_off;
     const int nz = D->nz_steps;
-    const int iscan = (int)(ls / nz), iz = (int)(ls % nz);
+    int iscan, iz;
+    if (ls < (1LL << 32)) {  // 32-bit division when it fits
+        iscan = (int)((unsigned)ls / (unsigned)nz);
+        iz = (int)((unsigned)ls - (unsigned)iscan * (unsigned)nz);
+    } else {
+        iscan = (int)(ls / nz);
+        iz = (int)(ls % nz);
+    }
     state_adjoint<true>(slab_view(*D, grid, stride), P, pts[D->pix_off + iscan], iz, PPs[st], dL[st], ubar + st, dk + st,
                         diag + st);
 }
@@ -540,7 +547,9 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
         const float4 pp = __ldg(PPs + st);
         C = corners_of<true>(G, mk3(pp.x, pp.y, pp.z));
         valid = C.ok;
-        stroke = D->pix_off + (st - D->state_off) / D->nz_steps;
+        const long long ls = st - D->state_off;
+        stroke = D->pix_off + (ls < (1LL << 32) ? (long long)((unsigned)ls / (unsigned)D->nz_steps)
+                                                : ls / D->nz_steps);
         nx = G.nx; ny = G.ny; z_lo = G.z_lo;
         base = gq + (size_t)D->grid_off * 4;
         scale = pow2(42 - scale_exp(__ldg(umax + m)));
