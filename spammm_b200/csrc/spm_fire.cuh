@@ -168,7 +168,7 @@ __device__ __forceinline__ float4 interp_fe(const GridView& G, V3 p) {
 // Axis-aligned grids: dinvA = (ax,0,0,aw), dinvB = (0,by,0,bw), dinvC =
 // (0,0,cz,cw).  The zero terms of interp_fe's coordinate FMAs are exact, so
 // u = fma(p.x, ax, aw) is interp_fe's u for every finite p (up to the sign of
-// an exact zero), and interp_fe_axis returns interp_fe's sample.
+// an exact zero), and the samplers on an AxisView return interp_fe's sample.
 struct AxisView {
     const float4* __restrict__ g;
     int nx, ny, nz, z_lo, nz_slab;
@@ -179,49 +179,6 @@ struct AxisView {
 // lerp_c on two packed channel pairs: fma(a, f1, ma*f0) per lane.
 __device__ __forceinline__ ulonglong2 lerp_pk(f2 a, f2 ma, ulonglong2 f0, ulonglong2 f1) {
     return make_ulonglong2(fma2(a, f1.x, mul2(ma, f0.x)), fma2(a, f1.y, mul2(ma, f0.y)));
-}
-
-// interp_fe on an AxisView: the same texel addressing and the same per-channel
-// operations, with the channel pairs (x,y) and (z,w) of a texel lerped by one
-// packed f32x2 instruction each.
-template <typename IDX, bool SLAB>
-__device__ __forceinline__ float4 interp_fe_axis(const AxisView& G, V3 p) {
-    const float u = __fmaf_rn(p.x, G.ax, G.aw);
-    const float v = __fmaf_rn(p.y, G.by, G.bw);
-    const float w = __fmaf_rn(p.z, G.cz, G.cw);
-    int x0, x1, y0, y1, z0, z1;
-    float ax, ay, az;
-    bool ok = tex_axis(u, G.nx, G.fnx, x0, x1, ax);
-    ok = tex_axis(v, G.ny, G.fny, y0, y1, ay) && ok;
-    ok = tex_axis(w, G.nz, G.fnz, z0, z1, az) && ok;
-    if (SLAB) {
-        z0 -= G.z_lo;
-        z1 -= G.z_lo;
-        ok = ok && (unsigned)z0 < (unsigned)G.nz_slab && (unsigned)z1 < (unsigned)G.nz_slab;
-    }
-    if (!ok) {
-        float nan = __int_as_float(0x7fc00000);
-        return make_float4(nan, nan, nan, nan);
-    }
-    const f2 AX = bc(ax), MX = bc(1.f - ax), AY = bc(ay), MY = bc(1.f - ay), AZ = bc(az), MZ = bc(1.f - az);
-    const IDX r00 = ((IDX)z0 * G.ny + y0) * G.nx, r10 = ((IDX)z0 * G.ny + y1) * G.nx;
-    const IDX r01 = ((IDX)z1 * G.ny + y0) * G.nx, r11 = ((IDX)z1 * G.ny + y1) * G.nx;
-    const ulonglong2* g = reinterpret_cast<const ulonglong2*>(G.g);
-    const ulonglong2 f000 = __ldg(g + r00 + x0), f100 = __ldg(g + r00 + x1);
-    const ulonglong2 f010 = __ldg(g + r10 + x0), f110 = __ldg(g + r10 + x1);
-    const ulonglong2 f001 = __ldg(g + r01 + x0), f101 = __ldg(g + r01 + x1);
-    const ulonglong2 f011 = __ldg(g + r11 + x0), f111 = __ldg(g + r11 + x1);
-    const ulonglong2 c00 = lerp_pk(AX, MX, f000, f100);
-    const ulonglong2 c10 = lerp_pk(AX, MX, f010, f110);
-    const ulonglong2 c01 = lerp_pk(AX, MX, f001, f101);
-    const ulonglong2 c11 = lerp_pk(AX, MX, f011, f111);
-    const ulonglong2 c0 = lerp_pk(AY, MY, c00, c10);
-    const ulonglong2 c1 = lerp_pk(AY, MY, c01, c11);
-    const ulonglong2 c = lerp_pk(AZ, MZ, c0, c1);
-    float4 r;
-    upk(c.x, r.x, r.y);
-    upk(c.y, r.z, r.w);
-    return r;
 }
 
 // 256-bit read-only load of an x-pair: (value(x), value(x+1)) as packed
@@ -257,10 +214,12 @@ __device__ __forceinline__ void load_cell(const AxisView& G, int x0, int y0, int
     }
 }
 
-// interp_fe_axis on an x-paired (LAYOUT 2) or xz-quad (LAYOUT 4) slab: the
-// same texel addressing and the same lerps on the same values, so the same
-// sample.  (In a slab the cell's upper layer is z0+1, or layer 0 when a
-// full-grid slab wraps; both layouts store exactly that layer.)
+// interp_fe on an AxisView over an x-paired (LAYOUT 2) or xz-quad (LAYOUT 4)
+// slab: the same texel addressing and the same lerps on the same values, so
+// the same sample, with the channel pairs (x,y) and (z,w) of a texel lerped
+// by one packed f32x2 instruction each.  (In a slab the cell's upper layer is
+// z0+1, or layer 0 when a full-grid slab wraps; both layouts store exactly
+// that layer.)
 template <typename IDX, bool SLAB, int LAYOUT>
 __device__ __forceinline__ float4 interp_fe_cell(const AxisView& G, V3 p) {
     const float u = __fmaf_rn(p.x, G.ax, G.aw);
