@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define SPM_ABI_VERSION 1
+#define SPM_ABI_VERSION 2
 
 enum spm_status {
     SPM_OK = 0,
@@ -450,11 +450,16 @@ int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_st
  * spm_batch_adjoint_scratch_bytes(totals, n_mol).  The scratch keeps the
  * cleared adjoint grid between calls, with a marker that says it is clear:
  * reuse one scratch buffer call after call; any other content (a fresh
- * allocation, a call that failed half-way) is cleared by the next call. */
+ * allocation, a call that failed half-way) is cleared by the next call.
+ * adj_flags: SPM_ADJ_PAIR_PARAMS computes grad columns 3-4 (the pair
+ * parameters); without it they are written as 0 and the node kernel skips
+ * their terms (fits of positions and charges only). */
+#define SPM_ADJ_PAIR_PARAMS 1
 int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol* mols, const long long* totals,
                              const spm_batch_shape* shape, const float* atoms, const float* params,
                              const float* Qs, const float* QZs, const float* PPs, const float* ubar,
-                             const float* dk, double* grad, double* dk_sum, void* scratch, void* stream);
+                             const float* dk, double* grad, double* dk_sum, int adj_flags, void* scratch,
+                             void* stream);
 long long spm_batch_adjoint_scratch_bytes(const long long* totals, int n_mol);
 
 /* ------------------------------------------------------------------------

@@ -31,6 +31,7 @@ SPM_RELAX_PP = 2
 SPM_RELAX_2D = 3
 SPM_FLAG_FLIP_Z = 2
 SPM_FLAG_PAIRED = 4
+SPM_ADJ_PAIR_PARAMS = 1
 
 _f4 = ctypes.c_float * 4
 
@@ -158,8 +159,8 @@ _SIGNATURES = {
     "spm_batch_loss_scratch_bytes": (_ll, [_ll, _i]),
     "spm_batch_failure_mask": (_i, [_ll, _vp, _vp, _vp, _vp]),
     "spm_batch_adjoint_state": (_i, [_i, _vp, _ll, _BS, _vp, _vp, _P, _vp, _vp, _vp, _vp, _vp, _vp]),
-    "spm_batch_adjoint_params": (_i, [_i, _i, _vp, _LLP, _BS, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                      _vp]),
+    "spm_batch_adjoint_params": (_i, [_i, _i, _vp, _LLP, _BS, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
+                                      _vp, _vp]),
     "spm_batch_adjoint_scratch_bytes": (_ll, [_LLP, _i]),
 }
 

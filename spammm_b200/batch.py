@@ -215,6 +215,8 @@ class AFMBatch:
         # loss / adjoint buffers: allocated by the first loss or adjoint call
         self.target = self.weights = self.df_c = self.dL = self.ubar = self.dk = self.diag = None
         self.grad = self.dk_sum = None
+        # grad columns 3-4 (pair parameters): computed unless a caller that never reads them turns them off
+        self.pair_param_grads = True
         self.loss = torch.empty((self.n,), dtype=F64, device=dev)
         self._Qs = hostvec(self.probe.tipQs)
         self._QZs = hostvec(self.probe.tipQZs)
@@ -311,8 +313,9 @@ class AFMBatch:
         rc = lib().spm_batch_adjoint_params(self.kind, self.n, ptr(self.mols_d), self.plan.totals,
                                             ctypes.byref(self.shape), ptr(self.atoms), ptr(self.params),
                                             hptr(self._Qs), hptr(self._QZs), ptr(self.PPs), ptr(self.ubar),
-                                            ptr(self.dk), ptr(self.grad), ptr(self.dk_sum), ptr(self.adj_scratch),
-                                            stream_ptr())
+                                            ptr(self.dk), ptr(self.grad), ptr(self.dk_sum),
+                                            _lib.SPM_ADJ_PAIR_PARAMS if self.pair_param_grads else 0,
+                                            ptr(self.adj_scratch), stream_ptr())
         check(rc, "spm_batch_adjoint_params")
 
     def forward(self, amp=None):
@@ -450,10 +453,12 @@ class BatchAdam:
     written with in-place torch ops on fixed buffers so one fitting step --
     forward, df loss, adjoint, update -- captures into one CUDA graph.
     Summing the per-molecule losses makes each molecule's update depend on its
-    own loss only."""
+    own loss only.  The update reads gradient columns 0-2 and 5 only, so the
+    batch's adjoint skips the pair-parameter columns."""
 
     def __init__(self, batch, lr=0.01, betas=(0.9, 0.999), eps=1e-8, cols=(0, 1, 2, 3)):
         self.b = batch
+        batch.pair_param_grads = False
         self.lr, self.b1, self.b2, self.eps = float(lr), float(betas[0]), float(betas[1]), float(eps)
         self.cols = list(cols)
         dev = batch.dev

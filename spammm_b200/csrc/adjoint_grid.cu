@@ -653,19 +653,22 @@ struct AtomC {
     f2 x, y, z;      // position
     f2 c0, c1, c2, c3;  // LJ: 12 c12, -6 c6, 168 c12, -48 c6; Morse: K log2e, -K R0 log2e, -2 K E0, 2 K^2 E0
     f2 c4;           // Morse: -2 K
-    f2 qw;           // Q * qon (on-node tip charges)
+    f2 qw, qw3;      // Q * qon and 3 Q * qon (on-node tip charges)
     float q;         // Q
 };
 
 // Derivatives of the pair laws of the grid build (LJ / Morse + point-charge
 // Coulomb, R2SAFE-softened, as pair_grad) at two nodes per call, contracted
 // with the nodes' adjoint vectors g = (gx,gy,gz,gw):
-//   acc[0..2] += dF/d(atom position)^T g   acc[3], acc[4] += dF/d(pair params)^T g
+//   acc[0..2] += dF/d(atom position)^T g   acc[3], acc[4] += dF/d(pair params)^T g (PAR)
 //   acc[5]    += dF/d(atom charge)^T g
 // with Blackwell's packed FP32 (two nodes per instruction), one MUFU rsqrt per
 // node for the pair law and the on-node charges together, MUFU ex2 for Morse.
-// LJ's acc[3] is accumulated negated (the sign is applied when it is folded).
-template <int KIND, bool ON>
+// The radial factors s = -E'(r)/r and sp2 = -2 s'(r)/r of the pair law and of
+// the on-node charges (Q qon / r) are summed before the powers of 1/r they
+// share are applied.  LJ's acc[3] is accumulated negated (the sign is applied
+// when it is folded).
+template <int KIND, bool ON, bool PAR>
 __device__ __forceinline__ void pair_adj2(f2 nx, f2 ny, f2 nz, f2 gx, f2 gy, f2 gz, f2 gw, const AtomC& C,
                                           const NodeSites& S, f2* acc) {
     const f2 dx = sub2(nx, C.x), dy = sub2(ny, C.y), dz = sub2(nz, C.z);
@@ -673,32 +676,47 @@ __device__ __forceinline__ void pair_adj2(f2 nx, f2 ny, f2 nz, f2 gx, f2 gy, f2 
     const f2 rs = rsqrt2(r2);
     const f2 ir2 = mul2(rs, rs);
     const f2 du = fma2(dx, gx, fma2(dy, gy, mul2(dz, gz)));
-    f2 s, sp2;  // sp2 = -2 s'(r)/r: the Hessian's radial term with the -2 of A folded in
+    f2 s, sp2;
     if (KIND == SPM_KIND_LJ) {
-        const f2 ir6 = mul2(mul2(ir2, ir2), ir2);
-        const f2 ir8 = mul2(ir6, ir2);
-        const f2 ir14 = mul2(ir8, ir6);
-        s = fma2(C.c0, ir14, mul2(C.c1, ir8));                // 12 c12 ir14 - 6 c6 ir8
-        sp2 = mul2(fma2(C.c2, ir14, mul2(C.c3, ir8)), ir2);   // (168 c12 ir14 - 48 c6 ir8) ir2
-        acc[3] = fma2(gw, ir6, fma2(du, mul2(bc(6.f), ir8), acc[3]));      // -(d/dc6)
-        acc[4] = fma2(gw, mul2(ir6, ir6), fma2(du, mul2(bc(12.f), ir14), acc[4]));
+        const f2 ir4 = mul2(ir2, ir2);
+        const f2 ir6 = mul2(ir4, ir2);
+        const f2 a1 = fma2(C.c0, ir6, C.c1);  // 12 c12 ir6 - 6 c6:   s = a1 ir8
+        const f2 a2 = fma2(C.c2, ir6, C.c3);  // 168 c12 ir6 - 48 c6: sp2 = a2 ir10
+        if (ON) {
+            s = mul2(fma2(a1, ir6, mul2(C.qw, rs)), ir2);     // + Q qon / r^3
+            sp2 = mul2(fma2(a2, ir6, mul2(C.qw3, rs)), ir4);  // + 3 Q qon / r^5
+        } else {
+            s = mul2(mul2(a1, ir6), ir2);
+            sp2 = mul2(mul2(a2, ir6), ir4);
+        }
+        if (PAR) {
+            const f2 h6 = mul2(bc(6.f), ir2);
+            const f2 t6 = fma2(du, h6, gw);                // gw + 6 du / r^2
+            const f2 t12 = fma2(du, h6, t6);               // gw + 12 du / r^2
+            acc[3] = fma2(t6, ir6, acc[3]);                // -(d/dc6):  gw ir6 + 6 du ir8
+            acc[4] = fma2(t12, mul2(ir6, ir6), acc[4]);    //   d/dc12:  gw ir12 + 12 du ir14
+        }
     } else {
         const f2 r = mul2(r2, rs);
         const f2 e = ex2_2(fma2(C.c0, r, C.c1));              // exp(K (r - R0))
         const f2 em1 = sub2(e, bc(1.f));
         const f2 nEp = mul2(mul2(C.c2, e), em1);              // -E'
         const f2 Epp = mul2(mul2(C.c3, e), fma2(bc(2.f), e, bc(-1.f)));
-        s = mul2(nEp, rs);
-        sp2 = mul2(fma2(Epp, rs, mul2(nEp, ir2)), rs);
-        acc[3] = fma2(gw, nEp, fma2(mul2(du, Epp), rs, acc[3]));
-        acc[4] = fma2(mul2(gw, e), sub2(e, bc(2.f)), fma2(mul2(du, mul2(mul2(C.c4, e), em1)), rs, acc[4]));
+        if (ON) {
+            s = mul2(fma2(C.qw, ir2, nEp), rs);                                   // + Q qon / r^3
+            sp2 = mul2(fma2(Epp, rs, mul2(fma2(C.qw3, ir2, nEp), ir2)), rs);     // + 3 Q qon / r^5
+        } else {
+            s = mul2(nEp, rs);
+            sp2 = mul2(fma2(Epp, rs, mul2(nEp, ir2)), rs);
+        }
+        if (PAR) {
+            acc[3] = fma2(gw, nEp, fma2(mul2(du, Epp), rs, acc[3]));
+            acc[4] = fma2(mul2(gw, e), sub2(e, bc(2.f)), fma2(mul2(du, mul2(mul2(C.c4, e), em1)), rs, acc[4]));
+        }
     }
     if (ON) {
         const f2 qr = mul2(bc(S.qon), rs);
-        const f2 sk = mul2(mul2(C.qw, rs), ir2);
-        s = add2(s, sk);
-        sp2 = fma2(mul2(bc(3.f), sk), ir2, sp2);
-        acc[5] = fma2(gw, qr, fma2(du, mul2(qr, ir2), acc[5]));
+        acc[5] = fma2(qr, fma2(du, ir2, gw), acc[5]);  // qon / r (gw + du / r^2)
     }
     const f2 A = fma2(gw, s, mul2(sp2, du));
     const f2 ns = mul2(s, bc(-1.f));
@@ -746,8 +764,8 @@ constexpr size_t NM_SMEM = 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(
 // Three CTAs per SM (80 registers, a few bytes spilled, 3 x 70 KB of shared
 // memory): the loop is bound by its dependency chains, so the third CTA's
 // warps pay (12.2 -> 10.7 ms on the 64-molecule fit against two CTAs at 128
-// registers).
-template <int KIND, bool ON>
+// registers).  PAR: also the pair-parameter columns 3-4 (else written as 0).
+template <int KIND, bool ON, bool PAR>
 __global__ void __launch_bounds__(NM_THREADS, 3)
 batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk,
                            const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
@@ -812,6 +830,7 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
         C.z = bc(at.z);
         C.q = at.w;
         C.qw = bc(at.w * S.qon);
+        C.qw3 = bc(3.f * (at.w * S.qon));
         if (KIND == SPM_KIND_LJ) {  // p1 = c6, p2 = c12
             C.c0 = bc(12.f * p2);
             C.c1 = bc(-6.f * p1);
@@ -842,11 +861,12 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
                 const int Lp = (L + 1) >> 1;
                 for (int jp = ph; jp < Lp; jp += P) {
                     const int j = 2 * jp;
-                    pair_adj2<KIND, ON>(lds2(&s_n[0][j]), lds2(&s_n[1][j]), lds2(&s_n[2][j]), lds2(&s_n[3][j]),
+                    pair_adj2<KIND, ON, PAR>(lds2(&s_n[0][j]), lds2(&s_n[1][j]), lds2(&s_n[2][j]), lds2(&s_n[3][j]),
                                         lds2(&s_n[4][j]), lds2(&s_n[5][j]), lds2(&s_n[6][j]), C, S, a32);
                     if (++n32 == NM_FLUSH / 2) {
 #pragma unroll
                         for (int c = 0; c < 6; c++) {
+                            if (!PAR && (c == 3 || c == 4)) continue;
                             float lo, hi;
                             upk(a32[c], lo, hi);
                             acc[c] += (double)lo + (double)hi;
@@ -857,6 +877,7 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
                 }
 #pragma unroll
                 for (int c = 0; c < 6; c++) {
+                    if (!PAR && (c == 3 || c == 4)) continue;
                     float lo, hi;
                     upk(a32[c], lo, hi);
                     acc[c] += (double)lo + (double)hi;
@@ -933,7 +954,7 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
         }
 #pragma unroll
         for (int c = 0; c < 6; c++) red[c][t] = act ? acc[c] : 0.0;
-        if (KIND == SPM_KIND_LJ) red[3][t] = -red[3][t];  // accumulated negated
+        if (KIND == SPM_KIND_LJ && PAR) red[3][t] = -red[3][t];  // accumulated negated
         __syncthreads();
         if (t < nag) {
             double* out = partial + ((size_t)D->row_off + (size_t)lc * na + a0 + t) * 6;
@@ -1029,10 +1050,12 @@ extern "C" long long spm_batch_adjoint_scratch_bytes(const long long* totals, in
 extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol* mols, const long long* totals,
                                         const spm_batch_shape* shape, const float* atoms, const float* params,
                                         const float* Qs, const float* QZs, const float* PPs, const float* ubar,
-                                        const float* dk, double* grad, double* dk_sum, void* scratch, void* stream) {
+                                        const float* dk, double* grad, double* dk_sum, int adj_flags, void* scratch,
+                                        void* stream) {
     using namespace spm;
     clear_error();
     SPM_REQUIRE(kind == SPM_KIND_LJ || kind == SPM_KIND_MORSE, "spm_batch_adjoint_params: kind=%d", kind);
+    SPM_REQUIRE((adj_flags & ~SPM_ADJ_PAIR_PARAMS) == 0, "spm_batch_adjoint_params: unknown flags 0x%x", adj_flags);
     SPM_REQUIRE(shape && totals && Qs && QZs && dk_sum && scratch, "spm_batch_adjoint_params: null pointer");
     SPM_REQUIRE(n_mol >= 0, "spm_batch_adjoint_params: n_mol=%d", n_mol);
     const long long n_units = totals[2], n_chunks = totals[3], n_states = totals[4], n_atoms = totals[5];
@@ -1064,9 +1087,14 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             if (cudaGetDevice(&dev) != cudaSuccess)
                 return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: no current device");
             if (dev < 0 || dev >= 64 || !smem_set[dev]) {
-                for (auto k : {batch_adjoint_nodes_kernel<SPM_KIND_LJ, true>, batch_adjoint_nodes_kernel<SPM_KIND_LJ, false>,
-                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true>,
-                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false>})
+                for (auto k : {batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, true>,
+                               batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, true>,
+                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, true>,
+                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, true>,
+                               batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, false>,
+                               batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, false>,
+                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, false>,
+                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, false>})
                     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)NM_SMEM) != cudaSuccess)
                         return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: cannot set shared memory size");
                 if (dev >= 0 && dev < 64) smem_set[dev] = true;
@@ -1083,10 +1111,16 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             const NodeSites S = make_node_sites(Qs, QZs);
             const int pstride = kind == SPM_KIND_MORSE ? 4 : 2;
             const bool on = S.qon != 0.f;
-            auto kern = kind == SPM_KIND_LJ ? (on ? batch_adjoint_nodes_kernel<SPM_KIND_LJ, true>
-                                                  : batch_adjoint_nodes_kernel<SPM_KIND_LJ, false>)
-                                            : (on ? batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true>
-                                                  : batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false>);
+            using NodeKern = decltype(&batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, true>);
+            // [pair-parameter columns][kind][on-node charges]
+            static const NodeKern table[2][2][2] = {
+                {{batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, false>, batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, false>},
+                 {batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, false>,
+                  batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, false>}},
+                {{batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, true>, batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, true>},
+                 {batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, true>,
+                  batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, true>}}};
+            const NodeKern kern = table[(adj_flags & SPM_ADJ_PAIR_PARAMS) ? 1 : 0][kind == SPM_KIND_MORSE ? 1 : 0][on ? 1 : 0];
             kern<<<(unsigned)n_units, NM_THREADS, NM_SMEM, st>>>(n_mol, mols, chunk,
                                                                  reinterpret_cast<const float4*>(atoms), params, pstride,
                                                                  S, gq, box, umax, part);

@@ -107,7 +107,7 @@ __device__ __forceinline__ void build_tile(int na, const float4* __restrict__ at
     f2 fx[ZP], fy[ZP], fz[ZP], fe[ZP];
 #pragma unroll
     for (int p = 0; p < ZP; p++) { fx[p] = zero; fy[p] = zero; fz[p] = zero; fe[p] = zero; }
-    const f2 two = bc(2.f), one = bc(1.f);
+    const f2 one = bc(1.f);
 
     for (int t0 = 0; t0 < na; t0 += GB_TILE) {
         const int nt = min(GB_TILE, na - t0);
@@ -142,28 +142,34 @@ __device__ __forceinline__ void build_tile(int na, const float4* __restrict__ at
                     const f2 dz = sub2(pz[p], az);
                     const f2 r2 = fma2(dz, dz, dxy2);
                     const f2 rs = rsqrt2(r2);
+                    // s = |F|/r of the pair law plus the on-node charges; the charges' Q/r^3 is
+                    // added before the last factor 1/r (Morse) or 1/r^2 (LJ) the two terms share
                     f2 s;
                     if (KIND == SPM_KIND_MORSE) {
-                        // E = E0 e (e-2), F = dp * (-2 K E0) e (e-1) / r, e = exp(K (r-R0))
+                        // E = E0 e (e-2) = E0 (w - e), F = dp * (-2 K E0) w / r, w = e (e-1), e = exp(K (r-R0))
                         const f2 r = mul2(r2, rs);
                         const f2 e = ex2_2(fma2(c0, r, c1));
-                        fe[p] = fma2(mul2(c2, e), sub2(e, two), fe[p]);
-                        s = mul2(mul2(mul2(c3, e), sub2(e, one)), rs);
+                        const f2 w = mul2(e, sub2(e, one));
+                        fe[p] = fma2(c2, sub2(w, e), fe[p]);
+                        const f2 m = mul2(c3, w);
                         if (ON) {
                             const f2 Ek = mul2(qon, rs);
                             fe[p] = add2(fe[p], Ek);
-                            s = fma2(Ek, mul2(rs, rs), s);
+                            s = mul2(fma2(Ek, rs, m), rs);
+                        } else {
+                            s = mul2(m, rs);
                         }
                     } else {
                         // E = (c12 ir6 - c6) ir6, F = dp * (12 c12 ir6 - 6 c6) ir6 ir2
                         const f2 ir2 = mul2(rs, rs);
                         const f2 ir6 = mul2(mul2(ir2, ir2), ir2);
                         fe[p] = fma2(fma2(c1, ir6, c0), ir6, fe[p]);
-                        s = mul2(mul2(fma2(c3, ir6, c2), ir6), ir2);
                         if (ON) {
                             const f2 Ek = mul2(qon, rs);
                             fe[p] = add2(fe[p], Ek);
-                            s = fma2(Ek, ir2, s);
+                            s = mul2(fma2(fma2(c3, ir6, c2), ir6, Ek), ir2);
+                        } else {
+                            s = mul2(mul2(fma2(c3, ir6, c2), ir6), ir2);
                         }
                     }
                     fx[p] = fma2(dx, s, fx[p]);

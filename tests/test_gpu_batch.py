@@ -1,6 +1,8 @@
 """Batched grid path on the GPU: every molecule of a batch against the
 per-molecule calls (bit-exact forward, loss and state adjoint; gradients to
 FP64 summation order), the CPU oracle, CUDA-graph replay and launch shapes."""
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -222,6 +224,31 @@ def test_adjoint_scratch_reuse_and_garbage(cuda, kind):
     b.adjoint_params()
     torch.cuda.synchronize()
     assert torch.equal(b.grad, g1)
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_adjoint_without_pair_parameter_columns(cuda, kind):
+    """Without SPM_ADJ_PAIR_PARAMS the node kernel drops the pair-parameter
+    terms: columns 3-4 are 0, the position and charge columns are the full
+    adjoint's bit for bit (their arithmetic is the same)."""
+    b = AFMBatch(_items(kind, n=4, seed=73 + kind), kind=kind)
+    _target(b)
+    b.forward_adjoint()
+    torch.cuda.synchronize()
+    full = b.grad.clone()
+    assert full[:, 3:5].abs().max() > 0
+    b.pair_param_grads = False
+    b.adjoint_params()
+    torch.cuda.synchronize()
+    assert torch.equal(b.grad[:, [0, 1, 2, 5]], full[:, [0, 1, 2, 5]])
+    assert not b.grad[:, 3:5].any()
+    with pytest.raises(ValueError):
+        _lib.check(_lib.lib().spm_batch_adjoint_params(b.kind, b.n, _lib.ptr(b.mols_d), b.plan.totals,
+                                                       ctypes.byref(b.shape), _lib.ptr(b.atoms), _lib.ptr(b.params),
+                                                       _lib.hptr(b._Qs), _lib.hptr(b._QZs), _lib.ptr(b.PPs),
+                                                       _lib.ptr(b.ubar), _lib.ptr(b.dk), _lib.ptr(b.grad),
+                                                       _lib.ptr(b.dk_sum), 2, _lib.ptr(b.adj_scratch),
+                                                       _lib.stream_ptr()), "spm_batch_adjoint_params")
 
 
 def test_batch_adam_reduces_loss(cuda):
