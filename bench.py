@@ -447,7 +447,8 @@ def run_batched(args, dev_index):
         from spammm_b200 import _lib
         shape, tune_rep = _lib.lib().spm_batch_default_shape(), None
     else:
-        shape, tune_rep = autotune.tuned_shape(items, max_molecules=args.fit_mols, reps=1)
+        # the fit (BatchAdam) reads the position and charge gradients only
+        shape, tune_rep = autotune.tuned_shape(items, max_molecules=args.fit_mols, reps=1, pair_param_grads=False)
     rng = np.random.default_rng(11)
     pert = []
     for it in items:

@@ -304,11 +304,14 @@ long long spm_adjoint_grid_scratch_bytes(int n_atoms, long long n_state);
  * the FP64 sums.  Scans are z-strokes: one probe frame and spring shared by
  * the batch (spm_scan_params), per-molecule grids, rasters and z-step counts.
  *
- * SLABS.  A molecule stores only layers [z_lo, z_lo + nz_slab) of its full
- * (nx,ny,nz) grid.  They are built and sampled in the full grid's coordinates,
- * so stored values and samples are bit-identical to the full grid's; a probe
- * that needs a layer outside the slab stops at once and its state reports
- * "not converged" (FEs NaN, PPs.w = -iterations).
+ * SLABS.  A molecule stores only the box of nodes [x_lo, x_lo + nx_slab) x
+ * [y_lo, y_lo + ny_slab) x [z_lo, z_lo + nz_slab) of its full (nx,ny,nz) grid
+ * (the nodes its probe can reach: the scan window and the tip's z-range, each
+ * widened by a margin).  Nodes are built and sampled in the full grid's
+ * coordinates, so stored values and samples are bit-identical to the full
+ * grid's; a probe that needs a node outside the box stops at once and its
+ * state reports "not converged" (FEs NaN, PPs.w = -iterations).  A box that
+ * spans an axis completely keeps that axis' periodic wrap.
  *
  * DESCRIPTORS.  One spm_batch_mol per molecule, in the order work is handed
  * out; every *_off field is non-decreasing in that order (kernels locate a
@@ -323,11 +326,14 @@ long long spm_adjoint_grid_scratch_bytes(int n_atoms, long long n_state);
  *   atoms  (total_atoms,4) x,y,z,Q;  params (total_atoms,2) LJ c6,c12 or
  *          (total_atoms,4) Morse R0,E0,K,-
  *   grid   slabs in one of two layouts (spm_batch_shape.grid_layout), node
- *          idx = ((z - z_lo)*ny + y)*nx + x of a molecule, zl = z - z_lo:
- *          0 x-pairs: grid[2*(grid_off + idx) + dx] = value((x+dx) mod nx, y, z),
- *            a trilinear cell row is one 32-byte load; 2*totals[7] float4;
- *          1 xz-quads: grid[4*(grid_off + idx) + 2*dz + dx] =
- *            value((x+dx) mod nx, y, z_lo + (zl+dz) mod nz_slab), a cell's
+ *          idx = (zl*ny_slab + yl)*nx_slab + xl of a molecule, (xl, yl, zl) =
+ *          (x - x_lo, y - y_lo, z - z_lo):
+ *          0 x-pairs: grid[2*(grid_off + idx) + dx] = value(x_lo + (xl+dx) mod
+ *            nx_slab, y, z), a trilinear cell row is one 32-byte load (the
+ *            wrapped second value of the last stored column is a real
+ *            neighbour only when nx_slab = nx); 2*totals[7] float4;
+ *          1 xz-quads: grid[4*(grid_off + idx) + 2*dz + dx] = value(x_lo +
+ *            (xl+dx) mod nx_slab, y, z_lo + (zl+dz) mod nz_slab), a cell's
  *            two (y) rows are two 64-byte chunks; 4*totals[7] float4
  *   points (total_pixels,4) tip start positions (raster ix-major when
  *          raster_ny > 0, as spm_relax_ex)
@@ -346,6 +352,8 @@ typedef struct spm_batch_mol {
     int z_lo, nz_slab;    /* stored layers */
     int nz_steps;         /* z-steps of every stroke */
     int raster_ny;        /* > 0: points form an (n_scan/raster_ny) x raster_ny raster */
+    int x_lo, nx_slab;    /* stored columns */
+    int y_lo, ny_slab;    /* stored rows */
     int reserved;
     float p0[4], dA[4], dB[4], dC[4];   /* node geometry (dA,dB,dC as spm_grid_build) */
     float dinvA[4], dinvB[4], dinvC[4]; /* sampling transform (as spm_scan_params) */
@@ -369,6 +377,8 @@ typedef struct spm_batch_shape {
     int rx_sync;        /* relaxation schedule: 0 = every lane draws its next pixel when its stroke ends,
                            1 = a warp draws a pixel tile and its lanes step down the z-steps together
                            (all lanes sample the same z-layer of neighbouring pixels) */
+    int adj_ilp;        /* adjoint node kernel: 1 = one node pair per step (3 CTAs per SM), 2 = two
+                           independent node pairs per step (2 CTAs per SM, more registers) */
 } spm_batch_shape;
 
 spm_batch_shape spm_batch_default_shape(void);

@@ -91,7 +91,9 @@ class BatchMol(ctypes.Structure):
         ("pix_off", ctypes.c_int), ("n_scan", ctypes.c_int),
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
         ("z_lo", ctypes.c_int), ("nz_slab", ctypes.c_int),
-        ("nz_steps", ctypes.c_int), ("raster_ny", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("nz_steps", ctypes.c_int), ("raster_ny", ctypes.c_int),
+        ("x_lo", ctypes.c_int), ("nx_slab", ctypes.c_int), ("y_lo", ctypes.c_int), ("ny_slab", ctypes.c_int),
+        ("reserved", ctypes.c_int),
         ("p0", _f4), ("dA", _f4), ("dB", _f4), ("dC", _f4),
         ("dinvA", _f4), ("dinvB", _f4), ("dinvC", _f4),
     ]
@@ -103,6 +105,7 @@ class BatchShape(ctypes.Structure):
         ("gb_ty", ctypes.c_int), ("gb_zb", ctypes.c_int), ("rx_threads", ctypes.c_int),
         ("rx_tile_h", ctypes.c_int), ("rx_ctas_per_sm", ctypes.c_int), ("adj_chunk", ctypes.c_int),
         ("rx_regs", ctypes.c_int), ("grid_layout", ctypes.c_int), ("rx_sync", ctypes.c_int),
+        ("adj_ilp", ctypes.c_int),
     ]
 
     def key(self):

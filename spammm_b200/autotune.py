@@ -9,7 +9,8 @@ Every batched stage reads only its own fields of ``spm_batch_shape``:
                at up to 128 or at 80 registers),
                grid_layout (x-pair or xz-quad slabs: the grid is rebuilt in the
                candidate's layout before the relaxation is timed)
-  adjoint      adj_chunk (slab nodes per node-major unit)
+  adjoint      adj_chunk (slab nodes per node-major unit), adj_ilp (node pairs
+               per step of the node kernel: 1 at 3 CTAs per SM, 2 at 2)
 
 so the stages are tuned one after another, each over its own candidates with
 the others held fixed, by timing the stage's launch with CUDA events on a
@@ -32,7 +33,7 @@ GRID_CANDIDATES = [dict(gb_ty=ty, gb_zb=zb) for ty in (2, 4, 8) for zb in (8, 16
 RELAX_CANDIDATES = [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=r, grid_layout=g) for g in (0, 1)
                     for h in (2, 4, 8, 16) for r in (0, 1, 2, 3)] + \
                    [dict(rx_sync=0, rx_threads=128, rx_tile_h=8, rx_regs=0, grid_layout=0)]
-ADJOINT_CANDIDATES = [dict(adj_chunk=c) for c in (4096, 16384, 65536)]
+ADJOINT_CANDIDATES = [dict(adj_chunk=c, adj_ilp=i) for c in (4096, 16384, 65536) for i in (1, 2)]
 
 _CACHE = {}
 
@@ -113,17 +114,20 @@ def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
 
 
 def tuned_shape(items, kind=0, probe=None, dtip=-0.1, max_molecules=24, reps=2, adjoint=True, cache_file=None,
-                log=None):
+                log=None, pair_param_grads=True):
     """Best BatchShape for a workload, tuned on a sub-batch of at most
-    max_molecules molecules (cached per device and workload signature)."""
+    max_molecules molecules (cached per device and workload signature).
+    pair_param_grads: whether the adjoint is timed with the pair-parameter
+    columns (False for fits that read positions and charges only)."""
     dev = torch.cuda.get_device_name()
-    key = json.dumps([dev, signature(items, kind), bool(adjoint)])
+    key = json.dumps([dev, signature(items, kind), bool(adjoint), bool(pair_param_grads)])
     if key not in _CACHE and cache_file and os.path.exists(cache_file):
         with open(cache_file) as f:
             _CACHE.update(json.load(f))
     if key in _CACHE:
         return _lib.BatchShape(*_CACHE[key]["shape"]), _CACHE[key]["report"]
     sub = AFMBatch(sub_batch(items, max_molecules), kind=kind, probe=probe, dtip=dtip)
+    sub.pair_param_grads = bool(pair_param_grads)
     shape, report = tune(sub, reps=reps, adjoint=adjoint, log=log)
     del sub
     torch.cuda.empty_cache()

@@ -17,9 +17,10 @@ include/spm_b200.h):
 
 Per molecule the results are those of the per-molecule calls (grid_build ->
 relax_pp -> adjoint on the same GridScanSpec): forward values bit for bit.
-Only the z-layers the probe can reach (the tip's z-range plus ``slab_margin``
-on both sides) are built and stored; a probe that leaves them is reported as
-not converged instead of sampling the missing layers.
+Only the nodes the probe can reach -- the scan window's columns and rows and
+the tip's z-range, each widened by ``slab_margin`` on both sides -- are built
+and stored; a probe that leaves them is reported as not converged instead of
+sampling the missing nodes.
 
 Molecules are laid out in descending order of relaxation work (longest
 first), so the persistent relaxation ends with small molecules filling in.
@@ -94,6 +95,26 @@ class ProbeSpec:
     f2conv: float = 1e-10
 
 
+def lateral_range(item, probe, margin, axis):
+    """Stored columns (axis 0) or rows (axis 1) [lo, lo + n) of the item's
+    grid: every node a trilinear sample can touch while the probe stays within
+    `margin` A of the scan window (the raster's tip positions + dpos0).  The
+    whole axis when that range reaches an edge (the periodic wrap then needs
+    both ends) or the scan is empty."""
+    n = int(item.ngrid[axis])
+    c = np.asarray(item.xs if axis == 0 else item.ys, np.float64)
+    if c.size == 0:
+        return 0, n
+    d0 = float(probe.dpos0[axis])
+    o, h = float(item.origin[axis]), float(item.step)
+    t_lo, t_hi = (float(c.min()) + d0 - margin - o) / h, (float(c.max()) + d0 + margin - o) / h
+    lo = int(math.floor(t_lo))
+    hi = int(math.floor(t_hi)) + 2
+    if lo < 0 or hi > n:
+        return 0, n
+    return lo, hi - lo
+
+
 def slab_range(item, probe, dtip, margin):
     """Stored layers [z_lo, z_lo + nz_slab) of the item's grid: every layer a
     trilinear sample can touch while the probe stays within `margin` A of the
@@ -146,12 +167,15 @@ class BatchPlan:
             dinv = spec.dinv()
             nx, ny, nzg = (int(v) for v in it.ngrid)
             z_lo, nzs = slab_range(it, self.probe, self.dtip, slab_margin)
+            x_lo, nxs = lateral_range(it, self.probe, slab_margin, 0)
+            y_lo, nys = lateral_range(it, self.probe, slab_margin, 1)
             D = self.mols[j]
             D.grid_off, D.state_off = go, so
             D.atom_off, D.n_atoms = ao, len(a)
             D.pix_off, D.n_scan = po, it.n_scan
             D.nx, D.ny, D.nz = nx, ny, nzg
             D.z_lo, D.nz_slab = z_lo, nzs
+            D.x_lo, D.nx_slab, D.y_lo, D.ny_slab = x_lo, nxs, y_lo, nys
             D.nz_steps, D.raster_ny = int(it.nz), len(it.ys)
             D.p0, D.dA, D.dB, D.dC = f4(p0), f4(dA), f4(dB), f4(dC)
             D.dinvA, D.dinvB, D.dinvC = f4(dinv[0]), f4(dinv[1]), f4(dinv[2])
@@ -161,7 +185,7 @@ class BatchPlan:
             ao += len(a)
             po += it.n_scan
             so += it.n_scan * int(it.nz)
-            go += nx * ny * nzs
+            go += nxs * nys * nzs
         self.atoms = np.ascontiguousarray(np.concatenate(atoms_l))
         self.params = np.ascontiguousarray(np.concatenate(params_l))
         self.points = np.ascontiguousarray(np.concatenate(pts_l))
@@ -188,9 +212,10 @@ class AFMBatch:
     """A batch of molecules resident on one GPU (see the module docstring).
 
     items: list of BatchItem; kind: 0 LJ / 1 Morse (one kind per batch);
-    probe: ProbeSpec; dtip: z-step (< 0: approach); slab_margin: A of z above
-    and below the tip's range whose layers are built; shape: BatchShape (None =
-    library default; ``spammm_b200.autotune`` searches better ones)."""
+    probe: ProbeSpec; dtip: z-step (< 0: approach); slab_margin: A beyond the
+    scan window (x, y) and the tip's z-range whose nodes are built; shape:
+    BatchShape (None = library default; ``spammm_b200.autotune`` searches
+    better ones)."""
 
     def __init__(self, items, kind=0, probe=None, dtip=-0.1, slab_margin=1.5, shape=None, order="lpt"):
         _lib.require_cuda()
@@ -377,13 +402,19 @@ class AFMBatch:
         return D.atom_off, D.atom_off + D.n_atoms
 
     def slab(self, i, slot=0):
-        """(nz_slab, ny, nx, 4) view of molecule i's stored layers (slot 0: the
-        nodes' own values; layer 0 is the full grid's layer z_lo).  Other slots
-        hold the (x+1), (z+1) and (x+1, z+1) neighbours of the layout."""
+        """(nz_slab, ny_slab, nx_slab, 4) view of molecule i's stored box (slot
+        0: the nodes' own values; [0, 0, 0] is the full grid's node (x_lo, y_lo,
+        z_lo)).  Other slots hold the (x+1), (z+1) and (x+1, z+1) neighbours of
+        the layout, wrapped inside the box."""
         D = self.desc(i)
-        n = D.nx * D.ny * D.nz_slab
+        n = D.nx_slab * D.ny_slab * D.nz_slab
         k = self.node_stride
-        return self.grid.view(-1, k, 4)[D.grid_off:D.grid_off + n, slot].reshape(D.nz_slab, D.ny, D.nx, 4)
+        return self.grid.view(-1, k, 4)[D.grid_off:D.grid_off + n, slot].reshape(D.nz_slab, D.ny_slab, D.nx_slab, 4)
+
+    def slab_of_full(self, i, full):
+        """The part of a full (nz, ny, nx, ...) grid of molecule i that its slab stores."""
+        D = self.desc(i)
+        return full[D.z_lo:D.z_lo + D.nz_slab, D.y_lo:D.y_lo + D.ny_slab, D.x_lo:D.x_lo + D.nx_slab]
 
     def fes(self, i):
         a, b = self._rows(i, "state")

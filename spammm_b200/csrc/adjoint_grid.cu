@@ -55,8 +55,13 @@ struct Corners {
     bool ok;
 };
 
+// Both texels i[0], i[1] of a cell along one axis lie in the stored range [lo, lo + n).
+__device__ __forceinline__ bool in_slab(const int* i, int lo, int n) {
+    return (unsigned)(i[0] - lo) < (unsigned)n && (unsigned)(i[1] - lo) < (unsigned)n;
+}
+
 // Texel cell of a point (the same REPEAT/LINEAR addressing as interp_fe).
-// Indices are the full grid's; SLAB: ok only if both z layers are stored.
+// Indices are the full grid's; SLAB: ok only if all eight texels are stored.
 template <bool SLAB>
 __device__ __forceinline__ Corners corners_of(const GridView& G, V3 p) {
     Corners C;
@@ -67,18 +72,18 @@ __device__ __forceinline__ Corners corners_of(const GridView& G, V3 p) {
     C.ok = tex_axis(v, G.ny, C.y[0], C.y[1], C.ay) && C.ok;
     C.ok = tex_axis(w, G.nz, C.z[0], C.z[1], C.az) && C.ok;
     if (SLAB)
-        C.ok = C.ok && (unsigned)(C.z[0] - G.z_lo) < (unsigned)G.nz_slab &&
-               (unsigned)(C.z[1] - G.z_lo) < (unsigned)G.nz_slab;
+        C.ok = C.ok && in_slab(C.x, G.x_lo, G.nx_slab) && in_slab(C.y, G.y_lo, G.ny_slab) &&
+               in_slab(C.z, G.z_lo, G.nz_slab);
     return C;
 }
 
-// Stored node (x, y, z) of a full grid or of a batch slab (z is the full
-// grid's layer; batch slabs hold G.stride float4 per node, its value first).
+// Stored node (x, y, z) (full-grid indices) of a full grid or of a batch slab
+// (batch slabs hold G.stride float4 per node, its value first).
 template <bool SLAB>
 __device__ __forceinline__ float4 node_at(const GridView& G, int x, int y, int z) {
-    const int zl = SLAB ? z - G.z_lo : z;
-    const size_t idx = ((size_t)zl * G.ny + y) * G.nx + x;
-    return __ldg(G.g + (SLAB ? (size_t)G.stride * idx : idx));
+    if (!SLAB) return __ldg(G.g + ((size_t)z * G.ny + y) * G.nx + x);
+    const size_t idx = ((size_t)(z - G.z_lo) * G.ny_slab + (y - G.y_lo)) * G.nx_slab + (x - G.x_lo);
+    return __ldg(G.g + (size_t)G.stride * idx);
 }
 
 struct Sites {
@@ -399,7 +404,7 @@ GridView view_of(const float* grid, int nx, int ny, int nz, const spm_scan_param
     GridView G;
     G.g = reinterpret_cast<const float4*>(grid);
     G.nx = nx; G.ny = ny; G.nz = nz;
-    G.z_lo = 0; G.nz_slab = nz; G.stride = 1;
+    G.x_lo = 0; G.nx_slab = nx; G.y_lo = 0; G.ny_slab = ny; G.z_lo = 0; G.nz_slab = nz; G.stride = 1;
     G.dA = make_float4(p->dinvA[0], p->dinvA[1], p->dinvA[2], p->dinvA[3]);
     G.dB = make_float4(p->dinvB[0], p->dinvB[1], p->dinvB[2], p->dinvB[3]);
     G.dC = make_float4(p->dinvC[0], p->dinvC[1], p->dinvC[2], p->dinvC[3]);
@@ -460,9 +465,10 @@ adj_clear_kernel(ulonglong2* __restrict__ gq, long long n2, const unsigned long 
 }
 
 // CTA per 256-state chunk (one molecule): per-molecule max |ubar| (as float
-// bits; order-free) and the bounding box of the rows and slab layers the
-// scatter will touch, box[4m..4m+3] = max of (ny-1-y, y+1, nz_slab-1-zl, zl+1)
-// over the cell corners of every state with a non-zero ubar (all zero: none).
+// bits; order-free) and the bounding box of the slab rows and layers the
+// scatter will touch, box[4m..4m+3] = max of (ny_slab-1-yl, yl+1,
+// nz_slab-1-zl, zl+1) over the cell corners of every state with a non-zero
+// ubar (all zero: none); yl, zl are slab rows and layers.
 // Block 0 marks the adjoint grid dirty (the scatter follows).
 __global__ void __launch_bounds__(256)
 batch_ubar_max_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float4* __restrict__ ubar,
@@ -488,8 +494,8 @@ batch_ubar_max_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const f
             if (C.ok) {
 #pragma unroll
                 for (int k = 0; k < 2; k++) {
-                    b[0] = max(b[0], G.ny - 1 - C.y[k]);
-                    b[1] = max(b[1], C.y[k] + 1);
+                    b[0] = max(b[0], G.ny_slab - 1 - (C.y[k] - G.y_lo));
+                    b[1] = max(b[1], C.y[k] - G.y_lo + 1);
                     b[2] = max(b[2], G.nz_slab - 1 - (C.z[k] - G.z_lo));
                     b[3] = max(b[3], C.z[k] - G.z_lo + 1);
                 }
@@ -537,7 +543,7 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
     bool valid = !(ub.x == 0.f && ub.y == 0.f && ub.z == 0.f && ub.w == 0.f);
     Corners C = {{0, 0}, {0, 0}, {0, 0}, 0.f, 0.f, 0.f, false};
     long long stroke = -1;
-    int nx = 0, ny = 0, z_lo = 0;
+    int nxs = 0, nys = 0, x_lo = 0, y_lo = 0, z_lo = 0;
     unsigned long long* base = gq;
     double scale = 0.0;
     if (valid) {
@@ -550,7 +556,8 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
         const long long ls = st - D->state_off;
         stroke = D->pix_off + (ls < (1LL << 32) ? (long long)((unsigned)ls / (unsigned)D->nz_steps)
                                                 : ls / D->nz_steps);
-        nx = G.nx; ny = G.ny; z_lo = G.z_lo;
+        nxs = G.nx_slab; nys = G.ny_slab;
+        x_lo = G.x_lo; y_lo = G.y_lo; z_lo = G.z_lo;
         base = gq + (size_t)D->grid_off * 4;
         scale = pow2(42 - scale_exp(__ldg(umax + m)));
     }
@@ -590,7 +597,7 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
                 if (c >= 4 && given) continue;
                 if (q[c] == 0) continue;
                 const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
-                const size_t node = ((size_t)(C.z[k] - z_lo) * ny + C.y[j]) * nx + C.x[i];
+                const size_t node = ((size_t)(C.z[k] - z_lo) * nys + (C.y[j] - y_lo)) * nxs + (C.x[i] - x_lo);
                 atomicAdd(base + node * 4 + ch, (unsigned long long)q[c]);
             }
         }
@@ -742,6 +749,20 @@ __device__ __forceinline__ void pair_adj2(f2 nx, f2 ny, f2 nz, f2 gx, f2 gy, f2 
 
 __device__ __forceinline__ f2 lds2(const float* p) { return *reinterpret_cast<const f2*>(p); }
 
+// acc[c] += the two lanes of sums[c] (FP64), sums[c] = 0; the pair-parameter
+// columns only with PAR.
+template <bool PAR>
+__device__ __forceinline__ void fold_sums(f2* sums, double* acc) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+        if (!PAR && (c == 3 || c == 4)) continue;
+        float lo, hi;
+        upk(sums[c], lo, hi);
+        acc[c] += (double)lo + (double)hi;
+        sums[c] = bc(0.f);
+    }
+}
+
 // Dynamic shared memory of batch_adjoint_nodes_kernel: x, y, z, gx, gy, gz, gw
 // of up to 2*NM_STAGE staged nodes (+1 zero-weight pad node), the phase
 // partials and the double-buffered warp counts of the compaction scan.
@@ -764,9 +785,11 @@ constexpr size_t NM_SMEM = 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(
 // Three CTAs per SM (80 registers, a few bytes spilled, 3 x 70 KB of shared
 // memory): the loop is bound by its dependency chains, so the third CTA's
 // warps pay (12.2 -> 10.7 ms on the 64-molecule fit against two CTAs at 128
-// registers).  PAR: also the pair-parameter columns 3-4 (else written as 0).
-template <int KIND, bool ON, bool PAR>
-__global__ void __launch_bounds__(NM_THREADS, 3)
+// registers).  ILP = 2: two independent node pairs per step at two CTAs per
+// SM (up to 128 registers).  PAR: also the pair-parameter columns 3-4 (else
+// written as 0).
+template <int KIND, bool ON, bool PAR, int ILP>
+__global__ void __launch_bounds__(NM_THREADS, ILP == 2 ? 2 : 3)
 batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk,
                            const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
                            NodeSites S, unsigned long long* __restrict__ gq, const int* __restrict__ box,
@@ -781,7 +804,8 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
     const int m = SPM_MOL_BY(unit_off, mols, n_mol, unit);
     const spm_batch_mol* D = mols + m;
     const long long lc = unit - D->unit_off;
-    const int nx = D->nx, ny = D->ny, z_lo = D->z_lo;
+    // slab pitches (stored columns, rows) and the stored box's corner in the full grid
+    const int nx = D->nx_slab, ny = D->ny_slab, x_lo = D->x_lo, y_lo = D->y_lo, z_lo = D->z_lo;
     const long long slab = (long long)nx * ny * D->nz_slab;
     const long long n0 = lc * chunk;
     const long long n1 = n0 + chunk < slab ? n0 + chunk : slab;
@@ -793,7 +817,7 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
     NG.dC = ld4f(D->dC);
     const double inv_scale = pow2(scale_exp(__ldg(umax + m)) - 42);
     ulonglong2* q2 = reinterpret_cast<ulonglong2*>(gq + (size_t)D->grid_off * 4);
-    // touched rows y in [ylo, yhi] and slab layers in [zlo, zhi] (empty: yhi < 0)
+    // touched slab rows in [ylo, yhi] and slab layers in [zlo, zhi] (empty: yhi < 0)
     const int ylo = ny - 1 - box[4 * m], yhi = box[4 * m + 1] - 1;
     const int zlo = D->nz_slab - 1 - box[4 * m + 2], zhi = box[4 * m + 3] - 1;
     auto touched = [&](long long b0, long long b1) {  // may nodes [b0, b1) be non-zero?
@@ -859,29 +883,34 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
                 f2 a32[6] = {zero, zero, zero, zero, zero, zero};
                 int n32 = 0;
                 const int Lp = (L + 1) >> 1;
-                for (int jp = ph; jp < Lp; jp += P) {
+                auto pair_at = [&](int jp, f2* sums) {
                     const int j = 2 * jp;
                     pair_adj2<KIND, ON, PAR>(lds2(&s_n[0][j]), lds2(&s_n[1][j]), lds2(&s_n[2][j]), lds2(&s_n[3][j]),
-                                        lds2(&s_n[4][j]), lds2(&s_n[5][j]), lds2(&s_n[6][j]), C, S, a32);
-                    if (++n32 == NM_FLUSH / 2) {
-#pragma unroll
-                        for (int c = 0; c < 6; c++) {
-                            if (!PAR && (c == 3 || c == 4)) continue;
-                            float lo, hi;
-                            upk(a32[c], lo, hi);
-                            acc[c] += (double)lo + (double)hi;
-                            a32[c] = zero;
+                                             lds2(&s_n[4][j]), lds2(&s_n[5][j]), lds2(&s_n[6][j]), C, S, sums);
+                };
+                int jp = ph;
+                if (ILP == 2) {
+                    // two independent node pairs per step, each into its own FP32 sums
+                    f2 b32[6] = {zero, zero, zero, zero, zero, zero};
+                    for (; jp + P < Lp; jp += 2 * P) {
+                        pair_at(jp, a32);
+                        pair_at(jp + P, b32);
+                        if (++n32 == NM_FLUSH / 2) {
+                            fold_sums<PAR>(a32, acc);
+                            fold_sums<PAR>(b32, acc);
+                            n32 = 0;
                         }
+                    }
+                    fold_sums<PAR>(b32, acc);
+                }
+                for (; jp < Lp; jp += P) {
+                    pair_at(jp, a32);
+                    if (++n32 == NM_FLUSH / 2) {
+                        fold_sums<PAR>(a32, acc);
                         n32 = 0;
                     }
                 }
-#pragma unroll
-                for (int c = 0; c < 6; c++) {
-                    if (!PAR && (c == 3 || c == 4)) continue;
-                    float lo, hi;
-                    upk(a32[c], lo, hi);
-                    acc[c] += (double)lo + (double)hi;
-                }
+                fold_sums<PAR>(a32, acc);
             }
             __syncthreads();  // the buffer is restaged next
         };
@@ -930,8 +959,8 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
                     q2[2 * li + 1] = make_ulonglong2(0ull, 0ull);
                 }
                 const unsigned l32 = (unsigned)li, yz = l32 / (unsigned)nx;  // slabs hold < 2^32 nodes
-                const int ix = (int)(l32 - yz * (unsigned)nx);
-                const int iy = (int)(yz % (unsigned)ny), iz = (int)(yz / (unsigned)ny) + z_lo;
+                const int ix = (int)(l32 - yz * (unsigned)nx) + x_lo;
+                const int iy = (int)(yz % (unsigned)ny) + y_lo, iz = (int)(yz / (unsigned)ny) + z_lo;
                 s_n[0][off] = NG.p0.x + NG.dA.x * ix + NG.dB.x * iy + NG.dC.x * iz;
                 s_n[1][off] = NG.p0.y + NG.dA.y * ix + NG.dB.y * iy + NG.dC.y * iz;
                 s_n[2][off] = NG.p0.z + NG.dA.z * ix + NG.dB.z * iy + NG.dC.z * iz;
@@ -980,7 +1009,7 @@ batch_fold_rows_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int ch
     const int c = blockIdx.y;
     const spm_batch_mol* D = mols + SPM_MOL_BY(atom_off, mols, n_mol, ga);
     const long long nst = (long long)D->n_scan * D->nz_steps;
-    const long long slab = (long long)D->nx * D->ny * D->nz_slab;
+    const long long slab = (long long)D->nx_slab * D->ny_slab * D->nz_slab;
     const long long nu = nst > 0 ? (slab + chunk - 1) / chunk : 0;
     const long long a = ga - D->atom_off;
     double acc = 0.0;
@@ -992,6 +1021,24 @@ batch_fold_rows_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int ch
         __syncthreads();
     }
     if (threadIdx.x == 0) grad[ga * 6 + c] = red[0];
+}
+
+using NodeKern = decltype(&batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, true, 1>);
+
+template <bool PAR, int ILP>
+NodeKern node_kernel(int kind, bool on) {
+    if (kind == SPM_KIND_MORSE)
+        return on ? batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, PAR, ILP>
+                  : batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, PAR, ILP>;
+    return on ? batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, PAR, ILP>
+              : batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, PAR, ILP>;
+}
+
+// The node kernel for a pair law, on-node charges or not, pair-parameter
+// columns or not, and 1 or 2 node pairs per step.
+NodeKern node_kernel(int kind, bool on, bool par, int ilp) {
+    if (ilp == 2) return par ? node_kernel<true, 2>(kind, on) : node_kernel<false, 2>(kind, on);
+    return par ? node_kernel<true, 1>(kind, on) : node_kernel<false, 1>(kind, on);
 }
 
 // Scratch layout of spm_batch_adjoint_params (byte offsets, 16-byte aligned):
@@ -1064,6 +1111,7 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
     const int chunk = shape->adj_chunk;
     SPM_REQUIRE(chunk >= 1024 && chunk <= (1 << 20) && chunk % 1024 == 0, "spm_batch_adjoint_params: adj_chunk=%d",
                 chunk);
+    SPM_REQUIRE(shape->adj_ilp == 1 || shape->adj_ilp == 2, "spm_batch_adjoint_params: adj_ilp=%d", shape->adj_ilp);
     SPM_REQUIRE((reinterpret_cast<uintptr_t>(scratch) & 15u) == 0, "spm_batch_adjoint_params: scratch not 16-byte aligned");
     SPM_REQUIRE(n_units < (1LL << 31) && n_chunks < (1LL << 31) && n_atoms < (1LL << 30) &&
                 (n_states + 255) / 256 < (1LL << 31), "spm_batch_adjoint_params: batch too large");
@@ -1087,16 +1135,12 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             if (cudaGetDevice(&dev) != cudaSuccess)
                 return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: no current device");
             if (dev < 0 || dev >= 64 || !smem_set[dev]) {
-                for (auto k : {batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, true>,
-                               batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, true>,
-                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, true>,
-                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, true>,
-                               batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, false>,
-                               batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, false>,
-                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, false>,
-                               batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, false>})
+                for (int v = 0; v < 16; v++) {
+                    const auto k = node_kernel(v & 1 ? SPM_KIND_MORSE : SPM_KIND_LJ, (v & 2) != 0, (v & 4) != 0,
+                                               v & 8 ? 2 : 1);
                     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)NM_SMEM) != cudaSuccess)
                         return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: cannot set shared memory size");
+                }
                 if (dev >= 0 && dev < 64) smem_set[dev] = true;
             }
             if (cudaMemsetAsync(umax, 0, (size_t)(SL.mark - SL.umax), st) != cudaSuccess)  // maxima + boxes
@@ -1111,16 +1155,7 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             const NodeSites S = make_node_sites(Qs, QZs);
             const int pstride = kind == SPM_KIND_MORSE ? 4 : 2;
             const bool on = S.qon != 0.f;
-            using NodeKern = decltype(&batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, true>);
-            // [pair-parameter columns][kind][on-node charges]
-            static const NodeKern table[2][2][2] = {
-                {{batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, false>, batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, false>},
-                 {batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, false>,
-                  batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, false>}},
-                {{batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, true>, batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, true>},
-                 {batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, true>,
-                  batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, true>}}};
-            const NodeKern kern = table[(adj_flags & SPM_ADJ_PAIR_PARAMS) ? 1 : 0][kind == SPM_KIND_MORSE ? 1 : 0][on ? 1 : 0];
+            const auto kern = node_kernel(kind, on, (adj_flags & SPM_ADJ_PAIR_PARAMS) != 0, shape->adj_ilp);
             kern<<<(unsigned)n_units, NM_THREADS, NM_SMEM, st>>>(n_mol, mols, chunk,
                                                                  reinterpret_cast<const float4*>(atoms), params, pstride,
                                                                  S, gq, box, umax, part);

@@ -2,7 +2,7 @@
 //
 // spm_batch_prepare validates a descriptor array and numbers the work items of
 // every batched stage across the batch for one launch shape:
-//   tile_off   grid-build CTA tiles  ceil(nx/32) x ceil(ny/gb_ty) x ceil(nz_slab/gb_zb)
+//   tile_off   grid-build CTA tiles  ceil(nx_slab/32) x ceil(ny_slab/gb_ty) x ceil(nz_slab/gb_zb)
 //   slot_off   relaxation slots      raster: 32 per (32/h) x h pixel tile, else one per pixel
 //                                    rounded up to 32 (a warp's 32 slots never span molecules)
 //   unit_off   adjoint node units    ceil(slab nodes/adj_chunk) (0 without states)
@@ -23,6 +23,7 @@ extern "C" spm_batch_shape spm_batch_default_shape(void) {
     s.rx_regs = 3;
     s.grid_layout = 0;
     s.rx_sync = 1;
+    s.adj_ilp = 1;
     return s;
 }
 
@@ -45,6 +46,7 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
     SPM_REQUIRE(S.rx_regs >= 0 && S.rx_regs <= 3, "spm_batch_prepare: rx_regs=%d", S.rx_regs);
     SPM_REQUIRE(S.grid_layout == 0 || S.grid_layout == 1, "spm_batch_prepare: grid_layout=%d", S.grid_layout);
     SPM_REQUIRE(S.rx_sync == 0 || S.rx_sync == 1, "spm_batch_prepare: rx_sync=%d", S.rx_sync);
+    SPM_REQUIRE(S.adj_ilp == 1 || S.adj_ilp == 2, "spm_batch_prepare: adj_ilp=%d", S.adj_ilp);
     const long long th = S.rx_tile_h, tw = 32 / S.rx_tile_h;
     long long tiles = 0, slots = 0, units = 0, chunks = 0, states = 0, atoms = 0, pixels = 0, grid_end = 0, rows = 0;
     for (int m = 0; m < n_mol; m++) {
@@ -59,7 +61,11 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
                     D.nz);
         SPM_REQUIRE(D.z_lo >= 0 && D.nz_slab >= 1 && (long long)D.z_lo + D.nz_slab <= D.nz,
                     "spm_batch_prepare: molecule %d: slab [%d,%d) outside [0,%d)", m, D.z_lo, D.z_lo + D.nz_slab, D.nz);
-        const long long slab = (long long)D.nx * D.ny * D.nz_slab;
+        SPM_REQUIRE(D.x_lo >= 0 && D.nx_slab >= 1 && (long long)D.x_lo + D.nx_slab <= D.nx && D.y_lo >= 0 &&
+                    D.ny_slab >= 1 && (long long)D.y_lo + D.ny_slab <= D.ny,
+                    "spm_batch_prepare: molecule %d: slab columns [%d,%d) / rows [%d,%d) outside the (%d,%d) grid", m,
+                    D.x_lo, D.x_lo + D.nx_slab, D.y_lo, D.y_lo + D.ny_slab, D.nx, D.ny);
+        const long long slab = (long long)D.nx_slab * D.ny_slab * D.nz_slab;
         SPM_REQUIRE(slab < (1LL << 32), "spm_batch_prepare: molecule %d: slab of %lld nodes >= 2^32", m, slab);
         SPM_REQUIRE(D.grid_off >= grid_end, "spm_batch_prepare: molecule %d: grid_off=%lld overlaps the previous slab "
                     "(ends at %lld)", m, D.grid_off, grid_end);
@@ -75,7 +81,8 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
         D.unit_off = units;
         D.chunk_off = chunks;
         D.row_off = rows;
-        tiles += ((D.nx + 31LL) / 32) * ((D.ny + S.gb_ty - 1LL) / S.gb_ty) * ((D.nz_slab + S.gb_zb - 1LL) / S.gb_zb);
+        tiles += ((D.nx_slab + 31LL) / 32) * ((D.ny_slab + S.gb_ty - 1LL) / S.gb_ty) *
+                 ((D.nz_slab + S.gb_zb - 1LL) / S.gb_zb);
         if (nst > 0) {
             if (D.raster_ny > 0) {
                 const long long nxr = D.n_scan / D.raster_ny;

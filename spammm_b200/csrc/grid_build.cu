@@ -73,19 +73,27 @@ __device__ __forceinline__ float node_xy(float p0, float da, float db, int ia, i
     return __fmaf_rn(db, (float)ib, __fmaf_rn(da, (float)ia, p0));
 }
 
-// One CTA tile: a (blockDim.x x blockDim.y) patch of z-columns, ZB nodes each
-// starting at global layer ic0; nodes at layers >= zst_hi are not stored, the
-// rest go to out[idx], idx = ((ic - zst_lo)*ny + ib)*nx + ia (LAYOUT 1).
-// LAYOUT 2, x-pairs: out[2*idx + dx] = value(x + dx mod nx), so a node's
-// value is also written to its x-1 neighbour's second slot.  LAYOUT 4,
-// xz-quads: out[4*idx + 2*dz + dx] = value(x + dx mod nx, z + dz mod nz_slab),
-// written to the four nodes whose quads contain it.
+// The stored box of a build: columns [x_lo, x_lo + nxs), rows [y_lo, y_lo +
+// nys) and layers [zst_lo, zst_hi) of the full grid.
+struct StoreBox {
+    int x_lo, nxs, y_lo, nys, zst_lo, zst_hi;
+};
+
+// One CTA tile: a (blockDim.x x blockDim.y) patch of z-columns (full-grid
+// column ia, row ib), ZB nodes each starting at global layer ic0; nodes
+// outside the box B are not stored, the rest go to out[idx], idx = (zl*nys +
+// yl)*nxs + xl with (xl, yl, zl) = (ia - x_lo, ib - y_lo, ic - zst_lo)
+// (LAYOUT 1).  LAYOUT 2, x-pairs: out[2*idx + dx] = value(x_lo + (xl + dx) mod
+// nxs), so a node's value is also written to its x-1 neighbour's second slot.
+// LAYOUT 4, xz-quads: out[4*idx + 2*dz + dx] = value(x_lo + (xl + dx) mod nxs,
+// zst_lo + (zl + dz) mod (zst_hi - zst_lo)), written to the four nodes whose
+// quads contain it.
 // KIND: SPM_KIND_LJ / SPM_KIND_MORSE; ON: an on-node charge term exists;
 // NOFF: number of off-node sites.
 template <int KIND, bool ON, int NOFF, int ZB, int LAYOUT = 1>
 __device__ __forceinline__ void build_tile(int na, const float4* __restrict__ atoms, const float* __restrict__ params,
                                            int pstride, float4* __restrict__ out, const GridGeom& G,
-                                           const TipSites& S, int ia, int ib, int ic0, int zst_lo, int zst_hi) {
+                                           const TipSites& S, const StoreBox& B, int ia, int ib, int ic0) {
     constexpr int ZP = ZB / 2;
     __shared__ float4 s_pos[GB_TILE];                   // (x, y, z, Q*qs_on)
     __shared__ float4 s_prm[GB_TILE];                   // transformed pair parameters
@@ -93,7 +101,8 @@ __device__ __forceinline__ void build_tile(int na, const float4* __restrict__ at
 
     const int nthr = blockDim.x * blockDim.y;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const bool active = (ia < G.nx) && (ib < G.ny);
+    const int xl = ia - B.x_lo, yl = ib - B.y_lo;
+    const bool active = (unsigned)xl < (unsigned)B.nxs && (unsigned)yl < (unsigned)B.nys;
 
     const float px = node_xy(G.p0.x, G.dA.x, G.dB.x, ia, ib);
     const float py = node_xy(G.p0.y, G.dA.y, G.dB.y, ia, ib);
@@ -203,26 +212,26 @@ __device__ __forceinline__ void build_tile(int na, const float4* __restrict__ at
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int ic = ic0 + 2 * p + h;
-            if (ic >= zst_hi) break;
+            if (ic >= B.zst_hi) break;
             float4 o = make_float4(x[h], y[h], z[h], e[h]);
             // |E| > 100 cap of the reference builders (AFM.cl:1053-1054)
             const float renorm = __fdiv_rn(100.f, fabsf(o.w));
             if (renorm < 1.f) { o.x *= renorm; o.y *= renorm; o.z *= renorm; o.w *= renorm; }
-            const int zl = ic - zst_lo;
-            const size_t row = ((size_t)zl * G.ny + ib) * G.nx;
-            const int il = ia > 0 ? ia - 1 : G.nx - 1;
+            const int zl = ic - B.zst_lo;
+            const size_t row = ((size_t)zl * B.nys + yl) * B.nxs;
+            const int il = xl > 0 ? xl - 1 : B.nxs - 1;
             if (LAYOUT == 2) {
-                out[2 * (row + ia)] = o;
+                out[2 * (row + xl)] = o;
                 out[2 * (row + il) + 1] = o;
             } else if (LAYOUT == 4) {
-                const int nzs = zst_hi - zst_lo;
-                const size_t rowb = ((size_t)(zl > 0 ? zl - 1 : nzs - 1) * G.ny + ib) * G.nx;
-                out[4 * (row + ia) + 0] = o;
+                const int nzs = B.zst_hi - B.zst_lo;
+                const size_t rowb = ((size_t)(zl > 0 ? zl - 1 : nzs - 1) * B.nys + yl) * B.nxs;
+                out[4 * (row + xl) + 0] = o;
                 out[4 * (row + il) + 1] = o;
-                out[4 * (rowb + ia) + 2] = o;
+                out[4 * (rowb + xl) + 2] = o;
                 out[4 * (rowb + il) + 3] = o;
             } else {
-                out[row + ia] = o;
+                out[row + xl] = o;
             }
         }
     }
@@ -232,8 +241,9 @@ template <int KIND, bool ON, int NOFF>
 __global__ void __launch_bounds__(GB_TX * GB_TY)
 grid_build_kernel(int na, const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
                   float4* __restrict__ grid, GridGeom G, TipSites S) {
-    build_tile<KIND, ON, NOFF, GB_ZB>(na, atoms, params, pstride, grid, G, S, blockIdx.x * GB_TX + threadIdx.x,
-                                      blockIdx.y * GB_TY + threadIdx.y, blockIdx.z * GB_ZB, 0, G.nz);
+    const StoreBox B = {0, G.nx, 0, G.ny, 0, G.nz};
+    build_tile<KIND, ON, NOFF, GB_ZB>(na, atoms, params, pstride, grid, G, S, B, blockIdx.x * GB_TX + threadIdx.x,
+                                      blockIdx.y * GB_TY + threadIdx.y, blockIdx.z * GB_ZB);
 }
 
 template <int KIND, bool ON>
@@ -277,7 +287,7 @@ TipSites make_sites(const float* Qs, const float* QZs, bool& on, int& noff) {
 
 // ---- batched slabs ----------------------------------------------------------
 // One CTA per tile of the batch; tiles of a molecule are numbered x fastest,
-// then y, then z over ceil(nx/32) x ceil(ny/TY) x ceil(nz_slab/ZB).
+// then y, then z over ceil(nx_slab/32) x ceil(ny_slab/TY) x ceil(nz_slab/ZB).
 template <int KIND, bool ON, int NOFF, int ZB, int LAYOUT>
 __global__ void __launch_bounds__(256)
 batch_grid_build_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float4* __restrict__ atoms,
@@ -285,25 +295,25 @@ batch_grid_build_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const
     const long long tile = blockIdx.x;
     const spm_batch_mol* D = mols + SPM_MOL_BY(tile_off, mols, n_mol, tile);
     const int ty = blockDim.y;
-    const int nx = D->nx, ny = D->ny, z_lo = D->z_lo, nzs = D->nz_slab;
+    const int z_lo = D->z_lo, nzs = D->nz_slab;
+    const StoreBox B = {D->x_lo, D->nx_slab, D->y_lo, D->ny_slab, z_lo, z_lo + nzs};
     const long long lt = tile - D->tile_off;
-    const int ntx = (nx + GB_TX - 1) / GB_TX, nty = (ny + ty - 1) / ty;
+    const int ntx = (B.nxs + GB_TX - 1) / GB_TX, nty = (B.nys + ty - 1) / ty;
     const int bx = (int)(lt % ntx);
     const long long r = lt / ntx;
     const int by = (int)(r % nty);
     const long long bz = r / nty;
     if (bz * ZB >= nzs) return;  // whole CTA: outside the slab (prefix of another shape)
     GridGeom G;
-    G.nx = nx; G.ny = ny; G.nz = D->nz;
+    G.nx = D->nx; G.ny = D->ny; G.nz = D->nz;
     G.p0 = ld4f(D->p0);
     G.dA = ld4f(D->dA);
     G.dB = ld4f(D->dB);
     G.dC = ld4f(D->dC);
     const int ao = D->atom_off;
     build_tile<KIND, ON, NOFF, ZB, LAYOUT>(D->n_atoms, atoms + ao, params + (size_t)ao * pstride, pstride,
-                                           grid + LAYOUT * D->grid_off,
-                                   G, S, bx * GB_TX + threadIdx.x, by * ty + threadIdx.y, z_lo + (int)bz * ZB, z_lo,
-                                   z_lo + nzs);
+                                           grid + LAYOUT * D->grid_off, G, S, B, B.x_lo + bx * GB_TX + threadIdx.x,
+                                           B.y_lo + by * ty + threadIdx.y, z_lo + (int)bz * ZB);
 }
 
 struct BatchLaunch {

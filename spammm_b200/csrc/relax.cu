@@ -105,21 +105,18 @@ __device__ __forceinline__ PPFrame pp_frame(const spm_scan_params& P) {
 
 // One SPM_RELAX_PP iteration (the direct path's bookkeeping: the convergence
 // test comes before the update).  Returns true when the z-step is finished;
-// conv tells whether it converged.  SLAB: a sample outside the stored layers
-// (NaN) ends the z-step at once, not converged.  CACHE: sample through the
-// texel cache T (full grids; fnx, fny, fnz the dimensions as floats).
-template <typename IDX, bool SLAB, bool CACHE>
+// conv tells whether it converged.  CACHE: sample through the texel cache T
+// (fnx, fny, fnz the dimensions as floats).
+template <typename IDX, bool CACHE>
 __device__ __forceinline__ bool pp_iter(const GridView& G, const PPFrame& F, V3 tip, V3& pos, V3& v, Integrator& I,
                                         float4& fe, int& it, int& total_it, bool& conv, TexelCache& T, float fnx,
                                         float fny, float fnz) {
-    static_assert(!(CACHE && SLAB), "the texel cache samples full grids");
     conv = false;
     if (it >= F.max_iter) return true;
     ++it;
     ++total_it;
     if constexpr (CACHE) fe = interp_fe_cached_full<IDX>(G, fnx, fny, fnz, pos, T);
-    else fe = interp_fe<IDX, SLAB>(G, pos);
-    if (SLAB && fe.w != fe.w) return true;
+    else fe = interp_fe<IDX>(G, pos);
     const V3 ft = rotmatT(tip_force(rotmat(sub3(pos, tip), F.a, F.b, F.c), F.kk, F.d0), F.a, F.b, F.c);
     V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
     f.x = __fmaf_rn(F.c.x, F.surf, f.x);
@@ -135,10 +132,10 @@ __device__ __forceinline__ bool pp_iter(const GridView& G, const PPFrame& F, V3 
 
 // Outputs of a finished SPM_RELAX_PP z-step: tip-frame FE at the final
 // position and PP = (pos, +iterations if converged and finite, else -iterations).
-template <typename IDX, bool SLAB>
+template <typename IDX>
 __device__ __forceinline__ void pp_emit(const GridView& G, const PPFrame& F, V3 pos, float4 fe, int it, bool conv,
                                         float4* fe_out, float4* pp_out) {
-    if (!conv) fe = interp_fe<IDX, SLAB>(G, pos);  // the position moved after the last sample
+    if (!conv) fe = interp_fe<IDX>(G, pos);  // the position moved after the last sample
     const V3 r = rotmat(mk3(fe.x, fe.y, fe.z), F.a, F.b, F.c);
     *fe_out = make_float4(r.x, r.y, r.z, fe.w);
     const bool finite = isfinite(fe.x) && isfinite(fe.y) && isfinite(fe.z) && isfinite(fe.w) && isfinite(pos.x) &&
@@ -209,9 +206,9 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
     while (k >= 0) {
         if (MODE == 2) {
             bool conv;
-            if (pp_iter<IDX, false, CACHE>(G, F, tip, pos, v, I, fe, it, total_it, conv, T, fnx, fny, fnz)) {
+            if (pp_iter<IDX, CACHE>(G, F, tip, pos, v, I, fe, it, total_it, conv, T, fnx, fny, fnz)) {
                 const size_t o = (size_t)k * nzs + iz;
-                pp_emit<IDX, false>(G, F, pos, fe, it, conv, FEs + o, disps + o);
+                pp_emit<IDX>(G, F, pos, fe, it, conv, FEs + o, disps + o);
                 tip = add3(tip, dTip);
                 pos = add3(pos, dTip);
                 v = mk3(0.f, 0.f, 0.f);
@@ -346,7 +343,7 @@ GridView make_view(const float* grid, int nx, int ny, int nz, const spm_scan_par
     GridView G;
     G.g = reinterpret_cast<const float4*>(grid);
     G.nx = nx; G.ny = ny; G.nz = nz;
-    G.z_lo = 0; G.nz_slab = nz; G.stride = 1;
+    G.x_lo = 0; G.nx_slab = nx; G.y_lo = 0; G.ny_slab = ny; G.z_lo = 0; G.nz_slab = nz; G.stride = 1;
     G.dA = make_float4(p->dinvA[0], p->dinvA[1], p->dinvA[2], p->dinvA[3]);
     G.dB = make_float4(p->dinvB[0], p->dinvB[1], p->dinvB[2], p->dinvB[3]);
     G.dC = make_float4(p->dinvC[0], p->dinvC[1], p->dinvC[2], p->dinvC[3]);
@@ -426,8 +423,8 @@ __device__ __forceinline__ bool next_batch_pixel(unsigned* counter, unsigned n_s
 // zero aside) -- and c*surf reduced to its z part.
 template <typename IDX, bool CACHE, int LAYOUT>
 __device__ __forceinline__ float4 sample_z(const AxisView& G, V3 p, TexelCache& T) {
-    if constexpr (CACHE) return interp_fe_cached<IDX, true, LAYOUT>(G, p, T);
-    else return interp_fe_cell<IDX, true, LAYOUT>(G, p);
+    if constexpr (CACHE) return interp_fe_cached<IDX, LAYOUT>(G, p, T);
+    else return interp_fe_cell<IDX, LAYOUT>(G, p);
 }
 
 template <typename IDX, bool CACHE, int LAYOUT>
@@ -458,6 +455,8 @@ __device__ __forceinline__ AxisView axis_view(const spm_batch_mol* D, const floa
     AxisView G;
     G.g = reinterpret_cast<const float4*>(grid) + LAYOUT * D->grid_off;
     G.nx = D->nx; G.ny = D->ny; G.nz = D->nz;
+    G.x_lo = D->x_lo; G.nx_slab = D->nx_slab;
+    G.y_lo = D->y_lo; G.ny_slab = D->ny_slab;
     G.z_lo = D->z_lo; G.nz_slab = D->nz_slab;
     G.fnx = (float)G.nx; G.fny = (float)G.ny; G.fnz = (float)G.nz;
     G.ax = D->dinvA[0]; G.aw = D->dinvA[3];

@@ -47,7 +47,7 @@ __device__ __forceinline__ bool slot_pixel(const spm_batch_mol* D, unsigned lt, 
     return ix < nxr && iy < ny;
 }
 
-// Sampling view of a molecule's slab (full-grid coordinates, stored layers
+// Sampling view of a molecule's slab (full-grid coordinates, the stored box
 // only; stride float4 per stored node: 2 x-pairs, 4 xz-quads, value first).
 __device__ __forceinline__ GridView slab_view(const spm_batch_mol& D, const float* grid, int stride = 2) {
     GridView G;
@@ -57,6 +57,10 @@ __device__ __forceinline__ GridView slab_view(const spm_batch_mol& D, const floa
     G.dA = ld4f(D.dinvA);
     G.dB = ld4f(D.dinvB);
     G.dC = ld4f(D.dinvC);
+    G.x_lo = D.x_lo;
+    G.nx_slab = D.nx_slab;
+    G.y_lo = D.y_lo;
+    G.ny_slab = D.ny_slab;
     G.z_lo = D.z_lo;
     G.nz_slab = D.nz_slab;
     return G;

@@ -121,16 +121,24 @@ struct GridView {
     const float4* __restrict__ g;
     int nx, ny, nz;
     float4 dA, dB, dC;  // normalized-coordinate transform rows
-    int z_lo, nz_slab;  // SLAB views: only layers [z_lo, z_lo + nz_slab) are stored
-    int stride;         // SLAB views: float4 per stored node (2 x-pairs, 4 xz-quads); node value first
+    // slab views: only the box [x_lo, x_lo + nx_slab) x [y_lo, y_lo + ny_slab) x [z_lo, z_lo + nz_slab)
+    // of the full grid is stored (full views: the whole grid)
+    int x_lo, nx_slab, y_lo, ny_slab, z_lo, nz_slab;
+    int stride;         // slab views: float4 per stored node (2 x-pairs, 4 xz-quads); node value first
 };
 
-// interpFE: exact FP32 trilinear sample with periodic wrap.  IDX is the type
-// of the node offsets (unsigned for grids below 2^32 nodes, size_t above).
-// SLAB: the grid holds only layers [z_lo, z_lo+nz_slab) of the full grid; the
-// coordinate arithmetic is the full grid's (identical results), and a sample
-// that needs a layer outside the slab returns NaN instead of reading it.
-template <typename IDX = size_t, bool SLAB = false>
+// The texels i0, i1 of a cell along one axis as indices of a stored range
+// [lo, lo + n): false when either lies outside it.
+__device__ __forceinline__ bool to_slab(int& i0, int& i1, int lo, int n) {
+    i0 -= lo;
+    i1 -= lo;
+    return (unsigned)i0 < (unsigned)n && (unsigned)i1 < (unsigned)n;
+}
+
+// interpFE: exact FP32 trilinear sample with periodic wrap on a full
+// (nz,ny,nx) grid.  IDX is the type of the node offsets (unsigned for grids
+// below 2^32 nodes, size_t above).
+template <typename IDX = size_t>
 __device__ __forceinline__ float4 interp_fe(const GridView& G, V3 p) {
     float u = __fmaf_rn(p.x, G.dA.x, __fmaf_rn(p.y, G.dA.y, __fmaf_rn(p.z, G.dA.z, G.dA.w)));
     float v = __fmaf_rn(p.x, G.dB.x, __fmaf_rn(p.y, G.dB.y, __fmaf_rn(p.z, G.dB.z, G.dB.w)));
@@ -140,11 +148,6 @@ __device__ __forceinline__ float4 interp_fe(const GridView& G, V3 p) {
     bool ok = tex_axis(u, G.nx, x0, x1, ax);
     ok = tex_axis(v, G.ny, y0, y1, ay) && ok;
     ok = tex_axis(w, G.nz, z0, z1, az) && ok;
-    if (SLAB) {
-        z0 -= G.z_lo;
-        z1 -= G.z_lo;
-        ok = ok && (unsigned)z0 < (unsigned)G.nz_slab && (unsigned)z1 < (unsigned)G.nz_slab;
-    }
     if (!ok) {
         float nan = __int_as_float(0x7fc00000);
         return make_float4(nan, nan, nan, nan);
@@ -171,7 +174,8 @@ __device__ __forceinline__ float4 interp_fe(const GridView& G, V3 p) {
 // an exact zero), and the samplers on an AxisView return interp_fe's sample.
 struct AxisView {
     const float4* __restrict__ g;
-    int nx, ny, nz, z_lo, nz_slab;
+    int nx, ny, nz;                                  // full grid
+    int x_lo, nx_slab, y_lo, ny_slab, z_lo, nz_slab;  // the stored box (batch slab)
     float fnx, fny, fnz;  // the dimensions as floats (converted once per pixel, not per sample)
     float ax, aw, by, bw, cz, cw;
 };
@@ -190,23 +194,23 @@ __device__ __forceinline__ void ld_pair(const float4* p, ulonglong2& lo, ulonglo
     hi = make_ulonglong2(c, d);
 }
 
-// The eight texels of cell (x0, y0..y1, z0..z1) of a slab in the x-pair
-// (LAYOUT 2: node idx at G.g[2*idx], its +x neighbour after it) or xz-quad
-// (LAYOUT 4: G.g[4*idx + 2*dz + dx]) layout, as packed channel pairs.  With
-// xz-quads the cell's 8 texels are two 64-byte chunks (rows y0 and y1).
+// The eight texels of cell (x0, y0..y1, z0..z1) (slab indices) of a slab in
+// the x-pair (LAYOUT 2: node idx at G.g[2*idx], its +x neighbour after it) or
+// xz-quad (LAYOUT 4: G.g[4*idx + 2*dz + dx]) layout, as packed channel pairs.
+// With xz-quads the cell's 8 texels are two 64-byte chunks (rows y0 and y1).
 template <int LAYOUT, typename IDX>
 __device__ __forceinline__ void load_cell(const AxisView& G, int x0, int y0, int y1, int z0, int z1,
                                           ulonglong2& f000, ulonglong2& f100, ulonglong2& f010, ulonglong2& f110,
                                           ulonglong2& f001, ulonglong2& f101, ulonglong2& f011, ulonglong2& f111) {
     if (LAYOUT == 4) {
-        const IDX q0 = ((IDX)z0 * G.ny + y0) * G.nx + x0, q1 = ((IDX)z0 * G.ny + y1) * G.nx + x0;
+        const IDX q0 = ((IDX)z0 * G.ny_slab + y0) * G.nx_slab + x0, q1 = ((IDX)z0 * G.ny_slab + y1) * G.nx_slab + x0;
         ld_pair(G.g + 4 * q0, f000, f100);
         ld_pair(G.g + 4 * q0 + 2, f001, f101);
         ld_pair(G.g + 4 * q1, f010, f110);
         ld_pair(G.g + 4 * q1 + 2, f011, f111);
     } else {
-        const IDX r00 = ((IDX)z0 * G.ny + y0) * G.nx + x0, r10 = ((IDX)z0 * G.ny + y1) * G.nx + x0;
-        const IDX r01 = ((IDX)z1 * G.ny + y0) * G.nx + x0, r11 = ((IDX)z1 * G.ny + y1) * G.nx + x0;
+        const IDX r00 = ((IDX)z0 * G.ny_slab + y0) * G.nx_slab + x0, r10 = ((IDX)z0 * G.ny_slab + y1) * G.nx_slab + x0;
+        const IDX r01 = ((IDX)z1 * G.ny_slab + y0) * G.nx_slab + x0, r11 = ((IDX)z1 * G.ny_slab + y1) * G.nx_slab + x0;
         ld_pair(G.g + 2 * r00, f000, f100);
         ld_pair(G.g + 2 * r10, f010, f110);
         ld_pair(G.g + 2 * r01, f001, f101);
@@ -217,10 +221,10 @@ __device__ __forceinline__ void load_cell(const AxisView& G, int x0, int y0, int
 // interp_fe on an AxisView over an x-paired (LAYOUT 2) or xz-quad (LAYOUT 4)
 // slab: the same texel addressing and the same lerps on the same values, so
 // the same sample, with the channel pairs (x,y) and (z,w) of a texel lerped
-// by one packed f32x2 instruction each.  (In a slab the cell's upper layer is
-// z0+1, or layer 0 when a full-grid slab wraps; both layouts store exactly
-// that layer.)
-template <typename IDX, bool SLAB, int LAYOUT>
+// by one packed f32x2 instruction each; NaN when the cell is not stored.  (The
+// cell's +x and +z texels are x0+1 and z0+1, or 0 when a slab spanning that
+// axis wraps; both layouts store exactly those.)
+template <typename IDX, int LAYOUT>
 __device__ __forceinline__ float4 interp_fe_cell(const AxisView& G, V3 p) {
     const float u = __fmaf_rn(p.x, G.ax, G.aw);
     const float v = __fmaf_rn(p.y, G.by, G.bw);
@@ -230,12 +234,8 @@ __device__ __forceinline__ float4 interp_fe_cell(const AxisView& G, V3 p) {
     bool ok = tex_axis(u, G.nx, G.fnx, x0, x1, ax);
     ok = tex_axis(v, G.ny, G.fny, y0, y1, ay) && ok;
     ok = tex_axis(w, G.nz, G.fnz, z0, z1, az) && ok;
-    (void)x1;  // the pair / quad holds it
-    if (SLAB) {
-        z0 -= G.z_lo;
-        z1 -= G.z_lo;
-        ok = ok && (unsigned)z0 < (unsigned)G.nz_slab && (unsigned)z1 < (unsigned)G.nz_slab;
-    }
+    ok = ok && to_slab(x0, x1, G.x_lo, G.nx_slab) && to_slab(y0, y1, G.y_lo, G.ny_slab) &&
+         to_slab(z0, z1, G.z_lo, G.nz_slab);
     if (!ok) {
         float nan = __int_as_float(0x7fc00000);
         return make_float4(nan, nan, nan, nan);
@@ -345,7 +345,7 @@ __device__ __forceinline__ float4 interp_fe_cached_full(const GridView& G, float
 // cell is identified by the floors of its three texel coordinates, so a
 // sample inside the cached cell needs no index arithmetic, wrap or range test
 // (a cached cell passed them; equal floors give the same indices).
-template <typename IDX, bool SLAB, int LAYOUT>
+template <typename IDX, int LAYOUT>
 __device__ __forceinline__ float4 interp_fe_cached(const AxisView& G, V3 p, TexelCache& T) {
     const float u = __fmaf_rn(p.x, G.ax, G.aw);
     const float v = __fmaf_rn(p.y, G.by, G.bw);
@@ -359,12 +359,8 @@ __device__ __forceinline__ float4 interp_fe_cached(const AxisView& G, V3 p, Texe
         bool ok = tex_index(fx, G.nx, G.fnx, x0, x1);
         ok = tex_index(fy, G.ny, G.fny, y0, y1) && ok;
         ok = tex_index(fz, G.nz, G.fnz, z0, z1) && ok;
-        (void)x1;
-        if (SLAB) {
-            z0 -= G.z_lo;
-            z1 -= G.z_lo;
-            ok = ok && (unsigned)z0 < (unsigned)G.nz_slab && (unsigned)z1 < (unsigned)G.nz_slab;
-        }
+        ok = ok && to_slab(x0, x1, G.x_lo, G.nx_slab) && to_slab(y0, y1, G.y_lo, G.ny_slab) &&
+             to_slab(z0, z1, G.z_lo, G.nz_slab);
         if (!ok) {
             float nan = __int_as_float(0x7fc00000);
             return make_float4(nan, nan, nan, nan);

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from spammm_b200 import _lib, synthetic
-from spammm_b200.batch import BatchPlan, ProbeSpec, slab_range
+from spammm_b200.batch import BatchPlan, ProbeSpec, lateral_range, slab_range
 
 
 def small_items(n=7, seed=5, kind=0):
@@ -15,9 +15,9 @@ def small_items(n=7, seed=5, kind=0):
 
 
 def test_struct_layout():
-    # spm_batch_mol: 7 int64 offsets, 12 int32 fields, 7 float[4] vectors
-    assert ctypes.sizeof(_lib.BatchMol) == 7 * 8 + 12 * 4 + 7 * 16
-    assert ctypes.sizeof(_lib.BatchShape) == 9 * 4
+    # spm_batch_mol: 7 int64 offsets, 16 int32 fields, 7 float[4] vectors
+    assert ctypes.sizeof(_lib.BatchMol) == 7 * 8 + 16 * 4 + 7 * 16
+    assert ctypes.sizeof(_lib.BatchShape) == 10 * 4
 
 
 @pytest.mark.parametrize("shape_kw", [{}, dict(gb_ty=2, gb_zb=16, rx_tile_h=1, adj_chunk=1024),
@@ -35,11 +35,11 @@ def test_prepare_totals(shape_kw):
     for j in range(plan.n):
         D = plan.mols[j]
         assert (D.tile_off, D.slot_off, D.unit_off, D.chunk_off, D.row_off) == (tiles, slots, units, chunks, rows)
-        tiles += -(-D.nx // 32) * -(-D.ny // shape.gb_ty) * -(-D.nz_slab // shape.gb_zb)
+        tiles += -(-D.nx_slab // 32) * -(-D.ny_slab // shape.gb_ty) * -(-D.nz_slab // shape.gb_zb)
         nst = D.n_scan * D.nz_steps
         nxr = D.n_scan // D.raster_ny
         slots += -(-nxr // tw) * -(-D.raster_ny // th) * 32
-        u = -(-(D.nx * D.ny * D.nz_slab) // shape.adj_chunk)
+        u = -(-(D.nx_slab * D.ny_slab * D.nz_slab) // shape.adj_chunk)
         units += u
         rows += u * D.n_atoms
         chunks += -(-nst // 256)
@@ -78,6 +78,29 @@ def test_slab_covers_probe_range():
     assert slab_range(it, probe, -0.1, 1.5) == (0, it.ngrid[2])
 
 
+def test_lateral_range_covers_scan_window():
+    """Stored columns and rows hold every texel a sample within the margin of
+    the scan window needs; a window whose margin reaches the grid edge keeps
+    the whole axis (periodic wrap)."""
+    probe = ProbeSpec()
+    items = synthetic.batch_molecules(12, seed=9)
+    for it in items:
+        for axis, c in ((0, it.xs), (1, it.ys)):
+            lo, n = lateral_range(it, probe, 1.5, axis)
+            o, h = float(it.origin[axis]), float(it.step)
+            for v in (float(c.min()) - 1.5, float(c.max()) + 1.5):
+                t = (v - o) / h
+                assert lo <= np.floor(t) and np.floor(t) + 1 < lo + n
+            assert 0 <= lo and lo + n <= it.ngrid[axis]
+    assert any(lateral_range(it, probe, 1.5, 0)[1] < it.ngrid[0] for it in items)  # boxes are smaller than grids
+    plan = BatchPlan(items)
+    assert plan.grid_float4 == sum(D.nx_slab * D.ny_slab * D.nz_slab for D in plan.mols)
+    it = items[0]
+    assert lateral_range(it, probe, float(it.ngrid[0]) * it.step, 0) == (0, it.ngrid[0])
+    import dataclasses
+    assert lateral_range(dataclasses.replace(it, xs=it.xs[:0]), probe, 1.5, 0) == (0, it.ngrid[0])
+
+
 def test_prepare_rejects_bad_descriptors():
     L = _lib.lib()
     shape = L.spm_batch_default_shape()
@@ -93,12 +116,22 @@ def test_prepare_rejects_bad_descriptors():
     plan.mols[1].nz_slab = plan.mols[1].nz + 1
     assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_ERR_ARG
     plan.mols[1].nz_slab = 4
+    # columns / rows outside the grid
+    for field, bad in (("x_lo", -1), ("nx_slab", 0), ("y_lo", -1), ("ny_slab", 0)):
+        old = getattr(plan.mols[0], field)
+        setattr(plan.mols[0], field, bad)
+        assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_ERR_ARG, field
+        setattr(plan.mols[0], field, old)
+    plan.mols[0].x_lo = plan.mols[0].nx - plan.mols[0].nx_slab + 1
+    assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_ERR_ARG
+    assert b"outside" in L.spm_last_error()
+    plan = BatchPlan(small_items(4))
     # overlapping slabs
     plan.mols[3].grid_off = plan.mols[2].grid_off
     assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_ERR_ARG
     plan = BatchPlan(small_items(4))
     for field, bad in (("gb_ty", 3), ("gb_zb", 4), ("rx_threads", 96), ("rx_tile_h", 6), ("adj_chunk", 1000), ("rx_regs", 4), ("grid_layout", 2),
-                       ("rx_sync", 2)):
+                       ("rx_sync", 2), ("adj_ilp", 3)):
         s = L.spm_batch_default_shape()
         setattr(s, field, bad)
         assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(s), totals) == _lib.SPM_ERR_ARG, field

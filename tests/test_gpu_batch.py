@@ -46,7 +46,7 @@ def test_batch_forward_matches_per_molecule(cuda, kind):
     for i, it in enumerate(b.items):
         spec, grid, P, pts, FEs, PPs = _per_molecule(b, i)
         D = b.desc(i)
-        full = grid[D.z_lo:D.z_lo + D.nz_slab]
+        full = b.slab_of_full(i, grid)
         assert torch.equal(b.slab(i), full), f"molecule {i}: slab differs from full grid"
         assert torch.equal(b.slab(i, 1), torch.roll(full, -1, dims=2)), f"molecule {i}: x-pair halves differ"
         assert (b.pps(i)[..., 3] > 0).all(), f"molecule {i}: a stroke left the slab or did not converge"
@@ -107,7 +107,7 @@ def test_batch_shapes_give_same_results(cuda):
                dict(grid_layout=1, rx_sync=0), dict(grid_layout=1, rx_regs=2), dict(grid_layout=1, rx_regs=1, gb_zb=16),
                dict(rx_sync=1, rx_regs=0), dict(rx_sync=1, rx_tile_h=1, rx_threads=64, rx_regs=2),
                dict(rx_sync=1, rx_tile_h=32, rx_regs=1, grid_layout=1), dict(rx_regs=3, rx_tile_h=2),
-               dict(rx_sync=0, rx_regs=3, grid_layout=1)):
+               dict(rx_sync=0, rx_regs=3, grid_layout=1), dict(adj_ilp=2), dict(adj_ilp=2, adj_chunk=4096)):
         s = L.spm_batch_default_shape()
         for k, v in kw.items():
             setattr(s, k, v)
