@@ -749,16 +749,16 @@ __device__ __forceinline__ void pair_adj2(f2 nx, f2 ny, f2 nz, f2 gx, f2 gy, f2 
 
 __device__ __forceinline__ f2 lds2(const float* p) { return *reinterpret_cast<const f2*>(p); }
 
-// acc[c] += the two lanes of sums[c] (FP64), sums[c] = 0; the pair-parameter
-// columns only with PAR.
+// acc[c * stride] += the two lanes of sums[c] (FP64), sums[c] = 0; the
+// pair-parameter columns only with PAR.
 template <bool PAR>
-__device__ __forceinline__ void fold_sums(f2* sums, double* acc) {
+__device__ __forceinline__ void fold_sums(f2* sums, double* acc, int stride) {
 #pragma unroll
     for (int c = 0; c < 6; c++) {
         if (!PAR && (c == 3 || c == 4)) continue;
         float lo, hi;
         upk(sums[c], lo, hi);
-        acc[c] += (double)lo + (double)hi;
+        acc[c * stride] += (double)lo + (double)hi;
         sums[c] = bc(0.f);
     }
 }
@@ -868,7 +868,10 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
             C.c3 = bc(2.f * p3 * p3 * p2);
             C.c4 = bc(-2.f * p3);
         }
-        double acc[6] = {0, 0, 0, 0, 0, 0};
+        // the atom's FP64 sums, in shared memory (red[c][t]) to keep registers for the pair loop
+        double* acc = &red[0][t];
+#pragma unroll
+        for (int c = 0; c < 6; c++) acc[c * NM_THREADS] = 0.0;
         // the staged nodes' derivative sums: FP32 over NM_FLUSH pairs, then FP64
         auto compute = [&](int L) {
             if (t == 0 && (L & 1)) {  // pad to whole pairs: a distant node of zero weight adds +-0
@@ -896,21 +899,22 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
                         pair_at(jp, a32);
                         pair_at(jp + P, b32);
                         if (++n32 == NM_FLUSH / 2) {
-                            fold_sums<PAR>(a32, acc);
-                            fold_sums<PAR>(b32, acc);
+                            fold_sums<PAR>(a32, acc, NM_THREADS);
+                            fold_sums<PAR>(b32, acc, NM_THREADS);
                             n32 = 0;
                         }
                     }
-                    fold_sums<PAR>(b32, acc);
-                }
-                for (; jp < Lp; jp += P) {
-                    pair_at(jp, a32);
-                    if (++n32 == NM_FLUSH / 2) {
-                        fold_sums<PAR>(a32, acc);
-                        n32 = 0;
+                    fold_sums<PAR>(b32, acc, NM_THREADS);
+                    for (; jp < Lp; jp += P) pair_at(jp, a32);
+                } else {
+                    // blocks of NM_FLUSH / 2 pairs between folds (the last one shorter)
+                    while (jp < Lp) {
+                        const int nb = min(NM_FLUSH / 2, (Lp - jp + P - 1) / P);
+                        for (int k = 0; k < nb; k++, jp += P) pair_at(jp, a32);
+                        if (jp < Lp) fold_sums<PAR>(a32, acc, NM_THREADS);
                     }
                 }
-                fold_sums<PAR>(a32, acc);
+                fold_sums<PAR>(a32, acc, NM_THREADS);
             }
             __syncthreads();  // the buffer is restaged next
         };
@@ -982,7 +986,7 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
             if (!more) break;
         }
 #pragma unroll
-        for (int c = 0; c < 6; c++) red[c][t] = act ? acc[c] : 0.0;
+        for (int c = 0; c < 6; c++) red[c][t] = act ? red[c][t] : 0.0;
         if (KIND == SPM_KIND_LJ && PAR) red[3][t] = -red[3][t];  // accumulated negated
         __syncthreads();
         if (t < nag) {
