@@ -533,7 +533,7 @@ def run_batched(args, dev_index):
     clocks = clk.stop()
     out["forward"] = {
         "workload": f"{args.batch_mols} molecules: U{{10..120}} atoms, grids 12-32 A per side at 0.1 A (slabs "
-                    f"of the reachable z-layers built), 64^2-256^2 px, 30-60 z-steps; grid slabs + relaxation + "
+                    f"of the reachable nodes built), 64^2-256^2 px, 30-60 z-steps; grid slabs + relaxation + "
                     "df in one CUDA graph",
         "ms_per_step": ms, "images_per_s": args.batch_mols / (ms * 1e-3), "states": b.total_states,
         "px_z_per_s": b.total_states / (ms * 1e-3), "slab_gb": b.grid_float4 * 16 / 1e9,
