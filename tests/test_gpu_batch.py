@@ -57,6 +57,30 @@ def test_batch_forward_matches_per_molecule(cuda, kind):
         assert torch.equal(b.df_image(i), df), f"molecule {i}: df differs"
 
 
+def test_batch_slab_box_spanning_an_axis(cuda):
+    """A box that spans an axis keeps that axis' periodic wrap (the x-pair
+    neighbour of the last column is column 0); a box cut to the window on
+    another axis stores only those rows.  Both give the full grid's nodes and
+    relaxation bit for bit."""
+    import dataclasses
+    items = _items(0, n=3, seed=95)
+    it = items[0]
+    cell = it.ngrid[0] * it.step
+    xs = (float(it.origin[0]) + (np.arange(24) + 0.5) * cell / 24).astype(np.float32)  # the whole cell in x
+    items[0] = dataclasses.replace(it, xs=xs, ys=it.ys[:max(2, len(it.ys) // 3)])
+    b = AFMBatch(items)
+    D = b.desc(0)
+    assert (D.x_lo, D.nx_slab) == (0, D.nx) and D.ny_slab < D.ny
+    b.forward()
+    torch.cuda.synchronize()
+    for i in range(len(items)):
+        spec, grid, P, pts, FEs, PPs = _per_molecule(b, i)
+        full = b.slab_of_full(i, grid)
+        assert torch.equal(b.slab(i), full) and torch.equal(b.slab(i, 1), torch.roll(full, -1, dims=2)), i
+        assert torch.equal(b.fes(i), FEs) and torch.equal(b.pps(i), PPs), i
+    assert torch.equal(b.slab(0, 1)[:, :, -1], b.slab(0)[:, :, 0])  # the wrap across the periodic seam
+
+
 def test_batch_relax_matches_oracle(cuda):
     b = AFMBatch(_items(0, n=3, seed=8))
     b.forward()
