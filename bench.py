@@ -343,7 +343,7 @@ def run_ours(args, rank, world, local_rank):
     relax_bytes = cfg.pxz * 32 + slab_nodes * 16
     ach_relax = relax_bytes / (stage[1] * 1e-3) / 1e9
     df_bytes = cfg.pxz * (16 + 4)
-    names = ["grid_build_kernel", "relax_kernel<0>", "df_amp_dir_kernel"]
+    names = ["grid_build_kernel", "relax_tile_kernel<0>", "df_amp_dir_kernel"]
     dom = int(np.argmax(stage))
     if dom == 0:
         roof = {"kernel": names[0], "bound": "fp32", "achieved": ach_fp32 / 1e12, "peak": fp32_peak / 1e12,

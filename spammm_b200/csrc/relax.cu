@@ -7,17 +7,17 @@
 // getFEinStrokesTilted (AFM.cl:210-233, AFMulator.get_raw_FE, AFM.py:2565-2574).
 //
 // The reference launches one work-item per work-group (local size 1).  Here
-// every lane runs one flattened loop over (pixel, z-step, integrator step) with
-// the stroke state (pos, v, dt, damp, tipPos) in registers:
-//   * a lane that converges moves straight on to its next z-step, and -- when
-//     a device-side pixel counter is supplied -- a lane that finishes its pixel
-//     takes the next one (warp-aggregated atomicAdd), so no lane idles while
-//     the slowest lane of its warp or the last CTA wave finishes.  (Warps that
-//     step down the z-steps together, as the batched kernel does, ran 6% slower
-//     on the 480x480-pixel slab scan, whose slowest pixels need up to 3000
-//     FIRE steps per stroke);
-//   * pixels are handed out in 4 (ix) x 8 (iy) tiles, so the eight texel rows
-//     a warp reads per step overlap in L1 and the in-flight set stays local;
+// every lane relaxes whole strokes with the stroke state (pos, v, dt, damp,
+// tipPos) and the eight texels of its current cell in registers:
+//   * with a device-side pixel counter (the workspace of spm_relax_ex), a
+//     persistent warp draws a 4 (ix) x 8 (iy) pixel tile at a time and its
+//     lanes step down the z-steps together (relax_tile_kernel), so the texel
+//     rows they read overlap in L1 and they run the sampling, FIRE and
+//     per-z-step code as one (the flattened per-lane loop below, where lanes
+//     drift to their own pixel, z-step and phase, kept 49% of the lanes of a
+//     warp busy on the 480x480-pixel scan and took 1.65x as long);
+//   * without one, relax_kernel's flattened (pixel, z-step, integrator step)
+//     loop runs one pixel per lane; relaxStrokes2D always uses it;
 //   * node offsets are 32-bit when the grid has fewer than 2^32 nodes.
 // Per-pixel arithmetic is exactly the reference's sequence (spm_fire.cuh), so
 // neither the scheduling nor the flattening changes a result bit.
@@ -300,6 +300,130 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
     }
 }
 
+// MODE 0-2 (relaxStrokes, relaxStrokesTilted, PP) under the z-synchronised
+// tile schedule: a warp draws the 32 pixels of one 4 (ix) x 8 (iy) raster tile
+// (32 consecutive pixels without a raster) from the device counter, and its
+// lanes relax their strokes one z-step at a time, meeting after each (their
+// FIRE loops reconverge there anyway).  Against relax_kernel's flattened loop,
+// where every lane is at its own pixel, z-step and phase and the warp runs the
+// sampling miss path and the per-z-step epilogue for a few lanes at a time
+// (49% of the lanes active per instruction on the 480x480-pixel scan), the
+// lanes of a warp run that code together: 3.81 -> 2.30 ms on that scan.  The
+// per-lane sequence is relax_kernel's (the same iteration, emit and texel
+// cache), so the results are the same bits.
+template <int MODE, typename IDX>
+__global__ void __launch_bounds__(RX_THREADS)
+relax_tile_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
+                  float4* __restrict__ FEs, float4* __restrict__ disps, int* __restrict__ iter_count,
+                  unsigned* __restrict__ counter) {
+    static_assert(MODE >= 0 && MODE <= 2, "relaxStrokes2D keeps the flattened loop");
+    const unsigned lane = threadIdx.x & 31u;
+    const float fnx = (float)G.nx, fny = (float)G.ny, fnz = (float)G.nz;
+    TexelCache T;
+    T.kx = __int_as_float(0x7fc00000);  // NaN matches no cell
+    const bool fire = (P.flags & SPM_FLAG_FIRE) != 0;
+    const bool flip = (P.flags & SPM_FLAG_FLIP_Z) != 0;
+    const int nzs = P.nz, max_iter = P.max_iter;
+    const float4 kk = ld4(P.stiffness), d0 = ld4(P.dpos0);
+    const float4 tc = ld4(P.tipC);
+    const V3 a = mk3(P.tipA[0], P.tipA[1], P.tipA[2]);
+    const V3 b = mk3(P.tipB[0], P.tipB[1], P.tipB[2]);
+    const V3 c = mk3(tc.x, tc.y, tc.z);
+    const float surf = P.surfFF[0];
+    const V3 dTip = (MODE == 0) ? mk3(P.dTip[0], P.dTip[1], P.dTip[2])
+                                : mk3(__fmul_rn(c.x, tc.w), __fmul_rn(c.y, tc.w), __fmul_rn(c.z, tc.w));
+    const V3 d0r = (MODE == 0) ? mk3(d0.x, d0.y, d0.z) : rotmatT(mk3(d0.x, d0.y, d0.z), a, b, c);
+    PPFrame F;
+    if (MODE == 2) F = pp_frame(P);
+    // SPM_FLAG_PAIRED (MODE 0): strokes of the second half go backward
+    const int half = (MODE == 0 && (P.flags & SPM_FLAG_PAIRED)) ? n_scan / 2 : n_scan;
+    const int ny = P.raster_ny;
+    const int nxr = ny > 0 ? n_scan / ny : 0;
+    const unsigned nty = ny > 0 ? (unsigned)(ny + 7) / 8 : 0u;
+    const unsigned nslots = ny > 0 ? ((unsigned)(nxr + 3) / 4) * nty * 32u : ((unsigned)n_scan + 31u) / 32u * 32u;
+    while (true) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(counter, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= nslots) return;  // warp-uniform
+        const unsigned t = base + lane;
+        int k = -1;
+        if (ny > 0) {
+            const unsigned tile = t >> 5, r = t & 31u;
+            const int ix = (int)((tile / nty) * 4 + (r >> 3));
+            const int iy = (int)((tile % nty) * 8 + (r & 7));
+            if (ix < nxr && iy < ny) k = ix * ny + iy;
+        } else if (t < (unsigned)n_scan) {
+            k = (int)t;
+        }
+        const unsigned members = __ballot_sync(0xffffffffu, k >= 0);
+        if (k >= 0) {
+            const float4 p4 = pts[k];
+            const bool bwd = k >= half;
+            const V3 dTipS = bwd ? mk3(-dTip.x, -dTip.y, -dTip.z) : dTip;
+            const bool flipS = flip != bwd;
+            V3 tip = mk3(p4.x, p4.y, p4.z);
+            V3 pos = (MODE == 0) ? mk3(tip.x + d0r.x, tip.y + d0r.y, tip.z + d0r.z) : add3(tip, d0r);
+            Integrator I;
+            I.dt = P.relax_params[0];
+            I.damp = P.relax_params[1];
+            I.dtmax = I.dt;
+            I.dtmin = __fmul_rn(I.dtmax, 0.1f);
+            I.damp0 = I.damp;
+            V3 v = mk3(0.f, 0.f, 0.f);
+            int total_it = 0;
+            for (int iz = 0; iz < nzs; ++iz) {
+                float4 fe = make_float4(0.f, 0.f, 0.f, 0.f);
+                int it = 0;
+                if (MODE == 2) {
+                    bool conv;
+                    while (!pp_iter<IDX, true>(G, F, tip, pos, v, I, fe, it, total_it, conv, T, fnx, fny, fnz)) {
+                    }
+                    const size_t o = (size_t)k * nzs + iz;
+                    pp_emit<IDX>(G, F, pos, fe, it, conv, FEs + o, disps + o);
+                } else {
+                    bool done = max_iter <= 0;
+                    while (!done) {
+                        fe = interp_fe_cached_full<IDX>(G, fnx, fny, fnz, pos, T);
+                        V3 f;
+                        if (MODE == 0) {
+                            const V3 ft = tip_force(sub3(pos, tip), kk, d0);
+                            f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
+                        } else {
+                            const V3 ft = rotmatT(tip_force(rotmat(sub3(pos, tip), a, b, c), kk, d0), a, b, c);
+                            f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
+                            f.x = __fmaf_rn(c.x, surf, f.x);
+                            f.y = __fmaf_rn(c.y, surf, f.y);
+                            f.z = __fmaf_rn(c.z, surf, f.z);
+                        }
+                        md_step(f, v, pos, I, fire);
+                        ++it;
+                        ++total_it;
+                        done = (dot3(f, f) < P.f2conv) || (it >= max_iter);
+                    }
+                    const int oz = flipS ? (nzs - 1 - iz) : iz;
+                    const size_t o = (size_t)k * nzs + oz;
+                    if (MODE == 0) {
+                        FEs[o] = fe;
+                        const V3 ref = mk3(tip.x + d0.x, tip.y + d0.y, tip.z + d0.z);
+                        disps[o] = make_float4(pos.x - ref.x, pos.y - ref.y, pos.z - ref.z, 0.f);
+                    } else {
+                        const float4 g = interp_fe<IDX>(G, pos);
+                        const V3 r = rotmat(mk3(g.x, g.y, g.z), a, b, c);
+                        FEs[o] = make_float4(r.x, r.y, r.z, g.w);
+                    }
+                }
+                tip = add3(tip, dTipS);
+                pos = add3(pos, dTipS);
+                v = mk3(0.f, 0.f, 0.f);
+                __syncwarp(members);  // the tile's lanes start the next z-step together
+            }
+            if (iter_count) iter_count[k] = total_it;
+        }
+        __syncwarp();  // the whole warp draws the next tile
+    }
+}
+
 __global__ void __launch_bounds__(RX_THREADS)
 raw_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P, float4* __restrict__ FEs) {
     const int k = pixel_of_thread(n_scan, P.raster_ny);
@@ -368,6 +492,9 @@ template <int MODE, typename IDX>
 int launch_relax(const GridView& G, const float4* pts, int n_scan, const spm_scan_params& P, float4* FEs,
                  float4* disps, int* iter_count, unsigned* counter, cudaStream_t st) {
     auto kern = relax_kernel<MODE, IDX, (MODE <= 2)>;
+    if constexpr (MODE <= 2) {
+        if (counter) kern = relax_tile_kernel<MODE, IDX>;  // z-synchronised tiles from the counter
+    }
     int blocks = static_blocks(n_scan, P);
     if (counter) {
         // persistent: as many CTAs as are co-resident; the counter balances the rest
