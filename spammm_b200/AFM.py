@@ -363,7 +363,7 @@ class AFMulator:
         disps = disps.reshape(*shape, 4)
         if not return_device:
             FEs = gpu.to_host(FEs)
-            disps = gpu.to_host(disps)
+            disps = gpu.to_host(disps[..., :3].contiguous())  # the fourth channel is 0: not copied
         return FEs, {"dx": disps[..., 0], "dy": disps[..., 1], "dz": disps[..., 2]}
 
     def scan_fdbm_2d(self, scan_xs, scan_ys, probe_heights, mol_z=0.0, K_LAT=0.03, dt=0.3, damp=0.2,
