@@ -907,11 +907,19 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
                     fold_sums<PAR>(b32, acc, NM_THREADS);
                     for (; jp < Lp; jp += P) pair_at(jp, a32);
                 } else {
-                    // blocks of NM_FLUSH / 2 pairs between folds (the last one shorter)
-                    while (jp < Lp) {
-                        const int nb = min(NM_FLUSH / 2, (Lp - jp + P - 1) / P);
-                        for (int k = 0; k < nb; k++, jp += P) pair_at(jp, a32);
-                        if (jp < Lp) fold_sums<PAR>(a32, acc, NM_THREADS);
+                    // blocks of NM_FLUSH / 2 pairs between folds (the last one shorter), walking one
+                    // pointer through the staged arrays (the seven components at fixed offsets from it)
+                    const float* sp = &s_n[0][2 * jp];
+                    const int sstep = 2 * P;
+                    int left = jp < Lp ? (Lp - jp + P - 1) / P : 0;  // pairs of this thread
+                    while (left > 0) {
+                        const int nb = min(NM_FLUSH / 2, left);
+                        for (int k = 0; k < nb; k++, sp += sstep)
+                            pair_adj2<KIND, ON, PAR>(lds2(sp), lds2(sp + NM_BUF), lds2(sp + 2 * NM_BUF),
+                                                     lds2(sp + 3 * NM_BUF), lds2(sp + 4 * NM_BUF),
+                                                     lds2(sp + 5 * NM_BUF), lds2(sp + 6 * NM_BUF), C, S, a32);
+                        left -= nb;
+                        if (left > 0) fold_sums<PAR>(a32, acc, NM_THREADS);
                     }
                 }
                 fold_sums<PAR>(a32, acc, NM_THREADS);
