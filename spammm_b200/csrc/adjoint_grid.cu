@@ -91,6 +91,54 @@ struct Sites {
     float qz[4];
 };
 
+__device__ __forceinline__ float4 add4(float4 p, float4 q) { return make_float4(p.x + q.x, p.y + q.y, p.z + q.z, p.w + q.w); }
+__device__ __forceinline__ float4 sub4(float4 p, float4 q) { return make_float4(p.x - q.x, p.y - q.y, p.z - q.z, p.w - q.w); }
+__device__ __forceinline__ float4 scale4(float4 p, float s) { return make_float4(p.x * s, p.y * s, p.z * s, p.w * s); }
+
+// Two float4 texels from one 32-byte read-only load (p 32-byte aligned).
+__device__ __forceinline__ void ld_texel_pair(const float4* p, float4& lo, float4& hi) {
+    unsigned long long a0, a1, b0, b1;
+    asm("ld.global.nc.v4.b64 {%0, %1, %2, %3}, [%4];" : "=l"(a0), "=l"(a1), "=l"(b0), "=l"(b1) : "l"(p));
+    upk(a0, lo.x, lo.y);
+    upk(a1, lo.z, lo.w);
+    upk(b0, hi.x, hi.y);
+    upk(b1, hi.z, hi.w);
+}
+
+// The eight texels f[k][j][i] of cell C (corner (x_i, y_j, z_k)).  Batch slabs
+// in the x-pair layout (stride 2) hold a node's +x neighbour after it, so each
+// (y, z) row of the cell is one 32-byte load; xz-quads (stride 4) hold the
+// (x, z), (x+1, z), (x, z+1), (x+1, z+1) texels of a node together, two
+// 32-byte loads per y row.  Full grids read the eight texels one by one.
+template <bool SLAB>
+__device__ __forceinline__ void load_cell_texels(const GridView& G, const Corners& C, float4 (&f)[2][2][2]) {
+    if (SLAB && G.stride == 2) {
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const size_t idx = ((size_t)(C.z[k] - G.z_lo) * G.ny_slab + (C.y[j] - G.y_lo)) * G.nx_slab +
+                                   (C.x[0] - G.x_lo);
+                ld_texel_pair(G.g + 2 * idx, f[k][j][0], f[k][j][1]);
+            }
+    } else if (SLAB && G.stride == 4) {
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const size_t idx = ((size_t)(C.z[0] - G.z_lo) * G.ny_slab + (C.y[j] - G.y_lo)) * G.nx_slab +
+                               (C.x[0] - G.x_lo);
+            ld_texel_pair(G.g + 4 * idx, f[0][j][0], f[0][j][1]);
+            ld_texel_pair(G.g + 4 * idx + 2, f[1][j][0], f[1][j][1]);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+#pragma unroll
+            for (int j = 0; j < 2; j++)
+#pragma unroll
+                for (int i = 0; i < 2; i++) f[k][j][i] = node_at<SLAB>(G, C.x[i], C.y[j], C.z[k]);
+    }
+}
+
 // Adjoint of one state: p4 = the stroke's start point, iz = its z-step,
 // pp = stored PP, u = dL/dFEs of the state; writes ubar, dk, diag.
 template <bool SLAB>
@@ -113,38 +161,71 @@ __device__ __forceinline__ void state_adjoint(const GridView& G, const spm_scan_
     const V3 q = mk3(pp.x, pp.y, pp.z);
     const Corners C = corners_of<SLAB>(G, q);
     if (!C.ok) { fail(0.f, 0.f, 0.f, 2.f); return; }
-    // value and texel-coordinate derivatives of the 4 channels
-    float val[4] = {0, 0, 0, 0}, dx[4] = {0, 0, 0, 0}, dy[4] = {0, 0, 0, 0}, dz[4] = {0, 0, 0, 0};
+    // the identity probe frame of z-strokes and axis-aligned grids drop the rotations and the zero
+    // terms of the coordinate derivatives (exact: only the sign of a zero can differ)
+    const bool ident = a.x == 1.f && a.y == 0.f && a.z == 0.f && b.x == 0.f && b.y == 1.f && b.z == 0.f &&
+                       c.x == 0.f && c.y == 0.f && c.z == 1.f;
+    const bool axis = G.dA.y == 0.f && G.dA.z == 0.f && G.dB.x == 0.f && G.dB.z == 0.f && G.dC.x == 0.f &&
+                      G.dC.y == 0.f;
+    // the cell's texels f[k][j][i] (x-pair / xz-quad slabs: one 32-byte load per x-pair)
+    float4 f[2][2][2];
+    load_cell_texels<SLAB>(G, C, f);
     bool capped = false;
+#pragma unroll
     for (int k = 0; k < 2; k++)
+#pragma unroll
         for (int j = 0; j < 2; j++)
-            for (int i = 0; i < 2; i++) {
-                const float4 f = node_at<SLAB>(G, C.x[i], C.y[j], C.z[k]);
-                capped |= fabsf(f.w) >= 99.9999f;
-                const float wx = i ? C.ax : 1.f - C.ax, wy = j ? C.ay : 1.f - C.ay, wz = k ? C.az : 1.f - C.az;
-                const float sx = i ? 1.f : -1.f, sy = j ? 1.f : -1.f, sz = k ? 1.f : -1.f;
-                const float fc[4] = {f.x, f.y, f.z, f.w};
-                for (int ch = 0; ch < 4; ch++) {
-                    val[ch] += wx * wy * wz * fc[ch];
-                    dx[ch] += sx * wy * wz * fc[ch];
-                    dy[ch] += wx * sy * wz * fc[ch];
-                    dz[ch] += wx * wy * sz * fc[ch];
-                }
-            }
+            capped |= fabsf(f[k][j][0].w) >= 99.9999f || fabsf(f[k][j][1].w) >= 99.9999f;
+    // value and texel-coordinate derivatives of the 4 channels, separably: lerps along x, then y,
+    // then z, carrying the differences along the axes already passed
+    const float ax = C.ax, ay = C.ay, az = C.az, mx = 1.f - ax, my = 1.f - ay, mz = 1.f - az;
+    float4 cx[2][2], ex[2][2];
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            cx[k][j] = add4(scale4(f[k][j][0], mx), scale4(f[k][j][1], ax));
+            ex[k][j] = sub4(f[k][j][1], f[k][j][0]);
+        }
+    float4 cy[2], exy[2], ey[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        cy[k] = add4(scale4(cx[k][0], my), scale4(cx[k][1], ay));
+        exy[k] = add4(scale4(ex[k][0], my), scale4(ex[k][1], ay));
+        ey[k] = sub4(cx[k][1], cx[k][0]);
+    }
+    const float4 v4 = add4(scale4(cy[0], mz), scale4(cy[1], az));
+    const float4 dx4 = add4(scale4(exy[0], mz), scale4(exy[1], az));
+    const float4 dy4 = add4(scale4(ey[0], mz), scale4(ey[1], az));
+    const float4 dz4 = sub4(cy[1], cy[0]);
+    const float val[4] = {v4.x, v4.y, v4.z, v4.w}, dx[4] = {dx4.x, dx4.y, dx4.z, dx4.w};
+    const float dy[4] = {dy4.x, dy4.y, dy4.z, dy4.w}, dz[4] = {dz4.x, dz4.y, dz4.z, dz4.w};
     // dt_axis/dq_m = n_axis * dinv_axis[m]
     const float ta[3] = {G.nx * G.dA.x, G.nx * G.dA.y, G.nx * G.dA.z};
     const float tb[3] = {G.ny * G.dB.x, G.ny * G.dB.y, G.ny * G.dB.z};
     const float tc[3] = {G.nz * G.dC.x, G.nz * G.dC.y, G.nz * G.dC.z};
     float Jg[3][3], gE[3];
-    for (int m = 0; m < 3; m++) {
-        for (int ch = 0; ch < 3; ch++) Jg[ch][m] = dx[ch] * ta[m] + dy[ch] * tb[m] + dz[ch] * tc[m];
-        gE[m] = dx[3] * ta[m] + dy[3] * tb[m] + dz[3] * tc[m];
+    if (axis) {
+#pragma unroll
+        for (int ch = 0; ch < 3; ch++) {
+            Jg[ch][0] = dx[ch] * ta[0];
+            Jg[ch][1] = dy[ch] * tb[1];
+            Jg[ch][2] = dz[ch] * tc[2];
+        }
+        gE[0] = dx[3] * ta[0];
+        gE[1] = dy[3] * tb[1];
+        gE[2] = dz[3] * tc[2];
+    } else {
+        for (int m = 0; m < 3; m++) {
+            for (int ch = 0; ch < 3; ch++) Jg[ch][m] = dx[ch] * ta[m] + dy[ch] * tb[m] + dz[ch] * tc[m];
+            gE[m] = dx[3] * ta[m] + dy[3] * tb[m] + dz[3] * tc[m];
+        }
     }
     // tip spring in the tip frame
     const float4 kk = make_float4(P.stiffness[0], P.stiffness[1], P.stiffness[2], P.stiffness[3]);
     const float4 d0 = make_float4(P.dpos0[0], P.dpos0[1], P.dpos0[2], P.dpos0[3]);
-    const V3 dl = rotmat(sub3(q, tip), a, b, c);
-    const V3 ft = rotmatT(tip_force(dl, kk, d0), a, b, c);
+    const V3 dl = ident ? sub3(q, tip) : rotmat(sub3(q, tip), a, b, c);
+    const V3 ft = ident ? tip_force(dl, kk, d0) : rotmatT(tip_force(dl, kk, d0), a, b, c);
     const float surf = P.surfFF[0];
     const V3 Gv = mk3(val[0] + ft.x + c.x * surf, val[1] + ft.y + c.y * surf, val[2] + ft.z + c.z * surf);
     const float resid = sqrtf(Gv.x * Gv.x + Gv.y * Gv.y + Gv.z * Gv.z);
@@ -159,15 +240,22 @@ __device__ __forceinline__ void state_adjoint(const GridView& G, const spm_scan_
                             {beta * dl.z * dl.x, beta * dl.z * dl.y, kk.z + phi + beta * dl.z * dl.z}};
     const float R[3][3] = {{a.x, a.y, a.z}, {b.x, b.y, b.z}, {c.x, c.y, c.z}};
     float J[3][3];
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) {
-            float s = Jg[i][j];
-            for (int m = 0; m < 3; m++)
-                for (int n = 0; n < 3; n++) s += R[m][i] * Jt[m][n] * R[n][j];
-            J[i][j] = s;
-        }
+    if (ident) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) J[i][j] = Jg[i][j] + Jt[i][j];
+    } else {
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                float s = Jg[i][j];
+                for (int m = 0; m < 3; m++)
+                    for (int n = 0; n < 3; n++) s += R[m][i] * Jt[m][n] * R[n][j];
+                J[i][j] = s;
+            }
+    }
     // b = Jg^T R^T u_xyz + gE u_w
-    const V3 uw = rotmatT(mk3(u.x, u.y, u.z), a, b, c);
+    const V3 uw = ident ? mk3(u.x, u.y, u.z) : rotmatT(mk3(u.x, u.y, u.z), a, b, c);
     const float uv[3] = {uw.x, uw.y, uw.z};
     float bv[3];
     for (int m = 0; m < 3; m++) bv[m] = Jg[0][m] * uv[0] + Jg[1][m] * uv[1] + Jg[2][m] * uv[2] + gE[m] * u.w;
@@ -194,20 +282,25 @@ __device__ __forceinline__ void state_adjoint(const GridView& G, const spm_scan_
     const float s01 = -0.5f * (J[0][1] + J[1][0]), s02 = -0.5f * (J[0][2] + J[2][0]), s12 = -0.5f * (J[1][2] + J[2][1]);
     float lmin;
     {
+        // (one reciprocal of p and one sincos: cos(phi + 2pi/3) = -cos(phi)/2 - sin(phi) sqrt(3)/2)
+        const float third = 1.f / 3.f;
         const float p1 = s01 * s01 + s02 * s02 + s12 * s12;
-        const float qm = (s00 + s11 + s22) / 3.f;
+        const float qm = (s00 + s11 + s22) * third;
         const float p2 = (s00 - qm) * (s00 - qm) + (s11 - qm) * (s11 - qm) + (s22 - qm) * (s22 - qm) + 2.f * p1;
-        const float pp2 = sqrtf(p2 / 6.f);
+        const float pp2 = sqrtf(p2 * (1.f / 6.f));
         if (pp2 < 1e-20f) {
             lmin = qm;
         } else {
-            const float b00 = (s00 - qm) / pp2, b11 = (s11 - qm) / pp2, b22 = (s22 - qm) / pp2;
-            const float b01 = s01 / pp2, b02 = s02 / pp2, b12 = s12 / pp2;
+            const float ip = 1.f / pp2;
+            const float b00 = (s00 - qm) * ip, b11 = (s11 - qm) * ip, b22 = (s22 - qm) * ip;
+            const float b01 = s01 * ip, b02 = s02 * ip, b12 = s12 * ip;
             const float detB = b00 * (b11 * b22 - b12 * b12) - b01 * (b01 * b22 - b12 * b02) +
                                b02 * (b01 * b12 - b11 * b02);
-            const float phi3 = acosf(fmaxf(-1.f, fminf(1.f, 0.5f * detB))) / 3.f;
-            const float e1 = qm + 2.f * pp2 * cosf(phi3);
-            const float e3 = qm + 2.f * pp2 * cosf(phi3 + 2.0943951023931953f);
+            const float phi3 = acosf(fmaxf(-1.f, fminf(1.f, 0.5f * detB))) * third;
+            float sn, cs;
+            sincosf(phi3, &sn, &cs);
+            const float e1 = qm + 2.f * pp2 * cs;
+            const float e3 = qm + 2.f * pp2 * (-0.5f * cs - 0.8660254037844386f * sn);
             lmin = fminf(e1, fminf(3.f * qm - e1 - e3, e3));
         }
     }
@@ -221,7 +314,7 @@ __device__ __forceinline__ void state_adjoint(const GridView& G, const spm_scan_
     if (!(cond < 1e6f)) { fail(resid, lmin, cond, 4.f); return; }
     *ubar_o = make_float4(uv[0] - lam[0], uv[1] - lam[1], uv[2] - lam[2], u.w);
     // spring-parameter terms  -lambda . R^T dg/dk   (lambda in the tip frame: R lambda)
-    const V3 lt = rotmat(mk3(lam[0], lam[1], lam[2]), a, b, c);
+    const V3 lt = ident ? mk3(lam[0], lam[1], lam[2]) : rotmat(mk3(lam[0], lam[1], lam[2]), a, b, c);
     const float rw = (r - d0.w) / r;
     *dk_o = make_float4(-lt.x * (dl.x - d0.x), -lt.y * (dl.y - d0.y), -lt.z * (dl.z - d0.z),
                         -(lt.x * dl.x + lt.y * dl.y + lt.z * dl.z) * rw);
@@ -415,9 +508,12 @@ long long n_chunks(long long n_state) { return n_state > 0 ? (n_state + AG_CHUNK
 long long n_rowblocks(long long n_state) { return n_state > 0 ? (n_state + 2047) / 2048 : 1; }
 
 // ---- batched ----------------------------------------------------------------
-// 64 registers (8 CTAs per SM; a few values spilled): the kernel waits on its
-// texel loads, so more resident warps pay (4.7 -> 4.2 ms on the 64-molecule fit).
-__global__ void __launch_bounds__(AG_THREADS, 8)
+// At most 85 registers (72 used, 7 CTAs per SM): the kernel waits on its
+// texel loads, so resident warps pay, but the separable cell arithmetic keeps
+// all eight texels live and spilled at 64 registers (3.41 -> 3.00 ms on the
+// 64-molecule fit; 4.14 ms before the x-pair loads, the separable lerps and the
+// identity-frame path).
+__global__ void __launch_bounds__(AG_THREADS, 6)
 batch_adjoint_state_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states, int stride,
                            const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
                            const float4* __restrict__ PPs, const float4* __restrict__ dL, float4* __restrict__ ubar,
