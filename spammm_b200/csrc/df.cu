@@ -8,9 +8,13 @@
 //   compute_dissipation spammm/SPM/AFM.py:3238-3277
 //   df_loss_seed        spammm/SPM/AFM.py:3125-3200
 // All arithmetic is FP64, as on the reference host.  The FEs volume is
-// (nx,ny,nz,4) float32 with z fastest; these kernels are HBM/L2 bound (a few
-// reads of one float4 per output element), one thread per output element.
-// Compiled with -fmad=false so the FP64 expression order matches NumPy's.
+// (nx,ny,nz,4) float32 with z fastest.  The amplitude df is FP64-arithmetic
+// bound (9 quadrature nodes x 2 interpolations per output): the z-column
+// kernels tabulate each interpolated sample once per column, and the finite
+// differences multiply by 1/dr and 1/(2 dr) instead of dividing (within an
+// FP64 ulp of numpy.gradient's division; the float32 results are unchanged at
+// the reference fixtures' tolerance).  Compiled with -fmad=false so the FP64
+// expression order otherwise matches NumPy's.
 #include "spm_internal.cuh"
 #include "spm_batch.cuh"
 #include <cmath>
@@ -27,6 +31,8 @@ struct DfGeom {
     double n[3];       // oscillation direction (unit)
     double dr[3];      // spacing
     double shift[3];   // amp * n / dr
+    double idr[3];     // 1 / dr and 1 / (2 dr): the one-sided and central differences multiply by them
+    double idr2[3];
     double uk[NQ];     // cos((2k+1) pi / 18)
     double wk;         // 1/9
     int act[3];        // active axes (|n| > 1e-15)
@@ -106,9 +112,9 @@ __device__ double grad_at(const T* __restrict__ FEs, const DfGeom& P, int ax, in
         q[ax] = j;
         return AMP ? shifted_fn(FEs, P, q[0], q[1], q[2], u) : fn_at(FEs, P, q[0], q[1], q[2]);
     };
-    if (i == 0) return (S(1) - S(0)) / P.dr[ax];
-    if (i == n - 1) return (S(n - 1) - S(n - 2)) / P.dr[ax];
-    return (S(i + 1) - S(i - 1)) / (2.0 * P.dr[ax]);
+    if (i == 0) return (S(1) - S(0)) * P.idr[ax];
+    if (i == n - 1) return (S(n - 1) - S(n - 2)) * P.idr[ax];
+    return (S(i + 1) - S(i - 1)) * P.idr2[ax];
 }
 
 template <typename T>
@@ -144,12 +150,27 @@ df_amp_dir_kernel(const T* __restrict__ FEs, DfGeom P, const int* __restrict__ o
 // there and the zero-weight corners are skipped), so results are identical.
 constexpr int DFZ_WARPS = 8;
 constexpr int DFZ_MAXNZ = 512;
+constexpr int DFZ_TAB = 64;  // columns up to this height take each quadrature sample once (a table row)
+
+// acc - wk * (central difference of the tabulated samples at height iz): the
+// per-node step of the amplitude average, the one-sided difference at the
+// column's ends (iz < 0 or >= nz: no output, acc unchanged).
+__device__ __forceinline__ double df_accumulate(double acc, int iz, int nz, const double* row, double idr,
+                                                double idr2, double wkn) {
+    if (iz < 0 || iz >= nz) return acc;
+    double g;
+    if (iz == 0) g = (row[1] - row[0]) * idr;
+    else if (iz == nz - 1) g = (row[nz - 1] - row[nz - 2]) * idr;
+    else g = (row[iz + 1] - row[iz - 1]) * idr2;
+    return acc - wkn * g;
+}
 
 template <typename T>
 __global__ void __launch_bounds__(DFZ_WARPS * 32)
 df_amp_z_kernel(const T* __restrict__ FEs, DfGeom P, const int* __restrict__ out_iz, int n_out,
                 float* __restrict__ df) {
     __shared__ double s_fn[DFZ_WARPS][DFZ_MAXNZ];
+    __shared__ double s_row[DFZ_WARPS][DFZ_TAB];
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     const long long pix = (long long)blockIdx.x * DFZ_WARPS + w;
     if (pix >= (long long)P.nx * P.ny) return;  // whole warp exits together: no CTA barrier below
@@ -160,7 +181,7 @@ df_amp_z_kernel(const T* __restrict__ FEs, DfGeom P, const int* __restrict__ out
         fn[z] = (f.x * P.n[0] + f.y * P.n[1]) + f.z * P.n[2];
     }
     __syncwarp();
-    const double sh = P.shift[2], dr = P.dr[2], nzc = P.n[2];
+    const double sh = P.shift[2], nzc = P.n[2];
     auto S = [&](int j, double u) {
         const double c = (double)j + u * sh;
         const double fl = floor(c);
@@ -172,6 +193,34 @@ df_amp_z_kernel(const T* __restrict__ FEs, DfGeom P, const int* __restrict__ out
         if (w1 != 0.0) acc += fn[clampi(i0 + 1, nz)] * w1;
         return acc;
     };
+    if (nz >= 2 && nz <= DFZ_TAB && n_out <= DFZ_TAB) {
+        // each S(j, u_k) once: per quadrature node the warp tabulates the column's nz samples, then
+        // every output takes its central difference from the table (same values, same order)
+        double* row = s_row[w];
+        int izs[DFZ_TAB / 32];
+        double acc[DFZ_TAB / 32];
+#pragma unroll
+        for (int m = 0; m < DFZ_TAB / 32; m++) {
+            const int o = l + 32 * m;
+            izs[m] = o < n_out ? (out_iz ? out_iz[o] : o) : -1;
+            acc[m] = 0.0;
+        }
+        for (int k = 0; k < NQ; k++) {
+            const double u = P.uk[k];
+            for (int j = l; j < nz; j += 32) row[j] = S(j, u);
+            __syncwarp();
+#pragma unroll
+            for (int m = 0; m < DFZ_TAB / 32; m++) acc[m] = df_accumulate(acc[m], izs[m], nz, row, P.idr[2], P.idr2[2], P.wk * nzc);
+            __syncwarp();  // the row is rewritten for the next node
+        }
+#pragma unroll
+        for (int m = 0; m < DFZ_TAB / 32; m++) {
+            const int o = l + 32 * m;
+            if (o < n_out)
+                df[pix * n_out + o] = (izs[m] < 0 || izs[m] >= nz) ? __int_as_float(0x7fc00000) : (float)acc[m];
+        }
+        return;
+    }
     for (int o = l; o < n_out; o += 32) {
         const int iz = out_iz ? out_iz[o] : o;
         float res;
@@ -182,9 +231,9 @@ df_amp_z_kernel(const T* __restrict__ FEs, DfGeom P, const int* __restrict__ out
             for (int k = 0; k < NQ; k++) {
                 const double u = P.uk[k];
                 double g;
-                if (iz == 0) g = (S(1, u) - S(0, u)) / dr;
-                else if (iz == nz - 1) g = (S(nz - 1, u) - S(nz - 2, u)) / dr;
-                else g = (S(iz + 1, u) - S(iz - 1, u)) / (2.0 * dr);
+                if (iz == 0) g = (S(1, u) - S(0, u)) * P.idr[2];
+                else if (iz == nz - 1) g = (S(nz - 1, u) - S(nz - 2, u)) * P.idr[2];
+                else g = (S(iz + 1, u) - S(iz - 1, u)) * P.idr2[2];
                 acc -= (P.wk * nzc) * g;
             }
             res = (float)acc;
@@ -338,6 +387,8 @@ int fill_geom(DfGeom& P, int nx, int ny, int nz, const double* n, const double* 
         P.n[d] = n[d];
         P.dr[d] = dr[d];
         P.shift[d] = (amp * n[d]) / dr[d];
+        P.idr[d] = 1.0 / dr[d];
+        P.idr2[d] = 1.0 / (2.0 * dr[d]);
         if (fabs(n[d]) > 1e-15) P.act[P.nact++] = d;
     }
     for (int k = 0; k < NQ; k++) P.uk[k] = cos((double)(2 * k + 1) / (double)(2 * NQ) * M_PI);
@@ -495,6 +546,7 @@ __global__ void __launch_bounds__(DFZ_WARPS * 32)
 batch_df_amp_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_pix,
                     const float* __restrict__ FEs, DfGeom P, float* __restrict__ df) {
     __shared__ double s_fn[DFZ_WARPS][DFZ_MAXNZ];
+    __shared__ double s_row[DFZ_WARPS][DFZ_TAB];
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     const long long pix = (long long)blockIdx.x * DFZ_WARPS + w;
     if (pix >= n_pix) return;  // whole warp exits together: no CTA barrier below
@@ -511,7 +563,7 @@ batch_df_amp_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long
         fn[z] = (f.x * P.n[0] + f.y * P.n[1]) + f.z * P.n[2];
     }
     __syncwarp();
-    const double sh = P.shift[2], dr = P.dr[2], nzc = P.n[2];
+    const double sh = P.shift[2], nzc = P.n[2];
     auto S = [&](int j, double u) {
         const double c = (double)j + u * sh;
         const double fl = floor(c);
@@ -523,14 +575,34 @@ batch_df_amp_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long
         if (w1 != 0.0) acc += fn[clampi(i0 + 1, nz)] * w1;
         return acc;
     };
+    if (nz <= DFZ_TAB) {  // each S(j, u_k) once, as df_amp_z_kernel
+        double* row = s_row[w];
+        double acc[DFZ_TAB / 32];
+#pragma unroll
+        for (int m = 0; m < DFZ_TAB / 32; m++) acc[m] = 0.0;
+        for (int k = 0; k < NQ; k++) {
+            const double u = P.uk[k];
+            for (int j = l; j < nz; j += 32) row[j] = S(j, u);
+            __syncwarp();
+#pragma unroll
+            for (int m = 0; m < DFZ_TAB / 32; m++) acc[m] = df_accumulate(acc[m], l + 32 * m, nz, row, P.idr[2], P.idr2[2], P.wk * nzc);
+            __syncwarp();  // the row is rewritten for the next node
+        }
+#pragma unroll
+        for (int m = 0; m < DFZ_TAB / 32; m++) {
+            const int iz = l + 32 * m;
+            if (iz < nz) df[s0 + (nz - 1 - iz)] = (float)acc[m];
+        }
+        return;
+    }
     for (int iz = l; iz < nz; iz += 32) {
         double acc = 0.0;
         for (int k = 0; k < NQ; k++) {
             const double u = P.uk[k];
             double g;
-            if (iz == 0) g = (S(1, u) - S(0, u)) / dr;
-            else if (iz == nz - 1) g = (S(nz - 1, u) - S(nz - 2, u)) / dr;
-            else g = (S(iz + 1, u) - S(iz - 1, u)) / (2.0 * dr);
+            if (iz == 0) g = (S(1, u) - S(0, u)) * P.idr[2];
+            else if (iz == nz - 1) g = (S(nz - 1, u) - S(nz - 2, u)) * P.idr[2];
+            else g = (S(iz + 1, u) - S(iz - 1, u)) * P.idr2[2];
             acc -= (P.wk * nzc) * g;
         }
         df[s0 + (nz - 1 - iz)] = (float)acc;
