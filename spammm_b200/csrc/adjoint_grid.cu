@@ -701,7 +701,7 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
 }
 
 constexpr int NM_THREADS = 256;
-constexpr int NM_PER_THREAD = 4;
+constexpr int NM_PER_THREAD = 2;
 constexpr int NM_STAGE = NM_THREADS * NM_PER_THREAD;  // nodes examined per staging pass
 constexpr int NM_FLUSH = 64;                          // FP32 partial sums folded into FP64 every 64 pairs
 constexpr float LOG2E = 1.4426950408889634f;
@@ -871,21 +871,22 @@ constexpr size_t NM_SMEM = 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(
 // a0 + t % nag and every P-th staged node pair (P = 256 / nag phases), so the
 // atom's derivative sums stay in its registers: no atomics, no cross-thread
 // reduction until the phases are folded once per unit.
-//   * 1024-node passes outside the molecule's box of touched rows and slab
+//   * NM_STAGE-node passes outside the molecule's box of touched rows and slab
 //     layers (box, from the ubar-maximum kernel) are skipped without being read;
 //   * the non-zero nodes of consecutive blocks accumulate in shared memory
 //     until at least NM_STAGE are staged, so every compute phase between two
 //     barriers is dense;
 //   * every non-zero node is zeroed after it is staged (by the last atom
 //     group), so the adjoint grid is left cleared for the next call.
-// Three CTAs per SM (80 registers, a few bytes spilled, 3 x 70 KB of shared
-// memory): the loop is bound by its dependency chains, so the third CTA's
-// warps pay (12.2 -> 10.7 ms on the 64-molecule fit against two CTAs at 128
-// registers).  ILP = 2: two independent node pairs per step at two CTAs per
-// SM (up to 128 registers).  PAR: also the pair-parameter columns 3-4 (else
-// written as 0).
+// Four CTAs per SM (64 registers, a few bytes spilled, 4 x 41 KB of shared
+// memory with 512-node passes): the loop is bound by its dependency chains,
+// so resident warps pay (64-molecule fit: two CTAs at 128 registers 12.2 ms,
+// three at 80 registers 10.7 ms, four at 64 registers 2% less than three;
+// five at 48 registers spill too much).  ILP = 2: two independent node pairs
+// per step at two CTAs per SM (up to 128 registers).  PAR: also the
+// pair-parameter columns 3-4 (else written as 0).
 template <int KIND, bool ON, bool PAR, int ILP>
-__global__ void __launch_bounds__(NM_THREADS, ILP == 2 ? 2 : 3)
+__global__ void __launch_bounds__(NM_THREADS, ILP == 2 ? 2 : 4)
 batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk,
                            const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
                            NodeSites S, unsigned long long* __restrict__ gq, const int* __restrict__ box,
