@@ -371,7 +371,8 @@ typedef struct spm_batch_shape {
     int rx_regs;        /* relaxation kernel variant: 0 = 80 registers per thread, 1 = 64 (more warps,
                            some spills), 2 = the cell's 8 texels kept in registers across FIRE
                            iterations (up to 128 registers, loads only when the cell changes),
-                           3 = the texel cache at 80 registers (some spills, more warps) */
+                           3 = the texel cache at 80 registers (some spills, more warps), 4 = the
+                           texel cache at up to 102 registers in CTAs of at most 128 threads */
     int grid_layout;    /* slab layout: 0 = x-pairs (2 float4 per node), 1 = xz-quads (4 float4 per
                            node: half the cache lines per sample, twice the memory) */
     int rx_sync;        /* relaxation schedule: 0 = every lane draws its next pixel when its stroke ends,

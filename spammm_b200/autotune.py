@@ -6,11 +6,11 @@ Every batched stage reads only its own fields of ``spm_batch_shape``:
   relaxation   rx_sync (z-synchronised warp tiles or independent lanes),
                rx_threads (CTA size), rx_tile_h (pixel tile (32/h) x h per warp
                draw), rx_regs (80 / 64 registers, or the register texel cache
-               at up to 128 or at 80 registers),
+               at up to 128, 80 or 102 registers),
                grid_layout (x-pair or xz-quad slabs: the grid is rebuilt in the
                candidate's layout before the relaxation is timed)
   adjoint      adj_chunk (slab nodes per node-major unit), adj_ilp (node pairs
-               per step of the node kernel: 1 at 3 CTAs per SM, 2 at 2)
+               per step of the node kernel: 1 at 4 CTAs per SM, 2 at 2)
 
 so the stages are tuned one after another, each over its own candidates with
 the others held fixed, by timing the stage's launch with CUDA events on a
@@ -31,7 +31,7 @@ GRID_CANDIDATES = [dict(gb_ty=ty, gb_zb=zb) for ty in (2, 4, 8) for zb in (8, 16
 # z-synchronised warp tiles ran 3x faster than lanes drawing pixels independently on the
 # 64-molecule fit (the CTA size made no difference); one independent-lane shape stays as a check
 RELAX_CANDIDATES = [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=r, grid_layout=g) for g in (0, 1)
-                    for h in (2, 4, 8, 16) for r in (0, 1, 2, 3)] + \
+                    for h in (2, 4, 8, 16) for r in (0, 1, 2, 3, 4)] + \
                    [dict(rx_sync=0, rx_threads=128, rx_tile_h=8, rx_regs=0, grid_layout=0)]
 ADJOINT_CANDIDATES = [dict(adj_chunk=c, adj_ilp=i) for c in (4096, 16384, 65536) for i in (1, 2)]
 

@@ -595,9 +595,10 @@ __device__ __forceinline__ AxisView axis_view(const spm_batch_mol* D, const floa
 // Variants (spm_batch_shape.rx_regs): MINB = 3: up to 80 registers per thread
 // (768 resident threads per SM); MINB = 4: 64 registers (1024 threads, a few
 // spilled values); CACHE: texels kept in registers across iterations (112
-// registers, MINB = 2).
+// registers, MINB = 2); MINB = 5: CTAs of at most 128 threads at up to 102
+// registers (640 threads per SM).
 template <int MINB, bool CACHE, int LAYOUT>
-__global__ void __launch_bounds__(256, MINB)
+__global__ void __launch_bounds__(MINB == 5 ? 128 : 256, MINB)
 batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
                    const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
                    float4* __restrict__ FEs, float4* __restrict__ PPs, int* __restrict__ iter_count,
@@ -718,7 +719,7 @@ __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const 
 }
 
 template <int MINB, bool CACHE, int LAYOUT>
-__global__ void __launch_bounds__(256, MINB)
+__global__ void __launch_bounds__(MINB == 5 ? 128 : 256, MINB)
 batch_relax_sync_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
                         const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
                         float4* __restrict__ FEs, float4* __restrict__ PPs, int* __restrict__ iter_count,
@@ -766,22 +767,26 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     SPM_REQUIRE(shape->rx_ctas_per_sm >= 0, "spm_batch_relax: rx_ctas_per_sm=%d", shape->rx_ctas_per_sm);
     int th_log2 = 0;
     while ((1 << th_log2) < h) th_log2++;
-    SPM_REQUIRE(shape->rx_regs >= 0 && shape->rx_regs <= 3, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
+    SPM_REQUIRE(shape->rx_regs >= 0 && shape->rx_regs <= 4, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
+    SPM_REQUIRE(shape->rx_regs != 4 || thr <= 128, "spm_batch_relax: rx_regs=4 takes CTAs of at most 128 threads, "
+                "rx_threads=%d", thr);
     SPM_REQUIRE(shape->grid_layout == 0 || shape->grid_layout == 1, "spm_batch_relax: grid_layout=%d",
                 shape->grid_layout);
     SPM_REQUIRE(shape->rx_sync == 0 || shape->rx_sync == 1, "spm_batch_relax: rx_sync=%d", shape->rx_sync);
     using Kern = decltype(&batch_relax_kernel<3, false, 2>);
     // [rx_sync][grid_layout][rx_regs]: 0 = 80 registers, 1 = 64, 2 = texel cache at up to 128,
-    // 3 = texel cache squeezed to 80 (some values spilled, 50% more warps)
-    static const Kern table[2][2][4] = {
+    // 3 = texel cache squeezed to 80 (some values spilled, 50% more warps), 4 = texel cache at up to 102
+    // (128-thread CTAs)
+    static const Kern table[2][2][5] = {
         {{batch_relax_kernel<3, false, 2>, batch_relax_kernel<4, false, 2>, batch_relax_kernel<2, true, 2>,
-          batch_relax_kernel<3, true, 2>},
+          batch_relax_kernel<3, true, 2>, batch_relax_kernel<5, true, 2>},
          {batch_relax_kernel<3, false, 4>, batch_relax_kernel<4, false, 4>, batch_relax_kernel<2, true, 4>,
-          batch_relax_kernel<3, true, 4>}},
+          batch_relax_kernel<3, true, 4>, batch_relax_kernel<5, true, 4>}},
         {{batch_relax_sync_kernel<3, false, 2>, batch_relax_sync_kernel<4, false, 2>,
-          batch_relax_sync_kernel<2, true, 2>, batch_relax_sync_kernel<3, true, 2>},
+          batch_relax_sync_kernel<2, true, 2>, batch_relax_sync_kernel<3, true, 2>, batch_relax_sync_kernel<5, true, 2>},
          {batch_relax_sync_kernel<3, false, 4>, batch_relax_sync_kernel<4, false, 4>,
-          batch_relax_sync_kernel<2, true, 4>, batch_relax_sync_kernel<3, true, 4>}}};
+          batch_relax_sync_kernel<2, true, 4>, batch_relax_sync_kernel<3, true, 4>,
+          batch_relax_sync_kernel<5, true, 4>}}};
     const Kern kern = table[shape->rx_sync][shape->grid_layout][shape->rx_regs];
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
