@@ -609,36 +609,25 @@ batch_df_amp_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long
     }
 }
 
-// CTA per 256-state chunk of one molecule: df and the chunk's (w, w*diff^2) sums.
-__global__ void __launch_bounds__(LS_THREADS)
-batch_loss_partials_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float* __restrict__ FEs,
-                           const double* __restrict__ tgt, const double* __restrict__ wts, double dz2,
-                           double* __restrict__ df_out, double* __restrict__ partial) {
-    __shared__ double s_w[LS_THREADS], s_l[LS_THREADS];
-    const long long ch = blockIdx.x;
-    const spm_batch_mol* D = mols + SPM_MOL_BY(chunk_off, mols, n_mol, ch);
-    const int nz = D->nz_steps;
-    const long long nst = (long long)D->n_scan * nz;
-    const long long ls = (ch - D->chunk_off) * LS_THREADS + threadIdx.x;
-    double w = 0.0, l = 0.0;
-    if (ls < nst) {
-        const long long gid = D->state_off + ls;
-        const int iz = ls < (1LL << 32) ? (int)((unsigned)ls % (unsigned)nz) : (int)(ls % nz);  // 32-bit when it fits
-        double d = 0.0;
-        if (iz > 0 && iz < nz - 1) {
-            const double fp = load_row(FEs, gid + 1).z, fm = load_row(FEs, gid - 1).z;
-            d = -(fp - fm) / dz2;
-        }
-        df_out[gid] = d;
-        w = wts ? wts[gid] : ((iz > 0 && iz < nz - 1) ? 1.0 : 0.0);
-        const double diff = d - tgt[gid];
-        l = w * (diff * diff);
-    }
+// Loss chunks per CTA of the partials and gradient kernels.  The first
+// chunk's molecule is found by binary search, the next ones by stepping
+// forward from it, so the search's dependent descriptor loads are paid once
+// per LS_CHUNKS chunks; every chunk is computed and reduced exactly as alone.
+constexpr int LS_CHUNKS = 4;
+
+// Molecule of loss chunk ch, stepping forward from m (the molecule of an earlier chunk).
+__device__ __forceinline__ int step_mol(const spm_batch_mol* __restrict__ mols, int n_mol, int m, long long ch) {
+    while (m + 1 < n_mol && __ldg(&mols[m + 1].chunk_off) <= ch) m++;
+    return m;
+}
+
+// The chunk's single-volume tree (v[t] += v[t+s], s = 128 .. 1) of its threads' (w, l):
+// levels >= 32 through shared memory, the last five in warp 0 by shuffles -- the same
+// additions in the same order.  Ends with a barrier, so s_w / s_l can be reused.
+__device__ __forceinline__ void chunk_partials(double w, double l, double* s_w, double* s_l, double* out) {
     s_w[threadIdx.x] = w;
     s_l[threadIdx.x] = l;
     __syncthreads();
-    // the single-volume tree (v[t] += v[t+s], s = 128 .. 1): levels >= 32 through shared
-    // memory, the last five in warp 0 by shuffles -- the same additions in the same order
     for (int s = LS_THREADS / 2; s >= 32; s >>= 1) {
         if (threadIdx.x < s) {
             s_w[threadIdx.x] += s_w[threadIdx.x + s];
@@ -654,10 +643,52 @@ batch_loss_partials_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, co
             vl += __shfl_down_sync(0xffffffffu, vl, s);
         }
         if (threadIdx.x == 0) {
-            partial[2 * ch] = vw;
-            partial[2 * ch + 1] = vl;
+            out[0] = vw;
+            out[1] = vl;
         }
     }
+    __syncthreads();
+}
+
+// LS_CHUNKS consecutive 256-state chunks per CTA: df and each chunk's (w, w*diff^2) sums.
+__global__ void __launch_bounds__(LS_THREADS)
+batch_loss_partials_kernel(int n_mol, long long n_chunks, const spm_batch_mol* __restrict__ mols,
+                           const float* __restrict__ FEs, const double* __restrict__ tgt,
+                           const double* __restrict__ wts, double dz2, double* __restrict__ df_out,
+                           double* __restrict__ partial) {
+    __shared__ double s_w[LS_THREADS], s_l[LS_THREADS];
+    const long long c0 = (long long)blockIdx.x * LS_CHUNKS;
+    int m = SPM_MOL_BY(chunk_off, mols, n_mol, c0);
+    // every state's terms first (independent loads of all chunks in flight), then the reductions
+    double wv[LS_CHUNKS], lv[LS_CHUNKS];
+#pragma unroll
+    for (int k = 0; k < LS_CHUNKS; k++) {
+        const long long ch = c0 + k;
+        wv[k] = 0.0;
+        lv[k] = 0.0;
+        if (ch >= n_chunks) continue;
+        m = step_mol(mols, n_mol, m, ch);
+        const spm_batch_mol* D = mols + m;
+        const int nz = D->nz_steps;
+        const long long nst = (long long)D->n_scan * nz;
+        const long long ls = (ch - D->chunk_off) * LS_THREADS + threadIdx.x;
+        if (ls < nst) {
+            const long long gid = D->state_off + ls;
+            const int iz = ls < (1LL << 32) ? (int)((unsigned)ls % (unsigned)nz) : (int)(ls % nz);  // 32-bit when it fits
+            double d = 0.0;
+            if (iz > 0 && iz < nz - 1) {
+                const double fp = load_row(FEs, gid + 1).z, fm = load_row(FEs, gid - 1).z;
+                d = -(fp - fm) / dz2;
+            }
+            df_out[gid] = d;
+            wv[k] = wts ? wts[gid] : ((iz > 0 && iz < nz - 1) ? 1.0 : 0.0);
+            const double diff = d - tgt[gid];
+            lv[k] = wv[k] * (diff * diff);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < LS_CHUNKS; k++)
+        if (c0 + k < n_chunks) chunk_partials(wv[k], lv[k], s_w, s_l, partial + 2 * (c0 + k));  // uniform over the CTA
 }
 
 // CTA per molecule: fold its chunk partials in the fixed single-volume order.
@@ -695,36 +726,40 @@ batch_loss_final_kernel(const spm_batch_mol* __restrict__ mols, const double* __
 }
 
 __global__ void __launch_bounds__(LS_THREADS)
-batch_loss_grad_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const double* __restrict__ df,
-                       const double* __restrict__ tgt, const double* __restrict__ wts, const double* __restrict__ sums,
-                       double coeff, float4* __restrict__ dL) {
-    const long long ch = blockIdx.x;
-    const int m = SPM_MOL_BY(chunk_off, mols, n_mol, ch);
-    const spm_batch_mol* D = mols + m;
-    const int nz = D->nz_steps;
-    const long long nst = (long long)D->n_scan * nz;
-    const long long ls = (ch - D->chunk_off) * LS_THREADS + threadIdx.x;
-    if (ls >= nst) return;
-    const long long gid = D->state_off + ls;
-    const int iz = ls < (1LL << 32) ? (int)((unsigned)ls % (unsigned)nz) : (int)(ls % nz);  // 32-bit when it fits
-    if (nz < 3) {  // no central difference: no gradient (and the stencil would leave the stroke)
-        dL[gid] = make_float4(0.f, 0.f, 0.f, 0.f);
-        return;
+batch_loss_grad_kernel(int n_mol, long long n_chunks, const spm_batch_mol* __restrict__ mols,
+                       const double* __restrict__ df, const double* __restrict__ tgt, const double* __restrict__ wts,
+                       const double* __restrict__ sums, double coeff, float4* __restrict__ dL) {
+    const long long c0 = (long long)blockIdx.x * LS_CHUNKS;
+    int m = SPM_MOL_BY(chunk_off, mols, n_mol, c0);
+#pragma unroll
+    for (int k = 0; k < LS_CHUNKS; k++) {
+        const long long ch = c0 + k;
+        if (ch >= n_chunks) return;
+        m = step_mol(mols, n_mol, m, ch);
+        const spm_batch_mol* D = mols + m;
+        const int nz = D->nz_steps;
+        const long long nst = (long long)D->n_scan * nz;
+        const long long ls = (ch - D->chunk_off) * LS_THREADS + threadIdx.x;
+        if (ls >= nst) continue;
+        const long long gid = D->state_off + ls;
+        const int iz = ls < (1LL << 32) ? (int)((unsigned)ls % (unsigned)nz) : (int)(ls % nz);  // 32-bit when it fits
+        const double wsum = sums[2 * m];
+        // no central difference (nz < 3: the stencil would leave the stroke) or zero total
+        // weight (no loss): no gradient
+        if (nz < 3 || !(wsum > 0.0)) {
+            dL[gid] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        auto g = [&](long long j, int jz) {  // jz: the z-step of state j
+            const double w = wts ? wts[j] : ((jz > 0 && jz < nz - 1) ? 1.0 : 0.0);
+            return w * (df[j] - tgt[j]) / wsum;
+        };
+        double v;
+        if (iz == 0) v = g(gid + 1, 1) * coeff;
+        else if (iz == nz - 1) v = -g(gid - 1, iz - 1) * coeff;
+        else v = (g(gid + 1, iz + 1) - g(gid - 1, iz - 1)) * coeff;
+        dL[gid] = make_float4(0.f, 0.f, (float)v, 0.f);
     }
-    const double wsum = sums[2 * m];
-    if (!(wsum > 0.0)) {  // zero total weight: no loss, no gradient
-        dL[gid] = make_float4(0.f, 0.f, 0.f, 0.f);
-        return;
-    }
-    auto g = [&](long long j, int jz) {  // jz: the z-step of state j
-        const double w = wts ? wts[j] : ((jz > 0 && jz < nz - 1) ? 1.0 : 0.0);
-        return w * (df[j] - tgt[j]) / wsum;
-    };
-    double v;
-    if (iz == 0) v = g(gid + 1, 1) * coeff;
-    else if (iz == nz - 1) v = -g(gid - 1, iz - 1) * coeff;
-    else v = (g(gid + 1, iz + 1) - g(gid - 1, iz - 1)) * coeff;
-    dL[gid] = make_float4(0.f, 0.f, (float)v, 0.f);
 }
 
 }  // namespace
@@ -802,14 +837,14 @@ extern "C" int spm_batch_df_loss_seed(int n_mol, const spm_batch_mol* mols, long
     double* sums = partial + 2 * n_chunks;
     const double dz = fabs(dtip);
     cudaStream_t st = as_stream(stream);
+    const unsigned nblk = (unsigned)((n_chunks + LS_CHUNKS - 1) / LS_CHUNKS);
     if (n_chunks > 0)
-        batch_loss_partials_kernel<<<(unsigned)n_chunks, LS_THREADS, 0, st>>>(n_mol, mols, FEs, target, weights,
-                                                                              2.0 * dz, df_out, partial);
+        batch_loss_partials_kernel<<<nblk, LS_THREADS, 0, st>>>(n_mol, n_chunks, mols, FEs, target, weights, 2.0 * dz,
+                                                                df_out, partial);
     batch_loss_final_kernel<<<(unsigned)n_mol, LS_THREADS, 0, st>>>(mols, partial, sums, loss_out);
     if (n_chunks > 0)
-        batch_loss_grad_kernel<<<(unsigned)n_chunks, LS_THREADS, 0, st>>>(n_mol, mols, df_out, target, weights, sums,
-                                                                          1.0 / (2.0 * dz),
-                                                                          reinterpret_cast<float4*>(dL_dFEs));
+        batch_loss_grad_kernel<<<nblk, LS_THREADS, 0, st>>>(n_mol, n_chunks, mols, df_out, target, weights, sums,
+                                                            1.0 / (2.0 * dz), reinterpret_cast<float4*>(dL_dFEs));
     return check_launch("spm_batch_df_loss_seed");
 }
 
