@@ -560,65 +560,86 @@ adj_clear_kernel(ulonglong2* __restrict__ gq, long long n2, const unsigned long 
         gq[i] = make_ulonglong2(0ull, 0ull);
 }
 
-// CTA per 256-state chunk (one molecule): per-molecule max |ubar| (as float
-// bits; order-free) and the bounding box of the slab rows and layers the
+// UM_CHUNKS consecutive 256-state chunks per CTA: per-molecule max |ubar| (as
+// float bits; order-free) and the bounding box of the slab rows and layers the
 // scatter will touch, box[4m..4m+3] = max of (ny_slab-1-yl, yl+1,
 // nz_slab-1-zl, zl+1) over the cell corners of every state with a non-zero
-// ubar (all zero: none); yl, zl are slab rows and layers.
+// ubar (all zero: none); yl, zl are slab rows and layers.  The CTA searches
+// the first chunk's molecule once and steps to the next ones; its maxima are
+// flushed to the molecule's atomics whenever the molecule changes.
 // Block 0 marks the adjoint grid dirty (the scatter follows).
+constexpr int UM_CHUNKS = 4;
+
 __global__ void __launch_bounds__(256)
-batch_ubar_max_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float4* __restrict__ ubar,
-                      const float4* __restrict__ PPs, unsigned* __restrict__ umax, int* __restrict__ box,
-                      unsigned long long* __restrict__ mark) {
+batch_ubar_max_kernel(int n_mol, long long n_chunks, const spm_batch_mol* __restrict__ mols,
+                      const float4* __restrict__ ubar, const float4* __restrict__ PPs, unsigned* __restrict__ umax,
+                      int* __restrict__ box, unsigned long long* __restrict__ mark) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *mark = ADJ_DIRTY;
     __shared__ float s_m[8];
     __shared__ int s_b[4][8];
-    const long long ch = blockIdx.x;
-    const int m = SPM_MOL_BY(chunk_off, mols, n_mol, ch);
-    const spm_batch_mol* D = mols + m;
-    const long long nst = (long long)D->n_scan * D->nz_steps;
-    const long long ls = (ch - D->chunk_off) * 256 + threadIdx.x;
     float v = 0.f;
     int b[4] = {0, 0, 0, 0};
-    if (ls < nst) {
-        const float4 u = __ldg(ubar + D->state_off + ls);
-        v = fmaxf(fmaxf(fabsf(u.x), fabsf(u.y)), fmaxf(fabsf(u.z), fabsf(u.w)));
-        if (!(u.x == 0.f && u.y == 0.f && u.z == 0.f && u.w == 0.f)) {  // the scatter's test
-            const GridView G = slab_view(*D, nullptr);
-            const float4 pp = __ldg(PPs + D->state_off + ls);
-            const Corners C = corners_of<true>(G, mk3(pp.x, pp.y, pp.z));
-            if (C.ok) {
+    // CTA-uniform: the block's maxima of molecule m into its atomics; v and b restart at zero
+    auto flush = [&](int m) {
+        for (int o = 16; o > 0; o >>= 1) {
+            v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
 #pragma unroll
-                for (int k = 0; k < 2; k++) {
-                    b[0] = max(b[0], G.ny_slab - 1 - (C.y[k] - G.y_lo));
-                    b[1] = max(b[1], C.y[k] - G.y_lo + 1);
-                    b[2] = max(b[2], G.nz_slab - 1 - (C.z[k] - G.z_lo));
-                    b[3] = max(b[3], C.z[k] - G.z_lo + 1);
+            for (int k = 0; k < 4; k++) b[k] = max(b[k], __shfl_xor_sync(0xffffffffu, b[k], o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            s_m[threadIdx.x >> 5] = v;
+#pragma unroll
+            for (int k = 0; k < 4; k++) s_b[k][threadIdx.x >> 5] = b[k];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float w = s_m[0];
+            for (int k = 1; k < 8; k++) w = fmaxf(w, s_m[k]);
+            if (w > 0.f) atomicMax(umax + m, __float_as_uint(w));
+        }
+        if (threadIdx.x < 4) {
+            int w = s_b[threadIdx.x][0];
+            for (int k = 1; k < 8; k++) w = max(w, s_b[threadIdx.x][k]);
+            if (w > 0) atomicMax(box + 4 * m + threadIdx.x, w);
+        }
+        __syncthreads();
+        v = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; k++) b[k] = 0;
+    };
+    const long long c0 = (long long)blockIdx.x * UM_CHUNKS;
+    int m = SPM_MOL_BY(chunk_off, mols, n_mol, c0);
+    for (int q = 0; q < UM_CHUNKS; q++) {
+        const long long ch = c0 + q;
+        if (ch >= n_chunks) break;
+        const int mq = SPM_MOL_STEP(chunk_off, mols, n_mol, m, ch);
+        if (mq != m) {
+            flush(m);
+            m = mq;
+        }
+        const spm_batch_mol* D = mols + m;
+        const long long nst = (long long)D->n_scan * D->nz_steps;
+        const long long ls = (ch - D->chunk_off) * 256 + threadIdx.x;
+        if (ls < nst) {
+            const float4 u = __ldg(ubar + D->state_off + ls);
+            v = fmaxf(v, fmaxf(fmaxf(fabsf(u.x), fabsf(u.y)), fmaxf(fabsf(u.z), fabsf(u.w))));
+            if (!(u.x == 0.f && u.y == 0.f && u.z == 0.f && u.w == 0.f)) {  // the scatter's test
+                const GridView G = slab_view(*D, nullptr);
+                const float4 pp = __ldg(PPs + D->state_off + ls);
+                const Corners C = corners_of<true>(G, mk3(pp.x, pp.y, pp.z));
+                if (C.ok) {
+#pragma unroll
+                    for (int k = 0; k < 2; k++) {
+                        b[0] = max(b[0], G.ny_slab - 1 - (C.y[k] - G.y_lo));
+                        b[1] = max(b[1], C.y[k] - G.y_lo + 1);
+                        b[2] = max(b[2], G.nz_slab - 1 - (C.z[k] - G.z_lo));
+                        b[3] = max(b[3], C.z[k] - G.z_lo + 1);
+                    }
                 }
             }
         }
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-#pragma unroll
-        for (int k = 0; k < 4; k++) b[k] = max(b[k], __shfl_xor_sync(0xffffffffu, b[k], o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-        s_m[threadIdx.x >> 5] = v;
-#pragma unroll
-        for (int k = 0; k < 4; k++) s_b[k][threadIdx.x >> 5] = b[k];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float w = s_m[0];
-        for (int k = 1; k < 8; k++) w = fmaxf(w, s_m[k]);
-        if (w > 0.f) atomicMax(umax + m, __float_as_uint(w));
-    }
-    if (threadIdx.x < 4) {
-        int w = s_b[threadIdx.x][0];
-        for (int k = 1; k < 8; k++) w = max(w, s_b[threadIdx.x][k]);
-        if (w > 0) atomicMax(box + 4 * m + threadIdx.x, w);
-    }
+    flush(m);
 }
 
 // Thread per state: w * ubar onto the eight corner nodes (exact integer sums).
@@ -1255,9 +1276,9 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             if (cudaMemsetAsync(umax, 0, (size_t)(SL.mark - SL.umax), st) != cudaSuccess)  // maxima + boxes
                 return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: memset failed");
             adj_clear_kernel<<<1184, 256, 0, st>>>(reinterpret_cast<ulonglong2*>(gq), totals[7] * 2, mark);
-            batch_ubar_max_kernel<<<(unsigned)n_chunks, 256, 0, st>>>(n_mol, mols, reinterpret_cast<const float4*>(ubar),
-                                                                      reinterpret_cast<const float4*>(PPs), umax, box,
-                                                                      mark);
+            batch_ubar_max_kernel<<<(unsigned)((n_chunks + UM_CHUNKS - 1) / UM_CHUNKS), 256, 0, st>>>(
+                n_mol, n_chunks, mols, reinterpret_cast<const float4*>(ubar), reinterpret_cast<const float4*>(PPs), umax,
+                box, mark);
             batch_scatter_kernel<<<(unsigned)((n_states + 255) / 256), 256, 0, st>>>(
                 n_mol, mols, n_states, reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar), umax,
                 gq);

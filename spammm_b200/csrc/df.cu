@@ -615,12 +615,6 @@ batch_df_amp_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long
 // per LS_CHUNKS chunks; every chunk is computed and reduced exactly as alone.
 constexpr int LS_CHUNKS = 4;
 
-// Molecule of loss chunk ch, stepping forward from m (the molecule of an earlier chunk).
-__device__ __forceinline__ int step_mol(const spm_batch_mol* __restrict__ mols, int n_mol, int m, long long ch) {
-    while (m + 1 < n_mol && __ldg(&mols[m + 1].chunk_off) <= ch) m++;
-    return m;
-}
-
 // The chunk's single-volume tree (v[t] += v[t+s], s = 128 .. 1) of its threads' (w, l):
 // levels >= 32 through shared memory, the last five in warp 0 by shuffles -- the same
 // additions in the same order.  Ends with a barrier, so s_w / s_l can be reused.
@@ -667,7 +661,7 @@ batch_loss_partials_kernel(int n_mol, long long n_chunks, const spm_batch_mol* _
         wv[k] = 0.0;
         lv[k] = 0.0;
         if (ch >= n_chunks) continue;
-        m = step_mol(mols, n_mol, m, ch);
+        m = SPM_MOL_STEP(chunk_off, mols, n_mol, m, ch);
         const spm_batch_mol* D = mols + m;
         const int nz = D->nz_steps;
         const long long nst = (long long)D->n_scan * nz;
@@ -735,7 +729,7 @@ batch_loss_grad_kernel(int n_mol, long long n_chunks, const spm_batch_mol* __res
     for (int k = 0; k < LS_CHUNKS; k++) {
         const long long ch = c0 + k;
         if (ch >= n_chunks) return;
-        m = step_mol(mols, n_mol, m, ch);
+        m = SPM_MOL_STEP(chunk_off, mols, n_mol, m, ch);
         const spm_batch_mol* D = mols + m;
         const int nz = D->nz_steps;
         const long long nst = (long long)D->n_scan * nz;

@@ -24,6 +24,17 @@ __device__ __forceinline__ int find_mol(const spm_batch_mol* __restrict__ mols, 
 
 #define SPM_MOL_BY(field, mols, n, x) find_mol<decltype(spm_batch_mol::field), &spm_batch_mol::field>(mols, n, x)
 
+// The molecule of item x, stepping forward from m, the molecule of an item <= x
+// (a CTA that takes several consecutive items searches once, then steps).
+template <typename T, T spm_batch_mol::*F>
+__device__ __forceinline__ int step_mol(const spm_batch_mol* __restrict__ mols, int n_mol, int m, long long x) {
+    while (m + 1 < n_mol && (long long)__ldg(&(mols[m + 1].*F)) <= x) m++;
+    return m;
+}
+
+#define SPM_MOL_STEP(field, mols, n, m, x) \
+    step_mol<decltype(spm_batch_mol::field), &spm_batch_mol::field>(mols, n, m, x)
+
 __device__ __forceinline__ float4 ld4f(const float* a) { return make_float4(__ldg(a), __ldg(a + 1), __ldg(a + 2), __ldg(a + 3)); }
 
 // Pixel k of relaxation slot lt (slot index within molecule D).  With a
