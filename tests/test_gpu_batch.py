@@ -229,6 +229,29 @@ def test_batch_with_empty_scan(cuda):
     assert float(b.loss_of(1)) == 0.0 and not b.grad_of(1).any()
 
 
+def test_batch_of_single_chunk_molecules(cuda):
+    """Molecules of at most one 256-state loss chunk each, so one CTA of the
+    loss and ubar-maxima kernels spans several molecules: every molecule's
+    loss equals its batch-of-one loss bit for bit, its gradient to rounding."""
+    items = synthetic.batch_molecules(11, seed=61, natoms=(6, 14), side=(5, 7), zside=(8, 10), npx=(2, 4),
+                                      nzs=(8, 12))
+    assert all(it.n_scan * it.nz <= 256 for it in items)
+    rng = np.random.default_rng(8)
+    tg = [rng.normal(0.0, 0.05, (len(it.xs), len(it.ys), it.nz)) for it in items]
+    b = AFMBatch(items)
+    for i in range(len(items)):
+        b.set_target(i, tg[i])
+    b.forward_adjoint()
+    for i, it in enumerate(items):
+        one = AFMBatch([it])
+        one.set_target(0, tg[i])
+        one.forward_adjoint()
+        torch.cuda.synchronize()
+        assert torch.equal(b.loss_of(i), one.loss_of(0)), i
+        torch.testing.assert_close(b.grad_of(i), one.grad_of(0), rtol=1e-5,
+                                   atol=1e-6 * float(one.grad.abs().max()))
+
+
 @pytest.mark.parametrize("kind", [0, 1])
 def test_adjoint_scratch_reuse_and_garbage(cuda, kind):
     """The node kernel leaves the adjoint grid cleared for the next call; a
