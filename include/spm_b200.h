@@ -195,12 +195,6 @@ int spm_convolve_z(const float* Fin, int n_col, int nz_in, int nz_out, const flo
  * float32, zMap (n_col) float32. */
 int spm_izo_z(const float* Fin, int n_col, int nz, float iso, float* zMap, void* stream);
 
-/* Replaces df_loss_seed (spammm/SPM/AFM.py:3125-3200): central-difference df of
- * Fz = FEs[...,2] with |dtip|, L = 0.5*sum(w (df - target)^2)/sum(w) and the
- * exact transpose dL/dFEs (only the z channel non-zero).  target, weights
- * (nx,ny,nz) float64 (weights NULL = 1 inside, 0 on the two boundary slices);
- * df_out (nx,ny,nz) f64, dL_dFEs (nx,ny,nz,4) f32, loss_out: device double[1].
- * Uses `scratch` (device, >= spm_df_loss_scratch_bytes(nx,ny,nz) bytes). */
 /* spm_df_loss_seed for callers that cannot allocate device memory around the
  * call (their allocator owns all device memory, or a cudaMalloc/cudaFree and
  * its implicit synchronisation is not allowed in their loop).  No counterpart
@@ -215,12 +209,22 @@ int spm_izo_z(const float* Fin, int n_col, int nz, float iso, float* zMap, void*
  *     (e.g. on two streams at once) race and give wrong results; serialise them;
  *   - every slot a call reads is written earlier by the same call, so no state
  *     carries over from the previous call;
+ *   - the device address found by that first call is kept for the life of
+ *     the process: after cudaDeviceReset (or anything else that destroys the
+ *     device's primary context) the kept address is stale; do not call this
+ *     entry point on that device again in the same process;
  *   - allocates nothing (no cudaMalloc/cudaFree or allocating library call). */
 #define SPM_DF_LOSS_NOALLOC_MAX_ELEMS 16777216LL
 int spm_df_loss_seed_noalloc(const void* FEs, int fes_dtype, const double* target, const double* weights,
                              int nx, int ny, int nz, double dtip, double* df_out, float* dL_dFEs,
                              double* loss_out, void* stream);
 
+/* Replaces df_loss_seed (spammm/SPM/AFM.py:3125-3200): central-difference df of
+ * Fz = FEs[...,2] with |dtip|, L = 0.5*sum(w (df - target)^2)/sum(w) and the
+ * exact transpose dL/dFEs (only the z channel non-zero).  target, weights
+ * (nx,ny,nz) float64 (weights NULL = 1 inside, 0 on the two boundary slices);
+ * df_out (nx,ny,nz) f64, dL_dFEs (nx,ny,nz,4) f32, loss_out: device double[1].
+ * Uses `scratch` (device, >= spm_df_loss_scratch_bytes(nx,ny,nz) bytes). */
 int spm_df_loss_seed(const void* FEs, int fes_dtype, const double* target, const double* weights,
                      int nx, int ny, int nz, double dtip, double* df_out, float* dL_dFEs,
                      double* loss_out, void* scratch, void* stream);

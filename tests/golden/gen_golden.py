@@ -1,8 +1,9 @@
 """Generates tests/golden/*.npz from the SPAMMM reference's own Python code.
 
-Run in a checkout that has the reference tree (default /root/reference):
+Run where the reference tree is available, giving its root with --ref or
+the SPAMMM_REF environment variable:
 
-    python tests/golden/gen_golden.py [--ref PATH]
+    python tests/golden/gen_golden.py --ref PATH
 
 The reference imports pyopencl and matplotlib at module level; only its CPU
 (NumPy/SciPy) functions are called here, so both are replaced by inert stub
@@ -83,8 +84,11 @@ def _trilin_periodic(grid, dinv, p):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("SPAMMM_REF"),
+                    help="root of the SPAMMM reference tree (default: $SPAMMM_REF)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference tree with --ref PATH or SPAMMM_REF")
     _install_stubs()
     sys.path.insert(0, args.ref)
     from spammm.SPM import AFM as A
