@@ -52,6 +52,14 @@ enum spm_status {
                                  opposite to the forward ones (SPM_FLAG_FLIP_Z inverted): the forward
                                  and reverse=True scans of AFMulator.scan_fdbm (AFM.py:584-633) in one
                                  launch; n_scan even */
+#define SPM_FLAG_POLISH 8     /* relaxations (not SPM_RELAX_2D): after FIRE stops, up to 4 Newton steps
+                                 q <- q - J^-1 G on the total force G(q) of the interpolated grid and the
+                                 spring (J = dG/dq, exact for the trilinear interpolant), each kept only
+                                 if it moves q by at most 0.1 A per axis and lowers |G|; outputs (FE,
+                                 disp / PP) are then taken at the polished position, the sample there.
+                                 The FIRE trajectory is unchanged (the next z-step starts from the
+                                 unpolished position).  Not in the reference: it removes FIRE's stopping
+                                 slack (~|F|/k_xy) from the equilibria */
 
 /* Scan/tip parameters shared by the relaxation and sampling kernels.  Field
  * names follow the reference's kernel arguments (kernels/AFM.cl:345-562). */

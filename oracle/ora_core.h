@@ -158,13 +158,175 @@ typedef struct {
     REAL dA[4], dB[4], dC[4];
 } SFX(gridref);
 
+/* ---- Newton polish (opt-in SPM_FLAG_POLISH; not in the reference) ----------
+ * After FIRE stops, up to POLISH_STEPS Newton steps q <- q - J^-1 G on the
+ * total force G(q) = F_grid(q) + spring(q) [+ c*surf], F_grid the trilinear
+ * sample of the force channels and J = dG/dq exact for that interpolant (its
+ * texel-coordinate derivatives times n*dinv, plus the spring's Jacobian); a
+ * step is kept only if it moves q by at most POLISH_MAX_STEP per axis and
+ * lowers |G|^2.  Same operations in the same order as the CUDA kernels
+ * (spm_fire.cuh: polish_eval / polish_step / newton_polish), so the FP32
+ * instantiation is bit-identical to them.  frame=0: relaxStrokes' spring
+ * (tip_force on q - tip); frame=1: tip frame a,b,c with surf along c. */
+#define POLISH_STEPS 4
+#define POLISH_MAX_STEP 0.1
+
+typedef struct {
+    SFX(v3) a, b, c;
+    REAL k[4], d0[4];
+    REAL surf;
+    int frame;
+} SFX(pspring);
+
+/* fetch the cell of q: texels t[4*k+2*j+i] (corner x_i,y_j,z_k) and weights */
+static inline int SFX(polish_fetch)(const GRID_T* g, const SFX(gridref)* G, SFX(v3) p, REAL t[8][4],
+                                    REAL* ax, REAL* ay, REAL* az) {
+    REAL u = FMA(p.x, G->dA[0], FMA(p.y, G->dA[1], FMA(p.z, G->dA[2], G->dA[3])));
+    REAL v = FMA(p.x, G->dB[0], FMA(p.y, G->dB[1], FMA(p.z, G->dB[2], G->dB[3])));
+    REAL w = FMA(p.x, G->dC[0], FMA(p.y, G->dC[1], FMA(p.z, G->dC[2], G->dC[3])));
+    int x[2] = {0, 0}, y[2] = {0, 0}, z[2] = {0, 0};
+    int ok = SFX(tex_axis)(u, G->nx, &x[0], &x[1], ax);
+    ok = SFX(tex_axis)(v, G->ny, &y[0], &y[1], ay) && ok;
+    ok = SFX(tex_axis)(w, G->nz, &z[0], &z[1], az) && ok;
+    if (!ok) return 0;
+    for (int k = 0; k < 2; k++)
+        for (int j = 0; j < 2; j++)
+            for (int i = 0; i < 2; i++) {
+                const GRID_T* f = g + (((size_t)z[k] * G->ny + y[j]) * G->nx + x[i]) * 4;
+                for (int c = 0; c < 4; c++) t[4 * k + 2 * j + i][c] = (REAL)f[c];
+            }
+    return 1;
+}
+
+static inline REAL SFX(lerp_c)(REAL a, REAL ma, REAL f0, REAL f1) { return FMA(a, f1, ma * f0); }
+
+static void SFX(polish_eval)(REAL t[8][4], REAL ax, REAL ay, REAL az, REAL T[3][3], const SFX(pspring)* S,
+                             SFX(v3) tip, SFX(v3) q, REAL* fe, SFX(v3)* Gv, REAL J[3][3]) {
+    const REAL mx = (REAL)1 - ax, my = (REAL)1 - ay, mz = (REAL)1 - az;
+    for (int ch = 0; ch < 4; ch++) {
+        const REAL f000 = t[0][ch], f100 = t[1][ch], f010 = t[2][ch], f110 = t[3][ch];
+        const REAL f001 = t[4][ch], f101 = t[5][ch], f011 = t[6][ch], f111 = t[7][ch];
+        const REAL c00 = SFX(lerp_c)(ax, mx, f000, f100), c10 = SFX(lerp_c)(ax, mx, f010, f110);
+        const REAL c01 = SFX(lerp_c)(ax, mx, f001, f101), c11 = SFX(lerp_c)(ax, mx, f011, f111);
+        const REAL c0 = SFX(lerp_c)(ay, my, c00, c10), c1 = SFX(lerp_c)(ay, my, c01, c11);
+        fe[ch] = SFX(lerp_c)(az, mz, c0, c1);
+        if (ch < 3) {
+            const REAL e0 = SFX(lerp_c)(ay, my, f100 - f000, f110 - f010);
+            const REAL e1 = SFX(lerp_c)(ay, my, f101 - f001, f111 - f011);
+            const REAL dX = SFX(lerp_c)(az, mz, e0, e1);
+            const REAL dY = SFX(lerp_c)(az, mz, c10 - c00, c11 - c01);
+            const REAL dZ = c1 - c0;
+            for (int m = 0; m < 3; m++) J[ch][m] = FMA(dZ, T[2][m], FMA(dY, T[1][m], dX * T[0][m]));
+        }
+    }
+    SFX(v3) d = S->frame ? SFX(rotmat)(SFX(sub3)(q, tip), S->a, S->b, S->c) : SFX(sub3)(q, tip);
+    SFX(v3) fs = SFX(tip_force)(d, S->k, S->d0);
+    SFX(v3) ft = S->frame ? SFX(rotmatT)(fs, S->a, S->b, S->c) : fs;
+    *Gv = SFX(mk3)(fe[0] + ft.x, fe[1] + ft.y, fe[2] + ft.z);
+    if (S->frame) {
+        Gv->x = FMA(S->c.x, S->surf, Gv->x);
+        Gv->y = FMA(S->c.y, S->surf, Gv->y);
+        Gv->z = FMA(S->c.z, S->surf, Gv->z);
+    }
+    REAL Jd[3][3] = {{S->k[0], 0, 0}, {0, S->k[1], 0}, {0, 0, S->k[2]}};
+    if (S->k[3] != (REAL)0) {
+        REAL r = SQRT(SFX(dot3)(d, d));
+        r = FMAX(r, (REAL)1e-10);
+        const REAL s = (S->k[3] * (r - S->d0[3])) / r;
+        const REAL beta = (S->k[3] * S->d0[3]) / ((r * r) * r);
+        const REAL dv[3] = {d.x, d.y, d.z};
+        Jd[0][0] = S->k[0] + s;
+        Jd[1][1] = S->k[1] + s;
+        Jd[2][2] = S->k[2] + s;
+        for (int i = 0; i < 3; i++) {
+            const REAL bd = beta * dv[i];
+            for (int j = 0; j < 3; j++) Jd[i][j] = FMA(bd, dv[j], Jd[i][j]);
+        }
+    }
+    if (S->frame) {
+        const REAL R[3][3] = {{S->a.x, S->a.y, S->a.z}, {S->b.x, S->b.y, S->b.z}, {S->c.x, S->c.y, S->c.z}};
+        REAL M[3][3];
+        for (int m = 0; m < 3; m++)
+            for (int j = 0; j < 3; j++) M[m][j] = FMA(Jd[m][2], R[2][j], FMA(Jd[m][1], R[1][j], Jd[m][0] * R[0][j]));
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                J[i][j] = J[i][j] + FMA(R[2][i], M[2][j], FMA(R[1][i], M[1][j], R[0][i] * M[0][j]));
+    } else {
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) J[i][j] = J[i][j] + Jd[i][j];
+    }
+}
+
+static int SFX(polish_step)(REAL J[3][3], SFX(v3) Gv, SFX(v3)* dq) {
+    REAL A[3][3];
+    A[0][0] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    A[0][1] = J[0][2] * J[2][1] - J[0][1] * J[2][2];
+    A[0][2] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+    A[1][0] = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    A[1][1] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+    A[1][2] = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+    A[2][0] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    A[2][1] = J[0][1] * J[2][0] - J[0][0] * J[2][1];
+    A[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    const REAL det = (J[0][0] * A[0][0] + J[0][1] * A[1][0]) + J[0][2] * A[2][0];
+    if (!(det != (REAL)0)) return 0;
+    REAL r[3];
+    for (int i = 0; i < 3; i++) {
+        const REAL tq = (A[i][0] * Gv.x + A[i][1] * Gv.y) + A[i][2] * Gv.z;
+        r[i] = (-tq) / det;
+    }
+    if (!(FABS(r[0]) <= (REAL)POLISH_MAX_STEP && FABS(r[1]) <= (REAL)POLISH_MAX_STEP &&
+          FABS(r[2]) <= (REAL)POLISH_MAX_STEP))
+        return 0;
+    *dq = SFX(mk3)(r[0], r[1], r[2]);
+    return 1;
+}
+
+/* q in/out; fe: the sample at the final q (left unchanged with q if q's cell
+ * is outside the sampler's range). */
+static void SFX(newton_polish)(const GRID_T* g, const SFX(gridref)* G, const SFX(pspring)* S, SFX(v3) tip,
+                               SFX(v3)* q, REAL* fe) {
+    REAL T[3][3];
+    const REAL fx = (REAL)G->nx, fy = (REAL)G->ny, fz = (REAL)G->nz;
+    for (int m = 0; m < 3; m++) { T[0][m] = fx * G->dA[m]; T[1][m] = fy * G->dB[m]; T[2][m] = fz * G->dC[m]; }
+    REAL t[8][4], ax = 0, ay = 0, az = 0;
+    if (!SFX(polish_fetch)(g, G, *q, t, &ax, &ay, &az)) return;
+    REAL J[3][3], fe0[4];
+    SFX(v3) Gv;
+    SFX(polish_eval)(t, ax, ay, az, T, S, tip, *q, fe0, &Gv, J);
+    REAL g2 = SFX(dot3)(Gv, Gv);
+    for (int it = 0; it < POLISH_STEPS; it++) {
+        SFX(v3) dq;
+        if (!SFX(polish_step)(J, Gv, &dq)) break;
+        const SFX(v3) q1 = SFX(add3)(*q, dq);
+        if (!SFX(polish_fetch)(g, G, q1, t, &ax, &ay, &az)) break;
+        REAL J1[3][3], fe1[4];
+        SFX(v3) G1;
+        SFX(polish_eval)(t, ax, ay, az, T, S, tip, q1, fe1, &G1, J1);
+        const REAL g21 = SFX(dot3)(G1, G1);
+        if (!(g21 < g2)) break;
+        *q = q1;
+        for (int c = 0; c < 4; c++) fe0[c] = fe1[c];
+        Gv = G1;
+        g2 = g21;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) J[i][j] = J1[i][j];
+    }
+    for (int c = 0; c < 4; c++) fe[c] = fe0[c];
+}
+
 /* relaxStrokes: one pixel, all z-steps                    AFM.cl:345-394
  * FEs/disps are (nzs,4) rows for this pixel in stroke order (iz=0 highest),
  * or reversed when flip!=0 (the z flip scan_fdbm applies on the host). */
 static void SFX(relax_strokes_pixel)(const GRID_T* g, const SFX(gridref)* G, const float* pt,
                                      int nzs, const REAL* dTip, const REAL* k, const REAL* d0,
                                      const REAL* relax, int max_iter, REAL f2conv, int use_fire,
-                                     int flip, REAL* FEs, REAL* disps) {
+                                     int flip, int polish, REAL* FEs, REAL* disps) {
+    SFX(pspring) S;
+    S.a = S.b = S.c = SFX(mk3)(0, 0, 0);
+    for (int i = 0; i < 4; i++) { S.k[i] = k[i]; S.d0[i] = d0[i]; }
+    S.surf = 0;
+    S.frame = 0;
     SFX(v3) tip = SFX(mk3)((REAL)pt[0], (REAL)pt[1], (REAL)pt[2]);
     SFX(v3) pos = SFX(mk3)(tip.x + d0[0], tip.y + d0[1], tip.z + d0[2]);
     REAL dt = relax[0], damp = relax[1];
@@ -180,11 +342,13 @@ static void SFX(relax_strokes_pixel)(const GRID_T* g, const SFX(gridref)* G, con
             if (SFX(dot3)(f, f) < f2conv) break;
         }
         int oz = flip ? (nzs - 1 - iz) : iz;
+        SFX(v3) q = pos;  /* output position; the next z-step starts from pos */
+        if (polish) SFX(newton_polish)(g, G, &S, tip, &q, fe);
         SFX(v3) ref = SFX(mk3)(tip.x + d0[0], tip.y + d0[1], tip.z + d0[2]);
         FEs[oz * 4 + 0] = fe[0]; FEs[oz * 4 + 1] = fe[1];
         FEs[oz * 4 + 2] = fe[2]; FEs[oz * 4 + 3] = fe[3];
-        disps[oz * 4 + 0] = pos.x - ref.x; disps[oz * 4 + 1] = pos.y - ref.y;
-        disps[oz * 4 + 2] = pos.z - ref.z; disps[oz * 4 + 3] = 0;
+        disps[oz * 4 + 0] = q.x - ref.x; disps[oz * 4 + 1] = q.y - ref.y;
+        disps[oz * 4 + 2] = q.z - ref.z; disps[oz * 4 + 3] = 0;
         tip.x = tip.x + dTip[0]; tip.y = tip.y + dTip[1]; tip.z = tip.z + dTip[2];
         pos.x = pos.x + dTip[0]; pos.y = pos.y + dTip[1]; pos.z = pos.z + dTip[2];
     }
@@ -227,7 +391,7 @@ static void SFX(relax_2d_pixel)(const GRID_T* g, const SFX(gridref)* G, const fl
 static void SFX(relax_tilted_pixel)(const GRID_T* g, const SFX(gridref)* G, const float* pt, int nzs,
                                     const REAL* tA, const REAL* tB, const REAL* tC, const REAL* k,
                                     const REAL* d0, const REAL* relax, const REAL* surf, int max_iter,
-                                    REAL f2conv, int use_fire, REAL* FEs) {
+                                    REAL f2conv, int use_fire, int polish, REAL* FEs) {
     SFX(v3) a = SFX(mk3)(tA[0], tA[1], tA[2]);
     SFX(v3) b = SFX(mk3)(tB[0], tB[1], tB[2]);
     SFX(v3) c = SFX(mk3)(tC[0], tC[1], tC[2]);
@@ -250,6 +414,15 @@ static void SFX(relax_tilted_pixel)(const GRID_T* g, const SFX(gridref)* G, cons
             if (SFX(dot3)(f, f) < f2conv) break;
         }
         SFX(interp_fe)(g, G->nx, G->ny, G->nz, G->dA, G->dB, G->dC, pos, fe);
+        if (polish) {
+            SFX(pspring) S;
+            S.a = a; S.b = b; S.c = c;
+            for (int i = 0; i < 4; i++) { S.k[i] = k[i]; S.d0[i] = d0[i]; }
+            S.surf = surf[0];
+            S.frame = 1;
+            SFX(v3) q = pos;
+            SFX(newton_polish)(g, G, &S, tip, &q, fe);
+        }
         SFX(v3) fr = SFX(rotmat)(SFX(mk3)(fe[0], fe[1], fe[2]), a, b, c);
         FEs[iz * 4 + 0] = fr.x; FEs[iz * 4 + 1] = fr.y; FEs[iz * 4 + 2] = fr.z; FEs[iz * 4 + 3] = fe[3];
         tip = SFX(add3)(tip, dTip);
@@ -384,7 +557,7 @@ static void SFX(relax_direct_pixel)(int na, const REAL* atoms, const REAL* cMs, 
 static void SFX(relax_pp_pixel)(const GRID_T* g, const SFX(gridref)* G, const float* pt, int nzs,
                                 const REAL* tA, const REAL* tB, const REAL* tC, const REAL* k,
                                 const REAL* d0, const REAL* relax, const REAL* surf, int max_iter,
-                                REAL f2conv, int use_fire, REAL* FEs, REAL* PPs) {
+                                REAL f2conv, int use_fire, int polish, REAL* FEs, REAL* PPs) {
     SFX(v3) a = SFX(mk3)(tA[0], tA[1], tA[2]);
     SFX(v3) b = SFX(mk3)(tB[0], tB[1], tB[2]);
     SFX(v3) c = SFX(mk3)(tC[0], tC[1], tC[2]);
@@ -409,11 +582,20 @@ static void SFX(relax_pp_pixel)(const GRID_T* g, const SFX(gridref)* G, const fl
             SFX(md_step)(f, &v, &pos, &dt, &damp, dtmin, dtmax, damp0, use_fire);
         }
         if (!conv) SFX(interp_fe)(g, G->nx, G->ny, G->nz, G->dA, G->dB, G->dC, pos, fe);
+        SFX(v3) q = pos;  /* output position; the next z-step starts from pos */
+        if (polish) {
+            SFX(pspring) S;
+            S.a = a; S.b = b; S.c = c;
+            for (int i = 0; i < 4; i++) { S.k[i] = k[i]; S.d0[i] = d0[i]; }
+            S.surf = surf[0];
+            S.frame = 1;
+            SFX(newton_polish)(g, G, &S, tip, &q, fe);
+        }
         SFX(v3) fr = SFX(rotmat)(SFX(mk3)(fe[0], fe[1], fe[2]), a, b, c);
         FEs[iz * 4 + 0] = fr.x; FEs[iz * 4 + 1] = fr.y; FEs[iz * 4 + 2] = fr.z; FEs[iz * 4 + 3] = fe[3];
         int finite = isfinite(fe[0]) && isfinite(fe[1]) && isfinite(fe[2]) && isfinite(fe[3]) &&
-                     isfinite(pos.x) && isfinite(pos.y) && isfinite(pos.z);
-        PPs[iz * 4 + 0] = pos.x; PPs[iz * 4 + 1] = pos.y; PPs[iz * 4 + 2] = pos.z;
+                     isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
+        PPs[iz * 4 + 0] = q.x; PPs[iz * 4 + 1] = q.y; PPs[iz * 4 + 2] = q.z;
         PPs[iz * 4 + 3] = (REAL)((conv && finite) ? itr : -itr);
         tip = SFX(add3)(tip, dTip);
         pos = SFX(add3)(pos, dTip);

@@ -62,23 +62,23 @@ def lib():
                                       _vp]),
         "ora_pair_fe_d": (None, [_i, _i, _vp, _vp, _i, _vp, _i, _vp, _vp, _vp]),
         "ora_relax_strokes_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _i, _f, _i,
-                                       _i, _vp, _vp]),
+                                       _i, _i, _vp, _vp]),
         "ora_relax_strokes_d": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _i, _d, _i,
-                                       _i, _vp, _vp]),
+                                       _i, _i, _vp, _vp]),
         "ora_relax_tilted_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                      _i, _f, _i, _vp]),
+                                      _i, _f, _i, _i, _vp]),
         "ora_relax_2d_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _f, _f, _f, _f, _i, _f, _i, _vp,
                                   _vp]),
         "ora_relax_tilted_d": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                      _i, _d, _i, _vp]),
+                                      _i, _d, _i, _i, _vp]),
         "ora_raw_tilted_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
         "ora_raw_tilted_d": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
         "ora_relax_direct_d": (None, [_i, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
                                       _d, _i, _vp, _vp]),
         "ora_relax_pp_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                  _i, _f, _i, _vp, _vp]),
+                                  _i, _f, _i, _i, _vp, _vp]),
         "ora_relax_pp_d": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                  _i, _d, _i, _vp, _vp]),
+                                  _i, _d, _i, _i, _vp, _vp]),
         "ora_convolve_z_f": (None, [_vp, _i, _i, _i, _vp, _vp]),
         "ora_izo_z_f": (None, [_vp, _i, _i, _f, _vp]),
     }
@@ -159,8 +159,9 @@ def _grid_args(grid):
 
 
 def relax_strokes(grid, dinv, pts, nz, dTip, stiffness, dpos0, relax, max_iter=128, f2conv=1e-8, use_fire=True,
-                  flip=False, prec="f32"):
-    """relaxStrokes -> FEs, disps (n_scan,nz,4). prec 'f32' (bit-exact canon) or 'f64'."""
+                  flip=False, prec="f32", polish=False):
+    """relaxStrokes -> FEs, disps (n_scan,nz,4). prec 'f32' (bit-exact canon) or 'f64'.
+    polish: Newton-polish each z-step's equilibrium (the kernels' SPM_FLAG_POLISH)."""
     dt = np.float32 if prec == "f32" else np.float64
     g = np.ascontiguousarray(grid, dtype=dt)
     pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 4)
@@ -171,7 +172,7 @@ def relax_strokes(grid, dinv, pts, nz, dTip, stiffness, dpos0, relax, max_iter=1
     ps = [_v4(v) for v in (dTip, stiffness, dpos0, relax)]
     fn = lib().ora_relax_strokes_f if prec == "f32" else lib().ora_relax_strokes_d
     fn(_p(g), *_grid_args(g), *[_p(v) for v in vs], _p(pts), n_scan, int(nz), *[_p(v) for v in ps], int(max_iter),
-       float(f2conv), int(bool(use_fire)), int(bool(flip)), _p(FEs), _p(disps))
+       float(f2conv), int(bool(use_fire)), int(bool(flip)), int(bool(polish)), _p(FEs), _p(disps))
     return FEs, disps
 
 
@@ -190,7 +191,7 @@ def relax_2d(grid, dinv, pts, nz, K_lat, dh, dt, damp, max_iter=128, f2conv=1e-8
 
 
 def relax_tilted(grid, dinv, pts, nz, tipA, tipB, tipC, stiffness, dpos0, relax, surfFF, max_iter=128, f2conv=1e-8,
-                 use_fire=True, prec="f32"):
+                 use_fire=True, prec="f32", polish=False):
     dt = np.float32 if prec == "f32" else np.float64
     g = np.ascontiguousarray(grid, dtype=dt)
     pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 4)
@@ -200,12 +201,12 @@ def relax_tilted(grid, dinv, pts, nz, tipA, tipB, tipC, stiffness, dpos0, relax,
     ps = [_v4(v) for v in (tipA, tipB, tipC, stiffness, dpos0, relax, surfFF)]
     fn = lib().ora_relax_tilted_f if prec == "f32" else lib().ora_relax_tilted_d
     fn(_p(g), *_grid_args(g), *[_p(v) for v in vs], _p(pts), n_scan, int(nz), *[_p(v) for v in ps], int(max_iter),
-       float(f2conv), int(bool(use_fire)), _p(FEs))
+       float(f2conv), int(bool(use_fire)), int(bool(polish)), _p(FEs))
     return FEs
 
 
 def relax_pp(grid, dinv, pts, nz, tipA, tipB, tipC, stiffness, dpos0, relax, surfFF, max_iter=128, f2conv=1e-8,
-             use_fire=True, prec="f32"):
+             use_fire=True, prec="f32", polish=False):
     """Grid relaxation with equilibrium bookkeeping -> FEs, PPs (n_scan,nz,4)."""
     dt = np.float32 if prec == "f32" else np.float64
     g = np.ascontiguousarray(grid, dtype=dt)
@@ -217,7 +218,7 @@ def relax_pp(grid, dinv, pts, nz, tipA, tipB, tipC, stiffness, dpos0, relax, sur
     ps = [_v4(v, dt) for v in (tipA, tipB, tipC, stiffness, dpos0, relax, surfFF)]
     fn = lib().ora_relax_pp_f if prec == "f32" else lib().ora_relax_pp_d
     fn(_p(g), *_grid_args(g), *[_p(v) for v in vs], _p(pts), n_scan, int(nz), *[_p(v) for v in ps], int(max_iter),
-       float(f2conv), int(bool(use_fire)), _p(FEs), _p(PPs))
+       float(f2conv), int(bool(use_fire)), int(bool(polish)), _p(FEs), _p(PPs))
     return FEs, PPs
 
 

@@ -170,19 +170,21 @@ void ora_pair_fe_d(int kind, int na, const double* atoms, const double* prm, int
 void ora_relax_strokes_f(const float* grid, int nx, int ny, int nz, const float* dinvA,
                          const float* dinvB, const float* dinvC, const float* pts, int nscan, int nzs,
                          const float* dTip, const float* k, const float* d0, const float* relax,
-                         int max_iter, float f2conv, int use_fire, int flip, float* FEs, float* disps) {
+                         int max_iter, float f2conv, int use_fire, int flip, int polish, float* FEs,
+                         float* disps) {
     gridref_f G; G.nx = nx; G.ny = ny; G.nz = nz;
     cvt4_f(dinvA, G.dA); cvt4_f(dinvB, G.dB); cvt4_f(dinvC, G.dC);
 #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < nscan; i++)
         relax_strokes_pixel_f(grid, &G, pts + 4 * (size_t)i, nzs, dTip, k, d0, relax, max_iter, f2conv,
-                              use_fire, flip, FEs + (size_t)i * nzs * 4, disps + (size_t)i * nzs * 4);
+                              use_fire, flip, polish, FEs + (size_t)i * nzs * 4, disps + (size_t)i * nzs * 4);
 }
 
 void ora_relax_strokes_d(const double* grid, int nx, int ny, int nz, const float* dinvA,
                          const float* dinvB, const float* dinvC, const float* pts, int nscan, int nzs,
                          const float* dTip, const float* k, const float* d0, const float* relax,
-                         int max_iter, double f2conv, int use_fire, int flip, double* FEs, double* disps) {
+                         int max_iter, double f2conv, int use_fire, int flip, int polish, double* FEs,
+                         double* disps) {
     gridref_d G; G.nx = nx; G.ny = ny; G.nz = nz;
     cvt4_d(dinvA, G.dA); cvt4_d(dinvB, G.dB); cvt4_d(dinvC, G.dC);
     double t[4], kk[4], dd[4], rr[4];
@@ -190,7 +192,7 @@ void ora_relax_strokes_d(const double* grid, int nx, int ny, int nz, const float
 #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < nscan; i++)
         relax_strokes_pixel_d(grid, &G, pts + 4 * (size_t)i, nzs, t, kk, dd, rr, max_iter, f2conv,
-                              use_fire, flip, FEs + (size_t)i * nzs * 4, disps + (size_t)i * nzs * 4);
+                              use_fire, flip, polish, FEs + (size_t)i * nzs * 4, disps + (size_t)i * nzs * 4);
 }
 
 void ora_relax_2d_f(const float* grid, int nx, int ny, int nz, const float* dinvA, const float* dinvB,
@@ -208,20 +210,20 @@ void ora_relax_tilted_f(const float* grid, int nx, int ny, int nz, const float* 
                         const float* dinvB, const float* dinvC, const float* pts, int nscan, int nzs,
                         const float* tA, const float* tB, const float* tC, const float* k, const float* d0,
                         const float* relax, const float* surf, int max_iter, float f2conv, int use_fire,
-                        float* FEs) {
+                        int polish, float* FEs) {
     gridref_f G; G.nx = nx; G.ny = ny; G.nz = nz;
     cvt4_f(dinvA, G.dA); cvt4_f(dinvB, G.dB); cvt4_f(dinvC, G.dC);
 #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < nscan; i++)
         relax_tilted_pixel_f(grid, &G, pts + 4 * (size_t)i, nzs, tA, tB, tC, k, d0, relax, surf, max_iter,
-                             f2conv, use_fire, FEs + (size_t)i * nzs * 4);
+                             f2conv, use_fire, polish, FEs + (size_t)i * nzs * 4);
 }
 
 void ora_relax_tilted_d(const double* grid, int nx, int ny, int nz, const float* dinvA,
                         const float* dinvB, const float* dinvC, const float* pts, int nscan, int nzs,
                         const float* tA, const float* tB, const float* tC, const float* k, const float* d0,
                         const float* relax, const float* surf, int max_iter, double f2conv, int use_fire,
-                        double* FEs) {
+                        int polish, double* FEs) {
     gridref_d G; G.nx = nx; G.ny = ny; G.nz = nz;
     cvt4_d(dinvA, G.dA); cvt4_d(dinvB, G.dB); cvt4_d(dinvC, G.dC);
     double a[4], b[4], c[4], kk[4], dd[4], rr[4], ss[4];
@@ -229,7 +231,7 @@ void ora_relax_tilted_d(const double* grid, int nx, int ny, int nz, const float*
 #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < nscan; i++)
         relax_tilted_pixel_d(grid, &G, pts + 4 * (size_t)i, nzs, a, b, c, kk, dd, rr, ss, max_iter, f2conv,
-                             use_fire, FEs + (size_t)i * nzs * 4);
+                             use_fire, polish, FEs + (size_t)i * nzs * 4);
 }
 
 void ora_raw_tilted_f(const float* grid, int nx, int ny, int nz, const float* dinvA, const float* dinvB,
@@ -281,13 +283,13 @@ void ora_relax_direct_d(int na, const double* atoms, const double* cMs, const fl
 void ora_relax_pp_f(const float* grid, int nx, int ny, int nz, const float* dinvA, const float* dinvB,
                     const float* dinvC, const float* pts, int nscan, int nzs, const float* tA, const float* tB,
                     const float* tC, const float* k, const float* d0, const float* relax, const float* surf,
-                    int max_iter, float f2conv, int use_fire, float* FEs, float* PPs) {
+                    int max_iter, float f2conv, int use_fire, int polish, float* FEs, float* PPs) {
     gridref_f G; G.nx = nx; G.ny = ny; G.nz = nz;
     cvt4_f(dinvA, G.dA); cvt4_f(dinvB, G.dB); cvt4_f(dinvC, G.dC);
 #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < nscan; i++)
         relax_pp_pixel_f(grid, &G, pts + 4 * (size_t)i, nzs, tA, tB, tC, k, d0, relax, surf, max_iter, f2conv,
-                         use_fire, FEs + (size_t)i * nzs * 4, PPs + (size_t)i * nzs * 4);
+                         use_fire, polish, FEs + (size_t)i * nzs * 4, PPs + (size_t)i * nzs * 4);
 }
 
 /* FP64 variant: every parameter vector is double (used by finite-difference
@@ -295,13 +297,13 @@ void ora_relax_pp_f(const float* grid, int nx, int ny, int nz, const float* dinv
 void ora_relax_pp_d(const double* grid, int nx, int ny, int nz, const double* dinvA, const double* dinvB,
                     const double* dinvC, const float* pts, int nscan, int nzs, const double* tA, const double* tB,
                     const double* tC, const double* k, const double* d0, const double* relax, const double* surf,
-                    int max_iter, double f2conv, int use_fire, double* FEs, double* PPs) {
+                    int max_iter, double f2conv, int use_fire, int polish, double* FEs, double* PPs) {
     gridref_d G; G.nx = nx; G.ny = ny; G.nz = nz;
     for (int c = 0; c < 4; c++) { G.dA[c] = dinvA[c]; G.dB[c] = dinvB[c]; G.dC[c] = dinvC[c]; }
 #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < nscan; i++)
         relax_pp_pixel_d(grid, &G, pts + 4 * (size_t)i, nzs, tA, tB, tC, k, d0, relax, surf, max_iter, f2conv, use_fire,
-                         FEs + (size_t)i * nzs * 4, PPs + (size_t)i * nzs * 4);
+                         polish, FEs + (size_t)i * nzs * 4, PPs + (size_t)i * nzs * 4);
 }
 
 /* convolveZ (kernels/AFM.cl:666-701): per z-column c,

@@ -105,40 +105,68 @@ class _Molecule:
         self.lvec = lvec
 
 
-def load_xyz_molecule(xyz_path):
-    """Minimal .xyz reader: element (name or Z), x, y, z[, q] per atom line."""
-    types = read_element_types()
-    by_z = {e.iZ: n for n, e in types.items()}
+# Chemical element symbols in order of atomic number (Z = index + 1).
+ELEMENT_SYMBOLS = (
+    "H", "He", "Li", "Be", "B", "C", "N", "O", "F", "Ne", "Na", "Mg", "Al", "Si", "P", "S", "Cl", "Ar", "K", "Ca",
+    "Sc", "Ti", "V", "Cr", "Mn", "Fe", "Co", "Ni", "Cu", "Zn", "Ga", "Ge", "As", "Se", "Br", "Kr", "Rb", "Sr", "Y",
+    "Zr", "Nb", "Mo", "Tc", "Ru", "Rh", "Pd", "Ag", "Cd", "In", "Sn", "Sb", "Te", "I", "Xe", "Cs", "Ba", "La", "Ce",
+    "Pr", "Nd", "Pm", "Sm", "Eu", "Gd", "Tb", "Dy", "Ho", "Er", "Tm", "Yb", "Lu", "Hf", "Ta", "W", "Re", "Os", "Ir",
+    "Pt", "Au", "Hg", "Tl", "Pb", "Bi", "Po", "At", "Rn", "Fr", "Ra", "Ac", "Th", "Pa", "U", "Np", "Pu", "Am", "Cm",
+    "Bk", "Cf", "Es", "Fm", "Md", "No", "Lr", "Rf", "Db", "Sg", "Bh", "Hs", "Mt", "Ds", "Rg", "Cn", "Nh", "Fl", "Mc",
+    "Lv", "Ts", "Og")
+_Z_OF_SYMBOL = {e: i + 1 for i, e in enumerate(ELEMENT_SYMBOLS)}
+
+
+def load_xyz_molecule(xyz_path, nmax=10000):
+    """.xyz reader with the line rules of the reference's loader (AtomicSystem(fname) ->
+    atomicUtils.load_xyz with bReadN, spammm/AtomicSystem.py:35-90, spammm/atomicUtils.py:1212):
+    an atom line is "element x y z [q]" where the element is an atomic number or a chemical
+    symbol; any other line before the first atom either gives the atom count (an integer first
+    word) or is the comment; reading stops after the count.  A comment starting with "lvs" holds
+    the periodic cell vectors (the first nine numbers on it, row-major)."""
     apos, enames, qs = [], [], []
-    lvec = None
+    comment = None
     with open(xyz_path) as f:
-        lines = f.read().splitlines()
-    for i, line in enumerate(lines):
-        w = line.split()
-        if i == 1 and "lvs" in line:
+        for line in f:
+            w = line.split()
+            atom = None
             try:
-                v = [float(x) for x in line.split("lvs", 1)[1].split()[:9]]
-                lvec = np.array(v, dtype=np.float64).reshape(3, 3)
+                xyz = (float(w[1]), float(w[2]), float(w[3]))
+                try:
+                    q = float(w[4])
+                except (IndexError, ValueError):
+                    q = 0.0
+                try:
+                    name = ELEMENT_SYMBOLS[int(w[0]) - 1]
+                except ValueError:
+                    name = w[0]
+                    if name not in _Z_OF_SYMBOL:
+                        raise KeyError(name)
+                atom = (xyz, name, q)
+            except (IndexError, ValueError, KeyError):
+                if not apos:
+                    try:
+                        nmax = int(w[0])
+                    except (IndexError, ValueError):
+                        comment = line.strip()
+            if atom is not None:
+                apos.append(atom[0])
+                enames.append(atom[1])
+                qs.append(atom[2])
+            if len(apos) >= nmax:
+                break
+    lvec = None
+    if comment is not None and comment[:3] == "lvs":
+        nums = []
+        for tok in comment.split():
+            try:
+                nums.append(float(tok))
             except ValueError:
-                pass
-        if len(w) < 4:
-            continue
-        try:
-            xyz = (float(w[1]), float(w[2]), float(w[3]))
-        except ValueError:
-            continue
-        try:
-            q = float(w[4])
-        except (IndexError, ValueError):
-            q = 0.0
-        try:
-            name = by_z[int(w[0])]
-        except (ValueError, KeyError):
-            name = w[0]
-        apos.append(xyz)
-        enames.append(name)
-        qs.append(q)
-    return _Molecule(np.array(apos, dtype=np.float64), enames, np.array(qs, dtype=np.float64), lvec)
+                continue
+        if len(nums) < 9:
+            raise ValueError(f"{xyz_path}: 'lvs' line holds {len(nums)} numbers, need 9")
+        lvec = np.array(nums[:9], dtype=np.float64).reshape(3, 3)
+    return _Molecule(np.array(apos, dtype=np.float64).reshape(-1, 3), enames, np.array(qs, dtype=np.float64), lvec)
 
 
 class AFMulator:
@@ -190,6 +218,9 @@ class AFMulator:
         self._vram_bytes = 0
         self.n_relax_max = N_RELAX_STEP_MAX
         self.f2conv = F2CONV
+        # not in the reference: Newton-polish every relaxed state (SPM_FLAG_POLISH) so that FEs and
+        # displacements sit at the equilibrium of the interpolated field instead of FIRE's stopping point
+        self.newton_polish = False
         self.mol = self.elem_types = None
         self.atoms_arr = self.cLJs_arr = None
         self.img_FF = self.n = self.p0 = self.L = None
@@ -227,6 +258,7 @@ class AFMulator:
         kw.setdefault("max_iter", self.n_relax_max)
         kw.setdefault("f2conv", self.f2conv)
         kw.setdefault("fire", self.use_fire)
+        kw.setdefault("polish", self.newton_polish)
         return _lib.make_scan_params(**kw)
 
     # ---------------------------------------------------------------- FDBM grid
@@ -388,7 +420,7 @@ class AFMulator:
         self.realloc_scan_buffers(nx_s * ny_s, nz_s)
         P = self._flags_params(dinv=(self.fdbm_dinvA, self.fdbm_dinvB, self.fdbm_dinvC), dTip=[0., 0., -dh, 0.],
                                stiffness=[K_LAT, 0., 0., 0.], relax_params=[dt, damp, 0., 0.], nz=nz_s, fire=False,
-                               flip_z=True, raster_ny=ny_s)
+                               flip_z=True, raster_ny=ny_s, polish=False)
         FEs, disps = gpu.relax_2d(self.img_FF_fdbm, P, torch.from_numpy(pts).to(self.device))
         FEs = FEs.reshape(nx_s, ny_s, nz_s, 4)
         disps = disps.reshape(nx_s, ny_s, nz_s, 4)
@@ -594,7 +626,7 @@ class AFMulator:
             raise ValueError(f"osc_dir must be a finite non-zero vector, got {osc_dir!r}")
         dTip = np.array([0., 0., dtip, 0.], dtype=np.float32)
         P = self._flags_params(dinv=(self.dinvA, self.dinvB, self.dinvC), tipA=self.tipA, tipB=self.tipB,
-                               tipC=self.tipC, dTip=dTip, dpos0=self.dpos0, nz=nz, raster_ny=ny_s)
+                               tipC=self.tipC, dTip=dTip, dpos0=self.dpos0, nz=nz, raster_ny=ny_s, polish=False)
         FEs = gpu.fe_in_strokes_tilted(self.img_FF, P, torch.from_numpy(pts).to(self.device))
         return gpu.to_host(FEs.reshape(nx_s, ny_s, nz, 4)), pts[:, :3].reshape(nx_s, ny_s, 3)
 
@@ -651,7 +683,8 @@ class AFMulator:
         tipC = self.tipC.copy()
         tipC[3] = np.float32(dtip)
         P = self._flags_params(tipA=self.tipA, tipB=self.tipB, tipC=tipC, stiffness=self.stiffness, dpos0=self.dpos0,
-                               relax_params=self.relax_pars, surfFF=self.surfFF, nz=nz, raster_ny=ny_s, fire=True)
+                               relax_params=self.relax_pars, surfFF=self.surfFF, nz=nz, raster_ny=ny_s, fire=True,
+                               polish=False)
         FEs_t, PPs_t = gpu.relax_direct_morse(self.atoms_arr, self.cLJs_arr, pts, P, self.tipQs, self.tipQZs)
         FEs = gpu.to_host(FEs_t.reshape(nx_s, ny_s, nz, 4))
         PPs = gpu.to_host(PPs_t.reshape(nx_s, ny_s, nz, 4))
@@ -747,7 +780,7 @@ class AFMulator:
         tipC = self.tipC.copy()
         tipC[3] = np.float32(dtip)
         P = self._flags_params(tipA=self.tipA, tipB=self.tipB, tipC=tipC, stiffness=self.stiffness, dpos0=self.dpos0,
-                               relax_params=self.relax_pars, surfFF=self.surfFF, nz=nz, fire=True)
+                               relax_params=self.relax_pars, surfFF=self.surfFF, nz=nz, fire=True, polish=False)
         pts = np.zeros((nx * ny, 4), dtype=np.float32)
         pts[:, :3] = points_xyz.reshape(-1, 3)
         lam, diag = gpu.adjoint_direct_state(self.atoms_arr, self.cLJs_arr, pts, P, self.tipQs, self.tipQZs,

@@ -103,6 +103,30 @@ __device__ __forceinline__ PPFrame pp_frame(const spm_scan_params& P) {
     return F;
 }
 
+__device__ __forceinline__ PolishSpring pp_spring(const PPFrame& F) {
+    PolishSpring S;
+    S.a = F.a; S.b = F.b; S.c = F.c;
+    S.kk = F.kk; S.d0 = F.d0;
+    S.surf = F.surf;
+    S.frame = true;
+    return S;
+}
+
+// The polished output of a relaxStrokes (MODE 0: plain spring) or relaxStrokesTilted (MODE 1:
+// tip frame) z-step: q and fe in, the polished position and the sample there out.
+template <int MODE, typename IDX>
+__device__ __forceinline__ void polish_state(const GridView& G, V3 a, V3 b, V3 c, float4 kk, float4 d0, float surf,
+                                             V3 tip, V3& q, float4& fe) {
+    PolishSpring S;
+    S.a = a; S.b = b; S.c = c;
+    S.kk = kk; S.d0 = d0;
+    S.surf = surf;
+    S.frame = MODE != 0;
+    float T[3][3];
+    polish_coefs(G, T);
+    newton_polish(FullCellFetch<IDX>{G}, T, S, tip, q, fe);
+}
+
 // One SPM_RELAX_PP iteration (the direct path's bookkeeping: the convergence
 // test comes before the update).  Returns true when the z-step is finished;
 // conv tells whether it converged.  CACHE: sample through the texel cache T
@@ -132,10 +156,17 @@ __device__ __forceinline__ bool pp_iter(const GridView& G, const PPFrame& F, V3 
 
 // Outputs of a finished SPM_RELAX_PP z-step: tip-frame FE at the final
 // position and PP = (pos, +iterations if converged and finite, else -iterations).
-template <typename IDX>
-__device__ __forceinline__ void pp_emit(const GridView& G, const PPFrame& F, V3 pos, float4 fe, int it, bool conv,
-                                        float4* fe_out, float4* pp_out) {
+// POLISH: the state is Newton-polished first (newton_polish); FE is then the sample at the
+// polished position, which PP reports.
+template <typename IDX, bool POLISH>
+__device__ __forceinline__ void pp_emit(const GridView& G, const PPFrame& F, V3 tip, V3 pos, float4 fe, int it,
+                                        bool conv, float4* fe_out, float4* pp_out) {
     if (!conv) fe = interp_fe<IDX>(G, pos);  // the position moved after the last sample
+    if constexpr (POLISH) {
+        float T[3][3];
+        polish_coefs(G, T);
+        newton_polish(FullCellFetch<IDX>{G}, T, pp_spring(F), tip, pos, fe);
+    }
     const V3 r = rotmat(mk3(fe.x, fe.y, fe.z), F.a, F.b, F.c);
     *fe_out = make_float4(r.x, r.y, r.z, fe.w);
     const bool finite = isfinite(fe.x) && isfinite(fe.y) && isfinite(fe.z) && isfinite(fe.w) && isfinite(pos.x) &&
@@ -148,7 +179,7 @@ __device__ __forceinline__ void pp_emit(const GridView& G, const PPFrame& F, V3 
 // CACHE (MODE 0-2): the FIRE loop samples through a register TexelCache (the
 // cell's eight texels reloaded only when the cell changes; same values; all
 // strokes share the grid, so a lane keeps its cache from pixel to pixel).
-template <int MODE, typename IDX, bool CACHE>
+template <int MODE, typename IDX, bool CACHE, bool POLISH>
 __global__ void __launch_bounds__(RX_THREADS)
 relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
              float4* __restrict__ FEs, float4* __restrict__ disps, int* __restrict__ iter_count,
@@ -208,7 +239,7 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
             bool conv;
             if (pp_iter<IDX, CACHE>(G, F, tip, pos, v, I, fe, it, total_it, conv, T, fnx, fny, fnz)) {
                 const size_t o = (size_t)k * nzs + iz;
-                pp_emit<IDX>(G, F, pos, fe, it, conv, FEs + o, disps + o);
+                pp_emit<IDX, POLISH>(G, F, tip, pos, fe, it, conv, FEs + o, disps + o);
                 tip = add3(tip, dTip);
                 pos = add3(pos, dTip);
                 v = mk3(0.f, 0.f, 0.f);
@@ -277,12 +308,16 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
         if (done) {
             const int oz = flipS ? (nzs - 1 - iz) : iz;
             const size_t o = (size_t)k * nzs + oz;
+            V3 q = pos;  // the output position (polished or not); the next z-step starts from pos
             if (MODE == 0) {
-                FEs[o] = fe;
+                float4 fo = fe;
+                if constexpr (POLISH) polish_state<MODE, IDX>(G, a, b, c, kk, d0, surf, tip, q, fo);
+                FEs[o] = fo;
                 const V3 ref = mk3(tip.x + d0.x, tip.y + d0.y, tip.z + d0.z);
-                disps[o] = make_float4(pos.x - ref.x, pos.y - ref.y, pos.z - ref.z, 0.f);
+                disps[o] = make_float4(q.x - ref.x, q.y - ref.y, q.z - ref.z, 0.f);
             } else {
-                const float4 g = interp_fe<IDX>(G, pos);
+                float4 g = interp_fe<IDX>(G, pos);
+                if constexpr (POLISH) polish_state<MODE, IDX>(G, a, b, c, kk, d0, surf, tip, q, g);
                 const V3 r = rotmat(mk3(g.x, g.y, g.z), a, b, c);
                 FEs[o] = make_float4(r.x, r.y, r.z, g.w);
             }
@@ -311,7 +346,7 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
 // lanes of a warp run that code together: 3.81 -> 2.30 ms on that scan.  The
 // per-lane sequence is relax_kernel's (the same iteration, emit and texel
 // cache), so the results are the same bits.
-template <int MODE, typename IDX>
+template <int MODE, typename IDX, bool POLISH>
 __global__ void __launch_bounds__(RX_THREADS)
 relax_tile_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
                   float4* __restrict__ FEs, float4* __restrict__ disps, int* __restrict__ iter_count,
@@ -380,7 +415,7 @@ relax_tile_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_sc
                     while (!pp_iter<IDX, true>(G, F, tip, pos, v, I, fe, it, total_it, conv, T, fnx, fny, fnz)) {
                     }
                     const size_t o = (size_t)k * nzs + iz;
-                    pp_emit<IDX>(G, F, pos, fe, it, conv, FEs + o, disps + o);
+                    pp_emit<IDX, POLISH>(G, F, tip, pos, fe, it, conv, FEs + o, disps + o);
                 } else {
                     bool done = max_iter <= 0;
                     while (!done) {
@@ -403,12 +438,16 @@ relax_tile_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_sc
                     }
                     const int oz = flipS ? (nzs - 1 - iz) : iz;
                     const size_t o = (size_t)k * nzs + oz;
+                    V3 q = pos;  // the output position; the next z-step starts from pos
                     if (MODE == 0) {
-                        FEs[o] = fe;
+                        float4 fo = fe;
+                        if constexpr (POLISH) polish_state<MODE, IDX>(G, a, b, c, kk, d0, surf, tip, q, fo);
+                        FEs[o] = fo;
                         const V3 ref = mk3(tip.x + d0.x, tip.y + d0.y, tip.z + d0.z);
-                        disps[o] = make_float4(pos.x - ref.x, pos.y - ref.y, pos.z - ref.z, 0.f);
+                        disps[o] = make_float4(q.x - ref.x, q.y - ref.y, q.z - ref.z, 0.f);
                     } else {
-                        const float4 g = interp_fe<IDX>(G, pos);
+                        float4 g = interp_fe<IDX>(G, pos);
+                        if constexpr (POLISH) polish_state<MODE, IDX>(G, a, b, c, kk, d0, surf, tip, q, g);
                         const V3 r = rotmat(mk3(g.x, g.y, g.z), a, b, c);
                         FEs[o] = make_float4(r.x, r.y, r.z, g.w);
                     }
@@ -458,8 +497,8 @@ int check_scan_args(const char* who, const float* grid, int nx, int ny, int nz, 
     SPM_REQUIRE(mul_ok((long long)nx * ny, nz, &t), "%s: grid size overflows", who);
     SPM_REQUIRE(mul_ok(n_scan, (long long)p->nz * 4, &t), "%s: output size overflows", who);
     SPM_REQUIRE(p->raster_ny >= 0, "%s: raster_ny=%d < 0", who, p->raster_ny);
-    SPM_REQUIRE((p->flags & ~(SPM_FLAG_FIRE | SPM_FLAG_FLIP_Z | SPM_FLAG_PAIRED)) == 0, "%s: unknown flags 0x%x", who,
-                p->flags);
+    SPM_REQUIRE((p->flags & ~(SPM_FLAG_FIRE | SPM_FLAG_FLIP_Z | SPM_FLAG_PAIRED | SPM_FLAG_POLISH)) == 0,
+                "%s: unknown flags 0x%x", who, p->flags);
     return SPM_OK;
 }
 
@@ -488,12 +527,12 @@ spm_scan_params normalized(const spm_scan_params* p, int n_scan) {
     return P;
 }
 
-template <int MODE, typename IDX>
+template <int MODE, typename IDX, bool POLISH>
 int launch_relax(const GridView& G, const float4* pts, int n_scan, const spm_scan_params& P, float4* FEs,
                  float4* disps, int* iter_count, unsigned* counter, cudaStream_t st) {
-    auto kern = relax_kernel<MODE, IDX, (MODE <= 2)>;
+    auto kern = relax_kernel<MODE, IDX, (MODE <= 2), POLISH>;
     if constexpr (MODE <= 2) {
-        if (counter) kern = relax_tile_kernel<MODE, IDX>;  // z-synchronised tiles from the counter
+        if (counter) kern = relax_tile_kernel<MODE, IDX, POLISH>;  // z-synchronised tiles from the counter
     }
     int blocks = static_blocks(n_scan, P);
     if (counter) {
@@ -516,9 +555,16 @@ int launch_relax(const GridView& G, const float4* pts, int n_scan, const spm_sca
 template <int MODE>
 int launch_mode(const GridView& G, long long nodes, const float4* pts, int n_scan, const spm_scan_params& P,
                 float4* FEs, float4* disps, int* iter_count, unsigned* counter, cudaStream_t st) {
+    if constexpr (MODE <= 2) {
+        if (P.flags & SPM_FLAG_POLISH) {
+            if (nodes < (1LL << 32))
+                return launch_relax<MODE, unsigned, true>(G, pts, n_scan, P, FEs, disps, iter_count, counter, st);
+            return launch_relax<MODE, size_t, true>(G, pts, n_scan, P, FEs, disps, iter_count, counter, st);
+        }
+    }
     if (nodes < (1LL << 32))
-        return launch_relax<MODE, unsigned>(G, pts, n_scan, P, FEs, disps, iter_count, counter, st);
-    return launch_relax<MODE, size_t>(G, pts, n_scan, P, FEs, disps, iter_count, counter, st);
+        return launch_relax<MODE, unsigned, false>(G, pts, n_scan, P, FEs, disps, iter_count, counter, st);
+    return launch_relax<MODE, size_t, false>(G, pts, n_scan, P, FEs, disps, iter_count, counter, st);
 }
 
 // ---- batched SPM_RELAX_PP ---------------------------------------------------
@@ -824,6 +870,8 @@ extern "C" int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz,
         SPM_REQUIRE(mode == SPM_RELAX_STROKES && n_scan % 2 == 0,
                     "spm_relax_ex: SPM_FLAG_PAIRED needs mode SPM_RELAX_STROKES and an even n_scan (mode=%d, n_scan=%d)",
                     mode, n_scan);
+    if (p->flags & SPM_FLAG_POLISH)
+        SPM_REQUIRE(mode != SPM_RELAX_2D, "spm_relax_ex: SPM_FLAG_POLISH is not defined for SPM_RELAX_2D");
     if (n_scan == 0 || p->nz == 0) return SPM_OK;
     if (mode != SPM_RELAX_TILTED)
         SPM_REQUIRE(disps != nullptr && aligned16(disps), "spm_relax_ex: disps/PPs null or misaligned");
@@ -863,7 +911,8 @@ extern "C" int spm_fe_in_strokes_tilted(const float* grid, int nx, int ny, int n
     clear_error();
     int rc = check_scan_args("spm_fe_in_strokes_tilted", grid, nx, ny, nz, points, n_scan, p, FEs);
     if (rc) return rc;
-    SPM_REQUIRE(!(p->flags & SPM_FLAG_PAIRED), "spm_fe_in_strokes_tilted: SPM_FLAG_PAIRED is for relaxStrokes only");
+    SPM_REQUIRE(!(p->flags & (SPM_FLAG_PAIRED | SPM_FLAG_POLISH)),
+                "spm_fe_in_strokes_tilted: SPM_FLAG_PAIRED / SPM_FLAG_POLISH are for the relaxations only");
     if (n_scan == 0 || p->nz == 0) return SPM_OK;
     spm_scan_params P = normalized(p, n_scan);
     raw_kernel<<<static_blocks(n_scan, P), RX_THREADS, 0, as_stream(stream)>>>(

@@ -374,4 +374,196 @@ __device__ __forceinline__ float4 interp_fe_cached(const AxisView& G, V3 p, Texe
     return blend_cached(T, ax, ay, az);
 }
 
+// ---- Newton polish of a relaxed state (SPM_FLAG_POLISH; not in the reference) --------------
+// FIRE stops once |G|^2 < f2conv, where G(q) = F_grid(q) + spring(q) [+ c*surf] is the total
+// force on the probe; with k_xy = 0.0156 eV/A^2 a 1e-5 eV/A stop leaves the probe up to ~5e-3 A
+// from the equilibrium of the interpolated field.  The polish takes that equilibrium directly:
+// G and its Jacobian J = dG/dq are exact functions of the sampled cell -- the trilinear
+// interpolant's texel-coordinate derivatives times dt/dq = n * dinv, plus the spring's
+// Jacobian -- and up to POLISH_STEPS Newton steps q <- q - J^-1 G are taken, each kept only if
+// |dq|_inf <= POLISH_MAX_STEP and it lowers |G|^2.  The oracle (ora_core.h, newton_polish)
+// repeats every operation in the same order, so results are bit-identical to it.
+constexpr int POLISH_STEPS = 4;
+constexpr float POLISH_MAX_STEP = 0.1f;
+
+// Spring and frame of a polished state: frame = false is relaxStrokes' spring (tip_force on
+// q - tip, no rotation, no surface bias); frame = true the tip frame a,b,c with surf along c.
+struct PolishSpring {
+    V3 a, b, c;
+    float4 kk, d0;
+    float surf;
+    bool frame;
+};
+
+// One evaluation at q from the cell's texels t[4*k + 2*j + i] (corner x_i, y_j, z_k) and
+// weights (ax, ay, az): fe = the trilinear sample (interp_fe's lerps, so the same value), G,
+// and J (row = force component, column = coordinate).  T[a][m] = n_a * dinv_a[m].
+__device__ __forceinline__ void polish_eval(const float4 (&t)[8], float ax, float ay, float az,
+                                            const float (&T)[3][3], const PolishSpring& S, V3 tip, V3 q,
+                                            float4& fe, V3& Gv, float (&J)[3][3]) {
+    const float mx = 1.f - ax, my = 1.f - ay, mz = 1.f - az;
+    float val[4];
+#pragma unroll
+    for (int ch = 0; ch < 4; ch++) {
+        const float f000 = (&t[0].x)[ch], f100 = (&t[1].x)[ch], f010 = (&t[2].x)[ch], f110 = (&t[3].x)[ch];
+        const float f001 = (&t[4].x)[ch], f101 = (&t[5].x)[ch], f011 = (&t[6].x)[ch], f111 = (&t[7].x)[ch];
+        const float c00 = lerp_c(ax, mx, f000, f100), c10 = lerp_c(ax, mx, f010, f110);
+        const float c01 = lerp_c(ax, mx, f001, f101), c11 = lerp_c(ax, mx, f011, f111);
+        const float c0 = lerp_c(ay, my, c00, c10), c1 = lerp_c(ay, my, c01, c11);
+        val[ch] = lerp_c(az, mz, c0, c1);
+        if (ch < 3) {
+            const float e0 = lerp_c(ay, my, f100 - f000, f110 - f010);
+            const float e1 = lerp_c(ay, my, f101 - f001, f111 - f011);
+            const float dX = lerp_c(az, mz, e0, e1);
+            const float dY = lerp_c(az, mz, c10 - c00, c11 - c01);
+            const float dZ = c1 - c0;
+#pragma unroll
+            for (int m = 0; m < 3; m++)
+                J[ch][m] = __fmaf_rn(dZ, T[2][m], __fmaf_rn(dY, T[1][m], __fmul_rn(dX, T[0][m])));
+        }
+    }
+    fe = make_float4(val[0], val[1], val[2], val[3]);
+    const V3 d = S.frame ? rotmat(sub3(q, tip), S.a, S.b, S.c) : sub3(q, tip);
+    const V3 fs = tip_force(d, S.kk, S.d0);
+    const V3 ft = S.frame ? rotmatT(fs, S.a, S.b, S.c) : fs;
+    Gv = mk3(val[0] + ft.x, val[1] + ft.y, val[2] + ft.z);
+    if (S.frame) {
+        Gv.x = __fmaf_rn(S.c.x, S.surf, Gv.x);
+        Gv.y = __fmaf_rn(S.c.y, S.surf, Gv.y);
+        Gv.z = __fmaf_rn(S.c.z, S.surf, Gv.z);
+    }
+    // spring Jacobian in the tip frame: diag(k) [+ s I + beta d d^T for the radial bond]
+    float Jd[3][3] = {{S.kk.x, 0.f, 0.f}, {0.f, S.kk.y, 0.f}, {0.f, 0.f, S.kk.z}};
+    if (S.kk.w != 0.f) {
+        float r = __fsqrt_rn(dot3(d, d));
+        r = fmaxf(r, 1e-10f);
+        const float s = __fdiv_rn(__fmul_rn(S.kk.w, r - S.d0.w), r);
+        const float beta = __fdiv_rn(__fmul_rn(S.kk.w, S.d0.w), __fmul_rn(__fmul_rn(r, r), r));
+        const float dv[3] = {d.x, d.y, d.z};
+        Jd[0][0] = S.kk.x + s;
+        Jd[1][1] = S.kk.y + s;
+        Jd[2][2] = S.kk.z + s;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const float bd = __fmul_rn(beta, dv[i]);
+#pragma unroll
+            for (int j = 0; j < 3; j++) Jd[i][j] = __fmaf_rn(bd, dv[j], Jd[i][j]);
+        }
+    }
+    if (S.frame) {
+        const float R[3][3] = {{S.a.x, S.a.y, S.a.z}, {S.b.x, S.b.y, S.b.z}, {S.c.x, S.c.y, S.c.z}};
+        float M[3][3];
+#pragma unroll
+        for (int m = 0; m < 3; m++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+                M[m][j] = __fmaf_rn(Jd[m][2], R[2][j], __fmaf_rn(Jd[m][1], R[1][j], __fmul_rn(Jd[m][0], R[0][j])));
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+                J[i][j] = J[i][j] + __fmaf_rn(R[2][i], M[2][j], __fmaf_rn(R[1][i], M[1][j], __fmul_rn(R[0][i], M[0][j])));
+    } else {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) J[i][j] = J[i][j] + Jd[i][j];
+    }
+}
+
+// Newton step dq = -J^-1 G (adjugate / determinant); false when J is singular or the step is
+// not finite or longer than POLISH_MAX_STEP along an axis.
+__device__ __forceinline__ bool polish_step(const float (&J)[3][3], V3 Gv, V3& dq) {
+    float A[3][3];
+    A[0][0] = __fmul_rn(J[1][1], J[2][2]) - __fmul_rn(J[1][2], J[2][1]);
+    A[0][1] = __fmul_rn(J[0][2], J[2][1]) - __fmul_rn(J[0][1], J[2][2]);
+    A[0][2] = __fmul_rn(J[0][1], J[1][2]) - __fmul_rn(J[0][2], J[1][1]);
+    A[1][0] = __fmul_rn(J[1][2], J[2][0]) - __fmul_rn(J[1][0], J[2][2]);
+    A[1][1] = __fmul_rn(J[0][0], J[2][2]) - __fmul_rn(J[0][2], J[2][0]);
+    A[1][2] = __fmul_rn(J[0][2], J[1][0]) - __fmul_rn(J[0][0], J[1][2]);
+    A[2][0] = __fmul_rn(J[1][0], J[2][1]) - __fmul_rn(J[1][1], J[2][0]);
+    A[2][1] = __fmul_rn(J[0][1], J[2][0]) - __fmul_rn(J[0][0], J[2][1]);
+    A[2][2] = __fmul_rn(J[0][0], J[1][1]) - __fmul_rn(J[0][1], J[1][0]);
+    const float det = (__fmul_rn(J[0][0], A[0][0]) + __fmul_rn(J[0][1], A[1][0])) + __fmul_rn(J[0][2], A[2][0]);
+    if (!(det != 0.f)) return false;  // also NaN
+    float r[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const float tq = (__fmul_rn(A[i][0], Gv.x) + __fmul_rn(A[i][1], Gv.y)) + __fmul_rn(A[i][2], Gv.z);
+        r[i] = __fdiv_rn(-tq, det);
+    }
+    if (!(fabsf(r[0]) <= POLISH_MAX_STEP && fabsf(r[1]) <= POLISH_MAX_STEP && fabsf(r[2]) <= POLISH_MAX_STEP))
+        return false;  // also NaN
+    dq = mk3(r[0], r[1], r[2]);
+    return true;
+}
+
+// The polish loop over any cell fetcher: fetch(q, ax, ay, az, t) -> false when q's cell is
+// not available (outside the sampler's range or the stored slab).  On return q is the polished
+// position and fe the sample there; when the first fetch fails both are left unchanged.
+template <class Fetch>
+__device__ __forceinline__ void newton_polish(const Fetch& fetch, const float (&T)[3][3], const PolishSpring& S,
+                                              V3 tip, V3& q, float4& fe) {
+    float4 t[8];
+    float ax, ay, az;
+    if (!fetch(q, ax, ay, az, t)) return;
+    float J[3][3];
+    V3 Gv;
+    float4 fe0;
+    polish_eval(t, ax, ay, az, T, S, tip, q, fe0, Gv, J);
+    float g2 = dot3(Gv, Gv);
+    for (int it = 0; it < POLISH_STEPS; it++) {
+        V3 dq;
+        if (!polish_step(J, Gv, dq)) break;
+        const V3 q1 = add3(q, dq);
+        if (!fetch(q1, ax, ay, az, t)) break;
+        float J1[3][3];
+        V3 G1;
+        float4 fe1;
+        polish_eval(t, ax, ay, az, T, S, tip, q1, fe1, G1, J1);
+        const float g21 = dot3(G1, G1);
+        if (!(g21 < g2)) break;
+        q = q1;
+        fe0 = fe1;
+        Gv = G1;
+        g2 = g21;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) J[i][j] = J1[i][j];
+    }
+    fe = fe0;
+}
+
+// Cell fetcher of a full (nz,ny,nx) grid with any sampling transform (interp_fe's addressing).
+template <typename IDX>
+struct FullCellFetch {
+    const GridView& G;
+    __device__ __forceinline__ bool operator()(V3 p, float& ax, float& ay, float& az, float4 (&t)[8]) const {
+        const float u = __fmaf_rn(p.x, G.dA.x, __fmaf_rn(p.y, G.dA.y, __fmaf_rn(p.z, G.dA.z, G.dA.w)));
+        const float v = __fmaf_rn(p.x, G.dB.x, __fmaf_rn(p.y, G.dB.y, __fmaf_rn(p.z, G.dB.z, G.dB.w)));
+        const float w = __fmaf_rn(p.x, G.dC.x, __fmaf_rn(p.y, G.dC.y, __fmaf_rn(p.z, G.dC.z, G.dC.w)));
+        int x0, x1, y0, y1, z0, z1;
+        bool ok = tex_axis(u, G.nx, x0, x1, ax);
+        ok = tex_axis(v, G.ny, y0, y1, ay) && ok;
+        ok = tex_axis(w, G.nz, z0, z1, az) && ok;
+        if (!ok) return false;
+        const IDX r00 = ((IDX)z0 * G.ny + y0) * G.nx, r10 = ((IDX)z0 * G.ny + y1) * G.nx;
+        const IDX r01 = ((IDX)z1 * G.ny + y0) * G.nx, r11 = ((IDX)z1 * G.ny + y1) * G.nx;
+        t[0] = __ldg(G.g + r00 + x0); t[1] = __ldg(G.g + r00 + x1);
+        t[2] = __ldg(G.g + r10 + x0); t[3] = __ldg(G.g + r10 + x1);
+        t[4] = __ldg(G.g + r01 + x0); t[5] = __ldg(G.g + r01 + x1);
+        t[6] = __ldg(G.g + r11 + x0); t[7] = __ldg(G.g + r11 + x1);
+        return true;
+    }
+};
+
+// T[a][m] = n_a * dinv_a[m] of a full-grid view.
+__device__ __forceinline__ void polish_coefs(const GridView& G, float (&T)[3][3]) {
+    const float fx = (float)G.nx, fy = (float)G.ny, fz = (float)G.nz;
+    T[0][0] = __fmul_rn(fx, G.dA.x); T[0][1] = __fmul_rn(fx, G.dA.y); T[0][2] = __fmul_rn(fx, G.dA.z);
+    T[1][0] = __fmul_rn(fy, G.dB.x); T[1][1] = __fmul_rn(fy, G.dB.y); T[1][2] = __fmul_rn(fy, G.dB.z);
+    T[2][0] = __fmul_rn(fz, G.dC.x); T[2][1] = __fmul_rn(fz, G.dC.y); T[2][2] = __fmul_rn(fz, G.dC.z);
+}
+
 }  // namespace spm

@@ -41,6 +41,9 @@ class GridScanSpec:
     f2conv: float = 1e-10
     raster_ny: int = 0
     strict: bool = True       # raise if any state fails the adjoint gates (else those states are masked)
+    polish: bool = False      # Newton-polish every equilibrium (SPM_FLAG_POLISH): the forward and the
+                              # adjoint then sit at the equilibrium of the interpolated field, not at
+                              # FIRE's stopping point
 
     def vectors(self):
         o, s = self.origin, float(self.step)
@@ -59,7 +62,7 @@ class GridScanSpec:
         return _lib.make_scan_params(dinv=self.dinv(), tipC=[0, 0, 1, self.dtip],
                                      stiffness=np.asarray(stiffness, np.float32), dpos0=self.dpos0,
                                      relax_params=self.relax_params, nz=self.nz, max_iter=self.max_iter,
-                                     f2conv=self.f2conv, fire=True, raster_ny=self.raster_ny)
+                                     f2conv=self.f2conv, fire=True, raster_ny=self.raster_ny, polish=self.polish)
 
 
 class AdjointFailure(RuntimeError):

@@ -86,12 +86,17 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("SPAMMM_REF"),
                     help="root of the SPAMMM reference tree (default: $SPAMMM_REF)")
+    ap.add_argument("--only", choices=["xyz"], default=None,
+                    help="write only one fixture file (xyz: xyz_golden.npz)")
     args = ap.parse_args()
     if not args.ref:
         ap.error("give the reference tree with --ref PATH or SPAMMM_REF")
     _install_stubs()
     sys.path.insert(0, args.ref)
     from spammm.SPM import AFM as A
+    if args.only == "xyz":
+        xyz_fixtures(A)
+        return
     from spammm.SPM import AFM_utils as U
     import tests.SPM.test_afm_morse as T
 
@@ -305,6 +310,54 @@ def main():
               strokes_FEs=np.array(FE_s), strokes_disps=np.array(D_s), tilted_FEs=np.array(FE_t), raw_FEs=np.array(raw))
     np.savez_compressed(os.path.join(OUT, "gridrelax_golden.npz"), **gr)
     print("wrote fixtures to", OUT)
+
+
+# xyz inputs for the loader fixture: element names or atomic numbers, an
+# optional charge column, a count line and an "lvs" comment line (the periodic
+# cell of setup_grid_lvec); written here, parsed by the reference.
+XYZ_TEXTS = {
+    "names_charges": "5\nmolecule with charges\nC 0.0 0.0 0.0 -0.12\nH 1.09 0.0 0.0 0.03\n"
+                     "O -0.7 1.1 0.05 -0.4\nN 0.6 -1.2 -0.02 0.25\nH -0.5 -0.9 0.1 0.24\n",
+    "numbers_no_charge": "4\n\n6 0.1 0.2 0.3\n1 1.2 0.2 0.3\n8 -1.0 0.4 0.2\n7 0.0 1.5 -0.1\n",
+    "lvs_skew": "6\nlvs 6.0 0.0 0.0   3.0 5.196152422706632 0.0   0.0 0.0 20.0\n"
+                "Na 0.0 0.0 0.0 0.8\nCl 2.0 0.0 0.0 -0.8\nNa 1.5 2.598 0.0 0.8\nCl 3.5 2.598 0.0 -0.8\n"
+                "C 2.2 1.3 3.0 0.1\nH 3.1 1.3 3.0 -0.1\n",
+}
+
+
+def xyz_fixtures(A):
+    """xyz_golden.npz: AFMulator.load_molecule's loader (spammm/AtomicSystem.py:35-90 ->
+    atomicUtils.load_xyz :1212) and setup_grid_lvec (spammm/SPM/AFM.py:839-893) on a skew cell."""
+    from types import SimpleNamespace
+    from spammm.AtomicSystem import AtomicSystem
+    out = {}
+    d = tempfile.mkdtemp(prefix="spm_xyz_")
+    for key, text in XYZ_TEXTS.items():
+        fn = os.path.join(d, key + ".xyz")
+        with open(fn, "w") as f:
+            f.write(text)
+        mol = AtomicSystem(fname=fn)
+        out[f"{key}_text"] = np.array(text)
+        out[f"{key}_apos"] = np.asarray(mol.apos, np.float64)
+        out[f"{key}_enames"] = np.array(list(mol.enames))
+        out[f"{key}_qs"] = np.asarray(mol.qs, np.float64)
+        out[f"{key}_lvec"] = np.asarray(mol.lvec, np.float64) if mol.lvec is not None else np.zeros(0)
+        if mol.lvec is not None:
+            atoms = np.zeros((len(mol.apos), 4), np.float32)
+            atoms[:, :3] = mol.apos
+            atoms[:, 3] = mol.qs
+            fake = SimpleNamespace(atoms_arr=atoms.copy(), mol=mol, _make_dinv_lvec=A.AFMulator._make_dinv_lvec,
+                                   _max_alloc=1 << 40)
+            n, margin_z, z_top = (60, 52, 230), 2.0, 12.0
+            L = A.AFMulator.setup_grid_lvec(fake, n, margin_z, z_top)
+            out.update({f"{key}_lvec_n": np.array(n), f"{key}_lvec_margin_z": np.float64(margin_z),
+                        f"{key}_lvec_z_top": np.float64(z_top), f"{key}_lvec_L": L,
+                        f"{key}_lvec_atoms": fake.atoms_arr, f"{key}_lvec_mol_shift": fake.mol_shift,
+                        f"{key}_lvec_dA": fake.dA, f"{key}_lvec_dB": fake.dB, f"{key}_lvec_dC": fake.dC,
+                        f"{key}_lvec_dinv": np.stack([fake.dinvA, fake.dinvB, fake.dinvC])})
+    out["keys"] = np.array(list(XYZ_TEXTS))
+    np.savez_compressed(os.path.join(OUT, "xyz_golden.npz"), **out)
+    print("wrote xyz_golden.npz to", OUT)
 
 
 if __name__ == "__main__":

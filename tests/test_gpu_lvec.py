@@ -1,0 +1,59 @@
+"""Periodic skew cell through the drop-in (setup_grid_lvec, spammm/SPM/AFM.py:
+839-893): a NaCl-like layer with a molecule in a 60-degree cell read by
+load_molecule from an .xyz with an "lvs" line (the fixture of
+tests/golden/xyz_golden.npz), LJ grid on the skew node lattice against the FP64
+oracle (grid-build tolerance: 2e-5 |ref| + 2e-6 max|ref|), and run_scan
+(relaxStrokesTilted) over a window larger than the cell -- probes sample across
+the periodic seam through the skew sampling transform -- bit-identical to the
+canonical-FP32 oracle on the same grid; unrelaxed samples of a window shifted
+by a cell vector equal the unshifted ones.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from spammm_b200.AFM import AFMulator
+
+pytestmark = pytest.mark.gpu
+
+
+def test_skew_periodic_cell_grid_and_scan(cuda, golden):
+    g = golden("xyz_golden.npz")
+    d = tempfile.mkdtemp(prefix="spm_lvec_")
+    fn = os.path.join(d, "cell.xyz")
+    with open(fn, "w") as f:
+        f.write(str(g["lvs_skew_text"]))
+    afm = AFMulator(use_morse=False)
+    afm.load_molecule(fn)
+    afm.assign_params()
+    afm.setup_grid_lvec(n=(60, 52, 230), margin_z=2.0, z_top=12.0)
+    afm.make_forcefield()
+    nx, ny, nz = (int(v) for v in afm.n)
+    grid = afm.img_FF.cpu().numpy()
+    ref = O.grid_build(0, afm.atoms_arr, afm.cLJs_arr, afm.n, afm.p0, afm.dA, afm.dB, afm.dC, afm.tipQs, afm.tipQZs,
+                       prec="f64")
+    scale = np.abs(ref).reshape(-1, 4).max(axis=0)
+    err = np.abs(grid.astype(np.float64) - ref)
+    assert not (err > 2e-5 * np.abs(ref) + 2e-6 * scale).any()
+    # a scan window of 9 x 8 A over a 6 A skew cell: the probes cross the periodic seam
+    nxy, nzs, dtip = (36, 32), 20, -0.1
+    p0 = np.array([-1.5, -1.0, 3.0 + afm.mol_z + 3.5], np.float32)
+    da = np.array([0.25, 0.0, 0.0], np.float32)
+    db = np.array([0.0, 0.25, 0.0], np.float32)
+    FEs, pts = afm.run_scan(nxy=nxy, nz=nzs, dtip=dtip, scan_p0=p0, scan_da=da, scan_db=db)
+    assert np.isfinite(FEs).all()
+    p4 = np.zeros((nxy[0] * nxy[1], 4), np.float32)
+    p4[:, :3] = pts.reshape(-1, 3)
+    tipC = afm.tipC.copy()
+    tipC[3] = dtip
+    o = O.relax_tilted(grid, (afm.dinvA, afm.dinvB, afm.dinvC), p4, nzs, afm.tipA, afm.tipB, tipC, afm.stiffness,
+                       afm.dpos0, afm.relax_pars, afm.surfFF, afm.n_relax_max, afm.f2conv)
+    assert np.array_equal(FEs.reshape(-1, nzs, 4), o)
+    # unrelaxed samples of a window shifted by one cell vector equal the unshifted ones (periodic field)
+    raw1, _ = afm.get_raw_FE(nxy=nxy, nz=nzs, dtip=dtip, scan_p0=p0, scan_da=da, scan_db=db)
+    raw2, _ = afm.get_raw_FE(nxy=nxy, nz=nzs, dtip=dtip, scan_p0=p0 + np.array([3.0, 5.196152, 0], np.float32),
+                             scan_da=da, scan_db=db)
+    assert np.abs(raw2 - raw1).max() < 1e-4 * np.abs(raw1).max()
