@@ -61,6 +61,7 @@ def lib():
         "ora_grid_build_d64": (None, [_i, _i, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _ll, _ll,
                                       _vp]),
         "ora_pair_fe_d": (None, [_i, _i, _vp, _vp, _i, _vp, _i, _vp, _vp, _vp]),
+        "ora_pair_fe_abs_d": (None, [_i, _i, _vp, _vp, _i, _vp, _i, _vp, _vp, _vp]),
         "ora_relax_strokes_f": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _i, _f, _i,
                                        _i, _i, _vp, _vp]),
         "ora_relax_strokes_d": (None, [_vp, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _i, _d, _i,
@@ -149,6 +150,20 @@ def pair_fe(kind, atoms, params, queries, Qs, QZs):
     qs, qz = _v4(Qs, np.float64), _v4(QZs, np.float64)
     lib().ora_pair_fe_d(int(kind), atoms.shape[0], _p(atoms), _p(params), pstride, _p(q), q.shape[0], _p(qs),
                         _p(qz), _p(out))
+    return out
+
+
+def pair_fe_abs(kind, atoms, params, queries, Qs, QZs):
+    """Per channel, the sum over atoms and tip-charge sites of |contribution| at (n,3) query points
+    (FP64, uncapped) -> (n,4): the cancellation scale of a grid value."""
+    atoms = np.ascontiguousarray(atoms, dtype=np.float64).reshape(-1, 4)
+    pstride = 2 if kind == 0 else 4
+    params = np.ascontiguousarray(params, dtype=np.float64).reshape(-1, pstride)
+    q = np.ascontiguousarray(queries, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros((q.shape[0], 4), dtype=np.float64)
+    qs, qz = _v4(Qs, np.float64), _v4(QZs, np.float64)
+    lib().ora_pair_fe_abs_d(int(kind), atoms.shape[0], _p(atoms), _p(params), pstride, _p(q), q.shape[0], _p(qs),
+                            _p(qz), _p(out))
     return out
 
 

@@ -164,6 +164,40 @@ void ora_pair_fe_d(int kind, int na, const double* atoms, const double* prm, int
     free(pr);
 }
 
+/* Sum over atoms (and tip-charge sites) of the ABSOLUTE value of each atom's
+ * contribution, per channel, at arbitrary query points, FP64: the scale of the
+ * cancellation in a grid value.  A floating-point sum of the contributions
+ * has an error proportional to this sum, not to |sum|; the grid-build tests
+ * state their FP32 tolerance against it. */
+void ora_pair_fe_abs_d(int kind, int na, const double* atoms, const double* prm, int pstride,
+                       const double* q, int nq, const double* Qs, const double* QZs, double* out) {
+    double qs[4];
+    for (int s = 0; s < 4; s++) qs[s] = Qs[s] * COULOMB_CONST;
+    double* pr = (double*)malloc(sizeof(double) * 4 * (size_t)(na > 0 ? na : 1));
+    for (int j = 0; j < na; j++)
+        for (int c = 0; c < 4; c++) pr[4 * j + c] = c < pstride ? prm[pstride * j + c] : 0;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nq; i++) {
+        v3_d p = mk3_d(q[3 * i], q[3 * i + 1], q[3 * i + 2]);
+        double acc[4] = {0, 0, 0, 0};
+        for (int j = 0; j < na; j++) {
+            const double* at = atoms + 4 * j;
+            double fe[4] = {0, 0, 0, 0};
+            if (kind == 0) acc_lj_d(fe, at, pr[4 * j], pr[4 * j + 1], p);
+            else acc_morse_d(fe, mk3_d(p.x - at[0], p.y - at[1], p.z - at[2]), pr[4 * j], pr[4 * j + 1], pr[4 * j + 2]);
+            for (int c = 0; c < 4; c++) acc[c] += fabs(fe[c]);
+            for (int s = 0; s < 4; s++) {
+                if (qs[s] == 0) continue;
+                double fc[4] = {0, 0, 0, 0};
+                acc_coulomb_d(fc, at, mk3_d(p.x, p.y, p.z + QZs[s]), qs[s]);
+                for (int c = 0; c < 4; c++) acc[c] += fabs(fc[c]);
+            }
+        }
+        for (int c = 0; c < 4; c++) out[4 * (size_t)i + c] = acc[c];
+    }
+    free(pr);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Stage (b): relaxation over strokes                                         */
 /* ------------------------------------------------------------------------ */

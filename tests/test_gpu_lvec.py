@@ -2,7 +2,8 @@
 839-893): a NaCl-like layer with a molecule in a 60-degree cell read by
 load_molecule from an .xyz with an "lvs" line (the fixture of
 tests/golden/xyz_golden.npz), LJ grid on the skew node lattice against the FP64
-oracle (grid-build tolerance: 2e-5 |ref| + 2e-6 max|ref|), and run_scan
+oracle (grid-build tolerance: 2e-5 |ref| + 2e-6 max|ref| + 1e-5 S, S the node's
+sum of contribution magnitudes), and run_scan
 (relaxStrokesTilted) over a window larger than the cell -- probes sample across
 the periodic seam through the skew sampling transform -- bit-identical to the
 canonical-FP32 oracle on the same grid; unrelaxed samples of a window shifted
@@ -35,9 +36,18 @@ def test_skew_periodic_cell_grid_and_scan(cuda, golden):
     grid = afm.img_FF.cpu().numpy()
     ref = O.grid_build(0, afm.atoms_arr, afm.cLJs_arr, afm.n, afm.p0, afm.dA, afm.dB, afm.dC, afm.tipQs, afm.tipQZs,
                        prec="f64")
-    scale = np.abs(ref).reshape(-1, 4).max(axis=0)
-    err = np.abs(grid.astype(np.float64) - ref)
-    assert not (err > 2e-5 * np.abs(ref) + 2e-6 * scale).any()
+    # node positions of the skew lattice, and each node's sum of contribution magnitudes S (FP32 sums err in
+    # proportion to S; the cell's +-0.8 e ions cancel)
+    iz, iy, ix = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    dA, dB, dC = (np.asarray(v, np.float64) for v in (afm.dA, afm.dB, afm.dC))
+    q = (ix[..., None] * dA[:3] + iy[..., None] * dB[:3] + iz[..., None] * dC[:3]).reshape(-1, 3)
+    a64, p64 = afm.atoms_arr.astype(np.float64), afm.cLJs_arr.astype(np.float64)
+    raw = O.pair_fe(0, a64, p64, q, afm.tipQs, afm.tipQZs)
+    S = O.pair_fe_abs(0, a64, p64, q, afm.tipQs, afm.tipQZs) * np.minimum(1.0, 100.0 / np.abs(raw[:, 3]))[:, None]
+    ref = ref.reshape(-1, 4)
+    scale = np.abs(ref).max(axis=0)
+    err = np.abs(grid.reshape(-1, 4).astype(np.float64) - ref)
+    assert not (err > 2e-5 * np.abs(ref) + 2e-6 * scale + 1e-5 * S).any()
     # a scan window of 9 x 8 A over a 6 A skew cell: the probes cross the periodic seam
     nxy, nzs, dtip = (36, 32), 20, -0.1
     p0 = np.array([-1.5, -1.0, 3.0 + afm.mol_z + 3.5], np.float32)
