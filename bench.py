@@ -43,7 +43,7 @@ EXEC_PAIR = {(0, True): (15, 23), (0, False): (13, 20), (1, True): (16, 23), (1,
 EXEC_SITE = (8, 13)
 # DRAM bytes of one grid_build_kernel launch on the 1200-atom / 480x480x240 workload, from the ncu
 # capture in profiles/grid_build_plain_large.md (dram__bytes_read.sum + dram__bytes_write.sum)
-GRID_BUILD_DRAM_BYTES = None
+GRID_BUILD_DRAM_BYTES = 6017024 + 826515456
 
 
 def parse():
@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--batch-only", action="store_true",
                     help="run only the many-molecule workloads (small sizes make profiling cases)")
     ap.add_argument("--no-tune", action="store_true", help="library default launch shapes, no autotuning")
+    ap.add_argument("--fit-cold", action="store_true",
+                    help="fit without the Newton polish and warm starts (every step relaxes from the strokes)")
     return ap.parse_args()
 
 
@@ -408,7 +410,9 @@ def run_ours(args, rank, world, local_rank):
     if dom == 0:
         roof = {"kernel": names[0], "bound": "fp32 pipe issue", "achieved": ach_pipe / 1e12,
                 "peak": fp32_peak / 1e12, "unit": "TFLOP/s", "frac": ach_pipe / fp32_peak,
-                "traffic": GRID_BUILD_DRAM_BYTES,
+                "traffic": GRID_BUILD_DRAM_BYTES if cfg.name == "plain_large" else None,
+                "traffic_note": "ncu dram__bytes_read.sum + write.sum of one launch (profiles/grid_build_plain_large.md); "
+                                "the grid it writes is 884.7 MB",
                 "peak_source": "measured live: FFMA-chain probe (spm_fp32_peak_probe) on this GPU",
                 "algorithmic": f"{cfg.pairs:.3e} (node,atom) pairs x {inst_pair} FP32 lane instructions as "
                                f"executed (FMA-equivalent: x2 flops)",
@@ -501,6 +505,46 @@ def _plain_images_per_s(items, probe):
                     "(numpy in/out), the same molecules as the fit, wall clock"}
 
 
+def _plain_gpu_ms_per_image(items, probe):
+    """GPU time of the per-image path's kernels alone: for every molecule, with its inputs resident on the
+    device, the full-grid build, the relaxation (relaxStrokes, the per-image kernels) and the amplitude df,
+    back to back on one stream, timed with CUDA events (no host work, no copies)."""
+    import torch
+    from spammm_b200 import _lib, gpu
+    from spammm_b200.AFM import AFMulator
+    dev = torch.device("cuda", torch.cuda.current_device())
+    work = []
+    for it in items:
+        L = np.array(it.ngrid) * it.step
+        dinv = AFMulator._make_dinv_axis_aligned(L, np.asarray(it.origin, np.float32), it.ngrid)
+        P = _lib.make_scan_params(dinv=dinv, dTip=[0, 0, -0.1, 0], stiffness=probe.stiffness, dpos0=probe.dpos0,
+                                  relax_params=probe.relax_params, nz=it.nz, max_iter=probe.max_iter,
+                                  f2conv=probe.f2conv, flip_z=True, raster_ny=len(it.ys))
+        gx, gy = np.meshgrid(it.xs, it.ys, indexing="ij")
+        pts = np.zeros((gx.size, 4), np.float32)
+        pts[:, 0], pts[:, 1], pts[:, 2] = gx.ravel(), gy.ravel(), it.z_top
+        s = it.step
+        vec = (np.array([*it.origin, 0], np.float32), np.array([s, 0, 0, 0], np.float32),
+               np.array([0, s, 0, 0], np.float32), np.array([0, 0, s, 0], np.float32))
+        work.append((it, P, torch.from_numpy(pts).to(dev), torch.from_numpy(it.atoms).to(dev),
+                     torch.from_numpy(it.params).to(dev), vec))
+
+    def run():
+        for it, P, pts, atoms, prm, (p0, dA, dB, dC) in work:
+            grid = gpu.grid_build(0, atoms, prm, it.ngrid, p0, dA, dB, dC, probe.tipQs, probe.tipQZs)
+            FEs, _ = gpu.relax_strokes(grid, P, pts)
+            gpu.df_amp_dir(FEs.view(len(it.xs), len(it.ys), it.nz, 4), (it.step, it.step, 0.1), (0., 0., 1.), 1.0)
+
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / len(items)
+
+
 def run_batched(args, dev_index):
     """Many-molecule workloads: (3) forward images of a 512-molecule batch,
     (4) 100 Adam steps of batched forward+adjoint fitting on 64 molecules."""
@@ -513,24 +557,29 @@ def run_batched(args, dev_index):
     # the per-image drop-in path on the same molecules first, on a device that holds no batch
     from spammm_b200.batch import ProbeSpec
     plain = _plain_images_per_s(items, ProbeSpec())
+    plain["gpu_kernel_ms_per_image"] = _plain_gpu_ms_per_image(items, ProbeSpec())
     torch.cuda.empty_cache()
+    polish, warm = not args.fit_cold, not args.fit_cold
     if args.no_tune:
         from spammm_b200 import _lib
         shape, tune_rep = _lib.lib().spm_batch_default_shape(), None
     else:
         # the fit (BatchAdam) reads the position and charge gradients only
-        shape, tune_rep = autotune.tuned_shape(items, max_molecules=args.fit_mols, reps=1, pair_param_grads=False)
+        shape, tune_rep = autotune.tuned_shape(items, max_molecules=args.fit_mols, reps=1, pair_param_grads=False,
+                                               polish=polish, warm=warm)
     rng = np.random.default_rng(11)
     pert = []
     for it in items:
         a = it.atoms.copy()
         a[:, :3] += rng.normal(0.0, 0.1, (len(a), 3)).astype(np.float32)
         pert.append(a)
-    b = AFMBatch(items, shape=shape)
+    b = AFMBatch(items, shape=shape).set_relax_options(polish=polish)
     for i, a in enumerate(pert):
         b.set_atoms(i, a)
     b.forward_adjoint()  # target 0: df_c is the perturbed structures' df
     target = b.df_c.clone()
+    b.set_relax_options(warm=warm)
+    b.reset_warm_start()
     start = torch.as_tensor(b.plan.atoms, device=b.atoms.device)
     truth = b.atoms.clone()
     b.atoms.copy_(start)
@@ -538,11 +587,13 @@ def run_batched(args, dev_index):
     b.enable_failure_mask()
     opt = BatchAdam(b, lr=0.01, cols=(0, 1, 2, 3))
     g = b.capture(opt.step, warmup=0)
+    b.reset_warm_start()
     b.forward_adjoint()
     loss0 = float(b.loss.sum())
     b.atoms.copy_(start)
     opt.reset()
     b.enable_failure_mask()
+    b.reset_warm_start()
     clk = ClockSampler(dev_index)
     clk.start()
     e0, e1 = _events()
@@ -563,6 +614,7 @@ def run_batched(args, dev_index):
         "workload": f"{args.fit_mols} molecules of the batch distribution, target df from N(0,0.1 A)-perturbed "
                     f"positions, {args.fit_steps} Adam steps (lr 0.01) on positions and charges from the "
                     "unperturbed structures, one CUDA-graph replay per step (forward + df loss + adjoint + update)",
+        "relax_options": {"newton_polish": polish, "warm_start": warm},
         "ms_per_step": ms, "images_per_s": args.fit_mols / (ms * 1e-3), "states_per_step": b.total_states,
         "loss_start": loss0, "loss_final": float(b.loss.sum()),
         "rmse_vs_unperturbed_A": rmse(b.atoms, start), "rmse_vs_target_structure_A": rmse(b.atoms, truth),
@@ -582,6 +634,8 @@ def run_batched(args, dev_index):
     out["fit"]["stage_ms"] = sr
     out["plain_per_image"] = plain
     out["fit"]["vs_plain_per_image"] = out["fit"]["images_per_s"] / out["plain_per_image"]["images_per_s"]
+    out["fit"]["vs_plain_gpu_kernels"] = plain["gpu_kernel_ms_per_image"] / (ms / args.fit_mols)
+    out["fit"]["fire_steps_per_state_last_step"] = float(b.iter_count.double().sum()) / b.total_states
     del g, b, opt
     torch.cuda.empty_cache()
     # ---- (3) forward images of a large batch in one graph

@@ -52,6 +52,13 @@ enum spm_status {
                                  opposite to the forward ones (SPM_FLAG_FLIP_Z inverted): the forward
                                  and reverse=True scans of AFMulator.scan_fdbm (AFM.py:584-633) in one
                                  launch; n_scan even */
+#define SPM_FLAG_WARM   16    /* spm_batch_relax only, with rx_sync = 1: PPs is read as well as written;
+                                 a z-step starts from the state's equilibrium in PPs (the previous
+                                 call's) when that converged and its displacement from the tip is
+                                 within 0.1 A per axis of the stroke continuation's start, else from
+                                 the continuation as without the flag (the probe jumped there, or no
+                                 previous equilibrium).  For fits whose atoms move a little per call;
+                                 with SPM_FLAG_POLISH both starts reach the same equilibrium */
 #define SPM_FLAG_POLISH 8     /* relaxations (not SPM_RELAX_2D): after FIRE stops, up to 4 Newton steps
                                  q <- q - J^-1 G on the total force G(q) of the interpolated grid and the
                                  spring (J = dG/dq, exact for the trilinear interpolant), each kept only
@@ -415,6 +422,8 @@ int spm_batch_grid_build(int kind, int n_mol, const spm_batch_mol* mols, long lo
  * `workspace` (>= spm_relax_workspace_bytes() bytes, reset by the call).
  * p: probe frame, spring, FIRE settings, flags, tipC[3] = z-step; its dinv*,
  * nz and raster_ny are ignored (per-molecule values come from mols).
+ * flags: SPM_FLAG_FIRE, SPM_FLAG_POLISH and SPM_FLAG_WARM (the last two with
+ * shape->rx_sync = 1).
  * FEs, PPs out (total_states,4); iter_count (total_pixels) or NULL. */
 int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n_slots, const spm_batch_shape* shape,
                     const float* grid, const float* points, const spm_scan_params* p,

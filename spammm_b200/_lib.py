@@ -34,6 +34,8 @@ SPM_FLAG_PAIRED = 4
 # Newton polish of every relaxed state (not in the reference): after FIRE stops, up to four Newton
 # steps on the total force of the interpolated grid and the spring; outputs at the polished position
 SPM_FLAG_POLISH = 8
+# batched relaxation: start each z-step from the previous call's equilibrium (PPs read and written)
+SPM_FLAG_WARM = 16
 SPM_ADJ_PAIR_PARAMS = 1
 
 _f4 = ctypes.c_float * 4
@@ -62,7 +64,7 @@ def f4(v):
 
 def make_scan_params(*, dinv=None, tipA=None, tipB=None, tipC=None, dTip=None, stiffness=None,
                      dpos0=None, relax_params=None, surfFF=None, nz=1, max_iter=128, f2conv=1e-8,
-                     fire=True, flip_z=False, raster_ny=0, paired=False, polish=False):
+                     fire=True, flip_z=False, raster_ny=0, paired=False, polish=False, warm=False):
     p = ScanParams()
     z4 = np.zeros(4, np.float32)
     if dinv is not None:
@@ -79,7 +81,7 @@ def make_scan_params(*, dinv=None, tipA=None, tipB=None, tipC=None, dTip=None, s
     p.max_iter = int(max_iter)
     p.f2conv = float(f2conv)
     p.flags = ((SPM_FLAG_FIRE if fire else 0) | (SPM_FLAG_FLIP_Z if flip_z else 0) | (SPM_FLAG_PAIRED if paired else 0)
-               | (SPM_FLAG_POLISH if polish else 0))
+               | (SPM_FLAG_POLISH if polish else 0) | (SPM_FLAG_WARM if warm else 0))
     p.raster_ny = int(raster_ny)
     return p
 

@@ -77,8 +77,13 @@ def sub_batch(items, max_molecules):
 
 def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
     """Tune batch.shape in place, stage by stage; returns (shape, timings).
-    max_grid_bytes: leave out slab layouts whose grid buffer would exceed it."""
+    max_grid_bytes: leave out slab layouts whose grid buffer would exceed it.  A batch relaxing
+    with the polish or warm starts (set_relax_options) is tuned over the z-synchronised schedules
+    only, the ones that support them; warm starts are timed cold (the relaxation of a fit step
+    lies between the two)."""
     report = {}
+    warm = batch.warm
+    batch.set_relax_options(warm=False)
     shape = batch.shape
 
     def pick(name, cands, run, prepare=None):
@@ -100,8 +105,9 @@ def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
     pick("grid", GRID_CANDIDATES, batch.build_grids)
     batch.set_shape(shape)
     batch.build_grids()
-    cands = RELAX_CANDIDATES if max_grid_bytes is None else [
-        c for c in RELAX_CANDIDATES if (4 if c["grid_layout"] else 2) * batch.grid_float4 * 16 <= max_grid_bytes]
+    cands = [c for c in RELAX_CANDIDATES if c["rx_sync"] == 1 or not (batch.polish or warm)]
+    if max_grid_bytes is not None:
+        cands = [c for c in cands if (4 if c["grid_layout"] else 2) * batch.grid_float4 * 16 <= max_grid_bytes]
     pick("relax", cands, batch.relax, prepare=batch.build_grids)
     if adjoint:
         batch.set_shape(shape)
@@ -110,17 +116,19 @@ def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
         batch.adjoint_state()
         pick("adjoint", ADJOINT_CANDIDATES, batch.adjoint_params)
     batch.set_shape(shape)
+    batch.set_relax_options(warm=warm)
     return shape, report
 
 
 def tuned_shape(items, kind=0, probe=None, dtip=-0.1, max_molecules=24, reps=2, adjoint=True, cache_file=None,
-                log=None, pair_param_grads=True):
+                log=None, pair_param_grads=True, polish=False, warm=False):
     """Best BatchShape for a workload, tuned on a sub-batch of at most
     max_molecules molecules (cached per device and workload signature).
     pair_param_grads: whether the adjoint is timed with the pair-parameter
-    columns (False for fits that read positions and charges only)."""
+    columns (False for fits that read positions and charges only); polish,
+    warm: the relaxation options the batch will run with (set_relax_options)."""
     dev = torch.cuda.get_device_name()
-    key = json.dumps([dev, signature(items, kind), bool(adjoint), bool(pair_param_grads)])
+    key = json.dumps([dev, signature(items, kind), bool(adjoint), bool(pair_param_grads), bool(polish), bool(warm)])
     if key not in _CACHE and cache_file and os.path.exists(cache_file):
         with open(cache_file) as f:
             _CACHE.update(json.load(f))
@@ -128,6 +136,7 @@ def tuned_shape(items, kind=0, probe=None, dtip=-0.1, max_molecules=24, reps=2, 
         return _lib.BatchShape(*_CACHE[key]["shape"]), _CACHE[key]["report"]
     sub = AFMBatch(sub_batch(items, max_molecules), kind=kind, probe=probe, dtip=dtip)
     sub.pair_param_grads = bool(pair_param_grads)
+    sub.set_relax_options(polish=polish, warm=warm)
     shape, report = tune(sub, reps=reps, adjoint=adjoint, log=log)
     del sub
     torch.cuda.empty_cache()

@@ -232,7 +232,8 @@ class AFMBatch:
         self.points = torch.as_tensor(plan.points, device=dev).contiguous()
         self.grid = None  # slabs: 2 (x-pairs) or 4 (xz-quads) float4 per node, allocated by set_shape
         self.FEs = torch.empty((so, 4), dtype=F32, device=dev)
-        self.PPs = torch.empty((so, 4), dtype=F32, device=dev)
+        # NaN: no previous equilibrium (a warm-started relaxation then starts every state from its stroke)
+        self.PPs = torch.full((so, 4), float("nan"), dtype=F32, device=dev)
         self.iter_count = torch.empty((po,), dtype=torch.int32, device=dev)
         self.df = torch.empty((so,), dtype=F32, device=dev)
         self.workspace = torch.zeros((max(1, int(lib().spm_relax_workspace_bytes()) // 4),), dtype=torch.int32,
@@ -245,12 +246,31 @@ class AFMBatch:
         self.loss = torch.empty((self.n,), dtype=F64, device=dev)
         self._Qs = hostvec(self.probe.tipQs)
         self._QZs = hostvec(self.probe.tipQZs)
+        self.polish = self.warm = False
+        self.set_relax_options()
+        self.shape = None
+        self.set_shape(shape if shape is not None else lib().spm_batch_default_shape())
+
+    def set_relax_options(self, polish=None, warm=None):
+        """polish: Newton-polish every equilibrium (SPM_FLAG_POLISH); warm: start each z-step from the
+        previous relaxation's equilibrium of the state (SPM_FLAG_WARM) -- for fits, whose atoms move a
+        little per step; with the polish both starts reach the same equilibrium.  Both need the
+        z-synchronised schedule (shape.rx_sync = 1).  The flags are read at launch time from the
+        scan-parameter struct held here, so a captured graph keeps the options it was captured with."""
+        if polish is not None:
+            self.polish = bool(polish)
+        if warm is not None:
+            self.warm = bool(warm)
         self.scan_params = _lib.make_scan_params(tipC=[0, 0, 1, self.dtip], stiffness=self.probe.stiffness,
                                                  dpos0=self.probe.dpos0, relax_params=self.probe.relax_params,
                                                  nz=0, max_iter=self.probe.max_iter, f2conv=self.probe.f2conv,
-                                                 fire=True)
-        self.shape = None
-        self.set_shape(shape if shape is not None else lib().spm_batch_default_shape())
+                                                 fire=True, polish=self.polish, warm=self.warm)
+        return self
+
+    def reset_warm_start(self):
+        """Forget the previous equilibria: the next warm-started relaxation starts every state from its
+        stroke (call after changing atoms by more than a fit step)."""
+        self.PPs.fill_(float("nan"))
 
     # ------------------------------------------------------------ planning
     def set_shape(self, shape):

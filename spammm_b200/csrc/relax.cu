@@ -718,9 +718,49 @@ batch_relax_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n
 // converges.  Each lane runs exactly the FIRE sequence of the other schedule
 // (pp_iter_z), so the results are the same bits.
 //
+// Cell fetcher of an axis-aligned batch slab for newton_polish: the same
+// addressing as interp_fe_cell, the eight texels unpacked to float4.
+template <int LAYOUT>
+struct SlabCellFetch {
+    const AxisView& G;
+    __device__ __forceinline__ bool operator()(V3 p, float& ax, float& ay, float& az, float4 (&t)[8]) const {
+        const float u = __fmaf_rn(p.x, G.ax, G.aw);
+        const float v = __fmaf_rn(p.y, G.by, G.bw);
+        const float w = __fmaf_rn(p.z, G.cz, G.cw);
+        int x0, x1, y0, y1, z0, z1;
+        bool ok = tex_axis(u, G.nx, G.fnx, x0, x1, ax);
+        ok = tex_axis(v, G.ny, G.fny, y0, y1, ay) && ok;
+        ok = tex_axis(w, G.nz, G.fnz, z0, z1, az) && ok;
+        ok = ok && to_slab(x0, x1, G.x_lo, G.nx_slab) && to_slab(y0, y1, G.y_lo, G.ny_slab) &&
+             to_slab(z0, z1, G.z_lo, G.nz_slab);
+        if (!ok) return false;
+        ulonglong2 c[8];
+        load_cell<LAYOUT, unsigned>(G, x0, y0, y1, z0, z1, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7]);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            upk(c[i].x, t[i].x, t[i].y);
+            upk(c[i].y, t[i].z, t[i].w);
+        }
+        return true;
+    }
+};
+
+// Warm start (SPM_FLAG_WARM): a z-step starts from the equilibrium the state
+// had in the previous call (PPs in) when that one converged and its
+// displacement from the tip differs by at most WARM_MAX_JUMP per axis from the
+// displacement the stroke continuation starts from (the previous z-step's end
+// position, shifted with the tip); otherwise -- the probe jumped between the
+// two z-steps in the previous call, or there is no previous equilibrium -- it
+// starts from the continuation as a cold call does, so every state stays on
+// its stroke's branch.
+constexpr float WARM_MAX_JUMP = 0.1f;
+
 // One lane's stroke of pixel k; every lane of `members` runs the same number
 // of z-steps (the molecule's nz_steps) and meets the others after each.
-template <bool CACHE, int LAYOUT>
+// POLISH: each z-step's equilibrium Newton-polished before it is stored (the
+// stroke continues from the unpolished position, as relax_pp_pixel and the
+// per-image kernels do).
+template <bool CACHE, int LAYOUT, bool POLISH>
 __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const float* __restrict__ grid,
                                                   const float4* __restrict__ pts, const spm_scan_params& P,
                                                   float4* __restrict__ FEs, float4* __restrict__ PPs,
@@ -732,6 +772,7 @@ __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const 
     const int pix = D->pix_off + k;
     const long long sbase = D->state_off + (long long)k * nzs;
     const float4 p4 = pts[pix];
+    const bool warm = (P.flags & SPM_FLAG_WARM) != 0;
     V3 tip = mk3(p4.x, p4.y, p4.z);
     V3 pos = mk3(tip.x + P.dpos0[0], tip.y + P.dpos0[1], tip.z + P.dpos0[2]);
     V3 v = mk3(0.f, 0.f, 0.f);
@@ -739,11 +780,30 @@ __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const 
     float4 fe = make_float4(0.f, 0.f, 0.f, 0.f);
     int total_it = 0;
     for (int iz = 0; iz < nzs; ++iz) {
+        if (warm) {
+            const float4 pw = PPs[sbase + iz];
+            const V3 dw = mk3(pw.x - tip.x, pw.y - tip.y, pw.z - tip.z);
+            const V3 dc = mk3(pos.x - tip.x, pos.y - tip.y, pos.z - tip.z);
+            if (pw.w > 0.f && fabsf(dw.x - dc.x) <= WARM_MAX_JUMP && fabsf(dw.y - dc.y) <= WARM_MAX_JUMP &&
+                fabsf(dw.z - dc.z) <= WARM_MAX_JUMP)  // false for NaN
+                pos = mk3(pw.x, pw.y, pw.z);
+        }
         int it = 0;
         bool conv;
         while (!pp_iter_z<unsigned, CACHE, LAYOUT>(G, T, P, tip, pos, v, dt, damp, fe, it, total_it, conv)) {
         }
         if (!conv) fe = sample_z<unsigned, CACHE, LAYOUT>(G, pos, T);  // the position moved after the last sample
+        V3 q = pos;
+        if constexpr (POLISH) {
+            PolishSpring S;
+            S.a = mk3(1.f, 0.f, 0.f); S.b = mk3(0.f, 1.f, 0.f); S.c = mk3(0.f, 0.f, 1.f);
+            S.kk = ld4(P.stiffness); S.d0 = ld4(P.dpos0);
+            S.surf = P.surfFF[0];
+            S.frame = true;
+            const float Tc[3][3] = {{__fmul_rn(G.fnx, G.ax), 0.f, 0.f}, {0.f, __fmul_rn(G.fny, G.by), 0.f},
+                                    {0.f, 0.f, __fmul_rn(G.fnz, G.cz)}};
+            if (fe.w == fe.w) newton_polish(SlabCellFetch<LAYOUT>{G}, Tc, S, tip, q, fe);
+        }
         const long long o = sbase + iz;
         FEs[o] = fe;
         // all seven values finite <=> the sum of their products with zero is zero
@@ -751,11 +811,11 @@ __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const 
         z0 = __fmaf_rn(fe.y, 0.f, z0);
         z0 = __fmaf_rn(fe.z, 0.f, z0);
         z0 = __fmaf_rn(fe.w, 0.f, z0);
-        z0 = __fmaf_rn(pos.x, 0.f, z0);
-        z0 = __fmaf_rn(pos.y, 0.f, z0);
-        z0 = __fmaf_rn(pos.z, 0.f, z0);
+        z0 = __fmaf_rn(q.x, 0.f, z0);
+        z0 = __fmaf_rn(q.y, 0.f, z0);
+        z0 = __fmaf_rn(q.z, 0.f, z0);
         const bool finite = (z0 == 0.f);
-        PPs[o] = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
+        PPs[o] = make_float4(q.x, q.y, q.z, (float)((conv && finite) ? it : -it));
         tip.z = __fadd_rn(tip.z, dz);
         pos.z = __fadd_rn(pos.z, dz);
         v = mk3(0.f, 0.f, 0.f);
@@ -764,7 +824,7 @@ __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const 
     if (iter_count) iter_count[pix] = total_it;
 }
 
-template <int MINB, bool CACHE, int LAYOUT>
+template <int MINB, bool CACHE, int LAYOUT, bool POLISH>
 __global__ void __launch_bounds__(MINB == 5 ? 128 : 256, MINB)
 batch_relax_sync_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
                         const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
@@ -782,7 +842,7 @@ batch_relax_sync_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsig
         int k;
         const bool valid = slot_pixel(D, base + lane - (unsigned)D->slot_off, th_log2, k);
         const unsigned members = __ballot_sync(0xffffffffu, valid);
-        if (valid) relax_tile_stroke<CACHE, LAYOUT>(D, grid, pts, P, FEs, PPs, iter_count, k, dz, members);
+        if (valid) relax_tile_stroke<CACHE, LAYOUT, POLISH>(D, grid, pts, P, FEs, PPs, iter_count, k, dz, members);
         __syncwarp();  // the whole warp draws the next tile
     }
 }
@@ -803,7 +863,8 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     SPM_REQUIRE(aligned16(grid) && aligned16(points) && aligned16(FEs) && aligned16(PPs) &&
                 (reinterpret_cast<uintptr_t>(workspace) & 3u) == 0 && (reinterpret_cast<uintptr_t>(mols) & 7u) == 0,
                 "spm_batch_relax: misaligned buffers");
-    SPM_REQUIRE((p->flags & ~(SPM_FLAG_FIRE | SPM_FLAG_FLIP_Z)) == 0, "spm_batch_relax: unknown flags 0x%x", p->flags);
+    SPM_REQUIRE((p->flags & ~(SPM_FLAG_FIRE | SPM_FLAG_FLIP_Z | SPM_FLAG_POLISH | SPM_FLAG_WARM)) == 0,
+                "spm_batch_relax: unknown flags 0x%x", p->flags);
     if (!(p->tipA[0] == 1.f && p->tipA[1] == 0.f && p->tipA[2] == 0.f && p->tipB[0] == 0.f && p->tipB[1] == 1.f &&
           p->tipB[2] == 0.f && p->tipC[0] == 0.f && p->tipC[1] == 0.f && p->tipC[2] == 1.f))
         return set_error(SPM_ERR_UNSUPPORTED, "spm_batch_relax: batches scan z-strokes: tipA,tipB,tipC must be x,y,z");
@@ -819,6 +880,9 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     SPM_REQUIRE(shape->grid_layout == 0 || shape->grid_layout == 1, "spm_batch_relax: grid_layout=%d",
                 shape->grid_layout);
     SPM_REQUIRE(shape->rx_sync == 0 || shape->rx_sync == 1, "spm_batch_relax: rx_sync=%d", shape->rx_sync);
+    if (p->flags & (SPM_FLAG_POLISH | SPM_FLAG_WARM))
+        SPM_REQUIRE(shape->rx_sync == 1, "spm_batch_relax: SPM_FLAG_POLISH / SPM_FLAG_WARM need the z-synchronised "
+                    "schedule (rx_sync = 1)");
     using Kern = decltype(&batch_relax_kernel<3, false, 2>);
     // [rx_sync][grid_layout][rx_regs]: 0 = 80 registers, 1 = 64, 2 = texel cache at up to 128,
     // 3 = texel cache squeezed to 80 (some values spilled, 50% more warps), 4 = texel cache at up to 102
@@ -828,12 +892,22 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
           batch_relax_kernel<3, true, 2>, batch_relax_kernel<5, true, 2>},
          {batch_relax_kernel<3, false, 4>, batch_relax_kernel<4, false, 4>, batch_relax_kernel<2, true, 4>,
           batch_relax_kernel<3, true, 4>, batch_relax_kernel<5, true, 4>}},
-        {{batch_relax_sync_kernel<3, false, 2>, batch_relax_sync_kernel<4, false, 2>,
-          batch_relax_sync_kernel<2, true, 2>, batch_relax_sync_kernel<3, true, 2>, batch_relax_sync_kernel<5, true, 2>},
-         {batch_relax_sync_kernel<3, false, 4>, batch_relax_sync_kernel<4, false, 4>,
-          batch_relax_sync_kernel<2, true, 4>, batch_relax_sync_kernel<3, true, 4>,
-          batch_relax_sync_kernel<5, true, 4>}}};
-    const Kern kern = table[shape->rx_sync][shape->grid_layout][shape->rx_regs];
+        {{batch_relax_sync_kernel<3, false, 2, false>, batch_relax_sync_kernel<4, false, 2, false>,
+          batch_relax_sync_kernel<2, true, 2, false>, batch_relax_sync_kernel<3, true, 2, false>,
+          batch_relax_sync_kernel<5, true, 2, false>},
+         {batch_relax_sync_kernel<3, false, 4, false>, batch_relax_sync_kernel<4, false, 4, false>,
+          batch_relax_sync_kernel<2, true, 4, false>, batch_relax_sync_kernel<3, true, 4, false>,
+          batch_relax_sync_kernel<5, true, 4, false>}}};
+    // the polished z-synchronised variants, [grid_layout][rx_regs]
+    static const Kern polished[2][5] = {
+        {batch_relax_sync_kernel<3, false, 2, true>, batch_relax_sync_kernel<4, false, 2, true>,
+         batch_relax_sync_kernel<2, true, 2, true>, batch_relax_sync_kernel<3, true, 2, true>,
+         batch_relax_sync_kernel<5, true, 2, true>},
+        {batch_relax_sync_kernel<3, false, 4, true>, batch_relax_sync_kernel<4, false, 4, true>,
+         batch_relax_sync_kernel<2, true, 4, true>, batch_relax_sync_kernel<3, true, 4, true>,
+         batch_relax_sync_kernel<5, true, 4, true>}};
+    const Kern kern = (p->flags & SPM_FLAG_POLISH) ? polished[shape->grid_layout][shape->rx_regs]
+                                                   : table[shape->rx_sync][shape->grid_layout][shape->rx_regs];
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||

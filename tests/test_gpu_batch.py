@@ -333,3 +333,68 @@ def test_autotune_returns_valid_shape(cuda):
     b.forward()
     torch.cuda.synchronize()
     assert torch.equal(ref.FEs, b.FEs) and torch.equal(ref.PPs, b.PPs)
+
+
+def test_batch_polished_relaxation_matches_per_molecule(cuda):
+    """SPM_FLAG_POLISH in the batched (z-synchronised) relaxation: every molecule bit-identical to the
+    per-molecule relax_pp with the polish, for both slab layouts and both register variants of the default
+    tile shape; the polish moves the equilibria and lowers the residual."""
+    items = _items(0, n=4, seed=61)
+    base = _lib.lib().spm_batch_default_shape()
+    for layout, regs in ((0, 4), (1, 2), (0, 0)):
+        shape = _lib.BatchShape(*base.key())
+        shape.grid_layout, shape.rx_regs, shape.rx_sync = layout, regs, 1
+        b = AFMBatch(items, shape=shape).set_relax_options(polish=True)
+        b.forward()
+        torch.cuda.synchronize()
+        for i, it in enumerate(b.items):
+            spec = it.spec(b.kind, b.probe, b.dtip)
+            spec.polish = True
+            p0, dA, dB, dC = spec.vectors()
+            grid = gpu.grid_build(b.kind, it.atoms.astype(np.float32), it.params.astype(np.float32), spec.ngrid, p0,
+                                  dA, dB, dC, spec.tipQs, spec.tipQZs)
+            P = spec.scan_params(b.probe.stiffness)
+            FEs, PPs = gpu.relax_pp(grid, P, torch.as_tensor(spec.points, device="cuda"))
+            assert torch.equal(b.fes(i), FEs) and torch.equal(b.pps(i), PPs), (layout, regs, i)
+
+
+def test_batch_warm_start_reaches_the_cold_equilibria(cuda):
+    """SPM_FLAG_WARM with the polish: after the atoms move by ~5e-3 A (an Adam step of the fit is <= 0.01 A),
+    a relaxation started from the previous equilibria reaches the equilibria of a cold start to the float32
+    floor, in fewer FIRE steps; a warm start with no previous equilibria (NaN) is the cold relaxation."""
+    items = _items(0, n=4, seed=62)
+    b = AFMBatch(items).set_relax_options(polish=True, warm=True)
+    b.forward()  # PPs NaN: every state starts from its stroke
+    cold = AFMBatch(items).set_relax_options(polish=True)
+    cold.forward()
+    torch.cuda.synchronize()
+    assert torch.equal(b.PPs, cold.PPs) and torch.equal(b.FEs, cold.FEs)
+    it_cold0 = int(cold.iter_count.sum())
+    rng = np.random.default_rng(3)
+    moved = b.atoms.clone()
+    moved[:, :3] += torch.as_tensor(rng.normal(0, 5e-3, (b.total_atoms, 3)), dtype=moved.dtype, device="cuda")
+    b.atoms.copy_(moved)
+    cold.atoms.copy_(moved)
+    b.forward()
+    cold.forward()
+    torch.cuda.synchronize()
+    ok = (b.PPs[:, 3] > 0) & (cold.PPs[:, 3] > 0)
+    assert float(ok.float().mean()) > 0.99
+    dq = (b.PPs[ok, :3] - cold.PPs[ok, :3]).abs().max(dim=1).values
+    print(f"\nwarm vs cold polished equilibria: max |dq| {float(dq.max()):.2e} A, 99.9% below "
+          f"{float(torch.quantile(dq.float(), 0.999)):.2e} A; FIRE steps warm {int(b.iter_count.sum())} vs cold "
+          f"{int(cold.iter_count.sum())} (first cold {it_cold0})")
+    assert float(torch.quantile(dq.float(), 0.999)) < 1e-4
+    assert int(b.iter_count.sum()) < 0.6 * int(cold.iter_count.sum())
+    b.reset_warm_start()
+    assert bool(torch.isnan(b.PPs).all())
+
+
+def test_batch_polish_and_warm_need_the_synchronised_schedule(cuda):
+    items = _items(0, n=2, seed=63)
+    shape = _lib.BatchShape(*_lib.lib().spm_batch_default_shape().key())
+    shape.rx_sync = 0
+    b = AFMBatch(items, shape=shape).set_relax_options(polish=True)
+    b.build_grids()
+    with pytest.raises((ValueError, RuntimeError), match="rx_sync"):
+        b.relax()
