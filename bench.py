@@ -158,6 +158,22 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(ms, world, device=None):
+    """The largest per-rank duration over all ranks (every rank receives it); the timed region of a
+    replica run ends when its slowest rank ends."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank, ms_per_step, world):
+    """Whole-job throughput of `world` replicas, each processing units_per_rank per step."""
+    return world * units_per_rank / (ms_per_step * 1e-3)
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -322,15 +338,11 @@ def run_ours(args, rank, world, local_rank):
     t1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms_total = t0.elapsed_time(t1)
+    ms_total = max_over_ranks(t0.elapsed_time(t1), world, dev)
     stage /= args.steps
-    if world > 1:
-        t = torch.tensor([ms_total], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_total = float(t.item())
     ms_step = ms_total / args.steps
     # the events above wrap each stage; the sum of stages is the kernel time of a step (host syncs excluded)
-    value = world * cfg.pxz / (ms_step * 1e-3)
+    value = replica_value(cfg.pxz, ms_step, world)
     out = {}
     # FIRE telemetry (outside the timed region): integrator steps per px*z
     cnt = torch.empty(cfg.n_pix, dtype=torch.int32, device=dev)
@@ -375,14 +387,10 @@ def run_ours(args, rank, world, local_rank):
             F, disp, df_h = e2e_step()
         a1.record(stream)
         torch.cuda.synchronize()
-        ms_e = a0.elapsed_time(a1)
-        if world > 1:
-            t = torch.tensor([ms_e], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms_e = float(t.item())
+        ms_e = max_over_ranks(a0.elapsed_time(a1), world, dev)
         h2d = cfg.atoms.nbytes + cfg.params.nbytes + cfg.n_pix * 16 + F.nbytes  # atoms, params, points, FEs for df
         d2h = F.nbytes + 3 * F[..., 0].nbytes + df_h.nbytes  # FEs, tip displacement, df
-        e2e = {"value": world * cfg.pxz / (ms_e / ke * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        e2e = {"value": replica_value(cfg.pxz, ms_e / ke, world), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e / ke,
                "path": "AFMulator.setup_grid_world/make_forcefield/scan_fdbm + compute_df_amp_dir (numpy in/out)"}
 
