@@ -57,8 +57,11 @@ enum spm_status {
                                  call's) when that converged and its displacement from the tip is
                                  within 0.1 A per axis of the stroke continuation's start, else from
                                  the continuation as without the flag (the probe jumped there, or no
-                                 previous equilibrium).  For fits whose atoms move a little per call;
-                                 with SPM_FLAG_POLISH both starts reach the same equilibrium */
+                                 previous equilibrium).  For fits whose atoms move a little per call.
+                                 With SPM_FLAG_POLISH a warm-started z-step first takes the polish's
+                                 Newton steps from the previous equilibrium and runs FIRE only if they
+                                 do not reach |F|^2 < f2conv (PPs.w then counts the Newton
+                                 evaluations); both starts reach the same equilibrium */
 #define SPM_FLAG_POLISH 8     /* relaxations (not SPM_RELAX_2D): after FIRE stops, up to 4 Newton steps
                                  q <- q - J^-1 G on the total force G(q) of the interpolated grid and the
                                  spring (J = dG/dq, exact for the trilinear interpolant), each kept only
@@ -151,6 +154,25 @@ long long spm_relax_workspace_bytes(void);
 int spm_relax_ex(int mode, const float* grid, int nx, int ny, int nz,
                  const float* points, int n_scan, const spm_scan_params* p,
                  float* FEs, float* disps, int* iter_count, void* workspace, void* stream);
+
+/* The forward + reverse=True scan_fdbm pair and compute_dissipation in ONE
+ * launch (spammm/SPM/AFM.py:584-633 twice, then AFM.py:3238-3277; no single
+ * counterpart in the reference): spm_relax_ex(SPM_RELAX_STROKES) with
+ * SPM_FLAG_PAIRED (required; n_scan even, pixel p's strokes are points p and
+ * p + n_scan/2), and per pixel E_diss[p, o] = |trapz over the stored heights
+ * idx[off[o]..off[o+1]) of (FE_fwd - FE_bwd).n| with abscissae h_scan
+ * (DEVICE double[p->nz], in the stored z order) -- the arithmetic of
+ * spm_dissipation, bit for bit.  The lane that finishes the second stroke of
+ * a pixel integrates it, reading both strokes' FEs back from L2; no lane
+ * waits.  n: HOST double[3] (normalised here); off (DEVICE int[n_out+1]), idx
+ * (DEVICE int[]); E_diss out (n_scan/2, n_out) float32; FEs, disps, iter_count
+ * as spm_relax_ex.  workspace: DEVICE, 16-byte aligned, >=
+ * spm_relax_pair_workspace_bytes(n_scan) bytes (reset by the call). */
+int spm_relax_pair_dissipation(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
+                               const spm_scan_params* p, float* FEs, float* disps, int* iter_count,
+                               const double* n, const double* h_scan, const int* off, const int* idx,
+                               int n_out, float* E_diss, void* workspace, void* stream);
+long long spm_relax_pair_workspace_bytes(int n_scan);
 
 /* Replaces AFMulator.run_scan -> relaxStrokesTilted (spammm/SPM/AFM.py:950-1010,
  * kernels/AFM.cl:478-562): tip-frame spring, surface bias, re-sampled FE after

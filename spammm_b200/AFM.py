@@ -338,7 +338,7 @@ class AFMulator:
 
     def scan_fdbm_pair(self, scan_xs, scan_ys, probe_heights, mol_z=0.0, ppm_mode=True, use_fire=True,
                        K_LAT=0.03, K_RAD=20.0, bond_length=3.0, stiffness=None, dpos0=None, relax_pars=None,
-                       osc_dir=(0., 0., 1.), base_pos=(0., 0., 0.), return_device=False):
+                       osc_dir=(0., 0., 1.), base_pos=(0., 0., 0.), return_device=False, dissipation=None):
         """The forward and the backward (reverse=True) strokes of scan_fdbm in
         one relaxation launch (SPM_FLAG_PAIRED), as run_morse_pp_afm and
         run_fdbm_pp_from_density (AFM_utils.py:3537-3553, 4091-4108) take them
@@ -346,7 +346,11 @@ class AFMulator:
         calls, so the results are theirs bit for bit.
 
         Returns ((FEs_fwd, tip_disp_fwd), (FEs_bwd, tip_disp_bwd)), both with
-        iz=0 the lowest height, as two scan_fdbm calls return them."""
+        iz=0 the lowest height, as two scan_fdbm calls return them.
+        dissipation=(h_scan, h_df, amp): also compute_dissipation(FEs_fwd,
+        FEs_bwd, h_scan, h_df, amp, osc_dir) in the same launch (the lane that
+        finishes a pixel's second stroke integrates it; spm_dissipation's
+        arithmetic, bit for bit) and return it third, (nx, ny, len(h_df))."""
         base, stiffness_v, dpos0_v, relax_pars_v = self._scan_fdbm_setup(osc_dir, base_pos, use_fire, K_LAT, K_RAD,
                                                                          bond_length, stiffness, dpos0, relax_pars)
         nx_s, ny_s, nz_s = len(scan_xs), len(scan_ys), len(probe_heights)
@@ -360,10 +364,17 @@ class AFMulator:
                                stiffness=stiffness_v, dpos0=dpos0_v, relax_params=relax_pars_v, nz=nz_s,
                                flip_z=True, raster_ny=ny_s, paired=True)
         pts = torch.from_numpy(np.concatenate([pts_f, pts_b])).to(self.device)
-        FEs, disps = gpu.relax_strokes(self.img_FF_fdbm, P, pts)
         shape = (nx_s, ny_s, nz_s)
+        if dissipation is None:
+            FEs, disps = gpu.relax_strokes(self.img_FF_fdbm, P, pts)
+            return (self._scan_outputs(FEs[:n_scan], disps[:n_scan], shape, return_device),
+                    self._scan_outputs(FEs[n_scan:], disps[n_scan:], shape, return_device))
+        h_scan, h_df, amp = dissipation
+        FEs, disps, E = gpu.relax_pair_dissipation(self.img_FF_fdbm, P, pts, h_scan, h_df, amp, osc_dir)
+        E = E.view(nx_s, ny_s, -1)
         return (self._scan_outputs(FEs[:n_scan], disps[:n_scan], shape, return_device),
-                self._scan_outputs(FEs[n_scan:], disps[n_scan:], shape, return_device))
+                self._scan_outputs(FEs[n_scan:], disps[n_scan:], shape, return_device),
+                E if return_device else gpu.to_host(E))
 
     def _scan_fdbm_setup(self, osc_dir, base_pos, use_fire, K_LAT, K_RAD, bond_length, stiffness, dpos0,
                          relax_pars):

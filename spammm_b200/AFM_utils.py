@@ -88,11 +88,13 @@ def _nearest_indices(h_scan, h_sel):
 
 
 def shared_postprocess(FEs_full, scan_spec, *, FEs_bwd=None, tip_disp=None, backend_name="unknown", fft_path="none",
-                       return_device=False):
+                       return_device=False, E_diss=None):
     """df / Fz / E_diss from a relaxed (nx,ny,nz_scan,4) volume (AFM_utils.py:3363-3414).
 
     ``FEs_full`` / ``FEs_bwd`` may be CUDA tensors (kept on the device) or
-    host arrays.  df is evaluated on the GPU only at the h_df slices."""
+    host arrays.  df is evaluated on the GPU only at the h_df slices.
+    E_diss: the dissipation already integrated (the paired relaxation's fused
+    epilogue, scan_fdbm_pair(dissipation=...)); then FEs_bwd is not read."""
     on_dev = isinstance(FEs_full, torch.Tensor)
     F = FEs_full if on_dev else np.asarray(FEs_full, dtype=np.float32)
     nx, ny, nz_scan = (int(s) for s in F.shape[:3])
@@ -106,7 +108,9 @@ def shared_postprocess(FEs_full, scan_spec, *, FEs_bwd=None, tip_disp=None, back
     df = gpu.df_amp_dir(F, (sx, sy, sz), osc_n, float(scan_spec.amplitude), out_iz=idx_df)
     Fv = F if on_dev else torch.from_numpy(F).to(df.device)
     Fz = Fv[..., 2][:, :, idx_Fz]
-    if FEs_bwd is not None:
+    if E_diss is not None:
+        E_diss = E_diss if isinstance(E_diss, torch.Tensor) else torch.as_tensor(np.asarray(E_diss), device=df.device)
+    elif FEs_bwd is not None:
         E_diss = gpu.dissipation(Fv, FEs_bwd, scan_spec.h_scan, scan_spec.h_df, float(scan_spec.amplitude), osc_n)
     else:
         E_diss = torch.zeros((nx, ny, len(scan_spec.h_df)), dtype=torch.float32, device=df.device)
@@ -236,16 +240,17 @@ def run_morse_pp_afm(tag, atomPos, atomTypes, origin, step, ngrid, outdir=None, 
     kw = dict(mol_z=mol_z, K_LAT=float(scan_spec.K_LAT), K_RAD=float(scan_spec.K_RAD),
               bond_length=float(scan_spec.bond_length), ppm_mode=True, use_fire=True, osc_dir=scan_spec.osc_dir,
               base_pos=(0., 0., 0.), return_device=True)
-    # forward and backward strokes in one relaxation launch (the reference's two scan_fdbm calls)
-    (FEs_full, tip_disp_full), (FEs_bwd_full, _) = afmulator.scan_fdbm_pair(scan_xs_full, scan_ys_full, h_scan,
-                                                                            **kw)
+    # forward and backward strokes and their dissipation in one relaxation launch (the reference's two
+    # scan_fdbm calls and compute_dissipation)
+    (FEs_full, tip_disp_full), (FEs_bwd_full, _), E_full = afmulator.scan_fdbm_pair(
+        scan_xs_full, scan_ys_full, h_scan, dissipation=(scan_spec.h_scan, scan_spec.h_df, float(scan_spec.amplitude)),
+        **kw)
     sx = slice(pad_x, pad_x + len(scan_xs))
     sy = slice(pad_y, pad_y + len(scan_ys))
     FEs = FEs_full[sx, sy].contiguous()
-    FEs_bwd = FEs_bwd_full[sx, sy].contiguous()
     tip_disp = {k: gpu.to_host(v[sx, sy]) for k, v in tip_disp_full.items()}
-    result = shared_postprocess(FEs, scan_spec, FEs_bwd=FEs_bwd, tip_disp=tip_disp, backend_name="morse",
-                                fft_path="none")
+    result = shared_postprocess(FEs, scan_spec, tip_disp=tip_disp, backend_name="morse", fft_path="none",
+                                E_diss=E_full[sx, sy].contiguous())
     result.tag = tag
     result.atomPos = atomPos
     result.origin = origin

@@ -145,6 +145,9 @@ _SIGNATURES = {
     "spm_df_amp_dir": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _d, _vp, _i, _vp, _vp]),
     "spm_df_dir": (_i, [_vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp]),
     "spm_dissipation": (_i, [_vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp]),
+    "spm_relax_pair_dissipation": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp,
+                                        _vp, _vp]),
+    "spm_relax_pair_workspace_bytes": (_ll, [_i]),
     "spm_convolve_z": (_i, [_vp, _i, _i, _i, _vp, _vp, _vp]),
     "spm_izo_z": (_i, [_vp, _i, _i, ctypes.c_float, _vp, _vp]),
     "spm_df_loss_seed": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _d, _vp, _vp, _vp, _vp, _vp]),

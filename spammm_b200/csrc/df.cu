@@ -16,6 +16,7 @@
 // the reference fixtures' tolerance).  Compiled with -fmad=false so the FP64
 // expression order otherwise matches NumPy's.
 #include "spm_internal.cuh"
+#include "spm_diss.cuh"
 #include "spm_batch.cuh"
 #include <cmath>
 #include <vector>
@@ -264,7 +265,22 @@ struct DissGeom {
     double n[3];
 };
 
-// |sum_j (x[j+1]-x[j]) * (y[j] + y[j+1]) / 2| over the masked heights.
+// |sum_j (x[j+1]-x[j]) * (y[j] + y[j+1]) / 2| over the masked heights.  Float
+// volumes use spm_diss.cuh's diss_value (shared with the fused epilogue of the
+// paired relaxation in relax.cu): the same operations, as written below.
+__global__ void __launch_bounds__(DF_THREADS)
+dissipation_f32_kernel(const float4* __restrict__ Ff, const float4* __restrict__ Fb, DissGeom P,
+                       const double* __restrict__ h, const int* __restrict__ off, const int* __restrict__ idx,
+                       float* __restrict__ E) {
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)P.nx * P.ny * P.n_out;
+    if (gid >= total) return;
+    const int o = (int)(gid % P.n_out);
+    const long long pix = gid / P.n_out;
+    const double n[3] = {P.n[0], P.n[1], P.n[2]};
+    E[gid] = diss_value(Ff, Fb, (size_t)pix * P.nz, P.nz, n, h, off, idx, o, LdgLoad{});
+}
+
 template <typename T>
 __global__ void __launch_bounds__(DF_THREADS)
 dissipation_kernel(const T* __restrict__ Ff, const T* __restrict__ Fb, DissGeom P,
@@ -481,9 +497,8 @@ extern "C" int spm_dissipation(const void* FEs_fwd, const void* FEs_bwd, int fes
     if (total == 0) return SPM_OK;
     const unsigned nb = (unsigned)((total + DF_THREADS - 1) / DF_THREADS);
     if (fes_dtype == SPM_F32)
-        dissipation_kernel<<<nb, DF_THREADS, 0, as_stream(stream)>>>(static_cast<const float*>(FEs_fwd),
-                                                                     static_cast<const float*>(FEs_bwd), P, h_scan,
-                                                                     off, idx, E_diss);
+        dissipation_f32_kernel<<<nb, DF_THREADS, 0, as_stream(stream)>>>(
+            static_cast<const float4*>(FEs_fwd), static_cast<const float4*>(FEs_bwd), P, h_scan, off, idx, E_diss);
     else
         dissipation_kernel<<<nb, DF_THREADS, 0, as_stream(stream)>>>(static_cast<const double*>(FEs_fwd),
                                                                      static_cast<const double*>(FEs_bwd), P, h_scan,

@@ -27,6 +27,7 @@
 #include "spm_internal.cuh"
 #include "spm_fire.cuh"
 #include "spm_batch.cuh"
+#include "spm_diss.cuh"
 
 namespace spm {
 namespace {
@@ -335,6 +336,20 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
     }
 }
 
+// The dissipation integral fused into the paired relaxation (spm_relax_pair_dissipation): the
+// strokes of pixel p are p (forward) and p + n_scan/2 (backward); the lane that finishes the
+// second of the two (a per-pixel atomic counter decides, no lane waits) integrates E_diss of the
+// pixel from both strokes' FEs as spm_dissipation does (spm_diss.cuh: the same bits).
+struct DissArgs {
+    const double* h;     // abscissae of the stored z order (DEVICE double[nz])
+    const int* off;      // per output: idx[off[o]..off[o+1]) (DEVICE int[n_out+1])
+    const int* idx;      // height indices (DEVICE)
+    float* E;            // (n_scan/2, n_out)
+    int* pair;           // per pixel: strokes finished (zeroed by the launch)
+    int n_out;
+    double n[3];         // oscillation direction (normalised)
+};
+
 // MODE 0-2 (relaxStrokes, relaxStrokesTilted, PP) under the z-synchronised
 // tile schedule: a warp draws the 32 pixels of one 4 (ix) x 8 (iy) raster tile
 // (32 consecutive pixels without a raster) from the device counter, and its
@@ -346,11 +361,12 @@ relax_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_pa
 // lanes of a warp run that code together: 3.81 -> 2.30 ms on that scan.  The
 // per-lane sequence is relax_kernel's (the same iteration, emit and texel
 // cache), so the results are the same bits.
-template <int MODE, typename IDX, bool POLISH>
+template <int MODE, typename IDX, bool POLISH, bool DISS = false>
 __global__ void __launch_bounds__(RX_THREADS)
 relax_tile_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_scan_params P,
                   float4* __restrict__ FEs, float4* __restrict__ disps, int* __restrict__ iter_count,
-                  unsigned* __restrict__ counter) {
+                  unsigned* __restrict__ counter, DissArgs DA = DissArgs{}) {
+    static_assert(!DISS || MODE == 0, "the fused dissipation is for relaxStrokes pairs");
     static_assert(MODE >= 0 && MODE <= 2, "relaxStrokes2D keeps the flattened loop");
     const unsigned lane = threadIdx.x & 31u;
     const float fnx = (float)G.nx, fny = (float)G.ny, fnz = (float)G.nz;
@@ -458,6 +474,19 @@ relax_tile_kernel(GridView G, const float4* __restrict__ pts, int n_scan, spm_sc
                 __syncwarp(members);  // the tile's lanes start the next z-step together
             }
             if (iter_count) iter_count[k] = total_it;
+            if constexpr (DISS) {
+                // publish this stroke's FEs, then count it; the second stroke of the pixel integrates
+                const int pix = k < half ? k : k - half;
+                __threadfence();
+                if (atomicAdd(DA.pair + pix, 1) == 1) {
+                    __threadfence();
+                    const float4* Ff = FEs;
+                    const float4* Fb = FEs + (size_t)half * nzs;
+                    for (int o = 0; o < DA.n_out; o++)
+                        DA.E[(size_t)pix * DA.n_out + o] =
+                            diss_value(Ff, Fb, (size_t)pix * nzs, nzs, DA.n, DA.h, DA.off, DA.idx, o, CgLoad{});
+                }
+            }
         }
         __syncwarp();  // the whole warp draws the next tile
     }
@@ -527,28 +556,42 @@ spm_scan_params normalized(const spm_scan_params* p, int n_scan) {
     return P;
 }
 
+// Persistent grid size of a counter-scheduled relaxation kernel: as many CTAs as are co-resident
+// (the counter balances the rest).
+template <class K>
+int persistent_blocks(K kern, int n_scan, int& blocks) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RX_THREADS, 0) != cudaSuccess)
+        return set_error(SPM_ERR_CUDA, "relax: cannot query the device occupancy");
+    const int cap = sms * (per_sm > 0 ? per_sm : 1);
+    const int need = (n_scan + RX_THREADS - 1) / RX_THREADS;
+    blocks = need < cap ? need : cap;
+    return SPM_OK;
+}
+
 template <int MODE, typename IDX, bool POLISH>
 int launch_relax(const GridView& G, const float4* pts, int n_scan, const spm_scan_params& P, float4* FEs,
                  float4* disps, int* iter_count, unsigned* counter, cudaStream_t st) {
-    auto kern = relax_kernel<MODE, IDX, (MODE <= 2), POLISH>;
-    if constexpr (MODE <= 2) {
-        if (counter) kern = relax_tile_kernel<MODE, IDX, POLISH>;  // z-synchronised tiles from the counter
-    }
-    int blocks = static_blocks(n_scan, P);
     if (counter) {
-        // persistent: as many CTAs as are co-resident; the counter balances the rest
-        int dev = 0, sms = 0, per_sm = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RX_THREADS, 0) != cudaSuccess)
-            return set_error(SPM_ERR_CUDA, "relax: cannot query the device occupancy");
-        const int cap = sms * (per_sm > 0 ? per_sm : 1);
-        const int need = (n_scan + RX_THREADS - 1) / RX_THREADS;
-        blocks = need < cap ? need : cap;
         if (cudaMemsetAsync(counter, 0, sizeof(unsigned), st) != cudaSuccess)
             return set_error(SPM_ERR_CUDA, "relax: cannot reset the pixel counter");
+        if constexpr (MODE <= 2) {  // z-synchronised tiles from the counter
+            auto kern = relax_tile_kernel<MODE, IDX, POLISH, false>;
+            int blocks = 0;
+            if (int rc = persistent_blocks(kern, n_scan, blocks)) return rc;
+            kern<<<blocks, RX_THREADS, 0, st>>>(G, pts, n_scan, P, FEs, disps, iter_count, counter, DissArgs{});
+            return check_launch("relax");
+        }
+        auto kern = relax_kernel<MODE, IDX, (MODE <= 2), POLISH>;
+        int blocks = 0;
+        if (int rc = persistent_blocks(kern, n_scan, blocks)) return rc;
+        kern<<<blocks, RX_THREADS, 0, st>>>(G, pts, n_scan, P, FEs, disps, iter_count, counter);
+        return check_launch("relax");
     }
-    kern<<<blocks, RX_THREADS, 0, st>>>(G, pts, n_scan, P, FEs, disps, iter_count, counter);
+    relax_kernel<MODE, IDX, (MODE <= 2), POLISH><<<static_blocks(n_scan, P), RX_THREADS, 0, st>>>(
+        G, pts, n_scan, P, FEs, disps, iter_count, counter);
     return check_launch("relax");
 }
 
@@ -745,6 +788,14 @@ struct SlabCellFetch {
     }
 };
 
+// newton_core on a batch slab, kept out of line: the FIRE loop of the batched kernel keeps its
+// registers, the (rare) Newton evaluations run in the callee's own allocation.
+template <int LAYOUT>
+__device__ __noinline__ bool slab_newton(const AxisView& G, const float (&Tc)[3][3], const PolishSpring& S, V3 tip,
+                                         V3& q, float4& fe, float& g2, int& evals) {
+    return newton_core(SlabCellFetch<LAYOUT>{G}, Tc, S, tip, q, fe, g2, evals);
+}
+
 // Warm start (SPM_FLAG_WARM): a z-step starts from the equilibrium the state
 // had in the previous call (PPs in) when that one converged and its
 // displacement from the tip differs by at most WARM_MAX_JUMP per axis from the
@@ -779,30 +830,62 @@ __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const 
     float dt = P.relax_params[0], damp = P.relax_params[1];
     float4 fe = make_float4(0.f, 0.f, 0.f, 0.f);
     int total_it = 0;
+    PolishSpring S;
+    float Tc[3][3];
+    if constexpr (POLISH) {
+        S.a = mk3(1.f, 0.f, 0.f); S.b = mk3(0.f, 1.f, 0.f); S.c = mk3(0.f, 0.f, 1.f);
+        S.kk = ld4(P.stiffness); S.d0 = ld4(P.dpos0);
+        S.surf = P.surfFF[0];
+        S.frame = true;
+        Tc[0][0] = __fmul_rn(G.fnx, G.ax); Tc[0][1] = 0.f; Tc[0][2] = 0.f;
+        Tc[1][0] = 0.f; Tc[1][1] = __fmul_rn(G.fny, G.by); Tc[1][2] = 0.f;
+        Tc[2][0] = 0.f; Tc[2][1] = 0.f; Tc[2][2] = __fmul_rn(G.fnz, G.cz);
+    }
     for (int iz = 0; iz < nzs; ++iz) {
+        bool warm_start = false;
         if (warm) {
             const float4 pw = PPs[sbase + iz];
             const V3 dw = mk3(pw.x - tip.x, pw.y - tip.y, pw.z - tip.z);
             const V3 dc = mk3(pos.x - tip.x, pos.y - tip.y, pos.z - tip.z);
             if (pw.w > 0.f && fabsf(dw.x - dc.x) <= WARM_MAX_JUMP && fabsf(dw.y - dc.y) <= WARM_MAX_JUMP &&
-                fabsf(dw.z - dc.z) <= WARM_MAX_JUMP)  // false for NaN
+                fabsf(dw.z - dc.z) <= WARM_MAX_JUMP) {  // false for NaN
                 pos = mk3(pw.x, pw.y, pw.z);
+                warm_start = true;
+            }
         }
         int it = 0;
-        bool conv;
-        while (!pp_iter_z<unsigned, CACHE, LAYOUT>(G, T, P, tip, pos, v, dt, damp, fe, it, total_it, conv)) {
+        bool conv = false, newton_done = false;
+        if constexpr (POLISH) {
+            // from a previous equilibrium Newton's method converges in a few steps: FIRE only if it does not
+            if (warm_start) {
+                V3 qn = pos;
+                float4 fn;
+                float g2;
+                int ev;
+                if (slab_newton<LAYOUT>(G, Tc, S, tip, qn, fn, g2, ev)) {
+                    pos = qn;
+                    if (g2 < P.f2conv) {
+                        fe = fn;
+                        it = ev;
+                        total_it += ev;
+                        conv = true;
+                        newton_done = true;
+                    }
+                }
+            }
         }
-        if (!conv) fe = sample_z<unsigned, CACHE, LAYOUT>(G, pos, T);  // the position moved after the last sample
+        if (!newton_done) {
+            while (!pp_iter_z<unsigned, CACHE, LAYOUT>(G, T, P, tip, pos, v, dt, damp, fe, it, total_it, conv)) {
+            }
+            if (!conv) fe = sample_z<unsigned, CACHE, LAYOUT>(G, pos, T);  // the position moved after the last sample
+        }
         V3 q = pos;
         if constexpr (POLISH) {
-            PolishSpring S;
-            S.a = mk3(1.f, 0.f, 0.f); S.b = mk3(0.f, 1.f, 0.f); S.c = mk3(0.f, 0.f, 1.f);
-            S.kk = ld4(P.stiffness); S.d0 = ld4(P.dpos0);
-            S.surf = P.surfFF[0];
-            S.frame = true;
-            const float Tc[3][3] = {{__fmul_rn(G.fnx, G.ax), 0.f, 0.f}, {0.f, __fmul_rn(G.fny, G.by), 0.f},
-                                    {0.f, 0.f, __fmul_rn(G.fnz, G.cz)}};
-            if (fe.w == fe.w) newton_polish(SlabCellFetch<LAYOUT>{G}, Tc, S, tip, q, fe);
+            if (!newton_done && fe.w == fe.w) {
+                float g2;
+                int ev;
+                slab_newton<LAYOUT>(G, Tc, S, tip, q, fe, g2, ev);
+            }
         }
         const long long o = sbase + iz;
         FEs[o] = fe;
@@ -993,4 +1076,52 @@ extern "C" int spm_fe_in_strokes_tilted(const float* grid, int nx, int ny, int n
         make_view(grid, nx, ny, nz, p), reinterpret_cast<const float4*>(points), n_scan, P,
         reinterpret_cast<float4*>(FEs));
     return check_launch("spm_fe_in_strokes_tilted");
+}
+
+extern "C" long long spm_relax_pair_workspace_bytes(int n_scan) {
+    if (n_scan < 0) return 0;
+    return 16 + 4LL * (n_scan / 2);
+}
+
+extern "C" int spm_relax_pair_dissipation(const float* grid, int nx, int ny, int nz, const float* points, int n_scan,
+                                          const spm_scan_params* p, float* FEs, float* disps, int* iter_count,
+                                          const double* n, const double* h_scan, const int* off, const int* idx,
+                                          int n_out, float* E_diss, void* workspace, void* stream) {
+    using namespace spm;
+    clear_error();
+    int rc = check_scan_args("spm_relax_pair_dissipation", grid, nx, ny, nz, points, n_scan, p, FEs);
+    if (rc) return rc;
+    SPM_REQUIRE((p->flags & SPM_FLAG_PAIRED) && n_scan % 2 == 0,
+                "spm_relax_pair_dissipation: needs SPM_FLAG_PAIRED and an even n_scan (n_scan=%d)", n_scan);
+    SPM_REQUIRE(n && workspace && n_out >= 0, "spm_relax_pair_dissipation: null direction/workspace or n_out < 0");
+    if (n_scan == 0 || p->nz == 0) return SPM_OK;
+    SPM_REQUIRE(disps && aligned16(disps), "spm_relax_pair_dissipation: disps null or misaligned");
+    SPM_REQUIRE(n_out == 0 || (h_scan && off && idx && E_diss), "spm_relax_pair_dissipation: null dissipation array");
+    SPM_REQUIRE((reinterpret_cast<uintptr_t>(workspace) & 15u) == 0,
+                "spm_relax_pair_dissipation: workspace not 16-byte aligned");
+    const double nn = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    SPM_REQUIRE(nn > 0.0 && isfinite(nn), "spm_relax_pair_dissipation: oscillation direction must be non-zero");
+    spm_scan_params P = normalized(p, n_scan);
+    const GridView G = make_view(grid, nx, ny, nz, p);
+    DissArgs DA;
+    DA.h = h_scan; DA.off = off; DA.idx = idx; DA.E = E_diss; DA.n_out = n_out;
+    // the oscillation direction as compute_dissipation takes it: n = osc_dir / |osc_dir|
+    for (int d = 0; d < 3; d++) DA.n[d] = n[d] / nn;
+    unsigned* ctr = static_cast<unsigned*>(workspace);
+    DA.pair = reinterpret_cast<int*>(static_cast<char*>(workspace) + 16);
+    cudaStream_t st = as_stream(stream);
+    if (cudaMemsetAsync(DA.pair, 0, sizeof(int) * (size_t)(n_scan / 2), st) != cudaSuccess)
+        return set_error(SPM_ERR_CUDA, "spm_relax_pair_dissipation: cannot reset the pair counters");
+    const bool big = (long long)nx * ny * nz >= (1LL << 32);
+    const bool pol = (P.flags & SPM_FLAG_POLISH) != 0;
+    auto kern = big ? (pol ? relax_tile_kernel<0, size_t, true, true> : relax_tile_kernel<0, size_t, false, true>)
+                    : (pol ? relax_tile_kernel<0, unsigned, true, true> : relax_tile_kernel<0, unsigned, false, true>);
+    int blocks = 0;
+    if (int rc2 = persistent_blocks(kern, n_scan, blocks)) return rc2;
+    if (cudaMemsetAsync(ctr, 0, sizeof(unsigned), st) != cudaSuccess)
+        return set_error(SPM_ERR_CUDA, "spm_relax_pair_dissipation: cannot reset the pixel counter");
+    kern<<<blocks, RX_THREADS, 0, st>>>(G, reinterpret_cast<const float4*>(points), n_scan, P,
+                                        reinterpret_cast<float4*>(FEs), reinterpret_cast<float4*>(disps), iter_count,
+                                        ctr, DA);
+    return check_launch("spm_relax_pair_dissipation");
 }

@@ -498,19 +498,22 @@ __device__ __forceinline__ bool polish_step(const float (&J)[3][3], V3 Gv, V3& d
     return true;
 }
 
-// The polish loop over any cell fetcher: fetch(q, ax, ay, az, t) -> false when q's cell is
+// The Newton loop over any cell fetcher: fetch(q, ax, ay, az, t) -> false when q's cell is
 // not available (outside the sampler's range or the stored slab).  On return q is the polished
-// position and fe the sample there; when the first fetch fails both are left unchanged.
+// position, fe the sample there, g2 = |G(q)|^2 and evals the cells evaluated; false (q and fe
+// unchanged) when the first fetch fails.
 template <class Fetch>
-__device__ __forceinline__ void newton_polish(const Fetch& fetch, const float (&T)[3][3], const PolishSpring& S,
-                                              V3 tip, V3& q, float4& fe) {
+__device__ __forceinline__ bool newton_core(const Fetch& fetch, const float (&T)[3][3], const PolishSpring& S,
+                                            V3 tip, V3& q, float4& fe, float& g2_out, int& evals) {
     float4 t[8];
     float ax, ay, az;
-    if (!fetch(q, ax, ay, az, t)) return;
+    evals = 0;
+    if (!fetch(q, ax, ay, az, t)) return false;
     float J[3][3];
     V3 Gv;
     float4 fe0;
     polish_eval(t, ax, ay, az, T, S, tip, q, fe0, Gv, J);
+    evals = 1;
     float g2 = dot3(Gv, Gv);
     for (int it = 0; it < POLISH_STEPS; it++) {
         V3 dq;
@@ -521,6 +524,7 @@ __device__ __forceinline__ void newton_polish(const Fetch& fetch, const float (&
         V3 G1;
         float4 fe1;
         polish_eval(t, ax, ay, az, T, S, tip, q1, fe1, G1, J1);
+        ++evals;
         const float g21 = dot3(G1, G1);
         if (!(g21 < g2)) break;
         q = q1;
@@ -533,6 +537,17 @@ __device__ __forceinline__ void newton_polish(const Fetch& fetch, const float (&
             for (int j = 0; j < 3; j++) J[i][j] = J1[i][j];
     }
     fe = fe0;
+    g2_out = g2;
+    return true;
+}
+
+// Newton polish of a relaxed state (see above): q, fe in and out.
+template <class Fetch>
+__device__ __forceinline__ void newton_polish(const Fetch& fetch, const float (&T)[3][3], const PolishSpring& S,
+                                              V3 tip, V3& q, float4& fe) {
+    float g2;
+    int evals;
+    newton_core(fetch, T, S, tip, q, fe, g2, evals);
 }
 
 // Cell fetcher of a full (nz,ny,nx) grid with any sampling transform (interp_fe's addressing).

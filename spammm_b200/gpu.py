@@ -267,6 +267,50 @@ def df_dir(FEs, spacing, osc_dir=(0., 0., 1.)):
     return df
 
 
+def _diss_lists(h_scan, h_df, amp, osc_dir, dev):
+    """compute_dissipation's integration windows (AFM.py:3266-3273): for every output height, the scan
+    heights within +-amp*|n_z| (all of them when fewer than two) -> (n, h, off, idx) for the kernels."""
+    h_scan = np.asarray(h_scan, dtype=np.float64)
+    nz = h_scan.shape[0]
+    n = np.asarray(osc_dir, dtype=np.float64)
+    n = np.ascontiguousarray(n / np.linalg.norm(n))
+    amp_z = float(amp) * abs(n[2])
+    off = [0]
+    idx = []
+    for h in np.asarray(h_df, dtype=np.float64):
+        mask = (h_scan >= h - amp_z) & (h_scan <= h + amp_z)
+        if mask.sum() < 2:
+            mask = np.ones(nz, dtype=bool)
+        idx.extend(np.flatnonzero(mask).tolist())
+        off.append(len(idx))
+    return (n, torch.as_tensor(h_scan, dtype=F64, device=dev), torch.as_tensor(np.asarray(off, np.int32), device=dev),
+            torch.as_tensor(np.asarray(idx if idx else [0], np.int32), device=dev))
+
+
+def relax_pair_dissipation(grid, params, points, h_scan, h_df, amp, osc_dir=(0., 0., 1.), iter_count=None):
+    """Forward + backward strokes (SPM_FLAG_PAIRED in params) and their dissipation in one launch ->
+    FEs, disps (n_scan,nz,4), E_diss (n_scan/2, len(h_df)) float32; h_scan in the stored z order."""
+    nx, ny, nz = _grid_dims(grid)
+    points = _as_dev(points, F32, (4,), "points")
+    n_scan = points.shape[0]
+    shape = (n_scan, params.nz, 4)
+    dev = points.device
+    FEs = torch.empty(shape, dtype=F32, device=dev)
+    disps = torch.empty(shape, dtype=F32, device=dev)
+    if len(np.asarray(h_scan)) != params.nz:
+        raise ValueError(f"h_scan must have {params.nz} entries")
+    n, h_t, off_t, idx_t = _diss_lists(h_scan, h_df, amp, osc_dir, dev)
+    n_out = len(np.asarray(h_df))
+    E = torch.empty((n_scan // 2, n_out), dtype=F32, device=dev)
+    ws = torch.empty(((int(lib().spm_relax_pair_workspace_bytes(n_scan)) + 15) // 16, 4), dtype=torch.int32,
+                     device=dev)
+    rc = lib().spm_relax_pair_dissipation(ptr(grid), nx, ny, nz, ptr(points), n_scan, ctypes.byref(params), ptr(FEs),
+                                          ptr(disps), ptr(iter_count), hptr(n), ptr(h_t), ptr(off_t), ptr(idx_t),
+                                          n_out, ptr(E), ptr(ws), stream_ptr())
+    check(rc, "spm_relax_pair_dissipation")
+    return FEs, disps, E
+
+
 def dissipation(FEs_fwd, FEs_bwd, h_scan, h_df, amp, osc_dir=(0., 0., 1.)):
     """compute_dissipation on the device -> (nx,ny,nz_df) float32."""
     Ff = _fes_volume(FEs_fwd)
@@ -280,21 +324,7 @@ def dissipation(FEs_fwd, FEs_bwd, h_scan, h_df, amp, osc_dir=(0., 0., 1.)):
     h_df = np.asarray(h_df, dtype=np.float64)
     if h_scan.shape != (nz,):
         raise ValueError(f"h_scan must have {nz} entries, got {h_scan.shape}")
-    n = np.asarray(osc_dir, dtype=np.float64)
-    n = np.ascontiguousarray(n / np.linalg.norm(n))
-    amp_z = float(amp) * abs(n[2])
-    off = [0]
-    idx = []
-    for h in h_df:
-        mask = (h_scan >= h - amp_z) & (h_scan <= h + amp_z)
-        if mask.sum() < 2:
-            mask = np.ones(nz, dtype=bool)
-        idx.extend(np.flatnonzero(mask).tolist())
-        off.append(len(idx))
-    dev = Ff.device
-    h_t = torch.as_tensor(h_scan, dtype=F64, device=dev)
-    off_t = torch.as_tensor(np.asarray(off, np.int32), device=dev)
-    idx_t = torch.as_tensor(np.asarray(idx if idx else [0], np.int32), device=dev)
+    n, h_t, off_t, idx_t = _diss_lists(h_scan, h_df, amp, osc_dir, Ff.device)
     E = torch.empty((nx, ny, len(h_df)), dtype=F32, device=dev)
     rc = lib().spm_dissipation(ptr(Ff), ptr(Fb), _dt(Ff), nx, ny, nz, hptr(n), ptr(h_t), ptr(off_t), ptr(idx_t), len(h_df),
                                ptr(E), stream_ptr())

@@ -6,7 +6,7 @@ import pytest
 import torch
 
 from oracle import oracle as O
-from spammm_b200 import AFM, _lib
+from spammm_b200 import AFM, _lib, gpu
 from spammm_b200.AFM import AFMulator
 
 pytestmark = pytest.mark.gpu
@@ -228,3 +228,26 @@ def test_make_forcefield_run_scan_and_raw(cuda):
         r = np.corrcoef(raw[..., 2].ravel(), rel[..., 2].ravel())[0, 1]
         assert r > 0.5
         assert np.sqrt(np.mean((raw[..., 2] - rel[..., 2]) ** 2)) > 1e-6 * np.abs(rel[..., 2]).max()
+
+
+def test_pair_dissipation_fused_equals_separate_calls(cuda):
+    """spm_relax_pair_dissipation: the forward + backward strokes and compute_dissipation in one launch
+    (the second stroke of each pixel integrates it) give scan_fdbm_pair's strokes and spm_dissipation's
+    E_diss bit for bit, for a window sweep of h_df / amplitudes and a tilted oscillation direction."""
+    rng = np.random.default_rng(31)
+    F_total = (0.02 * rng.standard_normal((24, 22, 30, 4))).astype(np.float32)
+    afm = AFMulator(use_morse=True)
+    afm.setup_fdbm_grid(F_total, np.array([-3., -2.75, -1.0], np.float32), 0.25)
+    xs = np.linspace(-1, 1, 9).astype(np.float32)
+    ys = np.linspace(-1, 1, 7).astype(np.float32)
+    hs = np.linspace(3.0, 4.5, 16).astype(np.float32)
+    kw = dict(mol_z=0.2, K_LAT=0.03, K_RAD=20.0, bond_length=3.0, return_device=True)
+    for h_df, amp, osc in ((hs[3:13:2], 0.3, (0., 0., 1.)), (np.array([3.6, 4.0]), 0.55, (0.3, 0., 1.)),
+                           (np.array([3.0, 4.5]), 0.01, (0., 0., 1.))):  # the last: windows of < 2 heights
+        (Ff, df_), (Fb, db_), E = afm.scan_fdbm_pair(xs, ys, hs, osc_dir=osc, dissipation=(hs, h_df, amp), **kw)
+        (Ff2, _), (Fb2, _) = afm.scan_fdbm_pair(xs, ys, hs, osc_dir=osc, **kw)
+        assert torch.equal(Ff, Ff2) and torch.equal(Fb, Fb2)
+        E2 = gpu.dissipation(Ff2, Fb2, hs, h_df, amp, osc)
+        assert E.shape == E2.shape == (9, 7, len(h_df))
+        assert torch.equal(E, E2)
+        assert float(E.abs().max()) > 0

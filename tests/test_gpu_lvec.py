@@ -2,8 +2,8 @@
 839-893): a NaCl-like layer with a molecule in a 60-degree cell read by
 load_molecule from an .xyz with an "lvs" line (the fixture of
 tests/golden/xyz_golden.npz), LJ grid on the skew node lattice against the FP64
-oracle (grid-build tolerance: 2e-5 |ref| + 2e-6 max|ref| + 1e-5 S, S the node's
-sum of contribution magnitudes), and run_scan
+oracle (grid-build tolerance of test_gpu_scale.py: 2e-5 |ref| + 2e-6 max|ref| +
+1e-5 S + the node-position rounding term), and run_scan
 (relaxStrokesTilted) over a window larger than the cell -- probes sample across
 the periodic seam through the skew sampling transform -- bit-identical to the
 canonical-FP32 oracle on the same grid; unrelaxed samples of a window shifted
@@ -47,7 +47,8 @@ def test_skew_periodic_cell_grid_and_scan(cuda, golden):
     ref = ref.reshape(-1, 4)
     scale = np.abs(ref).max(axis=0)
     err = np.abs(grid.reshape(-1, 4).astype(np.float64) - ref)
-    assert not (err > 2e-5 * np.abs(ref) + 2e-6 * scale + 1e-5 * S).any()
+    from test_gpu_scale import pos_term
+    assert not (err > 2e-5 * np.abs(ref) + 2e-6 * scale + 1e-5 * S + pos_term(q, a64, ref)).any()
     # a scan window of 9 x 8 A over a 6 A skew cell: the probes cross the periodic seam
     nxy, nzs, dtip = (36, 32), 20, -0.1
     p0 = np.array([-1.5, -1.0, 3.0 + afm.mol_z + 3.5], np.float32)
