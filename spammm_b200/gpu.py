@@ -324,7 +324,8 @@ def dissipation(FEs_fwd, FEs_bwd, h_scan, h_df, amp, osc_dir=(0., 0., 1.)):
     h_df = np.asarray(h_df, dtype=np.float64)
     if h_scan.shape != (nz,):
         raise ValueError(f"h_scan must have {nz} entries, got {h_scan.shape}")
-    n, h_t, off_t, idx_t = _diss_lists(h_scan, h_df, amp, osc_dir, Ff.device)
+    dev = Ff.device
+    n, h_t, off_t, idx_t = _diss_lists(h_scan, h_df, amp, osc_dir, dev)
     E = torch.empty((nx, ny, len(h_df)), dtype=F32, device=dev)
     rc = lib().spm_dissipation(ptr(Ff), ptr(Fb), _dt(Ff), nx, ny, nz, hptr(n), ptr(h_t), ptr(off_t), ptr(idx_t), len(h_df),
                                ptr(E), stream_ptr())
