@@ -111,6 +111,14 @@ int spm_grid_build(int kind, int n_atoms, const float* atoms, const float* param
                    const float* p0, const float* dA, const float* dB, const float* dC,
                    const float* Qs, const float* QZs, void* stream);
 
+/* The same pair sums at arbitrary points, uncapped: replaces
+ * cs_brute_afm_morse_c_points (kernels/contact_surface.cl:1341-1390) behind
+ * AFMulator._brute_afm_morse_c_queries (spammm/SPM/AFM.py:1051-1067), the
+ * direct reference of the grid builder.  queries (n_q,3) float32, out (n_q,4)
+ * = (Fx,Fy,Fz,E); atoms/params/Qs/QZs as spm_grid_build. */
+int spm_pair_fe_points(int kind, int n_atoms, const float* atoms, const float* params, const float* queries,
+                       int n_q, const float* Qs, const float* QZs, float* out, void* stream);
+
 /* ------------------------------------------------------------------------
  * (b) Probe relaxation on the grid.
  * spm_relax_strokes replaces AFMulator.scan_fdbm's launch of relaxStrokes
@@ -413,7 +421,9 @@ typedef struct spm_batch_shape {
                            some spills), 2 = the cell's 8 texels kept in registers across FIRE
                            iterations (up to 128 registers, loads only when the cell changes),
                            3 = the texel cache at 80 registers (some spills, more warps), 4 = the
-                           texel cache at up to 102 registers in CTAs of at most 128 threads */
+                           texel cache at up to 102 registers in CTAs of at most 128 threads, 5 = the
+                           texel cache with each warp's z-slab box staged in shared memory by bulk copies
+                           (128-thread CTAs, x-pair slabs, rx_sync = 1, no SPM_FLAG_POLISH / WARM) */
     int grid_layout;    /* slab layout: 0 = x-pairs (2 float4 per node), 1 = xz-quads (4 float4 per
                            node: half the cache lines per sample, twice the memory) */
     int rx_sync;        /* relaxation schedule: 0 = every lane draws its next pixel when its stroke ends,

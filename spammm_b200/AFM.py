@@ -96,6 +96,44 @@ class _Queue:
         torch.cuda.synchronize()
 
 
+# The reference kernels (kernels/AFM.cl, kernels/contact_surface.cl) this library implements, by the
+# reference's names: callers introspect AFMulator.prg.all_kernels() for them.
+IMPLEMENTED_KERNELS = (
+    "evalLJC_QZs_toImg", "evalMorseC_QZs_toImg", "relaxStrokes", "relaxStrokesTilted", "relaxStrokes2D",
+    "getFEinStrokesTilted", "convolveZ", "izoZ", "relaxStrokesTiltedMorseDirect", "morseDirectStateAdjoint",
+    "morseDirectParamPartials", "reduceMorseDirectParamPartials", "cs_brute_afm_morse_c_points")
+
+
+class _Kernel:
+    def __init__(self, name):
+        self.function_name = name
+
+
+class _Program:
+    """Stand-in for the reference's compiled cl.Program (AFMulator.prg): all_kernels() lists the reference
+    kernels whose work this library's CUDA kernels do."""
+
+    def all_kernels(self):
+        return [_Kernel(n) for n in IMPLEMENTED_KERNELS]
+
+
+class _Device:
+    def __init__(self, index):
+        props = torch.cuda.get_device_properties(index)
+        self.name = props.name
+        self.vendor = "NVIDIA Corporation"
+        self.opencl_c_version = "none (CUDA sm_100a kernels)"
+        self.max_compute_units = props.multi_processor_count
+        self.global_mem_size = props.total_memory
+
+
+class _Context:
+    """Stand-in for the reference's cl.Context (AFMulator.ctx): devices[0] describes the CUDA device."""
+
+    def __init__(self, index):
+        self.devices = [_Device(index)]
+
+
 class _Molecule:
     def __init__(self, apos, enames, qs, lvec=None):
         self.apos = apos
@@ -212,6 +250,8 @@ class AFMulator:
         self.cl_src_dir = cl_src_dir
         self.queue = _Queue()
         self.device = torch.device("cuda", torch.cuda.current_device())
+        self.prg = _Program()
+        self.ctx = _Context(self.device.index)
         props = torch.cuda.get_device_properties(self.device)
         self._max_alloc = int(props.total_memory)
         self._global_mem = int(props.total_memory)
@@ -640,6 +680,15 @@ class AFMulator:
                                tipC=self.tipC, dTip=dTip, dpos0=self.dpos0, nz=nz, raster_ny=ny_s, polish=False)
         FEs = gpu.fe_in_strokes_tilted(self.img_FF, P, torch.from_numpy(pts).to(self.device))
         return gpu.to_host(FEs.reshape(nx_s, ny_s, nz, 4)), pts[:, :3].reshape(nx_s, ny_s, 3)
+
+    def _brute_afm_morse_c_queries(self, queries):
+        """Uncapped Morse + Coulomb sums at arbitrary (n,3) points -> (E (n,), F (n,3)) float32
+        (AFM.py:1051-1067, the direct reference of the grid builder)."""
+        assert self.use_morse and self.atoms_arr is not None and self.cLJs_arr is not None
+        q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, 3)
+        out = gpu.to_host(gpu.pair_fe_points(_lib.SPM_KIND_MORSE, self.atoms_arr, self.cLJs_arr,
+                                             torch.from_numpy(q).to(self.device), self.tipQs, self.tipQZs))
+        return out[:, 3], out[:, :3]
 
     @property
     def mol_z(self):

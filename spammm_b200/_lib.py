@@ -137,6 +137,7 @@ _SIGNATURES = {
     "spm_abi_version": (_i, []),
     "spm_last_error": (ctypes.c_char_p, []),
     "spm_grid_build": (_i, [_i, _i, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "spm_pair_fe_points": (_i, [_i, _i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp]),
     "spm_relax_strokes": (_i, [_vp, _i, _i, _i, _vp, _i, _P, _vp, _vp, _vp]),
     "spm_relax_ex": (_i, [_i, _vp, _i, _i, _i, _vp, _i, _P, _vp, _vp, _vp, _vp, _vp]),
     "spm_relax_workspace_bytes": (_ll, []),

@@ -30,8 +30,10 @@ from .batch import AFMBatch
 GRID_CANDIDATES = [dict(gb_ty=ty, gb_zb=zb) for ty in (2, 4, 8) for zb in (8, 16)]
 # z-synchronised warp tiles ran 3x faster than lanes drawing pixels independently on the
 # 64-molecule fit (the CTA size made no difference); one independent-lane shape stays as a check
+# rx_regs = 5: the z-slab of each warp staged in shared memory by bulk copies (x-pair slabs only)
 RELAX_CANDIDATES = [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=r, grid_layout=g) for g in (0, 1)
                     for h in (2, 4, 8, 16) for r in (0, 1, 2, 3, 4)] + \
+                   [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=5, grid_layout=0) for h in (2, 4, 8, 16)] + \
                    [dict(rx_sync=0, rx_threads=128, rx_tile_h=8, rx_regs=0, grid_layout=0)]
 ADJOINT_CANDIDATES = [dict(adj_chunk=c, adj_ilp=i) for c in (4096, 16384, 65536) for i in (1, 2)]
 
@@ -100,12 +102,13 @@ def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
                 log(f"autotune {name} {kw}: {ms:.3f} ms")
         res.sort(key=lambda r: r[0])
         shape = _with(shape, **res[0][1])
-        report[name] = {"best": res[0][1], "ms": res[0][0], "worst_ms": res[-1][0], "tried": len(res)}
+        report[name] = {"best": res[0][1], "ms": res[0][0], "worst_ms": res[-1][0], "tried": len(res),
+                        "all": [[ms, kw] for ms, kw in res]}
 
     pick("grid", GRID_CANDIDATES, batch.build_grids)
     batch.set_shape(shape)
     batch.build_grids()
-    cands = [c for c in RELAX_CANDIDATES if c["rx_sync"] == 1 or not (batch.polish or warm)]
+    cands = [c for c in RELAX_CANDIDATES if (c["rx_sync"] == 1 and c["rx_regs"] != 5) or not (batch.polish or warm)]
     if max_grid_bytes is not None:
         cands = [c for c in cands if (4 if c["grid_layout"] else 2) * batch.grid_float4 * 16 <= max_grid_bytes]
     pick("relax", cands, batch.relax, prepare=batch.build_grids)

@@ -42,7 +42,57 @@ __device__ __forceinline__ float fast_ex2(float x) {
 struct Sites {
     float qs[4];  // Qs[k]*COULOMB_CONST (all four sites, zero allowed)
     float qz[4];
+    double qs64[4];  // the same sites in FP64 (Qs[k] * COULOMB_CONST in double), for the convergence check
+    double qz64[4];
+    int ns;
 };
+
+// |total force|^2 at p in FP64 -- the Morse + Coulomb sums from the atoms' float32 inputs with IEEE
+// double exp/sqrt (the reference's FP64 pair law, kernels/AFM.cl:730-757 in double), the spring and the
+// surface bias -- to confirm a convergence the FP32 sums report: near |F|^2 = f2conv their rounding
+// (MUFU rsqrt/ex2, and the radial spring's r - d0 of a 4 A bond at float32 resolution) can put the
+// FP32 test on the converged side of a state whose force is not.
+__device__ __noinline__ double force2_f64(V3 p, V3 tip, int na, const float4* __restrict__ atoms, const float4* __restrict__ cMs,
+                             const Sites& S, V3 a, V3 b, V3 c, float4 kk, float4 d0, float surf) {
+    const double px = p.x, py = p.y, pz = p.z;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int j = 0; j < na; j++) {
+        const float4 at = __ldg(atoms + j);
+        const float4 cm = __ldg(cMs + j);
+        const double dx = px - at.x, dy = py - at.y, dz = pz - at.z;
+        const double dxy2 = dx * dx + dy * dy;
+        const double r = sqrt(dxy2 + dz * dz + 1e-4);
+        const double K = cm.z, R0 = cm.x, E0 = cm.y;
+        const double e = exp(K * (r - R0));
+        const double sr = (-E0 * e * (e - 1.0) * 2.0 * K) / r;
+        fx += dx * sr;
+        fy += dy * sr;
+        fz += dz * sr;
+        for (int k = 0; k < S.ns; k++) {
+            if (S.qs64[k] == 0.0) continue;
+            const double dzk = dz + S.qz64[k];
+            const double ir2 = 1.0 / (dxy2 + dzk * dzk + 1e-4);
+            const double sk = S.qs64[k] * (double)at.w * sqrt(ir2) * ir2;
+            fx += dx * sk;
+            fy += dy * sk;
+            fz += dzk * sk;
+        }
+    }
+    // spring in the tip frame: (d - d0.xyz) k.xyz + d k.w (r - d0.w) / r, rotated back
+    const double ex = (double)p.x - tip.x, ey = (double)p.y - tip.y, ez = (double)p.z - tip.z;
+    const double dl[3] = {ex * a.x + ey * a.y + ez * a.z, ex * b.x + ey * b.y + ez * b.z, ex * c.x + ey * c.y + ez * c.z};
+    double ft[3] = {(dl[0] - d0.x) * kk.x, (dl[1] - d0.y) * kk.y, (dl[2] - d0.z) * kk.z};
+    if (kk.w != 0.f) {
+        double r = sqrt(dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2]);
+        r = r > 1e-10 ? r : 1e-10;
+        const double sr = kk.w * (r - d0.w) / r;
+        for (int i = 0; i < 3; i++) ft[i] += dl[i] * sr;
+    }
+    fx += a.x * ft[0] + b.x * ft[1] + c.x * ft[2] + c.x * (double)surf;
+    fy += a.y * ft[0] + b.y * ft[1] + c.y * ft[2] + c.y * (double)surf;
+    fz += a.z * ft[0] + b.z * ft[1] + c.z * ft[2] + c.z * (double)surf;
+    return fx * fx + fy * fy + fz * fz;
+}
 
 __device__ __forceinline__ int direct_pixel(int n_scan, int raster_ny) {
     if (raster_ny > 0) {
@@ -152,7 +202,9 @@ relax_direct_kernel(int na, const float4* __restrict__ atoms, const float4* __re
             f.x = fmaf(c.x, surf, f.x);
             f.y = fmaf(c.y, surf, f.y);
             f.z = fmaf(c.z, surf, f.z);
-            if (dot3(f, f) < P.f2conv) {  // convergence is tested before the update
+            // convergence is tested before the update; an FP32 "converged" is confirmed in FP64
+            if (dot3(f, f) < P.f2conv &&
+                force2_f64(pos, tip, na, atoms, cMs, S, a, b, c, kk, d0, surf) < (double)P.f2conv) {
                 done = conv = true;
             } else {
                 md_step(f, v, pos, I, true);
@@ -457,13 +509,20 @@ Sites make_sites(const float* Qs, const float* QZs, bool compact, int* ns) {
     int n = 0;
     for (int k = 0; k < 4; k++) {
         if (compact) {
-            if (Qs[k] != 0.f) { S.qs[n] = Qs[k] * COULOMB_CONST; S.qz[n] = QZs[k]; n++; }
+            if (Qs[k] != 0.f) {
+                S.qs[n] = Qs[k] * COULOMB_CONST; S.qz[n] = QZs[k];
+                S.qs64[n] = (double)Qs[k] * 14.3996448915; S.qz64[n] = QZs[k];
+                n++;
+            }
         } else {
             S.qs[k] = Qs[k] * COULOMB_CONST;
             S.qz[k] = QZs[k];
+            S.qs64[k] = (double)Qs[k] * 14.3996448915;
+            S.qz64[k] = QZs[k];
         }
     }
-    if (ns) *ns = compact ? n : 4;
+    S.ns = compact ? n : 4;
+    if (ns) *ns = S.ns;
     return S;
 }
 

@@ -437,3 +437,99 @@ extern "C" int spm_grid_build(int kind, int n_atoms, const float* atoms, const f
     if (kind == SPM_KIND_MORSE) return launch_kind<SPM_KIND_MORSE>(on, noff, grd, block, st, n_atoms, a4, params, pstride, g4, G, S);
     return launch_kind<SPM_KIND_LJ>(on, noff, grd, block, st, n_atoms, a4, params, pstride, g4, G, S);
 }
+
+// ---- the uncapped pair sums at arbitrary points ----------------------------
+// Replaces cs_brute_afm_morse_c_points (kernels/contact_surface.cl:1341-1390,
+// called by AFMulator._brute_afm_morse_c_queries, spammm/SPM/AFM.py:1051-1067):
+// per query point the LJ or Morse law plus the Coulomb law at the four
+// tip-charge sites (point + zhat*QZs[k], weighted by Qs[k]*COULOMB_CONST) summed
+// over all atoms, with no |E| > 100 cap.  One thread per point, atoms staged in
+// shared memory; FP32 with IEEE division, sqrt and exp.
+namespace spm {
+namespace {
+constexpr int PQ_THREADS = 128;
+
+template <int KIND>
+__global__ void __launch_bounds__(PQ_THREADS)
+pair_points_kernel(int na, const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
+                   const float* __restrict__ q, int nq, float4 qs, float4 qz, float4* __restrict__ out) {
+    __shared__ float4 s_a[PQ_THREADS];
+    __shared__ float4 s_p[PQ_THREADS];
+    const int iq = blockIdx.x * PQ_THREADS + threadIdx.x;
+    const bool act = iq < nq;
+    const float px = act ? q[3 * (size_t)iq] : 0.f, py = act ? q[3 * (size_t)iq + 1] : 0.f,
+                pz = act ? q[3 * (size_t)iq + 2] : 0.f;
+    const float sq[4] = {qs.x, qs.y, qs.z, qs.w}, sz[4] = {qz.x, qz.y, qz.z, qz.w};
+    float fx = 0.f, fy = 0.f, fz = 0.f, fe = 0.f;
+    for (int t0 = 0; t0 < na; t0 += PQ_THREADS) {
+        const int j = t0 + threadIdx.x;
+        if (j < na) {
+            s_a[threadIdx.x] = __ldg(atoms + j);
+            const float* pr = params + (size_t)j * pstride;
+            s_p[threadIdx.x] = make_float4(__ldg(pr), __ldg(pr + 1), KIND == SPM_KIND_MORSE ? __ldg(pr + 2) : 0.f, 0.f);
+        }
+        __syncthreads();
+        const int nt = min(PQ_THREADS, na - t0);
+        for (int jj = 0; jj < nt; jj++) {
+            const float4 a = s_a[jj];
+            const float4 c = s_p[jj];
+            const float dx = px - a.x, dy = py - a.y, dz = pz - a.z;
+            const float r2 = dx * dx + dy * dy + dz * dz + R2SAFE;
+            float s;
+            if (KIND == SPM_KIND_MORSE) {  // getMorse: E0 e (e - 2), F = dp * (-2 K E0 e (e-1)) / r
+                const float r = sqrtf(r2);
+                const float e = expf(c.z * (r - c.x));
+                fe += c.y * e * (e - 2.f);
+                s = __fdiv_rn(-c.y * e * (e - 1.f) * 2.f * c.z, r);
+            } else {  // getLJ: (c12 ir6 - c6) ir6, F = dp * (12 c12 ir6 - 6 c6) ir6 ir2
+                const float ir2 = __fdiv_rn(1.f, r2);
+                const float ir6 = ir2 * ir2 * ir2;
+                fe += (c.y * ir6 - c.x) * ir6;
+                s = (12.f * c.y * ir6 - 6.f * c.x) * ir6 * ir2;
+            }
+            fx += dx * s;
+            fy += dy * s;
+            fz += dz * s;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (sq[k] == 0.f) continue;
+                const float dzk = dz + sz[k];
+                const float ir2 = __fdiv_rn(1.f, dx * dx + dy * dy + dzk * dzk + R2SAFE);
+                const float E = a.w * sqrtf(ir2) * sq[k];
+                fe += E;
+                const float sk = E * ir2;
+                fx += dx * sk;
+                fy += dy * sk;
+                fz += dzk * sk;
+            }
+        }
+        __syncthreads();
+    }
+    if (act) out[iq] = make_float4(fx, fy, fz, fe);
+}
+}  // namespace
+}  // namespace spm
+
+extern "C" int spm_pair_fe_points(int kind, int n_atoms, const float* atoms, const float* params, const float* queries,
+                                  int n_q, const float* Qs, const float* QZs, float* out, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(kind == SPM_KIND_LJ || kind == SPM_KIND_MORSE, "spm_pair_fe_points: kind=%d", kind);
+    SPM_REQUIRE(n_atoms >= 0 && n_q >= 0, "spm_pair_fe_points: negative sizes");
+    SPM_REQUIRE(Qs && QZs, "spm_pair_fe_points: null host vectors");
+    if (n_q == 0) return SPM_OK;
+    SPM_REQUIRE(queries && out && (n_atoms == 0 || (atoms && params)), "spm_pair_fe_points: null device pointer");
+    SPM_REQUIRE(aligned16(out) && (n_atoms == 0 || aligned16(atoms)), "spm_pair_fe_points: out/atoms not aligned");
+    const float4 qs = make_float4(Qs[0] * COULOMB_CONST, Qs[1] * COULOMB_CONST, Qs[2] * COULOMB_CONST,
+                                  Qs[3] * COULOMB_CONST);
+    const float4 qz = make_float4(QZs[0], QZs[1], QZs[2], QZs[3]);
+    const unsigned nb = (unsigned)((n_q + PQ_THREADS - 1) / PQ_THREADS);
+    cudaStream_t st = as_stream(stream);
+    const float4* a4 = reinterpret_cast<const float4*>(atoms);
+    float4* o4 = reinterpret_cast<float4*>(out);
+    if (kind == SPM_KIND_MORSE)
+        pair_points_kernel<SPM_KIND_MORSE><<<nb, PQ_THREADS, 0, st>>>(n_atoms, a4, params, 4, queries, n_q, qs, qz, o4);
+    else
+        pair_points_kernel<SPM_KIND_LJ><<<nb, PQ_THREADS, 0, st>>>(n_atoms, a4, params, 2, queries, n_q, qs, qz, o4);
+    return check_launch("spm_pair_fe_points");
+}

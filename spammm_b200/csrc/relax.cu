@@ -24,6 +24,7 @@
 //
 // This translation unit is compiled with -fmad=false: the only fused
 // multiply-adds are the explicit __fmaf_rn calls shared with the CPU oracle.
+#include <climits>
 #include "spm_internal.cuh"
 #include "spm_fire.cuh"
 #include "spm_batch.cuh"
@@ -930,6 +931,242 @@ batch_relax_sync_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsig
     }
 }
 
+// ---- z-slab staging in shared memory through the bulk-copy (TMA) engine ----
+// spm_batch_shape.rx_regs = 5 (x-pair slabs, 128-thread CTAs, rx_sync = 1).  At
+// every z-step each warp computes the box of slab nodes around its lanes'
+// current cells (the cells' x range -1..+1, y and z ranges -1..+2: room for the
+// probe to move a cell) and copies its (z, y) rows -- contiguous runs of
+// x-pair nodes, 32 bytes each -- into the warp's shared-memory slice with
+// cp.async.bulk (one row per lane at a time, completion on the warp's
+// mbarrier).  A texel-cache miss then reads a cell inside the box from shared
+// memory, else from global memory as the default kernel does; a box larger
+// than STAGE_CAP nodes is not staged (all misses go to global memory).  The
+// wait is bounded: after STAGE_SPIN polls the warp records the timeout in the
+// workspace (word 1), waits once more (bounded) for its copies and stops
+// staging.  Results are the default kernel's bits (the same texel values).
+// Loads are plain bulk copies from this GPU's own memory (no multicast).
+constexpr int STAGE_WARPS = 4;
+constexpr int STAGE_CAP = 320;  // nodes per warp (10 KB)
+constexpr unsigned STAGE_SPIN = 1u << 20;
+
+struct StageBox {
+    const ulonglong2* s;  // the warp's slice: node (x, y, z) of the box at 2 * ((z * ny + y) * nx + x)
+    int x0, y0, z0, nx, ny, nz;
+    bool ok;
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// interp_fe_cached's miss path with the staged box first (x-pair slabs).
+__device__ __forceinline__ float4 interp_fe_staged(const AxisView& G, V3 p, TexelCache& T, const StageBox& B) {
+    const float u = __fmaf_rn(p.x, G.ax, G.aw);
+    const float v = __fmaf_rn(p.y, G.by, G.bw);
+    const float w = __fmaf_rn(p.z, G.cz, G.cw);
+    float fx, fy, fz;
+    const float ax = tex_coord(u, G.fnx, fx);
+    const float ay = tex_coord(v, G.fny, fy);
+    const float az = tex_coord(w, G.fnz, fz);
+    if (!(fx == T.kx && fy == T.ky && fz == T.kz)) {
+        int x0, x1, y0, y1, z0, z1;
+        bool ok = tex_index(fx, G.nx, G.fnx, x0, x1);
+        ok = tex_index(fy, G.ny, G.fny, y0, y1) && ok;
+        ok = tex_index(fz, G.nz, G.fnz, z0, z1) && ok;
+        ok = ok && to_slab(x0, x1, G.x_lo, G.nx_slab) && to_slab(y0, y1, G.y_lo, G.ny_slab) &&
+             to_slab(z0, z1, G.z_lo, G.nz_slab);
+        if (!ok) {
+            float nan = __int_as_float(0x7fc00000);
+            return make_float4(nan, nan, nan, nan);
+        }
+        const int bx = x0 - B.x0, by0 = y0 - B.y0, by1 = y1 - B.y0, bz0 = z0 - B.z0, bz1 = z1 - B.z0;
+        if (B.ok && (unsigned)bx < (unsigned)B.nx && (unsigned)by0 < (unsigned)B.ny && (unsigned)by1 < (unsigned)B.ny &&
+            (unsigned)bz0 < (unsigned)B.nz && (unsigned)bz1 < (unsigned)B.nz) {
+            const ulonglong2* q00 = B.s + 2 * ((bz0 * B.ny + by0) * B.nx + bx);
+            const ulonglong2* q10 = B.s + 2 * ((bz0 * B.ny + by1) * B.nx + bx);
+            const ulonglong2* q01 = B.s + 2 * ((bz1 * B.ny + by0) * B.nx + bx);
+            const ulonglong2* q11 = B.s + 2 * ((bz1 * B.ny + by1) * B.nx + bx);
+            T.f000 = q00[0]; T.f100 = q00[1];
+            T.f010 = q10[0]; T.f110 = q10[1];
+            T.f001 = q01[0]; T.f101 = q01[1];
+            T.f011 = q11[0]; T.f111 = q11[1];
+        } else {
+            load_cell<2, unsigned>(G, x0, y0, y1, z0, z1, T.f000, T.f100, T.f010, T.f110, T.f001, T.f101, T.f011,
+                                   T.f111);
+        }
+        T.kx = fx;
+        T.ky = fy;
+        T.kz = fz;
+    }
+    return blend_cached(T, ax, ay, az);
+}
+
+// The staged counterpart of relax_tile_stroke (no polish, no warm start).
+__device__ __forceinline__ void relax_tile_stroke_staged(const spm_batch_mol* D, const float* __restrict__ grid,
+                                                         const float4* __restrict__ pts, const spm_scan_params& P,
+                                                         float4* __restrict__ FEs, float4* __restrict__ PPs,
+                                                         int* __restrict__ iter_count, int k, float dz,
+                                                         unsigned members, ulonglong2* slice, unsigned bar,
+                                                         unsigned& parity, bool& staging, unsigned* status) {
+    const AxisView G = axis_view<2>(D, grid);
+    TexelCache T;
+    T.kx = __int_as_float(0x7fc00000);
+    const int nzs = D->nz_steps;
+    const int pix = D->pix_off + k;
+    const long long sbase = D->state_off + (long long)k * nzs;
+    const float4 p4 = pts[pix];
+    V3 tip = mk3(p4.x, p4.y, p4.z);
+    V3 pos = mk3(tip.x + P.dpos0[0], tip.y + P.dpos0[1], tip.z + P.dpos0[2]);
+    V3 v = mk3(0.f, 0.f, 0.f);
+    float dt = P.relax_params[0], damp = P.relax_params[1];
+    float4 fe = make_float4(0.f, 0.f, 0.f, 0.f);
+    int total_it = 0;
+    const unsigned lane = threadIdx.x & 31u;
+    const int leader = __ffs(members) - 1;
+    for (int iz = 0; iz < nzs; ++iz) {
+        StageBox B;
+        B.s = slice;
+        B.ok = false;
+        if (staging) {
+            // this lane's cell (slab indices), -1 if it is not an interior, stored cell
+            float fx, fy, fz;
+            tex_coord(__fmaf_rn(pos.x, G.ax, G.aw), G.fnx, fx);
+            tex_coord(__fmaf_rn(pos.y, G.by, G.bw), G.fny, fy);
+            tex_coord(__fmaf_rn(pos.z, G.cz, G.cw), G.fnz, fz);
+            const int cx = (int)fx - G.x_lo, cy = (int)fy - G.y_lo, cz = (int)fz - G.z_lo;
+            const bool in = fx == fx && fy == fy && fz == fz && cx >= 0 && cy >= 0 && cz >= 0 &&
+                            cx < G.nx_slab && cy + 1 < G.ny_slab && cz + 1 < G.nz_slab;
+            // warp min / max over the members (redux.sync: defined for any member mask); lanes without a
+            // stored interior cell contribute the neutral values
+            int mn[3], mx[3];
+            mn[0] = __reduce_min_sync(members, in ? cx : INT_MAX);
+            mn[1] = __reduce_min_sync(members, in ? cy : INT_MAX);
+            mn[2] = __reduce_min_sync(members, in ? cz : INT_MAX);
+            mx[0] = __reduce_max_sync(members, in ? cx : -1);
+            mx[1] = __reduce_max_sync(members, in ? cy : -1);
+            mx[2] = __reduce_max_sync(members, in ? cz : -1);
+            if (mn[0] != INT_MAX) {  // then every mn/mx is a cell index in [0, n_slab)
+                const int bx0 = max(mn[0] - 1, 0), bx1 = min(mx[0] + 1, G.nx_slab - 1);
+                const int by0 = max(mn[1] - 1, 0), by1 = min(mx[1] + 2, G.ny_slab - 1);
+                const int bz0 = max(mn[2] - 1, 0), bz1 = min(mx[2] + 2, G.nz_slab - 1);
+                B.x0 = bx0; B.y0 = by0; B.z0 = bz0;
+                B.nx = bx1 - bx0 + 1; B.ny = by1 - by0 + 1; B.nz = bz1 - bz0 + 1;
+                if (B.nx >= 1 && B.ny >= 1 && B.nz >= 1 && B.nx <= STAGE_CAP && B.ny <= STAGE_CAP &&
+                    B.nz <= STAGE_CAP && B.nx * B.ny * B.nz <= STAGE_CAP) {
+                    const int rows = B.ny * B.nz;
+                    const unsigned row_bytes = (unsigned)B.nx * 32u;
+                    if ((int)lane == leader) {
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                                     :: "r"(bar), "r"(row_bytes * (unsigned)rows) : "memory");
+                    }
+                    __syncwarp(members);
+                    const int rank = __popc(members & ((1u << lane) - 1u)), nmem = __popc(members);
+                    for (int r = rank; r < rows; r += nmem) {
+                        const int y = r % B.ny, z = r / B.ny;
+                        const float4* src = G.g + 2 * (((size_t)(bz0 + z) * G.ny_slab + (by0 + y)) * G.nx_slab + bx0);
+                        const unsigned dst = smem_addr(slice + 2 * (size_t)r * B.nx);
+                        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+                                     "[%0], [%1], %2, [%3];" :: "r"(dst), "l"(src), "r"(row_bytes), "r"(bar)
+                                     : "memory");
+                    }
+                    unsigned spins = 0;
+                    bool done = mbar_try_wait(bar, parity);
+                    while (!done && ++spins < STAGE_SPIN) done = mbar_try_wait(bar, parity);
+                    if (!done) {
+                        // record it, give the copies a last bounded chance, and stop staging for good
+                        atomicOr(status, 1u);
+                        spins = 0;
+                        while (!done && ++spins < STAGE_SPIN) done = mbar_try_wait(bar, parity);
+                        staging = false;
+                    } else {
+                        B.ok = true;
+                    }
+                    parity ^= 1u;
+                    __syncwarp(members);
+                }
+            }
+        }
+        int it = 0;
+        bool conv = false;
+        while (true) {
+            if (it >= P.max_iter) break;
+            ++it;
+            ++total_it;
+            fe = interp_fe_staged(G, pos, T, B);
+            if (fe.w != fe.w) break;
+            const V3 ft = tip_force(sub3(pos, tip), ld4(P.stiffness), ld4(P.dpos0));
+            V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
+            f.z = __fadd_rn(f.z, P.surfFF[0]);
+            if (dot3(f, f) < P.f2conv) {
+                conv = true;
+                break;
+            }
+            md_step_c(f, v, pos, dt, damp, __fmul_rn(P.relax_params[0], 0.1f), P.relax_params[0], P.relax_params[1],
+                      (P.flags & SPM_FLAG_FIRE) != 0);
+        }
+        if (!conv) fe = interp_fe_staged(G, pos, T, B);  // the position moved after the last sample
+        const long long o = sbase + iz;
+        FEs[o] = fe;
+        float z0 = __fmul_rn(fe.x, 0.f);
+        z0 = __fmaf_rn(fe.y, 0.f, z0);
+        z0 = __fmaf_rn(fe.z, 0.f, z0);
+        z0 = __fmaf_rn(fe.w, 0.f, z0);
+        z0 = __fmaf_rn(pos.x, 0.f, z0);
+        z0 = __fmaf_rn(pos.y, 0.f, z0);
+        z0 = __fmaf_rn(pos.z, 0.f, z0);
+        const bool finite = (z0 == 0.f);
+        PPs[o] = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
+        tip.z = __fadd_rn(tip.z, dz);
+        pos.z = __fadd_rn(pos.z, dz);
+        v = mk3(0.f, 0.f, 0.f);
+        __syncwarp(members);  // the tile's lanes start the next z-step (and its staging) together
+    }
+    if (iter_count) iter_count[pix] = total_it;
+}
+
+__global__ void __launch_bounds__(STAGE_WARPS * 32, 4)
+batch_relax_staged_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
+                          const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
+                          float4* __restrict__ FEs, float4* __restrict__ PPs, int* __restrict__ iter_count,
+                          unsigned* __restrict__ counter) {
+    __shared__ __align__(128) ulonglong2 s_box[STAGE_WARPS][2 * STAGE_CAP];
+    __shared__ __align__(8) unsigned long long s_bar[STAGE_WARPS];
+    const float dz = P.tipC[3];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned bar = smem_addr(&s_bar[warp]);
+    if (lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    unsigned parity = 0;
+    bool staging = true;
+    while (true) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(counter, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n_slots) return;  // warp-uniform
+        const int m = SPM_MOL_BY(slot_off, mols, n_mol, (long long)base);
+        const spm_batch_mol* D = mols + m;
+        int k;
+        const bool valid = slot_pixel(D, base + lane - (unsigned)D->slot_off, th_log2, k);
+        const unsigned members = __ballot_sync(0xffffffffu, valid);
+        if (valid)
+            relax_tile_stroke_staged(D, grid, pts, P, FEs, PPs, iter_count, k, dz, members, s_box[warp], bar, parity,
+                                     staging, counter + 1);
+        // lanes outside the tile keep the warp's staging state in step with the members'
+        parity = __shfl_sync(0xffffffffu, parity, __ffs(members) - 1);
+        staging = __shfl_sync(0xffffffffu, staging, __ffs(members) - 1);
+        __syncwarp();  // the whole warp draws the next tile
+    }
+}
+
 }  // namespace
 }  // namespace spm
 
@@ -957,7 +1194,12 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     SPM_REQUIRE(shape->rx_ctas_per_sm >= 0, "spm_batch_relax: rx_ctas_per_sm=%d", shape->rx_ctas_per_sm);
     int th_log2 = 0;
     while ((1 << th_log2) < h) th_log2++;
-    SPM_REQUIRE(shape->rx_regs >= 0 && shape->rx_regs <= 4, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
+    SPM_REQUIRE(shape->rx_regs >= 0 && shape->rx_regs <= 5, "spm_batch_relax: rx_regs=%d", shape->rx_regs);
+    if (shape->rx_regs == 5)
+        SPM_REQUIRE(thr == 128 && shape->grid_layout == 0 && shape->rx_sync == 1 &&
+                    !(p->flags & (SPM_FLAG_POLISH | SPM_FLAG_WARM)),
+                    "spm_batch_relax: rx_regs=5 (shared-memory slab staging) takes 128-thread CTAs, x-pair slabs, "
+                    "rx_sync = 1 and neither SPM_FLAG_POLISH nor SPM_FLAG_WARM");
     SPM_REQUIRE(shape->rx_regs != 4 || thr <= 128, "spm_batch_relax: rx_regs=4 takes CTAs of at most 128 threads, "
                 "rx_threads=%d", thr);
     SPM_REQUIRE(shape->grid_layout == 0 || shape->grid_layout == 1, "spm_batch_relax: grid_layout=%d",
@@ -989,8 +1231,9 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
         {batch_relax_sync_kernel<3, false, 4, true>, batch_relax_sync_kernel<4, false, 4, true>,
          batch_relax_sync_kernel<2, true, 4, true>, batch_relax_sync_kernel<3, true, 4, true>,
          batch_relax_sync_kernel<5, true, 4, true>}};
-    const Kern kern = (p->flags & SPM_FLAG_POLISH) ? polished[shape->grid_layout][shape->rx_regs]
-                                                   : table[shape->rx_sync][shape->grid_layout][shape->rx_regs];
+    const Kern kern = shape->rx_regs == 5 ? batch_relax_staged_kernel
+                      : (p->flags & SPM_FLAG_POLISH) ? polished[shape->grid_layout][shape->rx_regs]
+                                                      : table[shape->rx_sync][shape->grid_layout][shape->rx_regs];
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
@@ -1003,7 +1246,8 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     const unsigned blocks = (unsigned)(need < cap ? need : cap);
     cudaStream_t st = as_stream(stream);
     unsigned* ctr = static_cast<unsigned*>(workspace);
-    if (cudaMemsetAsync(ctr, 0, sizeof(unsigned), st) != cudaSuccess)
+    // word 0: the slot counter; word 1: the staged variant's wait-timeout flag
+    if (cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned), st) != cudaSuccess)
         return set_error(SPM_ERR_CUDA, "spm_batch_relax: cannot reset the slot counter");
     kern<<<blocks, thr, 0, st>>>(n_mol, mols, (unsigned)n_slots, th_log2, grid,
                                                reinterpret_cast<const float4*>(points), *p,

@@ -267,6 +267,20 @@ def df_dir(FEs, spacing, osc_dir=(0., 0., 1.)):
     return df
 
 
+def pair_fe_points(kind, atoms, params, queries, Qs, QZs):
+    """Uncapped pair sums (F, E) at (n,3) query points -> (n,4) float32 CUDA tensor."""
+    q = _as_dev(queries, F32, (3,), "queries")
+    dev = q.device
+    a = torch.as_tensor(np.ascontiguousarray(atoms, np.float32), device=dev).reshape(-1, 4).contiguous()
+    pstride = 4 if kind == _lib.SPM_KIND_MORSE else 2
+    prm = torch.as_tensor(np.ascontiguousarray(params, np.float32), device=dev).reshape(-1, pstride).contiguous()
+    out = torch.empty((q.shape[0], 4), dtype=F32, device=dev)
+    rc = lib().spm_pair_fe_points(int(kind), a.shape[0], ptr(a), ptr(prm), ptr(q), q.shape[0], hptr(hostvec(Qs)),
+                                  hptr(hostvec(QZs)), ptr(out), stream_ptr())
+    check(rc, "spm_pair_fe_points")
+    return out
+
+
 def _diss_lists(h_scan, h_df, amp, osc_dir, dev):
     """compute_dissipation's integration windows (AFM.py:3266-3273): for every output height, the scan
     heights within +-amp*|n_z| (all of them when fewer than two) -> (n, h, off, idx) for the kernels."""

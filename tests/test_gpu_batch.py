@@ -398,3 +398,21 @@ def test_batch_polish_and_warm_need_the_synchronised_schedule(cuda):
     b.build_grids()
     with pytest.raises((ValueError, RuntimeError), match="rx_sync"):
         b.relax()
+
+
+def test_batch_staged_relaxation_is_bit_identical(cuda):
+    """rx_regs = 5: each warp's z-slab staged in shared memory by bulk copies; every tile shape gives the
+    default kernel's FEs, PPs and step counts bit for bit, and no staging wait timed out."""
+    items = _items(0, n=5, seed=64)
+    base = _lib.lib().spm_batch_default_shape()
+    ref = AFMBatch(items)
+    ref.forward()
+    for h in (2, 4, 8, 16):
+        shape = _lib.BatchShape(*base.key())
+        shape.rx_regs, shape.grid_layout, shape.rx_sync, shape.rx_threads, shape.rx_tile_h = 5, 0, 1, 128, h
+        b = AFMBatch(items, shape=shape)
+        b.forward()
+        torch.cuda.synchronize()
+        assert torch.equal(b.FEs, ref.FEs) and torch.equal(b.PPs, ref.PPs), h
+        assert torch.equal(b.iter_count, ref.iter_count), h
+        assert int(b.workspace[1]) == 0, "a staging wait timed out"
