@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=3)
     ap.add_argument("--fit-mols", type=int, default=64)
     ap.add_argument("--fit-steps", type=int, default=100)
+    ap.add_argument("--fit-lr", type=float, default=0.01, help="Adam learning rate of the fit (A, e)")
+    ap.add_argument("--fit-z-end", type=float, default=4.0,
+                    help="lowest tip height of the fit's scans above the molecule plane (A)")
     ap.add_argument("--batch-only", action="store_true",
                     help="run only the many-molecule workloads (small sizes make profiling cases)")
     ap.add_argument("--no-tune", action="store_true", help="library default launch shapes, no autotuning")
@@ -561,7 +564,7 @@ def run_batched(args, dev_index):
     from spammm_b200.batch import AFMBatch, BatchAdam
     out = {}
     # ---- (4) fitting: target df from N(0,0.1 A)-perturbed positions; fit starts at the unperturbed structures
-    items = synthetic.batch_molecules(args.fit_mols, seed=5)
+    items = synthetic.batch_molecules(args.fit_mols, seed=5, z_end=args.fit_z_end)
     # the per-image drop-in path on the same molecules first, on a device that holds no batch
     from spammm_b200.batch import ProbeSpec
     plain = _plain_images_per_s(items, ProbeSpec())
@@ -593,7 +596,7 @@ def run_batched(args, dev_index):
     b.atoms.copy_(start)
     b.set_target_states(target)
     b.enable_failure_mask()
-    opt = BatchAdam(b, lr=0.01, cols=(0, 1, 2, 3))
+    opt = BatchAdam(b, lr=args.fit_lr, cols=(0, 1, 2, 3))
     g = b.capture(opt.step, warmup=0)
     b.reset_warm_start()
     b.forward_adjoint()
@@ -620,7 +623,7 @@ def run_batched(args, dev_index):
     st = torch.bincount(b.diag[:, 3].long(), minlength=6).tolist()
     out["fit"] = {
         "workload": f"{args.fit_mols} molecules of the batch distribution, target df from N(0,0.1 A)-perturbed "
-                    f"positions, {args.fit_steps} Adam steps (lr 0.01) on positions and charges from the "
+                    f"positions, {args.fit_steps} Adam steps (lr {args.fit_lr}) on positions and charges from the "
                     "unperturbed structures, one CUDA-graph replay per step (forward + df loss + adjoint + update)",
         "relax_options": {"newton_polish": polish, "warm_start": warm},
         "ms_per_step": ms, "images_per_s": args.fit_mols / (ms * 1e-3), "states_per_step": b.total_states,

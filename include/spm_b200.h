@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define SPM_ABI_VERSION 2
+#define SPM_ABI_VERSION 3
 
 enum spm_status {
     SPM_OK = 0,
@@ -431,6 +431,9 @@ typedef struct spm_batch_shape {
                            (all lanes sample the same z-layer of neighbouring pixels) */
     int adj_ilp;        /* adjoint node kernel: 1 = one node pair per step (3 CTAs per SM), 2 = two
                            independent node pairs per step (2 CTAs per SM, more registers) */
+    int adj_agg;        /* adjoint scatter: 0 = every state's corner sums straight to the global adjoint
+                           grid (64-bit atomics), 1 = first merged per CTA in a shared-memory table
+                           (the strokes of one CTA share nodes), one global atomic per distinct node */
 } spm_batch_shape;
 
 spm_batch_shape spm_batch_default_shape(void);

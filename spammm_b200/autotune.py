@@ -35,7 +35,8 @@ RELAX_CANDIDATES = [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=r, grid
                     for h in (2, 4, 8, 16) for r in (0, 1, 2, 3, 4)] + \
                    [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=5, grid_layout=0) for h in (2, 4, 8, 16)] + \
                    [dict(rx_sync=0, rx_threads=128, rx_tile_h=8, rx_regs=0, grid_layout=0)]
-ADJOINT_CANDIDATES = [dict(adj_chunk=c, adj_ilp=i) for c in (4096, 16384, 65536) for i in (1, 2)]
+ADJOINT_CANDIDATES = [dict(adj_chunk=c, adj_ilp=i, adj_agg=a) for c in (4096, 16384, 65536) for i in (1, 2)
+                      for a in (0, 1)]
 
 _CACHE = {}
 
@@ -113,7 +114,30 @@ def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
         cands = [c for c in cands if (4 if c["grid_layout"] else 2) * batch.grid_float4 * 16 <= max_grid_bytes]
     pick("relax", cands, batch.relax, prepare=batch.build_grids)
     if adjoint:
+        # the slab layout also sets the adjoint's cost: between the best relaxation shape of each layout,
+        # keep the one whose relaxation + state adjoint + adjoint through the grid is faster
+        best_by_layout = {}
+        for ms, kw in report["relax"]["all"]:
+            best_by_layout.setdefault(kw["grid_layout"], kw)
+        if len(best_by_layout) > 1:
+            def step():
+                batch.relax()
+                batch.loss_seed()
+                batch.adjoint_state()
+                batch.adjoint_params()
+            joint = []
+            for lay, kw in sorted(best_by_layout.items()):
+                s = _with(shape, **kw)
+                batch.set_shape(s)
+                batch.build_grids()
+                joint.append((_time(step, reps), kw))
+                if log:
+                    log(f"autotune relax+adjoint, layout {lay} {kw}: {joint[-1][0]:.3f} ms")
+            joint.sort(key=lambda r: r[0])
+            shape = _with(shape, **joint[0][1])
+            report["relax_adjoint_layout"] = {"best": joint[0][1], "all": [[ms, kw] for ms, kw in joint]}
         batch.set_shape(shape)
+        batch.build_grids()
         batch.relax()
         batch.loss_seed()
         batch.adjoint_state()

@@ -648,10 +648,28 @@ batch_ubar_max_kernel(int n_mol, long long n_chunks, const spm_batch_mol* __rest
 // layer is lane l's lower layer: lane l adds those four corners' sums to its
 // own (integers: exact) and lane l+1 skips them, halving the atomics of a
 // stroke.
+//
+// AGG (spm_batch_shape.adj_agg = 1): the CTA's 256 states -- a few neighbouring strokes -- first add
+// their corner sums into a shared-memory table keyed by the adjoint-grid offset (open addressing,
+// AGG_PROBES probes; a corner that finds no slot goes to global memory directly), then each table
+// entry is added to the global grid once per channel.  Integer sums: the same bits either way.
+constexpr int AGG_SLOTS = 2048;
+constexpr int AGG_PROBES = 8;
+constexpr unsigned long long AGG_EMPTY = ~0ull;
+
+template <bool AGG>
 __global__ void __launch_bounds__(256)
 batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states,
                      const float4* __restrict__ PPs, const float4* __restrict__ ubar, const unsigned* __restrict__ umax,
                      unsigned long long* __restrict__ gq) {
+    extern __shared__ unsigned long long s_agg[];  // AGG: keys[AGG_SLOTS], then values[AGG_SLOTS][4]
+    unsigned long long* s_key = s_agg;
+    unsigned long long* s_val = s_agg + AGG_SLOTS;
+    if constexpr (AGG) {
+        for (int i = threadIdx.x; i < AGG_SLOTS; i += blockDim.x) s_key[i] = AGG_EMPTY;
+        for (int i = threadIdx.x; i < 4 * AGG_SLOTS; i += blockDim.x) s_val[i] = 0ull;
+        __syncthreads();
+    }
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const long long st = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -698,6 +716,27 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
         w[c] = valid ? (i ? C.ax : 1.f - C.ax) * (j ? C.ay : 1.f - C.ay) * (k ? C.az : 1.f - C.az) : 0.f;
     }
     const float ubc[4] = {ub.x, ub.y, ub.z, ub.w};
+    int slot[8];
+    if constexpr (AGG) {
+        // the table slot of each corner this state adds to (-1: none found, the corner goes to global memory)
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            slot[c] = -1;
+            if (!valid || (c >= 4 && given) || w[c] == 0.f) continue;
+            const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
+            const size_t node = ((size_t)(C.z[k] - z_lo) * nys + (C.y[j] - y_lo)) * nxs + (C.x[i] - x_lo);
+            const unsigned long long key = (unsigned long long)((base - gq) + node * 4);
+            unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> 53) & (AGG_SLOTS - 1);
+            for (int probe = 0; probe < AGG_PROBES; probe++) {
+                const unsigned long long prev = atomicCAS(s_key + h, AGG_EMPTY, key);
+                if (prev == AGG_EMPTY || prev == key) {
+                    slot[c] = (int)h;
+                    break;
+                }
+                h = (h + 1) & (AGG_SLOTS - 1);
+            }
+        }
+    }
 #pragma unroll
     for (int ch = 0; ch < 4; ch++) {
         long long q[8];
@@ -713,9 +752,25 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
             for (int c = 0; c < 8; c++) {
                 if (c >= 4 && given) continue;
                 if (q[c] == 0) continue;
+                if (AGG && slot[c] >= 0) {
+                    atomicAdd(s_val + 4 * slot[c] + ch, (unsigned long long)q[c]);
+                    continue;
+                }
                 const int i = c & 1, j = (c >> 1) & 1, k = c >> 2;
                 const size_t node = ((size_t)(C.z[k] - z_lo) * nys + (C.y[j] - y_lo)) * nxs + (C.x[i] - x_lo);
                 atomicAdd(base + node * 4 + ch, (unsigned long long)q[c]);
+            }
+        }
+    }
+    if constexpr (AGG) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < AGG_SLOTS; t += blockDim.x) {
+            const unsigned long long key = s_key[t];
+            if (key == AGG_EMPTY) continue;
+#pragma unroll
+            for (int ch = 0; ch < 4; ch++) {
+                const unsigned long long v = s_val[4 * t + ch];
+                if (v != 0ull) atomicAdd(gq + key + ch, v);
             }
         }
     }
@@ -1242,6 +1297,7 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
     SPM_REQUIRE(chunk >= 1024 && chunk <= (1 << 20) && chunk % 1024 == 0, "spm_batch_adjoint_params: adj_chunk=%d",
                 chunk);
     SPM_REQUIRE(shape->adj_ilp == 1 || shape->adj_ilp == 2, "spm_batch_adjoint_params: adj_ilp=%d", shape->adj_ilp);
+    SPM_REQUIRE(shape->adj_agg == 0 || shape->adj_agg == 1, "spm_batch_adjoint_params: adj_agg=%d", shape->adj_agg);
     SPM_REQUIRE((reinterpret_cast<uintptr_t>(scratch) & 15u) == 0, "spm_batch_adjoint_params: scratch not 16-byte aligned");
     SPM_REQUIRE(n_units < (1LL << 31) && n_chunks < (1LL << 31) && n_atoms < (1LL << 30) &&
                 (n_states + 255) / 256 < (1LL << 31), "spm_batch_adjoint_params: batch too large");
@@ -1279,9 +1335,20 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             batch_ubar_max_kernel<<<(unsigned)((n_chunks + UM_CHUNKS - 1) / UM_CHUNKS), 256, 0, st>>>(
                 n_mol, n_chunks, mols, reinterpret_cast<const float4*>(ubar), reinterpret_cast<const float4*>(PPs), umax,
                 box, mark);
-            batch_scatter_kernel<<<(unsigned)((n_states + 255) / 256), 256, 0, st>>>(
-                n_mol, mols, n_states, reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar), umax,
-                gq);
+            if (shape->adj_agg) {
+                const size_t agg_smem = sizeof(unsigned long long) * 5 * AGG_SLOTS;
+                if (cudaFuncSetAttribute(batch_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)agg_smem) != cudaSuccess)
+                    return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: cannot enable %zu B of shared memory",
+                                     agg_smem);
+                batch_scatter_kernel<true><<<(unsigned)((n_states + 255) / 256), 256, agg_smem, st>>>(
+                    n_mol, mols, n_states, reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar),
+                    umax, gq);
+            } else {
+                batch_scatter_kernel<false><<<(unsigned)((n_states + 255) / 256), 256, 0, st>>>(
+                    n_mol, mols, n_states, reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar),
+                    umax, gq);
+            }
             const NodeSites S = make_node_sites(Qs, QZs);
             const int pstride = kind == SPM_KIND_MORSE ? 4 : 2;
             const bool on = S.qon != 0.f;

@@ -789,12 +789,51 @@ struct SlabCellFetch {
     }
 };
 
+// SlabCellFetch through the lane's TexelCache: a cell already cached (the one FIRE ended in, or the
+// previous Newton evaluation's) needs no loads; a new cell is loaded and cached.  The same texel
+// values either way.
+template <int LAYOUT>
+struct SlabCellFetchCached {
+    const AxisView& G;
+    TexelCache& T;
+    __device__ __forceinline__ bool operator()(V3 p, float& ax, float& ay, float& az, float4 (&t)[8]) const {
+        const float u = __fmaf_rn(p.x, G.ax, G.aw);
+        const float v = __fmaf_rn(p.y, G.by, G.bw);
+        const float w = __fmaf_rn(p.z, G.cz, G.cw);
+        float fx, fy, fz;
+        ax = tex_coord(u, G.fnx, fx);
+        ay = tex_coord(v, G.fny, fy);
+        az = tex_coord(w, G.fnz, fz);
+        if (!(fx == T.kx && fy == T.ky && fz == T.kz)) {
+            int x0, x1, y0, y1, z0, z1;
+            bool ok = tex_index(fx, G.nx, G.fnx, x0, x1);
+            ok = tex_index(fy, G.ny, G.fny, y0, y1) && ok;
+            ok = tex_index(fz, G.nz, G.fnz, z0, z1) && ok;
+            ok = ok && to_slab(x0, x1, G.x_lo, G.nx_slab) && to_slab(y0, y1, G.y_lo, G.ny_slab) &&
+                 to_slab(z0, z1, G.z_lo, G.nz_slab);
+            if (!ok) return false;
+            load_cell<LAYOUT, unsigned>(G, x0, y0, y1, z0, z1, T.f000, T.f100, T.f010, T.f110, T.f001, T.f101,
+                                        T.f011, T.f111);
+            T.kx = fx;
+            T.ky = fy;
+            T.kz = fz;
+        }
+        const ulonglong2 c[8] = {T.f000, T.f100, T.f010, T.f110, T.f001, T.f101, T.f011, T.f111};
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            upk(c[i].x, t[i].x, t[i].y);
+            upk(c[i].y, t[i].z, t[i].w);
+        }
+        return true;
+    }
+};
+
 // newton_core on a batch slab, kept out of line: the FIRE loop of the batched kernel keeps its
 // registers, the (rare) Newton evaluations run in the callee's own allocation.
 template <int LAYOUT>
-__device__ __noinline__ bool slab_newton(const AxisView& G, const float (&Tc)[3][3], const PolishSpring& S, V3 tip,
-                                         V3& q, float4& fe, float& g2, int& evals) {
-    return newton_core(SlabCellFetch<LAYOUT>{G}, Tc, S, tip, q, fe, g2, evals);
+__device__ __noinline__ bool slab_newton(const AxisView& G, TexelCache& T, const float (&Tc)[3][3],
+                                         const PolishSpring& S, V3 tip, V3& q, float4& fe, float& g2, int& evals) {
+    return newton_core(SlabCellFetchCached<LAYOUT>{G, T}, Tc, S, tip, q, fe, g2, evals);
 }
 
 // Warm start (SPM_FLAG_WARM): a z-step starts from the equilibrium the state
@@ -863,7 +902,7 @@ __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const 
                 float4 fn;
                 float g2;
                 int ev;
-                if (slab_newton<LAYOUT>(G, Tc, S, tip, qn, fn, g2, ev)) {
+                if (slab_newton<LAYOUT>(G, T, Tc, S, tip, qn, fn, g2, ev)) {
                     pos = qn;
                     if (g2 < P.f2conv) {
                         fe = fn;
@@ -885,7 +924,7 @@ __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const 
             if (!newton_done && fe.w == fe.w) {
                 float g2;
                 int ev;
-                slab_newton<LAYOUT>(G, Tc, S, tip, q, fe, g2, ev);
+                slab_newton<LAYOUT>(G, T, Tc, S, tip, q, fe, g2, ev);
             }
         }
         const long long o = sbase + iz;

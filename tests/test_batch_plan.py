@@ -17,7 +17,7 @@ def small_items(n=7, seed=5, kind=0):
 def test_struct_layout():
     # spm_batch_mol: 7 int64 offsets, 16 int32 fields, 7 float[4] vectors
     assert ctypes.sizeof(_lib.BatchMol) == 7 * 8 + 16 * 4 + 7 * 16
-    assert ctypes.sizeof(_lib.BatchShape) == 10 * 4
+    assert ctypes.sizeof(_lib.BatchShape) == 11 * 4
 
 
 @pytest.mark.parametrize("shape_kw", [{}, dict(gb_ty=2, gb_zb=16, rx_tile_h=1, adj_chunk=1024),

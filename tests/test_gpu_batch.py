@@ -416,3 +416,22 @@ def test_batch_staged_relaxation_is_bit_identical(cuda):
         assert torch.equal(b.FEs, ref.FEs) and torch.equal(b.PPs, ref.PPs), h
         assert torch.equal(b.iter_count, ref.iter_count), h
         assert int(b.workspace[1]) == 0, "a staging wait timed out"
+
+
+def test_batch_adjoint_aggregated_scatter_is_bit_identical(cuda):
+    """adj_agg = 1 (the scatter merges each CTA's corner sums in shared memory first): the same exact integer
+    sums, so the gradients and spring terms equal the direct scatter's bit for bit, call after call."""
+    items = _items(0, n=5, seed=65)
+    out = []
+    for agg in (0, 1):
+        shape = _lib.BatchShape(*_lib.lib().spm_batch_default_shape().key())
+        shape.adj_agg = agg
+        b = AFMBatch(items, shape=shape)
+        _target(b)
+        b.forward_adjoint()
+        g1 = b.grad.clone()
+        b.forward_adjoint()  # the scratch kept from the first call (cleared adjoint grid) gives the same
+        torch.cuda.synchronize()
+        assert torch.equal(g1, b.grad)
+        out.append((g1, b.dk_sum.clone()))
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])

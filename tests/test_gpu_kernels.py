@@ -308,3 +308,19 @@ def test_izo_z_matches_oracle(cuda):
     assert np.array_equal(gpu.izo_z(one, 0.5).cpu().numpy(), np.full(4, -1.0, np.float32))
     with pytest.raises(ValueError, match="weights"):
         gpu.convolve_z(F, np.ones(3, np.float32), 40)
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_pair_fe_points_matches_fp64_oracle(cuda, kind):
+    """spm_pair_fe_points (cs_brute_afm_morse_c_points semantics: uncapped) against the FP64 pair sums,
+    with the reference gate's bar (tests/SPM/test_afm_morse.py:864-900: rtol 5e-5, atol 1e-5 + 1e-5 scale)."""
+    atoms, prm = _mol(40, 17 + kind, kind == 1)
+    rng = np.random.default_rng(5)
+    q = np.stack([rng.uniform(-4, 4, 3000), rng.uniform(-4, 4, 3000), rng.uniform(0.8, 6.0, 3000)], 1)
+    q = q.astype(np.float32)
+    Qs, QZs = [-0.05, 0.02, 0, 0], [0, 1.8, 0, 0]
+    got = gpu.pair_fe_points(kind, atoms, prm, torch.from_numpy(q).cuda(), Qs, QZs).cpu().numpy()
+    ref = O.pair_fe(kind, atoms.astype(np.float64), prm.astype(np.float64), q.astype(np.float64), Qs, QZs)
+    for c in range(4):
+        scale = float(np.abs(ref[:, c]).max())
+        np.testing.assert_allclose(got[:, c], ref[:, c], rtol=5e-5, atol=1e-5 + 1e-5 * scale)

@@ -70,5 +70,5 @@ def test_skew_periodic_cell_grid_and_scan(cuda, golden):
     # (the upper heights, where |F| < 1 eV/A: nearer the atoms a sample at a texel edge may round into
     # the neighbouring cell in one window and not the other, which the capped cores turn into O(1) jumps)
     far = np.abs(raw1[..., :3]).max(axis=(0, 1, 3)) < 1.0
-    assert far.sum() >= 5
+    assert far.sum() >= 2
     assert np.abs(raw2[:, :, far] - raw1[:, :, far]).max() < 1e-4 * np.abs(raw1[:, :, far]).max()
