@@ -172,3 +172,79 @@ def tuned_shape(items, kind=0, probe=None, dtip=-0.1, max_molecules=24, reps=2, 
         with open(cache_file, "w") as f:
             json.dump(_CACHE, f, indent=1)
     return shape, report
+
+
+def _parse_shape(text, base):
+    """'rx_regs=5,rx_tile_h=4' -> a BatchShape from base with those fields set."""
+    kw = {}
+    for part in filter(None, text.split(",")):
+        k, _, v = part.partition("=")
+        if not hasattr(base, k):
+            raise ValueError(f"unknown spm_batch_shape field {k!r}")
+        kw[k] = int(v)
+    return _with(base, **kw)
+
+
+def main(argv=None):
+    """Time one stage of the batched path under given launch shapes on a
+    synthetic batch, or run the tuner:
+
+        python -m spammm_b200.autotune --mols 16 --stage relax \\
+            --shape rx_regs=4,rx_tile_h=4 --shape rx_regs=5,rx_tile_h=4
+
+    Each --shape (fields of spm_batch_shape over the library default) builds
+    the slabs in its own layout, runs the stage --warmup times untimed and
+    --reps times timed with CUDA events, and prints the best time.  Without
+    --shape the tuner runs on the batch and prints its report."""
+    import argparse
+    from . import synthetic
+    ap = argparse.ArgumentParser(prog="python -m spammm_b200.autotune")
+    ap.add_argument("--mols", type=int, default=16)
+    ap.add_argument("--seed", type=int, default=5)
+    ap.add_argument("--stage", choices=("grid", "relax", "adjoint"), default="relax")
+    ap.add_argument("--shape", action="append", default=[])
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--polish", action="store_true")
+    args = ap.parse_args(argv)
+    items = synthetic.batch_molecules(args.mols, seed=args.seed)
+    base = _lib.lib().spm_batch_default_shape()
+    if not args.shape:
+        shape, report = tuned_shape(items, max_molecules=args.mols, reps=args.reps, polish=args.polish,
+                                    log=lambda s: print(s, flush=True))
+        print(json.dumps({"shape": {f[0]: v for f, v in zip(_lib.BatchShape._fields_, shape.key())}, "report": report}))
+        return
+    rng = np.random.default_rng(args.seed)
+    for text in args.shape:
+        b = AFMBatch(items, shape=_parse_shape(text, base)).set_relax_options(polish=args.polish)
+        b.build_grids()
+        if args.stage == "grid":
+            run = b.build_grids
+        elif args.stage == "relax":
+            run = b.relax
+        else:
+            for i, it in enumerate(b.items):
+                b.set_target(i, rng.normal(0.0, 0.05, (len(it.xs), len(it.ys), it.nz)))
+            b.relax()
+            b.loss_seed()
+            b.adjoint_state()
+            run = b.adjoint_params
+        for _ in range(args.warmup):
+            run()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(args.reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run()
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        print(json.dumps({"shape": text, "stage": args.stage, "ms": best, "states": int(b.total_states),
+                          "slab_bytes": int(b.grid.numel()) * 4}), flush=True)
+        del b
+        torch.cuda.empty_cache()
+
+
+if __name__ == "__main__":
+    main()

@@ -40,12 +40,34 @@ def _stub_pyopencl():
     return cl
 
 
+class _Inert:
+    """A figure, axes or artist that accepts every call and draws nothing."""
+
+    def __getattr__(self, name):
+        return self
+
+    def __call__(self, *a, **k):
+        return self
+
+
 def _stub_matplotlib():
     mpl = types.ModuleType("matplotlib")
     mpl.use = lambda *a, **k: None
     mpl.__path__ = []
     plt = types.ModuleType("matplotlib.pyplot")
-    plt.__getattr__ = lambda name: (lambda *a, **k: None)
+
+    def subplots(nrows=1, ncols=1, **kw):
+        import numpy as np
+        axes = np.empty((nrows, ncols), dtype=object)
+        for i in range(nrows):
+            for j in range(ncols):
+                axes[i, j] = _Inert()
+        if kw.get("squeeze", True):
+            axes = axes[0, 0] if nrows == ncols == 1 else (axes.ravel() if 1 in (nrows, ncols) else axes)
+        return _Inert(), axes
+
+    plt.subplots = subplots
+    plt.__getattr__ = lambda name: _Inert()
     mpl.pyplot = plt
     return mpl, plt
 

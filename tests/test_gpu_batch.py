@@ -326,7 +326,7 @@ def test_autotune_returns_valid_shape(cuda):
     from spammm_b200 import autotune
     items = _items(0, n=5, seed=71)
     shape, report = autotune.tuned_shape(items, max_molecules=3, reps=1)
-    assert set(report) == {"grid", "relax", "adjoint"}
+    assert {"grid", "relax", "adjoint"} <= set(report) <= {"grid", "relax", "adjoint", "relax_adjoint_layout"}
     ref = AFMBatch(items)
     ref.forward()
     b = AFMBatch(items, shape=shape)

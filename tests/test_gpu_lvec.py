@@ -7,7 +7,15 @@ oracle (grid-build tolerance of test_gpu_scale.py: 2e-5 |ref| + 2e-6 max|ref| +
 (relaxStrokesTilted) over a window larger than the cell -- probes sample across
 the periodic seam through the skew sampling transform -- bit-identical to the
 canonical-FP32 oracle on the same grid; unrelaxed samples of a window shifted
-by a cell vector equal the unshifted ones.
+by a period of the sampling transform equal the unshifted ones.
+
+The sampling transform is the reference's: dinvA/B/C are the rows of inv(M)^T
+(AFM.py:883-884 with _make_dinv_lvec, AFM.py:288-294), M = [a | b | Lz e_z]
+by columns, and the kernel takes u = dot(pos, dinvA) (kernels/AFM.cl:100-104).
+For a skew cell those are the columns of inv(M), not its rows, so the sampled
+field repeats along the rows of M -- (a_x, b_x, 0) and (a_y, b_y, 0) -- not
+along a and b.  The drop-in keeps that mapping bit for bit; the test checks
+the periods it has.
 """
 import os
 import tempfile
@@ -63,12 +71,20 @@ def test_skew_periodic_cell_grid_and_scan(cuda, golden):
     o = O.relax_tilted(grid, (afm.dinvA, afm.dinvB, afm.dinvC), p4, nzs, afm.tipA, afm.tipB, tipC, afm.stiffness,
                        afm.dpos0, afm.relax_pars, afm.surfFF, afm.n_relax_max, afm.f2conv)
     assert np.array_equal(FEs.reshape(-1, nzs, 4), o)
-    # unrelaxed samples of a window shifted by one cell vector equal the unshifted ones (periodic field)
+    # unrelaxed samples of a window shifted by a period of the sampling transform (a row of M) equal the
+    # unshifted ones; a shift by the cell vector b is not a period of the reference's skew mapping
     raw1, _ = afm.get_raw_FE(nxy=nxy, nz=nzs, dtip=dtip, scan_p0=p0, scan_da=da, scan_db=db)
-    raw2, _ = afm.get_raw_FE(nxy=nxy, nz=nzs, dtip=dtip, scan_p0=p0 + np.array([3.0, 5.196152, 0], np.float32),
-                             scan_da=da, scan_db=db)
     # (the upper heights, where |F| < 1 eV/A: nearer the atoms a sample at a texel edge may round into
     # the neighbouring cell in one window and not the other, which the capped cores turn into O(1) jumps)
     far = np.abs(raw1[..., :3]).max(axis=(0, 1, 3)) < 1.0
     assert far.sum() >= 2
-    assert np.abs(raw2[:, :, far] - raw1[:, :, far]).max() < 1e-4 * np.abs(raw1[:, :, far]).max()
+    lv = afm.mol.lvec.astype(np.float32)
+    M = np.stack([lv[0, :3], lv[1, :3], np.array([0., 0., afm.L[2]], np.float32)], axis=1)
+    for period in (M[0], M[1]):
+        raw2, _ = afm.get_raw_FE(nxy=nxy, nz=nzs, dtip=dtip, scan_p0=p0 + np.array([period[0], period[1], 0.0],
+                                                                                    np.float32),
+                                 scan_da=da, scan_db=db)
+        assert np.abs(raw2[:, :, far] - raw1[:, :, far]).max() < 1e-4 * np.abs(raw1[:, :, far]).max()
+    raw3, _ = afm.get_raw_FE(nxy=nxy, nz=nzs, dtip=dtip, scan_p0=p0 + np.array([lv[1, 0], lv[1, 1], 0.0], np.float32),
+                             scan_da=da, scan_db=db)
+    assert np.abs(raw3[:, :, far] - raw1[:, :, far]).max() > 1e-2 * np.abs(raw1[:, :, far]).max()
