@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define SPM_ABI_VERSION 3
+#define SPM_ABI_VERSION 4
 
 enum spm_status {
     SPM_OK = 0,
@@ -52,12 +52,14 @@ enum spm_status {
                                  opposite to the forward ones (SPM_FLAG_FLIP_Z inverted): the forward
                                  and reverse=True scans of AFMulator.scan_fdbm (AFM.py:584-633) in one
                                  launch; n_scan even */
-#define SPM_FLAG_WARM   16    /* spm_batch_relax only, with rx_sync = 1: PPs is read as well as written;
+#define SPM_FLAG_WARM   16    /* spm_batch_relax only, with rx_sync = 1 or 2: PPs is read as well as written;
                                  a z-step starts from the state's equilibrium in PPs (the previous
-                                 call's) when that converged and its displacement from the tip is
-                                 within 0.1 A per axis of the stroke continuation's start, else from
-                                 the continuation as without the flag (the probe jumped there, or no
-                                 previous equilibrium).  For fits whose atoms move a little per call.
+                                 call's) when that converged and the stroke arrives at the z-step
+                                 where it did in the previous call (its continuation start within
+                                 0.1 A per axis of the previous call's equilibrium of the z-step
+                                 before, shifted by the z-step), else from the continuation as
+                                 without the flag (the probe jumped on the way, or no previous
+                                 equilibrium).  For fits whose atoms move a little per call.
                                  With SPM_FLAG_POLISH a warm-started z-step first takes the polish's
                                  Newton steps from the previous equilibrium and runs FIRE only if they
                                  do not reach |F|^2 < f2conv (PPs.w then counts the Newton
@@ -428,7 +430,11 @@ typedef struct spm_batch_shape {
                            node: half the cache lines per sample, twice the memory) */
     int rx_sync;        /* relaxation schedule: 0 = every lane draws its next pixel when its stroke ends,
                            1 = a warp draws a pixel tile and its lanes step down the z-steps together
-                           (all lanes sample the same z-layer of neighbouring pixels) */
+                           (all lanes sample the same z-layer of neighbouring pixels), 2 = with
+                           SPM_FLAG_POLISH and SPM_FLAG_WARM two passes: the tiles of 1 with Newton's
+                           method from the previous equilibria only, each stroke stopping at its first
+                           z-step that needs FIRE, then those strokes' remaining z-steps, 32 strokes
+                           per warp stepping together (without both flags: as 1).  Same results */
     int adj_ilp;        /* adjoint node kernel: 1 = one node pair per step (3 CTAs per SM), 2 = two
                            independent node pairs per step (2 CTAs per SM, more registers) */
     int adj_agg;        /* adjoint scatter: 0 = every state's corner sums straight to the global adjoint
@@ -453,16 +459,21 @@ int spm_batch_grid_build(int kind, int n_mol, const spm_batch_mol* mols, long lo
                          const float* Qs, const float* QZs, float* grid, void* stream);
 
 /* SPM_RELAX_PP relaxation of every stroke of every molecule in one persistent
- * launch: lanes draw (molecule, pixel) slots from a device counter in
- * `workspace` (>= spm_relax_workspace_bytes() bytes, reset by the call).
+ * launch (two with shape->rx_sync = 2): lanes draw (molecule, pixel) slots
+ * from a device counter in `workspace` (workspace_bytes >=
+ * spm_batch_relax_workspace_bytes(n_slots, shape) bytes, device memory, its
+ * counters reset by the call; rx_sync = 2 also keeps its list of strokes
+ * for the second pass there, 48 bytes per slot).
  * p: probe frame, spring, FIRE settings, flags, tipC[3] = z-step; its dinv*,
  * nz and raster_ny are ignored (per-molecule values come from mols).
  * flags: SPM_FLAG_FIRE, SPM_FLAG_POLISH and SPM_FLAG_WARM (the last two with
- * shape->rx_sync = 1).
+ * shape->rx_sync = 1 or 2).
  * FEs, PPs out (total_states,4); iter_count (total_pixels) or NULL. */
+long long spm_batch_relax_workspace_bytes(long long n_slots, const spm_batch_shape* shape);
 int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n_slots, const spm_batch_shape* shape,
                     const float* grid, const float* points, const spm_scan_params* p,
-                    float* FEs, float* PPs, int* iter_count, void* workspace, void* stream);
+                    float* FEs, float* PPs, int* iter_count, void* workspace, long long workspace_bytes,
+                    void* stream);
 
 /* Frequency shift of every stroke, as spm_df_amp_dir with n = z and
  * dr = |dtip| on the stroke taken in ascending z (the stroke reversed), the

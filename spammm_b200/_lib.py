@@ -166,7 +166,8 @@ _SIGNATURES = {
     "spm_batch_default_shape": (BatchShape, []),
     "spm_batch_prepare": (_i, [ctypes.POINTER(BatchMol), _i, _BS, _LLP]),
     "spm_batch_grid_build": (_i, [_i, _i, _vp, _ll, _BS, _vp, _vp, _vp, _vp, _vp, _vp]),
-    "spm_batch_relax": (_i, [_i, _vp, _ll, _BS, _vp, _vp, _P, _vp, _vp, _vp, _vp, _vp]),
+    "spm_batch_relax": (_i, [_i, _vp, _ll, _BS, _vp, _vp, _P, _vp, _vp, _vp, _vp, _ll, _vp]),
+    "spm_batch_relax_workspace_bytes": (_ll, [_ll, _BS]),
     "spm_batch_df_amp": (_i, [_i, _vp, _ll, _vp, _d, _d, _vp, _vp]),
     "spm_batch_df_loss_seed": (_i, [_i, _vp, _ll, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _vp]),
     "spm_batch_loss_scratch_bytes": (_ll, [_ll, _i]),

@@ -3,7 +3,8 @@
 Every batched stage reads only its own fields of ``spm_batch_shape``:
 
   grid build   gb_ty (CTA rows: 32 x gb_ty threads), gb_zb (z-nodes per thread)
-  relaxation   rx_sync (z-synchronised warp tiles or independent lanes),
+  relaxation   rx_sync (z-synchronised warp tiles, independent lanes, or -- warm polished fits --
+               a Newton-only pass in tiles and a FIRE pass over the strokes it stopped),
                rx_threads (CTA size), rx_tile_h (pixel tile (32/h) x h per warp
                draw), rx_regs (80 / 64 registers, or the register texel cache
                at up to 128, 80 or 102 registers),
@@ -62,6 +63,35 @@ def _time(fn, reps):
     return best
 
 
+def _warm_step_ms(batch, reps, sigma=5e-3, seed=0):
+    """Time of a warm-started relaxation after the atoms moved by N(0, sigma) A per coordinate (a fit
+    step's size): the equilibria of the unmoved atoms are restored before every timed call.  The atoms
+    and the previous equilibria are put back afterwards."""
+    atoms0 = batch.atoms.clone()
+    batch.PPs.fill_(float("nan"))
+    batch.build_grids()
+    batch.relax()
+    pps0 = batch.PPs.clone()
+    g = torch.Generator(device=batch.atoms.device).manual_seed(seed)
+    batch.atoms[:, :3] += sigma * torch.randn(batch.atoms[:, :3].shape, generator=g, device=batch.atoms.device,
+                                              dtype=batch.atoms.dtype)
+    batch.build_grids()
+    best = float("inf")
+    for _ in range(reps + 1):  # the first call warms up
+        batch.PPs.copy_(pps0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.relax()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    batch.atoms.copy_(atoms0)
+    batch.PPs.fill_(float("nan"))
+    batch.build_grids()
+    return best
+
+
 def signature(items, kind):
     """Workload key: molecule count, kind, total atoms / pixels / states."""
     return (len(items), int(kind), int(sum(len(it.atoms) for it in items)), int(sum(it.n_scan for it in items)),
@@ -82,8 +112,9 @@ def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
     """Tune batch.shape in place, stage by stage; returns (shape, timings).
     max_grid_bytes: leave out slab layouts whose grid buffer would exceed it.  A batch relaxing
     with the polish or warm starts (set_relax_options) is tuned over the z-synchronised schedules
-    only, the ones that support them; warm starts are timed cold (the relaxation of a fit step
-    lies between the two)."""
+    only, the ones that support them; the relaxation shapes are timed cold, and with the polish and
+    warm starts both the fastest of them are also timed warm after the atoms moved by a fit step's
+    size, in the one-pass and the two-pass schedules (rx_sync = 1, 2), which then decides."""
     report = {}
     warm = batch.warm
     batch.set_relax_options(warm=False)
@@ -113,15 +144,43 @@ def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
     if max_grid_bytes is not None:
         cands = [c for c in cands if (4 if c["grid_layout"] else 2) * batch.grid_float4 * 16 <= max_grid_bytes]
     pick("relax", cands, batch.relax, prepare=batch.build_grids)
+    warm_pick = {}
+    if warm and batch.polish:
+        # a fit's later calls: the fastest cold shapes timed warm, each in the one-pass (rx_sync = 1) and the
+        # two-pass (rx_sync = 2) schedule; the best shape per slab layout is kept for the layout choice below
+        batch.set_relax_options(warm=True)
+        tried = []
+        for ms_cold, kw in report["relax"]["all"][:3] + [r for r in report["relax"]["all"][3:]
+                                                         if r[1]["grid_layout"] != report["relax"]["best"]["grid_layout"]][:1]:
+            for sync in (1, 2):
+                k2 = dict(kw, rx_sync=sync)
+                batch.set_shape(_with(shape, **k2))
+                ms = _warm_step_ms(batch, reps)
+                tried.append((ms, k2))
+                if log:
+                    log(f"autotune relax (warm step) {k2}: {ms:.3f} ms")
+        batch.set_relax_options(warm=False)
+        tried.sort(key=lambda r: r[0])
+        for ms, kw in tried:
+            warm_pick.setdefault(kw["grid_layout"], (ms, kw))
+        shape = _with(shape, **tried[0][1])
+        report["relax_warm"] = {"best": tried[0][1], "ms": tried[0][0], "all": [[ms, kw] for ms, kw in tried]}
     if adjoint:
         # the slab layout also sets the adjoint's cost: between the best relaxation shape of each layout,
         # keep the one whose relaxation + state adjoint + adjoint through the grid is faster
         best_by_layout = {}
         for ms, kw in report["relax"]["all"]:
             best_by_layout.setdefault(kw["grid_layout"], kw)
+        if warm_pick:  # the warm-step timings stand for the relaxation
+            best_by_layout = {lay: kw for lay, (ms, kw) in warm_pick.items()}
         if len(best_by_layout) > 1:
             def step():
                 batch.relax()
+                batch.loss_seed()
+                batch.adjoint_state()
+                batch.adjoint_params()
+
+            def adjoint_stages():
                 batch.loss_seed()
                 batch.adjoint_state()
                 batch.adjoint_params()
@@ -130,7 +189,11 @@ def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
                 s = _with(shape, **kw)
                 batch.set_shape(s)
                 batch.build_grids()
-                joint.append((_time(step, reps), kw))
+                if warm_pick:
+                    batch.relax()
+                    joint.append((warm_pick[lay][0] + _time(adjoint_stages, reps), kw))
+                else:
+                    joint.append((_time(step, reps), kw))
                 if log:
                     log(f"autotune relax+adjoint, layout {lay} {kw}: {joint[-1][0]:.3f} ms")
             joint.sort(key=lambda r: r[0])
@@ -206,7 +269,11 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--polish", action="store_true")
+    ap.add_argument("--warm", action="store_true",
+                    help="relax stage: time a warm-started call after the atoms moved by 5e-3 A (implies --polish)")
     args = ap.parse_args(argv)
+    if args.warm:
+        args.polish = True
     items = synthetic.batch_molecules(args.mols, seed=args.seed)
     base = _lib.lib().spm_batch_default_shape()
     if not args.shape:
@@ -218,6 +285,15 @@ def main(argv=None):
     for text in args.shape:
         b = AFMBatch(items, shape=_parse_shape(text, base)).set_relax_options(polish=args.polish)
         b.build_grids()
+        if args.stage == "relax" and args.warm:
+            b.set_relax_options(warm=True)
+            ms = _warm_step_ms(b, args.reps)
+            n_tail = int(b.workspace[2]) if b.shape.rx_sync == 2 else None
+            print(json.dumps({"shape": text, "stage": "relax (warm step)", "ms": ms, "states": int(b.total_states),
+                              "strokes": int(b.total_pixels), "second_pass_strokes": n_tail}), flush=True)
+            del b
+            torch.cuda.empty_cache()
+            continue
         if args.stage == "grid":
             run = b.build_grids
         elif args.stage == "relax":

@@ -236,8 +236,7 @@ class AFMBatch:
         self.PPs = torch.full((so, 4), float("nan"), dtype=F32, device=dev)
         self.iter_count = torch.empty((po,), dtype=torch.int32, device=dev)
         self.df = torch.empty((so,), dtype=F32, device=dev)
-        self.workspace = torch.zeros((max(1, int(lib().spm_relax_workspace_bytes()) // 4),), dtype=torch.int32,
-                                     device=dev)
+        self.workspace = None  # sized for the launch shape by set_shape
         # loss / adjoint buffers: allocated by the first loss or adjoint call
         self.target = self.weights = self.df_c = self.dL = self.ubar = self.dk = self.diag = None
         self.grad = self.dk_sum = None
@@ -255,7 +254,7 @@ class AFMBatch:
         """polish: Newton-polish every equilibrium (SPM_FLAG_POLISH); warm: start each z-step from the
         previous relaxation's equilibrium of the state (SPM_FLAG_WARM) -- for fits, whose atoms move a
         little per step; with the polish both starts reach the same equilibrium.  Both need the
-        z-synchronised schedule (shape.rx_sync = 1).  The flags are read at launch time from the
+        z-synchronised schedules (shape.rx_sync = 1 or 2).  The flags are read at launch time from the
         scan-parameter struct held here, so a captured graph keeps the options it was captured with."""
         if polish is not None:
             self.polish = bool(polish)
@@ -282,6 +281,9 @@ class AFMBatch:
             self.grid = None  # release the old layout's buffer before allocating the new one
             self.grid = torch.empty((per_node * self.grid_float4, 4), dtype=F32, device=self.dev)
         (self.n_tiles, self.n_slots, self.n_units, self.n_chunks, states, atoms, pixels, gend, self.n_rows) = totals
+        ws = int(lib().spm_batch_relax_workspace_bytes(self.n_slots, ctypes.byref(self.shape)))
+        if self.workspace is None or self.workspace.numel() * 4 < ws:
+            self.workspace = torch.zeros(((ws + 15) // 16 * 4,), dtype=torch.int32, device=self.dev)
         assert (states, atoms, pixels, gend) == (self.total_states, self.total_atoms, self.total_pixels,
                                                  self.grid_float4)
         raw = bytes(memoryview(self.mols).cast("B"))
@@ -311,7 +313,8 @@ class AFMBatch:
     def relax(self):
         rc = lib().spm_batch_relax(self.n, ptr(self.mols_d), self.n_slots, ctypes.byref(self.shape), ptr(self.grid),
                                    ptr(self.points), ctypes.byref(self.scan_params), ptr(self.FEs), ptr(self.PPs),
-                                   ptr(self.iter_count), ptr(self.workspace), stream_ptr())
+                                   ptr(self.iter_count), ptr(self.workspace), self.workspace.numel() * 4,
+                                   stream_ptr())
         check(rc, "spm_batch_relax")
 
     def df_amp(self, amp=1.0):

@@ -828,23 +828,168 @@ struct SlabCellFetchCached {
     }
 };
 
-// newton_core on a batch slab, kept out of line: the FIRE loop of the batched kernel keeps its
-// registers, the (rare) Newton evaluations run in the callee's own allocation.
+// newton_core on a batch slab, kept out of line for the kernels that also run FIRE: the FIRE loop
+// keeps its registers, and every argument goes by value so that no caller variable (the lane's
+// texel cache above all) has its address taken and moves to local memory.  The callee fetches its
+// cells itself.  q: the start; ok false (q, fe not set) when its cell is not available.
+struct NewtonResult {
+    V3 q;
+    float4 fe;
+    float g2;
+    int evals;
+    bool ok;
+};
+
 template <int LAYOUT>
-__device__ __noinline__ bool slab_newton(const AxisView& G, TexelCache& T, const float (&Tc)[3][3],
-                                         const PolishSpring& S, V3 tip, V3& q, float4& fe, float& g2, int& evals) {
-    return newton_core(SlabCellFetchCached<LAYOUT>{G, T}, Tc, S, tip, q, fe, g2, evals);
+__device__ __noinline__ NewtonResult slab_newton(const AxisView G, const PolishSpring S, float t00, float t11,
+                                                 float t22, V3 tip, V3 q) {
+    const float Tc[3][3] = {{t00, 0.f, 0.f}, {0.f, t11, 0.f}, {0.f, 0.f, t22}};
+    NewtonResult r;
+    r.q = q;
+    r.fe = make_float4(0.f, 0.f, 0.f, 0.f);
+    r.g2 = 0.f;
+    r.evals = 0;
+    r.ok = newton_core(SlabCellFetch<LAYOUT>{G}, Tc, S, tip, r.q, r.fe, r.g2, r.evals);
+    return r;
 }
 
 // Warm start (SPM_FLAG_WARM): a z-step starts from the equilibrium the state
-// had in the previous call (PPs in) when that one converged and its
-// displacement from the tip differs by at most WARM_MAX_JUMP per axis from the
-// displacement the stroke continuation starts from (the previous z-step's end
-// position, shifted with the tip); otherwise -- the probe jumped between the
-// two z-steps in the previous call, or there is no previous equilibrium -- it
-// starts from the continuation as a cold call does, so every state stays on
+// had in the previous call (PPs in) when that one converged and the stroke
+// arrives at this z-step where it arrived in the previous call: its
+// continuation start (the previous z-step's end position, shifted with the
+// tip) within WARM_MAX_JUMP per axis of the previous call's (the previous
+// call's equilibrium of the previous z-step, shifted the same way; at the
+// first z-step both are the tip's start).  Otherwise -- the probe jumped on
+// the way down in one of the two calls, or there is no previous equilibrium --
+// it starts from the continuation as a cold call does, so every state stays on
 // its stroke's branch.
 constexpr float WARM_MAX_JUMP = 0.1f;
+
+// A lane's stroke state between z-steps: the tip, the continuation position,
+// the FIRE velocity and integrator state (carried down the stroke), the last
+// sample and the iteration total.
+struct StrokeLane {
+    V3 tip, pos, v;
+    V3 prev;  // SPM_FLAG_WARM: the previous call's continuation start of this z-step (x NaN: none)
+    float dt, damp;
+    float4 fe;
+    int total_it;
+};
+
+// The polish's spring and texel-coordinate transform of an axis-aligned batch slab.
+__device__ __forceinline__ void batch_polish_setup(const AxisView& G, const spm_scan_params& P, PolishSpring& S,
+                                                   float (&Tc)[3][3]) {
+    S.a = mk3(1.f, 0.f, 0.f); S.b = mk3(0.f, 1.f, 0.f); S.c = mk3(0.f, 0.f, 1.f);
+    S.kk = ld4(P.stiffness); S.d0 = ld4(P.dpos0);
+    S.surf = P.surfFF[0];
+    S.frame = true;
+    Tc[0][0] = __fmul_rn(G.fnx, G.ax); Tc[0][1] = 0.f; Tc[0][2] = 0.f;
+    Tc[1][0] = 0.f; Tc[1][1] = __fmul_rn(G.fny, G.by); Tc[1][2] = 0.f;
+    Tc[2][0] = 0.f; Tc[2][1] = 0.f; Tc[2][2] = __fmul_rn(G.fnz, G.cz);
+}
+
+// One z-step of a lane's stroke (state o): the warm start, Newton-first with
+// POLISH, FIRE, the polish, the outputs, and the step to the next z-step.
+// PREFIX (two-pass schedule, POLISH and SPM_FLAG_WARM): only a z-step that
+// Newton's method finishes from the previous equilibrium is done; any other
+// returns false with nothing stored and L unchanged, for the FIRE pass to
+// redo from the same state.
+template <bool CACHE, int LAYOUT, bool POLISH, bool PREFIX>
+__device__ __forceinline__ bool stroke_zstep(const AxisView& G, TexelCache& T, const spm_scan_params& P,
+                                             const PolishSpring& S, const float (&Tc)[3][3], StrokeLane& L,
+                                             long long o, float dz, float4* __restrict__ FEs,
+                                             float4* __restrict__ PPs) {
+    V3 pos = L.pos;
+    bool warm_start = false;
+    V3 next_prev = mk3(__int_as_float(0x7fc00000), 0.f, 0.f);
+    if (P.flags & SPM_FLAG_WARM) {
+        const float4 pw = PPs[o];
+        if (pw.w > 0.f) {  // false for NaN
+            if (fabsf(pos.x - L.prev.x) <= WARM_MAX_JUMP && fabsf(pos.y - L.prev.y) <= WARM_MAX_JUMP &&
+                fabsf(pos.z - L.prev.z) <= WARM_MAX_JUMP) {  // false for NaN
+                pos = mk3(pw.x, pw.y, pw.z);
+                warm_start = true;
+            }
+            next_prev = mk3(pw.x, pw.y, __fadd_rn(pw.z, dz));
+        }
+    }
+    int it = 0;
+    bool conv = false, newton_done = false;
+    float4 fe = L.fe;
+    if constexpr (POLISH) {
+        // from a previous equilibrium Newton's method converges in a few steps: FIRE only if it does not
+        if (warm_start) {
+            NewtonResult r;
+            if constexpr (PREFIX) {  // no FIRE in this kernel: inline, through the lane's texel cache
+                r.q = pos;
+                r.ok = newton_core(SlabCellFetchCached<LAYOUT>{G, T}, Tc, S, L.tip, r.q, r.fe, r.g2, r.evals);
+            } else {
+                r = slab_newton<LAYOUT>(G, S, Tc[0][0], Tc[1][1], Tc[2][2], L.tip, pos);
+            }
+            if (r.ok) {
+                pos = r.q;
+                if (r.g2 < P.f2conv) {
+                    fe = r.fe;
+                    it = r.evals;
+                    conv = true;
+                    newton_done = true;
+                }
+            }
+        }
+    }
+    if constexpr (PREFIX) {
+        if (!newton_done) return false;
+    }
+    L.total_it += it;
+    if (!newton_done) {
+        while (!pp_iter_z<unsigned, CACHE, LAYOUT>(G, T, P, L.tip, pos, L.v, L.dt, L.damp, fe, it, L.total_it,
+                                                   conv)) {
+        }
+        if (!conv) fe = sample_z<unsigned, CACHE, LAYOUT>(G, pos, T);  // the position moved after the last sample
+    }
+    V3 q = pos;
+    if constexpr (POLISH) {
+        if (!newton_done && fe.w == fe.w) {
+            const NewtonResult r = slab_newton<LAYOUT>(G, S, Tc[0][0], Tc[1][1], Tc[2][2], L.tip, q);
+            if (r.ok) {
+                q = r.q;
+                fe = r.fe;
+            }
+        }
+    }
+    FEs[o] = fe;
+    // all seven values finite <=> the sum of their products with zero is zero
+    float z0 = __fmul_rn(fe.x, 0.f);
+    z0 = __fmaf_rn(fe.y, 0.f, z0);
+    z0 = __fmaf_rn(fe.z, 0.f, z0);
+    z0 = __fmaf_rn(fe.w, 0.f, z0);
+    z0 = __fmaf_rn(q.x, 0.f, z0);
+    z0 = __fmaf_rn(q.y, 0.f, z0);
+    z0 = __fmaf_rn(q.z, 0.f, z0);
+    const bool finite = (z0 == 0.f);
+    PPs[o] = make_float4(q.x, q.y, q.z, (float)((conv && finite) ? it : -it));
+    L.fe = fe;
+    L.tip.z = __fadd_rn(L.tip.z, dz);
+    L.pos = mk3(pos.x, pos.y, __fadd_rn(pos.z, dz));
+    L.prev = next_prev;
+    L.v = mk3(0.f, 0.f, 0.f);
+    return true;
+}
+
+// A lane's stroke state at its first z-step.
+__device__ __forceinline__ StrokeLane stroke_start(const float4* __restrict__ pts, int pix, const spm_scan_params& P) {
+    const float4 p4 = pts[pix];
+    StrokeLane L;
+    L.tip = mk3(p4.x, p4.y, p4.z);
+    L.pos = mk3(L.tip.x + P.dpos0[0], L.tip.y + P.dpos0[1], L.tip.z + P.dpos0[2]);
+    L.prev = L.pos;  // the first z-step starts where it started in every call
+    L.v = mk3(0.f, 0.f, 0.f);
+    L.dt = P.relax_params[0];
+    L.damp = P.relax_params[1];
+    L.fe = make_float4(0.f, 0.f, 0.f, 0.f);
+    L.total_it = 0;
+    return L;
+}
 
 // One lane's stroke of pixel k; every lane of `members` runs the same number
 // of z-steps (the molecule's nz_steps) and meets the others after each.
@@ -862,89 +1007,139 @@ __device__ __forceinline__ void relax_tile_stroke(const spm_batch_mol* D, const 
     const int nzs = D->nz_steps;
     const int pix = D->pix_off + k;
     const long long sbase = D->state_off + (long long)k * nzs;
-    const float4 p4 = pts[pix];
-    const bool warm = (P.flags & SPM_FLAG_WARM) != 0;
-    V3 tip = mk3(p4.x, p4.y, p4.z);
-    V3 pos = mk3(tip.x + P.dpos0[0], tip.y + P.dpos0[1], tip.z + P.dpos0[2]);
-    V3 v = mk3(0.f, 0.f, 0.f);
-    float dt = P.relax_params[0], damp = P.relax_params[1];
-    float4 fe = make_float4(0.f, 0.f, 0.f, 0.f);
-    int total_it = 0;
+    StrokeLane L = stroke_start(pts, pix, P);
     PolishSpring S;
     float Tc[3][3];
-    if constexpr (POLISH) {
-        S.a = mk3(1.f, 0.f, 0.f); S.b = mk3(0.f, 1.f, 0.f); S.c = mk3(0.f, 0.f, 1.f);
-        S.kk = ld4(P.stiffness); S.d0 = ld4(P.dpos0);
-        S.surf = P.surfFF[0];
-        S.frame = true;
-        Tc[0][0] = __fmul_rn(G.fnx, G.ax); Tc[0][1] = 0.f; Tc[0][2] = 0.f;
-        Tc[1][0] = 0.f; Tc[1][1] = __fmul_rn(G.fny, G.by); Tc[1][2] = 0.f;
-        Tc[2][0] = 0.f; Tc[2][1] = 0.f; Tc[2][2] = __fmul_rn(G.fnz, G.cz);
-    }
+    if constexpr (POLISH) batch_polish_setup(G, P, S, Tc);
     for (int iz = 0; iz < nzs; ++iz) {
-        bool warm_start = false;
-        if (warm) {
-            const float4 pw = PPs[sbase + iz];
-            const V3 dw = mk3(pw.x - tip.x, pw.y - tip.y, pw.z - tip.z);
-            const V3 dc = mk3(pos.x - tip.x, pos.y - tip.y, pos.z - tip.z);
-            if (pw.w > 0.f && fabsf(dw.x - dc.x) <= WARM_MAX_JUMP && fabsf(dw.y - dc.y) <= WARM_MAX_JUMP &&
-                fabsf(dw.z - dc.z) <= WARM_MAX_JUMP) {  // false for NaN
-                pos = mk3(pw.x, pw.y, pw.z);
-                warm_start = true;
-            }
-        }
-        int it = 0;
-        bool conv = false, newton_done = false;
-        if constexpr (POLISH) {
-            // from a previous equilibrium Newton's method converges in a few steps: FIRE only if it does not
-            if (warm_start) {
-                V3 qn = pos;
-                float4 fn;
-                float g2;
-                int ev;
-                if (slab_newton<LAYOUT>(G, T, Tc, S, tip, qn, fn, g2, ev)) {
-                    pos = qn;
-                    if (g2 < P.f2conv) {
-                        fe = fn;
-                        it = ev;
-                        total_it += ev;
-                        conv = true;
-                        newton_done = true;
-                    }
-                }
-            }
-        }
-        if (!newton_done) {
-            while (!pp_iter_z<unsigned, CACHE, LAYOUT>(G, T, P, tip, pos, v, dt, damp, fe, it, total_it, conv)) {
-            }
-            if (!conv) fe = sample_z<unsigned, CACHE, LAYOUT>(G, pos, T);  // the position moved after the last sample
-        }
-        V3 q = pos;
-        if constexpr (POLISH) {
-            if (!newton_done && fe.w == fe.w) {
-                float g2;
-                int ev;
-                slab_newton<LAYOUT>(G, T, Tc, S, tip, q, fe, g2, ev);
-            }
-        }
-        const long long o = sbase + iz;
-        FEs[o] = fe;
-        // all seven values finite <=> the sum of their products with zero is zero
-        float z0 = __fmul_rn(fe.x, 0.f);
-        z0 = __fmaf_rn(fe.y, 0.f, z0);
-        z0 = __fmaf_rn(fe.z, 0.f, z0);
-        z0 = __fmaf_rn(fe.w, 0.f, z0);
-        z0 = __fmaf_rn(q.x, 0.f, z0);
-        z0 = __fmaf_rn(q.y, 0.f, z0);
-        z0 = __fmaf_rn(q.z, 0.f, z0);
-        const bool finite = (z0 == 0.f);
-        PPs[o] = make_float4(q.x, q.y, q.z, (float)((conv && finite) ? it : -it));
-        tip.z = __fadd_rn(tip.z, dz);
-        pos.z = __fadd_rn(pos.z, dz);
-        v = mk3(0.f, 0.f, 0.f);
+        stroke_zstep<CACHE, LAYOUT, POLISH, false>(G, T, P, S, Tc, L, sbase + iz, dz, FEs, PPs);
         __syncwarp(members);  // the tile's lanes start the next z-step together
     }
-    if (iter_count) iter_count[pix] = total_it;
+    if (iter_count) iter_count[pix] = L.total_it;
+}
+
+// ---- two-pass schedule (spm_batch_shape.rx_sync = 2, POLISH and WARM) ----
+// In a fit's later calls most z-steps finish with Newton's method from their
+// previous equilibrium, and a few need FIRE; in one z-synchronised tile the
+// few hold the whole warp at every z-step.  The prefix pass runs the tiles
+// with Newton only: a lane's stroke goes as far as its z-steps finish that
+// way, and at its first z-step that needs FIRE the lane stores its stroke
+// state (before that z-step) in the tail list and stops.  The tail pass runs
+// the listed strokes from there with the full z-step, 32 entries per warp
+// stepping together.  Each z-step does exactly the computation of the
+// one-pass schedule from the same state, so the results are the same bits.
+struct TailEntry {
+    int m, k, iz, total_it;
+    float tip_z, px, py, pz;
+    float qx, qy, qz, pad;  // StrokeLane::prev
+};
+static_assert(sizeof(TailEntry) == 48, "tail entries are 48 bytes");
+
+// Workspace of the two-pass schedule: words 0-1 as the one-pass kernels (slot
+// counter, staged-variant flag), word 2 the tail count, word 3 the tail pass's
+// draw counter, then the tail list from byte 16.
+constexpr long long TAIL_OFF = 16;
+
+template <int MINB, bool CACHE, int LAYOUT>
+__global__ void __launch_bounds__(MINB == 5 ? 128 : 256, MINB)
+batch_relax_prefix_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
+                          const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
+                          float4* __restrict__ FEs, float4* __restrict__ PPs, int* __restrict__ iter_count,
+                          unsigned* __restrict__ ws) {
+    const float dz = P.tipC[3];
+    const unsigned lane = threadIdx.x & 31u;
+    TailEntry* tail = reinterpret_cast<TailEntry*>(reinterpret_cast<char*>(ws) + TAIL_OFF);
+    while (true) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(ws, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n_slots) return;  // warp-uniform
+        const int m = SPM_MOL_BY(slot_off, mols, n_mol, (long long)base);
+        const spm_batch_mol* D = mols + m;
+        int k;
+        const bool valid = slot_pixel(D, base + lane - (unsigned)D->slot_off, th_log2, k);
+        const unsigned members = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            const AxisView G = axis_view<LAYOUT>(D, grid);
+            TexelCache T;
+            T.kx = __int_as_float(0x7fc00000);
+            const int nzs = D->nz_steps;
+            const int pix = D->pix_off + k;
+            const long long sbase = D->state_off + (long long)k * nzs;
+            StrokeLane L = stroke_start(pts, pix, P);
+            PolishSpring S;
+            float Tc[3][3];
+            batch_polish_setup(G, P, S, Tc);
+            bool active = true;
+            for (int iz = 0; iz < nzs; ++iz) {  // every member runs every z-step: the ballots stay uniform
+                const bool fail = active && !stroke_zstep<CACHE, LAYOUT, true, true>(G, T, P, S, Tc, L, sbase + iz,
+                                                                                      dz, FEs, PPs);
+                const unsigned fm = __ballot_sync(members, fail);
+                if (fm) {
+                    const int leader = __ffs(fm) - 1;
+                    unsigned at = 0;
+                    if ((int)lane == leader) at = atomicAdd(ws + 2, (unsigned)__popc(fm));
+                    at = __shfl_sync(members, at, leader);
+                    if (fail) {  // L is the state before this z-step (a failed prefix z-step leaves it)
+                        TailEntry e;
+                        e.m = m; e.k = k; e.iz = iz; e.total_it = L.total_it;
+                        e.tip_z = L.tip.z; e.px = L.pos.x; e.py = L.pos.y; e.pz = L.pos.z;
+                        e.qx = L.prev.x; e.qy = L.prev.y; e.qz = L.prev.z; e.pad = 0.f;
+                        tail[at + (unsigned)__popc(fm & ((1u << lane) - 1u))] = e;  // < n_slots: one per stroke
+                        active = false;
+                    }
+                }
+                __syncwarp(members);
+            }
+            if (active && iter_count) iter_count[pix] = L.total_it;
+        }
+        __syncwarp();  // the whole warp draws the next tile
+    }
+}
+
+template <int MINB, bool CACHE, int LAYOUT>
+__global__ void __launch_bounds__(MINB == 5 ? 128 : 256, MINB)
+batch_relax_tail_kernel(const spm_batch_mol* __restrict__ mols, const float* __restrict__ grid,
+                        const float4* __restrict__ pts, spm_scan_params P, float4* __restrict__ FEs,
+                        float4* __restrict__ PPs, int* __restrict__ iter_count, unsigned* __restrict__ ws) {
+    const float dz = P.tipC[3];
+    const unsigned lane = threadIdx.x & 31u;
+    const TailEntry* tail = reinterpret_cast<const TailEntry*>(reinterpret_cast<const char*>(ws) + TAIL_OFF);
+    const unsigned n_tail = ws[2];  // written by the prefix pass, which ran before this launch
+    while (true) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(ws + 3, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n_tail) return;  // warp-uniform
+        const bool valid = base + lane < n_tail;
+        const unsigned members = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            const TailEntry e = tail[base + lane];
+            const spm_batch_mol* D = mols + e.m;
+            const AxisView G = axis_view<LAYOUT>(D, grid);
+            TexelCache T;
+            T.kx = __int_as_float(0x7fc00000);
+            const int nzs = D->nz_steps;
+            const int pix = D->pix_off + e.k;
+            const long long sbase = D->state_off + (long long)e.k * nzs;
+            StrokeLane L = stroke_start(pts, pix, P);  // tip x, y and the integrator's start values
+            L.tip.z = e.tip_z;
+            L.pos = mk3(e.px, e.py, e.pz);
+            L.prev = mk3(e.qx, e.qy, e.qz);
+            L.total_it = e.total_it;
+            PolishSpring S;
+            float Tc[3][3];
+            batch_polish_setup(G, P, S, Tc);
+            const int steps = nzs - e.iz;
+            const int rounds = __reduce_max_sync(members, steps);
+            for (int r = 0; r < rounds; ++r) {  // the same count on every member
+                if (r < steps) stroke_zstep<CACHE, LAYOUT, true, false>(G, T, P, S, Tc, L, sbase + e.iz + r, dz, FEs, PPs);
+                __syncwarp(members);
+            }
+            if (iter_count) iter_count[pix] = L.total_it;
+        }
+        __syncwarp();
+    }
 }
 
 template <int MINB, bool CACHE, int LAYOUT, bool POLISH>
@@ -1209,9 +1404,15 @@ batch_relax_staged_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, uns
 }  // namespace
 }  // namespace spm
 
+extern "C" long long spm_batch_relax_workspace_bytes(long long n_slots, const spm_batch_shape* shape) {
+    if (n_slots < 0 || !shape) return -1;
+    return spm::TAIL_OFF + (shape->rx_sync == 2 ? (long long)sizeof(spm::TailEntry) * n_slots : 0);
+}
+
 extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n_slots, const spm_batch_shape* shape,
                                const float* grid, const float* points, const spm_scan_params* p, float* FEs,
-                               float* PPs, int* iter_count, void* workspace, void* stream) {
+                               float* PPs, int* iter_count, void* workspace, long long workspace_bytes,
+                               void* stream) {
     using namespace spm;
     clear_error();
     SPM_REQUIRE(shape && p, "spm_batch_relax: null shape/params");
@@ -1243,10 +1444,17 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
                 "rx_threads=%d", thr);
     SPM_REQUIRE(shape->grid_layout == 0 || shape->grid_layout == 1, "spm_batch_relax: grid_layout=%d",
                 shape->grid_layout);
-    SPM_REQUIRE(shape->rx_sync == 0 || shape->rx_sync == 1, "spm_batch_relax: rx_sync=%d", shape->rx_sync);
+    SPM_REQUIRE(shape->rx_sync >= 0 && shape->rx_sync <= 2, "spm_batch_relax: rx_sync=%d", shape->rx_sync);
     if (p->flags & (SPM_FLAG_POLISH | SPM_FLAG_WARM))
-        SPM_REQUIRE(shape->rx_sync == 1, "spm_batch_relax: SPM_FLAG_POLISH / SPM_FLAG_WARM need the z-synchronised "
-                    "schedule (rx_sync = 1)");
+        SPM_REQUIRE(shape->rx_sync >= 1, "spm_batch_relax: SPM_FLAG_POLISH / SPM_FLAG_WARM need the z-synchronised "
+                    "schedules (rx_sync = 1 or 2)");
+    SPM_REQUIRE(shape->rx_regs != 5 || shape->rx_sync == 1, "spm_batch_relax: rx_regs=5 takes rx_sync = 1");
+    const long long ws_need = spm_batch_relax_workspace_bytes(n_slots, shape);
+    SPM_REQUIRE(workspace_bytes >= ws_need, "spm_batch_relax: workspace of %lld bytes, %lld needed", workspace_bytes,
+                ws_need);
+    // rx_sync = 2 runs the two-pass schedule when a warm polished call can use it, else rx_sync = 1's
+    const bool two_pass = shape->rx_sync == 2 && (p->flags & SPM_FLAG_POLISH) && (p->flags & SPM_FLAG_WARM);
+    const int sync = shape->rx_sync == 2 ? 1 : shape->rx_sync;
     using Kern = decltype(&batch_relax_kernel<3, false, 2>);
     // [rx_sync][grid_layout][rx_regs]: 0 = 80 registers, 1 = 64, 2 = texel cache at up to 128,
     // 3 = texel cache squeezed to 80 (some values spilled, 50% more warps), 4 = texel cache at up to 102
@@ -1270,9 +1478,24 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
         {batch_relax_sync_kernel<3, false, 4, true>, batch_relax_sync_kernel<4, false, 4, true>,
          batch_relax_sync_kernel<2, true, 4, true>, batch_relax_sync_kernel<3, true, 4, true>,
          batch_relax_sync_kernel<5, true, 4, true>}};
+    // the two-pass schedule's passes, [grid_layout][rx_regs]
+    static const Kern prefix[2][5] = {
+        {batch_relax_prefix_kernel<3, false, 2>, batch_relax_prefix_kernel<4, false, 2>,
+         batch_relax_prefix_kernel<2, true, 2>, batch_relax_prefix_kernel<3, true, 2>,
+         batch_relax_prefix_kernel<5, true, 2>},
+        {batch_relax_prefix_kernel<3, false, 4>, batch_relax_prefix_kernel<4, false, 4>,
+         batch_relax_prefix_kernel<2, true, 4>, batch_relax_prefix_kernel<3, true, 4>,
+         batch_relax_prefix_kernel<5, true, 4>}};
+    using TailKern = decltype(&batch_relax_tail_kernel<3, false, 2>);
+    static const TailKern tails[2][5] = {
+        {batch_relax_tail_kernel<3, false, 2>, batch_relax_tail_kernel<4, false, 2>,
+         batch_relax_tail_kernel<2, true, 2>, batch_relax_tail_kernel<3, true, 2>, batch_relax_tail_kernel<5, true, 2>},
+        {batch_relax_tail_kernel<3, false, 4>, batch_relax_tail_kernel<4, false, 4>,
+         batch_relax_tail_kernel<2, true, 4>, batch_relax_tail_kernel<3, true, 4>, batch_relax_tail_kernel<5, true, 4>}};
     const Kern kern = shape->rx_regs == 5 ? batch_relax_staged_kernel
+                      : two_pass ? prefix[shape->grid_layout][shape->rx_regs]
                       : (p->flags & SPM_FLAG_POLISH) ? polished[shape->grid_layout][shape->rx_regs]
-                                                      : table[shape->rx_sync][shape->grid_layout][shape->rx_regs];
+                                                      : table[sync][shape->grid_layout][shape->rx_regs];
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
@@ -1285,13 +1508,30 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     const unsigned blocks = (unsigned)(need < cap ? need : cap);
     cudaStream_t st = as_stream(stream);
     unsigned* ctr = static_cast<unsigned*>(workspace);
-    // word 0: the slot counter; word 1: the staged variant's wait-timeout flag
-    if (cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned), st) != cudaSuccess)
+    // word 0: the slot counter; word 1: the staged variant's wait-timeout flag; words 2-3: the two-pass
+    // schedule's tail count and tail draw counter
+    if (cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned), st) != cudaSuccess)
         return set_error(SPM_ERR_CUDA, "spm_batch_relax: cannot reset the slot counter");
     kern<<<blocks, thr, 0, st>>>(n_mol, mols, (unsigned)n_slots, th_log2, grid,
                                                reinterpret_cast<const float4*>(points), *p,
                                                reinterpret_cast<float4*>(FEs), reinterpret_cast<float4*>(PPs),
                                                iter_count, ctr);
+    if (two_pass) {
+        int rc = check_launch("spm_batch_relax (prefix pass)");
+        if (rc) return rc;
+        // the tail list is drawn 32 entries per warp until the count the prefix pass left is used up
+        const TailKern tk = tails[shape->grid_layout][shape->rx_regs];
+        int per_sm_t = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, tk, thr, 0) != cudaSuccess)
+            return set_error(SPM_ERR_CUDA, "spm_batch_relax: cannot query the device occupancy");
+        if (per_sm_t < 1) per_sm_t = 1;
+        if (shape->rx_ctas_per_sm > 0 && shape->rx_ctas_per_sm < per_sm_t) per_sm_t = shape->rx_ctas_per_sm;
+        const long long cap_t = (long long)sms * per_sm_t;
+        tk<<<(unsigned)(need < cap_t ? need : cap_t), thr, 0, st>>>(mols, grid, reinterpret_cast<const float4*>(points),
+                                                                     *p, reinterpret_cast<float4*>(FEs),
+                                                                     reinterpret_cast<float4*>(PPs), iter_count, ctr);
+        return check_launch("spm_batch_relax (tail pass)");
+    }
     return check_launch("spm_batch_relax");
 }
 

@@ -39,7 +39,7 @@ def test_binding_covers_every_declared_symbol():
 
 def test_abi_version_and_error_text():
     L = _lib.lib()
-    assert L.spm_abi_version() == 3
+    assert L.spm_abi_version() == 4
     assert L.spm_last_error() == b""
 
 

@@ -131,7 +131,7 @@ def test_batch_shapes_give_same_results(cuda):
                dict(grid_layout=1, rx_sync=0), dict(grid_layout=1, rx_regs=2), dict(grid_layout=1, rx_regs=1, gb_zb=16),
                dict(rx_sync=1, rx_regs=0), dict(rx_sync=1, rx_tile_h=1, rx_threads=64, rx_regs=2),
                dict(rx_sync=1, rx_tile_h=32, rx_regs=1, grid_layout=1), dict(rx_regs=3, rx_tile_h=2),
-               dict(rx_sync=0, rx_regs=3, grid_layout=1), dict(adj_ilp=2), dict(adj_ilp=2, adj_chunk=4096),
+               dict(rx_sync=0, rx_regs=3, grid_layout=1), dict(adj_ilp=2), dict(adj_ilp=2, adj_chunk=4096), dict(rx_sync=2),
                dict(rx_regs=3), dict(rx_regs=4, grid_layout=1), dict(rx_sync=0, rx_regs=4, rx_tile_h=4)):
         s = L.spm_batch_default_shape()
         for k, v in kw.items():
@@ -388,6 +388,45 @@ def test_batch_warm_start_reaches_the_cold_equilibria(cuda):
     assert int(b.iter_count.sum()) < 0.6 * int(cold.iter_count.sum())
     b.reset_warm_start()
     assert bool(torch.isnan(b.PPs).all())
+
+
+def test_batch_two_pass_schedule_is_bit_identical(cuda):
+    """rx_sync = 2 (warm polished calls): the Newton-only prefix pass in z-synchronised tiles, then the FIRE
+    pass over the strokes that stopped, gives the one-pass schedule's FEs, PPs and step counts bit for bit --
+    on the cold first call (every stroke goes to the second pass at its first z-step) and after the atoms
+    move (strokes stop part-way down, at z-steps that need FIRE)."""
+    items = _items(0, n=5, seed=66)
+    base = _lib.lib().spm_batch_default_shape()
+    mid_stroke = 0
+    for layout, regs in ((0, 4), (1, 2), (0, 0)):
+        shapes = []
+        for sync in (1, 2):
+            sh = _lib.BatchShape(*base.key())
+            sh.grid_layout, sh.rx_regs, sh.rx_sync = layout, regs, sync
+            shapes.append(sh)
+        one = AFMBatch(items, shape=shapes[0]).set_relax_options(polish=True, warm=True)
+        two = AFMBatch(items, shape=shapes[1]).set_relax_options(polish=True, warm=True)
+        rng = np.random.default_rng(7)
+        for step, sigma in enumerate((0.0, 5e-3, 5e-3, 0.1, 5e-3)):
+            if sigma:
+                d = torch.as_tensor(rng.normal(0, sigma, (one.total_atoms, 3)), dtype=one.atoms.dtype, device="cuda")
+                one.atoms[:, :3] += d
+                two.atoms[:, :3] += d
+            one.forward()
+            two.forward()
+            torch.cuda.synchronize()
+            assert torch.equal(one.FEs, two.FEs) and torch.equal(one.PPs, two.PPs), (layout, regs, step)
+            assert torch.equal(one.iter_count, two.iter_count), (layout, regs, step)
+            ws = two.workspace.cpu().numpy()
+            n_tail = int(ws[2])
+            if step == 0:
+                assert n_tail == two.total_pixels  # no previous equilibria: every stroke from its first z-step
+            else:
+                assert n_tail < two.total_pixels
+                iz = ws[4:4 + 12 * n_tail].reshape(-1, 12)[:, 2]
+                mid_stroke += int((iz > 0).sum())
+            print(f"layout {layout} regs {regs} call {step}: {n_tail} of {two.total_pixels} strokes in the FIRE pass")
+    assert mid_stroke > 0
 
 
 def test_batch_polish_and_warm_need_the_synchronised_schedule(cuda):
