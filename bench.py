@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--fit-mols", type=int, default=64)
     ap.add_argument("--fit-steps", type=int, default=100)
     ap.add_argument("--fit-lr", type=float, default=0.01, help="Adam learning rate of the fit (A, e)")
-    ap.add_argument("--fit-z-end", type=float, default=4.0,
+    ap.add_argument("--fit-z-end", type=float, default=3.0,
                     help="lowest tip height of the fit's scans above the molecule plane (A)")
     ap.add_argument("--batch-only", action="store_true",
                     help="run only the many-molecule workloads (small sizes make profiling cases)")

@@ -504,11 +504,16 @@ long long spm_batch_loss_scratch_bytes(long long n_chunks, int n_mol);
 int spm_batch_failure_mask(long long n_states, const float* diag, const double* w_base, double* weights,
                            void* stream);
 
-/* spm_adjoint_grid_state over the batch (same outputs per state). */
+/* spm_adjoint_grid_state over the batch (same outputs per state).
+ * adj_scratch (optional, with totals: the scratch of spm_batch_adjoint_params
+ * for this batch): the call also leaves there each molecule's max |ubar| and
+ * box of touched slab rows and layers, which spm_batch_adjoint_params then
+ * takes with SPM_ADJ_STATE_MAXIMA instead of a pass over ubar of its own.
+ * NULL: no maxima (totals may be NULL). */
 int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_states,
                             const spm_batch_shape* shape, const float* grid, const float* points,
                             const spm_scan_params* p, const float* PPs, const float* dL_dFEs, float* ubar,
-                            float* dk, float* diag, void* stream);
+                            float* dk, float* diag, const long long* totals, void* adj_scratch, void* stream);
 
 /* spm_adjoint_grid_params over the batch, node-major: grad (total_atoms,6)
  * double as spm_adjoint_grid_params, dk_sum double[4] summed over the whole
@@ -531,8 +536,12 @@ int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_st
  * allocation, a call that failed half-way) is cleared by the next call.
  * adj_flags: SPM_ADJ_PAIR_PARAMS computes grad columns 3-4 (the pair
  * parameters); without it they are written as 0 and the node kernel skips
- * their terms (fits of positions and charges only). */
+ * their terms (fits of positions and charges only).  SPM_ADJ_STATE_MAXIMA:
+ * the scratch holds the maxima and boxes of this ubar from
+ * spm_batch_adjoint_state (called with this scratch after the last change
+ * of ubar); without it the call computes them. */
 #define SPM_ADJ_PAIR_PARAMS 1
+#define SPM_ADJ_STATE_MAXIMA 2
 int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol* mols, const long long* totals,
                              const spm_batch_shape* shape, const float* atoms, const float* params,
                              const float* Qs, const float* QZs, const float* PPs, const float* ubar,

@@ -37,6 +37,7 @@ SPM_FLAG_POLISH = 8
 # batched relaxation: start each z-step from the previous call's equilibrium (PPs read and written)
 SPM_FLAG_WARM = 16
 SPM_ADJ_PAIR_PARAMS = 1
+SPM_ADJ_STATE_MAXIMA = 2
 
 _f4 = ctypes.c_float * 4
 
@@ -172,7 +173,7 @@ _SIGNATURES = {
     "spm_batch_df_loss_seed": (_i, [_i, _vp, _ll, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _vp]),
     "spm_batch_loss_scratch_bytes": (_ll, [_ll, _i]),
     "spm_batch_failure_mask": (_i, [_ll, _vp, _vp, _vp, _vp]),
-    "spm_batch_adjoint_state": (_i, [_i, _vp, _ll, _BS, _vp, _vp, _P, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "spm_batch_adjoint_state": (_i, [_i, _vp, _ll, _BS, _vp, _vp, _P, _vp, _vp, _vp, _vp, _vp, _LLP, _vp, _vp]),
     "spm_batch_adjoint_params": (_i, [_i, _i, _vp, _LLP, _BS, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
                                       _vp, _vp]),
     "spm_batch_adjoint_scratch_bytes": (_ll, [_LLP, _i]),

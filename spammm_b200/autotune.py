@@ -269,6 +269,8 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--polish", action="store_true")
+    ap.add_argument("--positions-charges", action="store_true",
+                    help="adjoint stage: gradient columns of positions and charges only (as a fit's steps)")
     ap.add_argument("--warm", action="store_true",
                     help="relax stage: time a warm-started call after the atoms moved by 5e-3 A (implies --polish)")
     args = ap.parse_args(argv)
@@ -284,6 +286,7 @@ def main(argv=None):
     rng = np.random.default_rng(args.seed)
     for text in args.shape:
         b = AFMBatch(items, shape=_parse_shape(text, base)).set_relax_options(polish=args.polish)
+        b.pair_param_grads = not args.positions_charges
         b.build_grids()
         if args.stage == "relax" and args.warm:
             b.set_relax_options(warm=True)

@@ -346,23 +346,34 @@ class AFMBatch:
                                           ptr(self.loss_scratch), stream_ptr())
         check(rc, "spm_batch_df_loss_seed")
 
+    def _ensure_adj_scratch(self):
+        if self.adj_scratch is None:
+            self.adj_scratch = torch.empty(((self._adj_bytes + 15) // 16, 2), dtype=F64, device=self.dev)
+
     def adjoint_state(self):
+        """State adjoint; also leaves the per-molecule ubar maxima and touched boxes in the adjoint scratch
+        for adjoint_params (SPM_ADJ_STATE_MAXIMA)."""
         self._ensure_adjoint_buffers()
+        self._ensure_adj_scratch()
         rc = lib().spm_batch_adjoint_state(self.n, ptr(self.mols_d), self.total_states, ctypes.byref(self.shape),
                                            ptr(self.grid),
                                            ptr(self.points), ctypes.byref(self.scan_params), ptr(self.PPs),
-                                           ptr(self.dL), ptr(self.ubar), ptr(self.dk), ptr(self.diag), stream_ptr())
+                                           ptr(self.dL), ptr(self.ubar), ptr(self.dk), ptr(self.diag),
+                                           self.plan.totals, ptr(self.adj_scratch), stream_ptr())
         check(rc, "spm_batch_adjoint_state")
+        self._state_maxima = True
+
+    _state_maxima = False  # the adjoint scratch holds the maxima of the current ubar (from adjoint_state)
 
     def adjoint_params(self):
         self._ensure_adjoint_buffers()
-        if self.adj_scratch is None:
-            self.adj_scratch = torch.empty(((self._adj_bytes + 15) // 16, 2), dtype=F64, device=self.dev)
+        self._ensure_adj_scratch()
         rc = lib().spm_batch_adjoint_params(self.kind, self.n, ptr(self.mols_d), self.plan.totals,
                                             ctypes.byref(self.shape), ptr(self.atoms), ptr(self.params),
                                             hptr(self._Qs), hptr(self._QZs), ptr(self.PPs), ptr(self.ubar),
                                             ptr(self.dk), ptr(self.grad), ptr(self.dk_sum),
-                                            _lib.SPM_ADJ_PAIR_PARAMS if self.pair_param_grads else 0,
+                                            (_lib.SPM_ADJ_PAIR_PARAMS if self.pair_param_grads else 0) |
+                                            (_lib.SPM_ADJ_STATE_MAXIMA if self._state_maxima else 0),
                                             ptr(self.adj_scratch), stream_ptr())
         check(rc, "spm_batch_adjoint_params")
 

@@ -513,26 +513,92 @@ long long n_rowblocks(long long n_state) { return n_state > 0 ? (n_state + 2047)
 // all eight texels live and spilled at 64 registers (3.41 -> 3.00 ms on the
 // 64-molecule fit; 4.14 ms before the x-pair loads, the separable lerps and the
 // identity-frame path).
+//
+// umax, box (optional, zeroed before the launch): the per-molecule max |ubar| and touched box of
+// batch_ubar_max_kernel, from each state's ubar as it is written -- warp maxima (redux) into the
+// molecule's atomics, per lane where a warp spans two molecules.  Maxima are order-free.
 __global__ void __launch_bounds__(AG_THREADS, 6)
 batch_adjoint_state_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states, int stride,
                            const float* __restrict__ grid, const float4* __restrict__ pts, spm_scan_params P,
                            const float4* __restrict__ PPs, const float4* __restrict__ dL, float4* __restrict__ ubar,
-                           float4* __restrict__ dk, float4* __restrict__ diag) {
+                           float4* __restrict__ dk, float4* __restrict__ diag, unsigned* __restrict__ umax,
+                           int* __restrict__ box) {
     const long long st = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (st >= n_states) return;
-    const spm_batch_mol* D = mols + SPM_MOL_BY(state_off, mols, n_mol, st);
-    const long long ls = st - D->state_off;
-    const int nz = D->nz_steps;
-    int iscan, iz;
-    if (ls < (1LL << 32)) {  // 32-bit division when it fits
-        iscan = (int)((unsigned)ls / (unsigned)nz);
-        iz = (int)((unsigned)ls - (unsigned)iscan * (unsigned)nz);
-    } else {
-        iscan = (int)(ls / nz);
-        iz = (int)(ls % nz);
+    const bool in = st < n_states;
+    int m = 0;
+    float v = 0.f;
+    int b[4] = {0, 0, 0, 0};
+    if (in) {
+        m = SPM_MOL_BY(state_off, mols, n_mol, st);
+        const spm_batch_mol* D = mols + m;
+        const long long ls = st - D->state_off;
+        const int nz = D->nz_steps;
+        int iscan, iz;
+        if (ls < (1LL << 32)) {  // 32-bit division when it fits
+            iscan = (int)((unsigned)ls / (unsigned)nz);
+            iz = (int)((unsigned)ls - (unsigned)iscan * (unsigned)nz);
+        } else {
+            iscan = (int)(ls / nz);
+            iz = (int)(ls % nz);
+        }
+        const float4 pp = PPs[st];
+        state_adjoint<true>(slab_view(*D, grid, stride), P, pts[D->pix_off + iscan], iz, pp, dL[st], ubar + st,
+                            dk + st, diag + st);
+        if (umax) {
+            const float4 u = ubar[st];  // this thread's own store
+            v = fmaxf(fmaxf(fabsf(u.x), fabsf(u.y)), fmaxf(fabsf(u.z), fabsf(u.w)));
+            if (!(u.x == 0.f && u.y == 0.f && u.z == 0.f && u.w == 0.f)) {  // the scatter's test
+                const GridView G = slab_view(*D, nullptr);
+                const Corners C = corners_of<true>(G, mk3(pp.x, pp.y, pp.z));
+                if (C.ok) {
+#pragma unroll
+                    for (int k = 0; k < 2; k++) {
+                        b[0] = max(b[0], G.ny_slab - 1 - (C.y[k] - G.y_lo));
+                        b[1] = max(b[1], C.y[k] - G.y_lo + 1);
+                        b[2] = max(b[2], G.nz_slab - 1 - (C.z[k] - G.z_lo));
+                        b[3] = max(b[3], C.z[k] - G.z_lo + 1);
+                    }
+                }
+            }
+        }
     }
-    state_adjoint<true>(slab_view(*D, grid, stride), P, pts[D->pix_off + iscan], iz, PPs[st], dL[st], ubar + st, dk + st,
-                        diag + st);
+    if (umax) {  // launch-uniform: CTA maxima, one atomic per value and CTA when the CTA has one molecule
+        __shared__ int s_red[AG_THREADS / 32][5];
+        __shared__ int s_m[AG_THREADS / 32];
+        const unsigned FULL = 0xffffffffu;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const int m0 = __shfl_sync(FULL, m, 0);
+        const bool one = __all_sync(FULL, !in || m == m0);
+        const int wv = (int)__reduce_max_sync(FULL, __float_as_uint(v));  // v >= 0: bit order = value order
+        int wb[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) wb[k] = __reduce_max_sync(FULL, b[k]);
+        if (lane == 0) {
+            s_m[warp] = one ? m0 : -1;  // -1: the warp spans two molecules
+            s_red[warp][0] = wv;
+#pragma unroll
+            for (int k = 0; k < 4; k++) s_red[warp][k + 1] = wb[k];
+        }
+        __syncthreads();
+        bool cta_one = true;
+#pragma unroll
+        for (int w = 0; w < AG_THREADS / 32; w++) cta_one = cta_one && s_m[w] == s_m[0] && s_m[w] >= 0;
+        if (cta_one) {
+            if (threadIdx.x < 5) {
+                int val = 0;
+#pragma unroll
+                for (int w = 0; w < AG_THREADS / 32; w++) val = max(val, s_red[w][threadIdx.x]);
+                // the umax word holds a finite non-negative float's bits (< 2^31): int order = value order
+                int* dst = threadIdx.x == 0 ? reinterpret_cast<int*>(umax + s_m[0]) : box + 4 * s_m[0] + (threadIdx.x - 1);
+                if (val > 0) atomicMax(dst, val);
+            }
+        } else if (in) {  // the CTA at a molecule boundary: per lane
+            if (v > 0.f) atomicMax(umax + m, __float_as_uint(v));
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (b[k] > 0) atomicMax(box + 4 * m + k, b[k]);
+        }
+    }
 }
 
 // ---- node-major adjoint through the grid build (batched) -------------------
@@ -567,14 +633,12 @@ adj_clear_kernel(ulonglong2* __restrict__ gq, long long n2, const unsigned long 
 // ubar (all zero: none); yl, zl are slab rows and layers.  The CTA searches
 // the first chunk's molecule once and steps to the next ones; its maxima are
 // flushed to the molecule's atomics whenever the molecule changes.
-// Block 0 marks the adjoint grid dirty (the scatter follows).
 constexpr int UM_CHUNKS = 4;
 
 __global__ void __launch_bounds__(256)
 batch_ubar_max_kernel(int n_mol, long long n_chunks, const spm_batch_mol* __restrict__ mols,
                       const float4* __restrict__ ubar, const float4* __restrict__ PPs, unsigned* __restrict__ umax,
-                      int* __restrict__ box, unsigned long long* __restrict__ mark) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) *mark = ADJ_DIRTY;
+                      int* __restrict__ box) {
     __shared__ float s_m[8];
     __shared__ int s_b[4][8];
     float v = 0.f;
@@ -642,7 +706,8 @@ batch_ubar_max_kernel(int n_mol, long long n_chunks, const spm_batch_mol* __rest
     flush(m);
 }
 
-// Thread per state: w * ubar onto the eight corner nodes (exact integer sums).
+// Thread per state: w * ubar onto the eight corner nodes (exact integer sums).  Block 0 marks the
+// adjoint grid dirty until the node kernel has cleared it again.
 // Consecutive lanes are consecutive z-steps of a stroke; when lane l+1's cell
 // sits one layer below lane l's in the same (x,y) cell, lane l+1's upper
 // layer is lane l's lower layer: lane l adds those four corners' sums to its
@@ -661,7 +726,8 @@ template <bool AGG>
 __global__ void __launch_bounds__(256)
 batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long long n_states,
                      const float4* __restrict__ PPs, const float4* __restrict__ ubar, const unsigned* __restrict__ umax,
-                     unsigned long long* __restrict__ gq) {
+                     unsigned long long* __restrict__ gq, unsigned long long* __restrict__ mark) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *mark = ADJ_DIRTY;  // the adjoint grid is written from here on
     extern __shared__ unsigned long long s_agg[];  // AGG: keys[AGG_SLOTS], then values[AGG_SLOTS][4]
     unsigned long long* s_key = s_agg;
     unsigned long long* s_val = s_agg + AGG_SLOTS;
@@ -1252,7 +1318,8 @@ AdjScratch adj_scratch_layout(const long long* totals, int n_mol) {
 extern "C" int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_states,
                                        const spm_batch_shape* shape, const float* grid, const float* points,
                                        const spm_scan_params* p, const float* PPs, const float* dL_dFEs, float* ubar,
-                                       float* dk, float* diag, void* stream) {
+                                       float* dk, float* diag, const long long* totals, void* adj_scratch,
+                                       void* stream) {
     using namespace spm;
     clear_error();
     SPM_REQUIRE(p && shape, "spm_batch_adjoint_state: null params/shape");
@@ -1265,11 +1332,24 @@ extern "C" int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, lon
                 aligned16(dk) && aligned16(diag), "spm_batch_adjoint_state: buffers not 16-byte aligned");
     const long long nb = (n_states + AG_THREADS - 1) / AG_THREADS;
     SPM_REQUIRE(nb < (1LL << 31), "spm_batch_adjoint_state: too many states");
-    batch_adjoint_state_kernel<<<(unsigned)nb, AG_THREADS, 0, as_stream(stream)>>>(
+    cudaStream_t st = as_stream(stream);
+    unsigned* umax = nullptr;
+    int* box = nullptr;
+    if (adj_scratch) {  // the maxima and touched boxes of spm_batch_adjoint_params, from the ubar written here
+        SPM_REQUIRE(totals && (reinterpret_cast<uintptr_t>(adj_scratch) & 15u) == 0,
+                    "spm_batch_adjoint_state: adj_scratch needs totals and 16-byte alignment");
+        const AdjScratch SL = adj_scratch_layout(totals, n_mol);
+        char* base = static_cast<char*>(adj_scratch);
+        umax = reinterpret_cast<unsigned*>(base + SL.umax);
+        box = reinterpret_cast<int*>(base + SL.box);
+        if (cudaMemsetAsync(umax, 0, (size_t)(SL.mark - SL.umax), st) != cudaSuccess)
+            return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_state: memset failed");
+    }
+    batch_adjoint_state_kernel<<<(unsigned)nb, AG_THREADS, 0, st>>>(
         n_mol, mols, n_states, shape->grid_layout ? 4 : 2, grid, reinterpret_cast<const float4*>(points), *p,
         reinterpret_cast<const float4*>(PPs),
         reinterpret_cast<const float4*>(dL_dFEs), reinterpret_cast<float4*>(ubar), reinterpret_cast<float4*>(dk),
-        reinterpret_cast<float4*>(diag));
+        reinterpret_cast<float4*>(diag), umax, box);
     return check_launch("spm_batch_adjoint_state");
 }
 
@@ -1287,7 +1367,8 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
     using namespace spm;
     clear_error();
     SPM_REQUIRE(kind == SPM_KIND_LJ || kind == SPM_KIND_MORSE, "spm_batch_adjoint_params: kind=%d", kind);
-    SPM_REQUIRE((adj_flags & ~SPM_ADJ_PAIR_PARAMS) == 0, "spm_batch_adjoint_params: unknown flags 0x%x", adj_flags);
+    SPM_REQUIRE((adj_flags & ~(SPM_ADJ_PAIR_PARAMS | SPM_ADJ_STATE_MAXIMA)) == 0,
+                "spm_batch_adjoint_params: unknown flags 0x%x", adj_flags);
     SPM_REQUIRE(shape && totals && Qs && QZs && dk_sum && scratch, "spm_batch_adjoint_params: null pointer");
     SPM_REQUIRE(n_mol >= 0, "spm_batch_adjoint_params: n_mol=%d", n_mol);
     const long long n_units = totals[2], n_chunks = totals[3], n_states = totals[4], n_atoms = totals[5];
@@ -1329,12 +1410,14 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
                 }
                 if (dev >= 0 && dev < 64) smem_set[dev] = true;
             }
-            if (cudaMemsetAsync(umax, 0, (size_t)(SL.mark - SL.umax), st) != cudaSuccess)  // maxima + boxes
+            const bool given = (adj_flags & SPM_ADJ_STATE_MAXIMA) != 0;  // from spm_batch_adjoint_state
+            if (!given && cudaMemsetAsync(umax, 0, (size_t)(SL.mark - SL.umax), st) != cudaSuccess)  // maxima + boxes
                 return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: memset failed");
             adj_clear_kernel<<<1184, 256, 0, st>>>(reinterpret_cast<ulonglong2*>(gq), totals[7] * 2, mark);
-            batch_ubar_max_kernel<<<(unsigned)((n_chunks + UM_CHUNKS - 1) / UM_CHUNKS), 256, 0, st>>>(
-                n_mol, n_chunks, mols, reinterpret_cast<const float4*>(ubar), reinterpret_cast<const float4*>(PPs), umax,
-                box, mark);
+            if (!given)
+                batch_ubar_max_kernel<<<(unsigned)((n_chunks + UM_CHUNKS - 1) / UM_CHUNKS), 256, 0, st>>>(
+                    n_mol, n_chunks, mols, reinterpret_cast<const float4*>(ubar), reinterpret_cast<const float4*>(PPs),
+                    umax, box);
             if (shape->adj_agg) {
                 const size_t agg_smem = sizeof(unsigned long long) * 5 * AGG_SLOTS;
                 if (cudaFuncSetAttribute(batch_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1343,11 +1426,11 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
                                      agg_smem);
                 batch_scatter_kernel<true><<<(unsigned)((n_states + 255) / 256), 256, agg_smem, st>>>(
                     n_mol, mols, n_states, reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar),
-                    umax, gq);
+                    umax, gq, mark);
             } else {
                 batch_scatter_kernel<false><<<(unsigned)((n_states + 255) / 256), 256, 0, st>>>(
                     n_mol, mols, n_states, reinterpret_cast<const float4*>(PPs), reinterpret_cast<const float4*>(ubar),
-                    umax, gq);
+                    umax, gq, mark);
             }
             const NodeSites S = make_node_sites(Qs, QZs);
             const int pstride = kind == SPM_KIND_MORSE ? 4 : 2;

@@ -883,6 +883,7 @@ __device__ __forceinline__ void batch_polish_setup(const AxisView& G, const spm_
     S.kk = ld4(P.stiffness); S.d0 = ld4(P.dpos0);
     S.surf = P.surfFF[0];
     S.frame = true;
+    S.ident = true;  // batches scan z-strokes (a, b, c = x, y, z; checked at launch) on axis-aligned slabs
     Tc[0][0] = __fmul_rn(G.fnx, G.ax); Tc[0][1] = 0.f; Tc[0][2] = 0.f;
     Tc[1][0] = 0.f; Tc[1][1] = __fmul_rn(G.fny, G.by); Tc[1][2] = 0.f;
     Tc[2][0] = 0.f; Tc[2][1] = 0.f; Tc[2][2] = __fmul_rn(G.fnz, G.cz);

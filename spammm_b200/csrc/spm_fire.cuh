@@ -393,6 +393,9 @@ struct PolishSpring {
     float4 kk, d0;
     float surf;
     bool frame;
+    // frame with a, b, c = x, y, z and a diagonal texel transform T (batch slabs): the rotations
+    // and the zero terms of T are left out -- the same values, up to the sign of a zero
+    bool ident = false;
 };
 
 // One evaluation at q from the cell's texels t[4*k + 2*j + i] (corner x_i, y_j, z_k) and
@@ -417,17 +420,26 @@ __device__ __forceinline__ void polish_eval(const float4 (&t)[8], float ax, floa
             const float dX = lerp_c(az, mz, e0, e1);
             const float dY = lerp_c(az, mz, c10 - c00, c11 - c01);
             const float dZ = c1 - c0;
+            if (S.ident) {
+                J[ch][0] = __fmul_rn(dX, T[0][0]);
+                J[ch][1] = __fmul_rn(dY, T[1][1]);
+                J[ch][2] = __fmul_rn(dZ, T[2][2]);
+            } else {
 #pragma unroll
-            for (int m = 0; m < 3; m++)
-                J[ch][m] = __fmaf_rn(dZ, T[2][m], __fmaf_rn(dY, T[1][m], __fmul_rn(dX, T[0][m])));
+                for (int m = 0; m < 3; m++)
+                    J[ch][m] = __fmaf_rn(dZ, T[2][m], __fmaf_rn(dY, T[1][m], __fmul_rn(dX, T[0][m])));
+            }
         }
     }
     fe = make_float4(val[0], val[1], val[2], val[3]);
-    const V3 d = S.frame ? rotmat(sub3(q, tip), S.a, S.b, S.c) : sub3(q, tip);
+    const bool rot = S.frame && !S.ident;
+    const V3 d = rot ? rotmat(sub3(q, tip), S.a, S.b, S.c) : sub3(q, tip);
     const V3 fs = tip_force(d, S.kk, S.d0);
-    const V3 ft = S.frame ? rotmatT(fs, S.a, S.b, S.c) : fs;
+    const V3 ft = rot ? rotmatT(fs, S.a, S.b, S.c) : fs;
     Gv = mk3(val[0] + ft.x, val[1] + ft.y, val[2] + ft.z);
-    if (S.frame) {
+    if (S.ident) {
+        Gv.z = __fadd_rn(S.surf, Gv.z);  // surf along c = z
+    } else if (S.frame) {
         Gv.x = __fmaf_rn(S.c.x, S.surf, Gv.x);
         Gv.y = __fmaf_rn(S.c.y, S.surf, Gv.y);
         Gv.z = __fmaf_rn(S.c.z, S.surf, Gv.z);
@@ -450,7 +462,7 @@ __device__ __forceinline__ void polish_eval(const float4 (&t)[8], float ax, floa
             for (int j = 0; j < 3; j++) Jd[i][j] = __fmaf_rn(bd, dv[j], Jd[i][j]);
         }
     }
-    if (S.frame) {
+    if (rot) {
         const float R[3][3] = {{S.a.x, S.a.y, S.a.z}, {S.b.x, S.b.y, S.b.z}, {S.c.x, S.c.y, S.c.z}};
         float M[3][3];
 #pragma unroll

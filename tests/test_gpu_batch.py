@@ -255,7 +255,9 @@ def test_batch_of_single_chunk_molecules(cuda):
 @pytest.mark.parametrize("kind", [0, 1])
 def test_adjoint_scratch_reuse_and_garbage(cuda, kind):
     """The node kernel leaves the adjoint grid cleared for the next call; a
-    scratch buffer of arbitrary content (no clear marker) is cleared first."""
+    scratch buffer of arbitrary content (no clear marker) is cleared first.
+    The ubar maxima come from the state adjoint (SPM_ADJ_STATE_MAXIMA) or, without it, from the params
+    call itself: the same gradients."""
     b = AFMBatch(_items(kind, n=4, seed=71 + kind), kind=kind)
     _target(b)
     b.forward_adjoint()
@@ -264,14 +266,20 @@ def test_adjoint_scratch_reuse_and_garbage(cuda, kind):
     b.adjoint_params()
     torch.cuda.synchronize()
     assert torch.equal(b.grad, g1)
-    b.adj_scratch.view(torch.uint8).random_(0, 256)
-    b.adjoint_params()
-    torch.cuda.synchronize()
-    assert torch.equal(b.grad, g1)
-    b.adj_scratch.view(torch.uint8).fill_(0)  # all-zero buffer: no marker either
-    b.adjoint_params()
-    torch.cuda.synchronize()
-    assert torch.equal(b.grad, g1)
+    for fill in ("random", "zero"):  # all-zero buffer: no marker either
+        if fill == "random":
+            b.adj_scratch.view(torch.uint8).random_(0, 256)
+        else:
+            b.adj_scratch.view(torch.uint8).fill_(0)
+        b._state_maxima = False  # the maxima were overwritten: the params call computes them
+        b.adjoint_params()
+        torch.cuda.synchronize()
+        assert torch.equal(b.grad, g1), fill
+        b.adj_scratch.view(torch.uint8).random_(0, 256)
+        b.adjoint_state()  # maxima from the state adjoint, the adjoint grid left as garbage
+        b.adjoint_params()
+        torch.cuda.synchronize()
+        assert torch.equal(b.grad, g1), fill
 
 
 @pytest.mark.parametrize("kind", [0, 1])
@@ -295,7 +303,7 @@ def test_adjoint_without_pair_parameter_columns(cuda, kind):
                                                        ctypes.byref(b.shape), _lib.ptr(b.atoms), _lib.ptr(b.params),
                                                        _lib.hptr(b._Qs), _lib.hptr(b._QZs), _lib.ptr(b.PPs),
                                                        _lib.ptr(b.ubar), _lib.ptr(b.dk), _lib.ptr(b.grad),
-                                                       _lib.ptr(b.dk_sum), 2, _lib.ptr(b.adj_scratch),
+                                                       _lib.ptr(b.dk_sum), 4, _lib.ptr(b.adj_scratch),
                                                        _lib.stream_ptr()), "spm_batch_adjoint_params")
 
 
