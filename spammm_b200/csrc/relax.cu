@@ -842,14 +842,14 @@ struct NewtonResult {
 
 template <int LAYOUT>
 __device__ __noinline__ NewtonResult slab_newton(const AxisView G, const PolishSpring S, float t00, float t11,
-                                                 float t22, V3 tip, V3 q) {
+                                                 float t22, V3 tip, V3 q, bool early) {
     const float Tc[3][3] = {{t00, 0.f, 0.f}, {0.f, t11, 0.f}, {0.f, 0.f, t22}};
     NewtonResult r;
     r.q = q;
     r.fe = make_float4(0.f, 0.f, 0.f, 0.f);
     r.g2 = 0.f;
     r.evals = 0;
-    r.ok = newton_core(SlabCellFetch<LAYOUT>{G}, Tc, S, tip, r.q, r.fe, r.g2, r.evals);
+    r.ok = newton_core(SlabCellFetch<LAYOUT>{G}, Tc, S, tip, r.q, r.fe, r.g2, r.evals, early);
     return r;
 }
 
@@ -923,9 +923,9 @@ __device__ __forceinline__ bool stroke_zstep(const AxisView& G, TexelCache& T, c
             NewtonResult r;
             if constexpr (PREFIX) {  // no FIRE in this kernel: inline, through the lane's texel cache
                 r.q = pos;
-                r.ok = newton_core(SlabCellFetchCached<LAYOUT>{G, T}, Tc, S, L.tip, r.q, r.fe, r.g2, r.evals);
+                r.ok = newton_core(SlabCellFetchCached<LAYOUT>{G, T}, Tc, S, L.tip, r.q, r.fe, r.g2, r.evals, true);
             } else {
-                r = slab_newton<LAYOUT>(G, S, Tc[0][0], Tc[1][1], Tc[2][2], L.tip, pos);
+                r = slab_newton<LAYOUT>(G, S, Tc[0][0], Tc[1][1], Tc[2][2], L.tip, pos, true);
             }
             if (r.ok) {
                 pos = r.q;
@@ -951,7 +951,7 @@ __device__ __forceinline__ bool stroke_zstep(const AxisView& G, TexelCache& T, c
     V3 q = pos;
     if constexpr (POLISH) {
         if (!newton_done && fe.w == fe.w) {
-            const NewtonResult r = slab_newton<LAYOUT>(G, S, Tc[0][0], Tc[1][1], Tc[2][2], L.tip, q);
+            const NewtonResult r = slab_newton<LAYOUT>(G, S, Tc[0][0], Tc[1][1], Tc[2][2], L.tip, q, false);
             if (r.ok) {
                 q = r.q;
                 fe = r.fe;

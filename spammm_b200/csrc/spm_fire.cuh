@@ -514,9 +514,13 @@ __device__ __forceinline__ bool polish_step(const float (&J)[3][3], V3 Gv, V3& d
 // not available (outside the sampler's range or the stored slab).  On return q is the polished
 // position, fe the sample there, g2 = |G(q)|^2 and evals the cells evaluated; false (q and fe
 // unchanged) when the first fetch fails.
+// early (the warm starts' Newton-first, not the polish): also stop after a kept step that lowered
+// |G|^2 by less than 4x -- quadratic convergence has ended, |G| is at the float32 floor, and the
+// next step would most likely be refused.
 template <class Fetch>
 __device__ __forceinline__ bool newton_core(const Fetch& fetch, const float (&T)[3][3], const PolishSpring& S,
-                                            V3 tip, V3& q, float4& fe, float& g2_out, int& evals) {
+                                            V3 tip, V3& q, float4& fe, float& g2_out, int& evals,
+                                            bool early = false) {
     float4 t[8];
     float ax, ay, az;
     evals = 0;
@@ -539,10 +543,12 @@ __device__ __forceinline__ bool newton_core(const Fetch& fetch, const float (&T)
         ++evals;
         const float g21 = dot3(G1, G1);
         if (!(g21 < g2)) break;
+        const bool slow = !(g21 < 0.25f * g2);
         q = q1;
         fe0 = fe1;
         Gv = G1;
         g2 = g21;
+        if (early && slow) break;
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
