@@ -576,7 +576,7 @@ def run_batched(args, dev_index):
         shape, tune_rep = _lib.lib().spm_batch_default_shape(), None
     else:
         # the fit (BatchAdam) reads the position and charge gradients only
-        shape, tune_rep = autotune.tuned_shape(items, max_molecules=args.fit_mols, reps=1, pair_param_grads=False,
+        shape, tune_rep = autotune.tuned_shape(items, max_molecules=args.fit_mols, reps=2, pair_param_grads=False,
                                                polish=polish, warm=warm)
     rng = np.random.default_rng(11)
     pert = []

@@ -22,7 +22,7 @@ extern "C" spm_batch_shape spm_batch_default_shape(void) {
     s.adj_chunk = 16384;
     s.rx_regs = 4;
     s.grid_layout = 0;
-    s.rx_sync = 1;
+    s.rx_sync = 2;  // as 1 unless the call is warm and polished
     s.adj_ilp = 1;
     s.adj_agg = 0;
     return s;
