@@ -440,6 +440,9 @@ typedef struct spm_batch_shape {
     int adj_agg;        /* adjoint scatter: 0 = every state's corner sums straight to the global adjoint
                            grid (64-bit atomics), 1 = first merged per CTA in a shared-memory table
                            (the strokes of one CTA share nodes), one global atomic per distinct node */
+    int adj_stage;      /* adjoint node kernel: 0 = each block of adjoint-grid nodes read with plain
+                           loads, 1 = fetched into shared memory by a bulk copy while the previous
+                           block is examined and computed (with adj_ilp = 1) */
 } spm_batch_shape;
 
 spm_batch_shape spm_batch_default_shape(void);

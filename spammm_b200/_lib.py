@@ -112,7 +112,7 @@ class BatchShape(ctypes.Structure):
         ("gb_ty", ctypes.c_int), ("gb_zb", ctypes.c_int), ("rx_threads", ctypes.c_int),
         ("rx_tile_h", ctypes.c_int), ("rx_ctas_per_sm", ctypes.c_int), ("adj_chunk", ctypes.c_int),
         ("rx_regs", ctypes.c_int), ("grid_layout", ctypes.c_int), ("rx_sync", ctypes.c_int),
-        ("adj_ilp", ctypes.c_int), ("adj_agg", ctypes.c_int),
+        ("adj_ilp", ctypes.c_int), ("adj_agg", ctypes.c_int), ("adj_stage", ctypes.c_int),
     ]
 
     def key(self):

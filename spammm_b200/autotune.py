@@ -11,7 +11,8 @@ Every batched stage reads only its own fields of ``spm_batch_shape``:
                grid_layout (x-pair or xz-quad slabs: the grid is rebuilt in the
                candidate's layout before the relaxation is timed)
   adjoint      adj_chunk (slab nodes per node-major unit), adj_ilp (node pairs
-               per step of the node kernel: 1 at 4 CTAs per SM, 2 at 2)
+               per step of the node kernel: 1 at 4 CTAs per SM, 2 at 2), adj_agg
+               (the scatter's CTA table), adj_stage (node blocks by bulk copies)
 
 so the stages are tuned one after another, each over its own candidates with
 the others held fixed, by timing the stage's launch with CUDA events on a
@@ -36,8 +37,9 @@ RELAX_CANDIDATES = [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=r, grid
                     for h in (2, 4, 8, 16) for r in (0, 1, 2, 3, 4)] + \
                    [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=5, grid_layout=0) for h in (2, 4, 8, 16)] + \
                    [dict(rx_sync=0, rx_threads=128, rx_tile_h=8, rx_regs=0, grid_layout=0)]
-ADJOINT_CANDIDATES = [dict(adj_chunk=c, adj_ilp=i, adj_agg=a) for c in (4096, 16384, 65536) for i in (1, 2)
-                      for a in (0, 1)]
+ADJOINT_CANDIDATES = [dict(adj_chunk=c, adj_ilp=i, adj_agg=a, adj_stage=0) for c in (4096, 16384, 65536)
+                      for i in (1, 2) for a in (0, 1)] + \
+                     [dict(adj_chunk=c, adj_ilp=1, adj_agg=0, adj_stage=1) for c in (4096, 16384)]
 
 _CACHE = {}
 

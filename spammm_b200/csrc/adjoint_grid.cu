@@ -1006,6 +1006,19 @@ __device__ __forceinline__ void fold_sums(f2* sums, double* acc, int stride) {
 // partials and the double-buffered warp counts of the compaction scan.
 constexpr int NM_BUF = 2 * NM_STAGE + 2;
 constexpr size_t NM_SMEM = 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(double) + 2 * (NM_THREADS / 32) * sizeof(int);
+// BULK (spm_batch_shape.adj_stage = 1): a block of NM_THREADS adjoint-grid nodes (32 bytes each) is
+// fetched by one bulk copy into shared memory while the previous block is examined and computed,
+// completion on an mbarrier: 8 KB more per CTA (four still fit per SM)
+constexpr size_t NM_RAW = (size_t)NM_THREADS * 32;
+constexpr size_t NM_SMEM_BULK = (NM_SMEM + 15) / 16 * 16 + NM_RAW + 16;
+constexpr unsigned NM_SPIN = 1u << 22;  // bounded mbarrier polls before a block is read with plain loads
+
+__device__ __forceinline__ bool nm_try_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
 
 // CTA per node unit (molecule, `chunk` consecutive slab nodes).  Non-zero
 // adjoint-grid nodes are compacted into shared memory (one float array per
@@ -1027,18 +1040,32 @@ constexpr size_t NM_SMEM = 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(
 // five at 48 registers spill too much).  ILP = 2: two independent node pairs
 // per step at two CTAs per SM (up to 128 registers).  PAR: also the
 // pair-parameter columns 3-4 (else written as 0).
-template <int KIND, bool ON, bool PAR, int ILP>
+template <int KIND, bool ON, bool PAR, int ILP, bool BULK = false>
 __global__ void __launch_bounds__(NM_THREADS, ILP == 2 ? 2 : 4)
 batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk,
                            const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
                            NodeSites S, unsigned long long* __restrict__ gq, const int* __restrict__ box,
-                           const unsigned* __restrict__ umax, double* __restrict__ partial) {
+                           const unsigned* __restrict__ umax, double* __restrict__ partial,
+                           unsigned* __restrict__ status) {
+    static_assert(!BULK || ILP == 1, "bulk-copy staging with one node pair per step");
     extern __shared__ __align__(16) unsigned char nm_smem[];
     float(*s_n)[NM_BUF] = reinterpret_cast<float(*)[NM_BUF]>(nm_smem);
     double(*red)[NM_THREADS] = reinterpret_cast<double(*)[NM_THREADS]>(nm_smem + 7 * NM_BUF * sizeof(float));
     int(*s_wsum)[NM_THREADS / 32] = reinterpret_cast<int(*)[NM_THREADS / 32]>(
         nm_smem + 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(double));
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    // BULK: the raw block (node i of the block at s_raw[2i], s_raw[2i+1]) and its mbarrier
+    ulonglong2* s_raw = reinterpret_cast<ulonglong2*>(nm_smem + (NM_SMEM + 15) / 16 * 16);
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(nm_smem + (NM_SMEM + 15) / 16 * 16 + NM_RAW);
+    unsigned parity = 0;
+    bool bulk = BULK;  // false after a wait ran out: plain loads from then on
+    if (BULK) {
+        if (t == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+    }
     const long long unit = blockIdx.x;
     const int m = SPM_MOL_BY(unit_off, mols, n_mol, unit);
     const spm_batch_mol* D = mols + m;
@@ -1166,7 +1193,100 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
             __syncthreads();  // the buffer is restaged next
         };
         int staged = 0, pass = 0;  // block-uniform
-        for (long long b0 = n0;; b0 += NM_STAGE) {
+        if (BULK) {
+            // blocks of NM_THREADS nodes; the next touched block is fetched while this one is examined
+            // and while the staged nodes are computed
+            auto next_touched = [&](long long b) {
+                while (b < n1 && !touched(b, b + NM_THREADS < n1 ? b + NM_THREADS : n1)) b += NM_THREADS;
+                return b;
+            };
+            auto issue = [&](long long b) {  // thread 0; b < n1
+                const long long e = b + NM_THREADS < n1 ? b + NM_THREADS : n1;
+                const unsigned bytes = (unsigned)(e - b) * 32u;
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(bytes) : "memory");
+                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                             :: "r"((unsigned)__cvta_generic_to_shared(s_raw)), "l"(q2 + 2 * b), "r"(bytes), "r"(bar)
+                             : "memory");
+            };
+            long long b0 = next_touched(n0);
+            if (bulk && t == 0 && b0 < n1) issue(b0);
+            while (true) {
+                const bool more = b0 < n1;
+                if (more) {
+                    const long long b1 = b0 + NM_THREADS < n1 ? b0 + NM_THREADS : n1;
+                    bool from_smem = bulk;
+                    if (bulk) {  // every thread polls: bounded, then a second bounded wait for the copy in flight
+                        unsigned spins = 0;
+                        bool done = nm_try_wait(bar, parity);
+                        while (!done && ++spins < NM_SPIN) done = nm_try_wait(bar, parity);
+                        if (!done) {
+                            if (t == 0) atomicOr(status, 1u);
+                            spins = 0;
+                            while (!done && ++spins < NM_SPIN) done = nm_try_wait(bar, parity);
+                        }
+                        from_smem = __syncthreads_and(done);
+                        parity ^= 1u;
+                        if (!from_smem) bulk = false;  // block-uniform: plain loads from here on
+                    }
+                    const long long node = b0 + t;
+                    ulonglong2 lo = make_ulonglong2(0ull, 0ull), hi = lo;
+                    if (node < b1) {
+                        if (from_smem) {
+                            lo = s_raw[2 * t];
+                            hi = s_raw[2 * t + 1];
+                        } else {
+                            lo = q2[2 * node];
+                            hi = q2[2 * node + 1];
+                        }
+                    }
+                    const bool nzr = (lo.x | lo.y | hi.x | hi.y) != 0ull;
+                    int x = nzr ? 1 : 0;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, x, o);
+                        if (lane >= o) x += y;
+                    }
+                    int* ws = s_wsum[pass & 1];
+                    if (lane == 31) ws[warp] = x;
+                    __syncthreads();  // also: every thread has read its raw node
+                    int off = staged + x - (nzr ? 1 : 0), L = 0;
+#pragma unroll
+                    for (int w = 0; w < NM_THREADS / 32; w++) {
+                        const int c = ws[w];
+                        if (w < warp) off += c;
+                        L += c;
+                    }
+                    const long long bn = next_touched(b0 + NM_THREADS);
+                    if (bulk && t == 0 && bn < n1) issue(bn);  // the raw block is free: fetch the next one
+                    if (nzr) {
+                        if (last_group) {
+                            q2[2 * node] = make_ulonglong2(0ull, 0ull);
+                            q2[2 * node + 1] = make_ulonglong2(0ull, 0ull);
+                        }
+                        const unsigned l32 = (unsigned)node, yz = l32 / (unsigned)nx;
+                        const int ix = (int)(l32 - yz * (unsigned)nx) + x_lo;
+                        const int iy = (int)(yz % (unsigned)ny) + y_lo, iz = (int)(yz / (unsigned)ny) + z_lo;
+                        s_n[0][off] = NG.p0.x + NG.dA.x * ix + NG.dB.x * iy + NG.dC.x * iz;
+                        s_n[1][off] = NG.p0.y + NG.dA.y * ix + NG.dB.y * iy + NG.dC.y * iz;
+                        s_n[2][off] = NG.p0.z + NG.dA.z * ix + NG.dB.z * iy + NG.dC.z * iz;
+                        s_n[3][off] = (float)((double)(long long)lo.x * inv_scale);
+                        s_n[4][off] = (float)((double)(long long)lo.y * inv_scale);
+                        s_n[5][off] = (float)((double)(long long)hi.x * inv_scale);
+                        s_n[6][off] = (float)((double)(long long)hi.y * inv_scale);
+                    }
+                    staged += L;
+                    ++pass;
+                    b0 = bn;
+                }
+                if (staged >= NM_STAGE || (!more && staged > 0)) {
+                    compute(staged);
+                    staged = 0;
+                }
+                if (!more) break;
+            }
+        }
+        for (long long b0 = BULK ? n1 : n0; !BULK; b0 += NM_STAGE) {
             const bool more = b0 < n1;
             const long long b1 = b0 + NM_STAGE < n1 ? b0 + NM_STAGE : n1;
             if (more && touched(b0, b1)) {
@@ -1276,20 +1396,22 @@ batch_fold_rows_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int ch
 
 using NodeKern = decltype(&batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, true, 1>);
 
-template <bool PAR, int ILP>
+template <bool PAR, int ILP, bool BULK>
 NodeKern node_kernel(int kind, bool on) {
     if (kind == SPM_KIND_MORSE)
-        return on ? batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, PAR, ILP>
-                  : batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, PAR, ILP>;
-    return on ? batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, PAR, ILP>
-              : batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, PAR, ILP>;
+        return on ? batch_adjoint_nodes_kernel<SPM_KIND_MORSE, true, PAR, ILP, BULK>
+                  : batch_adjoint_nodes_kernel<SPM_KIND_MORSE, false, PAR, ILP, BULK>;
+    return on ? batch_adjoint_nodes_kernel<SPM_KIND_LJ, true, PAR, ILP, BULK>
+              : batch_adjoint_nodes_kernel<SPM_KIND_LJ, false, PAR, ILP, BULK>;
 }
 
 // The node kernel for a pair law, on-node charges or not, pair-parameter
-// columns or not, and 1 or 2 node pairs per step.
-NodeKern node_kernel(int kind, bool on, bool par, int ilp) {
-    if (ilp == 2) return par ? node_kernel<true, 2>(kind, on) : node_kernel<false, 2>(kind, on);
-    return par ? node_kernel<true, 1>(kind, on) : node_kernel<false, 1>(kind, on);
+// columns or not, 1 or 2 node pairs per step, and node blocks read with plain
+// loads or fetched by bulk copies (stage = 1, with one node pair per step).
+NodeKern node_kernel(int kind, bool on, bool par, int ilp, int stage) {
+    if (stage == 1) return par ? node_kernel<true, 1, true>(kind, on) : node_kernel<false, 1, true>(kind, on);
+    if (ilp == 2) return par ? node_kernel<true, 2, false>(kind, on) : node_kernel<false, 2, false>(kind, on);
+    return par ? node_kernel<true, 1, false>(kind, on) : node_kernel<false, 1, false>(kind, on);
 }
 
 // Scratch layout of spm_batch_adjoint_params (byte offsets, 16-byte aligned):
@@ -1379,6 +1501,8 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
                 chunk);
     SPM_REQUIRE(shape->adj_ilp == 1 || shape->adj_ilp == 2, "spm_batch_adjoint_params: adj_ilp=%d", shape->adj_ilp);
     SPM_REQUIRE(shape->adj_agg == 0 || shape->adj_agg == 1, "spm_batch_adjoint_params: adj_agg=%d", shape->adj_agg);
+    SPM_REQUIRE(shape->adj_stage == 0 || (shape->adj_stage == 1 && shape->adj_ilp == 1),
+                "spm_batch_adjoint_params: adj_stage=%d (1 takes adj_ilp = 1)", shape->adj_stage);
     SPM_REQUIRE((reinterpret_cast<uintptr_t>(scratch) & 15u) == 0, "spm_batch_adjoint_params: scratch not 16-byte aligned");
     SPM_REQUIRE(n_units < (1LL << 31) && n_chunks < (1LL << 31) && n_atoms < (1LL << 30) &&
                 (n_states + 255) / 256 < (1LL << 31), "spm_batch_adjoint_params: batch too large");
@@ -1402,10 +1526,12 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             if (cudaGetDevice(&dev) != cudaSuccess)
                 return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: no current device");
             if (dev < 0 || dev >= 64 || !smem_set[dev]) {
-                for (int v = 0; v < 16; v++) {
+                for (int v = 0; v < 24; v++) {
+                    const int stage = v >= 16 ? 1 : 0;
                     const auto k = node_kernel(v & 1 ? SPM_KIND_MORSE : SPM_KIND_LJ, (v & 2) != 0, (v & 4) != 0,
-                                               v & 8 ? 2 : 1);
-                    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)NM_SMEM) != cudaSuccess)
+                                               v & 8 ? 2 : 1, stage);
+                    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(stage ? NM_SMEM_BULK : NM_SMEM)) != cudaSuccess)
                         return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: cannot set shared memory size");
                 }
                 if (dev >= 0 && dev < 64) smem_set[dev] = true;
@@ -1435,10 +1561,13 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             const NodeSites S = make_node_sites(Qs, QZs);
             const int pstride = kind == SPM_KIND_MORSE ? 4 : 2;
             const bool on = S.qon != 0.f;
-            const auto kern = node_kernel(kind, on, (adj_flags & SPM_ADJ_PAIR_PARAMS) != 0, shape->adj_ilp);
-            kern<<<(unsigned)n_units, NM_THREADS, NM_SMEM, st>>>(n_mol, mols, chunk,
-                                                                 reinterpret_cast<const float4*>(atoms), params, pstride,
-                                                                 S, gq, box, umax, part);
+            const auto kern = node_kernel(kind, on, (adj_flags & SPM_ADJ_PAIR_PARAMS) != 0, shape->adj_ilp,
+                                          shape->adj_stage);
+            // status: the second word of the marker slot (bit 0: a bulk copy's wait ran out)
+            unsigned* status = reinterpret_cast<unsigned*>(mark + 1);
+            kern<<<(unsigned)n_units, NM_THREADS, shape->adj_stage ? NM_SMEM_BULK : NM_SMEM, st>>>(
+                n_mol, mols, chunk, reinterpret_cast<const float4*>(atoms), params, pstride, S, gq, box, umax, part,
+                status);
             nodes_ran = true;
         }
         batch_fold_rows_kernel<<<dim3((unsigned)n_atoms, 6), 256, 0, st>>>(n_mol, mols, chunk, part, grad,

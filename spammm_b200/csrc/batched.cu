@@ -25,6 +25,7 @@ extern "C" spm_batch_shape spm_batch_default_shape(void) {
     s.rx_sync = 2;  // as 1 unless the call is warm and polished
     s.adj_ilp = 1;
     s.adj_agg = 0;
+    s.adj_stage = 0;
     return s;
 }
 
@@ -49,6 +50,8 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
     SPM_REQUIRE(S.rx_sync >= 0 && S.rx_sync <= 2, "spm_batch_prepare: rx_sync=%d", S.rx_sync);
     SPM_REQUIRE(S.adj_ilp == 1 || S.adj_ilp == 2, "spm_batch_prepare: adj_ilp=%d", S.adj_ilp);
     SPM_REQUIRE(S.adj_agg == 0 || S.adj_agg == 1, "spm_batch_prepare: adj_agg=%d", S.adj_agg);
+    SPM_REQUIRE(S.adj_stage == 0 || (S.adj_stage == 1 && S.adj_ilp == 1), "spm_batch_prepare: adj_stage=%d",
+                S.adj_stage);
     const long long th = S.rx_tile_h, tw = 32 / S.rx_tile_h;
     long long tiles = 0, slots = 0, units = 0, chunks = 0, states = 0, atoms = 0, pixels = 0, grid_end = 0, rows = 0;
     for (int m = 0; m < n_mol; m++) {

@@ -17,7 +17,7 @@ def small_items(n=7, seed=5, kind=0):
 def test_struct_layout():
     # spm_batch_mol: 7 int64 offsets, 16 int32 fields, 7 float[4] vectors
     assert ctypes.sizeof(_lib.BatchMol) == 7 * 8 + 16 * 4 + 7 * 16
-    assert ctypes.sizeof(_lib.BatchShape) == 11 * 4
+    assert ctypes.sizeof(_lib.BatchShape) == 12 * 4
 
 
 @pytest.mark.parametrize("shape_kw", [{}, dict(gb_ty=2, gb_zb=16, rx_tile_h=1, adj_chunk=1024),
@@ -131,7 +131,7 @@ def test_prepare_rejects_bad_descriptors():
     assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_ERR_ARG
     plan = BatchPlan(small_items(4))
     for field, bad in (("gb_ty", 3), ("gb_zb", 4), ("rx_threads", 96), ("rx_tile_h", 6), ("adj_chunk", 1000), ("rx_regs", 6), ("grid_layout", 2),
-                       ("rx_sync", 3), ("adj_ilp", 3)):
+                       ("rx_sync", 3), ("adj_ilp", 3), ("adj_stage", 2)):
         s = L.spm_batch_default_shape()
         setattr(s, field, bad)
         assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(s), totals) == _lib.SPM_ERR_ARG, field

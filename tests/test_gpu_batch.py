@@ -465,6 +465,28 @@ def test_batch_staged_relaxation_is_bit_identical(cuda):
         assert int(b.workspace[1]) == 0, "a staging wait timed out"
 
 
+def test_batch_adjoint_bulk_staged_node_blocks(cuda):
+    """adj_stage = 1: the node kernel fetches each block of adjoint-grid nodes by a bulk copy into
+    shared memory.  The same pair terms; blocks of 256 instead of 512 nodes put the non-zero nodes in
+    another order within a compute phase, so the FP32 partial sums round differently: within 1e-6 of
+    the plain-load kernel's gradients (relative to the largest), and repeatable call after call."""
+    items = _items(0, n=5, seed=67)
+    out = []
+    for stage in (0, 1):
+        shape = _lib.BatchShape(*_lib.lib().spm_batch_default_shape().key())
+        shape.adj_stage = stage
+        b = AFMBatch(items, shape=shape)
+        _target(b)
+        b.forward_adjoint()
+        g1 = b.grad.clone()
+        b.adjoint_params()
+        torch.cuda.synchronize()
+        assert torch.equal(g1, b.grad)
+        out.append(g1)
+    scale = float(out[0].abs().max())
+    torch.testing.assert_close(out[1], out[0], rtol=1e-6, atol=1e-6 * scale)
+
+
 def test_batch_adjoint_aggregated_scatter_is_bit_identical(cuda):
     """adj_agg = 1 (the scatter merges each CTA's corner sums in shared memory first): the same exact integer
     sums, so the gradients and spring terms equal the direct scatter's bit for bit, call after call."""
