@@ -842,6 +842,153 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
     }
 }
 
+// Tile scatter (spm_batch_shape.adj_agg = 2): a warp takes one relaxation slot tile -- 32 pixels of
+// one molecule, (32/h) x h of the raster -- and its lanes walk their strokes down together, one
+// z-step at a time.  A state's upper corner layer is its stroke predecessor's lower layer when the
+// cell column is the same: the lane adds the carried lower-layer sums there (as the default
+// kernel's lane pairs do).  The warp then merges equal nodes across its lanes before the 64-bit
+// atomics: a corner goes to slot ((x0+i)&1) | ((y0+j)&1)<<1 | ((z0+k)&1)<<2 (unwrapped indices), so
+// a lane has at most one node per slot and neighbouring pixels' shared nodes meet in the same slot;
+// per slot __match_any_sync groups the lanes holding the same node and the group's first lane adds
+// the group's sums (from shared memory) with one atomic per channel.  Integer sums of the same
+// fixed-point terms: the default kernel's bits.  Carried corners that share a slot with the upper
+// layer (the column moved within the same layer parity) are flushed in a second round.
+constexpr int SCT_WARPS = 4;
+constexpr unsigned SCT_NONE = 0xffffffffu;  // no node (slab nodes are fewer than 2^32 - 32)
+
+__global__ void __launch_bounds__(SCT_WARPS * 32)
+batch_scatter_tile_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
+                          const float4* __restrict__ PPs, const float4* __restrict__ ubar,
+                          const unsigned* __restrict__ umax, unsigned long long* __restrict__ gq,
+                          unsigned long long* __restrict__ mark, unsigned* __restrict__ counter) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *mark = ADJ_DIRTY;  // the adjoint grid is written from here on
+    __shared__ long long s_v[SCT_WARPS][4][32];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    while (true) {
+        unsigned tb = 0;
+        if (lane == 0) tb = atomicAdd(counter, 32u);
+        tb = __shfl_sync(FULL, tb, 0);
+        if (tb >= n_slots) return;  // warp-uniform
+        const int m = SPM_MOL_BY(slot_off, mols, n_mol, (long long)tb);
+        const spm_batch_mol* D = mols + m;
+        int k = 0;
+        const bool lv = slot_pixel(D, tb + lane - (unsigned)D->slot_off, th_log2, k);
+        const int nz = D->nz_steps;
+        const GridView G = slab_view(*D, nullptr);
+        const long long sbase = D->state_off + (long long)(lv ? k : 0) * nz;
+        unsigned long long* base = gq + (size_t)D->grid_off * 4;
+        const double scale = pow2(42 - scale_exp(__ldg(umax + m)));
+        const int nxs = G.nx_slab, nys = G.ny_slab, x_lo = G.x_lo, y_lo = G.y_lo, z_lo = G.z_lo;
+        auto node_of = [&](int x, int y, int z) {
+            return ((unsigned)(z - z_lo) * (unsigned)nys + (unsigned)(y - y_lo)) * (unsigned)nxs + (unsigned)(x - x_lo);
+        };
+        auto fixq = [&](float w, float u) {  // the default kernel's fixed-point term
+            return w == 0.f ? 0ll : __double2ll_rn((double)(w * u) * scale);
+        };
+        // this z-step's state and the carried lower layer of the previous one (weights and ubar kept,
+        // the fixed-point terms recomputed when flushed)
+        bool cv = false;
+        int cx0 = 0, cy0 = 0, cz0 = 0, cx1 = 0, cy1 = 0, cpx = 0, cpy = 0, cpz = 0;
+        float cw[4] = {0.f, 0.f, 0.f, 0.f};
+        float4 cub = make_float4(0.f, 0.f, 0.f, 0.f);
+        // one merge round: per slot, this lane's entry (has, node, 4 values) from `entry`
+        auto round = [&](auto entry) {
+#pragma unroll
+            for (int sl = 0; sl < 8; sl++) {
+                unsigned key = SCT_NONE - (unsigned)lane;
+                long long v[4] = {0, 0, 0, 0};
+                const bool has = entry(sl, key, v);
+                const unsigned grp = __match_any_sync(FULL, has ? key : SCT_NONE - (unsigned)lane);
+#pragma unroll
+                for (int ch = 0; ch < 4; ch++) s_v[warp][ch][lane] = v[ch];
+                __syncwarp();
+                if (has && lane == __ffs(grp) - 1) {
+#pragma unroll
+                    for (int ch = 0; ch < 4; ch++) {
+                        long long sum = 0;
+                        for (unsigned g = grp; g; g &= g - 1) sum += s_v[warp][ch][__ffs(g) - 1];
+                        if (sum != 0) atomicAdd(base + (size_t)key * 4 + ch, (unsigned long long)sum);
+                    }
+                }
+                __syncwarp();
+            }
+        };
+        for (int iz = 0; iz <= nz; ++iz) {  // iz == nz: flush the last carried layer only
+            bool valid = false;
+            Corners C = {{0, 0}, {0, 0}, {0, 0}, 0.f, 0.f, 0.f, false};
+            float4 ub = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (lv && iz < nz) {
+                ub = __ldg(ubar + sbase + iz);
+                valid = !(ub.x == 0.f && ub.y == 0.f && ub.z == 0.f && ub.w == 0.f);
+                if (valid) {
+                    const float4 pp = __ldg(PPs + sbase + iz);
+                    C = corners_of<true>(G, mk3(pp.x, pp.y, pp.z));
+                    valid = C.ok;
+                }
+            }
+            // upper-layer weights (k = 1) and lower-layer weights (k = 0) of corner (i, j)
+            float wu[4], wl[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int i = c & 1, j = c >> 1;
+                const float wxy = (i ? C.ax : 1.f - C.ax) * (j ? C.ay : 1.f - C.ay);
+                wu[c] = valid ? wxy * C.az : 0.f;
+                wl[c] = valid ? wxy * (1.f - C.az) : 0.f;
+            }
+            // unwrapped parities of the cell's lower corner
+            const int px = C.x[0] & 1, py = C.y[0] & 1, pz = C.z[0] & 1;
+            const bool merge = valid && cv && C.x[0] == cx0 && C.y[0] == cy0 && C.z[1] == cz0;
+            const bool carried_out = cv && !merge;  // the carried layer goes out on its own
+            const bool clash = carried_out && valid && (cpz == ((pz + 1) & 1));  // shares the upper layer's slots
+            // the upper layer (+ the carried layer when it is the same nodes), and a carried layer that
+            // does not clash
+            round([&](int sl, unsigned& key, long long (&v)[4]) {
+                const int si = sl & 1, sj = (sl >> 1) & 1, sk = sl >> 2;
+                if (valid && sk == ((pz + 1) & 1)) {
+                    const int i = si ^ px, j = sj ^ py, c = i + 2 * j;
+                    key = node_of(C.x[i], C.y[j], C.z[1]);
+                    const float u4[4] = {ub.x, ub.y, ub.z, ub.w}, c4[4] = {cub.x, cub.y, cub.z, cub.w};
+#pragma unroll
+                    for (int ch = 0; ch < 4; ch++) v[ch] = fixq(wu[c], u4[ch]) + (merge ? fixq(cw[c], c4[ch]) : 0ll);
+                    return true;
+                }
+                if (carried_out && !clash && sk == cpz) {
+                    const int i = si ^ cpx, j = sj ^ cpy, c = i + 2 * j;
+                    key = node_of(i ? cx1 : cx0, j ? cy1 : cy0, cz0);
+                    const float c4[4] = {cub.x, cub.y, cub.z, cub.w};
+#pragma unroll
+                    for (int ch = 0; ch < 4; ch++) v[ch] = fixq(cw[c], c4[ch]);
+                    return true;
+                }
+                return false;
+            });
+            if (__any_sync(FULL, clash)) {
+                round([&](int sl, unsigned& key, long long (&v)[4]) {
+                    const int si = sl & 1, sj = (sl >> 1) & 1, sk = sl >> 2;
+                    if (clash && sk == cpz) {
+                        const int i = si ^ cpx, j = sj ^ cpy, c = i + 2 * j;
+                        key = node_of(i ? cx1 : cx0, j ? cy1 : cy0, cz0);
+                        const float c4[4] = {cub.x, cub.y, cub.z, cub.w};
+#pragma unroll
+                        for (int ch = 0; ch < 4; ch++) v[ch] = fixq(cw[c], c4[ch]);
+                        return true;
+                    }
+                    return false;
+                });
+            }
+            // carry this state's lower layer
+            cv = valid;
+            cx0 = C.x[0]; cx1 = C.x[1]; cy0 = C.y[0]; cy1 = C.y[1]; cz0 = C.z[0];
+            cpx = px; cpy = py; cpz = pz;
+#pragma unroll
+            for (int c = 0; c < 4; c++) cw[c] = wl[c];
+            cub = ub;
+        }
+        __syncwarp();  // the whole warp draws the next tile
+    }
+}
+
 constexpr int NM_THREADS = 256;
 constexpr int NM_PER_THREAD = 2;
 constexpr int NM_STAGE = NM_THREADS * NM_PER_THREAD;  // nodes examined per staging pass
@@ -1500,7 +1647,8 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
     SPM_REQUIRE(chunk >= 1024 && chunk <= (1 << 20) && chunk % 1024 == 0, "spm_batch_adjoint_params: adj_chunk=%d",
                 chunk);
     SPM_REQUIRE(shape->adj_ilp == 1 || shape->adj_ilp == 2, "spm_batch_adjoint_params: adj_ilp=%d", shape->adj_ilp);
-    SPM_REQUIRE(shape->adj_agg == 0 || shape->adj_agg == 1, "spm_batch_adjoint_params: adj_agg=%d", shape->adj_agg);
+    SPM_REQUIRE(shape->adj_agg >= 0 && shape->adj_agg <= 2, "spm_batch_adjoint_params: adj_agg=%d", shape->adj_agg);
+    SPM_REQUIRE(totals[1] >= 0 && totals[1] < (1LL << 31), "spm_batch_adjoint_params: slots=%lld", totals[1]);
     SPM_REQUIRE(shape->adj_stage == 0 || (shape->adj_stage == 1 && shape->adj_ilp == 1),
                 "spm_batch_adjoint_params: adj_stage=%d (1 takes adj_ilp = 1)", shape->adj_stage);
     SPM_REQUIRE((reinterpret_cast<uintptr_t>(scratch) & 15u) == 0, "spm_batch_adjoint_params: scratch not 16-byte aligned");
@@ -1544,7 +1692,24 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
                 batch_ubar_max_kernel<<<(unsigned)((n_chunks + UM_CHUNKS - 1) / UM_CHUNKS), 256, 0, st>>>(
                     n_mol, n_chunks, mols, reinterpret_cast<const float4*>(ubar), reinterpret_cast<const float4*>(PPs),
                     umax, box);
-            if (shape->adj_agg) {
+            if (shape->adj_agg == 2) {
+                int th_log2 = 0;
+                while ((1 << th_log2) < shape->rx_tile_h) th_log2++;
+                unsigned* counter = reinterpret_cast<unsigned*>(mark + 1) + 1;  // the marker slot's last word
+                if (cudaMemsetAsync(counter, 0, sizeof(unsigned), st) != cudaSuccess)
+                    return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: memset failed");
+                int dev_t = 0, sms = 0, per_sm = 0;
+                if (cudaGetDevice(&dev_t) != cudaSuccess ||
+                    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_t) != cudaSuccess ||
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_scatter_tile_kernel, SCT_WARPS * 32,
+                                                                  0) != cudaSuccess)
+                    return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: cannot query the device occupancy");
+                const long long need = (totals[1] + SCT_WARPS * 32 - 1) / (SCT_WARPS * 32);
+                const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
+                batch_scatter_tile_kernel<<<(unsigned)(need < cap ? need : cap), SCT_WARPS * 32, 0, st>>>(
+                    n_mol, mols, (unsigned)totals[1], th_log2, reinterpret_cast<const float4*>(PPs),
+                    reinterpret_cast<const float4*>(ubar), umax, gq, mark, counter);
+            } else if (shape->adj_agg) {
                 const size_t agg_smem = sizeof(unsigned long long) * 5 * AGG_SLOTS;
                 if (cudaFuncSetAttribute(batch_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)agg_smem) != cudaSuccess)

@@ -488,13 +488,15 @@ def test_batch_adjoint_bulk_staged_node_blocks(cuda):
 
 
 def test_batch_adjoint_aggregated_scatter_is_bit_identical(cuda):
-    """adj_agg = 1 (the scatter merges each CTA's corner sums in shared memory first): the same exact integer
-    sums, so the gradients and spring terms equal the direct scatter's bit for bit, call after call."""
+    """adj_agg = 1 (the scatter merges each CTA's corner sums in shared memory first) and 2 (a warp walks a
+    pixel tile down its strokes and merges its lanes' shared nodes): the same exact integer sums, so the
+    gradients and spring terms equal the direct scatter's bit for bit, call after call, for every tile
+    height."""
     items = _items(0, n=5, seed=65)
     out = []
-    for agg in (0, 1):
+    for agg, h in ((0, 8), (1, 8), (2, 8), (2, 1), (2, 4), (2, 32)):
         shape = _lib.BatchShape(*_lib.lib().spm_batch_default_shape().key())
-        shape.adj_agg = agg
+        shape.adj_agg, shape.rx_tile_h = agg, h
         b = AFMBatch(items, shape=shape)
         _target(b)
         b.forward_adjoint()
@@ -503,4 +505,5 @@ def test_batch_adjoint_aggregated_scatter_is_bit_identical(cuda):
         torch.cuda.synchronize()
         assert torch.equal(g1, b.grad)
         out.append((g1, b.dk_sum.clone()))
-    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+    for g, dks in out[1:]:
+        assert torch.equal(out[0][0], g) and torch.equal(out[0][1], dks)
