@@ -457,12 +457,96 @@ def run_ours(args, rank, world, local_rank):
     line["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
     if not args.no_batch and world == 1:
         line["batched"] = run_batched(args, local_rank)
+    if world == 1:
+        line["direct"] = run_direct(args, local_rank)
     if not args.no_cpu and world == 1:
         v, det = cpu_sample(cfg)
         det["value"] = v
         det["unit"] = UNIT
         line["cpu_baseline"] = det
     return line
+
+
+# ---------------------------------------------------------------------------- direct path
+# per (FIRE step, atom) of relax_direct_kernel's pair loop: Morse 18 FP32 lane instructions + 2 MUFU
+# (rsqrt, ex2), each non-zero tip-charge site 9 + 1 (the loop as written in csrc/direct.cu)
+DIRECT_PAIR = (18, 2)
+DIRECT_SITE = (9, 1)
+
+
+def run_direct(args, dev_index):
+    """The grid-free Morse path (run_scan_morse_direct / vjp_scan_morse_direct): the config-0 molecule
+    with Morse parameters, 100x100 pixels x 40 z-steps, the AFMulator's default probe (radial 4 A
+    bond) and FIRE settings; forward and the implicit VJP of a df-like seed, device-resident inputs,
+    CUDA events."""
+    import torch
+    from spammm_b200 import _lib, gpu, synthetic
+    from spammm_b200.AFM import AFMulator, N_RELAX_STEP_MAX, F2CONV
+    cfg = synthetic.plain_small(kind=1)
+    n = len(cfg.scan_xs)
+    gx, gy = np.meshgrid(cfg.scan_xs, cfg.scan_ys, indexing="ij")
+    dpos0 = AFMulator.DEFAULT_dpos0
+    pts = np.zeros((n * n, 4), np.float32)
+    pts[:, 0], pts[:, 1], pts[:, 2] = gx.ravel(), gy.ravel(), cfg.z_top - dpos0[2]  # the probe starts at z_top
+    tipC = AFMulator.DEFAULT_tipC.copy()
+    tipC[3] = -cfg.dz
+    P = _lib.make_scan_params(tipA=AFMulator.DEFAULT_tipA, tipB=AFMulator.DEFAULT_tipB, tipC=tipC,
+                              stiffness=AFMulator.DEFAULT_stiffness, dpos0=dpos0, relax_params=AFMulator.DEFAULT_relax_pars,
+                              surfFF=AFMulator.DEFAULT_surfFF, nz=cfg.nz, raster_ny=n, max_iter=N_RELAX_STEP_MAX,
+                              f2conv=F2CONV, fire=True)
+    dev = torch.device("cuda", dev_index)
+    atoms = torch.from_numpy(cfg.atoms).to(dev)
+    cMs = torch.from_numpy(cfg.params).to(dev)
+    pts_d = torch.from_numpy(pts).to(dev)
+    Qs, QZs = AFMulator.DEFAULT_tipQs, AFMulator.DEFAULT_tipQZs
+    for _ in range(max(3, args.warmup)):
+        FEs, PPs = gpu.relax_direct_morse(atoms, cMs, pts_d, P, Qs, QZs)
+    torch.cuda.synchronize()
+    steps = max(3, args.steps)
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(steps):
+        FEs, PPs = gpu.relax_direct_morse(atoms, cMs, pts_d, P, Qs, QZs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_fwd = e0.elapsed_time(e1) / steps
+    fire_steps = float(PPs[..., 3].abs().double().sum())
+    converged = float((PPs[..., 3] > 0).float().mean())
+    # the VJP of a df-like seed (dL/dFz only), the reference's two adjoint passes
+    dL = torch.zeros_like(FEs)
+    dL[..., 2] = torch.randn(FEs.shape[:2], generator=torch.Generator(device=dev).manual_seed(3), device=dev) * 1e-3
+    ok = PPs[..., 3] > 0
+    dL[~ok] = 0.0
+    PPv = PPs.clone()
+    PPv[..., 3] = PPv[..., 3].abs()  # the VJP takes converged states; the few that are not carry a zero seed
+    for _ in range(3):
+        lam, diag = gpu.adjoint_direct_state(atoms, cMs, pts_d, P, Qs, QZs, PPv, dL)
+        grad = gpu.adjoint_direct_params(atoms, cMs, pts_d, P, Qs, QZs, PPv, dL, lam)
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(steps):
+        lam, diag = gpu.adjoint_direct_state(atoms, cMs, pts_d, P, Qs, QZs, PPv, dL)
+        grad = gpu.adjoint_direct_params(atoms, cMs, pts_d, P, Qs, QZs, PPv, dL, lam)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_vjp = e0.elapsed_time(e1) / steps
+    na = cfg.atoms.shape[0]
+    sites = int(sum(1 for q in Qs if q != 0.0))
+    fp32_per, mufu_per = DIRECT_PAIR[0] + sites * DIRECT_SITE[0], DIRECT_PAIR[1] + sites * DIRECT_SITE[1]
+    pair_steps = fire_steps * na
+    fp32_peak = gpu.fp32_peak_flops(1 << 15)
+    lane_rate = pair_steps * fp32_per / (ms_fwd * 1e-3)  # FP32 lane instructions per second
+    pxz = n * n * cfg.nz
+    return {"workload": f"config-0 molecule ({na} atoms, Morse + {sites} tip-charge sites), {n}x{n} px x {cfg.nz} "
+                        "z-steps, the AFMulator's default probe and FIRE (<= 128 steps, |F|^2 < 1e-8), no grid",
+            "forward_ms": ms_fwd, "px_z_per_s": pxz / (ms_fwd * 1e-3), "fire_steps_per_state": fire_steps / pxz,
+            "converged_frac": converged, "vjp_ms": ms_vjp, "vjp_states_per_s": pxz / (ms_vjp * 1e-3),
+            "roofline": {"bound": "fp32 pipe issue (+ MUFU)", "unit": "TFLOP/s",
+                         "achieved": 2.0 * lane_rate / 1e12, "peak": fp32_peak / 1e12,
+                         "frac": 2.0 * lane_rate / fp32_peak,
+                         "algorithmic": f"{pair_steps:.3e} (FIRE step, atom) pairs x {fp32_per} FP32 lane instructions "
+                                        f"(+{mufu_per} MUFU) as written; FMA-equivalent x2"}}
 
 
 # ---------------------------------------------------------------------------- batched path
