@@ -11,8 +11,10 @@
 //
 // B200 shape.  The forward keeps every atom of the molecule in shared memory
 // in the pre-transformed form of the grid builder (MUFU rsqrt/ex2 inner loop)
-// and runs each pixel's (z-step, FIRE step) sequence as one flattened loop per
-// lane with the stroke state in registers.  The adjoint solves one symmetric
+// and gives each pixel a group of 4-32 lanes that split the atoms of every
+// force evaluation and sum them by a butterfly, each lane then holding the same
+// stroke state in registers -- a scan of 10^4 pixels fills the GPU, and a FIRE
+// step costs the latency of na/LPP pair terms instead of na.  The adjoint solves one symmetric
 // 3x3 system per state in registers (cofactors, as the reference) and forms
 // the per-atom parameter partials with a CTA per (atom, 128-scan chunk) that
 // reduces in shared memory in a fixed order; a second pass folds the chunks in
@@ -47,16 +49,81 @@ struct Sites {
     int ns;
 };
 
+__device__ __forceinline__ void stage_atoms(int na, const float4* __restrict__ atoms, const float4* __restrict__ cMs,
+                                            const float* qs_nz, int ns, float4* s_pos, float4* s_m, float* s_q) {
+    for (int j = threadIdx.x; j < na; j += blockDim.x) {
+        const float4 a = __ldg(atoms + j);
+        const float4 c = __ldg(cMs + j);
+        s_pos[j] = make_float4(a.x, a.y, a.z, a.w);
+        s_m[j] = make_float4(c.z * LOG2E, -c.z * c.x * LOG2E, c.y, -2.f * c.z * c.y);
+        for (int k = 0; k < ns; k++) s_q[k * na + j] = a.w * qs_nz[k];
+    }
+}
+
+// LPP lanes per pixel: the group's lanes split the atoms (lane `sub` takes atoms sub, sub + LPP, ...)
+// and sum their partial forces by an xor butterfly over the group, so every lane of the group ends
+// with the same bits (each level adds the same two values, in either order) and runs the same FIRE
+// update: the group stays converged without a broadcast.  gmask: the group's lanes.
+template <int LPP>
+__device__ __forceinline__ float group_sum(float v, unsigned gmask) {
+#pragma unroll
+    for (int o = 1; o < LPP; o <<= 1) v += __shfl_xor_sync(gmask, v, o);
+    return v;
+}
+template <int LPP>
+__device__ __forceinline__ double group_sum(double v, unsigned gmask) {
+#pragma unroll
+    for (int o = 1; o < LPP; o <<= 1) v += __shfl_xor_sync(gmask, v, o);
+    return v;
+}
+
+template <int NS, int LPP>
+__device__ __forceinline__ float4 group_pair_sum(V3 p, int na, int sub, unsigned gmask, const float4* s_pos,
+                                                 const float4* s_m, const float* s_q, const float* qz) {
+    float fx = 0.f, fy = 0.f, fz = 0.f, fe = 0.f;
+    for (int j = sub; j < na; j += LPP) {
+        const float4 a = s_pos[j];
+        const float4 m = s_m[j];
+        const float dx = p.x - a.x, dy = p.y - a.y, dz = p.z - a.z;
+        const float dxy2 = fmaf(dx, dx, fmaf(dy, dy, R2SAFE));
+        const float r2 = fmaf(dz, dz, dxy2);
+        const float rs = fast_rsqrt(r2);
+        const float r = r2 * rs;
+        const float e = fast_ex2(fmaf(m.x, r, m.y));
+        fe = fmaf(m.z * e, e - 2.f, fe);
+        const float sg = (m.w * e) * (e - 1.f) * rs;
+        fx = fmaf(dx, sg, fx);
+        fy = fmaf(dy, sg, fy);
+        fz = fmaf(dz, sg, fz);
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            const float dzk = dz + qz[k];
+            const float rsk = fast_rsqrt(fmaf(dzk, dzk, dxy2));
+            const float Ek = s_q[k * na + j] * rsk;
+            fe += Ek;
+            const float sk = Ek * rsk * rsk;
+            fx = fmaf(dx, sk, fx);
+            fy = fmaf(dy, sk, fy);
+            fz = fmaf(dzk, sk, fz);
+        }
+    }
+    return make_float4(group_sum<LPP>(fx, gmask), group_sum<LPP>(fy, gmask), group_sum<LPP>(fz, gmask),
+                       group_sum<LPP>(fe, gmask));
+}
+
 // |total force|^2 at p in FP64 -- the Morse + Coulomb sums from the atoms' float32 inputs with IEEE
 // double exp/sqrt (the reference's FP64 pair law, kernels/AFM.cl:730-757 in double), the spring and the
 // surface bias -- to confirm a convergence the FP32 sums report: near |F|^2 = f2conv their rounding
 // (MUFU rsqrt/ex2, and the radial spring's r - d0 of a 4 A bond at float32 resolution) can put the
-// FP32 test on the converged side of a state whose force is not.
-__device__ __noinline__ double force2_f64(V3 p, V3 tip, int na, const float4* __restrict__ atoms, const float4* __restrict__ cMs,
-                             const Sites& S, V3 a, V3 b, V3 c, float4 kk, float4 d0, float surf) {
+// FP32 test on the converged side of a state whose force is not.  The atoms are split over the
+// group and the FP64 sums reduced by the same butterfly.
+template <int LPP>
+__device__ __noinline__ double group_force2_f64(V3 p, V3 tip, int na, int sub, unsigned gmask,
+                                                const float4* __restrict__ atoms, const float4* __restrict__ cMs,
+                                                const Sites& S, V3 a, V3 b, V3 c, float4 kk, float4 d0, float surf) {
     const double px = p.x, py = p.y, pz = p.z;
     double fx = 0.0, fy = 0.0, fz = 0.0;
-    for (int j = 0; j < na; j++) {
+    for (int j = sub; j < na; j += LPP) {
         const float4 at = __ldg(atoms + j);
         const float4 cm = __ldg(cMs + j);
         const double dx = px - at.x, dy = py - at.y, dz = pz - at.z;
@@ -78,7 +145,9 @@ __device__ __noinline__ double force2_f64(V3 p, V3 tip, int na, const float4* __
             fz += dzk * sk;
         }
     }
-    // spring in the tip frame: (d - d0.xyz) k.xyz + d k.w (r - d0.w) / r, rotated back
+    fx = group_sum<LPP>(fx, gmask);
+    fy = group_sum<LPP>(fy, gmask);
+    fz = group_sum<LPP>(fz, gmask);
     const double ex = (double)p.x - tip.x, ey = (double)p.y - tip.y, ez = (double)p.z - tip.z;
     const double dl[3] = {ex * a.x + ey * a.y + ez * a.z, ex * b.x + ey * b.y + ez * b.z, ex * c.x + ey * c.y + ez * c.z};
     double ft[3] = {(dl[0] - d0.x) * kk.x, (dl[1] - d0.y) * kk.y, (dl[2] - d0.z) * kk.z};
@@ -94,69 +163,11 @@ __device__ __noinline__ double force2_f64(V3 p, V3 tip, int na, const float4* __
     return fx * fx + fy * fy + fz * fz;
 }
 
-__device__ __forceinline__ int direct_pixel(int n_scan, int raster_ny) {
-    if (raster_ny > 0) {
-        const int nxr = n_scan / raster_ny;
-        const int nby = (raster_ny + 15) / 16;
-        const int bx = blockIdx.x / nby, by = blockIdx.x % nby;
-        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        const int ix = bx * 8 + (w >> 1) * 4 + (l >> 3);
-        const int iy = by * 16 + (w & 1) * 8 + (l & 7);
-        if (ix >= nxr || iy >= raster_ny) return -1;
-        return ix * raster_ny + iy;
-    }
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    return k < n_scan ? k : -1;
-}
-
-// Sum of the uncapped Morse + Coulomb law over the atoms staged in shared
-// memory (s_pos: x,y,z ; s_m: K log2e, -K R0 log2e, E0, -2 K E0 ; s_q[k*na+j]).
-template <int NS>
-__device__ __forceinline__ float4 pair_sum(V3 p, int na, const float4* s_pos, const float4* s_m, const float* s_q,
-                                           const float* qz) {
-    float fx = 0.f, fy = 0.f, fz = 0.f, fe = 0.f;
-#pragma unroll 4
-    for (int j = 0; j < na; j++) {
-        const float4 a = s_pos[j];
-        const float4 m = s_m[j];
-        const float dx = p.x - a.x, dy = p.y - a.y, dz = p.z - a.z;
-        const float dxy2 = fmaf(dx, dx, fmaf(dy, dy, R2SAFE));
-        const float r2 = fmaf(dz, dz, dxy2);
-        const float rs = fast_rsqrt(r2);
-        const float r = r2 * rs;
-        const float e = fast_ex2(fmaf(m.x, r, m.y));
-        fe = fmaf(m.z * e, e - 2.f, fe);
-        const float s = (m.w * e) * (e - 1.f) * rs;
-        fx = fmaf(dx, s, fx);
-        fy = fmaf(dy, s, fy);
-        fz = fmaf(dz, s, fz);
-#pragma unroll
-        for (int k = 0; k < NS; k++) {
-            const float dzk = dz + qz[k];
-            const float rsk = fast_rsqrt(fmaf(dzk, dzk, dxy2));
-            const float Ek = s_q[k * na + j] * rsk;
-            fe += Ek;
-            const float sk = Ek * rsk * rsk;
-            fx = fmaf(dx, sk, fx);
-            fy = fmaf(dy, sk, fy);
-            fz = fmaf(dzk, sk, fz);
-        }
-    }
-    return make_float4(fx, fy, fz, fe);
-}
-
-__device__ __forceinline__ void stage_atoms(int na, const float4* __restrict__ atoms, const float4* __restrict__ cMs,
-                                            const float* qs_nz, int ns, float4* s_pos, float4* s_m, float* s_q) {
-    for (int j = threadIdx.x; j < na; j += blockDim.x) {
-        const float4 a = __ldg(atoms + j);
-        const float4 c = __ldg(cMs + j);
-        s_pos[j] = make_float4(a.x, a.y, a.z, a.w);
-        s_m[j] = make_float4(c.z * LOG2E, -c.z * c.x * LOG2E, c.y, -2.f * c.z * c.y);
-        for (int k = 0; k < ns; k++) s_q[k * na + j] = a.w * qs_nz[k];
-    }
-}
-
-template <int NS>
+// Groups of LPP lanes, one pixel per group (DX_THREADS / LPP pixels per CTA, in raster order); the
+// whole molecule staged in shared memory; each group runs its pixel's (z-step, FIRE step) sequence
+// with the stroke state held identically by every lane of the group.  Convergence is tested before
+// the update, and an FP32 "converged" is confirmed in FP64.
+template <int NS, int LPP>
 __global__ void __launch_bounds__(DX_THREADS)
 relax_direct_kernel(int na, const float4* __restrict__ atoms, const float4* __restrict__ cMs,
                     const float4* __restrict__ pts, int n_scan, spm_scan_params P, Sites S,
@@ -167,8 +178,10 @@ relax_direct_kernel(int na, const float4* __restrict__ atoms, const float4* __re
     float* s_q = reinterpret_cast<float*>(smem + 2 * na);
     stage_atoms(na, atoms, cMs, S.qs, NS, s_pos, s_m, s_q);
     __syncthreads();
-    const int k = direct_pixel(n_scan, P.raster_ny);
-    if (k < 0) return;
+    const int lane = threadIdx.x & 31, sub = lane & (LPP - 1);
+    const unsigned gmask = (LPP == 32) ? 0xffffffffu : (((1u << LPP) - 1u) << (lane & ~(LPP - 1)));
+    const int k = blockIdx.x * (DX_THREADS / LPP) + threadIdx.x / LPP;
+    if (k >= n_scan) return;  // the whole group
 
     const float4 kk = make_float4(P.stiffness[0], P.stiffness[1], P.stiffness[2], P.stiffness[3]);
     const float4 d0 = make_float4(P.dpos0[0], P.dpos0[1], P.dpos0[2], P.dpos0[3]);
@@ -196,15 +209,15 @@ relax_direct_kernel(int na, const float4* __restrict__ atoms, const float4* __re
         float4 fe = make_float4(0.f, 0.f, 0.f, 0.f);
         if (it < P.max_iter) {
             ++it;
-            fe = pair_sum<NS>(pos, na, s_pos, s_m, s_q, S.qz);
+            fe = group_pair_sum<NS, LPP>(pos, na, sub, gmask, s_pos, s_m, s_q, S.qz);
             const V3 ft = rotmatT(tip_force(rotmat(sub3(pos, tip), a, b, c), kk, d0), a, b, c);
             V3 f = mk3(fe.x + ft.x, fe.y + ft.y, fe.z + ft.z);
             f.x = fmaf(c.x, surf, f.x);
             f.y = fmaf(c.y, surf, f.y);
             f.z = fmaf(c.z, surf, f.z);
-            // convergence is tested before the update; an FP32 "converged" is confirmed in FP64
             if (dot3(f, f) < P.f2conv &&
-                force2_f64(pos, tip, na, atoms, cMs, S, a, b, c, kk, d0, surf) < (double)P.f2conv) {
+                group_force2_f64<LPP>(pos, tip, na, sub, gmask, atoms, cMs, S, a, b, c, kk, d0, surf) <
+                    (double)P.f2conv) {
                 done = conv = true;
             } else {
                 md_step(f, v, pos, I, true);
@@ -214,12 +227,14 @@ relax_direct_kernel(int na, const float4* __restrict__ atoms, const float4* __re
             done = true;  // max_iter == 0
         }
         if (done) {
-            if (!conv) fe = pair_sum<NS>(pos, na, s_pos, s_m, s_q, S.qz);  // position moved since the last sample
-            const V3 r = rotmat(mk3(fe.x, fe.y, fe.z), a, b, c);
-            fe_out[iz] = make_float4(r.x, r.y, r.z, fe.w);
-            const bool finite = isfinite(fe.x) && isfinite(fe.y) && isfinite(fe.z) && isfinite(fe.w) &&
-                                isfinite(pos.x) && isfinite(pos.y) && isfinite(pos.z);
-            pp_out[iz] = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
+            if (!conv) fe = group_pair_sum<NS, LPP>(pos, na, sub, gmask, s_pos, s_m, s_q, S.qz);  // moved since
+            if (sub == 0) {
+                const V3 r = rotmat(mk3(fe.x, fe.y, fe.z), a, b, c);
+                fe_out[iz] = make_float4(r.x, r.y, r.z, fe.w);
+                const bool finite = isfinite(fe.x) && isfinite(fe.y) && isfinite(fe.z) && isfinite(fe.w) &&
+                                    isfinite(pos.x) && isfinite(pos.y) && isfinite(pos.z);
+                pp_out[iz] = make_float4(pos.x, pos.y, pos.z, (float)((conv && finite) ? it : -it));
+            }
             tip = add3(tip, dTip);
             pos = add3(pos, dTip);
             v = mk3(0.f, 0.f, 0.f);
@@ -526,19 +541,29 @@ Sites make_sites(const float* Qs, const float* QZs, bool compact, int* ns) {
     return S;
 }
 
+// Lanes per pixel: about four atoms per lane, at least 4 and at most 32 lanes, more while the scan
+// leaves the GPU short of warps (fewer than ~8 warps per SM of a 148-SM part).
+int direct_lpp(int na, int n_scan) {
+    int lpp = 4;
+    while (lpp < 32 && lpp * 4 < na) lpp *= 2;
+    while (lpp < 32 && (long long)n_scan * lpp < 148LL * 8 * 32) lpp *= 2;
+    return lpp;
+}
+
 template <int NS>
 int launch_direct(int na, const float* atoms, const float* cMs, const float* points, int n_scan,
                   const spm_scan_params& P, const Sites& S, float* FEs, float* PPs, cudaStream_t st) {
     const size_t smem = (size_t)na * (2 * sizeof(float4) + NS * sizeof(float));
-    auto kern = relax_direct_kernel<NS>;
+    const int lpp = direct_lpp(na, n_scan);
+    auto kern = lpp == 4 ? relax_direct_kernel<NS, 4> : lpp == 8 ? relax_direct_kernel<NS, 8>
+              : lpp == 16 ? relax_direct_kernel<NS, 16> : relax_direct_kernel<NS, 32>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return set_error(SPM_ERR_CUDA, "spm_relax_direct_morse: smem %zu B: %s", smem,
                                                cudaGetErrorString(e));
     }
-    int blocks;
-    if (P.raster_ny > 0) blocks = ((n_scan / P.raster_ny + 7) / 8) * ((P.raster_ny + 15) / 16);
-    else blocks = (n_scan + DX_THREADS - 1) / DX_THREADS;
+    const int per_cta = DX_THREADS / lpp;
+    const int blocks = (n_scan + per_cta - 1) / per_cta;
     kern<<<blocks, DX_THREADS, smem, st>>>(na, reinterpret_cast<const float4*>(atoms),
                                            reinterpret_cast<const float4*>(cMs),
                                            reinterpret_cast<const float4*>(points), n_scan, P, S,
