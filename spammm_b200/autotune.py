@@ -206,7 +206,9 @@ def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
         batch.relax()
         batch.loss_seed()
         batch.adjoint_state()
-        pick("adjoint", ADJOINT_CANDIDATES, batch.adjoint_params)
+        # the state adjoint before each candidate: a launch shape with another scratch size starts without the
+        # maxima the state call leaves there
+        pick("adjoint", ADJOINT_CANDIDATES, batch.adjoint_params, prepare=batch.adjoint_state)
     batch.set_shape(shape)
     batch.set_relax_options(warm=warm)
     return shape, report

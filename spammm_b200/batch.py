@@ -292,6 +292,7 @@ class AFMBatch:
                                         dtype=F64, device=self.dev)
         self._adj_bytes = int(lib().spm_batch_adjoint_scratch_bytes(self.plan.totals, self.n))
         self.adj_scratch = None  # allocated by the first adjoint (it holds the adjoint grid: 32 B per slab node)
+        self._state_maxima = False  # a new scratch holds no maxima until the next adjoint_state
         return self
 
     def desc(self, i):

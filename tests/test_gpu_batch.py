@@ -487,6 +487,24 @@ def test_batch_adjoint_bulk_staged_node_blocks(cuda):
     torch.testing.assert_close(out[1], out[0], rtol=1e-6, atol=1e-6 * scale)
 
 
+def test_batch_shape_change_drops_the_state_maxima(cuda):
+    """A launch shape whose adjoint scratch differs (adj_chunk) reallocates the scratch: the next params
+    call must compute the ubar maxima itself, not take the new buffer's content for them."""
+    items = _items(0, n=4, seed=69)
+    b = AFMBatch(items)
+    _target(b)
+    b.forward_adjoint()
+    torch.cuda.synchronize()
+    g1 = b.grad.clone()
+    shape = _lib.BatchShape(*b.shape.key())
+    shape.adj_chunk = 4096 if shape.adj_chunk != 4096 else 65536
+    b.set_shape(shape)
+    b.build_grids()
+    b.adjoint_params()  # same states, ubar unchanged; the scratch is new
+    torch.cuda.synchronize()
+    torch.testing.assert_close(b.grad, g1, rtol=1e-6, atol=1e-6 * float(g1.abs().max()))
+
+
 def test_batch_adjoint_aggregated_scatter_is_bit_identical(cuda):
     """adj_agg = 1 (the scatter merges each CTA's corner sums in shared memory first) and 2 (a warp walks a
     pixel tile down its strokes and merges its lanes' shared nodes): the same exact integer sums, so the
