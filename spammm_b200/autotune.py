@@ -152,8 +152,10 @@ def tune(batch, reps=2, adjoint=True, log=None, max_grid_bytes=None):
         # two-pass (rx_sync = 2) schedule; the best shape per slab layout is kept for the layout choice below
         batch.set_relax_options(warm=True)
         tried = []
-        for ms_cold, kw in report["relax"]["all"][:3] + [r for r in report["relax"]["all"][3:]
-                                                         if r[1]["grid_layout"] != report["relax"]["best"]["grid_layout"]][:1]:
+        first = {}  # the fastest cold shape of each (register variant, slab layout): the warm step weighs
+        for ms_cold, kw in report["relax"]["all"]:  # the Newton evaluations, not FIRE, so its order differs
+            first.setdefault((kw["rx_regs"], kw["grid_layout"]), (ms_cold, kw))
+        for ms_cold, kw in first.values():
             for sync in (1, 2):
                 k2 = dict(kw, rx_sync=sync)
                 batch.set_shape(_with(shape, **k2))
