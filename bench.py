@@ -738,6 +738,8 @@ def run_batched(args, dev_index):
     from spammm_b200 import _lib
     from spammm_b200.batch import BatchPlan
     plan = BatchPlan(items)
+    if tune_rep is not None:  # a cold unpolished relaxation: the tuner's fastest cold shape, not the fit's warm one
+        shape = autotune._with(shape, **tune_rep["relax"]["best"])
     need = (4 if shape.grid_layout else 2) * plan.grid_float4 * 16 + plan.total_states * 36
     layout_note = None
     if shape.grid_layout and need > 0.85 * torch.cuda.mem_get_info()[0]:
