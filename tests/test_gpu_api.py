@@ -143,6 +143,43 @@ def test_direct_toy_matches_reference_golden(cuda, golden):
     assert np.abs(PPs.reshape(-1, 5, 4)[..., :3] - ref_PP[..., :3]).max() < 2e-3
 
 
+@pytest.mark.parametrize("na,nxy", [(10, (100, 100)), (30, (80, 80)), (60, (60, 60)), (60, (20, 20))])
+def test_direct_lane_groups(cuda, na, nxy):
+    """The direct relaxation's lane groups (4, 8, 16 and 32 lanes per pixel for these atom counts and
+    scan sizes): every state converged with an FP64 residual below the reference's 1e-4 eV/A gate, the
+    same convergence branch as the FP32 oracle run with the kernel's loop semantics, and PPs within
+    2e-3 A of it (the lanes' partial sums round differently from the oracle's one loop)."""
+    from spammm_b200 import synthetic
+    pos, Z, q = synthetic.planar_molecule({"C": max(1, na - na // 4), "H": na // 4}, 900 + na)
+    atoms, cMs = synthetic._morse_atoms_from_Z(pos, Z)
+    atoms[:, 3] = q.astype(np.float32)
+    afm = AFMulator(use_morse=True)
+    afm.atoms_arr, afm.cLJs_arr = atoms.astype(np.float32), cMs.astype(np.float32)
+    nz, dtip = 6, -0.1
+    span = np.abs(pos[:, :2]).max() + 1.0
+    p0 = np.array([-span, -span, 6.0 + 4.0], np.float32)  # the probe from 6 A above the plane
+    da = np.array([2 * span / (nxy[0] - 1), 0, 0], np.float32)
+    db = np.array([0, 2 * span / (nxy[1] - 1), 0], np.float32)
+    FEs, pts, PPs = afm.run_scan_morse_direct(nxy=nxy, nz=nz, dtip=dtip, scan_p0=p0, scan_da=da, scan_db=db)
+    assert (PPs[..., 3] > 0).all()
+    n = nxy[0] * nxy[1]
+    ref_FE, ref_PP = O.relax_direct(atoms, cMs, np.c_[pts.reshape(-1, 3), np.zeros(n)].astype(np.float32), nz,
+                                    afm.tipA, afm.tipB, afm.tipC.copy() * np.array([1, 1, 1, 0], np.float32) +
+                                    np.array([0, 0, 0, dtip], np.float32), afm.stiffness, afm.dpos0,
+                                    afm.relax_pars, afm.surfFF, afm.tipQs, afm.tipQZs)
+    tip = pts.reshape(-1, 3).astype(np.float64)
+    PPf = PPs.reshape(-1, nz, 4)
+    for iz in range(nz):
+        qz = PPf[:, iz, :3].astype(np.float64)
+        fe = O.pair_fe(1, atoms.astype(np.float64), cMs.astype(np.float64), qz, afm.tipQs, afm.tipQZs)
+        dpos = qz - (tip + iz * np.array([0, 0, dtip]))
+        rn = np.linalg.norm(dpos, axis=1)
+        ft = (dpos - afm.dpos0[:3]) * afm.stiffness[:3] + dpos * (afm.stiffness[3] * (rn - afm.dpos0[3]) / rn)[:, None]
+        assert np.linalg.norm(fe[:, :3] + ft, axis=1).max() < 1e-4, iz
+    assert np.array_equal(np.sign(PPf[..., 3]), np.sign(ref_PP[..., 3]))
+    assert np.abs(PPf[..., :3] - ref_PP[..., :3]).max() < 2e-3
+
+
 def test_direct_contract_errors(cuda):
     afm, atoms, cMs = _toy_afm(129, 129)
     p0, da, db = _toy_scan(atoms, (2, 2))
