@@ -167,12 +167,13 @@ def test_direct_lane_groups(cuda, na, nxy):
                                     afm.tipA, afm.tipB, afm.tipC.copy() * np.array([1, 1, 1, 0], np.float32) +
                                     np.array([0, 0, 0, dtip], np.float32), afm.stiffness, afm.dpos0,
                                     afm.relax_pars, afm.surfFF, afm.tipQs, afm.tipQZs)
-    tip = pts.reshape(-1, 3).astype(np.float64)
     PPf = PPs.reshape(-1, nz, 4)
+    tip = pts.reshape(-1, 3).astype(np.float32)  # stepped down in float32 as the kernel does
     for iz in range(nz):
         qz = PPf[:, iz, :3].astype(np.float64)
         fe = O.pair_fe(1, atoms.astype(np.float64), cMs.astype(np.float64), qz, afm.tipQs, afm.tipQZs)
-        dpos = qz - (tip + iz * np.array([0, 0, dtip]))
+        dpos = qz - tip.astype(np.float64)
+        tip[:, 2] = tip[:, 2] + np.float32(dtip)
         rn = np.linalg.norm(dpos, axis=1)
         ft = (dpos - afm.dpos0[:3]) * afm.stiffness[:3] + dpos * (afm.stiffness[3] * (rn - afm.dpos0[3]) / rn)[:, None]
         assert np.linalg.norm(fe[:, :3] + ft, axis=1).max() < 1e-4, iz
