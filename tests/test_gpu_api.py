@@ -147,8 +147,8 @@ def test_direct_toy_matches_reference_golden(cuda, golden):
 def test_direct_lane_groups(cuda, na, nxy):
     """The direct relaxation's lane groups (4, 8, 16 and 32 lanes per pixel for these atom counts and
     scan sizes): every state converged with an FP64 residual below the reference's 1e-4 eV/A gate, the
-    same convergence branch as the FP32 oracle run with the kernel's loop semantics, and PPs within
-    2e-3 A of it (the lanes' partial sums round differently from the oracle's one loop)."""
+    same convergence branch as the FP64 oracle run with the kernel's loop semantics, and PPs within the
+    stopping slack of it (the lanes' partial sums round differently from the oracle's one loop)."""
     from spammm_b200 import synthetic
     pos, Z, q = synthetic.planar_molecule({"C": max(1, na - na // 4), "H": na // 4}, 900 + na)
     atoms, cMs = synthetic._morse_atoms_from_Z(pos, Z)
@@ -178,7 +178,10 @@ def test_direct_lane_groups(cuda, na, nxy):
         ft = (dpos - afm.dpos0[:3]) * afm.stiffness[:3] + dpos * (afm.stiffness[3] * (rn - afm.dpos0[3]) / rn)[:, None]
         assert np.linalg.norm(fe[:, :3] + ft, axis=1).max() < 1e-4, iz
     assert np.array_equal(np.sign(PPf[..., 3]), np.sign(ref_PP[..., 3]))
-    assert np.abs(PPf[..., :3] - ref_PP[..., :3]).max() < 2e-3
+    # both stop at |F| < 1e-4 eV/A: along the softest spring mode (k = 0.03 eV/A^2) two converged states
+    # may differ by up to 2 * 1e-4 / 0.03 = 6.7e-3 A; almost all agree to ~1e-6 A
+    dq = np.abs(PPf[..., :3] - ref_PP[..., :3]).max(axis=-1)
+    assert dq.max() < 6.7e-3 and np.quantile(dq, 0.999) < 2e-3
 
 
 def test_direct_contract_errors(cuda):
