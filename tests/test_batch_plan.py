@@ -146,3 +146,37 @@ def test_partial_raster_falls_back_to_1d():
     assert plan.mols[0].raster_ny == 0
     assert plan.mols[1].slot_off == -(-plan.mols[0].n_scan // 32) * 32  # a warp's 32 slots stay in one molecule
     assert tot[1] > 0
+
+
+def test_relax_workspace_sizes_and_shape_combinations():
+    """spm_batch_relax_workspace_bytes: the counters alone for the one-pass schedules, plus one 48-byte tail
+    entry per slot for the two-pass one; shape combinations the kernels do not have are refused."""
+    L = _lib.lib()
+    s = L.spm_batch_default_shape()
+    for sync, extra in ((0, 0), (1, 0), (2, 48)):
+        s.rx_sync = sync
+        assert L.spm_batch_relax_workspace_bytes(1000, ctypes.byref(s)) == 16 + extra * 1000
+    assert L.spm_batch_relax_workspace_bytes(-1, ctypes.byref(s)) < 0
+    totals = (ctypes.c_longlong * _lib.SPM_BATCH_TOTALS)()
+    plan = BatchPlan(small_items(3))
+    for kw, ok in ((dict(adj_stage=1, adj_ilp=1), True), (dict(adj_stage=1, adj_ilp=2), False),
+                   (dict(adj_agg=2), True), (dict(rx_sync=2, rx_regs=4), True)):
+        s = L.spm_batch_default_shape()
+        for k, v in kw.items():
+            setattr(s, k, v)
+        rc = L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(s), totals)
+        assert (rc == _lib.SPM_OK) == ok, kw
+
+
+def test_autotune_shape_text():
+    from spammm_b200 import autotune
+    base = _lib.lib().spm_batch_default_shape()
+    s = autotune._parse_shape("rx_regs=2,rx_tile_h=4,adj_stage=1", base)
+    assert (s.rx_regs, s.rx_tile_h, s.adj_stage) == (2, 4, 1)
+    assert s.gb_ty == base.gb_ty  # the other fields keep the base's values
+    with pytest.raises(ValueError, match="unknown"):
+        autotune._parse_shape("rx_bogus=1", base)
+    # every candidate list names real fields
+    for cands in (autotune.GRID_CANDIDATES, autotune.RELAX_CANDIDATES, autotune.ADJOINT_CANDIDATES):
+        for kw in cands:
+            assert all(hasattr(base, k) for k in kw), kw
