@@ -435,8 +435,9 @@ typedef struct spm_batch_shape {
                            method from the previous equilibria only, each stroke stopping at its first
                            z-step that needs FIRE, then those strokes' remaining z-steps, 32 strokes
                            per warp stepping together (without both flags: as 1).  Same results */
-    int adj_ilp;        /* adjoint node kernel: 1 = one node pair per step (3 CTAs per SM), 2 = two
-                           independent node pairs per step (2 CTAs per SM, more registers) */
+    int adj_ilp;        /* adjoint node kernel: 1 = one atom and one node pair per step (4 CTAs per SM),
+                           2 = two independent node pairs per step (2 CTAs per SM, more registers),
+                           3 = two atoms per thread sharing each node pair's loads (2 CTAs per SM) */
     int adj_agg;        /* adjoint scatter: 0 = every state's corner sums straight to the global adjoint
                            grid (64-bit atomics), 1 = first merged per CTA in a shared-memory table
                            (the strokes of one CTA share nodes), one global atomic per distinct node,

@@ -38,7 +38,7 @@ RELAX_CANDIDATES = [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=r, grid
                    [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=5, grid_layout=0) for h in (2, 4, 8, 16)] + \
                    [dict(rx_sync=0, rx_threads=128, rx_tile_h=8, rx_regs=0, grid_layout=0)]
 ADJOINT_CANDIDATES = [dict(adj_chunk=c, adj_ilp=i, adj_agg=a, adj_stage=0) for c in (4096, 16384, 65536)
-                      for i in (1, 2) for a in (0, 1)] + \
+                      for i in (1, 2, 3) for a in (0, 1)] + \
                      [dict(adj_chunk=c, adj_ilp=1, adj_agg=0, adj_stage=1) for c in (4096, 16384)]
 
 _CACHE = {}

@@ -1159,6 +1159,8 @@ constexpr size_t NM_SMEM = 7 * NM_BUF * sizeof(float) + 6 * NM_THREADS * sizeof(
 constexpr size_t NM_RAW = (size_t)NM_THREADS * 32;
 constexpr size_t NM_SMEM_BULK = (NM_SMEM + 15) / 16 * 16 + NM_RAW + 16;
 constexpr unsigned NM_SPIN = 1u << 22;  // bounded mbarrier polls before a block is read with plain loads
+// ILP = 3 (two atoms per thread): the second atom's FP64 sums after the first's
+constexpr size_t NM_SMEM_2ATOM = (NM_SMEM + 15) / 16 * 16 + 6 * NM_THREADS * sizeof(double);
 
 __device__ __forceinline__ bool nm_try_wait(unsigned bar, unsigned parity) {
     unsigned ok;
@@ -1188,13 +1190,14 @@ __device__ __forceinline__ bool nm_try_wait(unsigned bar, unsigned parity) {
 // per step at two CTAs per SM (up to 128 registers).  PAR: also the
 // pair-parameter columns 3-4 (else written as 0).
 template <int KIND, bool ON, bool PAR, int ILP, bool BULK = false>
-__global__ void __launch_bounds__(NM_THREADS, ILP == 2 ? 2 : 4)
+__global__ void __launch_bounds__(NM_THREADS, ILP == 1 ? 4 : 2)
 batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk,
                            const float4* __restrict__ atoms, const float* __restrict__ params, int pstride,
                            NodeSites S, unsigned long long* __restrict__ gq, const int* __restrict__ box,
                            const unsigned* __restrict__ umax, double* __restrict__ partial,
                            unsigned* __restrict__ status) {
     static_assert(!BULK || ILP == 1, "bulk-copy staging with one node pair per step");
+    constexpr int APT = ILP == 3 ? 2 : 1;  // atoms per thread
     extern __shared__ __align__(16) unsigned char nm_smem[];
     float(*s_n)[NM_BUF] = reinterpret_cast<float(*)[NM_BUF]>(nm_smem);
     double(*red)[NM_THREADS] = reinterpret_cast<double(*)[NM_THREADS]>(nm_smem + 7 * NM_BUF * sizeof(float));
@@ -1241,23 +1244,9 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
         const int ya = (int)(r0 - (unsigned)za * ny), yb = (int)(r1 - (unsigned)za * ny);
         return !(yb < ylo || ya > yhi);
     };
-    for (int a0 = 0, nag = 0; a0 < na; a0 += nag) {
-        // atom group: nag atoms x P phases <= 256 threads.  The remaining atoms go in one group when
-        // that keeps >= 85% of the threads busy, else a group of 256/P atoms with P = ceil(256/rem)
-        // and the rest after it (65 atoms: 64 at 4 phases + 1 at 256 instead of 65 at 3)
-        const int rem = na - a0;
-        if (rem >= NM_THREADS) {
-            nag = NM_THREADS;
-        } else if ((NM_THREADS / rem) * rem * 100 >= 85 * NM_THREADS) {
-            nag = rem;
-        } else {
-            nag = NM_THREADS / ((NM_THREADS + rem - 1) / rem);
-        }
-        const int P = NM_THREADS / nag;
-        const bool last_group = a0 + nag >= na;
-        const bool act = t < nag * P;
-        const int a = a0 + (act ? t % nag : 0), ph = act ? t / nag : 0;
-        const int ga = D->atom_off + a;
+    // ILP = 3: the second atom's FP64 sums (red2[c][t]), after the shared arrays
+    double(*red2)[NM_THREADS] = reinterpret_cast<double(*)[NM_THREADS]>(nm_smem + (NM_SMEM + 15) / 16 * 16);
+    auto atom_consts = [&](int ga) {
         const float4 at = __ldg(atoms + ga);
         const float* pr = params + (size_t)ga * pstride;
         const float p1 = __ldg(pr + 0), p2 = __ldg(pr + 1), p3 = (pstride > 2) ? __ldg(pr + 2) : 0.f;
@@ -1281,10 +1270,47 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
             C.c3 = bc(2.f * p3 * p3 * p2);
             C.c4 = bc(-2.f * p3);
         }
+        return C;
+    };
+    for (int a0 = 0, nag = 0; a0 < na; a0 += nag) {
+        // atom group: nslot thread slots x P phases <= 256 threads, APT atoms per slot (slot s takes atoms
+        // a0 + s and a0 + nslot + s).  The remaining atoms go in one group when that keeps >= 85% of the
+        // threads busy, else a group of 256/P slots with P = ceil(256/slots needed) and the rest after it
+        // (65 atoms, one per thread: 64 at 4 phases + 1 at 256 instead of 65 at 3)
+        const int rem = na - a0;
+        int nslot;
+        if (rem >= APT * NM_THREADS) {
+            nslot = NM_THREADS;
+        } else {
+            const int rs = (rem + APT - 1) / APT;
+            nslot = (NM_THREADS / rs) * rs * 100 >= 85 * NM_THREADS ? rs : NM_THREADS / ((NM_THREADS + rs - 1) / rs);
+        }
+        nag = min(rem, APT * nslot);
+        const int P = NM_THREADS / nslot;
+        const bool last_group = a0 + nag >= na;
+        const bool act = t < nslot * P;
+        const int a = a0 + (act ? t % nslot : 0), ph = act ? t / nslot : 0;
+        const AtomC C = atom_consts(D->atom_off + a);
+        // ILP = 3: the slot's second atom, or an inert one (zero constants; its sums are not written)
+        const bool has_b = APT == 2 && act && (t % nslot) + nslot < nag;
+        AtomC CB;
+        if (APT == 2) {
+            if (has_b) {
+                CB = atom_consts(D->atom_off + a + nslot);
+            } else {
+                const f2 z = bc(0.f);
+                CB.x = z; CB.y = z; CB.z = z; CB.c0 = z; CB.c1 = z; CB.c2 = z; CB.c3 = z; CB.c4 = z;
+                CB.qw = z; CB.qw3 = z; CB.q = 0.f;
+            }
+        }
         // the atom's FP64 sums, in shared memory (red[c][t]) to keep registers for the pair loop
         double* acc = &red[0][t];
+        double* acc2 = &red2[0][t];
 #pragma unroll
-        for (int c = 0; c < 6; c++) acc[c * NM_THREADS] = 0.0;
+        for (int c = 0; c < 6; c++) {
+            acc[c * NM_THREADS] = 0.0;
+            if (APT == 2) acc2[c * NM_THREADS] = 0.0;
+        }
         // the staged nodes' derivative sums: FP32 over NM_FLUSH pairs, then FP64
         auto compute = [&](int L) {
             if (t == 0 && (L & 1)) {  // pad to whole pairs: a distant node of zero weight adds +-0
@@ -1305,7 +1331,24 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
                                              lds2(&s_n[4][j]), lds2(&s_n[5][j]), lds2(&s_n[6][j]), C, S, sums);
                 };
                 int jp = ph;
-                if (ILP == 2) {
+                if (ILP == 3) {
+                    // each staged node pair loaded once for the slot's two atoms
+                    f2 b32[6] = {zero, zero, zero, zero, zero, zero};
+                    for (; jp < Lp; jp += P) {
+                        const int j = 2 * jp;
+                        const f2 nx = lds2(&s_n[0][j]), ny = lds2(&s_n[1][j]), nz = lds2(&s_n[2][j]);
+                        const f2 gx = lds2(&s_n[3][j]), gy = lds2(&s_n[4][j]), gz = lds2(&s_n[5][j]);
+                        const f2 gw = lds2(&s_n[6][j]);
+                        pair_adj2<KIND, ON, PAR>(nx, ny, nz, gx, gy, gz, gw, C, S, a32);
+                        pair_adj2<KIND, ON, PAR>(nx, ny, nz, gx, gy, gz, gw, CB, S, b32);
+                        if (++n32 == NM_FLUSH / 2) {
+                            fold_sums<PAR>(a32, acc, NM_THREADS);
+                            fold_sums<PAR>(b32, acc2, NM_THREADS);
+                            n32 = 0;
+                        }
+                    }
+                    fold_sums<PAR>(b32, acc2, NM_THREADS);
+                } else if (ILP == 2) {
                     // two independent node pairs per step, each into its own FP32 sums
                     f2 b32[6] = {zero, zero, zero, zero, zero, zero};
                     for (; jp + P < Lp; jp += 2 * P) {
@@ -1500,16 +1543,31 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
             if (!more) break;
         }
 #pragma unroll
-        for (int c = 0; c < 6; c++) red[c][t] = act ? red[c][t] : 0.0;
-        if (KIND == SPM_KIND_LJ && PAR) red[3][t] = -red[3][t];  // accumulated negated
+        for (int c = 0; c < 6; c++) {
+            red[c][t] = act ? red[c][t] : 0.0;
+            if (APT == 2) red2[c][t] = act ? red2[c][t] : 0.0;
+        }
+        if (KIND == SPM_KIND_LJ && PAR) {  // accumulated negated
+            red[3][t] = -red[3][t];
+            if (APT == 2) red2[3][t] = -red2[3][t];
+        }
         __syncthreads();
-        if (t < nag) {
+        if (t < nslot) {
             double* out = partial + ((size_t)D->row_off + (size_t)lc * na + a0 + t) * 6;
 #pragma unroll
             for (int c = 0; c < 6; c++) {
                 double s6 = 0.0;
-                for (int q = 0; q < P; q++) s6 += red[c][t + q * nag];
+                for (int q = 0; q < P; q++) s6 += red[c][t + q * nslot];
                 out[c] = s6;
+            }
+            if (APT == 2 && t + nslot < nag) {
+                double* out2 = partial + ((size_t)D->row_off + (size_t)lc * na + a0 + nslot + t) * 6;
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    double s6 = 0.0;
+                    for (int q = 0; q < P; q++) s6 += red2[c][t + q * nslot];
+                    out2[c] = s6;
+                }
             }
         }
         __syncthreads();
@@ -1557,6 +1615,7 @@ NodeKern node_kernel(int kind, bool on) {
 // loads or fetched by bulk copies (stage = 1, with one node pair per step).
 NodeKern node_kernel(int kind, bool on, bool par, int ilp, int stage) {
     if (stage == 1) return par ? node_kernel<true, 1, true>(kind, on) : node_kernel<false, 1, true>(kind, on);
+    if (ilp == 3) return par ? node_kernel<true, 3, false>(kind, on) : node_kernel<false, 3, false>(kind, on);
     if (ilp == 2) return par ? node_kernel<true, 2, false>(kind, on) : node_kernel<false, 2, false>(kind, on);
     return par ? node_kernel<true, 1, false>(kind, on) : node_kernel<false, 1, false>(kind, on);
 }
@@ -1646,7 +1705,7 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
     const int chunk = shape->adj_chunk;
     SPM_REQUIRE(chunk >= 1024 && chunk <= (1 << 20) && chunk % 1024 == 0, "spm_batch_adjoint_params: adj_chunk=%d",
                 chunk);
-    SPM_REQUIRE(shape->adj_ilp == 1 || shape->adj_ilp == 2, "spm_batch_adjoint_params: adj_ilp=%d", shape->adj_ilp);
+    SPM_REQUIRE(shape->adj_ilp >= 1 && shape->adj_ilp <= 3, "spm_batch_adjoint_params: adj_ilp=%d", shape->adj_ilp);
     SPM_REQUIRE(shape->adj_agg >= 0 && shape->adj_agg <= 2, "spm_batch_adjoint_params: adj_agg=%d", shape->adj_agg);
     SPM_REQUIRE(totals[1] >= 0 && totals[1] < (1LL << 31), "spm_batch_adjoint_params: slots=%lld", totals[1]);
     SPM_REQUIRE(shape->adj_stage == 0 || (shape->adj_stage == 1 && shape->adj_ilp == 1),
@@ -1674,12 +1733,12 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             if (cudaGetDevice(&dev) != cudaSuccess)
                 return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: no current device");
             if (dev < 0 || dev >= 64 || !smem_set[dev]) {
-                for (int v = 0; v < 24; v++) {
-                    const int stage = v >= 16 ? 1 : 0;
+                for (int v = 0; v < 32; v++) {
+                    const int stage = (v >> 3) == 2 ? 1 : 0, ilp = (v >> 3) == 1 ? 2 : (v >> 3) == 3 ? 3 : 1;
                     const auto k = node_kernel(v & 1 ? SPM_KIND_MORSE : SPM_KIND_LJ, (v & 2) != 0, (v & 4) != 0,
-                                               v & 8 ? 2 : 1, stage);
-                    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(stage ? NM_SMEM_BULK : NM_SMEM)) != cudaSuccess)
+                                               ilp, stage);
+                    const size_t bytes = stage ? NM_SMEM_BULK : ilp == 3 ? NM_SMEM_2ATOM : NM_SMEM;
+                    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
                         return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: cannot set shared memory size");
                 }
                 if (dev >= 0 && dev < 64) smem_set[dev] = true;
@@ -1730,7 +1789,8 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
                                           shape->adj_stage);
             // status: the second word of the marker slot (bit 0: a bulk copy's wait ran out)
             unsigned* status = reinterpret_cast<unsigned*>(mark + 1);
-            kern<<<(unsigned)n_units, NM_THREADS, shape->adj_stage ? NM_SMEM_BULK : NM_SMEM, st>>>(
+            const size_t nm_bytes = shape->adj_stage ? NM_SMEM_BULK : shape->adj_ilp == 3 ? NM_SMEM_2ATOM : NM_SMEM;
+            kern<<<(unsigned)n_units, NM_THREADS, nm_bytes, st>>>(
                 n_mol, mols, chunk, reinterpret_cast<const float4*>(atoms), params, pstride, S, gq, box, umax, part,
                 status);
             nodes_ran = true;

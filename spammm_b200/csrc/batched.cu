@@ -48,7 +48,7 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
     SPM_REQUIRE(S.rx_regs >= 0 && S.rx_regs <= 5, "spm_batch_prepare: rx_regs=%d", S.rx_regs);
     SPM_REQUIRE(S.grid_layout == 0 || S.grid_layout == 1, "spm_batch_prepare: grid_layout=%d", S.grid_layout);
     SPM_REQUIRE(S.rx_sync >= 0 && S.rx_sync <= 2, "spm_batch_prepare: rx_sync=%d", S.rx_sync);
-    SPM_REQUIRE(S.adj_ilp == 1 || S.adj_ilp == 2, "spm_batch_prepare: adj_ilp=%d", S.adj_ilp);
+    SPM_REQUIRE(S.adj_ilp >= 1 && S.adj_ilp <= 3, "spm_batch_prepare: adj_ilp=%d", S.adj_ilp);
     SPM_REQUIRE(S.adj_agg >= 0 && S.adj_agg <= 2, "spm_batch_prepare: adj_agg=%d", S.adj_agg);
     SPM_REQUIRE(S.adj_stage == 0 || (S.adj_stage == 1 && S.adj_ilp == 1), "spm_batch_prepare: adj_stage=%d",
                 S.adj_stage);

@@ -131,7 +131,7 @@ def test_prepare_rejects_bad_descriptors():
     assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(shape), totals) == _lib.SPM_ERR_ARG
     plan = BatchPlan(small_items(4))
     for field, bad in (("gb_ty", 3), ("gb_zb", 4), ("rx_threads", 96), ("rx_tile_h", 6), ("adj_chunk", 1000), ("rx_regs", 6), ("grid_layout", 2),
-                       ("rx_sync", 3), ("adj_ilp", 3), ("adj_stage", 2), ("adj_agg", 3)):
+                       ("rx_sync", 3), ("adj_ilp", 4), ("adj_stage", 2), ("adj_agg", 3)):
         s = L.spm_batch_default_shape()
         setattr(s, field, bad)
         assert L.spm_batch_prepare(plan.mols, plan.n, ctypes.byref(s), totals) == _lib.SPM_ERR_ARG, field

@@ -132,6 +132,7 @@ def test_batch_shapes_give_same_results(cuda):
                dict(rx_sync=1, rx_regs=0), dict(rx_sync=1, rx_tile_h=1, rx_threads=64, rx_regs=2),
                dict(rx_sync=1, rx_tile_h=32, rx_regs=1, grid_layout=1), dict(rx_regs=3, rx_tile_h=2),
                dict(rx_sync=0, rx_regs=3, grid_layout=1), dict(adj_ilp=2), dict(adj_ilp=2, adj_chunk=4096), dict(rx_sync=2),
+               dict(adj_ilp=3), dict(adj_ilp=3, adj_chunk=4096),
                dict(rx_regs=3), dict(rx_regs=4, grid_layout=1), dict(rx_sync=0, rx_regs=4, rx_tile_h=4)):
         s = L.spm_batch_default_shape()
         for k, v in kw.items():
