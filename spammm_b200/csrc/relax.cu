@@ -1107,12 +1107,17 @@ batch_relax_tail_kernel(const spm_batch_mol* __restrict__ mols, const float* __r
     const unsigned lane = threadIdx.x & 31u;
     const TailEntry* tail = reinterpret_cast<const TailEntry*>(reinterpret_cast<const char*>(ws) + TAIL_OFF);
     const unsigned n_tail = ws[2];  // written by the prefix pass, which ran before this launch
+    // entries per draw: 32 while the list fills every launched warp; a shorter list is spread over
+    // all of them (a warp's time is the sum over its rounds of its slowest lane's FIRE steps, so
+    // strokes sharing a warp wait for one another while whole warps would sit idle)
+    const unsigned warps = gridDim.x * (blockDim.x >> 5);
+    const unsigned per = min(32u, max(1u, (n_tail + warps - 1u) / warps));
     while (true) {
         unsigned base = 0;
-        if (lane == 0) base = atomicAdd(ws + 3, 32u);
+        if (lane == 0) base = atomicAdd(ws + 3, per);
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= n_tail) return;  // warp-uniform
-        const bool valid = base + lane < n_tail;
+        const bool valid = lane < per && base + lane < n_tail;
         const unsigned members = __ballot_sync(0xffffffffu, valid);
         if (valid) {
             const TailEntry e = tail[base + lane];
@@ -1520,7 +1525,7 @@ extern "C" int spm_batch_relax(int n_mol, const spm_batch_mol* mols, long long n
     if (two_pass) {
         int rc = check_launch("spm_batch_relax (prefix pass)");
         if (rc) return rc;
-        // the tail list is drawn 32 entries per warp until the count the prefix pass left is used up
+        // the tail list is drawn up to 32 entries per warp until the count the prefix pass left is used up
         const TailKern tk = tails[shape->grid_layout][shape->rx_regs];
         int per_sm_t = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, tk, thr, 0) != cudaSuccess)

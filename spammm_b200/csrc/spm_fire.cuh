@@ -384,6 +384,7 @@ __device__ __forceinline__ float4 interp_fe_cached(const AxisView& G, V3 p, Texe
 // |dq|_inf <= POLISH_MAX_STEP and it lowers |G|^2.  The oracle (ora_core.h, newton_polish)
 // repeats every operation in the same order, so results are bit-identical to it.
 constexpr int POLISH_STEPS = 4;
+constexpr float NEWTON_FLOOR_STEP = 1e-5f;  // A; the early stop of the warm starts' Newton-first
 constexpr float POLISH_MAX_STEP = 0.1f;
 
 // Spring and frame of a polished state: frame = false is relaxStrokes' spring (tip_force on
@@ -514,9 +515,14 @@ __device__ __forceinline__ bool polish_step(const float (&J)[3][3], V3 Gv, V3& d
 // not available (outside the sampler's range or the stored slab).  On return q is the polished
 // position, fe the sample there, g2 = |G(q)|^2 and evals the cells evaluated; false (q and fe
 // unchanged) when the first fetch fails.
-// early (the warm starts' Newton-first, not the polish): also stop after a kept step that lowered
-// |G|^2 by less than 4x -- quadratic convergence has ended, |G| is at the float32 floor, and the
-// next step would most likely be refused.
+// early (the warm starts' Newton-first, not the polish): also stop
+//  - before a step whose every component is at most NEWTON_FLOOR_STEP: the predicted distance to
+//    the root is at the float32 floor of the positions' noise (the spread of polished equilibria
+//    reached from different starts is ~1e-6 A), so the step would change nothing measurable and
+//    its cell evaluation is saved -- the previous equilibrium of an unmoved state is kept after one
+//    evaluation, a state that moved ~1e-3 A after one step;
+//  - after a kept step that lowered |G|^2 by less than 4x -- quadratic convergence has ended, |G|
+//    is at the float32 floor, and the next step would most likely be refused.
 template <class Fetch>
 __device__ __forceinline__ bool newton_core(const Fetch& fetch, const float (&T)[3][3], const PolishSpring& S,
                                             V3 tip, V3& q, float4& fe, float& g2_out, int& evals,
@@ -534,6 +540,9 @@ __device__ __forceinline__ bool newton_core(const Fetch& fetch, const float (&T)
     for (int it = 0; it < POLISH_STEPS; it++) {
         V3 dq;
         if (!polish_step(J, Gv, dq)) break;
+        if (early && fabsf(dq.x) <= NEWTON_FLOOR_STEP && fabsf(dq.y) <= NEWTON_FLOOR_STEP &&
+            fabsf(dq.z) <= NEWTON_FLOOR_STEP)
+            break;
         const V3 q1 = add3(q, dq);
         if (!fetch(q1, ax, ay, az, t)) break;
         float J1[3][3];
