@@ -17,9 +17,10 @@ include/spm_b200.h):
 
 Per molecule the results are those of the per-molecule calls (grid_build ->
 relax_pp -> adjoint on the same GridScanSpec): forward values bit for bit.
-Only the nodes the probe can reach -- the scan window's columns and rows and
-the tip's z-range, each widened by ``slab_margin`` on both sides -- are built
-and stored; a probe that leaves them is reported as not converged instead of
+Only the nodes the probe can reach -- the scan window's columns and rows
+widened by ``slab_margin`` on both sides, the tip's z-range by
+``slab_margin_z`` (the spring's vertical give, ``z_margin``) -- are built and
+stored; a probe that leaves them is reported as not converged instead of
 sampling the missing nodes.
 
 Molecules are laid out in descending order of relaxation work (longest
@@ -115,6 +116,25 @@ def lateral_range(item, probe, margin, axis):
     return lo, hi - lo
 
 
+# The probe's vertical offset from its tip is F_z / k_z on a Cartesian spring: slab layers are built
+# for |F_z| up to 1 nN (0.624 eV/A) -- 0.5 A at the default k_z of 20 N/m, where the batch
+# distributions' states stay within 0.06 A of the tip's z -- and at most the lateral margin.
+Z_FORCE_BOUND = 0.624
+Z_MARGIN_MIN = 0.3
+
+
+def z_margin(probe, margin):
+    """Default margin (A) of the stored layers beyond the tip's z-range:
+    Z_FORCE_BOUND / k_z, between Z_MARGIN_MIN and `margin` (the lateral
+    one); `margin` itself for a radial spring (stiffness[3] != 0) or a
+    probe without a restoring k_z."""
+    k = np.asarray(probe.stiffness, np.float64)
+    kz = -float(k[2])
+    if float(k[3]) != 0.0 or not kz > 0.0:
+        return float(margin)
+    return min(float(margin), max(Z_MARGIN_MIN, Z_FORCE_BOUND / kz))
+
+
 def slab_range(item, probe, dtip, margin):
     """Stored layers [z_lo, z_lo + nz_slab) of the item's grid: every layer a
     trilinear sample can touch while the probe stays within `margin` A of the
@@ -137,7 +157,7 @@ class BatchPlan:
     """Host side of a batch: descriptors in work order and the concatenated
     atom / parameter / point arrays (no device memory; see AFMBatch)."""
 
-    def __init__(self, items, kind=0, probe=None, dtip=-0.1, slab_margin=1.5, order="lpt"):
+    def __init__(self, items, kind=0, probe=None, dtip=-0.1, slab_margin=1.5, order="lpt", slab_margin_z=None):
         if not items:
             raise ValueError("a batch needs at least one molecule")
         if dtip >= 0:
@@ -153,6 +173,8 @@ class BatchPlan:
         self.pos = np.empty(n, np.int64)
         self.pos[self.order] = np.arange(n)
         pcols = 2 if self.kind == _lib.SPM_KIND_LJ else 4
+        self.slab_margin = float(slab_margin)
+        self.slab_margin_z = z_margin(self.probe, slab_margin) if slab_margin_z is None else float(slab_margin_z)
         self.mols = (BatchMol * n)()
         atoms_l, params_l, pts_l = [], [], []
         ao = po = so = go = 0
@@ -166,7 +188,7 @@ class BatchPlan:
             p0, dA, dB, dC = spec.vectors()
             dinv = spec.dinv()
             nx, ny, nzg = (int(v) for v in it.ngrid)
-            z_lo, nzs = slab_range(it, self.probe, self.dtip, slab_margin)
+            z_lo, nzs = slab_range(it, self.probe, self.dtip, self.slab_margin_z)
             x_lo, nxs = lateral_range(it, self.probe, slab_margin, 0)
             y_lo, nys = lateral_range(it, self.probe, slab_margin, 1)
             D = self.mols[j]
@@ -213,13 +235,15 @@ class AFMBatch:
 
     items: list of BatchItem; kind: 0 LJ / 1 Morse (one kind per batch);
     probe: ProbeSpec; dtip: z-step (< 0: approach); slab_margin: A beyond the
-    scan window (x, y) and the tip's z-range whose nodes are built; shape:
-    BatchShape (None = library default; ``spammm_b200.autotune`` searches
-    better ones)."""
+    scan window (x, y) whose nodes are built; slab_margin_z: A beyond the
+    tip's z-range (None: ``z_margin(probe, slab_margin)``, 0.5 A for the
+    default probe); shape: BatchShape (None = library default;
+    ``spammm_b200.autotune`` searches better ones)."""
 
-    def __init__(self, items, kind=0, probe=None, dtip=-0.1, slab_margin=1.5, shape=None, order="lpt"):
+    def __init__(self, items, kind=0, probe=None, dtip=-0.1, slab_margin=1.5, shape=None, order="lpt",
+                 slab_margin_z=None):
         _lib.require_cuda()
-        plan = BatchPlan(items, kind, probe, dtip, slab_margin, order)
+        plan = BatchPlan(items, kind, probe, dtip, slab_margin, order, slab_margin_z)
         self.plan = plan
         self.dev = torch.device("cuda", torch.cuda.current_device())
         self.kind, self.probe, self.dtip, self.items, self.n = plan.kind, plan.probe, plan.dtip, plan.items, plan.n

@@ -78,6 +78,32 @@ def test_slab_covers_probe_range():
     assert slab_range(it, probe, -0.1, 1.5) == (0, it.ngrid[2])
 
 
+def test_z_margin_follows_the_spring():
+    """The stored layers' margin beyond the tip's z-range: 1 nN over k_z (0.5 A at 20 N/m), between 0.3 A and
+    the lateral margin; the lateral margin itself for a radial spring or no restoring k_z.  A plan's slabs
+    use it unless slab_margin_z is given."""
+    import dataclasses
+    from spammm_b200.batch import z_margin
+    probe = ProbeSpec()
+    assert abs(z_margin(probe, 1.5) - 0.5) < 1e-3
+    assert z_margin(probe, 0.4) == 0.4
+    soft = dataclasses.replace(probe, stiffness=probe.stiffness * np.float32(0.01))
+    assert z_margin(soft, 1.5) == 1.5
+    stiff = dataclasses.replace(probe, stiffness=probe.stiffness * np.float32(100.0))
+    assert z_margin(stiff, 1.5) == 0.3
+    radial = dataclasses.replace(probe, stiffness=np.array([*probe.stiffness[:3], -0.5], np.float32))
+    assert z_margin(radial, 1.5) == 1.5
+    items = small_items(5, seed=8)
+    tight, wide = BatchPlan(items), BatchPlan(items, slab_margin_z=1.5)
+    assert tight.slab_margin_z == z_margin(probe, 1.5) and wide.slab_margin_z == 1.5
+    for i, it in enumerate(items):
+        Dt, Dw = tight.desc(i), wide.desc(i)
+        assert (Dt.z_lo, Dt.nz_slab) == slab_range(it, probe, -0.1, tight.slab_margin_z)
+        assert (Dt.x_lo, Dt.nx_slab, Dt.y_lo, Dt.ny_slab) == (Dw.x_lo, Dw.nx_slab, Dw.y_lo, Dw.ny_slab)
+        assert Dw.z_lo <= Dt.z_lo and Dt.z_lo + Dt.nz_slab <= Dw.z_lo + Dw.nz_slab
+    assert tight.grid_float4 < wide.grid_float4
+
+
 def test_lateral_range_covers_scan_window():
     """Stored columns and rows hold every texel a sample within the margin of
     the scan window needs; a window whose margin reaches the grid edge keeps

@@ -528,3 +528,24 @@ def test_batch_adjoint_aggregated_scatter_is_bit_identical(cuda):
         out.append((g1, b.dk_sum.clone()))
     for g, dks in out[1:]:
         assert torch.equal(out[0][0], g) and torch.equal(out[0][1], dks)
+
+
+def test_batch_tight_z_margin_keeps_every_state(cuda):
+    """Slab layers for 1 nN of vertical spring give (0.5 A beyond the tip's z-range at the default 20 N/m,
+    against 1.5 A): on molecules of the fitting distribution scanned down to 3 A above the molecule plane the
+    relaxation, df and loss are the wide slabs' bit for bit (no probe leaves the thinner slab) and the
+    gradients agree to rounding (node partials are grouped by slab layout)."""
+    items = synthetic.batch_molecules(4, seed=5, z_end=3.0)
+    tight, wide = AFMBatch(items), AFMBatch(items, slab_margin_z=1.5)
+    assert tight.grid_float4 < 0.85 * wide.grid_float4
+    _target(tight)
+    _target(wide)
+    for b in (tight, wide):
+        b.set_relax_options(polish=True)
+        b.forward_adjoint()
+    torch.cuda.synchronize()
+    assert bool((tight.PPs[:, 3] > 0).all())
+    assert torch.equal(tight.FEs, wide.FEs) and torch.equal(tight.PPs, wide.PPs)
+    assert torch.equal(tight.df_c, wide.df_c) and torch.equal(tight.loss, wide.loss)
+    assert torch.equal(tight.ubar, wide.ubar)
+    torch.testing.assert_close(tight.grad, wide.grad, rtol=1e-5, atol=1e-6 * float(wide.grad.abs().max()))
