@@ -842,14 +842,15 @@ struct NewtonResult {
 
 template <int LAYOUT>
 __device__ __noinline__ NewtonResult slab_newton(const AxisView G, const PolishSpring S, float t00, float t11,
-                                                 float t22, V3 tip, V3 q, bool early) {
+                                                 float t22, V3 tip, V3 q, bool early, float f2stop) {
     const float Tc[3][3] = {{t00, 0.f, 0.f}, {0.f, t11, 0.f}, {0.f, 0.f, t22}};
     NewtonResult r;
     r.q = q;
     r.fe = make_float4(0.f, 0.f, 0.f, 0.f);
     r.g2 = 0.f;
     r.evals = 0;
-    r.ok = newton_core(SlabCellFetch<LAYOUT>{G}, Tc, S, tip, r.q, r.fe, r.g2, r.evals, early);
+    r.ok = newton_core(SlabCellFetch<LAYOUT>{G}, Tc, S, tip, r.q, r.fe, r.g2, r.evals, early, f2stop,
+                       early ? WARM_NEWTON_STEPS : POLISH_STEPS);
     return r;
 }
 
@@ -863,7 +864,10 @@ __device__ __noinline__ NewtonResult slab_newton(const AxisView G, const PolishS
 // the way down in one of the two calls, or there is no previous equilibrium --
 // it starts from the continuation as a cold call does, so every state stays on
 // its stroke's branch.
-constexpr float WARM_MAX_JUMP = 0.1f;
+// An optimiser step that moves every atom by 0.01 A and every charge by 0.01 e moves 99% of the
+// equilibria -- and so of the continuation starts -- by less than 0.35 A (the soft lateral
+// spring); a bound of 0.1 A sent 3% of the strokes back to FIRE after such a step.
+constexpr float WARM_MAX_JUMP = 0.3f;
 
 // A lane's stroke state between z-steps: the tip, the continuation position,
 // the FIRE velocity and integrator state (carried down the stroke), the last
@@ -923,9 +927,10 @@ __device__ __forceinline__ bool stroke_zstep(const AxisView& G, TexelCache& T, c
             NewtonResult r;
             if constexpr (PREFIX) {  // no FIRE in this kernel: inline, through the lane's texel cache
                 r.q = pos;
-                r.ok = newton_core(SlabCellFetchCached<LAYOUT>{G, T}, Tc, S, L.tip, r.q, r.fe, r.g2, r.evals, true);
+                r.ok = newton_core(SlabCellFetchCached<LAYOUT>{G, T}, Tc, S, L.tip, r.q, r.fe, r.g2, r.evals, true,
+                                   P.f2conv, WARM_NEWTON_STEPS);
             } else {
-                r = slab_newton<LAYOUT>(G, S, Tc[0][0], Tc[1][1], Tc[2][2], L.tip, pos, true);
+                r = slab_newton<LAYOUT>(G, S, Tc[0][0], Tc[1][1], Tc[2][2], L.tip, pos, true, P.f2conv);
             }
             if (r.ok) {
                 pos = r.q;
@@ -951,7 +956,7 @@ __device__ __forceinline__ bool stroke_zstep(const AxisView& G, TexelCache& T, c
     V3 q = pos;
     if constexpr (POLISH) {
         if (!newton_done && fe.w == fe.w) {
-            const NewtonResult r = slab_newton<LAYOUT>(G, S, Tc[0][0], Tc[1][1], Tc[2][2], L.tip, q, false);
+            const NewtonResult r = slab_newton<LAYOUT>(G, S, Tc[0][0], Tc[1][1], Tc[2][2], L.tip, q, false, 0.f);
             if (r.ok) {
                 q = r.q;
                 fe = r.fe;

@@ -385,7 +385,13 @@ __device__ __forceinline__ float4 interp_fe_cached(const AxisView& G, V3 p, Texe
 // repeats every operation in the same order, so results are bit-identical to it.
 constexpr int POLISH_STEPS = 4;
 constexpr float NEWTON_FLOOR_STEP = 1e-5f;  // A; the early stop of the warm starts' Newton-first
+constexpr int WARM_NEWTON_STEPS = 8;         // steps of the warm starts' Newton-first
 constexpr float POLISH_MAX_STEP = 0.1f;
+// The warm starts' Newton-first steps up to WARM_MAX_STEP per axis: on the soft lateral spring
+// (k_xy = 0.0156 eV/A^2) a 1.6 meV/A change of the grid force moves an equilibrium by 0.1 A, and
+// an optimiser step that moves every atom by 0.01 A and every charge by 0.01 e moves half of them
+// by more than 0.075 A.
+constexpr float WARM_MAX_STEP = 0.3f;
 
 // Spring and frame of a polished state: frame = false is relaxStrokes' spring (tip_force on
 // q - tip, no rotation, no surface bias); frame = true the tip frame a,b,c with surf along c.
@@ -485,8 +491,8 @@ __device__ __forceinline__ void polish_eval(const float4 (&t)[8], float ax, floa
 }
 
 // Newton step dq = -J^-1 G (adjugate / determinant); false when J is singular or the step is
-// not finite or longer than POLISH_MAX_STEP along an axis.
-__device__ __forceinline__ bool polish_step(const float (&J)[3][3], V3 Gv, V3& dq) {
+// not finite or longer than max_step along an axis.
+__device__ __forceinline__ bool polish_step(const float (&J)[3][3], V3 Gv, V3& dq, float max_step = POLISH_MAX_STEP) {
     float A[3][3];
     A[0][0] = __fmul_rn(J[1][1], J[2][2]) - __fmul_rn(J[1][2], J[2][1]);
     A[0][1] = __fmul_rn(J[0][2], J[2][1]) - __fmul_rn(J[0][1], J[2][2]);
@@ -505,7 +511,7 @@ __device__ __forceinline__ bool polish_step(const float (&J)[3][3], V3 Gv, V3& d
         const float tq = (__fmul_rn(A[i][0], Gv.x) + __fmul_rn(A[i][1], Gv.y)) + __fmul_rn(A[i][2], Gv.z);
         r[i] = __fdiv_rn(-tq, det);
     }
-    if (!(fabsf(r[0]) <= POLISH_MAX_STEP && fabsf(r[1]) <= POLISH_MAX_STEP && fabsf(r[2]) <= POLISH_MAX_STEP))
+    if (!(fabsf(r[0]) <= max_step && fabsf(r[1]) <= max_step && fabsf(r[2]) <= max_step))
         return false;  // also NaN
     dq = mk3(r[0], r[1], r[2]);
     return true;
@@ -521,12 +527,14 @@ __device__ __forceinline__ bool polish_step(const float (&J)[3][3], V3 Gv, V3& d
 //    reached from different starts is ~1e-6 A), so the step would change nothing measurable and
 //    its cell evaluation is saved -- the previous equilibrium of an unmoved state is kept after one
 //    evaluation, a state that moved ~1e-3 A after one step;
-//  - after a kept step that lowered |G|^2 by less than 4x -- quadratic convergence has ended, |G|
-//    is at the float32 floor, and the next step would most likely be refused.
+//  - after a kept step that lowered |G|^2 by less than 4x to below f2stop (the caller's convergence
+//    bound) -- quadratic convergence has ended, |G| is at the float32 floor, and the next step
+//    would most likely be refused; above f2stop (a step that crossed into a cell with another
+//    Jacobian) the iteration goes on, up to max_steps steps.
 template <class Fetch>
 __device__ __forceinline__ bool newton_core(const Fetch& fetch, const float (&T)[3][3], const PolishSpring& S,
                                             V3 tip, V3& q, float4& fe, float& g2_out, int& evals,
-                                            bool early = false) {
+                                            bool early = false, float f2stop = 0.f, int max_steps = POLISH_STEPS) {
     float4 t[8];
     float ax, ay, az;
     evals = 0;
@@ -537,9 +545,9 @@ __device__ __forceinline__ bool newton_core(const Fetch& fetch, const float (&T)
     polish_eval(t, ax, ay, az, T, S, tip, q, fe0, Gv, J);
     evals = 1;
     float g2 = dot3(Gv, Gv);
-    for (int it = 0; it < POLISH_STEPS; it++) {
+    for (int it = 0; it < max_steps; it++) {
         V3 dq;
-        if (!polish_step(J, Gv, dq)) break;
+        if (!polish_step(J, Gv, dq, early ? WARM_MAX_STEP : POLISH_MAX_STEP)) break;
         if (early && fabsf(dq.x) <= NEWTON_FLOOR_STEP && fabsf(dq.y) <= NEWTON_FLOOR_STEP &&
             fabsf(dq.z) <= NEWTON_FLOOR_STEP)
             break;
@@ -557,7 +565,7 @@ __device__ __forceinline__ bool newton_core(const Fetch& fetch, const float (&T)
         fe0 = fe1;
         Gv = G1;
         g2 = g21;
-        if (early && slow) break;
+        if (early && slow && g21 < f2stop) break;
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll

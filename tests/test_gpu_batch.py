@@ -417,7 +417,7 @@ def test_batch_two_pass_schedule_is_bit_identical(cuda, kind):
         one = AFMBatch(items, kind=kind, shape=shapes[0]).set_relax_options(polish=True, warm=True)
         two = AFMBatch(items, kind=kind, shape=shapes[1]).set_relax_options(polish=True, warm=True)
         rng = np.random.default_rng(7)
-        for step, sigma in enumerate((0.0, 5e-3, 5e-3, 0.1, 5e-3)):
+        for step, sigma in enumerate((0.0, 5e-3, 5e-3, 0.1, 5e-3, 0.3, 0.5)):
             if sigma:
                 d = torch.as_tensor(rng.normal(0, sigma, (one.total_atoms, 3)), dtype=one.atoms.dtype, device="cuda")
                 one.atoms[:, :3] += d
