@@ -537,9 +537,13 @@ int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_st
  *      again.
  * totals: the HOST array of spm_batch_prepare; scratch (device) >=
  * spm_batch_adjoint_scratch_bytes(totals, n_mol).  The scratch keeps the
- * cleared adjoint grid between calls, with a marker that says it is clear:
- * reuse one scratch buffer call after call; any other content (a fresh
- * allocation, a call that failed half-way) is cleared by the next call.
+ * cleared adjoint grid between calls, with a marker that says it is clear
+ * (tied to the buffer's address and the layout): reuse one scratch buffer
+ * call after call, and zero-fill a newly allocated one before its first call
+ * (memory that held an earlier scratch of the same layout at the same
+ * address can still carry its marker over content written since); other
+ * content -- a zero-filled buffer, a call that failed half-way -- is cleared
+ * by the next call.
  * adj_flags: SPM_ADJ_PAIR_PARAMS computes grad columns 3-4 (the pair
  * parameters); without it they are written as 0 and the node kernel skips
  * their terms (fits of positions and charges only).  SPM_ADJ_STATE_MAXIMA:

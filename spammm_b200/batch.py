@@ -373,7 +373,9 @@ class AFMBatch:
 
     def _ensure_adj_scratch(self):
         if self.adj_scratch is None:
-            self.adj_scratch = torch.empty(((self._adj_bytes + 15) // 16, 2), dtype=F64, device=self.dev)
+            # zero-filled: memory handed out again by the caching allocator can hold an earlier scratch's
+            # clear marker (same address, same layout) over an adjoint grid that other tensors overwrote
+            self.adj_scratch = torch.zeros(((self._adj_bytes + 15) // 16, 2), dtype=F64, device=self.dev)
 
     def adjoint_state(self):
         """State adjoint; also leaves the per-molecule ubar maxima and touched boxes in the adjoint scratch

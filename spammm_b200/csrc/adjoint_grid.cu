@@ -612,16 +612,27 @@ __device__ __forceinline__ int scale_exp(unsigned umax_bits) {
 }
 __device__ __forceinline__ double pow2(int k) { return __longlong_as_double((long long)(1023 + k) << 52); }
 
-constexpr unsigned long long ADJ_CLEAN = 0x4e41454c434d5053ull;  // marker: the adjoint grid is all zero
+constexpr unsigned long long ADJ_CLEAN = 0x4e41454c434d5053ull;  // marker base: the adjoint grid is all zero
 constexpr unsigned long long ADJ_DIRTY = 1ull;
+
+// The clear marker of one scratch buffer and layout: ADJ_CLEAN mixed with the buffer's address and
+// the layout's size and molecule count, so that memory which held a scratch of another address or
+// layout -- whose marker slot may sit exactly where this layout's does -- does not carry it.
+unsigned long long adj_clean_token(const void* scratch, long long total, int n_mol) {
+    const unsigned long long t = ADJ_CLEAN ^ (reinterpret_cast<uintptr_t>(scratch) * 0x9E3779B97F4A7C15ull) ^
+                                 ((unsigned long long)total * 0xC2B2AE3D27D4EB4Full) ^
+                                 ((unsigned long long)n_mol << 40);
+    return t == ADJ_DIRTY ? t ^ 2ull : t;
+}
 
 // Zeroes the fixed-point adjoint grid (n2 16-byte pairs) unless its marker
 // says it is clear.  The node kernel zeroes every node it reads, so after a
 // completed call the grid is clear again; only a first use, or a call that
 // stopped between the scatter and the node kernel, leaves work here.
 __global__ void __launch_bounds__(256)
-adj_clear_kernel(ulonglong2* __restrict__ gq, long long n2, const unsigned long long* __restrict__ mark) {
-    if (*mark == ADJ_CLEAN) return;
+adj_clear_kernel(ulonglong2* __restrict__ gq, long long n2, const unsigned long long* __restrict__ mark,
+                 unsigned long long clean) {
+    if (*mark == clean) return;
     for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < n2; i += (long long)gridDim.x * 256)
         gq[i] = make_ulonglong2(0ull, 0ull);
 }
@@ -1578,8 +1589,8 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
 // node kernel ran before it (mark != null), block 0 marks the adjoint grid clear.
 __global__ void __launch_bounds__(256)
 batch_fold_rows_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, int chunk, const double* __restrict__ partial,
-                       double* __restrict__ grad, unsigned long long* __restrict__ mark) {
-    if (mark && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *mark = ADJ_CLEAN;
+                       double* __restrict__ grad, unsigned long long* __restrict__ mark, unsigned long long clean) {
+    if (mark && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *mark = clean;
     __shared__ double red[256];
     const long long ga = blockIdx.x;
     const int c = blockIdx.y;
@@ -1722,6 +1733,7 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
     unsigned* umax = reinterpret_cast<unsigned*>(base + SL.umax);
     int* box = reinterpret_cast<int*>(base + SL.box);
     unsigned long long* mark = reinterpret_cast<unsigned long long*>(base + SL.mark);
+    const unsigned long long clean = adj_clean_token(scratch, SL.total, n_mol);
     bool nodes_ran = false;
     if (n_mol > 0 && n_atoms > 0) {
         SPM_REQUIRE(mols && atoms && params && grad && aligned16(atoms), "spm_batch_adjoint_params: null atoms/grad");
@@ -1746,7 +1758,7 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             const bool given = (adj_flags & SPM_ADJ_STATE_MAXIMA) != 0;  // from spm_batch_adjoint_state
             if (!given && cudaMemsetAsync(umax, 0, (size_t)(SL.mark - SL.umax), st) != cudaSuccess)  // maxima + boxes
                 return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: memset failed");
-            adj_clear_kernel<<<1184, 256, 0, st>>>(reinterpret_cast<ulonglong2*>(gq), totals[7] * 2, mark);
+            adj_clear_kernel<<<1184, 256, 0, st>>>(reinterpret_cast<ulonglong2*>(gq), totals[7] * 2, mark, clean);
             if (!given)
                 batch_ubar_max_kernel<<<(unsigned)((n_chunks + UM_CHUNKS - 1) / UM_CHUNKS), 256, 0, st>>>(
                     n_mol, n_chunks, mols, reinterpret_cast<const float4*>(ubar), reinterpret_cast<const float4*>(PPs),
@@ -1796,7 +1808,7 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
             nodes_ran = true;
         }
         batch_fold_rows_kernel<<<dim3((unsigned)n_atoms, 6), 256, 0, st>>>(n_mol, mols, chunk, part, grad,
-                                                                           nodes_ran ? mark : nullptr);
+                                                                           nodes_ran ? mark : nullptr, clean);
     }
     if (n_states > 0) {
         SPM_REQUIRE(dk && aligned16(dk), "spm_batch_adjoint_params: null dk");

@@ -281,6 +281,34 @@ def test_adjoint_scratch_reuse_and_garbage(cuda, kind):
         b.adjoint_params()
         torch.cuda.synchronize()
         assert torch.equal(b.grad, g1), fill
+    # garbage under the clear marker of another buffer with the same layout (memory handed out again can
+    # hold one exactly where this buffer's marker sits): the marker is the buffer's own, so it is cleared
+    other = AFMBatch(_items(kind, n=4, seed=71 + kind), kind=kind)
+    _target(other)
+    other.forward_adjoint()
+    torch.cuda.synchronize()
+    at = _adj_mark_offset(b) // 8
+    assert at == _adj_mark_offset(other) // 8
+    b.adj_scratch.view(torch.uint8).random_(0, 256)
+    b.adj_scratch.view(torch.int64).reshape(-1)[at] = other.adj_scratch.view(torch.int64).reshape(-1)[at]
+    b._state_maxima = False
+    b.adjoint_params()
+    torch.cuda.synchronize()
+    assert torch.equal(b.grad, g1)
+    # a new scratch in memory that held this one (same address and layout, so its own marker) and was written
+    # by other tensors since: AFMBatch zero-fills a new scratch
+    torch.cuda.synchronize()
+    clean = b.adj_scratch.view(torch.int64).reshape(-1)[at].clone()
+    nbytes = b.adj_scratch.numel() * 8
+    b.adj_scratch = None
+    junk = torch.empty((nbytes,), dtype=torch.uint8, device="cuda").random_(0, 256)
+    junk.view(torch.int64)[at] = clean
+    del junk
+    b._ensure_adj_scratch()
+    b._state_maxima = False
+    b.adjoint_params()
+    torch.cuda.synchronize()
+    assert torch.equal(b.grad, g1)
 
 
 @pytest.mark.parametrize("kind", [0, 1])
@@ -549,3 +577,8 @@ def test_batch_tight_z_margin_keeps_every_state(cuda):
     assert torch.equal(tight.df_c, wide.df_c) and torch.equal(tight.loss, wide.loss)
     assert torch.equal(tight.ubar, wide.ubar)
     torch.testing.assert_close(tight.grad, wide.grad, rtol=1e-5, atol=1e-6 * float(wide.grad.abs().max()))
+
+
+def _adj_mark_offset(b):
+    """Byte offset of the adjoint scratch's 16-byte marker slot: the scratch's last 16 bytes."""
+    return int(_lib.lib().spm_batch_adjoint_scratch_bytes(b.plan.totals, b.n)) - 16
