@@ -743,7 +743,8 @@ def run_batched(args, dev_index):
     sr["update_and_rest"] = sr["step"] - sum(sr[k] for k, _ in stages)
     out["fit"]["stage_ms"] = sr
     out["fit"]["stage_ms_note"] = ("eager fit steps after an Adam update (median of 3), each stage between CUDA "
-                                   "events; the graph replay above runs the same launches without host gaps")
+                                   "events; the failure mask runs on a side stream beside adjoint_params; the graph "
+                                   "replay above runs the same launches without host gaps")
     out["plain_per_image"] = plain
     out["fit"]["vs_plain_per_image"] = out["fit"]["images_per_s"] / out["plain_per_image"]["images_per_s"]
     out["fit"]["vs_plain_gpu_kernels"] = plain["gpu_kernel_ms_per_image"] / (ms / args.fit_mols)

@@ -515,7 +515,9 @@ int spm_batch_failure_mask(long long n_states, const float* diag, const double* 
  * for this batch): the call also leaves there each molecule's max |ubar| and
  * box of touched slab rows and layers, which spm_batch_adjoint_params then
  * takes with SPM_ADJ_STATE_MAXIMA instead of a pass over ubar of its own.
- * NULL: no maxima (totals may be NULL). */
+ * NULL: no maxima (totals may be NULL).  dk may be NULL: the spring-parameter
+ * terms are not written (fits that do not move the spring; pass NULL to
+ * spm_batch_adjoint_params too). */
 int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_states,
                             const spm_batch_shape* shape, const float* grid, const float* points,
                             const spm_scan_params* p, const float* PPs, const float* dL_dFEs, float* ubar,
@@ -523,7 +525,7 @@ int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, long long n_st
 
 /* spm_adjoint_grid_params over the batch, node-major: grad (total_atoms,6)
  * double as spm_adjoint_grid_params, dk_sum double[4] summed over the whole
- * batch (one probe).
+ * batch (one probe; 0 when dk is NULL).
  *   1. the states' w*ubar are scattered onto an adjoint grid over each slab
  *      (the transpose of the trilinear sample) in 64-bit fixed point with a
  *      per-molecule power-of-two scale (2^42 / max|ubar|), so the integer

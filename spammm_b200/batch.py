@@ -266,6 +266,7 @@ class AFMBatch:
         self.grad = self.dk_sum = None
         # grad columns 3-4 (pair parameters): computed unless a caller that never reads them turns them off
         self.pair_param_grads = True
+        self.stiffness_grads = True  # False: no spring-parameter terms (dk, dk_sum = 0)
         self.loss = torch.empty((self.n,), dtype=F64, device=dev)
         self._Qs = hostvec(self.probe.tipQs)
         self._QZs = hostvec(self.probe.tipQZs)
@@ -385,7 +386,8 @@ class AFMBatch:
         rc = lib().spm_batch_adjoint_state(self.n, ptr(self.mols_d), self.total_states, ctypes.byref(self.shape),
                                            ptr(self.grid),
                                            ptr(self.points), ctypes.byref(self.scan_params), ptr(self.PPs),
-                                           ptr(self.dL), ptr(self.ubar), ptr(self.dk), ptr(self.diag),
+                                           ptr(self.dL), ptr(self.ubar),
+                                           ptr(self.dk) if self.stiffness_grads else None, ptr(self.diag),
                                            self.plan.totals, ptr(self.adj_scratch), stream_ptr())
         check(rc, "spm_batch_adjoint_state")
         self._state_maxima = True
@@ -398,7 +400,8 @@ class AFMBatch:
         rc = lib().spm_batch_adjoint_params(self.kind, self.n, ptr(self.mols_d), self.plan.totals,
                                             ctypes.byref(self.shape), ptr(self.atoms), ptr(self.params),
                                             hptr(self._Qs), hptr(self._QZs), ptr(self.PPs), ptr(self.ubar),
-                                            ptr(self.dk), ptr(self.grad), ptr(self.dk_sum),
+                                            ptr(self.dk) if self.stiffness_grads else None, ptr(self.grad),
+                                            ptr(self.dk_sum),
                                             (_lib.SPM_ADJ_PAIR_PARAMS if self.pair_param_grads else 0) |
                                             (_lib.SPM_ADJ_STATE_MAXIMA if self._state_maxima else 0),
                                             ptr(self.adj_scratch), stream_ptr())
@@ -418,11 +421,22 @@ class AFMBatch:
         self.relax()
         self.loss_seed()
         self.adjoint_state()
-        self.adjoint_params()
-        if self._mask_failed:
+        if not self._mask_failed:
+            self.adjoint_params()
+            return
+        # the next call's loss weights from this call's adjoint status, on a side stream beside the
+        # parameter adjoint (which neither reads nor writes them; graph capture keeps the fork and join)
+        main = torch.cuda.current_stream()
+        if self._side is None:
+            self._side = torch.cuda.Stream(device=self.dev)
+        self._side.wait_stream(main)
+        with torch.cuda.stream(self._side):
             self._update_mask()
+        self.adjoint_params()
+        main.wait_stream(self._side)
 
     _mask_failed = False
+    _side = None
 
     def enable_failure_mask(self):
         """Keep the loss consistent with its gradient: after each
@@ -546,11 +560,12 @@ class BatchAdam:
     forward, df loss, adjoint, update -- captures into one CUDA graph.
     Summing the per-molecule losses makes each molecule's update depend on its
     own loss only.  The update reads gradient columns 0-2 and 5 only, so the
-    batch's adjoint skips the pair-parameter columns."""
+    batch's adjoint skips the pair-parameter columns and the spring terms."""
 
     def __init__(self, batch, lr=0.01, betas=(0.9, 0.999), eps=1e-8, cols=(0, 1, 2, 3)):
         self.b = batch
         batch.pair_param_grads = False
+        batch.stiffness_grads = False
         self.lr, self.b1, self.b2, self.eps = float(lr), float(betas[0]), float(betas[1]), float(eps)
         self.cols = list(cols)
         dev = batch.dev

@@ -140,14 +140,14 @@ __device__ __forceinline__ void load_cell_texels(const GridView& G, const Corner
 }
 
 // Adjoint of one state: p4 = the stroke's start point, iz = its z-step,
-// pp = stored PP, u = dL/dFEs of the state; writes ubar, dk, diag.
+// pp = stored PP, u = dL/dFEs of the state; writes ubar, dk (unless dk_o is null), diag.
 template <bool SLAB>
 __device__ __forceinline__ void state_adjoint(const GridView& G, const spm_scan_params& P, float4 p4, int iz,
                                               float4 pp, float4 u, float4* ubar_o, float4* dk_o, float4* diag_o) {
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     auto fail = [&](float res, float lmin, float cond, float status) {
         *ubar_o = zero;
-        *dk_o = zero;
+        if (dk_o) *dk_o = zero;
         *diag_o = make_float4(res, lmin, cond, status);
     };
     if (!(isfinite(pp.x) && isfinite(pp.y) && isfinite(pp.z) && isfinite(pp.w) && isfinite(u.x) && isfinite(u.y) &&
@@ -316,8 +316,9 @@ __device__ __forceinline__ void state_adjoint(const GridView& G, const spm_scan_
     // spring-parameter terms  -lambda . R^T dg/dk   (lambda in the tip frame: R lambda)
     const V3 lt = ident ? mk3(lam[0], lam[1], lam[2]) : rotmat(mk3(lam[0], lam[1], lam[2]), a, b, c);
     const float rw = (r - d0.w) / r;
-    *dk_o = make_float4(-lt.x * (dl.x - d0.x), -lt.y * (dl.y - d0.y), -lt.z * (dl.z - d0.z),
-                        -(lt.x * dl.x + lt.y * dl.y + lt.z * dl.z) * rw);
+    if (dk_o)
+        *dk_o = make_float4(-lt.x * (dl.x - d0.x), -lt.y * (dl.y - d0.y), -lt.z * (dl.z - d0.z),
+                            -(lt.x * dl.x + lt.y * dl.y + lt.z * dl.z) * rw);
     *diag_o = make_float4(resid, lmin, cond, 0.f);
 }
 
@@ -543,7 +544,7 @@ batch_adjoint_state_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, lo
         }
         const float4 pp = PPs[st];
         state_adjoint<true>(slab_view(*D, grid, stride), P, pts[D->pix_off + iscan], iz, pp, dL[st], ubar + st,
-                            dk + st, diag + st);
+                            dk ? dk + st : nullptr, diag + st);
         if (umax) {
             const float4 u = ubar[st];  // this thread's own store
             v = fmaxf(fmaxf(fabsf(u.x), fabsf(u.y)), fmaxf(fabsf(u.z), fabsf(u.w)));
@@ -1666,7 +1667,7 @@ extern "C" int spm_batch_adjoint_state(int n_mol, const spm_batch_mol* mols, lon
                 shape->grid_layout);
     SPM_REQUIRE(n_mol >= 0 && n_states >= 0, "spm_batch_adjoint_state: negative sizes");
     if (n_mol == 0 || n_states == 0) return SPM_OK;
-    SPM_REQUIRE(mols && grid && points && PPs && dL_dFEs && ubar && dk && diag, "spm_batch_adjoint_state: null pointer");
+    SPM_REQUIRE(mols && grid && points && PPs && dL_dFEs && ubar && diag, "spm_batch_adjoint_state: null pointer");
     SPM_REQUIRE(aligned16(grid) && aligned16(points) && aligned16(PPs) && aligned16(dL_dFEs) && aligned16(ubar) &&
                 aligned16(dk) && aligned16(diag), "spm_batch_adjoint_state: buffers not 16-byte aligned");
     const long long nb = (n_states + AG_THREADS - 1) / AG_THREADS;
@@ -1810,8 +1811,11 @@ extern "C" int spm_batch_adjoint_params(int kind, int n_mol, const spm_batch_mol
         batch_fold_rows_kernel<<<dim3((unsigned)n_atoms, 6), 256, 0, st>>>(n_mol, mols, chunk, part, grad,
                                                                            nodes_ran ? mark : nullptr, clean);
     }
-    if (n_states > 0) {
-        SPM_REQUIRE(dk && aligned16(dk), "spm_batch_adjoint_params: null dk");
+    if (n_states > 0 && !dk) {  // no spring-parameter terms: dk_sum = 0
+        if (cudaMemsetAsync(dk_sum, 0, 4 * sizeof(double), st) != cudaSuccess)
+            return set_error(SPM_ERR_CUDA, "spm_batch_adjoint_params: memset failed");
+    } else if (n_states > 0) {
+        SPM_REQUIRE(aligned16(dk), "spm_batch_adjoint_params: dk not 16-byte aligned");
         const long long rb = n_rowblocks(n_states);
         sum_rows_kernel<<<(unsigned)rb, 256, 0, st>>>(reinterpret_cast<const float4*>(dk), n_states, dkpart);
         fold_chunks_kernel<<<dim3(1, 4), 256, 0, st>>>(dkpart, (int)rb, 4, dk_sum);

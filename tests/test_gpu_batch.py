@@ -334,6 +334,21 @@ def test_adjoint_without_pair_parameter_columns(cuda, kind):
                                                        _lib.ptr(b.ubar), _lib.ptr(b.dk), _lib.ptr(b.grad),
                                                        _lib.ptr(b.dk_sum), 4, _lib.ptr(b.adj_scratch),
                                                        _lib.stream_ptr()), "spm_batch_adjoint_params")
+    # without the spring terms (dk NULL in both calls): the same gradient, dk_sum = 0, dk left untouched
+    dk_sum = b.dk_sum.clone()
+    assert dk_sum.abs().max() > 0
+    b.dk.fill_(7.0)
+    b.stiffness_grads = False
+    b.adjoint_state()
+    b.adjoint_params()
+    torch.cuda.synchronize()
+    assert torch.equal(b.grad[:, [0, 1, 2, 5]], full[:, [0, 1, 2, 5]])
+    assert not b.dk_sum.any() and bool((b.dk == 7.0).all())
+    b.stiffness_grads = True
+    b.adjoint_state()
+    b.adjoint_params()
+    torch.cuda.synchronize()
+    assert torch.equal(b.dk_sum, dk_sum)
 
 
 def test_batch_adam_reduces_loss(cuda):
