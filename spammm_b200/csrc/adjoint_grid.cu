@@ -1382,6 +1382,7 @@ batch_adjoint_nodes_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, in
                     int left = jp < Lp ? (Lp - jp + P - 1) / P : 0;  // pairs of this thread
                     while (left > 0) {
                         const int nb = min(NM_FLUSH / 2, left);
+#pragma unroll 4
                         for (int k = 0; k < nb; k++, sp += sstep)
                             pair_adj2<KIND, ON, PAR>(lds2(sp), lds2(sp + NM_BUF), lds2(sp + 2 * NM_BUF),
                                                      lds2(sp + 3 * NM_BUF), lds2(sp + 4 * NM_BUF),
