@@ -521,7 +521,8 @@ __device__ __forceinline__ bool polish_step(const float (&J)[3][3], V3 Gv, V3& d
 // not available (outside the sampler's range or the stored slab).  On return q is the polished
 // position, fe the sample there, g2 = |G(q)|^2 and evals the cells evaluated; false (q and fe
 // unchanged) when the first fetch fails.
-// early (the warm starts' Newton-first, not the polish): also stop
+// early (the warm starts' Newton-first, not the polish): steps of up to WARM_MAX_STEP per axis
+// (the polish's: POLISH_MAX_STEP), and also stop
 //  - before a step whose every component is at most NEWTON_FLOOR_STEP: the predicted distance to
 //    the root is at the float32 floor of the positions' noise (the spread of polished equilibria
 //    reached from different starts is ~1e-6 A), so the step would change nothing measurable and
