@@ -374,6 +374,44 @@ def test_batch_adam_reduces_loss(cuda):
     assert float(b.loss.sum()) < float(loss0.sum())
 
 
+def test_batch_adam_graph_with_failure_mask_equals_eager(cuda):
+    """With the failure mask on, a fitting step runs the mask beside the parameter adjoint on a side
+    stream; a captured step replayed equals the same steps run eagerly bit for bit (atoms, the moment
+    buffers and the next step's loss weights)."""
+    items = _items(0, n=4, seed=64)
+    truth = AFMBatch(items)
+    truth.forward_adjoint()
+    rng = np.random.default_rng(9)
+    moved = [it.atoms.copy() for it in items]
+    for a in moved:
+        a[:, :3] += rng.normal(0.0, 0.05, (len(a), 3)).astype(np.float32)
+    runs = []
+    for graph in (False, True):
+        b = AFMBatch(items).set_relax_options(polish=True, warm=True)
+        b.set_target_states(truth.df_c)
+        for i, a in enumerate(moved):
+            b.set_atoms(i, a)
+        b.enable_failure_mask()
+        opt = BatchAdam(b, lr=0.005, cols=(0, 1, 2, 3))
+        if graph:
+            g = b.capture(opt.step, warmup=0)
+            b.reset_warm_start()
+            b.atoms.copy_(torch.as_tensor(b.plan.atoms, device="cuda"))
+            for i, a in enumerate(moved):
+                b.set_atoms(i, a)
+            opt.reset()
+            b.enable_failure_mask()  # a second call resets the weights in place
+            for _ in range(4):
+                g.replay()
+        else:
+            for _ in range(4):
+                opt.step()
+        torch.cuda.synchronize()
+        runs.append((b.atoms.clone(), opt.m.clone(), b.weights.clone(), b.loss.clone()))
+    for x, y in zip(*runs):
+        assert torch.equal(x, y)
+
+
 def test_autotune_returns_valid_shape(cuda):
     from spammm_b200 import autotune
     items = _items(0, n=5, seed=71)
