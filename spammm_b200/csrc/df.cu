@@ -316,7 +316,7 @@ constexpr int LS_THREADS = 256;
 template <typename T>
 __global__ void __launch_bounds__(LS_THREADS)
 loss_partials_kernel(const T* __restrict__ FEs, const double* __restrict__ tgt, const double* __restrict__ wts,
-                     int nx, int ny, int nz, double dz2, double* __restrict__ df_out, double* __restrict__ partial) {
+                     int nx, int ny, int nz, double idz2, double* __restrict__ df_out, double* __restrict__ partial) {
     __shared__ double s_w[LS_THREADS], s_l[LS_THREADS];
     const long long total = (long long)nx * ny * nz;
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -326,7 +326,7 @@ loss_partials_kernel(const T* __restrict__ FEs, const double* __restrict__ tgt, 
         double d = 0.0;
         if (iz > 0 && iz < nz - 1) {
             const double fp = load_row(FEs, gid + 1).z, fm = load_row(FEs, gid - 1).z;
-            d = -(fp - fm) / dz2;
+            d = -(fp - fm) * idz2;
         }
         df_out[gid] = d;
         w = wts ? wts[gid] : ((iz > 0 && iz < nz - 1) ? 1.0 : 0.0);
@@ -375,7 +375,9 @@ loss_final_kernel(const double* __restrict__ partial, int nblk, double* __restri
     }
 }
 
-// dL/dFz = transpose of the central-difference stencil applied to w*(df-t)/wsum.
+// dL/dFz = transpose of the central-difference stencil applied to w*(df-t)/wsum (df and the
+// gradient multiply by the reciprocals 1/(2 dz) and 1/wsum, computed once: within an ulp of the
+// divisions, which cost the loss kernels a divergent FP64 division per state).
 __global__ void __launch_bounds__(LS_THREADS)
 loss_grad_kernel(const double* __restrict__ df, const double* __restrict__ tgt, const double* __restrict__ wts,
                  const double* __restrict__ sums, int nx, int ny, int nz, double coeff, float4* __restrict__ dL) {
@@ -383,11 +385,11 @@ loss_grad_kernel(const double* __restrict__ df, const double* __restrict__ tgt, 
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= total) return;
     const int iz = (int)(gid % nz);
-    const double wsum = sums[0];
+    const double iwsum = 1.0 / sums[0];  // one division per thread, the same for every thread
     auto g = [&](long long j) {
         const int jz = (int)(j % nz);
         const double w = wts ? wts[j] : ((jz > 0 && jz < nz - 1) ? 1.0 : 0.0);
-        return w * (df[j] - tgt[j]) / wsum;
+        return w * (df[j] - tgt[j]) * iwsum;
     };
     double v;
     if (iz == 0) v = g(gid + 1) * coeff;
@@ -534,10 +536,10 @@ extern "C" int spm_df_loss_seed(const void* FEs, int fes_dtype, const double* ta
     cudaStream_t st = as_stream(stream);
     if (fes_dtype == SPM_F32)
         loss_partials_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(static_cast<const float*>(FEs), target, weights,
-                                                                    nx, ny, nz, 2.0 * dz, df_out, partial);
+                                                                    nx, ny, nz, 1.0 / (2.0 * dz), df_out, partial);
     else
         loss_partials_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(static_cast<const double*>(FEs), target, weights,
-                                                                    nx, ny, nz, 2.0 * dz, df_out, partial);
+                                                                    nx, ny, nz, 1.0 / (2.0 * dz), df_out, partial);
     loss_final_kernel<<<1, LS_THREADS, 0, st>>>(partial, (int)nblk, sums, loss_out);
     loss_grad_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(df_out, target, weights, sums, nx, ny, nz,
                                                             1.0 / (2.0 * dz), reinterpret_cast<float4*>(dL_dFEs));
@@ -663,7 +665,7 @@ __device__ __forceinline__ void chunk_partials(double w, double l, double* s_w, 
 __global__ void __launch_bounds__(LS_THREADS)
 batch_loss_partials_kernel(int n_mol, long long n_chunks, const spm_batch_mol* __restrict__ mols,
                            const float* __restrict__ FEs, const double* __restrict__ tgt,
-                           const double* __restrict__ wts, double dz2, double* __restrict__ df_out,
+                           const double* __restrict__ wts, double idz2, double* __restrict__ df_out,
                            double* __restrict__ partial) {
     __shared__ double s_w[LS_THREADS], s_l[LS_THREADS];
     const long long c0 = (long long)blockIdx.x * LS_CHUNKS;
@@ -687,7 +689,7 @@ batch_loss_partials_kernel(int n_mol, long long n_chunks, const spm_batch_mol* _
             double d = 0.0;
             if (iz > 0 && iz < nz - 1) {
                 const double fp = load_row(FEs, gid + 1).z, fm = load_row(FEs, gid - 1).z;
-                d = -(fp - fm) / dz2;
+                d = -(fp - fm) * idz2;
             }
             df_out[gid] = d;
             wv[k] = wts ? wts[gid] : ((iz > 0 && iz < nz - 1) ? 1.0 : 0.0);
@@ -759,9 +761,10 @@ batch_loss_grad_kernel(int n_mol, long long n_chunks, const spm_batch_mol* __res
             dL[gid] = make_float4(0.f, 0.f, 0.f, 0.f);
             continue;
         }
+        const double iwsum = 1.0 / wsum;  // one division per thread, uniform over the molecule's chunk
         auto g = [&](long long j, int jz) {  // jz: the z-step of state j
             const double w = wts ? wts[j] : ((jz > 0 && jz < nz - 1) ? 1.0 : 0.0);
-            return w * (df[j] - tgt[j]) / wsum;
+            return w * (df[j] - tgt[j]) * iwsum;
         };
         double v;
         if (iz == 0) v = g(gid + 1, 1) * coeff;
@@ -848,8 +851,8 @@ extern "C" int spm_batch_df_loss_seed(int n_mol, const spm_batch_mol* mols, long
     cudaStream_t st = as_stream(stream);
     const unsigned nblk = (unsigned)((n_chunks + LS_CHUNKS - 1) / LS_CHUNKS);
     if (n_chunks > 0)
-        batch_loss_partials_kernel<<<nblk, LS_THREADS, 0, st>>>(n_mol, n_chunks, mols, FEs, target, weights, 2.0 * dz,
-                                                                df_out, partial);
+        batch_loss_partials_kernel<<<nblk, LS_THREADS, 0, st>>>(n_mol, n_chunks, mols, FEs, target, weights,
+                                                                1.0 / (2.0 * dz), df_out, partial);
     batch_loss_final_kernel<<<(unsigned)n_mol, LS_THREADS, 0, st>>>(mols, partial, sums, loss_out);
     if (n_chunks > 0)
         batch_loss_grad_kernel<<<nblk, LS_THREADS, 0, st>>>(n_mol, n_chunks, mols, df_out, target, weights, sums,
@@ -935,10 +938,10 @@ extern "C" int spm_df_loss_seed_noalloc(const void* FEs, int fes_dtype, const do
     cudaStream_t st = as_stream(stream);
     if (fes_dtype == SPM_F32)
         loss_partials_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(static_cast<const float*>(FEs), target, weights,
-                                                                    nx, ny, nz, 2.0 * dz, df_out, partial);
+                                                                    nx, ny, nz, 1.0 / (2.0 * dz), df_out, partial);
     else
         loss_partials_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(static_cast<const double*>(FEs), target, weights,
-                                                                    nx, ny, nz, 2.0 * dz, df_out, partial);
+                                                                    nx, ny, nz, 1.0 / (2.0 * dz), df_out, partial);
     loss_final_kernel<<<1, LS_THREADS, 0, st>>>(partial, (int)nblk, sums, loss_out);
     loss_grad_kernel<<<(unsigned)nblk, LS_THREADS, 0, st>>>(df_out, target, weights, sums, nx, ny, nz,
                                                             1.0 / (2.0 * dz), reinterpret_cast<float4*>(dL_dFEs));
