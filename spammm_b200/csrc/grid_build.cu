@@ -215,8 +215,11 @@ __device__ __forceinline__ void build_tile(int na, const float4* __restrict__ at
             if (ic >= B.zst_hi) break;
             float4 o = make_float4(x[h], y[h], z[h], e[h]);
             // |E| > 100 cap of the reference builders (AFM.cl:1053-1054)
-            const float renorm = __fdiv_rn(100.f, fabsf(o.w));
-            if (renorm < 1.f) { o.x *= renorm; o.y *= renorm; o.z *= renorm; o.w *= renorm; }
+            // (the division only where it can scale: 100/|E| < 1 needs |E| > 100; NaN compares false)
+            if (fabsf(o.w) > 100.f) {
+                const float renorm = __fdiv_rn(100.f, fabsf(o.w));
+                if (renorm < 1.f) { o.x *= renorm; o.y *= renorm; o.z *= renorm; o.w *= renorm; }
+            }
             const int zl = ic - B.zst_lo;
             const size_t row = ((size_t)zl * B.nys + yl) * B.nxs;
             const int il = xl > 0 ? xl - 1 : B.nxs - 1;
