@@ -441,8 +441,10 @@ typedef struct spm_batch_shape {
     int adj_agg;        /* adjoint scatter: 0 = every state's corner sums straight to the global adjoint
                            grid (64-bit atomics), 1 = first merged per CTA in a shared-memory table
                            (the strokes of one CTA share nodes), one global atomic per distinct node,
-                           2 = a warp walks a relaxation pixel tile (rx_tile_h) down its strokes and
-                           merges the nodes its lanes share before the atomics.  Same sums */
+                           2 = a warp walks a relaxation pixel tile (rx_tile_h) down its strokes; each
+                           lane carries its lower corner layer down the stroke and takes over the
+                           nodes its raster neighbours (next row, next column) share with it before
+                           the atomics (the default).  Same sums */
     int adj_stage;      /* adjoint node kernel: 0 = each block of adjoint-grid nodes read with plain
                            loads, 1 = fetched into shared memory by a bulk copy while the previous
                            block is examined and computed (with adj_ilp = 1) */

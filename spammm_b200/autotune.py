@@ -12,7 +12,9 @@ Every batched stage reads only its own fields of ``spm_batch_shape``:
                candidate's layout before the relaxation is timed)
   adjoint      adj_chunk (slab nodes per node-major unit), adj_ilp (node pairs
                per step of the node kernel: 1 at 4 CTAs per SM, 2 at 2), adj_agg
-               (the scatter's CTA table), adj_stage (node blocks by bulk copies)
+               (the scatter: per state, a CTA table, or a tile walk merging the
+               nodes neighbouring pixels share), adj_stage (node blocks by bulk
+               copies)
 
 so the stages are tuned one after another, each over its own candidates with
 the others held fixed, by timing the stage's launch with CUDA events on a
@@ -38,7 +40,7 @@ RELAX_CANDIDATES = [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=r, grid
                    [dict(rx_sync=1, rx_threads=128, rx_tile_h=h, rx_regs=5, grid_layout=0) for h in (2, 4, 8, 16)] + \
                    [dict(rx_sync=0, rx_threads=128, rx_tile_h=8, rx_regs=0, grid_layout=0)]
 ADJOINT_CANDIDATES = [dict(adj_chunk=c, adj_ilp=i, adj_agg=a, adj_stage=0) for c in (4096, 16384, 65536)
-                      for i in (1, 2, 3) for a in (0, 1)] + \
+                      for i in (1, 2, 3) for a in (0, 1, 2)] + \
                      [dict(adj_chunk=c, adj_ilp=1, adj_agg=0, adj_stage=1) for c in (4096, 16384)]
 
 _CACHE = {}

@@ -858,15 +858,15 @@ batch_scatter_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, long lon
 // one molecule, (32/h) x h of the raster -- and its lanes walk their strokes down together, one
 // z-step at a time.  A state's upper corner layer is its stroke predecessor's lower layer when the
 // cell column is the same: the lane adds the carried lower-layer sums there (as the default
-// kernel's lane pairs do).  The warp then merges equal nodes across its lanes before the 64-bit
-// atomics: a corner goes to slot ((x0+i)&1) | ((y0+j)&1)<<1 | ((z0+k)&1)<<2 (unwrapped indices), so
-// a lane has at most one node per slot and neighbouring pixels' shared nodes meet in the same slot;
-// per slot __match_any_sync groups the lanes holding the same node and the group's first lane adds
-// the group's sums (from shared memory) with one atomic per channel.  Integer sums of the same
-// fixed-point terms: the default kernel's bits.  Carried corners that share a slot with the upper
-// layer (the column moved within the same layer parity) are flushed in a second round.
+// kernel's lane pairs do).  Then the pixel one row up the raster (the next lane of the tile column)
+// hands over the nodes its upper layer shares with this lane's: all four when its cell is the same,
+// the two of its lower row when its cell is the next one in y; it drops them from its own atomics.
+// Then the same across the tile's columns (lane + h, the next raster column): all four nodes, or
+// the two of its first column when its cell is the next one in x.  In each round a lane gives only
+// to one neighbour and takes only from the other, moving sums between lanes that hold the same node,
+// so the integer sums are the default kernel's bits.  A carried layer whose column moved goes to the
+// grid on its own.
 constexpr int SCT_WARPS = 4;
-constexpr unsigned SCT_NONE = 0xffffffffu;  // no node (slab nodes are fewer than 2^32 - 32)
 
 __global__ void __launch_bounds__(SCT_WARPS * 32)
 batch_scatter_tile_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, unsigned n_slots, int th_log2,
@@ -874,9 +874,11 @@ batch_scatter_tile_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, uns
                           const unsigned* __restrict__ umax, unsigned long long* __restrict__ gq,
                           unsigned long long* __restrict__ mark, unsigned* __restrict__ counter) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *mark = ADJ_DIRTY;  // the adjoint grid is written from here on
-    __shared__ long long s_v[SCT_WARPS][4][32];
     const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int th = 1 << th_log2;
+    const bool has_above = (lane & (th - 1)) < th - 1;  // the next lane is the next raster row, same column
+    const bool has_below = (lane & (th - 1)) > 0;
     while (true) {
         unsigned tb = 0;
         if (lane == 0) tb = atomicAdd(counter, 32u);
@@ -892,40 +894,19 @@ batch_scatter_tile_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, uns
         unsigned long long* base = gq + (size_t)D->grid_off * 4;
         const double scale = pow2(42 - scale_exp(__ldg(umax + m)));
         const int nxs = G.nx_slab, nys = G.ny_slab, x_lo = G.x_lo, y_lo = G.y_lo, z_lo = G.z_lo;
-        auto node_of = [&](int x, int y, int z) {
-            return ((unsigned)(z - z_lo) * (unsigned)nys + (unsigned)(y - y_lo)) * (unsigned)nxs + (unsigned)(x - x_lo);
+        auto add = [&](int x, int y, int z, int ch, long long v) {
+            if (v == 0) return;
+            const size_t node = ((size_t)(z - z_lo) * nys + (y - y_lo)) * nxs + (x - x_lo);
+            atomicAdd(base + node * 4 + ch, (unsigned long long)v);
         };
         auto fixq = [&](float w, float u) {  // the default kernel's fixed-point term
             return w == 0.f ? 0ll : __double2ll_rn((double)(w * u) * scale);
         };
-        // this z-step's state and the carried lower layer of the previous one (weights and ubar kept,
-        // the fixed-point terms recomputed when flushed)
+        // the carried lower layer of the previous z-step (weights and ubar)
         bool cv = false;
-        int cx0 = 0, cy0 = 0, cz0 = 0, cx1 = 0, cy1 = 0, cpx = 0, cpy = 0, cpz = 0;
+        int cx0 = 0, cy0 = 0, cz0 = 0, cx1 = 0, cy1 = 0;
         float cw[4] = {0.f, 0.f, 0.f, 0.f};
         float4 cub = make_float4(0.f, 0.f, 0.f, 0.f);
-        // one merge round: per slot, this lane's entry (has, node, 4 values) from `entry`
-        auto round = [&](auto entry) {
-#pragma unroll
-            for (int sl = 0; sl < 8; sl++) {
-                unsigned key = SCT_NONE - (unsigned)lane;
-                long long v[4] = {0, 0, 0, 0};
-                const bool has = entry(sl, key, v);
-                const unsigned grp = __match_any_sync(FULL, has ? key : SCT_NONE - (unsigned)lane);
-#pragma unroll
-                for (int ch = 0; ch < 4; ch++) s_v[warp][ch][lane] = v[ch];
-                __syncwarp();
-                if (has && lane == __ffs(grp) - 1) {
-#pragma unroll
-                    for (int ch = 0; ch < 4; ch++) {
-                        long long sum = 0;
-                        for (unsigned g = grp; g; g &= g - 1) sum += s_v[warp][ch][__ffs(g) - 1];
-                        if (sum != 0) atomicAdd(base + (size_t)key * 4 + ch, (unsigned long long)sum);
-                    }
-                }
-                __syncwarp();
-            }
-        };
         for (int iz = 0; iz <= nz; ++iz) {  // iz == nz: flush the last carried layer only
             bool valid = false;
             Corners C = {{0, 0}, {0, 0}, {0, 0}, 0.f, 0.f, 0.f, false};
@@ -939,7 +920,7 @@ batch_scatter_tile_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, uns
                     valid = C.ok;
                 }
             }
-            // upper-layer weights (k = 1) and lower-layer weights (k = 0) of corner (i, j)
+            // upper-layer weights (k = 1) and lower-layer weights (k = 0) of corner c = i + 2 j
             float wu[4], wl[4];
 #pragma unroll
             for (int c = 0; c < 4; c++) {
@@ -948,51 +929,84 @@ batch_scatter_tile_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, uns
                 wu[c] = valid ? wxy * C.az : 0.f;
                 wl[c] = valid ? wxy * (1.f - C.az) : 0.f;
             }
-            // unwrapped parities of the cell's lower corner
-            const int px = C.x[0] & 1, py = C.y[0] & 1, pz = C.z[0] & 1;
             const bool merge = valid && cv && C.x[0] == cx0 && C.y[0] == cy0 && C.z[1] == cz0;
-            const bool carried_out = cv && !merge;  // the carried layer goes out on its own
-            const bool clash = carried_out && valid && (cpz == ((pz + 1) & 1));  // shares the upper layer's slots
-            // the upper layer (+ the carried layer when it is the same nodes), and a carried layer that
-            // does not clash
-            round([&](int sl, unsigned& key, long long (&v)[4]) {
-                const int si = sl & 1, sj = (sl >> 1) & 1, sk = sl >> 2;
-                if (valid && sk == ((pz + 1) & 1)) {
-                    const int i = si ^ px, j = sj ^ py, c = i + 2 * j;
-                    key = node_of(C.x[i], C.y[j], C.z[1]);
-                    const float u4[4] = {ub.x, ub.y, ub.z, ub.w}, c4[4] = {cub.x, cub.y, cub.z, cub.w};
+            if (cv && !merge) {  // the carried layer's column moved: its own atomics
+                const float c4[4] = {cub.x, cub.y, cub.z, cub.w};
 #pragma unroll
-                    for (int ch = 0; ch < 4; ch++) v[ch] = fixq(wu[c], u4[ch]) + (merge ? fixq(cw[c], c4[ch]) : 0ll);
-                    return true;
+                for (int c = 0; c < 4; c++) {
+                    const int i = c & 1, j = c >> 1;
+#pragma unroll
+                    for (int ch = 0; ch < 4; ch++) add(i ? cx1 : cx0, j ? cy1 : cy0, cz0, ch, fixq(cw[c], c4[ch]));
                 }
-                if (carried_out && !clash && sk == cpz) {
-                    const int i = si ^ cpx, j = sj ^ cpy, c = i + 2 * j;
-                    key = node_of(i ? cx1 : cx0, j ? cy1 : cy0, cz0);
-                    const float c4[4] = {cub.x, cub.y, cub.z, cub.w};
+            }
+            // the lane above (next raster row): same cell (A) or the next cell in y (B), same x and layer
+            const int ax0 = __shfl_down_sync(FULL, C.x[0], 1), ay0 = __shfl_down_sync(FULL, C.y[0], 1);
+            const int az1 = __shfl_down_sync(FULL, C.z[1], 1);
+            const bool av = __shfl_down_sync(FULL, valid, 1);
+            const bool col = valid && av && has_above && ax0 == C.x[0] && az1 == C.z[1];
+            const bool take_all = col && ay0 == C.y[0];
+            const bool take_row = col && !take_all && ay0 == C.y[1];
+            const bool give_all = __shfl_up_sync(FULL, take_all, 1) && has_below;
+            const bool give_row = __shfl_up_sync(FULL, take_row, 1) && has_below;
+            // then the lane one tile column over (next raster column, same row): same cell, or the next
+            // cell in x (its column i = 0 is this lane's i = 1), same y row and layer
+            const int bx0 = __shfl_down_sync(FULL, C.x[0], th), by0 = __shfl_down_sync(FULL, C.y[0], th);
+            const int bz1 = __shfl_down_sync(FULL, C.z[1], th);
+            const bool bv = __shfl_down_sync(FULL, valid, th);
+            const bool colx = valid && bv && lane + th < 32 && by0 == C.y[0] && bz1 == C.z[1];
+            const bool takex_all = colx && bx0 == C.x[0];
+            const bool takex_col = colx && !takex_all && bx0 == C.x[1];
+            const bool givex_all = __shfl_up_sync(FULL, takex_all, th) && lane >= th;
+            const bool givex_col = __shfl_up_sync(FULL, takex_col, th) && lane >= th;
+            const float u4[4] = {ub.x, ub.y, ub.z, ub.w}, c4[4] = {cub.x, cub.y, cub.z, cub.w};
 #pragma unroll
-                    for (int ch = 0; ch < 4; ch++) v[ch] = fixq(cw[c], c4[ch]);
-                    return true;
+            for (int ch = 0; ch < 4; ch++) {
+                if (__all_sync(FULL, u4[ch] == 0.f && (!merge || c4[ch] == 0.f))) continue;  // warp-uniform
+                long long v[4];
+#pragma unroll
+                for (int c = 0; c < 4; c++) v[c] = fixq(wu[c], u4[ch]) + (merge ? fixq(cw[c], c4[ch]) : 0ll);
+                long long up[4];
+#pragma unroll
+                for (int c = 0; c < 4; c++) up[c] = __shfl_down_sync(FULL, v[c], 1);  // the lane above's, as computed
+                if (give_all) {
+#pragma unroll
+                    for (int c = 0; c < 4; c++) v[c] = 0;
+                } else if (give_row) {
+                    v[0] = 0;
+                    v[1] = 0;
                 }
-                return false;
-            });
-            if (__any_sync(FULL, clash)) {
-                round([&](int sl, unsigned& key, long long (&v)[4]) {
-                    const int si = sl & 1, sj = (sl >> 1) & 1, sk = sl >> 2;
-                    if (clash && sk == cpz) {
-                        const int i = si ^ cpx, j = sj ^ cpy, c = i + 2 * j;
-                        key = node_of(i ? cx1 : cx0, j ? cy1 : cy0, cz0);
-                        const float c4[4] = {cub.x, cub.y, cub.z, cub.w};
+                if (take_all) {
 #pragma unroll
-                        for (int ch = 0; ch < 4; ch++) v[ch] = fixq(cw[c], c4[ch]);
-                        return true;
-                    }
-                    return false;
-                });
+                    for (int c = 0; c < 4; c++) v[c] += up[c];
+                } else if (take_row) {
+                    v[2] += up[0];  // its row j = 0 is this lane's row j = 1
+                    v[3] += up[1];
+                }
+                long long rt[4];
+#pragma unroll
+                for (int c = 0; c < 4; c++) rt[c] = __shfl_down_sync(FULL, v[c], th);  // after the row merge
+                if (givex_all) {
+#pragma unroll
+                    for (int c = 0; c < 4; c++) v[c] = 0;
+                } else if (givex_col) {
+                    v[0] = 0;
+                    v[2] = 0;
+                }
+                if (takex_all) {
+#pragma unroll
+                    for (int c = 0; c < 4; c++) v[c] += rt[c];
+                } else if (takex_col) {
+                    v[1] += rt[0];  // its column i = 0 is this lane's column i = 1
+                    v[3] += rt[2];
+                }
+                if (valid) {
+#pragma unroll
+                    for (int c = 0; c < 4; c++) add(C.x[c & 1], C.y[c >> 1], C.z[1], ch, v[c]);
+                }
             }
             // carry this state's lower layer
             cv = valid;
             cx0 = C.x[0]; cx1 = C.x[1]; cy0 = C.y[0]; cy1 = C.y[1]; cz0 = C.z[0];
-            cpx = px; cpy = py; cpz = pz;
 #pragma unroll
             for (int c = 0; c < 4; c++) cw[c] = wl[c];
             cub = ub;

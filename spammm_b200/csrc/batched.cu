@@ -24,7 +24,7 @@ extern "C" spm_batch_shape spm_batch_default_shape(void) {
     s.grid_layout = 0;
     s.rx_sync = 2;  // as 1 unless the call is warm and polished
     s.adj_ilp = 1;
-    s.adj_agg = 0;
+    s.adj_agg = 2;  // the tile walk with neighbour merges: 14.1 -> 11.8 ms on the 64-molecule fit's adjoint
     s.adj_stage = 0;
     return s;
 }
