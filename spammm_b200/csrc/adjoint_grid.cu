@@ -962,6 +962,11 @@ batch_scatter_tile_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, uns
             const bool givex_all = __shfl_up_sync(FULL, takex_all, th) && lane >= th;
             const bool givex_col = __shfl_up_sync(FULL, takex_col, th) && lane >= th;
             const float u4[4] = {ub.x, ub.y, ub.z, ub.w}, c4[4] = {cub.x, cub.y, cub.z, cub.w};
+            unsigned nd[4];  // the upper layer's slab nodes, once for the four channels
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                nd[c] = ((unsigned)(C.z[1] - z_lo) * (unsigned)nys + (unsigned)(C.y[c >> 1] - y_lo)) * (unsigned)nxs +
+                        (unsigned)(C.x[c & 1] - x_lo);
 #pragma unroll
             for (int ch = 0; ch < 4; ch++) {
                 if (__all_sync(FULL, u4[ch] == 0.f && (!merge || c4[ch] == 0.f))) continue;  // warp-uniform
@@ -1004,7 +1009,8 @@ batch_scatter_tile_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, uns
                 }
                 if (valid) {
 #pragma unroll
-                    for (int c = 0; c < 4; c++) add(C.x[c & 1], C.y[c >> 1], C.z[1], ch, v[c]);
+                    for (int c = 0; c < 4; c++)
+                        if (v[c] != 0) atomicAdd(base + (size_t)nd[c] * 4 + ch, (unsigned long long)v[c]);
                 }
             }
             // carry this state's lower layer
