@@ -902,9 +902,9 @@ batch_scatter_tile_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, uns
             const size_t node = ((size_t)(z - z_lo) * nys + (y - y_lo)) * nxs + (x - x_lo);
             atomicAdd(base + node * 4 + ch, (unsigned long long)v);
         };
-        auto fixq = [&](float w, float u) {  // the default kernel's fixed-point term
-            return w == 0.f ? 0ll : __double2ll_rn((double)(w * u) * scale);
-        };
+        // the default kernel's fixed-point term (its w == 0 test is redundant: ubar is finite, so a zero
+        // weight gives a zero product and the integer 0 either way)
+        auto fixq = [&](float w, float u) { return __double2ll_rn((double)(w * u) * scale); };
         // the carried lower layer of the previous z-step (weights and ubar)
         bool cv = false;
         int cx0 = 0, cy0 = 0, cz0 = 0, cx1 = 0, cy1 = 0;
