@@ -2,7 +2,7 @@
 //
 // spm_batch_prepare validates a descriptor array and numbers the work items of
 // every batched stage across the batch for one launch shape:
-//   tile_off   grid-build CTA tiles  ceil(nx_slab/32) x ceil(ny_slab/gb_ty) x ceil(nz_slab/gb_zb)
+//   tile_off   grid-build CTA tiles  ceil(nx_slab*ny_slab / (32*gb_ty)) x ceil(nz_slab/gb_zb)
 //   slot_off   relaxation slots      raster: 32 per (32/h) x h pixel tile, else one per pixel
 //                                    rounded up to 32 (a warp's 32 slots never span molecules)
 //   unit_off   adjoint node units    ceil(slab nodes/adj_chunk) (0 without states)
@@ -86,7 +86,7 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
         D.unit_off = units;
         D.chunk_off = chunks;
         D.row_off = rows;
-        tiles += ((D.nx_slab + 31LL) / 32) * ((D.ny_slab + S.gb_ty - 1LL) / S.gb_ty) *
+        tiles += (((long long)D.nx_slab * D.ny_slab + 32LL * S.gb_ty - 1) / (32LL * S.gb_ty)) *
                  ((D.nz_slab + S.gb_zb - 1LL) / S.gb_zb);
         if (nst > 0) {
             if (D.raster_ny > 0) {

@@ -289,8 +289,11 @@ TipSites make_sites(const float* Qs, const float* QZs, bool& on, int& noff) {
 }
 
 // ---- batched slabs ----------------------------------------------------------
-// One CTA per tile of the batch; tiles of a molecule are numbered x fastest,
-// then y, then z over ceil(nx_slab/32) x ceil(ny_slab/TY) x ceil(nz_slab/ZB).
+// One CTA per tile of the batch: 32*TY consecutive (x fastest) of the slab's
+// nx_slab*ny_slab columns, ZB layers; tiles of a molecule are numbered columns
+// first, then z, over ceil(nx_slab*ny_slab / (32*TY)) x ceil(nz_slab/ZB).
+// (Column tiles need not fit the slab's rows: a 32 x TY box of rows would
+// leave a quarter of the node-atom pairs idle on the batch distribution.)
 template <int KIND, bool ON, int NOFF, int ZB, int LAYOUT>
 __global__ void __launch_bounds__(256)
 batch_grid_build_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const float4* __restrict__ atoms,
@@ -301,12 +304,14 @@ batch_grid_build_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const
     const int z_lo = D->z_lo, nzs = D->nz_slab;
     const StoreBox B = {D->x_lo, D->nx_slab, D->y_lo, D->ny_slab, z_lo, z_lo + nzs};
     const long long lt = tile - D->tile_off;
-    const int ntx = (B.nxs + GB_TX - 1) / GB_TX, nty = (B.nys + ty - 1) / ty;
-    const int bx = (int)(lt % ntx);
-    const long long r = lt / ntx;
-    const int by = (int)(r % nty);
-    const long long bz = r / nty;
+    const long long ncol = (long long)B.nxs * B.nys;
+    const int cpt = GB_TX * ty;  // columns per tile
+    const long long ntc = (ncol + cpt - 1) / cpt;
+    const long long bc = lt % ntc, bz = lt / ntc;
     if (bz * ZB >= nzs) return;  // whole CTA: outside the slab (prefix of another shape)
+    const long long col = bc * cpt + threadIdx.y * GB_TX + threadIdx.x;
+    // a column past the slab's last gets a row outside the box: computed by nobody, stored nowhere
+    const int yl = col < ncol ? (int)(col / B.nxs) : B.nys, xl = col < ncol ? (int)(col - (long long)yl * B.nxs) : 0;
     GridGeom G;
     G.nx = D->nx; G.ny = D->ny; G.nz = D->nz;
     G.p0 = ld4f(D->p0);
@@ -315,8 +320,8 @@ batch_grid_build_kernel(int n_mol, const spm_batch_mol* __restrict__ mols, const
     G.dC = ld4f(D->dC);
     const int ao = D->atom_off;
     build_tile<KIND, ON, NOFF, ZB, LAYOUT>(D->n_atoms, atoms + ao, params + (size_t)ao * pstride, pstride,
-                                           grid + LAYOUT * D->grid_off, G, S, B, B.x_lo + bx * GB_TX + threadIdx.x,
-                                           B.y_lo + by * ty + threadIdx.y, z_lo + (int)bz * ZB);
+                                           grid + LAYOUT * D->grid_off, G, S, B, B.x_lo + xl, B.y_lo + yl,
+                                           z_lo + (int)bz * ZB);
 }
 
 struct BatchLaunch {

@@ -35,7 +35,7 @@ def test_prepare_totals(shape_kw):
     for j in range(plan.n):
         D = plan.mols[j]
         assert (D.tile_off, D.slot_off, D.unit_off, D.chunk_off, D.row_off) == (tiles, slots, units, chunks, rows)
-        tiles += -(-D.nx_slab // 32) * -(-D.ny_slab // shape.gb_ty) * -(-D.nz_slab // shape.gb_zb)
+        tiles += -(-(D.nx_slab * D.ny_slab) // (32 * shape.gb_ty)) * -(-D.nz_slab // shape.gb_zb)
         nst = D.n_scan * D.nz_steps
         nxr = D.n_scan // D.raster_ny
         slots += -(-nxr // tw) * -(-D.raster_ny // th) * 32
