@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--fit-mols", type=int, default=64)
     ap.add_argument("--fit-steps", type=int, default=100)
     ap.add_argument("--fit-lr", type=float, default=0.01, help="Adam learning rate of the fit (A, e)")
+    ap.add_argument("--fit-groups", type=int, default=4,
+                    help="fit molecules dealt into this many batches, each on its own stream in one graph")
     ap.add_argument("--fit-z-end", type=float, default=3.0,
                     help="lowest tip height of the fit's scans above the molecule plane (A)")
     ap.add_argument("--batch-only", action="store_true",
@@ -668,27 +670,36 @@ def run_batched(args, dev_index):
         a = it.atoms.copy()
         a[:, :3] += rng.normal(0.0, 0.1, (len(a), 3)).astype(np.float32)
         pert.append(a)
-    b = AFMBatch(items, shape=shape).set_relax_options(polish=polish)
-    for i, a in enumerate(pert):
-        b.set_atoms(i, a)
-    b.forward_adjoint()  # target 0: df_c is the perturbed structures' df
-    target = b.df_c.clone()
-    b.set_relax_options(warm=warm)
-    b.reset_warm_start()
-    start = torch.as_tensor(b.plan.atoms, device=b.atoms.device)
-    truth = b.atoms.clone()
-    b.atoms.copy_(start)
-    b.set_target_states(target)
-    b.enable_failure_mask()
-    opt = BatchAdam(b, lr=args.fit_lr, cols=(0, 1, 2, 3))
-    g = b.capture(opt.step, warmup=0)
-    b.reset_warm_start()
-    b.forward_adjoint()
-    loss0 = float(b.loss.sum())
-    b.atoms.copy_(start)
-    opt.reset()
-    b.enable_failure_mask()
-    b.reset_warm_start()
+    from spammm_b200.batch import StreamGroup, molecule_groups
+    groups = molecule_groups(len(items), args.fit_groups)
+    bs, opts, starts, truths = [], [], [], []
+    loss0 = 0.0
+    for idx in groups:
+        b = AFMBatch([items[i] for i in idx], shape=shape).set_relax_options(polish=polish)
+        for j, i in enumerate(idx):
+            b.set_atoms(j, pert[i])
+        b.forward_adjoint()  # target 0: df_c is the perturbed structures' df
+        target = b.df_c.clone()
+        b.set_relax_options(warm=warm)
+        b.reset_warm_start()
+        start = torch.as_tensor(b.plan.atoms, device=b.atoms.device)
+        truths.append(b.atoms.clone())
+        b.atoms.copy_(start)
+        b.set_target_states(target)
+        b.enable_failure_mask()
+        opt = BatchAdam(b, lr=args.fit_lr, cols=(0, 1, 2, 3))
+        b.forward_adjoint()
+        loss0 += float(b.loss.sum())
+        bs.append(b)
+        opts.append(opt)
+        starts.append(start)
+    sg = StreamGroup([opt.step for opt in opts])
+    g = sg.capture()
+    for b, opt, start in zip(bs, opts, starts):
+        b.atoms.copy_(start)
+        opt.reset()
+        b.enable_failure_mask()
+        b.reset_warm_start()
     clk = ClockSampler(dev_index)
     clk.start()
     e0, e1 = _events()
@@ -699,25 +710,32 @@ def run_batched(args, dev_index):
     torch.cuda.synchronize()
     clocks = clk.stop()
     ms = e0.elapsed_time(e1) / args.fit_steps
-    b.forward_adjoint()
+    for b in bs:
+        b.forward_adjoint()
     torch.cuda.synchronize()
+    atoms = torch.cat([b.atoms for b in bs])
+    start, truth = torch.cat(starts), torch.cat(truths)
+    n_states = sum(b.total_states for b in bs)
 
     def rmse(x, y):
         return float(((x[:, :3] - y[:, :3]) ** 2).sum(1).mean().sqrt())
-    st = torch.bincount(b.diag[:, 3].long(), minlength=6).tolist()
+    st = torch.stack([torch.bincount(b.diag[:, 3].long(), minlength=6)[:6] for b in bs]).sum(0).tolist()
     out["fit"] = {
         "workload": f"{args.fit_mols} molecules of the batch distribution, target df from N(0,0.1 A)-perturbed "
                     f"positions, {args.fit_steps} Adam steps (lr {args.fit_lr}) on positions and charges from the "
                     "unperturbed structures, one CUDA-graph replay per step (forward + df loss + adjoint + update)",
+        "groups": f"{len(bs)} batches of {'/'.join(str(len(i)) for i in groups)} molecules (dealt round-robin), "
+                  "each on its own stream, forked and joined inside the one graph",
         "relax_options": {"newton_polish": polish, "warm_start": warm},
-        "ms_per_step": ms, "images_per_s": args.fit_mols / (ms * 1e-3), "states_per_step": b.total_states,
-        "loss_start": loss0, "loss_final": float(b.loss.sum()),
-        "rmse_vs_unperturbed_A": rmse(b.atoms, start), "rmse_vs_target_structure_A": rmse(b.atoms, truth),
+        "ms_per_step": ms, "images_per_s": args.fit_mols / (ms * 1e-3), "states_per_step": n_states,
+        "loss_start": loss0, "loss_final": float(sum(float(b.loss.sum()) for b in bs)),
+        "rmse_vs_unperturbed_A": rmse(atoms, start), "rmse_vs_target_structure_A": rmse(atoms, truth),
         "rmse_start_vs_target_structure_A": rmse(start, truth), "adjoint_status_counts": st,
         "shape": dict(zip([f for f, _ in type(shape)._fields_], shape.key())), "autotune": tune_rep,
         "clocks": clocks}
-    # where a step goes: eager fit steps, each stage bracketed by CUDA events; the first step repeats the
-    # final forward's atoms and is not counted, so every counted step relaxes atoms the update moved
+    # where a step goes: eager fit steps, the groups one after another on one stream, each stage bracketed by
+    # CUDA events and summed over the groups; the first step repeats the final forward's atoms and is not
+    # counted, so every counted step relaxes atoms the update moved
     stages = (("grid", "build_grids"), ("relax", "relax"), ("loss", "loss_seed"), ("adjoint_state", "adjoint_state"),
               ("adjoint_params", "adjoint_params"), ("failure_mask", "_update_mask"))
     ev = {k: [] for k, _ in stages + (("step", None),)}
@@ -730,27 +748,38 @@ def run_batched(args, dev_index):
             e1.record()
             ev[key].append((e0, e1))
         return run
-    for key, meth in stages:
-        setattr(b, meth, timed(key, getattr(b, meth)))  # instance attributes shadow the methods
+
+    def eager_step():
+        for opt in opts:
+            opt.step()
+    for b in bs:
+        for key, meth in stages:
+            setattr(b, meth, timed(key, getattr(b, meth)))  # instance attributes shadow the methods
     try:
         for _ in range(4):
-            timed("step", opt.step)()
+            timed("step", eager_step)()
     finally:
-        for _, meth in stages:
-            delattr(b, meth)
+        for b in bs:
+            for _, meth in stages:
+                delattr(b, meth)
     torch.cuda.synchronize()
-    sr = {k: float(np.median([e0.elapsed_time(e1) for e0, e1 in v[1:]])) for k, v in ev.items()}
+    sr = {}
+    for k, v in ev.items():
+        per = len(v) // 4  # calls per step: one per group, one for the whole step
+        ts = [e0.elapsed_time(e1) for e0, e1 in v]
+        sr[k] = float(np.median([sum(ts[i * per:(i + 1) * per]) for i in range(1, 4)]))
     # the failure mask runs on a side stream beside adjoint_params: not part of the critical path's sum
     sr["update_and_rest"] = sr["step"] - sum(sr[k] for k, _ in stages if k != "failure_mask")
     out["fit"]["stage_ms"] = sr
-    out["fit"]["stage_ms_note"] = ("eager fit steps after an Adam update (median of 3), each stage between CUDA "
-                                   "events; the failure mask runs on a side stream beside adjoint_params; the graph "
-                                   "replay above runs the same launches without host gaps")
+    out["fit"]["stage_ms_note"] = ("eager fit steps after an Adam update (median of 3), the groups one after "
+                                   "another, each stage between CUDA events and summed over the groups; the failure "
+                                   "mask runs on a side stream beside adjoint_params; the graph replay above runs "
+                                   "the groups' launches concurrently and without host gaps")
     out["plain_per_image"] = plain
     out["fit"]["vs_plain_per_image"] = out["fit"]["images_per_s"] / out["plain_per_image"]["images_per_s"]
     out["fit"]["vs_plain_gpu_kernels"] = plain["gpu_kernel_ms_per_image"] / (ms / args.fit_mols)
-    out["fit"]["fire_steps_per_state_last_step"] = float(b.iter_count.double().sum()) / b.total_states
-    del g, b, opt
+    out["fit"]["fire_steps_per_state_last_step"] = float(sum(float(b.iter_count.double().sum()) for b in bs)) / n_states
+    del g, sg, bs, opts, b, opt
     torch.cuda.empty_cache()
     # ---- (3) forward images of a large batch in one graph
     items = synthetic.batch_molecules(args.batch_mols, seed=3)

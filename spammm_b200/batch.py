@@ -600,3 +600,43 @@ class BatchAdam:
         self._upd.sqrt_().add_(self.eps)
         torch.div(self.m / bc1, self._upd, out=self._upd)
         b.atoms.sub_(self._upd, alpha=self.lr)
+
+
+class StreamGroup:
+    """Independent calls -- typically the ``BatchAdam.step`` of batches over
+    disjoint molecule groups, each AFMBatch with its own buffers -- each on a
+    stream of its own, forked from and joined back to the caller's stream.
+    Captured into one CUDA graph (``capture``), the groups' kernels overlap:
+    one group's launches fill the SMs that another group's kernel boundaries
+    (its last wave, the dependent launch after it) leave idle.  The calls must
+    share no buffer they write; each group's results are those of running it
+    alone."""
+
+    def __init__(self, calls, device=None):
+        self.calls = list(calls)
+        self.streams = [torch.cuda.Stream(device=device) for _ in self.calls]
+
+    def __call__(self):
+        main = torch.cuda.current_stream()
+        for s in self.streams:
+            s.wait_stream(main)
+        for fn, s in zip(self.calls, self.streams):
+            with torch.cuda.stream(s):
+                fn()
+        for s in self.streams:
+            main.wait_stream(s)
+
+    def capture(self):
+        """CUDA graph of one call of every group (the fork and join included)."""
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self()
+        return g
+
+
+def molecule_groups(n, k):
+    """Indices of n molecules dealt round-robin into k groups (sizes within one
+    of each other; the batch distribution's large and small molecules spread
+    evenly)."""
+    k = max(1, min(int(k), n)) if n > 0 else 1
+    return [list(range(j, n, k)) for j in range(k)]

@@ -412,6 +412,64 @@ def test_batch_adam_graph_with_failure_mask_equals_eager(cuda):
         assert torch.equal(x, y)
 
 
+def test_stream_group_fit_equals_groups_run_one_after_another(cuda):
+    """Fitting steps of two molecule groups captured on two streams in one graph equal the same
+    groups' steps run eagerly one after another bit for bit (atoms, moments, next weights, losses);
+    the first step's per-molecule losses equal those of one batch over all the molecules."""
+    from spammm_b200.batch import StreamGroup, molecule_groups
+    items = _items(0, n=5, seed=66)
+    truth = AFMBatch(items)
+    truth.forward_adjoint()
+    rng = np.random.default_rng(12)
+    moved = [it.atoms.copy() for it in items]
+    for a in moved:
+        a[:, :3] += rng.normal(0.0, 0.05, (len(a), 3)).astype(np.float32)
+    groups = molecule_groups(len(items), 2)
+    assert groups == [[0, 2, 4], [1, 3]]
+
+    def setup(b, idx):
+        b.set_relax_options(polish=True, warm=True)
+        for j, i in enumerate(idx):
+            lo, hi = truth._rows(i, "state")
+            b.set_target(j, truth.df_c[lo:hi])
+            b.set_atoms(j, moved[i])
+        b.enable_failure_mask()
+    whole = AFMBatch(items)
+    setup(whole, list(range(len(items))))
+    whole.forward_adjoint()
+    runs = []
+    for graph in (False, True):
+        parts = [AFMBatch([items[i] for i in idx]) for idx in groups]
+        for b, idx in zip(parts, groups):
+            setup(b, idx)
+        opts = [BatchAdam(b, lr=0.005, cols=(0, 1, 2, 3)) for b in parts]
+        sg = StreamGroup([o.step for o in opts])
+        if graph:
+            g = sg.capture()
+            for b, o, idx in zip(parts, opts, groups):
+                b.reset_warm_start()
+                setup(b, idx)  # a second enable_failure_mask resets the weights in place
+                o.reset()
+        first = None
+        for k in range(3):
+            if graph:
+                g.replay()
+            else:
+                for o in opts:
+                    o.step()
+            if k == 0:
+                torch.cuda.synchronize()
+                first = [[b.loss_of(j).clone() for j in range(len(idx))] for b, idx in zip(parts, groups)]
+        torch.cuda.synchronize()
+        for ls, idx in zip(first, groups):
+            for l0, i in zip(ls, idx):
+                assert torch.equal(l0, whole.loss_of(i)), (i, graph)
+        runs.append([(b.atoms.clone(), o.m.clone(), b.weights.clone(), b.loss.clone()) for b, o in zip(parts, opts)])
+    for pa, pb in zip(*runs):
+        for x, y in zip(pa, pb):
+            assert torch.equal(x, y)
+
+
 def test_autotune_returns_valid_shape(cuda):
     from spammm_b200 import autotune
     items = _items(0, n=5, seed=71)
