@@ -206,3 +206,13 @@ def test_autotune_shape_text():
     for cands in (autotune.GRID_CANDIDATES, autotune.RELAX_CANDIDATES, autotune.ADJOINT_CANDIDATES):
         for kw in cands:
             assert all(hasattr(base, k) for k in kw), kw
+
+
+def test_molecule_groups_deal_round_robin():
+    from spammm_b200.batch import molecule_groups
+    assert molecule_groups(10, 4) == [[0, 4, 8], [1, 5, 9], [2, 6], [3, 7]]
+    assert molecule_groups(3, 8) == [[0], [1], [2]]  # no empty group
+    assert molecule_groups(5, 1) == [list(range(5))]
+    assert molecule_groups(5, 0) == [list(range(5))]
+    g = molecule_groups(64, 4)
+    assert sorted(i for grp in g for i in grp) == list(range(64)) and {len(x) for x in g} == {16}
