@@ -512,6 +512,17 @@ long long spm_batch_loss_scratch_bytes(long long n_chunks, int n_mol);
 int spm_batch_failure_mask(long long n_states, const float* diag, const double* w_base, double* weights,
                            void* stream);
 
+/* One Adam step (Kingma & Ba, 2015) of a fit over the batch's atoms, in place, FP32: for every atom i
+ * and every column c set in `cols` (bit 0-3: x, y, z, charge), g = grad[6 i + (c < 3 ? c : 5)],
+ * m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2, atoms -= lr (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps)
+ * with t = *t_steps + 1, which is stored back (a device float, so graph replays count the steps);
+ * 1 - b1, 1 - b2 and the bias corrections are formed in FP64 and rounded once.
+ * grad (n_atoms,6) f64 as spm_batch_adjoint_params writes it; atoms, m, v (n_atoms,4) f32, 16-byte
+ * aligned.  One launch of one CTA.  Replaces the in-place tensor updates of a fitting loop (the
+ * reference fits with host-side optimisers; this has no reference counterpart). */
+int spm_batch_adam_step(long long n_atoms, const double* grad, float* atoms, float* m, float* v, float* t_steps,
+                        double lr, double beta1, double beta2, double eps, int cols, void* stream);
+
 /* spm_adjoint_grid_state over the batch (same outputs per state).
  * adj_scratch (optional, with totals: the scratch of spm_batch_adjoint_params
  * for this batch): the call also leaves there each molecule's max |ubar| and

@@ -173,6 +173,7 @@ _SIGNATURES = {
     "spm_batch_df_loss_seed": (_i, [_i, _vp, _ll, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _vp]),
     "spm_batch_loss_scratch_bytes": (_ll, [_ll, _i]),
     "spm_batch_failure_mask": (_i, [_ll, _vp, _vp, _vp, _vp]),
+    "spm_batch_adam_step": (_i, [_ll, _vp, _vp, _vp, _vp, _vp, _d, _d, _d, _d, _i, _vp]),
     "spm_batch_adjoint_state": (_i, [_i, _vp, _ll, _BS, _vp, _vp, _P, _vp, _vp, _vp, _vp, _vp, _LLP, _vp, _vp]),
     "spm_batch_adjoint_params": (_i, [_i, _i, _vp, _LLP, _BS, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i,
                                       _vp, _vp]),

@@ -556,8 +556,9 @@ class AFMBatch:
 
 class BatchAdam:
     """Adam (Kingma & Ba, 2015) on the batch's atom positions and charges,
-    written with in-place torch ops on fixed buffers so one fitting step --
-    forward, df loss, adjoint, update -- captures into one CUDA graph.
+    one kernel (spm_batch_adam_step) on fixed buffers with the step count on
+    the device, so one fitting step -- forward, df loss, adjoint, update --
+    captures into one CUDA graph.
     Summing the per-molecule losses makes each molecule's update depend on its
     own loss only.  The update reads gradient columns 0-2 and 5 only, so the
     batch's adjoint skips the pair-parameter columns and the spring terms."""
@@ -572,11 +573,10 @@ class BatchAdam:
         na = batch.total_atoms
         self.m = torch.zeros((na, 4), dtype=F32, device=dev)
         self.v = torch.zeros((na, 4), dtype=F32, device=dev)
-        self.g = torch.zeros((na, 4), dtype=F32, device=dev)
-        self.t = torch.zeros((), dtype=F32, device=dev)
-        self.mask = torch.zeros((1, 4), dtype=F32, device=dev)
-        self.mask[0, self.cols] = 1.0
-        self._upd = torch.zeros((na, 4), dtype=F32, device=dev)
+        self.t = torch.zeros((), dtype=F32, device=dev)  # steps taken (device-side, for graph replays)
+        self.col_bits = sum(1 << int(c) for c in set(self.cols))
+        if not 0 <= self.col_bits < 16:
+            raise ValueError(f"BatchAdam: cols={cols} (0-3: x, y, z, charge)")
 
     def reset(self):
         self.m.zero_()
@@ -584,22 +584,13 @@ class BatchAdam:
         self.t.zero_()
 
     def step(self):
-        """One fitting step on the current stream (graph-capturable)."""
+        """One fitting step on the current stream (graph-capturable): forward + adjoint, then the
+        update in one launch (spm_batch_adam_step)."""
         b = self.b
         b.forward_adjoint()
-        gr = b.grad
-        self.g[:, 0:3].copy_(gr[:, 0:3])
-        self.g[:, 3].copy_(gr[:, 5])
-        self.g.mul_(self.mask)
-        self.t.add_(1.0)
-        self.m.mul_(self.b1).add_(self.g, alpha=1.0 - self.b1)
-        self.v.mul_(self.b2).addcmul_(self.g, self.g, value=1.0 - self.b2)
-        bc1 = 1.0 - torch.pow(self.b1, self.t)
-        bc2 = 1.0 - torch.pow(self.b2, self.t)
-        torch.div(self.v, bc2, out=self._upd)
-        self._upd.sqrt_().add_(self.eps)
-        torch.div(self.m / bc1, self._upd, out=self._upd)
-        b.atoms.sub_(self._upd, alpha=self.lr)
+        check(lib().spm_batch_adam_step(b.total_atoms, ptr(b.grad), ptr(b.atoms), ptr(self.m), ptr(self.v),
+                                        ptr(self.t), self.lr, self.b1, self.b2, self.eps, self.col_bits,
+                                        stream_ptr()), "spm_batch_adam_step")
 
 
 class StreamGroup:

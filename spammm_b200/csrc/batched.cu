@@ -11,6 +11,7 @@
 // The kernels find the molecule of a work item by binary search over these
 // prefixes, so one launch per stage covers any mix of molecule sizes.
 #include "spm_internal.cuh"
+#include <cmath>
 
 extern "C" spm_batch_shape spm_batch_default_shape(void) {
     spm_batch_shape s;
@@ -118,4 +119,63 @@ extern "C" int spm_batch_prepare(spm_batch_mol* mols, int n_mol, const spm_batch
     totals_out[7] = grid_end;
     totals_out[8] = rows;
     return SPM_OK;
+}
+
+// ---- fitting update -----------------------------------------------------------
+namespace spm {
+namespace {
+constexpr int ADAM_THREADS = 1024;
+
+// One Adam step over every (atom, column) of the column mask, in FP32.  A single CTA strides over
+// the atoms (a fit's batch holds thousands of atoms: one launch of a few microseconds), reads the
+// step count before the barrier and writes the incremented count after it, so every thread uses
+// the same step and the count stays on the device for graph replays.
+__global__ void __launch_bounds__(ADAM_THREADS)
+batch_adam_kernel(long long n_atoms, const double* __restrict__ grad, float4* __restrict__ atoms,
+                  float4* __restrict__ m, float4* __restrict__ v, float* __restrict__ t, double lr_, double b1_,
+                  double b2_, double eps_, int cols) {
+    const float t1 = *t + 1.f;
+    // the coefficients in FP64, then rounded once: 1 - b in FP32 would lose 1e-5 of (1 - 0.999)
+    const float b1 = (float)b1_, b2 = (float)b2_, c1 = (float)(1.0 - b1_), c2 = (float)(1.0 - b2_);
+    const float bc1 = (float)(1.0 - pow(b1_, (double)t1)), bc2 = (float)(1.0 - pow(b2_, (double)t1));
+    const float lr = (float)lr_, eps = (float)eps_;
+    for (long long i = threadIdx.x; i < n_atoms; i += ADAM_THREADS) {
+        float4 a = atoms[i], mi = m[i], vi = v[i];
+        const double* gr = grad + 6 * i;
+        float* ac = &a.x;
+        float* mc = &mi.x;
+        float* vc = &vi.x;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            if (!((cols >> c) & 1)) continue;
+            const float g = (float)gr[c < 3 ? c : 5];  // x, y, z, then the charge column
+            mc[c] = mc[c] * b1 + c1 * g;
+            vc[c] = vc[c] * b2 + c2 * (g * g);
+            ac[c] -= lr * ((mc[c] / bc1) / (sqrtf(vc[c] / bc2) + eps));
+        }
+        atoms[i] = a;
+        m[i] = mi;
+        v[i] = vi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *t = t1;
+}
+}  // namespace
+}  // namespace spm
+
+extern "C" int spm_batch_adam_step(long long n_atoms, const double* grad, float* atoms, float* m, float* v, float* t,
+                                   double lr, double beta1, double beta2, double eps, int cols, void* stream) {
+    using namespace spm;
+    clear_error();
+    SPM_REQUIRE(n_atoms >= 0, "spm_batch_adam_step: n_atoms=%lld", n_atoms);
+    SPM_REQUIRE(grad && atoms && m && v && t, "spm_batch_adam_step: null pointer");
+    SPM_REQUIRE(aligned16(atoms) && aligned16(m) && aligned16(v), "spm_batch_adam_step: buffers not 16-byte aligned");
+    SPM_REQUIRE(std::isfinite(lr) && beta1 >= 0.0 && beta1 < 1.0 && beta2 >= 0.0 && beta2 < 1.0 && eps > 0.0,
+                "spm_batch_adam_step: lr=%g beta1=%g beta2=%g eps=%g", lr, beta1, beta2, eps);
+    SPM_REQUIRE((cols & ~15) == 0, "spm_batch_adam_step: cols=%d (bits 0-3: x, y, z, charge)", cols);
+    batch_adam_kernel<<<1, ADAM_THREADS, 0, as_stream(stream)>>>(n_atoms, grad, reinterpret_cast<float4*>(atoms),
+                                                                 reinterpret_cast<float4*>(m),
+                                                                 reinterpret_cast<float4*>(v), t, lr, beta1, beta2,
+                                                                 eps, cols);
+    return check_launch("spm_batch_adam_step");
 }

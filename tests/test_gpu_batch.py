@@ -693,3 +693,35 @@ def test_batch_tight_z_margin_keeps_every_state(cuda):
 def _adj_mark_offset(b):
     """Byte offset of the adjoint scratch's 16-byte marker slot: the scratch's last 16 bytes."""
     return int(_lib.lib().spm_batch_adjoint_scratch_bytes(b.plan.totals, b.n)) - 16
+
+
+def test_batch_adam_step_matches_the_adam_formula(cuda):
+    """spm_batch_adam_step against Adam written out with tensor ops (FP32), two steps in a row, a
+    column mask without y: the masked column and its moments stay untouched."""
+    from spammm_b200._lib import check, lib, ptr, stream_ptr
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    n = 3001
+    grad = torch.randn((n, 6), dtype=torch.float64, device="cuda", generator=gen)
+    atoms = torch.randn((n, 4), dtype=torch.float32, device="cuda", generator=gen) * 5
+    m = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    v = torch.zeros_like(m)
+    t = torch.zeros((), dtype=torch.float32, device="cuda")
+    ra, rm, rv = atoms.clone(), m.clone(), v.clone()
+    lr, b1, b2, eps, cols = 0.01, 0.9, 0.999, 1e-8, (0, 2, 3)
+    mask = torch.zeros(4, dtype=torch.float32, device="cuda")
+    mask[list(cols)] = 1.0
+    for k in range(1, 3):
+        check(lib().spm_batch_adam_step(n, ptr(grad), ptr(atoms), ptr(m), ptr(v), ptr(t), lr, b1, b2, eps,
+                                        sum(1 << c for c in cols), stream_ptr()), "spm_batch_adam_step")
+        g = torch.stack([grad[:, 0], grad[:, 1], grad[:, 2], grad[:, 5]], 1).float() * mask
+        rm = rm * b1 + (1 - b1) * g
+        rv = rv * b2 + (1 - b2) * g * g
+        upd = (rm / (1 - b1 ** k)) / ((rv / (1 - b2 ** k)).sqrt() + eps)
+        ra = ra - lr * upd
+        grad = grad * 0.5 + 0.1  # the next step sees another gradient
+        torch.cuda.synchronize()
+        assert float(t) == k
+        torch.testing.assert_close(m, rm, rtol=1e-6, atol=1e-7)
+        torch.testing.assert_close(v, rv, rtol=1e-6, atol=1e-9)
+        torch.testing.assert_close(atoms, ra, rtol=1e-6, atol=1e-6)
+    assert torch.equal(m[:, 1], torch.zeros(n, device="cuda")) and torch.equal(atoms[:, 1], ra[:, 1])
