@@ -69,6 +69,26 @@ def test_argument_errors_are_reported_without_a_device():
     assert rc == _lib.SPM_ERR_ARG
 
 
+def test_adam_step_arguments_are_checked_before_any_launch():
+    """spm_batch_adam_step refuses bad arguments with an error code and text; nothing is launched,
+    so the (never dereferenced) buffer addresses need no device."""
+    L = _lib.lib()
+    p = ctypes.c_void_p(256)
+    ok = (0.01, 0.9, 0.999, 1e-8, 15)
+    rc = L.spm_batch_adam_step(4, None, p, p, p, p, *ok, None)
+    assert rc == _lib.SPM_ERR_ARG and b"null" in L.spm_last_error()
+    rc = L.spm_batch_adam_step(4, p, ctypes.c_void_p(260), p, p, p, *ok, None)
+    assert rc == _lib.SPM_ERR_ARG and b"aligned" in L.spm_last_error()
+    rc = L.spm_batch_adam_step(4, p, p, p, p, p, 0.01, 1.0, 0.999, 1e-8, 15, None)
+    assert rc == _lib.SPM_ERR_ARG and b"beta1" in L.spm_last_error()
+    rc = L.spm_batch_adam_step(4, p, p, p, p, p, 0.01, 0.9, 0.999, 0.0, 15, None)
+    assert rc == _lib.SPM_ERR_ARG and b"eps" in L.spm_last_error()
+    rc = L.spm_batch_adam_step(4, p, p, p, p, p, 0.01, 0.9, 0.999, 1e-8, 16, None)
+    assert rc == _lib.SPM_ERR_ARG and b"cols" in L.spm_last_error()
+    rc = L.spm_batch_adam_step(-1, p, p, p, p, p, *ok, None)
+    assert rc == _lib.SPM_ERR_ARG and b"n_atoms" in L.spm_last_error()
+
+
 def test_check_raises_value_error_for_argument_errors():
     L = _lib.lib()
     v = np.zeros(4, np.float32)
